@@ -1,0 +1,431 @@
+/*
+ * lsmps_b200.h - C ABI of the B200-native LSMPS per-step particle hot path.
+ *
+ * Every entry point below replaces one function or method of the lsmps3D C++
+ * module API (paths are relative to the lsmps-3D project root).  The POD view
+ * structs are layout-identical to the reference's views when the reference is
+ * built with LSMPS3D_USE_DOUBLE (real = double, index_t = int32_t,
+ * size_type = size_t), so a reference view can be passed by address.
+ *
+ * Memory: every device pointer in a view is owned by the caller.  The opaque
+ * context owns only scratch (radix-sort ping-pong buffers, scan partials, the
+ * device status word) and the CUDA stream the work is queued on.
+ *
+ * Errors: no entry point exits the process.  Each returns an lsmps_status; a
+ * human-readable message for the last failure is available from
+ * lsmps_ctx_last_error().  In synchronous mode (the default) each call waits
+ * for its kernels and folds the device-side status (CSR capacity overflow,
+ * non-SPD moment matrices, non-finite coordinates) into the return value.
+ */
+#ifndef LSMPS_B200_H
+#define LSMPS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------- */
+/* Status codes                                                              */
+/* ------------------------------------------------------------------------- */
+typedef enum lsmps_status {
+  LSMPS_OK = 0,
+  /* CSR (or PPE) capacity smaller than required; lsmps_ctx_required() gives
+   * the required entry count.  Reference: std::exit in
+   * src/neighbor/neighbor_search.cu:22-30. */
+  LSMPS_CAPACITY_EXCEEDED = 1,
+  /* Invalid grid, null buffer, size mismatch, radius > cell size, ...
+   * Reference: std::exit in neighbor_search.cu:257-273, 354-361 and the
+   * validate_* helpers of every module. */
+  LSMPS_INVALID_ARGUMENT = 2,
+  /* A consumer was given a moment view that was never prepared.
+   * Reference: moment_matrix.cu:571-576. */
+  LSMPS_NOT_PREPARED = 3,
+  /* At least one moment matrix failed the Cholesky factorisation (its info
+   * entry is > 0).  The reference never checks potrf info
+   * (moment_matrix.cu:438-439); this status is informational and only
+   * returned when the context asks for strict SPD checking. */
+  LSMPS_NON_SPD = 4,
+  LSMPS_CUDA_ERROR = 5,
+  /* A count exceeds the 32-bit index range (reference: neighbor_search.cu:270). */
+  LSMPS_INDEX_OVERFLOW = 6,
+  /* A particle coordinate is NaN or infinite. */
+  LSMPS_NON_FINITE = 7
+} lsmps_status;
+
+typedef enum lsmps_precision {
+  /* Every floating operation in double, the reference's real type. */
+  LSMPS_PRECISION_PLAIN = 0,
+  /* FP32 neighbour geometry and compensated FP32 moment assembly with FP64
+   * refinement; FP64 kept for ill-conditioned matrices and the PPE RHS. */
+  LSMPS_PRECISION_MIXED = 1
+} lsmps_precision;
+
+/* Surface labels: include/lsmps3d/surface/surface_type.cuh:5-10. */
+enum {
+  LSMPS_SURFACE_INNER = 0,
+  LSMPS_SURFACE_NEAR_SURFACE = 1,
+  LSMPS_SURFACE_SURFACE = 2,
+  LSMPS_SURFACE_SPLASH = 3
+};
+
+/* Moment matrix kinds: include/lsmps3d/moment_matrix/moment_matrix.cuh:39-44. */
+typedef enum lsmps_moment_kind {
+  LSMPS_MOMENT_VELOCITY_WALL_DIRICHLET_A = 0,
+  LSMPS_MOMENT_PRESSURE_WALL_NEUMANN_A = 1,
+  LSMPS_MOMENT_PRESSURE_WALL_NEUMANN_B = 2,
+  LSMPS_MOMENT_FLUID_ONLY_A = 3
+} lsmps_moment_kind;
+
+/* ------------------------------------------------------------------------- */
+/* Views (caller-owned device memory)                                        */
+/* ------------------------------------------------------------------------- */
+
+/* lsmps3d::FluidParticleSoA, include/lsmps3d/particle/particle_data.cuh:7-17. */
+typedef struct lsmps_fluid {
+  size_t count;
+  double* x;
+  double* y;
+  double* z;
+  double* vx;
+  double* vy;
+  double* vz;
+  double* pressure;
+  int32_t* surface_type;
+} lsmps_fluid;
+
+/* lsmps3d::WallParticleSoA, particle_data.cuh:19-30. */
+typedef struct lsmps_walls {
+  size_t count;
+  double* x;
+  double* y;
+  double* z;
+  double* vx;
+  double* vy;
+  double* vz;
+  double* normal_x;
+  double* normal_y;
+  double* normal_z;
+} lsmps_walls;
+
+/* lsmps3d::CellGrid, include/lsmps3d/neighbor/cell_list.cuh:7-15. */
+typedef struct lsmps_grid {
+  double origin[3];
+  double cell_size;
+  int32_t dims[3];
+} lsmps_grid;
+
+/* lsmps3d::CellListView, cell_list.cuh:17-24.  particle_count and
+ * cell_count are capacities; cell_ids holds the SORTED cell id of each sorted
+ * position, sorted_indices the particle index at that position, and
+ * cell_begin/cell_end the [first, last+1) sorted range of each cell or -1. */
+typedef struct lsmps_cells {
+  size_t particle_count;
+  size_t cell_count;
+  int32_t* cell_ids;
+  int32_t* sorted_indices;
+  int32_t* cell_begin;
+  int32_t* cell_end;
+} lsmps_cells;
+
+/* lsmps3d::NeighborListView, include/lsmps3d/particle/neighbor_list.cuh:7-12.
+ * neighbor_count is the capacity of indices. */
+typedef struct lsmps_csr {
+  size_t particle_count;
+  size_t neighbor_count;
+  int32_t* offsets;
+  int32_t* indices;
+} lsmps_csr;
+
+/* lsmps3d::ProvisionVelocityView (include/lsmps3d/provision/explicit_update.cuh:11-16)
+ * and lsmps3d::CorrectionVectorView
+ * (include/lsmps3d/correction/pressure_correction.cuh:11-16) share this layout. */
+typedef struct lsmps_vector {
+  size_t count;
+  double* x;
+  double* y;
+  double* z;
+} lsmps_vector;
+
+/* lsmps3d::SurfaceDetectionDiagnosticsView,
+ * include/lsmps3d/surface/surface_detection.cuh:10-21.  Any pointer may be NULL. */
+typedef struct lsmps_surface_diagnostics {
+  int32_t* fluid_neighbor_count;
+  int32_t* wall_neighbor_count;
+  double* number_density;
+  double* number_density_ratio;
+  double* anisotropy;
+  double* air_open_ratio;
+  double* air_anisotropy;
+  double* surface_normal_x;
+  double* surface_normal_y;
+  double* surface_normal_z;
+} lsmps_surface_diagnostics;
+
+/* Output buffers and metadata of one moment-matrix kind: the device side of
+ * lsmps3d::MomentMatrixView (moment_matrix.cuh:46-60).  inverse_matrices holds
+ * particle_count blocks of matrix_size^2 doubles, column-major
+ * ([row + col * n]), full symmetric storage.  moment_trace is the trace
+ * before regularisation, regularization_added the lambda*tr/n added to the
+ * diagonal, info the Cholesky status (0 = SPD, k = leading minor k failed).
+ * inversion_count is a single device int incremented once per build. */
+typedef struct lsmps_moment {
+  size_t particle_count;
+  int32_t matrix_size;
+  int32_t kind;
+  double support_radius;
+  double wall_weight_scale;
+  double* inverse_matrices;
+  double* moment_trace;
+  double* regularization_added;
+  int32_t* info;
+  int32_t* inversion_count;
+} lsmps_moment;
+
+/* lsmps3d::CsrMatrixView, include/lsmps3d/ppe/ppe_matrix.cuh:15-22. */
+typedef struct lsmps_csr_matrix {
+  size_t rows;
+  size_t cols;
+  size_t nnz;
+  int32_t* row_offsets;
+  int32_t* col_indices;
+  double* values;
+} lsmps_csr_matrix;
+
+/* lsmps3d::PpeWorkspaceView, ppe_matrix.cuh:24-30. */
+typedef struct lsmps_ppe {
+  lsmps_csr_matrix matrix;
+  double* rhs;
+  double* pressure;
+  double* divergence;
+  double* pressure_laplacian;
+} lsmps_ppe;
+
+/* The scalar fields of lsmps3d::SimulationConfig (include/lsmps3d/core/config.hpp:12-82)
+ * that hot-path kernels read.  File paths, the INI layer and the time-step
+ * controller fields stay on the host side of the reference and are omitted. */
+typedef struct lsmps_params {
+  double particle_spacing;
+  double support_radius;
+  double near_surface_radius;
+  lsmps_grid grid;
+  double time_step;
+  double density;
+  double kinematic_viscosity;
+  double gravity[3];
+  int32_t splash_neighbor_threshold;
+  int32_t include_wall_neighbors;
+  double number_density_ratio_threshold;
+  double air_open_ratio_threshold;
+  double air_anisotropy_threshold;
+  double wall_normal_independence_threshold;
+  double virtual_light_cone_cosine;
+  double lsmps_regularization;
+  double lsmps_wall_weight_scale;
+  double ps_displacement_scale;
+  double ps_min_distance_ratio;
+  double ps_max_displacement_ratio;
+  double wall_clearance_ratio;
+  double velocity_smoothing_strength;
+} lsmps_params;
+
+/* Every buffer one time step touches.  The step runs, in the reference
+ * driver's order (src/app/simulation_driver.cu:346-383):
+ *   provision -> PPE assembly -> pressure correction -> neighbour rebuild ->
+ *   surface classification,
+ * where the pressure handed to the correction is `pressure` (the PPE solve
+ * is outside this path). */
+typedef struct lsmps_step_state {
+  lsmps_fluid fluid;
+  lsmps_walls walls;
+  lsmps_cells fluid_cells;
+  lsmps_cells wall_cells;
+  lsmps_csr fluid_neighbors;
+  lsmps_csr wall_neighbors;
+  lsmps_fluid temporary_velocity;
+  lsmps_walls temporary_wall_velocity;
+  lsmps_vector velocity_laplacian;
+  lsmps_moment velocity_moment;
+  lsmps_moment pressure_moment;
+  lsmps_ppe ppe;
+  lsmps_vector pressure_gradient;
+  lsmps_vector ps_displacement;
+  lsmps_vector smoothed_velocity;
+  double* pressure;
+} lsmps_step_state;
+
+typedef struct lsmps_ctx lsmps_ctx;
+
+/* ------------------------------------------------------------------------- */
+/* Context                                                                   */
+/* ------------------------------------------------------------------------- */
+lsmps_status lsmps_ctx_create(int device, lsmps_ctx** out);
+void lsmps_ctx_destroy(lsmps_ctx* ctx);
+/* Queue all further work of this context on `stream` (a cudaStream_t; NULL =
+ * the context's own non-blocking stream). */
+lsmps_status lsmps_ctx_set_stream(lsmps_ctx* ctx, void* stream);
+void* lsmps_ctx_stream(lsmps_ctx* ctx);
+lsmps_status lsmps_ctx_set_precision(lsmps_ctx* ctx, int precision);
+/* 1 (default): every call waits for its kernels and returns the device status.
+ * 0: calls only queue work; lsmps_ctx_synchronize() returns the folded status. */
+lsmps_status lsmps_ctx_set_synchronous(lsmps_ctx* ctx, int synchronous);
+/* Pre-size scratch so that no call of this size allocates (needed before
+ * graph capture). */
+lsmps_status lsmps_ctx_reserve(lsmps_ctx* ctx, size_t fluid_capacity, size_t wall_capacity,
+                               size_t cell_capacity);
+lsmps_status lsmps_ctx_synchronize(lsmps_ctx* ctx);
+/* Required entry count recorded by the last LSMPS_CAPACITY_EXCEEDED. */
+uint64_t lsmps_ctx_required(lsmps_ctx* ctx);
+/* Number of kernel launches this context has queued since creation. */
+uint64_t lsmps_ctx_launch_count(lsmps_ctx* ctx);
+const char* lsmps_ctx_last_error(lsmps_ctx* ctx);
+const char* lsmps_status_string(int status);
+/* SimulationConfig defaults (include/lsmps3d/core/config.hpp:12-60). */
+void lsmps_params_default(lsmps_params* out);
+
+/* ------------------------------------------------------------------------- */
+/* Neighbour search: include/lsmps3d/neighbor/neighbor_search.cuh            */
+/* ------------------------------------------------------------------------- */
+/* build_cell_list(FluidParticleSoA|WallParticleSoA, CellGrid, CellListView),
+ * neighbor_search.cuh:10-16.  Stable: particles of one cell keep ascending
+ * index order, as Thrust's stable radix sort_by_key does in the reference. */
+lsmps_status lsmps_build_cell_list(lsmps_ctx* ctx, const double* x, const double* y,
+                                   const double* z, size_t count, const lsmps_grid* grid,
+                                   const lsmps_cells* cells);
+
+/* build_neighbor_lists(...), neighbor_search.cuh:18-24.  Rows follow the
+ * reference traversal order (27 cells dz -> dy -> dx, ascending sorted
+ * position inside each cell); fluid rows exclude the particle itself. */
+lsmps_status lsmps_build_neighbor_lists(lsmps_ctx* ctx, const lsmps_fluid* fluid,
+                                        const lsmps_walls* walls, const lsmps_params* params,
+                                        const lsmps_cells* fluid_cells,
+                                        const lsmps_cells* wall_cells,
+                                        const lsmps_csr* fluid_neighbors,
+                                        const lsmps_csr* wall_neighbors);
+
+/* ------------------------------------------------------------------------- */
+/* Surface detection: include/lsmps3d/surface/surface_detection.cuh          */
+/* ------------------------------------------------------------------------- */
+/* compute_uniform_reference_number_density(real, real), surface_detection.cuh:28
+ * (host loop, surface_detection.cu:494-520).  Returns a negative value on
+ * invalid input. */
+double lsmps_reference_number_density(double particle_spacing, double support_radius);
+
+/* classify_surface_particles(...), surface_detection.cuh:31-36.
+ * diagnostics may be NULL. */
+lsmps_status lsmps_classify_surface(lsmps_ctx* ctx, const lsmps_fluid* fluid,
+                                    const lsmps_walls* walls, const lsmps_csr* fluid_neighbors,
+                                    const lsmps_csr* wall_neighbors, const lsmps_params* params,
+                                    const lsmps_surface_diagnostics* diagnostics);
+
+/* ------------------------------------------------------------------------- */
+/* Moment matrices: include/lsmps3d/moment_matrix/moment_matrix.cuh          */
+/* ------------------------------------------------------------------------- */
+/* Build and invert the moment matrices of `count` kinds at once
+ * (DeviceMomentMatrix::prepare_matrices, moment_matrix.cuh:80-84, without the
+ * host-side generation cache, which the C++/Python owners keep).  Kinds that
+ * share the Type-A fluid sum are assembled in one pass over the rows.  Each
+ * inversion_count is incremented once. */
+lsmps_status lsmps_prepare_moments(lsmps_ctx* ctx, const lsmps_fluid* fluid,
+                                   const lsmps_walls* walls, const lsmps_csr* fluid_neighbors,
+                                   const lsmps_csr* wall_neighbors, const lsmps_params* params,
+                                   const lsmps_moment* kinds, int count);
+
+/* ------------------------------------------------------------------------- */
+/* Provision: include/lsmps3d/provision/explicit_update.cuh                  */
+/* ------------------------------------------------------------------------- */
+/* compute_velocity_laplacian_kernel launch inside
+ * DeviceProvisionExplicitUpdate::compute_temporary_velocity
+ * (src/provision/explicit_update.cu:178-248, 391-395). */
+lsmps_status lsmps_velocity_laplacian(lsmps_ctx* ctx, const lsmps_fluid* fluid,
+                                      const lsmps_walls* walls, const lsmps_csr* fluid_neighbors,
+                                      const lsmps_csr* wall_neighbors,
+                                      const lsmps_moment* velocity_moment,
+                                      const lsmps_vector* laplacian);
+/* compute_provision_temporary_velocity(...), explicit_update.cuh:84-87. */
+lsmps_status lsmps_temporary_velocity(lsmps_ctx* ctx, const lsmps_fluid* fluid,
+                                      const lsmps_params* params, const lsmps_vector* laplacian,
+                                      const lsmps_fluid* temporary_velocity);
+/* compute_provision_temporary_wall_velocity(...), explicit_update.cuh:89-91. */
+lsmps_status lsmps_temporary_wall_velocity(lsmps_ctx* ctx, const lsmps_walls* walls,
+                                           const lsmps_params* params,
+                                           const lsmps_walls* temporary_wall_velocity);
+
+/* ------------------------------------------------------------------------- */
+/* PPE assembly: include/lsmps3d/ppe/ppe_matrix.cuh                          */
+/* ------------------------------------------------------------------------- */
+/* assemble_ppe_matrix_and_rhs(...), ppe_matrix.cuh:120-129.  Row i starts at
+ * i + fluid_offsets[i]; the diagonal comes first, then one slot per fluid
+ * neighbour in CSR order.  Surface and Splash rows are Dirichlet rows. */
+lsmps_status lsmps_assemble_ppe(lsmps_ctx* ctx, const lsmps_fluid* fluid,
+                                const lsmps_walls* walls, const lsmps_params* params,
+                                const lsmps_csr* fluid_neighbors, const lsmps_csr* wall_neighbors,
+                                const lsmps_fluid* temporary_velocity,
+                                const lsmps_walls* temporary_wall_velocity,
+                                const lsmps_moment* velocity_moment,
+                                const lsmps_moment* pressure_moment, const lsmps_ppe* workspace);
+
+/* ------------------------------------------------------------------------- */
+/* Pressure correction: include/lsmps3d/correction/pressure_correction.cuh   */
+/* ------------------------------------------------------------------------- */
+/* clamp_particle_pressure(...), pressure_correction.cuh:91. */
+lsmps_status lsmps_clamp_particle_pressure(lsmps_ctx* ctx, const lsmps_fluid* fluid,
+                                           double* pressure);
+/* compute_pressure_gradient(...), pressure_correction.cuh:93-100. */
+lsmps_status lsmps_pressure_gradient(lsmps_ctx* ctx, const lsmps_fluid* fluid,
+                                     const lsmps_walls* walls, const lsmps_csr* fluid_neighbors,
+                                     const lsmps_csr* wall_neighbors, const double* pressure,
+                                     const lsmps_params* params,
+                                     const lsmps_moment* pressure_moment,
+                                     const lsmps_vector* gradient);
+/* compute_particle_shifting_displacement(...), pressure_correction.cuh:102-107. */
+lsmps_status lsmps_particle_shifting(lsmps_ctx* ctx, const lsmps_fluid* fluid,
+                                     const lsmps_walls* walls, const lsmps_csr* fluid_neighbors,
+                                     const lsmps_csr* wall_neighbors, const lsmps_params* params,
+                                     const lsmps_vector* displacement);
+/* update_velocity_and_position(...), pressure_correction.cuh:109-113. */
+lsmps_status lsmps_update_velocity_position(lsmps_ctx* ctx, const lsmps_fluid* fluid,
+                                            const lsmps_fluid* temporary_velocity,
+                                            const lsmps_params* params,
+                                            const lsmps_vector* gradient,
+                                            const lsmps_vector* displacement);
+/* anti_penetration_kernel launch in DevicePressureCorrection::apply
+ * (src/correction/pressure_correction.cu:404-444, 639-643). */
+lsmps_status lsmps_anti_penetration(lsmps_ctx* ctx, const lsmps_fluid* fluid,
+                                    const lsmps_walls* walls, const lsmps_csr* wall_neighbors,
+                                    const lsmps_params* params);
+/* smooth_particle_velocity(...), pressure_correction.cuh:115-118. */
+lsmps_status lsmps_smooth_particle_velocity(lsmps_ctx* ctx, const lsmps_fluid* fluid,
+                                            const lsmps_csr* fluid_neighbors,
+                                            const lsmps_params* params,
+                                            const lsmps_vector* smoothed_velocity);
+/* DevicePressureCorrection::apply(...) after prepare_matrices,
+ * pressure_correction.cuh:69-76 (src/correction/pressure_correction.cu:598-645):
+ * clamp -> gradient -> shifting -> update -> anti-penetration -> smoothing. */
+lsmps_status lsmps_pressure_correction(lsmps_ctx* ctx, const lsmps_fluid* fluid,
+                                       const lsmps_walls* walls,
+                                       const lsmps_csr* fluid_neighbors,
+                                       const lsmps_csr* wall_neighbors,
+                                       const lsmps_fluid* temporary_velocity, double* pressure,
+                                       const lsmps_params* params,
+                                       const lsmps_moment* pressure_moment,
+                                       const lsmps_vector* gradient,
+                                       const lsmps_vector* displacement,
+                                       const lsmps_vector* smoothed_velocity);
+
+/* ------------------------------------------------------------------------- */
+/* Whole step (src/app/simulation_driver.cu:346-383 minus the solve and I/O) */
+/* ------------------------------------------------------------------------- */
+/* One time step on the state's buffers: moments (velocity and pressure
+ * Type-A, once per geometry) -> provision -> PPE assembly -> correction with
+ * `pressure` -> neighbour rebuild -> surface labels.  Uses the context's
+ * precision mode. */
+lsmps_status lsmps_step(lsmps_ctx* ctx, const lsmps_params* params, const lsmps_step_state* state);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LSMPS_B200_H */

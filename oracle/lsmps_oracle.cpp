@@ -1,0 +1,1147 @@
+// lsmps_oracle.cpp -- TEST INFRASTRUCTURE, not part of the product.
+//
+// CPU FP64 restatement of the lsmps3D per-step hot path, used only by tests/,
+// __graft_entry__.smoke() and the cpu_baseline leg of bench.py as the checker.
+// Each function follows the cited reference kernel (paths relative to the
+// lsmps-3D project root) in the same loop and summation order, one particle
+// per OpenMP iteration.  The reference has no CPU path of its own; its CUDA
+// path is built separately (oracle/Makefile -> oracle/_ref) and pins this
+// restatement on the GPU box.
+//
+// The moment-matrix inverse restates cuSOLVER's batched potrf (lower) +
+// potrs-against-identity-columns with the textbook Cholesky-Banachiewicz
+// factorisation and forward/back substitution (Golub & Van Loan, Alg. 4.2.1);
+// cuSOLVER itself is closed and was not consulted.
+//
+// Built with -ffp-contract=off so that every a*b+c rounds twice, which makes
+// the oracle's results independent of the host CPU's FMA support.
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <limits>
+#include <vector>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#include "lsmps_b200.h"
+
+namespace {
+
+using index_t = int32_t;
+constexpr int kInner = LSMPS_SURFACE_INNER;
+constexpr int kNearSurface = LSMPS_SURFACE_NEAR_SURFACE;
+constexpr int kSurface = LSMPS_SURFACE_SURFACE;
+constexpr int kSplash = LSMPS_SURFACE_SPLASH;
+
+// ---------------------------------------------------------------------------
+// Neighbour search: src/neighbor/neighbor_search.cu
+// ---------------------------------------------------------------------------
+
+// neighbor_search.cu:32-34
+index_t flatten_cell(index_t ix, index_t iy, index_t iz, const int32_t dims[3]) {
+  return (iz * dims[1] + iy) * dims[0] + ix;
+}
+
+// neighbor_search.cu:36-46.  A non-finite coordinate maps to cell 0 (the
+// reference's float->int conversion of NaN is undefined); callers reject
+// such inputs before they get here.
+index_t clamp_cell_index(double coordinate, double origin, double cell_size, index_t dim) {
+  const double scaled = (coordinate - origin) / cell_size;
+  if (!(scaled == scaled)) return 0;
+  const double f = std::floor(scaled);
+  if (f < 0.0) return 0;
+  if (f >= static_cast<double>(dim)) return dim - 1;
+  const index_t index = static_cast<index_t>(f);
+  if (index >= dim) return dim - 1;
+  return index;
+}
+
+// neighbor_search.cu:48-59
+bool within_radius(double ax, double ay, double az, double bx, double by, double bz,
+                   double radius_squared) {
+  const double dx = ax - bx;
+  const double dy = ay - by;
+  const double dz = az - bz;
+  return dx * dx + dy * dy + dz * dz <= radius_squared;
+}
+
+// build_cell_list_impl, neighbor_search.cu:255-292: assign cells (:61-73),
+// stable sort by cell id (:285-287), cell ranges (:75-98).  The stable sort
+// is a counting sort, which keeps ascending particle index inside a cell.
+int cell_list(const double* x, const double* y, const double* z, size_t count,
+              const lsmps_grid* grid, const lsmps_cells* cells) {
+  if (grid->cell_size <= 0.0 || grid->dims[0] <= 0 || grid->dims[1] <= 0 || grid->dims[2] <= 0)
+    return LSMPS_INVALID_ARGUMENT;
+  const int64_t ncell = static_cast<int64_t>(grid->dims[0]) * grid->dims[1] * grid->dims[2];
+  if (ncell > std::numeric_limits<index_t>::max()) return LSMPS_INDEX_OVERFLOW;
+  if (static_cast<size_t>(ncell) != cells->cell_count) return LSMPS_INVALID_ARGUMENT;
+  if (count > cells->particle_count) return LSMPS_INVALID_ARGUMENT;
+  if (count > static_cast<size_t>(std::numeric_limits<index_t>::max())) return LSMPS_INDEX_OVERFLOW;
+  for (int64_t c = 0; c < ncell; ++c) {
+    cells->cell_begin[c] = -1;
+    cells->cell_end[c] = -1;
+  }
+  if (count == 0) return LSMPS_OK;
+  std::vector<index_t> key(count);
+  for (size_t i = 0; i < count; ++i) {
+    const index_t ix = clamp_cell_index(x[i], grid->origin[0], grid->cell_size, grid->dims[0]);
+    const index_t iy = clamp_cell_index(y[i], grid->origin[1], grid->cell_size, grid->dims[1]);
+    const index_t iz = clamp_cell_index(z[i], grid->origin[2], grid->cell_size, grid->dims[2]);
+    key[i] = flatten_cell(ix, iy, iz, grid->dims);
+  }
+  std::vector<int64_t> start(static_cast<size_t>(ncell) + 1, 0);
+  for (size_t i = 0; i < count; ++i) ++start[static_cast<size_t>(key[i]) + 1];
+  for (int64_t c = 0; c < ncell; ++c) start[c + 1] += start[c];
+  std::vector<int64_t> cursor(start.begin(), start.end() - 1);
+  for (size_t i = 0; i < count; ++i) {
+    const int64_t pos = cursor[key[i]]++;
+    cells->cell_ids[pos] = key[i];
+    cells->sorted_indices[pos] = static_cast<index_t>(i);
+  }
+  for (size_t pos = 0; pos < count; ++pos) {
+    const index_t c = cells->cell_ids[pos];
+    if (pos == 0 || cells->cell_ids[pos - 1] != c) cells->cell_begin[c] = static_cast<index_t>(pos);
+    if (pos + 1 == count || cells->cell_ids[pos + 1] != c)
+      cells->cell_end[c] = static_cast<index_t>(pos + 1);
+  }
+  return LSMPS_OK;
+}
+
+// One fluid particle's traversal, shared by count_source_neighbors_for_fluid
+// (neighbor_search.cu:100-159) and write_source_neighbors_for_fluid
+// (:161-219): 27 cells in dz -> dy -> dx order, ascending sorted position.
+template <typename Emit>
+void traverse(size_t i, const lsmps_fluid* fluid, const double* sx, const double* sy,
+              const double* sz, const lsmps_cells* src_cells, const lsmps_grid* grid,
+              double radius_squared, bool exclude_self, Emit emit) {
+  const double px = fluid->x[i];
+  const double py = fluid->y[i];
+  const double pz = fluid->z[i];
+  const index_t cx = clamp_cell_index(px, grid->origin[0], grid->cell_size, grid->dims[0]);
+  const index_t cy = clamp_cell_index(py, grid->origin[1], grid->cell_size, grid->dims[1]);
+  const index_t cz = clamp_cell_index(pz, grid->origin[2], grid->cell_size, grid->dims[2]);
+  for (index_t dz = -1; dz <= 1; ++dz) {
+    const index_t nz = cz + dz;
+    if (nz < 0 || nz >= grid->dims[2]) continue;
+    for (index_t dy = -1; dy <= 1; ++dy) {
+      const index_t ny = cy + dy;
+      if (ny < 0 || ny >= grid->dims[1]) continue;
+      for (index_t dx = -1; dx <= 1; ++dx) {
+        const index_t nx = cx + dx;
+        if (nx < 0 || nx >= grid->dims[0]) continue;
+        const index_t cell = flatten_cell(nx, ny, nz, grid->dims);
+        const index_t begin = src_cells->cell_begin[cell];
+        const index_t end = src_cells->cell_end[cell];
+        if (begin < 0 || end < 0) continue;
+        for (index_t pos = begin; pos < end; ++pos) {
+          const index_t j = src_cells->sorted_indices[pos];
+          if (exclude_self && static_cast<size_t>(j) == i) continue;
+          if (within_radius(px, py, pz, sx[j], sy[j], sz[j], radius_squared)) emit(j);
+        }
+      }
+    }
+  }
+}
+
+// build_one_neighbor_list, neighbor_search.cu:294-333: count, exclusive scan,
+// capacity check, write.
+int one_neighbor_list(const lsmps_fluid* fluid, const double* sx, const double* sy,
+                      const double* sz, const lsmps_cells* src_cells, const lsmps_grid* grid,
+                      double radius, bool exclude_self, const lsmps_csr* out, uint64_t* required) {
+  if (fluid->count > out->particle_count) return LSMPS_INVALID_ARGUMENT;
+  const double r2 = radius * radius;
+  const int64_t n = static_cast<int64_t>(fluid->count);
+  if (n == 0) {
+    out->offsets[0] = 0;
+    *required = 0;
+    return LSMPS_OK;
+  }
+  std::vector<int64_t> counts(n);
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int64_t i = 0; i < n; ++i) {
+    int64_t c = 0;
+    traverse(static_cast<size_t>(i), fluid, sx, sy, sz, src_cells, grid, r2, exclude_self,
+             [&](index_t) { ++c; });
+    counts[i] = c;
+  }
+  int64_t total = 0;
+  for (int64_t i = 0; i < n; ++i) {
+    const int64_t c = counts[i];
+    counts[i] = total;
+    total += c;
+  }
+  *required = static_cast<uint64_t>(total);
+  if (total > std::numeric_limits<index_t>::max()) return LSMPS_INDEX_OVERFLOW;
+  for (int64_t i = 0; i < n; ++i) out->offsets[i] = static_cast<index_t>(counts[i]);
+  out->offsets[n] = static_cast<index_t>(total);
+  if (static_cast<uint64_t>(total) > out->neighbor_count) return LSMPS_CAPACITY_EXCEEDED;
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int64_t i = 0; i < n; ++i) {
+    index_t o = out->offsets[i];
+    traverse(static_cast<size_t>(i), fluid, sx, sy, sz, src_cells, grid, r2, exclude_self,
+             [&](index_t j) { out->indices[o++] = j; });
+  }
+  return LSMPS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Surface detection: src/surface/surface_detection.cu
+// ---------------------------------------------------------------------------
+
+// safe_rsqrt, surface_detection.cu:21-24 (1/sqrt of the clamped value).
+double safe_rsqrt(double value) {
+  const double v = value > 1.0e-20 ? value : 1.0e-20;
+  return 1.0 / std::sqrt(v);
+}
+
+// particle_weight, surface_detection.cu:26-31 (also moment_weight,
+// provision_weight: identical formulas in the other modules).
+double particle_weight(double distance, double support_radius) {
+  if (distance >= support_radius) return 0.0;
+  return 1.0 - distance / support_radius;
+}
+
+// accumulate_neighbor_moments, surface_detection.cu:33-59
+void accumulate_neighbor(double dx, double dy, double dz, double support_radius, double& nd,
+                         double& sx, double& sy, double& sz, int& weighted) {
+  const double d2 = dx * dx + dy * dy + dz * dz;
+  if (d2 <= 0.0) return;
+  const double d = std::sqrt(d2);
+  const double w = particle_weight(d, support_radius);
+  if (w <= 0.0) return;
+  const double inv_d = 1.0 / d;
+  nd += w;
+  sx += w * dx * inv_d;
+  sy += w * dy * inv_d;
+  sz += w * dz * inv_d;
+  ++weighted;
+}
+
+struct WallBasis {
+  int count = 0;
+  double x[3] = {0, 0, 0};
+  double y[3] = {0, 0, 0};
+  double z[3] = {0, 0, 0};
+};
+
+// add_wall_basis_direction, surface_detection.cu:123-149 (Gram-Schmidt)
+void add_wall_basis_direction(WallBasis& b, double x, double y, double z, double threshold) {
+  double rx = x, ry = y, rz = z;
+  for (int k = 0; k < b.count; ++k) {
+    const double proj = rx * b.x[k] + ry * b.y[k] + rz * b.z[k];
+    rx -= proj * b.x[k];
+    ry -= proj * b.y[k];
+    rz -= proj * b.z[k];
+  }
+  const double len2 = rx * rx + ry * ry + rz * rz;
+  if (len2 <= threshold * threshold || b.count >= 3) return;
+  const double inv = safe_rsqrt(len2);
+  b.x[b.count] = rx * inv;
+  b.y[b.count] = ry * inv;
+  b.z[b.count] = rz * inv;
+  ++b.count;
+}
+
+// build_wall_basis, surface_detection.cu:151-197
+WallBasis build_wall_basis(size_t i, const lsmps_fluid* f, const lsmps_walls* w,
+                           const lsmps_csr* wn, const lsmps_params* p) {
+  WallBasis basis;
+  if (!p->include_wall_neighbors) return basis;
+  const double px = f->x[i], py = f->y[i], pz = f->z[i];
+  for (index_t o = wn->offsets[i]; o < wn->offsets[i + 1]; ++o) {
+    const index_t j = wn->indices[o];
+    const double dx = w->x[j] - px, dy = w->y[j] - py, dz = w->z[j] - pz;
+    const double d2 = dx * dx + dy * dy + dz * dz;
+    if (d2 <= 0.0) continue;
+    const double d = std::sqrt(d2);
+    if (particle_weight(d, p->support_radius) <= 0.0) continue;
+    const double nl2 = w->normal_x[j] * w->normal_x[j] + w->normal_y[j] * w->normal_y[j] +
+                       w->normal_z[j] * w->normal_z[j];
+    if (nl2 <= 0.0) continue;
+    const double inv = safe_rsqrt(nl2);
+    add_wall_basis_direction(basis, -w->normal_x[j] * inv, -w->normal_y[j] * inv,
+                             -w->normal_z[j] * inv, p->wall_normal_independence_threshold);
+  }
+  return basis;
+}
+
+// compute_uniform_reference_number_density, surface_detection.cu:494-520
+double reference_number_density(double l0, double re) {
+  if (l0 <= 0.0 || re <= 0.0) return -1.0;
+  const index_t extent = static_cast<index_t>(std::ceil(re / l0));
+  double n0 = 0.0;
+  for (index_t iz = -extent; iz <= extent; ++iz)
+    for (index_t iy = -extent; iy <= extent; ++iy)
+      for (index_t ix = -extent; ix <= extent; ++ix) {
+        if (ix == 0 && iy == 0 && iz == 0) continue;
+        const double dx = static_cast<double>(ix) * l0;
+        const double dy = static_cast<double>(iy) * l0;
+        const double dz = static_cast<double>(iz) * l0;
+        n0 += particle_weight(std::sqrt(dx * dx + dy * dy + dz * dz), re);
+      }
+  return n0;
+}
+
+// ---------------------------------------------------------------------------
+// Moment matrices: src/moment_matrix/moment_matrix.cu
+// ---------------------------------------------------------------------------
+
+// basis_vector, moment_matrix.cu:152-175 (divides by the support radius).
+int basis_vector(double dx, double dy, double dz, bool type_b, double re, double b[10]) {
+  const double sx = dx / re, sy = dy / re, sz = dz / re;
+  int o = 0;
+  if (type_b) b[o++] = 1.0;
+  b[o++] = sx;
+  b[o++] = sy;
+  b[o++] = sz;
+  b[o++] = sx * sx;
+  b[o++] = sy * sy;
+  b[o++] = sz * sz;
+  b[o++] = sx * sy;
+  b[o++] = sy * sz;
+  b[o++] = sz * sx;
+  return o;
+}
+
+// wall_neumann_vector, moment_matrix.cu:177-201
+int wall_neumann_vector(double dx, double dy, double dz, double nx, double ny, double nz,
+                        bool type_b, double re, double q[10]) {
+  int o = 0;
+  const double inv = 1.0 / re;
+  if (type_b) q[o++] = 0.0;
+  q[o++] = nx;
+  q[o++] = ny;
+  q[o++] = nz;
+  q[o++] = 2.0 * dx * nx * inv;
+  q[o++] = 2.0 * dy * ny * inv;
+  q[o++] = 2.0 * dz * nz * inv;
+  q[o++] = (dy * nx + dx * ny) * inv;
+  q[o++] = (dz * ny + dy * nz) * inv;
+  q[o++] = (dx * nz + dz * nx) * inv;
+  return o;
+}
+
+// add_outer_product, moment_matrix.cu:203-209 (full n x n, column-major).
+void add_outer_product(const double* v, int n, double w, double* m) {
+  for (int r = 0; r < n; ++r)
+    for (int c = 0; c < n; ++c) m[r + c * n] += w * v[r] * v[c];
+}
+
+// Request of one kind, make_matrix_request, moment_matrix.cu:494-538.
+struct Request {
+  bool type_b;
+  int boundary;  // 0 none, 1 wall Dirichlet sample, 2 wall pressure Neumann
+};
+
+Request request_of(int kind) {
+  switch (kind) {
+    case LSMPS_MOMENT_VELOCITY_WALL_DIRICHLET_A: return {false, 1};
+    case LSMPS_MOMENT_PRESSURE_WALL_NEUMANN_A: return {false, 2};
+    case LSMPS_MOMENT_PRESSURE_WALL_NEUMANN_B: return {true, 2};
+    default: return {false, 0};
+  }
+}
+
+// build_matrix_cache_kernel, moment_matrix.cu:254-309, for particle i.
+void build_matrix(size_t i, const lsmps_fluid* f, const lsmps_walls* w, const lsmps_csr* fn,
+                  const lsmps_csr* wn, const lsmps_params* p, Request rq, double* m, double* trace,
+                  double* reg) {
+  const int n = rq.type_b ? 10 : 9;
+  const double re = p->support_radius;
+  for (int e = 0; e < n * n; ++e) m[e] = 0.0;
+  const double xi = f->x[i], yi = f->y[i], zi = f->z[i];
+  double b[10];
+  // add_sample_to_matrix, moment_matrix.cu:211-229
+  auto sample = [&](double dx, double dy, double dz, double scale) {
+    const double d2 = dx * dx + dy * dy + dz * dz;
+    if (d2 <= 0.0) return;
+    const double d = std::sqrt(d2);
+    const double wt = scale * particle_weight(d, re);
+    if (wt <= 0.0) return;
+    const int nb = basis_vector(dx, dy, dz, rq.type_b, re, b);
+    add_outer_product(b, nb, wt, m);
+  };
+  for (index_t o = fn->offsets[i]; o < fn->offsets[i + 1]; ++o) {
+    const index_t j = fn->indices[o];
+    sample(f->x[j] - xi, f->y[j] - yi, f->z[j] - zi, 1.0);
+  }
+  if (rq.boundary != 0) {
+    for (index_t o = wn->offsets[i]; o < wn->offsets[i + 1]; ++o) {
+      const index_t j = wn->indices[o];
+      const double dx = w->x[j] - xi, dy = w->y[j] - yi, dz = w->z[j] - zi;
+      if (rq.boundary == 2) {
+        // add_wall_neumann_to_matrix, moment_matrix.cu:231-252
+        const double d2 = dx * dx + dy * dy + dz * dz;
+        if (d2 <= 0.0) continue;
+        const double d = std::sqrt(d2);
+        const double wt = p->lsmps_wall_weight_scale * particle_weight(d, re);
+        if (wt <= 0.0) continue;
+        double q[10];
+        const int nq = wall_neumann_vector(dx, dy, dz, w->normal_x[j], w->normal_y[j],
+                                           w->normal_z[j], rq.type_b, re, q);
+        add_outer_product(q, nq, wt, m);
+      } else {
+        sample(dx, dy, dz, p->lsmps_wall_weight_scale);
+      }
+    }
+  }
+  double tr = 0.0;
+  for (int r = 0; r < n; ++r) tr += m[r + r * n];
+  const double rg = p->lsmps_regularization * (tr > 0.0 ? tr / static_cast<double>(n) : 1.0);
+  for (int r = 0; r < n; ++r) m[r + r * n] += rg;
+  *trace = tr;
+  *reg = rg;
+}
+
+// Cholesky (lower, Banachiewicz order) of the lower triangle of m in place,
+// then the inverse by forward/back substitution against each identity column,
+// i.e. the potrf + potrs sequence of moment_matrix.cu:430-471.
+int cholesky_inverse(double* m, int n, double* inv) {
+  int info = 0;
+  for (int j = 0; j < n; ++j) {
+    double s = m[j + j * n];
+    for (int k = 0; k < j; ++k) s -= m[j + k * n] * m[j + k * n];
+    if (!(s > 0.0)) {
+      info = j + 1;
+      break;
+    }
+    const double ljj = std::sqrt(s);
+    m[j + j * n] = ljj;
+    for (int i = j + 1; i < n; ++i) {
+      double t = m[i + j * n];
+      for (int k = 0; k < j; ++k) t -= m[i + k * n] * m[j + k * n];
+      m[i + j * n] = t / ljj;
+    }
+  }
+  if (info != 0) {
+    for (int e = 0; e < n * n; ++e) inv[e] = std::numeric_limits<double>::quiet_NaN();
+    return info;
+  }
+  double y[10];
+  for (int c = 0; c < n; ++c) {
+    for (int i = 0; i < n; ++i) {  // L y = e_c
+      double t = (i == c) ? 1.0 : 0.0;
+      for (int k = 0; k < i; ++k) t -= m[i + k * n] * y[k];
+      y[i] = t / m[i + i * n];
+    }
+    for (int i = n - 1; i >= 0; --i) {  // L^T x = y
+      double t = y[i];
+      for (int k = i + 1; k < n; ++k) t -= m[k + i * n] * inv[k + c * n];
+      inv[i + c * n] = t / m[i + i * n];
+    }
+  }
+  return 0;
+}
+
+int prepare_moment(const lsmps_fluid* f, const lsmps_walls* w, const lsmps_csr* fn,
+                   const lsmps_csr* wn, const lsmps_params* p, const lsmps_moment* out) {
+  const Request rq = request_of(out->kind);
+  const int n = rq.type_b ? 10 : 9;
+  if (out->matrix_size != n || out->particle_count < f->count) return LSMPS_INVALID_ARGUMENT;
+  const int64_t count = static_cast<int64_t>(f->count);
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int64_t i = 0; i < count; ++i) {
+    double m[100];
+    double tr, rg;
+    build_matrix(static_cast<size_t>(i), f, w, fn, wn, p, rq, m, &tr, &rg);
+    out->moment_trace[i] = tr;
+    out->regularization_added[i] = rg;
+    out->info[i] = cholesky_inverse(m, n, out->inverse_matrices + i * n * n);
+  }
+  if (out->inversion_count) ++out->inversion_count[0];
+  return LSMPS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Provision: src/provision/explicit_update.cu
+// ---------------------------------------------------------------------------
+
+// provision_type_a_basis, explicit_update.cu:128-146 (multiplies by 1/r_e;
+// ppe_type_a_basis and correction_type_a_basis are identical).
+void type_a_basis_inv(double dx, double dy, double dz, double re, double b[9]) {
+  const double inv = 1.0 / re;
+  const double sx = dx * inv, sy = dy * inv, sz = dz * inv;
+  b[0] = sx;
+  b[1] = sy;
+  b[2] = sz;
+  b[3] = sx * sx;
+  b[4] = sy * sy;
+  b[5] = sz * sz;
+  b[6] = sx * sy;
+  b[7] = sy * sz;
+  b[8] = sz * sx;
+}
+
+// accumulate_velocity_rhs, explicit_update.cu:148-162 / ppe_matrix.cu:217-231
+void accumulate_velocity_rhs(const double b[9], double w, double ux, double uy, double uz,
+                             double* rx, double* ry, double* rz) {
+  for (int r = 0; r < 9; ++r) {
+    const double wb = w * b[r];
+    rx[r] += wb * ux;
+    ry[r] += wb * uy;
+    rz[r] += wb * uz;
+  }
+}
+
+// laplacian_from_inverse_rhs, explicit_update.cu:164-176
+double laplacian_from_inverse_rhs(const double* inv, const double* rhs, double re) {
+  double second = 0.0;
+  for (int r = 3; r <= 5; ++r) {
+    double c = 0.0;
+    for (int col = 0; col < 9; ++col) c += inv[r + col * 9] * rhs[col];
+    second += c;
+  }
+  return 2.0 * second / (re * re);
+}
+
+// compute_velocity_laplacian_kernel, explicit_update.cu:178-248
+int velocity_laplacian(const lsmps_fluid* f, const lsmps_walls* w, const lsmps_csr* fn,
+                       const lsmps_csr* wn, const lsmps_moment* vm, const lsmps_vector* lap) {
+  const int64_t count = static_cast<int64_t>(f->count);
+  const double re = vm->support_radius;
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int64_t i = 0; i < count; ++i) {
+    const double xi = f->x[i], yi = f->y[i], zi = f->z[i];
+    double rx[9] = {0}, ry[9] = {0}, rz[9] = {0};
+    double b[9];
+    for (index_t o = fn->offsets[i]; o < fn->offsets[i + 1]; ++o) {
+      const index_t j = fn->indices[o];
+      const double dx = f->x[j] - xi, dy = f->y[j] - yi, dz = f->z[j] - zi;
+      const double d = std::sqrt(dx * dx + dy * dy + dz * dz);
+      const double wt = particle_weight(d, re);
+      if (wt <= 0.0) continue;
+      type_a_basis_inv(dx, dy, dz, re, b);
+      accumulate_velocity_rhs(b, wt, f->vx[j] - f->vx[i], f->vy[j] - f->vy[i],
+                              f->vz[j] - f->vz[i], rx, ry, rz);
+    }
+    for (index_t o = wn->offsets[i]; o < wn->offsets[i + 1]; ++o) {
+      const index_t j = wn->indices[o];
+      const double dx = w->x[j] - xi, dy = w->y[j] - yi, dz = w->z[j] - zi;
+      const double d = std::sqrt(dx * dx + dy * dy + dz * dz);
+      const double wt = vm->wall_weight_scale * particle_weight(d, re);
+      if (wt <= 0.0) continue;
+      type_a_basis_inv(dx, dy, dz, re, b);
+      accumulate_velocity_rhs(b, wt, w->vx[j] - f->vx[i], w->vy[j] - f->vy[i],
+                              w->vz[j] - f->vz[i], rx, ry, rz);
+    }
+    const double* inv = vm->inverse_matrices + i * 81;
+    lap->x[i] = laplacian_from_inverse_rhs(inv, rx, re);
+    lap->y[i] = laplacian_from_inverse_rhs(inv, ry, re);
+    lap->z[i] = laplacian_from_inverse_rhs(inv, rz, re);
+  }
+  return LSMPS_OK;
+}
+
+// combine_explicit_velocity_kernel, explicit_update.cu:250-270
+int temporary_velocity(const lsmps_fluid* f, const lsmps_params* p, const lsmps_vector* lap,
+                       const lsmps_fluid* t) {
+  const int64_t count = static_cast<int64_t>(f->count);
+  for (int64_t i = 0; i < count; ++i) {
+    const bool splash = f->surface_type != nullptr && f->surface_type[i] == kSplash;
+    const double nu = splash ? 0.0 : p->kinematic_viscosity;
+    const double dt = p->time_step;
+    t->vx[i] = f->vx[i] + dt * (nu * lap->x[i] + p->gravity[0]);
+    t->vy[i] = f->vy[i] + dt * (nu * lap->y[i] + p->gravity[1]);
+    t->vz[i] = f->vz[i] + dt * (nu * lap->z[i] + p->gravity[2]);
+  }
+  return LSMPS_OK;
+}
+
+// combine_explicit_wall_velocity_kernel, explicit_update.cu:272-284
+int temporary_wall_velocity(const lsmps_walls* w, const lsmps_params* p, const lsmps_walls* t) {
+  for (size_t i = 0; i < w->count; ++i) {
+    const double dt = p->time_step;
+    t->vx[i] = w->vx[i] + dt * p->gravity[0];
+    t->vy[i] = w->vy[i] + dt * p->gravity[1];
+    t->vz[i] = w->vz[i] + dt * p->gravity[2];
+  }
+  return LSMPS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// PPE assembly: src/ppe/ppe_matrix.cu
+// ---------------------------------------------------------------------------
+
+// ppe_wall_neumann_vector, ppe_matrix.cu:175-193 (Type-A layout)
+void neumann_a(double dx, double dy, double dz, double nx, double ny, double nz, double re,
+               double q[9]) {
+  wall_neumann_vector(dx, dy, dz, nx, ny, nz, false, re, q);
+}
+
+// dot9, ppe_matrix.cu:195-201
+double dot9(const double* a, const double* b) {
+  double v = 0.0;
+  for (int k = 0; k < 9; ++k) v += a[k] * b[k];
+  return v;
+}
+
+// first_coefficient_from_inverse_rhs, ppe_matrix.cu:233-241
+double coefficient_row(const double* inv, const double* rhs, int row) {
+  double c = 0.0;
+  for (int col = 0; col < 9; ++col) c += inv[row + col * 9] * rhs[col];
+  return c;
+}
+
+// build_ppe_row_offsets_kernel + assemble_ppe_system_kernel, ppe_matrix.cu:133-146, 243-370
+int assemble_ppe(const lsmps_fluid* f, const lsmps_walls* w, const lsmps_params* p,
+                 const lsmps_csr* fn, const lsmps_csr* wn, const lsmps_fluid* tv,
+                 const lsmps_walls* tw, const lsmps_moment* vm, const lsmps_moment* pm,
+                 const lsmps_ppe* ws) {
+  const int64_t count = static_cast<int64_t>(f->count);
+  if (count == 0) return LSMPS_OK;
+  for (int64_t i = 0; i < count; ++i)
+    ws->matrix.row_offsets[i] = static_cast<index_t>(i) + fn->offsets[i];
+  ws->matrix.row_offsets[count] = static_cast<index_t>(count) + fn->offsets[count];
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int64_t i = 0; i < count; ++i) {
+    const index_t row_begin = ws->matrix.row_offsets[i];
+    const index_t nb = fn->offsets[i], ne = fn->offsets[i + 1];
+    const int type = f->surface_type ? f->surface_type[i] : kInner;
+    if (f->surface_type && (type == kSurface || type == kSplash)) {
+      ws->matrix.col_indices[row_begin] = static_cast<index_t>(i);
+      ws->matrix.values[row_begin] = 1.0;
+      for (index_t o = nb; o < ne; ++o) {
+        const index_t out = row_begin + 1 + o - nb;
+        ws->matrix.col_indices[out] = fn->indices[o];
+        ws->matrix.values[out] = 0.0;
+      }
+      ws->rhs[i] = 0.0;
+      ws->divergence[i] = 0.0;
+      if (ws->pressure_laplacian) ws->pressure_laplacian[i] = 0.0;
+      continue;
+    }
+    const double xi = f->x[i], yi = f->y[i], zi = f->z[i];
+    const double re = pm->support_radius;
+    double L[9];
+    const double* pinv = pm->inverse_matrices + i * 81;
+    for (int col = 0; col < 9; ++col)
+      L[col] = pinv[3 + col * 9] + pinv[4 + col * 9] + pinv[5 + col * 9];
+    double rx[9] = {0}, ry[9] = {0}, rz[9] = {0};
+    double diag = 0.0;
+    double b[9];
+    for (index_t o = nb; o < ne; ++o) {
+      const index_t j = fn->indices[o];
+      const double dx = f->x[j] - xi, dy = f->y[j] - yi, dz = f->z[j] - zi;
+      const double d = std::sqrt(dx * dx + dy * dy + dz * dz);
+      const double wt = particle_weight(d, re);
+      double off = 0.0;
+      if (wt > 0.0) {
+        type_a_basis_inv(dx, dy, dz, re, b);
+        off = 2.0 * wt * dot9(L, b) / (re * re * p->density);
+        diag -= off;
+        accumulate_velocity_rhs(b, wt, tv->vx[j] - tv->vx[i], tv->vy[j] - tv->vy[i],
+                                tv->vz[j] - tv->vz[i], rx, ry, rz);
+      }
+      const index_t out = row_begin + 1 + o - nb;
+      ws->matrix.col_indices[out] = j;
+      ws->matrix.values[out] = off;
+    }
+    double wall_rhs = 0.0;
+    for (index_t o = wn->offsets[i]; o < wn->offsets[i + 1]; ++o) {
+      const index_t j = wn->indices[o];
+      const double dx = w->x[j] - xi, dy = w->y[j] - yi, dz = w->z[j] - zi;
+      const double d = std::sqrt(dx * dx + dy * dy + dz * dz);
+      const double bw = particle_weight(d, re);
+      if (bw <= 0.0) continue;
+      type_a_basis_inv(dx, dy, dz, re, b);
+      accumulate_velocity_rhs(b, vm->wall_weight_scale * bw, tw->vx[j] - tv->vx[i],
+                              tw->vy[j] - tv->vy[i], tw->vz[j] - tv->vz[i], rx, ry, rz);
+      const double ng = p->gravity[0] * w->normal_x[j] + p->gravity[1] * w->normal_y[j] +
+                        p->gravity[2] * w->normal_z[j];
+      double q[9];
+      neumann_a(dx, dy, dz, w->normal_x[j], w->normal_y[j], w->normal_z[j], re, q);
+      wall_rhs += 2.0 * pm->wall_weight_scale * bw * ng * dot9(L, q) / re;
+    }
+    const double* vinv = vm->inverse_matrices + i * 81;
+    const double div = (coefficient_row(vinv, rx, 0) + coefficient_row(vinv, ry, 1) +
+                        coefficient_row(vinv, rz, 2)) /
+                       re;
+    ws->matrix.col_indices[row_begin] = static_cast<index_t>(i);
+    ws->matrix.values[row_begin] = diag;
+    ws->divergence[i] = div;
+    ws->rhs[i] = div / p->time_step - wall_rhs;
+    if (ws->pressure_laplacian) ws->pressure_laplacian[i] = wall_rhs;
+  }
+  return LSMPS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Pressure correction: src/correction/pressure_correction.cu
+// ---------------------------------------------------------------------------
+
+bool is_splash(const lsmps_fluid* f, size_t i) {  // :113-116
+  return f->surface_type != nullptr && f->surface_type[i] == kSplash;
+}
+bool is_surface(const lsmps_fluid* f, size_t i) {  // :118-125
+  if (f->surface_type == nullptr) return false;
+  const int t = f->surface_type[i];
+  return t == kSurface || t == kSplash;
+}
+double correction_weight(double d, double re) {  // :127-132
+  if (d >= re || d <= 0.0) return 0.0;
+  return 1.0 - d / re;
+}
+
+// clamp_fluid_pressure_kernel, :188-198
+int clamp_pressure(const lsmps_fluid* f, double* p) {
+  for (size_t i = 0; i < f->count; ++i) {
+    const double c = p[i] < 0.0 ? 0.0 : p[i];
+    p[i] = c;
+    if (f->pressure != nullptr && f->pressure != p) f->pressure[i] = c;
+  }
+  return LSMPS_OK;
+}
+
+// compute_pressure_gradient_kernel, :200-276
+int pressure_gradient(const lsmps_fluid* f, const lsmps_walls* w, const lsmps_csr* fn,
+                      const lsmps_csr* wn, const double* pr, const lsmps_params* p,
+                      const lsmps_moment* pm, const lsmps_vector* g) {
+  const int64_t count = static_cast<int64_t>(f->count);
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int64_t i = 0; i < count; ++i) {
+    if (is_splash(f, i)) {
+      g->x[i] = g->y[i] = g->z[i] = 0.0;
+      continue;
+    }
+    const double xi = f->x[i], yi = f->y[i], zi = f->z[i];
+    const double re = pm->support_radius;
+    double rhs[9] = {0};
+    double b[9];
+    for (index_t o = fn->offsets[i]; o < fn->offsets[i + 1]; ++o) {
+      const index_t j = fn->indices[o];
+      const double dx = f->x[j] - xi, dy = f->y[j] - yi, dz = f->z[j] - zi;
+      const double d = std::sqrt(dx * dx + dy * dy + dz * dz);
+      const double wt = correction_weight(d, re);
+      if (wt <= 0.0) continue;
+      type_a_basis_inv(dx, dy, dz, re, b);
+      const double dp = pr[j] - pr[i];
+      for (int r = 0; r < 9; ++r) rhs[r] += wt * b[r] * dp;
+    }
+    for (index_t o = wn->offsets[i]; o < wn->offsets[i + 1]; ++o) {
+      const index_t j = wn->indices[o];
+      const double dx = w->x[j] - xi, dy = w->y[j] - yi, dz = w->z[j] - zi;
+      const double d = std::sqrt(dx * dx + dy * dy + dz * dz);
+      const double wt = pm->wall_weight_scale * correction_weight(d, re);
+      if (wt <= 0.0) continue;
+      double q[9];
+      neumann_a(dx, dy, dz, w->normal_x[j], w->normal_y[j], w->normal_z[j], re, q);
+      const double ng = p->gravity[0] * w->normal_x[j] + p->gravity[1] * w->normal_y[j] +
+                        p->gravity[2] * w->normal_z[j];
+      const double wr = re * p->density * ng;
+      for (int r = 0; r < 9; ++r) rhs[r] += wt * q[r] * wr;
+    }
+    const double* inv = pm->inverse_matrices + i * 81;
+    g->x[i] = coefficient_row(inv, rhs, 0) / re;
+    g->y[i] = coefficient_row(inv, rhs, 1) / re;
+    g->z[i] = coefficient_row(inv, rhs, 2) / re;
+  }
+  return LSMPS_OK;
+}
+
+// compute_particle_shifting_kernel, :278-367
+int particle_shifting(const lsmps_fluid* f, const lsmps_walls* w, const lsmps_csr* fn,
+                      const lsmps_csr* wn, const lsmps_params* p, const lsmps_vector* s) {
+  const int64_t count = static_cast<int64_t>(f->count);
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int64_t i = 0; i < count; ++i) {
+    if (p->ps_displacement_scale <= 0.0 || is_splash(f, i)) {
+      s->x[i] = s->y[i] = s->z[i] = 0.0;
+      continue;
+    }
+    const double xi = f->x[i], yi = f->y[i], zi = f->z[i];
+    const double dmin = p->ps_min_distance_ratio * p->particle_spacing;
+    const double smax = p->ps_max_displacement_ratio * p->particle_spacing;
+    double shx = 0, shy = 0, shz = 0, nx = 0, ny = 0, nz = 0;
+    for (index_t o = fn->offsets[i]; o < fn->offsets[i + 1]; ++o) {
+      const index_t j = fn->indices[o];
+      const double dx = xi - f->x[j], dy = yi - f->y[j], dz = zi - f->z[j];
+      const double d = std::sqrt(dx * dx + dy * dy + dz * dz);
+      if (d <= 0.0 || d >= dmin) continue;
+      const double push = p->ps_displacement_scale * (dmin - d) / d;
+      shx += push * dx;
+      shy += push * dy;
+      shz += push * dz;
+      nx += dx / d;
+      ny += dy / d;
+      nz += dz / d;
+    }
+    for (index_t o = wn->offsets[i]; o < wn->offsets[i + 1]; ++o) {
+      const index_t j = wn->indices[o];
+      const double dx = xi - w->x[j], dy = yi - w->y[j], dz = zi - w->z[j];
+      const double d = std::sqrt(dx * dx + dy * dy + dz * dz);
+      if (d <= 0.0 || d >= dmin) continue;
+      const double push = p->ps_displacement_scale * (dmin - d);
+      shx += push * w->normal_x[j];
+      shy += push * w->normal_y[j];
+      shz += push * w->normal_z[j];
+    }
+    if (is_surface(f, i)) {
+      const double nn = std::sqrt(nx * nx + ny * ny + nz * nz);
+      if (nn > 0.0) {
+        nx /= nn;
+        ny /= nn;
+        nz /= nn;
+        const double nc = shx * nx + shy * ny + shz * nz;
+        shx -= nc * nx;
+        shy -= nc * ny;
+        shz -= nc * nz;
+      }
+    }
+    const double sn = std::sqrt(shx * shx + shy * shy + shz * shz);
+    if (sn > smax && sn > 0.0) {
+      const double sc = smax / sn;
+      shx *= sc;
+      shy *= sc;
+      shz *= sc;
+    }
+    s->x[i] = shx;
+    s->y[i] = shy;
+    s->z[i] = shz;
+  }
+  return LSMPS_OK;
+}
+
+// update_velocity_position_kernel, :369-402
+int update_velocity_position(const lsmps_fluid* f, const lsmps_fluid* t, const lsmps_params* p,
+                             const lsmps_vector* g, const lsmps_vector* s) {
+  for (size_t i = 0; i < f->count; ++i) {
+    const bool splash = is_splash(f, i);
+    const double ox = f->vx[i], oy = f->vy[i], oz = f->vz[i];
+    double nx = t->vx[i], ny = t->vy[i], nz = t->vz[i];
+    if (!splash) {
+      const double sc = p->time_step / p->density;
+      nx -= sc * g->x[i];
+      ny -= sc * g->y[i];
+      nz -= sc * g->z[i];
+    }
+    f->x[i] += 0.5 * p->time_step * (ox + nx) + s->x[i];
+    f->y[i] += 0.5 * p->time_step * (oy + ny) + s->y[i];
+    f->z[i] += 0.5 * p->time_step * (oz + nz) + s->z[i];
+    f->vx[i] = nx;
+    f->vy[i] = ny;
+    f->vz[i] = nz;
+  }
+  return LSMPS_OK;
+}
+
+// anti_penetration_kernel, :404-444 (sequential over the wall row)
+int anti_penetration(const lsmps_fluid* f, const lsmps_walls* w, const lsmps_csr* wn,
+                     const lsmps_params* p) {
+  const double clearance = p->wall_clearance_ratio * p->particle_spacing;
+  if (clearance <= 0.0) return LSMPS_OK;
+  const int64_t count = static_cast<int64_t>(f->count);
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int64_t i = 0; i < count; ++i) {
+    for (index_t o = wn->offsets[i]; o < wn->offsets[i + 1]; ++o) {
+      const index_t j = wn->indices[o];
+      const double dx = f->x[i] - w->x[j], dy = f->y[i] - w->y[j], dz = f->z[i] - w->z[j];
+      const double sd = dx * w->normal_x[j] + dy * w->normal_y[j] + dz * w->normal_z[j];
+      if (sd >= clearance) continue;
+      const double c = clearance - sd;
+      f->x[i] += c * w->normal_x[j];
+      f->y[i] += c * w->normal_y[j];
+      f->z[i] += c * w->normal_z[j];
+      const double nv = f->vx[i] * w->normal_x[j] + f->vy[i] * w->normal_y[j] +
+                        f->vz[i] * w->normal_z[j];
+      if (nv < 0.0) {
+        f->vx[i] -= nv * w->normal_x[j];
+        f->vy[i] -= nv * w->normal_y[j];
+        f->vz[i] -= nv * w->normal_z[j];
+      }
+    }
+  }
+  return LSMPS_OK;
+}
+
+// smooth_velocity_kernel + copy_smoothed_velocity_kernel, :446-515
+int smooth_velocity(const lsmps_fluid* f, const lsmps_csr* fn, const lsmps_params* p,
+                    const lsmps_vector* sm) {
+  const int64_t count = static_cast<int64_t>(f->count);
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int64_t i = 0; i < count; ++i) {
+    if (p->velocity_smoothing_strength <= 0.0 || is_splash(f, i)) {
+      sm->x[i] = f->vx[i];
+      sm->y[i] = f->vy[i];
+      sm->z[i] = f->vz[i];
+      continue;
+    }
+    double ws = 0, ax = 0, ay = 0, az = 0;
+    const double xi = f->x[i], yi = f->y[i], zi = f->z[i];
+    for (index_t o = fn->offsets[i]; o < fn->offsets[i + 1]; ++o) {
+      const index_t j = fn->indices[o];
+      if (is_splash(f, j)) continue;
+      const double dx = f->x[j] - xi, dy = f->y[j] - yi, dz = f->z[j] - zi;
+      const double d = std::sqrt(dx * dx + dy * dy + dz * dz);
+      const double wt = correction_weight(d, p->support_radius);
+      if (wt <= 0.0) continue;
+      ws += wt;
+      ax += wt * f->vx[j];
+      ay += wt * f->vy[j];
+      az += wt * f->vz[j];
+    }
+    if (ws <= 0.0) {
+      sm->x[i] = f->vx[i];
+      sm->y[i] = f->vy[i];
+      sm->z[i] = f->vz[i];
+      continue;
+    }
+    double a = p->velocity_smoothing_strength;
+    a = a < 0.0 ? 0.0 : (a > 1.0 ? 1.0 : a);
+    sm->x[i] = (1.0 - a) * f->vx[i] + a * ax / ws;
+    sm->y[i] = (1.0 - a) * f->vy[i] + a * ay / ws;
+    sm->z[i] = (1.0 - a) * f->vz[i] + a * az / ws;
+  }
+  for (int64_t i = 0; i < count; ++i) {
+    f->vx[i] = sm->x[i];
+    f->vy[i] = sm->y[i];
+    f->vz[i] = sm->z[i];
+  }
+  return LSMPS_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI of the oracle (host pointers in the same view structs)
+// ---------------------------------------------------------------------------
+extern "C" {
+
+int oracle_build_cell_list(const double* x, const double* y, const double* z, size_t count,
+                           const lsmps_grid* grid, const lsmps_cells* cells) {
+  return cell_list(x, y, z, count, grid, cells);
+}
+
+// build_neighbor_lists, neighbor_search.cu:345-367.  required[0..1] receive
+// the fluid and wall CSR totals.
+int oracle_build_neighbor_lists(const lsmps_fluid* f, const lsmps_walls* w, const lsmps_params* p,
+                                const lsmps_cells* fc, const lsmps_cells* wc, const lsmps_csr* fn,
+                                const lsmps_csr* wn, uint64_t* required) {
+  const double radius = p->support_radius;
+  if (radius <= 0.0 || radius > p->grid.cell_size) return LSMPS_INVALID_ARGUMENT;
+  int st = cell_list(f->x, f->y, f->z, f->count, &p->grid, fc);
+  if (st) return st;
+  st = cell_list(w->x, w->y, w->z, w->count, &p->grid, wc);
+  if (st) return st;
+  st = one_neighbor_list(f, f->x, f->y, f->z, fc, &p->grid, radius, true, fn, &required[0]);
+  if (st) return st;
+  return one_neighbor_list(f, w->x, w->y, w->z, wc, &p->grid, radius, false, wn, &required[1]);
+}
+
+double oracle_reference_number_density(double l0, double re) {
+  return reference_number_density(l0, re);
+}
+
+// classify_surface_particles, surface_detection.cu:522-553:
+// classify_primary_surface_kernel (:199-320) then expand_near_surface_kernel (:322-348).
+int oracle_classify_surface(const lsmps_fluid* f, const lsmps_walls* w, const lsmps_csr* fn,
+                            const lsmps_csr* wn, const lsmps_params* p,
+                            const lsmps_surface_diagnostics* diag) {
+  if (p->support_radius <= 0.0 || p->near_surface_radius < 0.0) return LSMPS_INVALID_ARGUMENT;
+  const double n0 = reference_number_density(p->particle_spacing, p->support_radius);
+  if (!(n0 > 0.0)) return LSMPS_INVALID_ARGUMENT;
+  const int64_t count = static_cast<int64_t>(f->count);
+  lsmps_surface_diagnostics none;
+  std::memset(&none, 0, sizeof(none));
+  const lsmps_surface_diagnostics* dg = diag ? diag : &none;
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int64_t i = 0; i < count; ++i) {
+    const index_t fc = fn->offsets[i + 1] - fn->offsets[i];
+    const index_t wc = wn->offsets[i + 1] - wn->offsets[i];
+    const index_t cls = p->include_wall_neighbors ? fc + wc : fc;
+    double nd = 0, sx = 0, sy = 0, sz = 0;
+    int weighted = 0;
+    const double px = f->x[i], py = f->y[i], pz = f->z[i];
+    for (index_t o = fn->offsets[i]; o < fn->offsets[i + 1]; ++o) {
+      const index_t j = fn->indices[o];
+      accumulate_neighbor(f->x[j] - px, f->y[j] - py, f->z[j] - pz, p->support_radius, nd, sx, sy,
+                          sz, weighted);
+    }
+    if (p->include_wall_neighbors) {
+      for (index_t o = wn->offsets[i]; o < wn->offsets[i + 1]; ++o) {
+        const index_t j = wn->indices[o];
+        accumulate_neighbor(w->x[j] - px, w->y[j] - py, w->z[j] - pz, p->support_radius, nd, sx,
+                            sy, sz, weighted);
+      }
+    }
+    double aniso = 0.0;
+    if (weighted > 0) aniso = std::sqrt(sx * sx + sy * sy + sz * sz) / static_cast<double>(weighted);
+    const double ratio = nd / n0;
+    const double mx = -sx, my = -sy, mz = -sz;
+    const double ml2 = mx * mx + my * my + mz * mz;
+    double ax = mx, ay = my, az = mz;
+    if (ml2 > 0.0) {
+      const WallBasis basis = build_wall_basis(static_cast<size_t>(i), f, w, wn, p);
+      for (int k = 0; k < basis.count; ++k) {
+        const double proj = ax * basis.x[k] + ay * basis.y[k] + az * basis.z[k];
+        if (proj > 0.0) {
+          ax -= proj * basis.x[k];
+          ay -= proj * basis.y[k];
+          az -= proj * basis.z[k];
+        }
+      }
+    }
+    const double al2 = ax * ax + ay * ay + az * az;
+    const double al = std::sqrt(al2);
+    const double ml = std::sqrt(ml2);
+    const double open = ml > 0.0 ? al / ml : 0.0;
+    const double aaniso = weighted > 0 ? al / static_cast<double>(weighted) : 0.0;
+    double snx = 0, sny = 0, snz = 0;
+    if (al2 > 0.0) {
+      const double inv = safe_rsqrt(al2);
+      snx = ax * inv;
+      sny = ay * inv;
+      snz = az * inv;
+    }
+    int type = kInner;
+    if (cls < p->splash_neighbor_threshold) {
+      type = kSplash;
+    } else if (ratio < p->number_density_ratio_threshold && open > p->air_open_ratio_threshold &&
+               aaniso > p->air_anisotropy_threshold) {
+      type = kSurface;
+    }
+    f->surface_type[i] = type;
+    if (dg->fluid_neighbor_count) dg->fluid_neighbor_count[i] = fc;
+    if (dg->wall_neighbor_count) dg->wall_neighbor_count[i] = wc;
+    if (dg->number_density) dg->number_density[i] = nd;
+    if (dg->number_density_ratio) dg->number_density_ratio[i] = ratio;
+    if (dg->anisotropy) dg->anisotropy[i] = aniso;
+    if (dg->air_open_ratio) dg->air_open_ratio[i] = open;
+    if (dg->air_anisotropy) dg->air_anisotropy[i] = aaniso;
+    if (dg->surface_normal_x) dg->surface_normal_x[i] = snx;
+    if (dg->surface_normal_y) dg->surface_normal_y[i] = sny;
+    if (dg->surface_normal_z) dg->surface_normal_z[i] = snz;
+  }
+  if (p->near_surface_radius > 0.0) {
+    const double r2 = p->near_surface_radius * p->near_surface_radius;
+    // Labels only move Inner -> NearSurface and the test reads Surface, so
+    // the order of this pass does not matter (as in the reference kernel).
+#pragma omp parallel for schedule(dynamic, 256)
+    for (int64_t i = 0; i < count; ++i) {
+      if (f->surface_type[i] != kInner) continue;
+      const double px = f->x[i], py = f->y[i], pz = f->z[i];
+      for (index_t o = fn->offsets[i]; o < fn->offsets[i + 1]; ++o) {
+        const index_t j = fn->indices[o];
+        if (f->surface_type[j] != kSurface) continue;
+        const double dx = f->x[j] - px, dy = f->y[j] - py, dz = f->z[j] - pz;
+        if (dx * dx + dy * dy + dz * dz <= r2) {
+          f->surface_type[i] = kNearSurface;
+          break;
+        }
+      }
+    }
+  }
+  return LSMPS_OK;
+}
+
+int oracle_prepare_moment(const lsmps_fluid* f, const lsmps_walls* w, const lsmps_csr* fn,
+                          const lsmps_csr* wn, const lsmps_params* p, const lsmps_moment* out) {
+  return prepare_moment(f, w, fn, wn, p, out);
+}
+
+int oracle_velocity_laplacian(const lsmps_fluid* f, const lsmps_walls* w, const lsmps_csr* fn,
+                              const lsmps_csr* wn, const lsmps_moment* vm,
+                              const lsmps_vector* lap) {
+  return velocity_laplacian(f, w, fn, wn, vm, lap);
+}
+
+int oracle_temporary_velocity(const lsmps_fluid* f, const lsmps_params* p,
+                              const lsmps_vector* lap, const lsmps_fluid* t) {
+  return temporary_velocity(f, p, lap, t);
+}
+
+int oracle_temporary_wall_velocity(const lsmps_walls* w, const lsmps_params* p,
+                                   const lsmps_walls* t) {
+  return temporary_wall_velocity(w, p, t);
+}
+
+int oracle_assemble_ppe(const lsmps_fluid* f, const lsmps_walls* w, const lsmps_params* p,
+                        const lsmps_csr* fn, const lsmps_csr* wn, const lsmps_fluid* tv,
+                        const lsmps_walls* tw, const lsmps_moment* vm, const lsmps_moment* pm,
+                        const lsmps_ppe* ws) {
+  return assemble_ppe(f, w, p, fn, wn, tv, tw, vm, pm, ws);
+}
+
+int oracle_clamp_pressure(const lsmps_fluid* f, double* p) { return clamp_pressure(f, p); }
+
+int oracle_pressure_gradient(const lsmps_fluid* f, const lsmps_walls* w, const lsmps_csr* fn,
+                             const lsmps_csr* wn, const double* pr, const lsmps_params* p,
+                             const lsmps_moment* pm, const lsmps_vector* g) {
+  return pressure_gradient(f, w, fn, wn, pr, p, pm, g);
+}
+
+int oracle_particle_shifting(const lsmps_fluid* f, const lsmps_walls* w, const lsmps_csr* fn,
+                             const lsmps_csr* wn, const lsmps_params* p, const lsmps_vector* s) {
+  return particle_shifting(f, w, fn, wn, p, s);
+}
+
+int oracle_update_velocity_position(const lsmps_fluid* f, const lsmps_fluid* t,
+                                    const lsmps_params* p, const lsmps_vector* g,
+                                    const lsmps_vector* s) {
+  return update_velocity_position(f, t, p, g, s);
+}
+
+int oracle_anti_penetration(const lsmps_fluid* f, const lsmps_walls* w, const lsmps_csr* wn,
+                            const lsmps_params* p) {
+  return anti_penetration(f, w, wn, p);
+}
+
+int oracle_smooth_velocity(const lsmps_fluid* f, const lsmps_csr* fn, const lsmps_params* p,
+                           const lsmps_vector* sm) {
+  return smooth_velocity(f, fn, p, sm);
+}
+
+// DevicePressureCorrection::apply, pressure_correction.cu:598-645 (after the
+// moment preparation, whose pressure view is passed in).
+int oracle_pressure_correction(const lsmps_fluid* f, const lsmps_walls* w, const lsmps_csr* fn,
+                               const lsmps_csr* wn, const lsmps_fluid* tv, double* pr,
+                               const lsmps_params* p, const lsmps_moment* pm,
+                               const lsmps_vector* g, const lsmps_vector* s,
+                               const lsmps_vector* sm) {
+  clamp_pressure(f, pr);
+  pressure_gradient(f, w, fn, wn, pr, p, pm, g);
+  particle_shifting(f, w, fn, wn, p, s);
+  update_velocity_position(f, tv, p, g, s);
+  anti_penetration(f, w, wn, p);
+  return smooth_velocity(f, fn, p, sm);
+}
+
+// One benchmark step (simulation_driver.cu:346-383 minus solve and I/O).
+// The moments are built for the state's current geometry (the caller's CSR
+// and labels), as the driver's prepare_matrices cache does once per generation.
+int oracle_step(const lsmps_params* p, const lsmps_step_state* s, uint64_t* required) {
+  int st = prepare_moment(&s->fluid, &s->walls, &s->fluid_neighbors, &s->wall_neighbors, p,
+                          &s->velocity_moment);
+  if (st) return st;
+  st = prepare_moment(&s->fluid, &s->walls, &s->fluid_neighbors, &s->wall_neighbors, p,
+                      &s->pressure_moment);
+  if (st) return st;
+  velocity_laplacian(&s->fluid, &s->walls, &s->fluid_neighbors, &s->wall_neighbors,
+                     &s->velocity_moment, &s->velocity_laplacian);
+  temporary_velocity(&s->fluid, p, &s->velocity_laplacian, &s->temporary_velocity);
+  temporary_wall_velocity(&s->walls, p, &s->temporary_wall_velocity);
+  assemble_ppe(&s->fluid, &s->walls, p, &s->fluid_neighbors, &s->wall_neighbors,
+               &s->temporary_velocity, &s->temporary_wall_velocity, &s->velocity_moment,
+               &s->pressure_moment, &s->ppe);
+  oracle_pressure_correction(&s->fluid, &s->walls, &s->fluid_neighbors, &s->wall_neighbors,
+                             &s->temporary_velocity, s->pressure, p, &s->pressure_moment,
+                             &s->pressure_gradient, &s->ps_displacement, &s->smoothed_velocity);
+  st = oracle_build_neighbor_lists(&s->fluid, &s->walls, p, &s->fluid_cells, &s->wall_cells,
+                                   &s->fluid_neighbors, &s->wall_neighbors, required);
+  if (st) return st;
+  return oracle_classify_surface(&s->fluid, &s->walls, &s->fluid_neighbors, &s->wall_neighbors, p,
+                                 nullptr);
+}
+
+int oracle_max_threads() {
+#ifdef _OPENMP
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
+}
+
+}  // extern "C"
