@@ -1,0 +1,156 @@
+"""Device API: a thin Python layer over the C ABI (include/lsmps_b200.h).
+
+Every call goes through liblsmps_b200.so; there is no CPU fallback and the
+module raises at import time if the library is missing.  Device memory comes
+from torch (plumbing only), see buffers.TorchAlloc.
+
+Errors: the reference exits the process on a failed check; here a non-OK
+status raises LsmpsError carrying the status code and the library's message.
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+from . import abi
+from .buffers import StepBuffers, TorchAlloc
+
+_lib = abi.load_library()
+
+
+class LsmpsError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{abi.STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+        self.message = message
+
+
+def r(x):
+    return ctypes.byref(x)
+
+
+def reference_number_density(particle_spacing: float, support_radius: float) -> float:
+    """compute_uniform_reference_number_density (surface_detection.cuh:28)."""
+    v = float(_lib.lsmps_reference_number_density(particle_spacing, support_radius))
+    if v <= 0.0:
+        raise LsmpsError(abi.INVALID_ARGUMENT, "Reference number density requires positive spacing and support radius")
+    return v
+
+
+class Context:
+    """Owns one lsmps_ctx (stream, scratch, device status)."""
+
+    def __init__(self, device: int = 0, precision: int = abi.PRECISION_PLAIN, synchronous: bool = True,
+                 use_torch_stream: bool = True):
+        import torch
+
+        self.torch = torch
+        self.device = device
+        h = ctypes.c_void_p()
+        st = _lib.lsmps_ctx_create(device, ctypes.byref(h))
+        if st != abi.OK:
+            raise LsmpsError(st, "lsmps_ctx_create failed")
+        self.h = h
+        if use_torch_stream:
+            s = torch.cuda.current_stream(device)
+            _lib.lsmps_ctx_set_stream(self.h, ctypes.c_void_p(s.cuda_stream))
+        self.set_precision(precision)
+        self.set_synchronous(synchronous)
+
+    def close(self):
+        if getattr(self, "h", None):
+            _lib.lsmps_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- context controls ---------------------------------------------------
+    def check(self, st: int) -> None:
+        if st != abi.OK:
+            msg = _lib.lsmps_ctx_last_error(self.h)
+            raise LsmpsError(st, msg.decode() if msg else "")
+
+    def set_precision(self, precision: int) -> None:
+        self.check(_lib.lsmps_ctx_set_precision(self.h, precision))
+
+    def set_synchronous(self, sync: bool) -> None:
+        self.check(_lib.lsmps_ctx_set_synchronous(self.h, 1 if sync else 0))
+
+    def set_stream(self, stream_handle: int | None) -> None:
+        self.check(_lib.lsmps_ctx_set_stream(self.h, ctypes.c_void_p(stream_handle or 0)))
+
+    def reserve(self, n_fluid: int, n_wall: int, n_cells: int) -> None:
+        self.check(_lib.lsmps_ctx_reserve(self.h, n_fluid, n_wall, n_cells))
+
+    def synchronize(self) -> None:
+        self.check(_lib.lsmps_ctx_synchronize(self.h))
+
+    @property
+    def required(self) -> int:
+        return int(_lib.lsmps_ctx_required(self.h))
+
+    @property
+    def launch_count(self) -> int:
+        return int(_lib.lsmps_ctx_launch_count(self.h))
+
+    # -- hot-path operations on a StepBuffers --------------------------------
+    def build_cell_list(self, x_ptr: int, y_ptr: int, z_ptr: int, count: int, grid: abi.Grid, cells: abi.Cells):
+        self.check(_lib.lsmps_build_cell_list(self.h, x_ptr, y_ptr, z_ptr, count, r(grid), r(cells)))
+
+    def build_neighbor_lists(self, b: StepBuffers, params: abi.Params) -> None:
+        self.check(_lib.lsmps_build_neighbor_lists(
+            self.h, r(b.fluid_view()), r(b.walls_view()), r(params), r(b.cells_view("fluid")),
+            r(b.cells_view("wall")), r(b.csr_view("fluid")), r(b.csr_view("wall"))))
+
+    def classify_surface(self, b: StepBuffers, params: abi.Params, diagnostics: abi.SurfaceDiagnostics | None = None):
+        self.check(_lib.lsmps_classify_surface(
+            self.h, r(b.fluid_view()), r(b.walls_view()), r(b.csr_view("fluid")), r(b.csr_view("wall")),
+            r(params), r(diagnostics) if diagnostics is not None else None))
+
+    def prepare_moments(self, b: StepBuffers, params: abi.Params, kinds) -> None:
+        b.params_for_moment = params
+        arr = (abi.Moment * len(kinds))(*[b.moment_view(k) for k in kinds])
+        self.check(_lib.lsmps_prepare_moments(self.h, r(b.fluid_view()), r(b.walls_view()), r(b.csr_view("fluid")),
+                                              r(b.csr_view("wall")), r(params), arr, len(kinds)))
+
+    def provision(self, b: StepBuffers, params: abi.Params) -> None:
+        b.params_for_moment = params
+        lap = b.vector_view(b.velocity_laplacian)
+        self.check(_lib.lsmps_velocity_laplacian(
+            self.h, r(b.fluid_view()), r(b.walls_view()), r(b.csr_view("fluid")), r(b.csr_view("wall")),
+            r(b.moment_view(abi.VELOCITY_WALL_DIRICHLET_A)), r(lap)))
+        self.check(_lib.lsmps_temporary_velocity(self.h, r(b.fluid_view()), r(params), r(lap), r(b.temporary_view())))
+        self.check(_lib.lsmps_temporary_wall_velocity(self.h, r(b.walls_view()), r(params),
+                                                      r(b.temporary_walls_view())))
+
+    def assemble_ppe(self, b: StepBuffers, params: abi.Params) -> None:
+        b.params_for_moment = params
+        self.check(_lib.lsmps_assemble_ppe(
+            self.h, r(b.fluid_view()), r(b.walls_view()), r(params), r(b.csr_view("fluid")), r(b.csr_view("wall")),
+            r(b.temporary_view()), r(b.temporary_walls_view()), r(b.moment_view(abi.VELOCITY_WALL_DIRICHLET_A)),
+            r(b.moment_view(abi.PRESSURE_WALL_NEUMANN_A)), r(b.ppe_view())))
+
+    def pressure_correction(self, b: StepBuffers, params: abi.Params, pressure_ptr: int | None = None) -> None:
+        b.params_for_moment = params
+        p = pressure_ptr if pressure_ptr is not None else b.alloc.ptr(b.fluid["pressure"])
+        self.check(_lib.lsmps_pressure_correction(
+            self.h, r(b.fluid_view()), r(b.walls_view()), r(b.csr_view("fluid")), r(b.csr_view("wall")),
+            r(b.temporary_view()), ctypes.c_void_p(p), r(params), r(b.moment_view(abi.PRESSURE_WALL_NEUMANN_A)),
+            r(b.vector_view(b.pressure_gradient)), r(b.vector_view(b.ps_displacement)),
+            r(b.vector_view(b.smoothed_velocity))))
+
+    def step(self, b: StepBuffers, params: abi.Params, state: abi.StepState | None = None) -> None:
+        s = state if state is not None else b.step_state(params)
+        self.check(_lib.lsmps_step(self.h, r(params), r(s)))
+
+
+def device_buffers(case, max_fluid_neighbors: int = 256, max_wall_neighbors: int = 256, device="cuda") -> StepBuffers:
+    """StepBuffers in device memory loaded with a synthetic case."""
+    b = StepBuffers(TorchAlloc(device), case.n_fluid, case.n_wall, case.n_cells, max_fluid_neighbors,
+                    max_wall_neighbors)
+    b.load_case(case)
+    return b

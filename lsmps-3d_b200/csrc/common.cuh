@@ -1,0 +1,158 @@
+// common.cuh - shared internals of the sm_100a LSMPS hot path: the context,
+// the device status word, launch bookkeeping and the per-neighbour formulas
+// every gather kernel uses.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <string>
+
+#include "lsmps_b200.h"
+
+namespace lsmps {
+
+using index_t = int32_t;
+
+constexpr int kWarp = 32;
+
+// Bits of DeviceStatus::flags.
+constexpr unsigned kFlagCapacity = 1u;
+constexpr unsigned kFlagNonFinite = 2u;
+constexpr unsigned kFlagIndexOverflow = 4u;
+constexpr unsigned kFlagNonSpd = 8u;
+
+// Written by kernels, read back once per synchronous call (or per
+// lsmps_ctx_synchronize in asynchronous mode).
+struct DeviceStatus {
+  unsigned int flags;
+  unsigned int non_spd;
+  unsigned long long required;
+};
+
+__device__ __forceinline__ void raise_flag(DeviceStatus* s, unsigned f) { atomicOr(&s->flags, f); }
+
+__device__ __forceinline__ void record_required(DeviceStatus* s, unsigned long long required) {
+  atomicOr(&s->flags, kFlagCapacity);
+  atomicMax(&s->required, required);
+}
+
+// Linear kernel weight, identical in every reference module:
+// surface_detection.cu:26-31, moment_matrix.cu:145-150,
+// explicit_update.cu:121-126, ppe_matrix.cu:148-153.
+__device__ __forceinline__ double lin_weight(double distance, double support_radius) {
+  return distance >= support_radius ? 0.0 : 1.0 - distance / support_radius;
+}
+
+// correction_weight also rejects zero distance (pressure_correction.cu:127-132).
+__device__ __forceinline__ double correction_weight(double distance, double support_radius) {
+  return (distance >= support_radius || distance <= 0.0) ? 0.0 : 1.0 - distance / support_radius;
+}
+
+// Type-A quadratic basis of the r_e-scaled offset with the multiply-by-inverse
+// form of explicit_update.cu:128-146 (ppe_matrix.cu:155-173 and
+// pressure_correction.cu:138-156 are the same).
+__device__ __forceinline__ void basis_a_mul(double dx, double dy, double dz, double inv_re, double b[9]) {
+  const double sx = dx * inv_re, sy = dy * inv_re, sz = dz * inv_re;
+  b[0] = sx;
+  b[1] = sy;
+  b[2] = sz;
+  b[3] = sx * sx;
+  b[4] = sy * sy;
+  b[5] = sz * sz;
+  b[6] = sx * sy;
+  b[7] = sy * sz;
+  b[8] = sz * sx;
+}
+
+// Wall Neumann vector q of moment_matrix.cu:177-201 (Type-A part).
+__device__ __forceinline__ void neumann_a(double dx, double dy, double dz, double nx, double ny, double nz,
+                                          double inv_re, double q[9]) {
+  q[0] = nx;
+  q[1] = ny;
+  q[2] = nz;
+  q[3] = 2.0 * dx * nx * inv_re;
+  q[4] = 2.0 * dy * ny * inv_re;
+  q[5] = 2.0 * dz * nz * inv_re;
+  q[6] = (dy * nx + dx * ny) * inv_re;
+  q[7] = (dz * ny + dy * nz) * inv_re;
+  q[8] = (dx * nz + dz * nx) * inv_re;
+}
+
+inline int div_up(long long a, long long b) { return static_cast<int>((a + b - 1) / b); }
+
+}  // namespace lsmps
+
+// Opaque context of the C ABI.
+struct lsmps_ctx {
+  int device = 0;
+  int sm_count = 148;
+  cudaStream_t stream = nullptr;
+  cudaStream_t own_stream = nullptr;
+  int precision = LSMPS_PRECISION_PLAIN;
+  bool synchronous = true;
+  lsmps::DeviceStatus* d_status = nullptr;
+  lsmps::DeviceStatus* h_status = nullptr;  // pinned mirror
+  void* scratch = nullptr;
+  size_t scratch_bytes = 0;
+  size_t scratch_used = 0;
+  unsigned long long launches = 0;
+  unsigned long long required = 0;
+  std::string last_error;
+};
+
+namespace lsmps {
+
+// Bump allocator over the context's scratch; reset at the start of each API
+// call.  Grows (outside stream capture) when a call needs more.
+class Scratch {
+ public:
+  explicit Scratch(lsmps_ctx* ctx) : ctx_(ctx) { ctx_->scratch_used = 0; }
+  // Ensure `bytes` of scratch in total for this call.
+  bool reserve(size_t bytes);
+  template <typename T>
+  T* take(size_t count) {
+    const size_t bytes = ((count * sizeof(T)) + 255) & ~size_t(255);
+    if (ctx_->scratch_used + bytes > ctx_->scratch_bytes) return nullptr;
+    T* p = reinterpret_cast<T*>(static_cast<char*>(ctx_->scratch) + ctx_->scratch_used);
+    ctx_->scratch_used += bytes;
+    return p;
+  }
+
+ private:
+  lsmps_ctx* ctx_;
+};
+
+lsmps_status fail(lsmps_ctx* ctx, lsmps_status st, const char* what);
+lsmps_status check_launch(lsmps_ctx* ctx, const char* what);
+// Begin an API call: clear the device status in synchronous mode.
+lsmps_status begin_call(lsmps_ctx* ctx);
+// End an API call: in synchronous mode wait and fold the device status.
+lsmps_status end_call(lsmps_ctx* ctx, lsmps_status st);
+lsmps_status fold_status(lsmps_ctx* ctx);
+
+template <typename Kernel, typename... Args>
+inline void launch(lsmps_ctx* ctx, Kernel kernel, dim3 grid, dim3 block, size_t smem, Args... args) {
+  if (grid.x == 0 || grid.y == 0 || grid.z == 0) return;
+  kernel<<<grid, block, smem, ctx->stream>>>(args...);
+  ++ctx->launches;
+}
+
+// Scan helpers (scan.cu).  Exclusive scan of n int32 values into out (may
+// alias in); values and partial sums are accumulated in 64 bits and any
+// result above INT32_MAX raises kFlagIndexOverflow.  The grand total is
+// written to *total and/or *total_i32 (device pointers) when they are non-null.
+size_t scan_scratch_bytes(size_t n);
+lsmps_status exclusive_scan_i32(lsmps_ctx* ctx, Scratch& scratch, const index_t* in, index_t* out, size_t n,
+                                unsigned long long* total, index_t* total_i32);
+
+// Cell-list build shared by lsmps_build_cell_list and the neighbour search
+// (cells.cu).
+size_t cell_list_scratch_bytes(size_t n, size_t ncell);
+lsmps_status build_cell_list_impl(lsmps_ctx* ctx, Scratch& scratch, const double* x, const double* y,
+                                  const double* z, size_t count, const lsmps_grid& grid,
+                                  const lsmps_cells& cells);
+lsmps_status validate_grid(lsmps_ctx* ctx, const lsmps_grid& grid);
+
+}  // namespace lsmps

@@ -1,0 +1,213 @@
+// context.cu - the opaque context of the C ABI: stream, scratch, device status.
+#include <cstring>
+#include <new>
+
+#include "common.cuh"
+
+namespace lsmps {
+
+bool Scratch::reserve(size_t bytes) {
+  if (bytes <= ctx_->scratch_bytes) return true;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  cudaStreamIsCapturing(ctx_->stream, &cap);
+  if (cap != cudaStreamCaptureStatusNone) return false;  // sizes must be reserved before capture
+  if (ctx_->scratch) {
+    cudaStreamSynchronize(ctx_->stream);
+    cudaFree(ctx_->scratch);
+    ctx_->scratch = nullptr;
+    ctx_->scratch_bytes = 0;
+  }
+  const size_t grown = bytes + bytes / 4;
+  if (cudaMalloc(&ctx_->scratch, grown) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  ctx_->scratch_bytes = grown;
+  return true;
+}
+
+lsmps_status fail(lsmps_ctx* ctx, lsmps_status st, const char* what) {
+  if (ctx) ctx->last_error = what;
+  return st;
+}
+
+lsmps_status check_launch(lsmps_ctx* ctx, const char* what) {
+  const cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) return LSMPS_OK;
+  ctx->last_error = std::string(what) + ": " + cudaGetErrorString(e);
+  return LSMPS_CUDA_ERROR;
+}
+
+lsmps_status begin_call(lsmps_ctx* ctx) {
+  if (ctx->synchronous) {
+    if (cudaMemsetAsync(ctx->d_status, 0, sizeof(DeviceStatus), ctx->stream) != cudaSuccess)
+      return check_launch(ctx, "status reset");
+  }
+  return LSMPS_OK;
+}
+
+lsmps_status fold_status(lsmps_ctx* ctx) {
+  if (cudaMemcpyAsync(ctx->h_status, ctx->d_status, sizeof(DeviceStatus), cudaMemcpyDeviceToHost,
+                      ctx->stream) != cudaSuccess)
+    return check_launch(ctx, "status readback");
+  const cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) {
+    ctx->last_error = std::string("stream synchronize: ") + cudaGetErrorString(e);
+    return LSMPS_CUDA_ERROR;
+  }
+  const DeviceStatus s = *ctx->h_status;
+  cudaMemsetAsync(ctx->d_status, 0, sizeof(DeviceStatus), ctx->stream);
+  if (s.flags & kFlagNonFinite) {
+    ctx->last_error = "non-finite particle coordinate";
+    return LSMPS_NON_FINITE;
+  }
+  if (s.flags & kFlagIndexOverflow) {
+    ctx->last_error = "count exceeds the 32-bit index range";
+    return LSMPS_INDEX_OVERFLOW;
+  }
+  if (s.flags & kFlagCapacity) {
+    ctx->required = s.required;
+    ctx->last_error = "neighbour list capacity exceeded: required " + std::to_string(s.required);
+    return LSMPS_CAPACITY_EXCEEDED;
+  }
+  return LSMPS_OK;
+}
+
+lsmps_status end_call(lsmps_ctx* ctx, lsmps_status st) {
+  if (st != LSMPS_OK) return st;
+  const lsmps_status ls = check_launch(ctx, "kernel launch");
+  if (ls != LSMPS_OK) return ls;
+  if (!ctx->synchronous) return LSMPS_OK;
+  return fold_status(ctx);
+}
+
+}  // namespace lsmps
+
+using namespace lsmps;
+
+extern "C" {
+
+lsmps_status lsmps_ctx_create(int device, lsmps_ctx** out) {
+  if (!out) return LSMPS_INVALID_ARGUMENT;
+  *out = nullptr;
+  if (cudaSetDevice(device) != cudaSuccess) {
+    cudaGetLastError();
+    return LSMPS_CUDA_ERROR;
+  }
+  lsmps_ctx* ctx = new (std::nothrow) lsmps_ctx();
+  if (!ctx) return LSMPS_CUDA_ERROR;
+  ctx->device = device;
+  cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device);
+  if (cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaMalloc(&ctx->d_status, sizeof(DeviceStatus)) != cudaSuccess ||
+      cudaMallocHost(&ctx->h_status, sizeof(DeviceStatus)) != cudaSuccess) {
+    cudaGetLastError();
+    lsmps_ctx_destroy(ctx);
+    return LSMPS_CUDA_ERROR;
+  }
+  ctx->stream = ctx->own_stream;
+  cudaMemsetAsync(ctx->d_status, 0, sizeof(DeviceStatus), ctx->stream);
+  std::memset(ctx->h_status, 0, sizeof(DeviceStatus));
+  cudaStreamSynchronize(ctx->stream);
+  *out = ctx;
+  return LSMPS_OK;
+}
+
+void lsmps_ctx_destroy(lsmps_ctx* ctx) {
+  if (!ctx) return;
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->scratch) cudaFree(ctx->scratch);
+  if (ctx->d_status) cudaFree(ctx->d_status);
+  if (ctx->h_status) cudaFreeHost(ctx->h_status);
+  if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+  delete ctx;
+}
+
+lsmps_status lsmps_ctx_set_stream(lsmps_ctx* ctx, void* stream) {
+  if (!ctx) return LSMPS_INVALID_ARGUMENT;
+  ctx->stream = stream ? static_cast<cudaStream_t>(stream) : ctx->own_stream;
+  return LSMPS_OK;
+}
+
+void* lsmps_ctx_stream(lsmps_ctx* ctx) { return ctx ? static_cast<void*>(ctx->stream) : nullptr; }
+
+lsmps_status lsmps_ctx_set_precision(lsmps_ctx* ctx, int precision) {
+  if (!ctx || (precision != LSMPS_PRECISION_PLAIN && precision != LSMPS_PRECISION_MIXED))
+    return LSMPS_INVALID_ARGUMENT;
+  ctx->precision = precision;
+  return LSMPS_OK;
+}
+
+lsmps_status lsmps_ctx_set_synchronous(lsmps_ctx* ctx, int synchronous) {
+  if (!ctx) return LSMPS_INVALID_ARGUMENT;
+  ctx->synchronous = synchronous != 0;
+  return LSMPS_OK;
+}
+
+lsmps_status lsmps_ctx_reserve(lsmps_ctx* ctx, size_t fluid_capacity, size_t wall_capacity, size_t cell_capacity) {
+  if (!ctx) return LSMPS_INVALID_ARGUMENT;
+  const size_t n = fluid_capacity > wall_capacity ? fluid_capacity : wall_capacity;
+  size_t need = cell_list_scratch_bytes(n, cell_capacity);
+  const size_t s2 = scan_scratch_bytes(fluid_capacity + 1) + 4096;
+  if (s2 > need) need = s2;
+  Scratch s(ctx);
+  if (!s.reserve(need)) return fail(ctx, LSMPS_CUDA_ERROR, "scratch allocation failed");
+  return LSMPS_OK;
+}
+
+lsmps_status lsmps_ctx_synchronize(lsmps_ctx* ctx) {
+  if (!ctx) return LSMPS_INVALID_ARGUMENT;
+  const lsmps_status ls = check_launch(ctx, "kernel launch");
+  if (ls != LSMPS_OK) return ls;
+  return fold_status(ctx);
+}
+
+uint64_t lsmps_ctx_required(lsmps_ctx* ctx) { return ctx ? ctx->required : 0; }
+
+uint64_t lsmps_ctx_launch_count(lsmps_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+const char* lsmps_ctx_last_error(lsmps_ctx* ctx) { return ctx ? ctx->last_error.c_str() : "null context"; }
+
+const char* lsmps_status_string(int status) {
+  switch (status) {
+    case LSMPS_OK: return "OK";
+    case LSMPS_CAPACITY_EXCEEDED: return "CAPACITY_EXCEEDED";
+    case LSMPS_INVALID_ARGUMENT: return "INVALID_ARGUMENT";
+    case LSMPS_NOT_PREPARED: return "NOT_PREPARED";
+    case LSMPS_NON_SPD: return "NON_SPD";
+    case LSMPS_CUDA_ERROR: return "CUDA_ERROR";
+    case LSMPS_INDEX_OVERFLOW: return "INDEX_OVERFLOW";
+    case LSMPS_NON_FINITE: return "NON_FINITE";
+    default: return "UNKNOWN";
+  }
+}
+
+void lsmps_params_default(lsmps_params* p) {
+  if (!p) return;
+  std::memset(p, 0, sizeof(*p));
+  p->particle_spacing = 0.01;
+  p->support_radius = 0.031;
+  p->near_surface_radius = 0.015;
+  p->grid.cell_size = 0.031;
+  p->grid.dims[0] = p->grid.dims[1] = p->grid.dims[2] = 1;
+  p->time_step = 1.0e-4;
+  p->density = 1000.0;
+  p->kinematic_viscosity = 1.0e-6;
+  p->gravity[2] = -9.81;
+  p->splash_neighbor_threshold = 4;
+  p->include_wall_neighbors = 1;
+  p->number_density_ratio_threshold = 0.85;
+  p->air_open_ratio_threshold = 0.33;
+  p->air_anisotropy_threshold = 0.033;
+  p->wall_normal_independence_threshold = 0.25;
+  p->virtual_light_cone_cosine = 0.8660254037844386;
+  p->lsmps_regularization = 1.0e-8;
+  p->lsmps_wall_weight_scale = 1.0;
+  p->ps_displacement_scale = 0.05;
+  p->ps_min_distance_ratio = 0.85;
+  p->ps_max_displacement_ratio = 0.2;
+  p->wall_clearance_ratio = 0.25;
+  p->velocity_smoothing_strength = 0.1;
+}
+
+}  // extern "C"

@@ -1,0 +1,460 @@
+// correction.cu - pressure-gradient correction of velocity and position.
+// Replaces DevicePressureCorrection::apply and its free functions
+// (src/correction/pressure_correction.cu:188-515, 598-734): pressure clamp,
+// LSMPS pressure gradient, particle shifting, velocity/position update,
+// wall anti-penetration and velocity smoothing.
+#include "impl.cuh"
+
+namespace lsmps {
+namespace {
+
+constexpr int kThreads = 128;
+
+__device__ __forceinline__ bool is_splash(const int32_t* type, index_t i) {
+  return type != nullptr && type[i] == LSMPS_SURFACE_SPLASH;
+}
+
+__device__ __forceinline__ bool is_surface(const int32_t* type, index_t i) {
+  if (type == nullptr) return false;
+  const int t = type[i];
+  return t == LSMPS_SURFACE_SURFACE || t == LSMPS_SURFACE_SPLASH;
+}
+
+// clamp_fluid_pressure_kernel, pressure_correction.cu:188-198
+__global__ void clamp_kernel(index_t n, double* pressure, double* fluid_pressure) {
+  for (index_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double p = pressure[i];
+    const double c = p < 0.0 ? 0.0 : p;
+    pressure[i] = c;
+    if (fluid_pressure != nullptr && fluid_pressure != pressure) fluid_pressure[i] = c;
+  }
+}
+
+struct GatherArgs {
+  lsmps_fluid fluid;
+  lsmps_walls walls;
+  const index_t* fo;
+  const index_t* fi;
+  const index_t* wo;
+  const index_t* wi;
+  lsmps_params p;
+};
+
+// compute_pressure_gradient_kernel, pressure_correction.cu:200-276
+__global__ void __launch_bounds__(kThreads) gradient_kernel(GatherArgs a, const double* __restrict__ pressure,
+                                                            const double* __restrict__ pinv, double re,
+                                                            double wall_scale, double* gx, double* gy,
+                                                            double* gz) {
+  const index_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= static_cast<index_t>(a.fluid.count)) return;
+  if (is_splash(a.fluid.surface_type, i)) {
+    gx[i] = gy[i] = gz[i] = 0.0;
+    return;
+  }
+  const double* __restrict__ fx = a.fluid.x;
+  const double* __restrict__ fy = a.fluid.y;
+  const double* __restrict__ fz = a.fluid.z;
+  const double xi = fx[i], yi = fy[i], zi = fz[i];
+  const double inv_re = 1.0 / re;
+  const double pi = pressure[i];
+  double rhs[9], b[9];
+#pragma unroll
+  for (int r = 0; r < 9; ++r) rhs[r] = 0.0;
+  const index_t fe = a.fo[i + 1];
+  for (index_t o = a.fo[i]; o < fe; ++o) {
+    const index_t j = a.fi[o];
+    const double dx = fx[j] - xi, dy = fy[j] - yi, dz = fz[j] - zi;
+    const double w = correction_weight(sqrt(dx * dx + dy * dy + dz * dz), re);
+    if (w <= 0.0) continue;
+    basis_a_mul(dx, dy, dz, inv_re, b);
+    const double dp = pressure[j] - pi;
+#pragma unroll
+    for (int r = 0; r < 9; ++r) rhs[r] = fma(w * b[r], dp, rhs[r]);
+  }
+  const index_t we = a.wo[i + 1];
+  for (index_t o = a.wo[i]; o < we; ++o) {
+    const index_t j = a.wi[o];
+    const double dx = a.walls.x[j] - xi, dy = a.walls.y[j] - yi, dz = a.walls.z[j] - zi;
+    const double w = wall_scale * correction_weight(sqrt(dx * dx + dy * dy + dz * dz), re);
+    if (w <= 0.0) continue;
+    const double nx = a.walls.normal_x[j], ny = a.walls.normal_y[j], nz = a.walls.normal_z[j];
+    double q[9];
+    neumann_a(dx, dy, dz, nx, ny, nz, inv_re, q);
+    const double ng = a.p.gravity[0] * nx + a.p.gravity[1] * ny + a.p.gravity[2] * nz;
+    const double wr = re * a.p.density * ng;
+#pragma unroll
+    for (int r = 0; r < 9; ++r) rhs[r] = fma(w * q[r], wr, rhs[r]);
+  }
+  const double* __restrict__ inv = pinv + static_cast<size_t>(i) * 81;
+  double c0 = 0.0, c1 = 0.0, c2 = 0.0;
+#pragma unroll
+  for (int col = 0; col < 9; ++col) {
+    c0 = fma(inv[0 + col * 9], rhs[col], c0);
+    c1 = fma(inv[1 + col * 9], rhs[col], c1);
+    c2 = fma(inv[2 + col * 9], rhs[col], c2);
+  }
+  gx[i] = c0 * inv_re;
+  gy[i] = c1 * inv_re;
+  gz[i] = c2 * inv_re;
+}
+
+// compute_particle_shifting_kernel, pressure_correction.cu:278-367
+__global__ void __launch_bounds__(kThreads) shifting_kernel(GatherArgs a, double* sx_out, double* sy_out,
+                                                            double* sz_out) {
+  const index_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= static_cast<index_t>(a.fluid.count)) return;
+  if (a.p.ps_displacement_scale <= 0.0 || is_splash(a.fluid.surface_type, i)) {
+    sx_out[i] = sy_out[i] = sz_out[i] = 0.0;
+    return;
+  }
+  const double* __restrict__ fx = a.fluid.x;
+  const double* __restrict__ fy = a.fluid.y;
+  const double* __restrict__ fz = a.fluid.z;
+  const double xi = fx[i], yi = fy[i], zi = fz[i];
+  const double dmin = a.p.ps_min_distance_ratio * a.p.particle_spacing;
+  const double smax = a.p.ps_max_displacement_ratio * a.p.particle_spacing;
+  const double scale = a.p.ps_displacement_scale;
+  double shx = 0.0, shy = 0.0, shz = 0.0, nx = 0.0, ny = 0.0, nz = 0.0;
+  const index_t fe = a.fo[i + 1];
+  for (index_t o = a.fo[i]; o < fe; ++o) {
+    const index_t j = a.fi[o];
+    const double dx = xi - fx[j], dy = yi - fy[j], dz = zi - fz[j];
+    const double d = sqrt(dx * dx + dy * dy + dz * dz);
+    if (d <= 0.0 || d >= dmin) continue;
+    const double inv_d = 1.0 / d;
+    const double push = scale * (dmin - d) * inv_d;
+    shx = fma(push, dx, shx);
+    shy = fma(push, dy, shy);
+    shz = fma(push, dz, shz);
+    nx = fma(dx, inv_d, nx);
+    ny = fma(dy, inv_d, ny);
+    nz = fma(dz, inv_d, nz);
+  }
+  const index_t we = a.wo[i + 1];
+  for (index_t o = a.wo[i]; o < we; ++o) {
+    const index_t j = a.wi[o];
+    const double dx = xi - a.walls.x[j], dy = yi - a.walls.y[j], dz = zi - a.walls.z[j];
+    const double d = sqrt(dx * dx + dy * dy + dz * dz);
+    if (d <= 0.0 || d >= dmin) continue;
+    const double push = scale * (dmin - d);
+    shx = fma(push, a.walls.normal_x[j], shx);
+    shy = fma(push, a.walls.normal_y[j], shy);
+    shz = fma(push, a.walls.normal_z[j], shz);
+  }
+  if (is_surface(a.fluid.surface_type, i)) {
+    const double nn = sqrt(nx * nx + ny * ny + nz * nz);
+    if (nn > 0.0) {
+      nx /= nn;
+      ny /= nn;
+      nz /= nn;
+      const double nc = shx * nx + shy * ny + shz * nz;
+      shx -= nc * nx;
+      shy -= nc * ny;
+      shz -= nc * nz;
+    }
+  }
+  const double sn = sqrt(shx * shx + shy * shy + shz * shz);
+  if (sn > smax && sn > 0.0) {
+    const double sc = smax / sn;
+    shx *= sc;
+    shy *= sc;
+    shz *= sc;
+  }
+  sx_out[i] = shx;
+  sy_out[i] = shy;
+  sz_out[i] = shz;
+}
+
+// update_velocity_position_kernel, pressure_correction.cu:369-402
+__global__ void update_kernel(lsmps_fluid f, const double* __restrict__ tx, const double* __restrict__ ty,
+                              const double* __restrict__ tz, double dt, double density,
+                              const double* __restrict__ gx, const double* __restrict__ gy,
+                              const double* __restrict__ gz, const double* __restrict__ sx,
+                              const double* __restrict__ sy, const double* __restrict__ sz) {
+  for (index_t i = blockIdx.x * blockDim.x + threadIdx.x; i < static_cast<index_t>(f.count);
+       i += gridDim.x * blockDim.x) {
+    const bool splash = is_splash(f.surface_type, i);
+    const double ox = f.vx[i], oy = f.vy[i], oz = f.vz[i];
+    double nx = tx[i], ny = ty[i], nz = tz[i];
+    if (!splash) {
+      const double ps = dt / density;
+      nx -= ps * gx[i];
+      ny -= ps * gy[i];
+      nz -= ps * gz[i];
+    }
+    f.x[i] += 0.5 * dt * (ox + nx) + sx[i];
+    f.y[i] += 0.5 * dt * (oy + ny) + sy[i];
+    f.z[i] += 0.5 * dt * (oz + nz) + sz[i];
+    f.vx[i] = nx;
+    f.vy[i] = ny;
+    f.vz[i] = nz;
+  }
+}
+
+// anti_penetration_kernel, pressure_correction.cu:404-444: sequential over the
+// wall row in CSR order, one thread per particle.
+__global__ void __launch_bounds__(kThreads) anti_penetration_kernel(lsmps_fluid f, lsmps_walls w,
+                                                                    const index_t* __restrict__ wo,
+                                                                    const index_t* __restrict__ wi,
+                                                                    double clearance) {
+  const index_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= static_cast<index_t>(f.count)) return;
+  const index_t we = wo[i + 1];
+  index_t o = wo[i];
+  if (o >= we) return;
+  double x = f.x[i], y = f.y[i], z = f.z[i];
+  double vx = f.vx[i], vy = f.vy[i], vz = f.vz[i];
+  bool moved = false;
+  for (; o < we; ++o) {
+    const index_t j = wi[o];
+    const double nx = w.normal_x[j], ny = w.normal_y[j], nz = w.normal_z[j];
+    const double sd = (x - w.x[j]) * nx + (y - w.y[j]) * ny + (z - w.z[j]) * nz;
+    if (sd >= clearance) continue;
+    const double c = clearance - sd;
+    x += c * nx;
+    y += c * ny;
+    z += c * nz;
+    const double nv = vx * nx + vy * ny + vz * nz;
+    if (nv < 0.0) {
+      vx -= nv * nx;
+      vy -= nv * ny;
+      vz -= nv * nz;
+    }
+    moved = true;
+  }
+  if (moved) {
+    f.x[i] = x;
+    f.y[i] = y;
+    f.z[i] = z;
+    f.vx[i] = vx;
+    f.vy[i] = vy;
+    f.vz[i] = vz;
+  }
+}
+
+// smooth_velocity_kernel, pressure_correction.cu:446-504
+__global__ void __launch_bounds__(kThreads) smooth_kernel(lsmps_fluid f, const index_t* __restrict__ fo,
+                                                          const index_t* __restrict__ fi, double re, double strength,
+                                                          double* ox, double* oy, double* oz) {
+  const index_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= static_cast<index_t>(f.count)) return;
+  const double* __restrict__ vx = f.vx;
+  const double* __restrict__ vy = f.vy;
+  const double* __restrict__ vz = f.vz;
+  if (strength <= 0.0 || is_splash(f.surface_type, i)) {
+    ox[i] = vx[i];
+    oy[i] = vy[i];
+    oz[i] = vz[i];
+    return;
+  }
+  const double* __restrict__ fx = f.x;
+  const double* __restrict__ fy = f.y;
+  const double* __restrict__ fz = f.z;
+  const double xi = fx[i], yi = fy[i], zi = fz[i];
+  double ws = 0.0, ax = 0.0, ay = 0.0, az = 0.0;
+  const index_t fe = fo[i + 1];
+  for (index_t o = fo[i]; o < fe; ++o) {
+    const index_t j = fi[o];
+    if (is_splash(f.surface_type, j)) continue;
+    const double dx = fx[j] - xi, dy = fy[j] - yi, dz = fz[j] - zi;
+    const double w = correction_weight(sqrt(dx * dx + dy * dy + dz * dz), re);
+    if (w <= 0.0) continue;
+    ws += w;
+    ax = fma(w, vx[j], ax);
+    ay = fma(w, vy[j], ay);
+    az = fma(w, vz[j], az);
+  }
+  if (ws <= 0.0) {
+    ox[i] = vx[i];
+    oy[i] = vy[i];
+    oz[i] = vz[i];
+    return;
+  }
+  const double alpha = strength < 0.0 ? 0.0 : (strength > 1.0 ? 1.0 : strength);
+  ox[i] = (1.0 - alpha) * vx[i] + alpha * ax / ws;
+  oy[i] = (1.0 - alpha) * vy[i] + alpha * ay / ws;
+  oz[i] = (1.0 - alpha) * vz[i] + alpha * az / ws;
+}
+
+// copy_smoothed_velocity_kernel, pressure_correction.cu:506-515
+__global__ void copy_kernel(index_t n, const double* __restrict__ sx, const double* __restrict__ sy,
+                            const double* __restrict__ sz, double* vx, double* vy, double* vz) {
+  for (index_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    vx[i] = sx[i];
+    vy[i] = sy[i];
+    vz[i] = sz[i];
+  }
+}
+
+int pointwise_blocks(lsmps_ctx* ctx, size_t n) {
+  const long long b = div_up(static_cast<long long>(n), 256);
+  const long long cap = static_cast<long long>(ctx->sm_count) * 8;
+  return static_cast<int>(b < cap ? b : cap);
+}
+
+lsmps_status check_fluid(lsmps_ctx* ctx, const lsmps_fluid& f) {
+  if (f.count > 0 && (!f.x || !f.y || !f.z || !f.vx || !f.vy || !f.vz))
+    return fail(ctx, LSMPS_INVALID_ARGUMENT, "Pressure correction requires fluid position and velocity arrays");
+  return LSMPS_OK;
+}
+
+lsmps_status check_vector(lsmps_ctx* ctx, const lsmps_fluid& f, const lsmps_vector& v, const char* what) {
+  if (v.count < f.count || (f.count > 0 && (!v.x || !v.y || !v.z))) return fail(ctx, LSMPS_INVALID_ARGUMENT, what);
+  return LSMPS_OK;
+}
+
+}  // namespace
+
+lsmps_status clamp_pressure_impl(lsmps_ctx* ctx, const lsmps_fluid& f, double* pressure) {
+  if (f.count > 0 && !pressure) return fail(ctx, LSMPS_INVALID_ARGUMENT, "Pressure correction requires a pressure array");
+  if (f.count == 0) return LSMPS_OK;
+  launch(ctx, clamp_kernel, dim3(pointwise_blocks(ctx, f.count)), dim3(256), 0, static_cast<index_t>(f.count),
+         pressure, f.pressure);
+  return check_launch(ctx, "pressure clamp");
+}
+
+lsmps_status pressure_gradient_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const lsmps_walls& w, const lsmps_csr& fn,
+                                    const lsmps_csr& wn, const double* pressure, const lsmps_params& p,
+                                    const lsmps_moment& pm, const lsmps_vector& g) {
+  lsmps_status st = check_fluid(ctx, f);
+  if (st) return st;
+  if ((st = check_vector(ctx, f, g, "Pressure gradient workspace is too small"))) return st;
+  if (pm.kind != LSMPS_MOMENT_PRESSURE_WALL_NEUMANN_A || pm.matrix_size != 9 || pm.particle_count < f.count)
+    return fail(ctx, LSMPS_NOT_PREPARED, "Pressure correction requires a prepared pressure Type-A moment matrix");
+  if (f.count > 0 && (!pressure || !pm.inverse_matrices))
+    return fail(ctx, LSMPS_INVALID_ARGUMENT, "Pressure gradient requires pressure and inverse buffers");
+  if (f.count == 0) return LSMPS_OK;
+  GatherArgs a{f, w, fn.offsets, fn.indices, wn.offsets, wn.indices, p};
+  launch(ctx, gradient_kernel, dim3(div_up(static_cast<long long>(f.count), kThreads)), dim3(kThreads), 0, a,
+         pressure, static_cast<const double*>(pm.inverse_matrices), pm.support_radius, pm.wall_weight_scale, g.x, g.y,
+         g.z);
+  return check_launch(ctx, "pressure gradient");
+}
+
+lsmps_status particle_shifting_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const lsmps_walls& w, const lsmps_csr& fn,
+                                    const lsmps_csr& wn, const lsmps_params& p, const lsmps_vector& s) {
+  lsmps_status st = check_fluid(ctx, f);
+  if (st) return st;
+  if ((st = check_vector(ctx, f, s, "PS displacement workspace is too small"))) return st;
+  if (f.count == 0) return LSMPS_OK;
+  GatherArgs a{f, w, fn.offsets, fn.indices, wn.offsets, wn.indices, p};
+  launch(ctx, shifting_kernel, dim3(div_up(static_cast<long long>(f.count), kThreads)), dim3(kThreads), 0, a, s.x, s.y,
+         s.z);
+  return check_launch(ctx, "particle shifting");
+}
+
+lsmps_status update_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const lsmps_fluid& t, const lsmps_params& p,
+                         const lsmps_vector& g, const lsmps_vector& s) {
+  lsmps_status st = check_fluid(ctx, f);
+  if (st) return st;
+  if (t.count < f.count || (f.count && (!t.vx || !t.vy || !t.vz)))
+    return fail(ctx, LSMPS_INVALID_ARGUMENT, "Pressure correction temporary velocity target is too small");
+  if ((st = check_vector(ctx, f, g, "Pressure gradient workspace is too small"))) return st;
+  if ((st = check_vector(ctx, f, s, "PS displacement workspace is too small"))) return st;
+  if (f.count == 0) return LSMPS_OK;
+  launch(ctx, update_kernel, dim3(pointwise_blocks(ctx, f.count)), dim3(256), 0, f,
+         static_cast<const double*>(t.vx), static_cast<const double*>(t.vy), static_cast<const double*>(t.vz),
+         p.time_step, p.density, static_cast<const double*>(g.x), static_cast<const double*>(g.y),
+         static_cast<const double*>(g.z), static_cast<const double*>(s.x), static_cast<const double*>(s.y),
+         static_cast<const double*>(s.z));
+  return check_launch(ctx, "velocity/position update");
+}
+
+lsmps_status anti_penetration_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const lsmps_walls& w, const lsmps_csr& wn,
+                                   const lsmps_params& p) {
+  const double clearance = p.wall_clearance_ratio * p.particle_spacing;
+  if (f.count == 0 || clearance <= 0.0) return LSMPS_OK;
+  launch(ctx, anti_penetration_kernel, dim3(div_up(static_cast<long long>(f.count), kThreads)), dim3(kThreads), 0, f,
+         w, static_cast<const index_t*>(wn.offsets), static_cast<const index_t*>(wn.indices), clearance);
+  return check_launch(ctx, "anti-penetration");
+}
+
+lsmps_status smooth_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const lsmps_csr& fn, const lsmps_params& p,
+                         const lsmps_vector& sm) {
+  lsmps_status st = check_fluid(ctx, f);
+  if (st) return st;
+  if ((st = check_vector(ctx, f, sm, "Velocity smoothing workspace is too small"))) return st;
+  if (f.count == 0) return LSMPS_OK;
+  launch(ctx, smooth_kernel, dim3(div_up(static_cast<long long>(f.count), kThreads)), dim3(kThreads), 0, f,
+         static_cast<const index_t*>(fn.offsets), static_cast<const index_t*>(fn.indices), p.support_radius,
+         p.velocity_smoothing_strength, sm.x, sm.y, sm.z);
+  launch(ctx, copy_kernel, dim3(pointwise_blocks(ctx, f.count)), dim3(256), 0, static_cast<index_t>(f.count),
+         static_cast<const double*>(sm.x), static_cast<const double*>(sm.y), static_cast<const double*>(sm.z), f.vx,
+         f.vy, f.vz);
+  return check_launch(ctx, "velocity smoothing");
+}
+
+lsmps_status pressure_correction_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const lsmps_walls& w,
+                                      const lsmps_csr& fn, const lsmps_csr& wn, const lsmps_fluid& t,
+                                      double* pressure, const lsmps_params& p, const lsmps_moment& pm,
+                                      const lsmps_vector& g, const lsmps_vector& s, const lsmps_vector& sm) {
+  lsmps_status st = clamp_pressure_impl(ctx, f, pressure);
+  if (!st) st = pressure_gradient_impl(ctx, f, w, fn, wn, pressure, p, pm, g);
+  if (!st) st = particle_shifting_impl(ctx, f, w, fn, wn, p, s);
+  if (!st) st = update_impl(ctx, f, t, p, g, s);
+  if (!st) st = anti_penetration_impl(ctx, f, w, wn, p);
+  if (!st) st = smooth_impl(ctx, f, fn, p, sm);
+  return st;
+}
+
+}  // namespace lsmps
+
+using namespace lsmps;
+
+#define LSMPS_API_BODY(expr)                  \
+  do {                                        \
+    lsmps_status st_ = begin_call(ctx);       \
+    if (st_) return st_;                      \
+    return end_call(ctx, (expr));             \
+  } while (0)
+
+extern "C" {
+
+lsmps_status lsmps_clamp_particle_pressure(lsmps_ctx* ctx, const lsmps_fluid* fluid, double* pressure) {
+  if (!ctx || !fluid) return LSMPS_INVALID_ARGUMENT;
+  LSMPS_API_BODY(clamp_pressure_impl(ctx, *fluid, pressure));
+}
+
+lsmps_status lsmps_pressure_gradient(lsmps_ctx* ctx, const lsmps_fluid* fluid, const lsmps_walls* walls,
+                                     const lsmps_csr* fn, const lsmps_csr* wn, const double* pressure,
+                                     const lsmps_params* params, const lsmps_moment* pm, const lsmps_vector* g) {
+  if (!ctx || !fluid || !walls || !fn || !wn || !params || !pm || !g) return LSMPS_INVALID_ARGUMENT;
+  LSMPS_API_BODY(pressure_gradient_impl(ctx, *fluid, *walls, *fn, *wn, pressure, *params, *pm, *g));
+}
+
+lsmps_status lsmps_particle_shifting(lsmps_ctx* ctx, const lsmps_fluid* fluid, const lsmps_walls* walls,
+                                     const lsmps_csr* fn, const lsmps_csr* wn, const lsmps_params* params,
+                                     const lsmps_vector* s) {
+  if (!ctx || !fluid || !walls || !fn || !wn || !params || !s) return LSMPS_INVALID_ARGUMENT;
+  LSMPS_API_BODY(particle_shifting_impl(ctx, *fluid, *walls, *fn, *wn, *params, *s));
+}
+
+lsmps_status lsmps_update_velocity_position(lsmps_ctx* ctx, const lsmps_fluid* fluid, const lsmps_fluid* t,
+                                            const lsmps_params* params, const lsmps_vector* g,
+                                            const lsmps_vector* s) {
+  if (!ctx || !fluid || !t || !params || !g || !s) return LSMPS_INVALID_ARGUMENT;
+  LSMPS_API_BODY(update_impl(ctx, *fluid, *t, *params, *g, *s));
+}
+
+lsmps_status lsmps_anti_penetration(lsmps_ctx* ctx, const lsmps_fluid* fluid, const lsmps_walls* walls,
+                                    const lsmps_csr* wn, const lsmps_params* params) {
+  if (!ctx || !fluid || !walls || !wn || !params) return LSMPS_INVALID_ARGUMENT;
+  LSMPS_API_BODY(anti_penetration_impl(ctx, *fluid, *walls, *wn, *params));
+}
+
+lsmps_status lsmps_smooth_particle_velocity(lsmps_ctx* ctx, const lsmps_fluid* fluid, const lsmps_csr* fn,
+                                            const lsmps_params* params, const lsmps_vector* sm) {
+  if (!ctx || !fluid || !fn || !params || !sm) return LSMPS_INVALID_ARGUMENT;
+  LSMPS_API_BODY(smooth_impl(ctx, *fluid, *fn, *params, *sm));
+}
+
+lsmps_status lsmps_pressure_correction(lsmps_ctx* ctx, const lsmps_fluid* fluid, const lsmps_walls* walls,
+                                       const lsmps_csr* fn, const lsmps_csr* wn, const lsmps_fluid* t,
+                                       double* pressure, const lsmps_params* params, const lsmps_moment* pm,
+                                       const lsmps_vector* g, const lsmps_vector* s, const lsmps_vector* sm) {
+  if (!ctx || !fluid || !walls || !fn || !wn || !t || !params || !pm || !g || !s || !sm)
+    return LSMPS_INVALID_ARGUMENT;
+  LSMPS_API_BODY(pressure_correction_impl(ctx, *fluid, *walls, *fn, *wn, *t, pressure, *params, *pm, *g, *s, *sm));
+}
+
+}  // extern "C"

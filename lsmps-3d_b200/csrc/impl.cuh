@@ -1,0 +1,38 @@
+// impl.cuh - stream-ordered implementations behind the C ABI entry points.
+// Each queues its kernels on ctx->stream and returns host-side validation
+// failures; device-side status is folded by end_call / lsmps_ctx_synchronize.
+#pragma once
+
+#include "common.cuh"
+
+namespace lsmps {
+
+double reference_number_density(double l0, double re);
+lsmps_status classify_surface_impl(lsmps_ctx* ctx, const lsmps_fluid& fluid, const lsmps_walls& walls,
+                                   const lsmps_csr& fn, const lsmps_csr& wn, const lsmps_params& p,
+                                   const lsmps_surface_diagnostics* diag);
+lsmps_status prepare_moments_impl(lsmps_ctx* ctx, const lsmps_fluid& fluid, const lsmps_walls& walls,
+                                  const lsmps_csr& fn, const lsmps_csr& wn, const lsmps_params& p,
+                                  const lsmps_moment* kinds, int count);
+lsmps_status velocity_laplacian_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const lsmps_walls& w,
+                                     const lsmps_csr& fn, const lsmps_csr& wn, const lsmps_moment& vm,
+                                     const lsmps_vector& lap);
+lsmps_status temporary_velocity_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const lsmps_params& p,
+                                     const lsmps_vector& lap, const lsmps_fluid& t);
+lsmps_status temporary_wall_velocity_impl(lsmps_ctx* ctx, const lsmps_walls& w, const lsmps_params& p,
+                                          const lsmps_walls& t);
+lsmps_status assemble_ppe_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const lsmps_walls& w, const lsmps_params& p,
+                               const lsmps_csr& fn, const lsmps_csr& wn, const lsmps_fluid& tv,
+                               const lsmps_walls& tw, const lsmps_moment& vm, const lsmps_moment& pm,
+                               const lsmps_ppe& ws);
+lsmps_status pressure_correction_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const lsmps_walls& w,
+                                      const lsmps_csr& fn, const lsmps_csr& wn, const lsmps_fluid& t,
+                                      double* pressure, const lsmps_params& p, const lsmps_moment& pm,
+                                      const lsmps_vector& g, const lsmps_vector& s, const lsmps_vector& sm);
+lsmps_status build_neighbor_lists_impl(lsmps_ctx* ctx, Scratch& scratch, const lsmps_fluid& fluid,
+                                       const lsmps_walls& walls, const lsmps_params& p,
+                                       const lsmps_cells& fc, const lsmps_cells& wc, const lsmps_csr& fn,
+                                       const lsmps_csr& wn);
+size_t neighbor_scratch_bytes(size_t n_fluid, size_t n_wall, size_t ncell);
+
+}  // namespace lsmps

@@ -1,0 +1,287 @@
+// neighbors.cu - fluid-fluid and fluid-wall CSR neighbour tables.
+// Replaces build_neighbor_lists / build_one_neighbor_list of
+// src/neighbor/neighbor_search.cu:294-367 (count kernel :221-236, Thrust
+// exclusive scan :319-320, host capacity check :323-328, write kernel
+// :238-253).
+//
+// Layout of the work: one block per home cell.  The block stages the
+// candidate set of the 27 surrounding source cells (in the reference's
+// dz -> dy -> dx order, ascending sorted position inside a cell) into shared
+// memory once, as cell-relative FP32 coordinates, and every warp then tests
+// its home particles against the staged set 32 candidates at a time.  The
+// accepted candidates of one warp step are compacted with a ballot, so a row
+// comes out in exactly the reference's traversal order.
+//
+// Exactness: the FP32 distance is only a screen.  With coordinates scaled by
+// 1/h and re-centred on the home cell, every component is at most 2 in
+// magnitude for particles inside the grid, and the FP32 squared distance
+// differs from the exact one by less than 384 * 2^-24 < 2.3e-5.  A candidate
+// is accepted or rejected from FP32 only when it is more than
+// kScreenMargin = 1e-4 away from (r/h)^2; everything closer, and every
+// particle outside the +-2 window (clamped into an edge cell), is decided by
+// the reference's own FP64 test dx*dx + dy*dy + dz*dz <= r^2
+// (neighbor_search.cu:48-59).  The neighbour sets are therefore the FP64 ones.
+#include <climits>
+#include <cmath>
+
+#include "impl.cuh"
+
+namespace lsmps {
+namespace {
+
+constexpr int kCsrThreads = 128;
+constexpr int kCsrWarps = kCsrThreads / kWarp;
+constexpr int kStageCap = 1024;
+constexpr float kScreenMargin = 1.0e-4f;
+constexpr float kFarLimit = 2.0f;
+
+struct CsrArgs {
+  const double* fx;
+  const double* fy;
+  const double* fz;
+  const double* sx;
+  const double* sy;
+  const double* sz;
+  const index_t* home_begin;
+  const index_t* home_end;
+  const index_t* home_sorted;
+  const index_t* src_begin;
+  const index_t* src_end;
+  const index_t* src_sorted;
+  lsmps_grid grid;
+  double r2;
+  double inv_h;
+  float lo2;
+  float hi2;
+  index_t ncell;
+  int exclude_self;
+  index_t* offsets;  // count pass: per-particle counts; write pass: row offsets
+  index_t* indices;
+  unsigned long long capacity;
+  const index_t* total;  // write pass: offsets[N]
+  DeviceStatus* status;
+};
+
+__device__ __forceinline__ bool within_radius(double ax, double ay, double az, double bx, double by, double bz,
+                                              double r2) {
+  const double dx = ax - bx;
+  const double dy = ay - by;
+  const double dz = az - bz;
+  return dx * dx + dy * dy + dz * dz <= r2;
+}
+
+__device__ __forceinline__ float to_rel(double v, double centre, double inv_h) {
+  const float r = static_cast<float>((v - centre) * inv_h);
+  return fabsf(r) <= kFarLimit ? r : __int_as_float(0x7fc00000);  // NaN forces the exact test
+}
+
+template <bool kWrite>
+__global__ void __launch_bounds__(kCsrThreads) csr_kernel(CsrArgs a) {
+  __shared__ float4 s_rel[kStageCap];
+  __shared__ index_t s_idx[kStageCap];
+  __shared__ index_t s_cb[27];
+  __shared__ index_t s_cnt[27];
+  __shared__ index_t s_pre[28];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const unsigned lanemask_lt = (1u << lane) - 1u;
+  const int dimx = a.grid.dims[0], dimy = a.grid.dims[1], dimz = a.grid.dims[2];
+  if (kWrite && blockIdx.x == 0 && threadIdx.x == 0 && static_cast<unsigned long long>(*a.total) > a.capacity)
+    record_required(a.status, static_cast<unsigned long long>(*a.total));
+  for (index_t c = blockIdx.x; c < a.ncell; c += gridDim.x) {
+    const index_t hb = a.home_begin[c];
+    if (hb < 0) continue;  // uniform across the block
+    const index_t he = a.home_end[c];
+    const int cx = c % dimx;
+    const int cy = (c / dimx) % dimy;
+    const int cz = c / (dimx * dimy);
+    if (threadIdx.x < 27) {
+      const int t = threadIdx.x;
+      const int nz = cz + t / 9 - 1, ny = cy + (t / 3) % 3 - 1, nx = cx + t % 3 - 1;
+      index_t b = -1, n = 0;
+      if (nz >= 0 && nz < dimz && ny >= 0 && ny < dimy && nx >= 0 && nx < dimx) {
+        const index_t cell = (nz * dimy + ny) * dimx + nx;
+        b = a.src_begin[cell];
+        const index_t e = a.src_end[cell];
+        if (b >= 0 && e >= 0) n = e - b;
+      }
+      s_cb[t] = b;
+      s_cnt[t] = n;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      index_t run = 0;
+      for (int t = 0; t < 27; ++t) {
+        s_pre[t] = run;
+        run += s_cnt[t];
+      }
+      s_pre[27] = run;
+    }
+    __syncthreads();
+    const index_t nc = s_pre[27];
+    const double ccx = a.grid.origin[0] + (cx + 0.5) * a.grid.cell_size;
+    const double ccy = a.grid.origin[1] + (cy + 0.5) * a.grid.cell_size;
+    const double ccz = a.grid.origin[2] + (cz + 0.5) * a.grid.cell_size;
+    const bool staged = nc <= kStageCap;
+    if (staged) {
+      for (index_t k = threadIdx.x; k < nc; k += kCsrThreads) {
+        int t = 0;
+        while (s_pre[t + 1] <= k) ++t;
+        const index_t j = a.src_sorted[s_cb[t] + (k - s_pre[t])];
+        s_idx[k] = j;
+        s_rel[k] = make_float4(to_rel(a.sx[j], ccx, a.inv_h), to_rel(a.sy[j], ccy, a.inv_h),
+                               to_rel(a.sz[j], ccz, a.inv_h), 0.0f);
+      }
+    }
+    __syncthreads();
+    for (index_t h = hb + warp; h < he; h += kCsrWarps) {
+      const index_t i = a.home_sorted[h];
+      const double xi = a.fx[i], yi = a.fy[i], zi = a.fz[i];
+      index_t out = 0;
+      if (kWrite) out = a.offsets[i];
+      index_t count = 0;
+      if (staged) {
+        const float rx = to_rel(xi, ccx, a.inv_h), ry = to_rel(yi, ccy, a.inv_h), rz = to_rel(zi, ccz, a.inv_h);
+        for (index_t base = 0; base < nc; base += kWarp) {
+          const index_t k = base + lane;
+          bool pass = false;
+          index_t j = 0;
+          if (k < nc) {
+            j = s_idx[k];
+            if (!(a.exclude_self && j == i)) {
+              const float4 q = s_rel[k];
+              const float dx = rx - q.x, dy = ry - q.y, dz = rz - q.z;
+              const float d2 = dx * dx + dy * dy + dz * dz;
+              if (d2 < a.lo2) {
+                pass = true;
+              } else if (!(d2 > a.hi2)) {  // near the boundary, or NaN (far)
+                pass = within_radius(xi, yi, zi, a.sx[j], a.sy[j], a.sz[j], a.r2);
+              }
+            }
+          }
+          const unsigned m = __ballot_sync(0xffffffffu, pass);
+          if (kWrite) {
+            if (pass) {
+              const unsigned long long pos = static_cast<unsigned long long>(out) + __popc(m & lanemask_lt);
+              if (pos < a.capacity) a.indices[pos] = j;
+            }
+            out += __popc(m);
+          } else {
+            count += __popc(m);
+          }
+        }
+      } else {
+        // More candidates than the stage holds (overloaded edge cells):
+        // exact tests straight from global memory, same order.
+        for (int t = 0; t < 27; ++t) {
+          const index_t cnt = s_cnt[t];
+          const index_t b = s_cb[t];
+          for (index_t base = 0; base < cnt; base += kWarp) {
+            const index_t k = base + lane;
+            bool pass = false;
+            index_t j = 0;
+            if (k < cnt) {
+              j = a.src_sorted[b + k];
+              if (!(a.exclude_self && j == i)) pass = within_radius(xi, yi, zi, a.sx[j], a.sy[j], a.sz[j], a.r2);
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, pass);
+            if (kWrite) {
+              if (pass) {
+                const unsigned long long pos = static_cast<unsigned long long>(out) + __popc(m & lanemask_lt);
+                if (pos < a.capacity) a.indices[pos] = j;
+              }
+              out += __popc(m);
+            } else {
+              count += __popc(m);
+            }
+          }
+        }
+      }
+      if (!kWrite && lane == 0) a.offsets[i] = count;
+    }
+    __syncthreads();
+  }
+}
+
+lsmps_status one_neighbor_list(lsmps_ctx* ctx, Scratch& scratch, const lsmps_fluid& fluid, const double* sx,
+                               const double* sy, const double* sz, const lsmps_cells& home, const lsmps_cells& src,
+                               const lsmps_grid& grid, double radius, bool exclude_self, const lsmps_csr& out) {
+  if (fluid.count > out.particle_count || !out.offsets)
+    return fail(ctx, LSMPS_INVALID_ARGUMENT, "Neighbor list particle capacity is smaller than fluid count");
+  const size_t n = fluid.count;
+  CsrArgs a{};
+  a.fx = fluid.x;
+  a.fy = fluid.y;
+  a.fz = fluid.z;
+  a.sx = sx;
+  a.sy = sy;
+  a.sz = sz;
+  a.home_begin = home.cell_begin;
+  a.home_end = home.cell_end;
+  a.home_sorted = home.sorted_indices;
+  a.src_begin = src.cell_begin;
+  a.src_end = src.cell_end;
+  a.src_sorted = src.sorted_indices;
+  a.grid = grid;
+  a.r2 = radius * radius;
+  a.inv_h = 1.0 / grid.cell_size;
+  const double r2n = a.r2 * a.inv_h * a.inv_h;
+  a.lo2 = static_cast<float>(r2n) - kScreenMargin;
+  a.hi2 = static_cast<float>(r2n) + kScreenMargin;
+  a.ncell = static_cast<index_t>(static_cast<long long>(grid.dims[0]) * grid.dims[1] * grid.dims[2]);
+  a.exclude_self = exclude_self ? 1 : 0;
+  a.offsets = out.offsets;
+  a.indices = out.indices;
+  a.capacity = out.neighbor_count;
+  a.total = out.offsets + n;
+  a.status = ctx->d_status;
+  const int blocks = static_cast<int>(std::min<long long>(a.ncell, static_cast<long long>(ctx->sm_count) * 16));
+  if (n) launch(ctx, csr_kernel<false>, dim3(blocks), dim3(kCsrThreads), 0, a);
+  lsmps_status st = exclusive_scan_i32(ctx, scratch, out.offsets, out.offsets, n, nullptr, out.offsets + n);
+  if (st) return st;
+  if (n) launch(ctx, csr_kernel<true>, dim3(blocks), dim3(kCsrThreads), 0, a);
+  return check_launch(ctx, "neighbour list");
+}
+
+}  // namespace
+
+size_t neighbor_scratch_bytes(size_t n_fluid, size_t n_wall, size_t ncell) {
+  const size_t nmax = n_fluid > n_wall ? n_fluid : n_wall;
+  return 2 * cell_list_scratch_bytes(nmax, ncell) + 2 * scan_scratch_bytes(n_fluid + 1) + 4096;
+}
+
+lsmps_status build_neighbor_lists_impl(lsmps_ctx* ctx, Scratch& scratch, const lsmps_fluid& fluid,
+                                       const lsmps_walls& walls, const lsmps_params& p, const lsmps_cells& fc,
+                                       const lsmps_cells& wc, const lsmps_csr& fn, const lsmps_csr& wn) {
+  const double radius = p.support_radius;
+  if (!(radius > 0.0)) return fail(ctx, LSMPS_INVALID_ARGUMENT, "Neighbor search radius must be positive");
+  if (radius > p.grid.cell_size)
+    return fail(ctx, LSMPS_INVALID_ARGUMENT, "Neighbor search currently requires radius <= cell_size");
+  lsmps_status st = build_cell_list_impl(ctx, scratch, fluid.x, fluid.y, fluid.z, fluid.count, p.grid, fc);
+  if (!st) st = build_cell_list_impl(ctx, scratch, walls.x, walls.y, walls.z, walls.count, p.grid, wc);
+  if (!st)
+    st = one_neighbor_list(ctx, scratch, fluid, fluid.x, fluid.y, fluid.z, fc, fc, p.grid, radius, true, fn);
+  if (!st)
+    st = one_neighbor_list(ctx, scratch, fluid, walls.x, walls.y, walls.z, fc, wc, p.grid, radius, false, wn);
+  return st;
+}
+
+}  // namespace lsmps
+
+using namespace lsmps;
+
+extern "C" lsmps_status lsmps_build_neighbor_lists(lsmps_ctx* ctx, const lsmps_fluid* fluid,
+                                                   const lsmps_walls* walls, const lsmps_params* params,
+                                                   const lsmps_cells* fluid_cells, const lsmps_cells* wall_cells,
+                                                   const lsmps_csr* fluid_neighbors,
+                                                   const lsmps_csr* wall_neighbors) {
+  if (!ctx || !fluid || !walls || !params || !fluid_cells || !wall_cells || !fluid_neighbors || !wall_neighbors)
+    return LSMPS_INVALID_ARGUMENT;
+  lsmps_status st = begin_call(ctx);
+  if (st) return st;
+  Scratch scratch(ctx);
+  if (!scratch.reserve(neighbor_scratch_bytes(fluid->count, walls->count, fluid_cells->cell_count)))
+    return fail(ctx, LSMPS_CUDA_ERROR, "scratch allocation failed");
+  st = build_neighbor_lists_impl(ctx, scratch, *fluid, *walls, *params, *fluid_cells, *wall_cells, *fluid_neighbors,
+                                 *wall_neighbors);
+  return end_call(ctx, st);
+}

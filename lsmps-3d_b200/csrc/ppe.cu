@@ -1,0 +1,211 @@
+// ppe.cu - PPE CSR rows and right-hand side.
+// Replaces assemble_ppe_matrix_and_rhs (src/ppe/ppe_matrix.cu:517-551):
+// build_ppe_row_offsets_kernel (:133-146) is folded into the row kernel, which
+// restates assemble_ppe_system_kernel (:243-370).  Row i starts at
+// i + fluid_offsets[i]; slot 0 is the diagonal, then one slot per fluid
+// neighbour in CSR order (columns unsorted).  Surface and Splash rows are
+// Dirichlet rows: diagonal 1, neighbour slots 0, rhs 0 (:124-131, :262-276).
+#include "impl.cuh"
+
+namespace lsmps {
+namespace {
+
+constexpr int kThreads = 128;
+
+struct PpeArgs {
+  lsmps_fluid fluid;
+  lsmps_walls walls;
+  const index_t* fo;
+  const index_t* fi;
+  const index_t* wo;
+  const index_t* wi;
+  const double* tvx;
+  const double* tvy;
+  const double* tvz;
+  const double* twx;
+  const double* twy;
+  const double* twz;
+  const double* vinv;
+  const double* pinv;
+  double re;
+  double inv_re;
+  double vwall_scale;
+  double pwall_scale;
+  double density;
+  double dt;
+  double gx, gy, gz;
+  index_t* row_offsets;
+  index_t* col;
+  double* val;
+  double* rhs;
+  double* divergence;
+  double* wall_rhs_out;  // pressure_laplacian (holds the wall Neumann term, :367-369)
+};
+
+__device__ __forceinline__ double dot9(const double a[9], const double b[9]) {
+  double v = 0.0;
+#pragma unroll
+  for (int k = 0; k < 9; ++k) v = fma(a[k], b[k], v);
+  return v;
+}
+
+__device__ __forceinline__ void acc_rhs(const double b[9], double w, double ux, double uy, double uz, double rx[9],
+                                        double ry[9], double rz[9]) {
+#pragma unroll
+  for (int r = 0; r < 9; ++r) {
+    const double wb = w * b[r];
+    rx[r] = fma(wb, ux, rx[r]);
+    ry[r] = fma(wb, uy, ry[r]);
+    rz[r] = fma(wb, uz, rz[r]);
+  }
+}
+
+__device__ __forceinline__ double coeff_row(const double* __restrict__ inv, const double rhs[9], int row) {
+  double c = 0.0;
+#pragma unroll
+  for (int col = 0; col < 9; ++col) c = fma(inv[row + col * 9], rhs[col], c);
+  return c;
+}
+
+__global__ void __launch_bounds__(kThreads) ppe_kernel(PpeArgs a) {
+  const index_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  const index_t n = static_cast<index_t>(a.fluid.count);
+  if (i >= n) return;
+  const index_t nb = a.fo[i], ne = a.fo[i + 1];
+  const index_t row = i + nb;
+  a.row_offsets[i] = row;
+  if (i + 1 == n) a.row_offsets[n] = n + ne;
+  const int type = a.fluid.surface_type ? a.fluid.surface_type[i] : LSMPS_SURFACE_INNER;
+  if (type == LSMPS_SURFACE_SURFACE || type == LSMPS_SURFACE_SPLASH) {
+    a.col[row] = i;
+    a.val[row] = 1.0;
+    for (index_t o = nb; o < ne; ++o) {
+      a.col[row + 1 + o - nb] = a.fi[o];
+      a.val[row + 1 + o - nb] = 0.0;
+    }
+    a.rhs[i] = 0.0;
+    a.divergence[i] = 0.0;
+    if (a.wall_rhs_out) a.wall_rhs_out[i] = 0.0;
+    return;
+  }
+  const double* __restrict__ fx = a.fluid.x;
+  const double* __restrict__ fy = a.fluid.y;
+  const double* __restrict__ fz = a.fluid.z;
+  const double xi = fx[i], yi = fy[i], zi = fz[i];
+  // compute_pressure_laplacian_row, ppe_matrix.cu:203-215
+  const double* __restrict__ pinv = a.pinv + static_cast<size_t>(i) * 81;
+  double L[9];
+#pragma unroll
+  for (int col = 0; col < 9; ++col) L[col] = pinv[3 + col * 9] + pinv[4 + col * 9] + pinv[5 + col * 9];
+  const double uxi = a.tvx[i], uyi = a.tvy[i], uzi = a.tvz[i];
+  const double scale = 2.0 / (a.re * a.re * a.density);
+  double rx[9], ry[9], rz[9], b[9];
+#pragma unroll
+  for (int r = 0; r < 9; ++r) rx[r] = ry[r] = rz[r] = 0.0;
+  double diag = 0.0;
+  for (index_t o = nb; o < ne; ++o) {
+    const index_t j = a.fi[o];
+    const double dx = fx[j] - xi, dy = fy[j] - yi, dz = fz[j] - zi;
+    const double w = lin_weight(sqrt(dx * dx + dy * dy + dz * dz), a.re);
+    double off = 0.0;
+    if (w > 0.0) {
+      basis_a_mul(dx, dy, dz, a.inv_re, b);
+      off = w * dot9(L, b) * scale;
+      diag -= off;
+      acc_rhs(b, w, a.tvx[j] - uxi, a.tvy[j] - uyi, a.tvz[j] - uzi, rx, ry, rz);
+    }
+    a.col[row + 1 + o - nb] = j;
+    a.val[row + 1 + o - nb] = off;
+  }
+  double wall_rhs = 0.0;
+  const index_t we = a.wo[i + 1];
+  for (index_t o = a.wo[i]; o < we; ++o) {
+    const index_t j = a.wi[o];
+    const double dx = a.walls.x[j] - xi, dy = a.walls.y[j] - yi, dz = a.walls.z[j] - zi;
+    const double bw = lin_weight(sqrt(dx * dx + dy * dy + dz * dz), a.re);
+    if (bw <= 0.0) continue;
+    basis_a_mul(dx, dy, dz, a.inv_re, b);
+    acc_rhs(b, a.vwall_scale * bw, a.twx[j] - uxi, a.twy[j] - uyi, a.twz[j] - uzi, rx, ry, rz);
+    const double nx = a.walls.normal_x[j], ny = a.walls.normal_y[j], nz = a.walls.normal_z[j];
+    const double ng = a.gx * nx + a.gy * ny + a.gz * nz;
+    double q[9];
+    neumann_a(dx, dy, dz, nx, ny, nz, a.inv_re, q);
+    wall_rhs += 2.0 * a.pwall_scale * bw * ng * dot9(L, q) * a.inv_re;
+  }
+  const double* __restrict__ vinv = a.vinv + static_cast<size_t>(i) * 81;
+  const double div = (coeff_row(vinv, rx, 0) + coeff_row(vinv, ry, 1) + coeff_row(vinv, rz, 2)) * a.inv_re;
+  a.col[row] = i;
+  a.val[row] = diag;
+  a.divergence[i] = div;
+  a.rhs[i] = div / a.dt - wall_rhs;
+  if (a.wall_rhs_out) a.wall_rhs_out[i] = wall_rhs;
+}
+
+}  // namespace
+
+lsmps_status assemble_ppe_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const lsmps_walls& w, const lsmps_params& p,
+                               const lsmps_csr& fn, const lsmps_csr& wn, const lsmps_fluid& tv,
+                               const lsmps_walls& tw, const lsmps_moment& vm, const lsmps_moment& pm,
+                               const lsmps_ppe& ws) {
+  // validate_matrix_workspace, ppe_matrix.cu:62-84 (nnz checked against the
+  // CSR capacity, as the reference does).
+  if (ws.matrix.rows < f.count || ws.matrix.cols < f.count || ws.matrix.nnz < f.count + fn.neighbor_count)
+    return fail(ctx, LSMPS_INVALID_ARGUMENT, "PPE matrix workspace is smaller than the requested fluid system");
+  if (vm.kind != LSMPS_MOMENT_VELOCITY_WALL_DIRICHLET_A || vm.matrix_size != 9 || vm.particle_count < f.count)
+    return fail(ctx, LSMPS_NOT_PREPARED, "PPE requires a prepared velocity Type-A moment matrix");
+  if (pm.kind != LSMPS_MOMENT_PRESSURE_WALL_NEUMANN_A || pm.matrix_size != 9 || pm.particle_count < f.count)
+    return fail(ctx, LSMPS_NOT_PREPARED, "PPE requires a prepared pressure Type-A moment matrix");
+  if (f.count == 0) return LSMPS_OK;
+  if (!ws.matrix.row_offsets || !ws.matrix.col_indices || !ws.matrix.values || !ws.rhs || !ws.divergence ||
+      !tv.vx || !tv.vy || !tv.vz || !vm.inverse_matrices || !pm.inverse_matrices)
+    return fail(ctx, LSMPS_INVALID_ARGUMENT, "PPE workspace requires matrix, rhs, divergence and velocity buffers");
+  if (tw.count > 0 && (!tw.vx || !tw.vy || !tw.vz))
+    return fail(ctx, LSMPS_INVALID_ARGUMENT, "PPE RHS assembly requires temporary wall velocity buffers");
+  PpeArgs a{};
+  a.fluid = f;
+  a.walls = w;
+  a.fo = fn.offsets;
+  a.fi = fn.indices;
+  a.wo = wn.offsets;
+  a.wi = wn.indices;
+  a.tvx = tv.vx;
+  a.tvy = tv.vy;
+  a.tvz = tv.vz;
+  a.twx = tw.vx;
+  a.twy = tw.vy;
+  a.twz = tw.vz;
+  a.vinv = vm.inverse_matrices;
+  a.pinv = pm.inverse_matrices;
+  a.re = pm.support_radius;
+  a.inv_re = 1.0 / pm.support_radius;
+  a.vwall_scale = vm.wall_weight_scale;
+  a.pwall_scale = pm.wall_weight_scale;
+  a.density = p.density;
+  a.dt = p.time_step;
+  a.gx = p.gravity[0];
+  a.gy = p.gravity[1];
+  a.gz = p.gravity[2];
+  a.row_offsets = ws.matrix.row_offsets;
+  a.col = ws.matrix.col_indices;
+  a.val = ws.matrix.values;
+  a.rhs = ws.rhs;
+  a.divergence = ws.divergence;
+  a.wall_rhs_out = ws.pressure_laplacian;
+  launch(ctx, ppe_kernel, dim3(div_up(static_cast<long long>(f.count), kThreads)), dim3(kThreads), 0, a);
+  return check_launch(ctx, "PPE assembly");
+}
+
+}  // namespace lsmps
+
+using namespace lsmps;
+
+extern "C" lsmps_status lsmps_assemble_ppe(lsmps_ctx* ctx, const lsmps_fluid* fluid, const lsmps_walls* walls,
+                                           const lsmps_params* params, const lsmps_csr* fn, const lsmps_csr* wn,
+                                           const lsmps_fluid* tv, const lsmps_walls* tw, const lsmps_moment* vm,
+                                           const lsmps_moment* pm, const lsmps_ppe* ws) {
+  if (!ctx || !fluid || !walls || !params || !fn || !wn || !tv || !tw || !vm || !pm || !ws)
+    return LSMPS_INVALID_ARGUMENT;
+  lsmps_status st = begin_call(ctx);
+  if (st) return st;
+  return end_call(ctx, assemble_ppe_impl(ctx, *fluid, *walls, *params, *fn, *wn, *tv, *tw, *vm, *pm, *ws));
+}

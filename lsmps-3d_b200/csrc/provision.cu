@@ -1,0 +1,194 @@
+// provision.cu - explicit viscous/gravity update u* (the PPE's velocity input).
+// Replaces DeviceProvisionExplicitUpdate::compute_temporary_velocity of
+// src/provision/explicit_update.cu:366-399: compute_velocity_laplacian_kernel
+// (:178-248), combine_explicit_velocity_kernel (:250-270) and
+// combine_explicit_wall_velocity_kernel (:272-284).
+#include "impl.cuh"
+
+namespace lsmps {
+namespace {
+
+constexpr int kThreads = 128;
+
+struct LaplacianArgs {
+  lsmps_fluid fluid;
+  lsmps_walls walls;
+  const index_t* fo;
+  const index_t* fi;
+  const index_t* wo;
+  const index_t* wi;
+  const double* inverse;
+  double re;
+  double inv_re;
+  double wall_scale;
+  double* lx;
+  double* ly;
+  double* lz;
+};
+
+// accumulate_velocity_rhs, explicit_update.cu:148-162
+__device__ __forceinline__ void acc_rhs(const double b[9], double w, double ux, double uy, double uz, double rx[9],
+                                        double ry[9], double rz[9]) {
+#pragma unroll
+  for (int r = 0; r < 9; ++r) {
+    const double wb = w * b[r];
+    rx[r] = fma(wb, ux, rx[r]);
+    ry[r] = fma(wb, uy, ry[r]);
+    rz[r] = fma(wb, uz, rz[r]);
+  }
+}
+
+// laplacian_from_inverse_rhs, explicit_update.cu:164-176
+__device__ __forceinline__ double lap_from(const double* __restrict__ inv, const double rhs[9], double re) {
+  double second = 0.0;
+#pragma unroll
+  for (int r = 3; r <= 5; ++r) {
+    double c = 0.0;
+#pragma unroll
+    for (int col = 0; col < 9; ++col) c = fma(inv[r + col * 9], rhs[col], c);
+    second += c;
+  }
+  return 2.0 * second / (re * re);
+}
+
+__global__ void __launch_bounds__(kThreads) laplacian_kernel(LaplacianArgs a) {
+  const index_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= static_cast<index_t>(a.fluid.count)) return;
+  const double* __restrict__ fx = a.fluid.x;
+  const double* __restrict__ fy = a.fluid.y;
+  const double* __restrict__ fz = a.fluid.z;
+  const double* __restrict__ vx = a.fluid.vx;
+  const double* __restrict__ vy = a.fluid.vy;
+  const double* __restrict__ vz = a.fluid.vz;
+  const double xi = fx[i], yi = fy[i], zi = fz[i];
+  const double uxi = vx[i], uyi = vy[i], uzi = vz[i];
+  double rx[9], ry[9], rz[9], b[9];
+#pragma unroll
+  for (int r = 0; r < 9; ++r) rx[r] = ry[r] = rz[r] = 0.0;
+  const index_t fe = a.fo[i + 1];
+  for (index_t o = a.fo[i]; o < fe; ++o) {
+    const index_t j = a.fi[o];
+    const double dx = fx[j] - xi, dy = fy[j] - yi, dz = fz[j] - zi;
+    const double w = lin_weight(sqrt(dx * dx + dy * dy + dz * dz), a.re);
+    if (w <= 0.0) continue;
+    basis_a_mul(dx, dy, dz, a.inv_re, b);
+    acc_rhs(b, w, vx[j] - uxi, vy[j] - uyi, vz[j] - uzi, rx, ry, rz);
+  }
+  const index_t we = a.wo[i + 1];
+  for (index_t o = a.wo[i]; o < we; ++o) {
+    const index_t j = a.wi[o];
+    const double dx = a.walls.x[j] - xi, dy = a.walls.y[j] - yi, dz = a.walls.z[j] - zi;
+    const double w = a.wall_scale * lin_weight(sqrt(dx * dx + dy * dy + dz * dz), a.re);
+    if (w <= 0.0) continue;
+    basis_a_mul(dx, dy, dz, a.inv_re, b);
+    acc_rhs(b, w, a.walls.vx[j] - uxi, a.walls.vy[j] - uyi, a.walls.vz[j] - uzi, rx, ry, rz);
+  }
+  const double* inv = a.inverse + static_cast<size_t>(i) * 81;
+  a.lx[i] = lap_from(inv, rx, a.re);
+  a.ly[i] = lap_from(inv, ry, a.re);
+  a.lz[i] = lap_from(inv, rz, a.re);
+}
+
+// combine_explicit_velocity_kernel, explicit_update.cu:250-270
+__global__ void combine_kernel(lsmps_fluid f, lsmps_params p, const double* __restrict__ lx,
+                               const double* __restrict__ ly, const double* __restrict__ lz, double* tx, double* ty,
+                               double* tz) {
+  for (index_t i = blockIdx.x * blockDim.x + threadIdx.x; i < static_cast<index_t>(f.count);
+       i += gridDim.x * blockDim.x) {
+    const bool splash = f.surface_type != nullptr && f.surface_type[i] == LSMPS_SURFACE_SPLASH;
+    const double nu = splash ? 0.0 : p.kinematic_viscosity;
+    const double dt = p.time_step;
+    tx[i] = f.vx[i] + dt * (nu * lx[i] + p.gravity[0]);
+    ty[i] = f.vy[i] + dt * (nu * ly[i] + p.gravity[1]);
+    tz[i] = f.vz[i] + dt * (nu * lz[i] + p.gravity[2]);
+  }
+}
+
+// combine_explicit_wall_velocity_kernel, explicit_update.cu:272-284
+__global__ void wall_combine_kernel(lsmps_walls w, lsmps_params p, double* tx, double* ty, double* tz) {
+  for (index_t i = blockIdx.x * blockDim.x + threadIdx.x; i < static_cast<index_t>(w.count);
+       i += gridDim.x * blockDim.x) {
+    const double dt = p.time_step;
+    tx[i] = w.vx[i] + dt * p.gravity[0];
+    ty[i] = w.vy[i] + dt * p.gravity[1];
+    tz[i] = w.vz[i] + dt * p.gravity[2];
+  }
+}
+
+int pointwise_blocks(lsmps_ctx* ctx, size_t n) {
+  const long long b = div_up(static_cast<long long>(n), 256);
+  const long long cap = static_cast<long long>(ctx->sm_count) * 8;
+  return static_cast<int>(b < cap ? b : cap);
+}
+
+}  // namespace
+
+lsmps_status velocity_laplacian_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const lsmps_walls& w,
+                                     const lsmps_csr& fn, const lsmps_csr& wn, const lsmps_moment& vm,
+                                     const lsmps_vector& lap) {
+  if (vm.kind != LSMPS_MOMENT_VELOCITY_WALL_DIRICHLET_A || vm.matrix_size != 9 || vm.particle_count < f.count)
+    return fail(ctx, LSMPS_NOT_PREPARED, "Provision requires a prepared velocity Type-A moment matrix");
+  if (lap.count < f.count) return fail(ctx, LSMPS_INVALID_ARGUMENT, "Provision laplacian workspace is too small");
+  if (f.count == 0) return LSMPS_OK;
+  if (!vm.inverse_matrices || !lap.x || !lap.y || !lap.z || !f.vx || !f.vy || !f.vz)
+    return fail(ctx, LSMPS_INVALID_ARGUMENT, "Provision buffers missing");
+  LaplacianArgs a{f, w, fn.offsets, fn.indices, wn.offsets, wn.indices, vm.inverse_matrices, vm.support_radius,
+                  1.0 / vm.support_radius, vm.wall_weight_scale, lap.x, lap.y, lap.z};
+  launch(ctx, laplacian_kernel, dim3(div_up(static_cast<long long>(f.count), kThreads)), dim3(kThreads), 0, a);
+  return check_launch(ctx, "velocity laplacian");
+}
+
+lsmps_status temporary_velocity_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const lsmps_params& p,
+                                     const lsmps_vector& lap, const lsmps_fluid& t) {
+  if (t.count < f.count || lap.count < f.count)
+    return fail(ctx, LSMPS_INVALID_ARGUMENT, "Provision temporary velocity target is smaller than fluid particle count");
+  if (f.count == 0) return LSMPS_OK;
+  if (!t.vx || !t.vy || !t.vz) return fail(ctx, LSMPS_INVALID_ARGUMENT, "temporary velocity requires vx/vy/vz");
+  launch(ctx, combine_kernel, dim3(pointwise_blocks(ctx, f.count)), dim3(256), 0, f, p,
+         static_cast<const double*>(lap.x), static_cast<const double*>(lap.y), static_cast<const double*>(lap.z),
+         t.vx, t.vy, t.vz);
+  return check_launch(ctx, "temporary velocity");
+}
+
+lsmps_status temporary_wall_velocity_impl(lsmps_ctx* ctx, const lsmps_walls& w, const lsmps_params& p,
+                                          const lsmps_walls& t) {
+  if (t.count < w.count)
+    return fail(ctx, LSMPS_INVALID_ARGUMENT, "Provision temporary wall velocity target is smaller than wall particle count");
+  if (w.count == 0) return LSMPS_OK;
+  if (!t.vx || !t.vy || !t.vz) return fail(ctx, LSMPS_INVALID_ARGUMENT, "temporary wall velocity requires vx/vy/vz");
+  launch(ctx, wall_combine_kernel, dim3(pointwise_blocks(ctx, w.count)), dim3(256), 0, w, p, t.vx, t.vy, t.vz);
+  return check_launch(ctx, "temporary wall velocity");
+}
+
+}  // namespace lsmps
+
+using namespace lsmps;
+
+extern "C" {
+
+lsmps_status lsmps_velocity_laplacian(lsmps_ctx* ctx, const lsmps_fluid* fluid, const lsmps_walls* walls,
+                                      const lsmps_csr* fn, const lsmps_csr* wn, const lsmps_moment* vm,
+                                      const lsmps_vector* lap) {
+  if (!ctx || !fluid || !walls || !fn || !wn || !vm || !lap) return LSMPS_INVALID_ARGUMENT;
+  lsmps_status st = begin_call(ctx);
+  if (st) return st;
+  return end_call(ctx, velocity_laplacian_impl(ctx, *fluid, *walls, *fn, *wn, *vm, *lap));
+}
+
+lsmps_status lsmps_temporary_velocity(lsmps_ctx* ctx, const lsmps_fluid* fluid, const lsmps_params* params,
+                                      const lsmps_vector* lap, const lsmps_fluid* t) {
+  if (!ctx || !fluid || !params || !lap || !t) return LSMPS_INVALID_ARGUMENT;
+  lsmps_status st = begin_call(ctx);
+  if (st) return st;
+  return end_call(ctx, temporary_velocity_impl(ctx, *fluid, *params, *lap, *t));
+}
+
+lsmps_status lsmps_temporary_wall_velocity(lsmps_ctx* ctx, const lsmps_walls* walls, const lsmps_params* params,
+                                           const lsmps_walls* t) {
+  if (!ctx || !walls || !params || !t) return LSMPS_INVALID_ARGUMENT;
+  lsmps_status st = begin_call(ctx);
+  if (st) return st;
+  return end_call(ctx, temporary_wall_velocity_impl(ctx, *walls, *params, *t));
+}
+
+}  // extern "C"

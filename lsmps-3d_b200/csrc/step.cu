@@ -1,0 +1,41 @@
+// step.cu - one LSMPS time step on caller-owned buffers, in the reference
+// driver's order (src/app/simulation_driver.cu:346-383 without the PPE solve
+// and the I/O): moments -> provision -> PPE assembly -> pressure correction ->
+// neighbour rebuild -> surface labels.  All work is queued on the context's
+// stream with no host synchronisation inside, so a step can be captured in a
+// CUDA graph once the context's scratch is reserved.
+#include "impl.cuh"
+
+using namespace lsmps;
+
+extern "C" lsmps_status lsmps_step(lsmps_ctx* ctx, const lsmps_params* params, const lsmps_step_state* s) {
+  if (!ctx || !params || !s) return LSMPS_INVALID_ARGUMENT;
+  lsmps_status st = begin_call(ctx);
+  if (st) return st;
+  Scratch scratch(ctx);
+  if (!scratch.reserve(neighbor_scratch_bytes(s->fluid.count, s->walls.count, s->fluid_cells.cell_count)))
+    return fail(ctx, LSMPS_CUDA_ERROR, "scratch allocation failed (reserve before graph capture)");
+  // The driver prepares the moment caches once per geometry generation; the
+  // geometry changes every step, so every step builds them once.
+  const lsmps_moment kinds[2] = {s->velocity_moment, s->pressure_moment};
+  st = prepare_moments_impl(ctx, s->fluid, s->walls, s->fluid_neighbors, s->wall_neighbors, *params, kinds, 2);
+  if (!st)
+    st = velocity_laplacian_impl(ctx, s->fluid, s->walls, s->fluid_neighbors, s->wall_neighbors, s->velocity_moment,
+                                 s->velocity_laplacian);
+  if (!st) st = temporary_velocity_impl(ctx, s->fluid, *params, s->velocity_laplacian, s->temporary_velocity);
+  if (!st) st = temporary_wall_velocity_impl(ctx, s->walls, *params, s->temporary_wall_velocity);
+  if (!st)
+    st = assemble_ppe_impl(ctx, s->fluid, s->walls, *params, s->fluid_neighbors, s->wall_neighbors,
+                           s->temporary_velocity, s->temporary_wall_velocity, s->velocity_moment,
+                           s->pressure_moment, s->ppe);
+  if (!st)
+    st = pressure_correction_impl(ctx, s->fluid, s->walls, s->fluid_neighbors, s->wall_neighbors,
+                                  s->temporary_velocity, s->pressure, *params, s->pressure_moment,
+                                  s->pressure_gradient, s->ps_displacement, s->smoothed_velocity);
+  if (!st)
+    st = build_neighbor_lists_impl(ctx, scratch, s->fluid, s->walls, *params, s->fluid_cells, s->wall_cells,
+                                   s->fluid_neighbors, s->wall_neighbors);
+  if (!st)
+    st = classify_surface_impl(ctx, s->fluid, s->walls, s->fluid_neighbors, s->wall_neighbors, *params, nullptr);
+  return end_call(ctx, st);
+}

@@ -1,0 +1,250 @@
+// surface.cu - Inner / NearSurface / Surface / Splash labels.
+// Replaces classify_surface_particles (src/surface/surface_detection.cu:522-553):
+// classify_primary_surface_kernel (:199-320) and expand_near_surface_kernel
+// (:322-348), plus the host-side reference number density (:494-520).
+//
+// The labels compare floating sums with thresholds, so each particle's sums
+// are accumulated by one thread in CSR row order with the reference's own
+// expressions: the FP64 values, and hence the labels, are the reference's.
+#include <cmath>
+
+#include "impl.cuh"
+
+namespace lsmps {
+namespace {
+
+constexpr int kSurfaceThreads = 128;
+
+__device__ __forceinline__ double safe_rsqrt(double v) { return rsqrt(v > 1.0e-20 ? v : 1.0e-20); }
+
+// accumulate_neighbor_moments, surface_detection.cu:33-59
+__device__ __forceinline__ void accumulate(double dx, double dy, double dz, double re, double& nd, double& sx,
+                                           double& sy, double& sz, int& weighted) {
+  const double d2 = dx * dx + dy * dy + dz * dz;
+  if (d2 <= 0.0) return;
+  const double d = sqrt(d2);
+  const double w = lin_weight(d, re);
+  if (w <= 0.0) return;
+  const double inv_d = 1.0 / d;
+  nd += w;
+  sx += w * dx * inv_d;
+  sy += w * dy * inv_d;
+  sz += w * dz * inv_d;
+  ++weighted;
+}
+
+struct Basis3 {
+  int count;
+  double x[3], y[3], z[3];
+};
+
+// add_wall_basis_direction, surface_detection.cu:123-149
+__device__ __forceinline__ void add_direction(Basis3& b, double x, double y, double z, double thr) {
+  double rx = x, ry = y, rz = z;
+  for (int k = 0; k < b.count; ++k) {
+    const double proj = rx * b.x[k] + ry * b.y[k] + rz * b.z[k];
+    rx -= proj * b.x[k];
+    ry -= proj * b.y[k];
+    rz -= proj * b.z[k];
+  }
+  const double len2 = rx * rx + ry * ry + rz * rz;
+  if (len2 <= thr * thr || b.count >= 3) return;
+  const double inv = safe_rsqrt(len2);
+  b.x[b.count] = rx * inv;
+  b.y[b.count] = ry * inv;
+  b.z[b.count] = rz * inv;
+  ++b.count;
+}
+
+struct SurfaceArgs {
+  lsmps_fluid fluid;
+  lsmps_walls walls;
+  const index_t* fo;
+  const index_t* fi;
+  const index_t* wo;
+  const index_t* wi;
+  lsmps_params p;
+  double n0;
+  lsmps_surface_diagnostics diag;
+};
+
+__global__ void __launch_bounds__(kSurfaceThreads) classify_kernel(SurfaceArgs a) {
+  const index_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= static_cast<index_t>(a.fluid.count)) return;
+  const double* __restrict__ fx = a.fluid.x;
+  const double* __restrict__ fy = a.fluid.y;
+  const double* __restrict__ fz = a.fluid.z;
+  const index_t fb = a.fo[i], fe = a.fo[i + 1];
+  const index_t wb = a.wo[i], we = a.wo[i + 1];
+  const index_t fcount = fe - fb, wcount = we - wb;
+  const index_t cls = a.p.include_wall_neighbors ? fcount + wcount : fcount;
+  const double re = a.p.support_radius;
+  const double px = fx[i], py = fy[i], pz = fz[i];
+  double nd = 0.0, sx = 0.0, sy = 0.0, sz = 0.0;
+  int weighted = 0;
+  for (index_t o = fb; o < fe; ++o) {
+    const index_t j = a.fi[o];
+    accumulate(fx[j] - px, fy[j] - py, fz[j] - pz, re, nd, sx, sy, sz, weighted);
+  }
+  if (a.p.include_wall_neighbors) {
+    for (index_t o = wb; o < we; ++o) {
+      const index_t j = a.wi[o];
+      accumulate(a.walls.x[j] - px, a.walls.y[j] - py, a.walls.z[j] - pz, re, nd, sx, sy, sz, weighted);
+    }
+  }
+  double aniso = 0.0;
+  if (weighted > 0) aniso = sqrt(sx * sx + sy * sy + sz * sz) / static_cast<double>(weighted);
+  const double ratio = nd / a.n0;
+  const double mx = -sx, my = -sy, mz = -sz;
+  const double ml2 = mx * mx + my * my + mz * mz;
+  double ax = mx, ay = my, az = mz;
+  if (ml2 > 0.0 && a.p.include_wall_neighbors) {
+    // build_wall_basis, surface_detection.cu:151-197
+    Basis3 basis;
+    basis.count = 0;
+    for (index_t o = wb; o < we; ++o) {
+      const index_t j = a.wi[o];
+      const double dx = a.walls.x[j] - px, dy = a.walls.y[j] - py, dz = a.walls.z[j] - pz;
+      const double d2 = dx * dx + dy * dy + dz * dz;
+      if (d2 <= 0.0) continue;
+      const double d = sqrt(d2);
+      if (lin_weight(d, re) <= 0.0) continue;
+      const double nx = a.walls.normal_x[j], ny = a.walls.normal_y[j], nz = a.walls.normal_z[j];
+      const double nl2 = nx * nx + ny * ny + nz * nz;
+      if (nl2 <= 0.0) continue;
+      const double inv = safe_rsqrt(nl2);
+      add_direction(basis, -nx * inv, -ny * inv, -nz * inv, a.p.wall_normal_independence_threshold);
+    }
+    for (int k = 0; k < basis.count; ++k) {
+      const double proj = ax * basis.x[k] + ay * basis.y[k] + az * basis.z[k];
+      if (proj > 0.0) {
+        ax -= proj * basis.x[k];
+        ay -= proj * basis.y[k];
+        az -= proj * basis.z[k];
+      }
+    }
+  }
+  const double al2 = ax * ax + ay * ay + az * az;
+  const double al = sqrt(al2);
+  const double ml = sqrt(ml2);
+  const double open = ml > 0.0 ? al / ml : 0.0;
+  const double aaniso = weighted > 0 ? al / static_cast<double>(weighted) : 0.0;
+  int type = LSMPS_SURFACE_INNER;
+  if (cls < a.p.splash_neighbor_threshold) {
+    type = LSMPS_SURFACE_SPLASH;
+  } else if (ratio < a.p.number_density_ratio_threshold && open > a.p.air_open_ratio_threshold &&
+             aaniso > a.p.air_anisotropy_threshold) {
+    type = LSMPS_SURFACE_SURFACE;
+  }
+  a.fluid.surface_type[i] = type;
+  const lsmps_surface_diagnostics& d = a.diag;
+  if (d.fluid_neighbor_count) d.fluid_neighbor_count[i] = fcount;
+  if (d.wall_neighbor_count) d.wall_neighbor_count[i] = wcount;
+  if (d.number_density) d.number_density[i] = nd;
+  if (d.number_density_ratio) d.number_density_ratio[i] = ratio;
+  if (d.anisotropy) d.anisotropy[i] = aniso;
+  if (d.air_open_ratio) d.air_open_ratio[i] = open;
+  if (d.air_anisotropy) d.air_anisotropy[i] = aaniso;
+  if (d.surface_normal_x || d.surface_normal_y || d.surface_normal_z) {
+    double snx = 0.0, sny = 0.0, snz = 0.0;
+    if (al2 > 0.0) {
+      const double inv = safe_rsqrt(al2);
+      snx = ax * inv;
+      sny = ay * inv;
+      snz = az * inv;
+    }
+    if (d.surface_normal_x) d.surface_normal_x[i] = snx;
+    if (d.surface_normal_y) d.surface_normal_y[i] = sny;
+    if (d.surface_normal_z) d.surface_normal_z[i] = snz;
+  }
+}
+
+// expand_near_surface_kernel, surface_detection.cu:322-348.  Only Inner rows
+// are written and only Surface labels are read, so the pass is race-free.
+__global__ void __launch_bounds__(kSurfaceThreads) expand_kernel(const double* __restrict__ fx,
+                                                                 const double* __restrict__ fy,
+                                                                 const double* __restrict__ fz, int32_t* type,
+                                                                 index_t n, const index_t* __restrict__ fo,
+                                                                 const index_t* __restrict__ fi, double r2) {
+  const index_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || type[i] != LSMPS_SURFACE_INNER) return;
+  const double px = fx[i], py = fy[i], pz = fz[i];
+  for (index_t o = fo[i]; o < fo[i + 1]; ++o) {
+    const index_t j = fi[o];
+    if (type[j] != LSMPS_SURFACE_SURFACE) continue;
+    const double dx = fx[j] - px, dy = fy[j] - py, dz = fz[j] - pz;
+    if (dx * dx + dy * dy + dz * dz <= r2) {
+      type[i] = LSMPS_SURFACE_NEAR_SURFACE;
+      return;
+    }
+  }
+}
+
+}  // namespace
+
+// compute_uniform_reference_number_density, surface_detection.cu:494-520.
+double reference_number_density(double l0, double re) {
+  if (!(l0 > 0.0) || !(re > 0.0)) return -1.0;
+  const int extent = static_cast<int>(std::ceil(re / l0));
+  double n0 = 0.0;
+  for (int iz = -extent; iz <= extent; ++iz)
+    for (int iy = -extent; iy <= extent; ++iy)
+      for (int ix = -extent; ix <= extent; ++ix) {
+        if (ix == 0 && iy == 0 && iz == 0) continue;
+        const double dx = ix * l0, dy = iy * l0, dz = iz * l0;
+        const double d = std::sqrt(dx * dx + dy * dy + dz * dz);
+        n0 += d >= re ? 0.0 : 1.0 - d / re;
+      }
+  return n0;
+}
+
+lsmps_status classify_surface_impl(lsmps_ctx* ctx, const lsmps_fluid& fluid, const lsmps_walls& walls,
+                                   const lsmps_csr& fn, const lsmps_csr& wn, const lsmps_params& p,
+                                   const lsmps_surface_diagnostics* diag) {
+  if (!(p.support_radius > 0.0))
+    return fail(ctx, LSMPS_INVALID_ARGUMENT, "Surface detection support radius must be positive");
+  if (fluid.count > fn.particle_count || fluid.count > wn.particle_count)
+    return fail(ctx, LSMPS_INVALID_ARGUMENT, "Surface detection neighbor lists are smaller than fluid particle count");
+  if (p.near_surface_radius < 0.0) return fail(ctx, LSMPS_INVALID_ARGUMENT, "Near-surface radius must be non-negative");
+  const double n0 = reference_number_density(p.particle_spacing, p.support_radius);
+  if (!(n0 > 0.0)) return fail(ctx, LSMPS_INVALID_ARGUMENT, "Reference number density must be positive");
+  if (fluid.count == 0) return LSMPS_OK;
+  if (!fluid.surface_type) return fail(ctx, LSMPS_INVALID_ARGUMENT, "surface_type buffer missing");
+  SurfaceArgs a{};
+  a.fluid = fluid;
+  a.walls = walls;
+  a.fo = fn.offsets;
+  a.fi = fn.indices;
+  a.wo = wn.offsets;
+  a.wi = wn.indices;
+  a.p = p;
+  a.n0 = n0;
+  if (diag) a.diag = *diag;
+  const index_t n = static_cast<index_t>(fluid.count);
+  launch(ctx, classify_kernel, dim3(div_up(n, kSurfaceThreads)), dim3(kSurfaceThreads), 0, a);
+  if (p.near_surface_radius > 0.0)
+    launch(ctx, expand_kernel, dim3(div_up(n, kSurfaceThreads)), dim3(kSurfaceThreads), 0,
+           static_cast<const double*>(fluid.x), static_cast<const double*>(fluid.y),
+           static_cast<const double*>(fluid.z), fluid.surface_type, n, static_cast<const index_t*>(fn.offsets),
+           static_cast<const index_t*>(fn.indices), p.near_surface_radius * p.near_surface_radius);
+  return check_launch(ctx, "surface classification");
+}
+
+}  // namespace lsmps
+
+using namespace lsmps;
+
+extern "C" double lsmps_reference_number_density(double particle_spacing, double support_radius) {
+  return reference_number_density(particle_spacing, support_radius);
+}
+
+extern "C" lsmps_status lsmps_classify_surface(lsmps_ctx* ctx, const lsmps_fluid* fluid, const lsmps_walls* walls,
+                                               const lsmps_csr* fluid_neighbors, const lsmps_csr* wall_neighbors,
+                                               const lsmps_params* params,
+                                               const lsmps_surface_diagnostics* diagnostics) {
+  if (!ctx || !fluid || !walls || !fluid_neighbors || !wall_neighbors || !params) return LSMPS_INVALID_ARGUMENT;
+  lsmps_status st = begin_call(ctx);
+  if (st) return st;
+  st = classify_surface_impl(ctx, *fluid, *walls, *fluid_neighbors, *wall_neighbors, *params, diagnostics);
+  return end_call(ctx, st);
+}

@@ -1,0 +1,340 @@
+"""Parity of the sm_100a path (through the C ABI) with the CPU oracle.
+
+Integer outputs (sorted cell ids, sorted indices, cell ranges, CSR offsets
+and rows in their native order, surface labels) must be bit-exact.  Floating
+outputs are compared per element as |gpu - oracle| / max(|oracle|, floor)
+where floor = 1e-6 * max|oracle| of that output; the plain (FP64) form must
+stay within PLAIN_RTOL.  The two sides differ only in operation order (FMA
+contraction, multiply-by-reciprocal) and, for the moment inverse, in the
+factorisation route (L^-T L^-1 versus substitution against identity columns),
+so the bound is set by rounding times the moment matrices' conditioning.
+"""
+
+import numpy as np
+import pytest
+
+from kat_util import buffers_from, params_from, rows
+
+pytestmark = pytest.mark.gpu
+
+PLAIN_RTOL = 1e-9
+
+
+def rel_err(g, o, floor_frac=1e-6):
+    g = np.asarray(g, dtype=np.float64)
+    o = np.asarray(o, dtype=np.float64)
+    if o.size == 0:
+        return 0.0
+    floor = floor_frac * max(float(np.max(np.abs(o))), 1e-300)
+    return float(np.max(np.abs(g - o) / np.maximum(np.abs(o), floor)))
+
+
+def both(pkg, device_api, case_or_kat, kat=False, **kw):
+    """Device and host StepBuffers loaded with the same input."""
+    if kat:
+        dev = buffers_from(pkg, pkg.buffers.TorchAlloc("cuda"), case_or_kat)
+        host = buffers_from(pkg, pkg.buffers.NumpyAlloc(), case_or_kat)
+    else:
+        c = case_or_kat
+        dev = pkg.buffers.StepBuffers(pkg.buffers.TorchAlloc("cuda"), c.n_fluid, c.n_wall, c.n_cells, **kw)
+        host = pkg.buffers.StepBuffers(pkg.buffers.NumpyAlloc(), c.n_fluid, c.n_wall, c.n_cells, **kw)
+        dev.load_case(c)
+        host.load_case(c)
+    return dev, host
+
+
+@pytest.fixture(scope="module")
+def ctx(device_api):
+    return device_api.Context(0)
+
+
+# --- reference known-answer tests on the device -----------------------------
+
+def test_neighbor_search_kat_gpu(pkg, device_api, ctx, oracle, kats):
+    k = kats["neighbor_search"]
+    dev, host = both(pkg, device_api, k, kat=True)
+    p = params_from(pkg, k)
+    ctx.build_neighbor_lists(dev, p)
+    off, idx = dev.csr_rows("fluid")
+    assert off.tolist() == k["expected_fluid_offsets"]
+    assert rows(off, idx, 5) == [sorted(x) for x in k["expected_fluid_rows"]]
+    off, idx = dev.csr_rows("wall")
+    assert off.tolist() == k["expected_wall_offsets"]
+    assert rows(off, idx, 5) == [sorted(x) for x in k["expected_wall_rows"]]
+    oracle.build_neighbor_lists(host, p)
+    for which in ("fluid", "wall"):
+        go, gi = dev.csr_rows(which)
+        ho, hi = host.csr_rows(which)
+        assert np.array_equal(go, ho) and np.array_equal(gi, hi)
+
+
+def test_neighbor_capacity_exceeded_gpu(pkg, device_api, ctx, kats):
+    k = kats["neighbor_search"]
+    dev = buffers_from(pkg, pkg.buffers.TorchAlloc("cuda"), k)
+    dev.cap_f = 5
+    p = params_from(pkg, k)
+    with pytest.raises(device_api.LsmpsError) as e:
+        ctx.build_neighbor_lists(dev, p)
+    assert e.value.status == pkg.abi.CAPACITY_EXCEEDED and ctx.required == 6
+
+
+def test_surface_detection_kat_gpu(pkg, device_api, ctx, kats):
+    k = kats["surface_detection"]
+    dev = buffers_from(pkg, pkg.buffers.TorchAlloc("cuda"), k)
+    p = params_from(pkg, k)
+    ctx.build_neighbor_lists(dev, p)
+    ctx.classify_surface(dev, p)
+    lab = dev.numpy("fluid")["surface_type"]
+    for i, v in k["expected_labels_at"].items():
+        assert lab[int(i)] == v
+
+
+@pytest.mark.parametrize("name", ["provision", "ppe", "pressure_correction"])
+def test_operator_kats_gpu(pkg, device_api, ctx, oracle, kats, name):
+    k = kats[name]
+    dev, host = both(pkg, device_api, k, kat=True)
+    p = params_from(pkg, k)
+    if name != "provision":
+        for comp in ("vx", "vy", "vz"):
+            dev.alloc.copy_(dev.temporary_velocity[comp], np.asarray(k["fluid"][comp]))
+            host.temporary_velocity[comp][:] = np.asarray(k["fluid"][comp])
+    ctx.prepare_moments(dev, p, [0, 1])
+    oracle.prepare_moment(host, p, 0)
+    oracle.prepare_moment(host, p, 1)
+    c, tol = k["center"], k["tolerance"]
+    if name == "provision":
+        ctx.provision(dev, p)
+        oracle.provision(host, p)
+        lap = dev.numpy("velocity_laplacian")
+        assert abs(lap["x"][c] - k["expected_laplacian_x_center"]) <= tol
+        for comp in ("vx", "vy", "vz"):
+            assert rel_err(dev.numpy("temporary_velocity")[comp], host.temporary_velocity[comp]) < PLAIN_RTOL
+    elif name == "ppe":
+        ctx.assemble_ppe(dev, p)
+        oracle.assemble_ppe(host, p)
+        ppe = dev.numpy("ppe")
+        assert abs(ppe["divergence"][c] - k["expected_divergence_center"]) <= tol
+        assert abs(ppe["rhs"][c] - k["expected_rhs_center"]) <= tol
+        assert np.array_equal(ppe["row_offsets"], host.ppe["row_offsets"])
+        assert np.array_equal(ppe["col_indices"], host.ppe["col_indices"])
+        assert rel_err(ppe["values"], host.ppe["values"]) < PLAIN_RTOL
+    else:
+        ctx.pressure_correction(dev, p)
+        oracle.pressure_correction(host, p)
+        g = dev.numpy("pressure_gradient")
+        assert np.allclose([g[a][c] for a in "xyz"], k["expected_gradient_center"], atol=tol)
+        f = dev.numpy("fluid")
+        for comp in ("x", "y", "z", "vx", "vy", "vz"):
+            assert rel_err(f[comp], host.fluid[comp]) < PLAIN_RTOL
+
+
+# --- full pipeline on seeded synthetic cases ---------------------------------
+
+CASES = [
+    ("hydrostatic", dict(n=20, l0=0.01)),
+    ("dam_break", dict(nx=24, ny=12, nz=24, l0=0.005)),
+    ("splash", dict(nx=40, ny=10, nz=40, l0=0.0025)),
+]
+
+
+@pytest.fixture(scope="module", params=CASES, ids=[c[0] for c in CASES])
+def pipeline(request, pkg, device_api, ctx, oracle):
+    """Run each stage on both sides from the same inputs; return both buffer
+    sets after every stage has been compared."""
+    name, kw = request.param
+    case = pkg.cases.CASES[name](**kw)
+    p = case.params
+    dev, host = both(pkg, device_api, case)
+    ctx.build_neighbor_lists(dev, p)
+    st, req = oracle.build_neighbor_lists(host, p)
+    assert st == 0
+    return case, dev, host
+
+
+def test_cells_bit_exact(pipeline):
+    case, dev, host = pipeline
+    for which in ("fluid_cells", "wall_cells"):
+        g, h = dev.numpy(which), host.numpy(which)
+        for k in ("cell_ids", "sorted_indices", "cell_begin", "cell_end"):
+            assert np.array_equal(g[k], h[k]), (which, k)
+
+
+def test_csr_bit_exact_native_order(pipeline):
+    case, dev, host = pipeline
+    for which in ("fluid", "wall"):
+        go, gi = dev.csr_rows(which)
+        ho, hi = host.csr_rows(which)
+        assert np.array_equal(go, ho), which
+        assert np.array_equal(gi, hi), which
+
+
+def test_pipeline_stages_match_oracle(pkg, pipeline, ctx, oracle):
+    case, dev, host = pipeline
+    p = case.params
+    # labels
+    ctx.classify_surface(dev, p)
+    assert oracle.classify_surface(host, p) == 0
+    assert np.array_equal(dev.numpy("fluid")["surface_type"], host.fluid["surface_type"])
+    # moments (velocity Dirichlet-A and pressure Neumann-A, fused on the device)
+    ctx.prepare_moments(dev, p, [0, 1])
+    for kind in (0, 1):
+        assert oracle.prepare_moment(host, p, kind) == 0
+        gm = {k: dev.alloc.to_numpy(v) for k, v in dev.moments[kind].items()}
+        hm = host.moments[kind]
+        assert np.array_equal(gm["info"], hm["info"])
+        assert gm["inversion_count"][0] >= 1
+        assert rel_err(gm["moment_trace"], hm["moment_trace"]) < 1e-12
+        ok = hm["info"] == 0
+        gi = gm["inverse_matrices"].reshape(-1, 81)[ok]
+        hi = hm["inverse_matrices"].reshape(-1, 81)[ok]
+        per = np.max(np.abs(gi - hi), axis=1) / np.max(np.abs(hi), axis=1)
+        print(f"{case.name} kind {kind}: inverse max rel err {per.max():.3e} median {np.median(per):.3e}")
+        assert per.max() < 1e-7
+    # provision
+    ctx.provision(dev, p)
+    oracle.provision(host, p)
+    for comp in ("vx", "vy", "vz"):
+        e = rel_err(dev.numpy("temporary_velocity")[comp], host.temporary_velocity[comp])
+        assert e < PLAIN_RTOL, (comp, e)
+    # PPE
+    ctx.assemble_ppe(dev, p)
+    oracle.assemble_ppe(host, p)
+    g = dev.numpy("ppe")
+    nnz = int(host.ppe["row_offsets"][-1])
+    assert np.array_equal(g["row_offsets"], host.ppe["row_offsets"])
+    assert np.array_equal(g["col_indices"][:nnz], host.ppe["col_indices"][:nnz])
+    for k in ("values", "rhs", "divergence", "pressure_laplacian"):
+        a, b = (g[k][:nnz], host.ppe[k][:nnz]) if k == "values" else (g[k], host.ppe[k])
+        e = rel_err(a, b)
+        print(f"{case.name} ppe {k}: max rel err {e:.3e}")
+        assert e < 1e-7, (k, e)
+    # correction (pressure = clamped fluid.pressure, in place)
+    ctx.pressure_correction(dev, p)
+    oracle.pressure_correction(host, p)
+    f = dev.numpy("fluid")
+    for comp in ("x", "y", "z", "vx", "vy", "vz", "pressure"):
+        e = rel_err(f[comp], host.fluid[comp])
+        print(f"{case.name} corrected {comp}: max rel err {e:.3e}")
+        assert e < 1e-7, (comp, e)
+
+
+@pytest.mark.parametrize("name,kw", CASES, ids=[c[0] for c in CASES])
+def test_full_step_matches_oracle(pkg, device_api, ctx, oracle, name, kw):
+    """lsmps_step == the oracle's step on the same state (geometry rebuilt
+    first on both sides so both start from identical CSR and labels)."""
+    case = pkg.cases.CASES[name](**kw)
+    p = case.params
+    dev, host = both(pkg, device_api, case)
+    ctx.build_neighbor_lists(dev, p)
+    ctx.classify_surface(dev, p)
+    oracle.build_neighbor_lists(host, p)
+    oracle.classify_surface(host, p)
+    ctx.step(dev, p)
+    st, _ = oracle.step(host, p)
+    assert st == 0
+    assert np.array_equal(dev.numpy("fluid")["surface_type"], host.fluid["surface_type"])
+    for which in ("fluid", "wall"):
+        go, gi = dev.csr_rows(which)
+        ho, hi = host.csr_rows(which)
+        assert np.array_equal(go, ho) and np.array_equal(gi, hi)
+    f = dev.numpy("fluid")
+    for comp in ("x", "y", "z", "vx", "vy", "vz"):
+        assert rel_err(f[comp], host.fluid[comp]) < 1e-7, comp
+
+
+def test_deterministic_repeat(pkg, device_api, ctx):
+    case = pkg.cases.dam_break(nx=16, ny=8, nz=16, l0=0.005)
+    outs = []
+    for _ in range(2):
+        dev = device_api.device_buffers(case)
+        ctx.build_neighbor_lists(dev, case.params)
+        ctx.classify_surface(dev, case.params)
+        ctx.step(dev, case.params)
+        outs.append((dev.csr_rows("fluid"), dev.numpy("fluid")))
+    (o0, f0), (o1, f1) = outs
+    assert np.array_equal(o0[0], o1[0]) and np.array_equal(o0[1], o1[1])
+    for k in f0:
+        assert np.array_equal(f0[k], f1[k]), k
+
+
+# --- edge cases ---------------------------------------------------------------
+
+def test_empty_fluid(pkg, device_api, ctx):
+    case = pkg.cases.hydrostatic_box(n=4)
+    p = case.params
+    b = pkg.buffers.StepBuffers(pkg.buffers.TorchAlloc("cuda"), 0, case.n_wall, case.n_cells)
+    b.load_case(type(case)(case.name, case.l0, {k: v[:0] for k, v in case.fluid.items()}, case.walls, p))
+    ctx.build_neighbor_lists(b, p)
+    assert b.csr_rows("fluid")[0].tolist() == [0]
+    ctx.classify_surface(b, p)
+    ctx.step(b, p)
+
+
+def test_non_finite_coordinate_reported(pkg, device_api, ctx):
+    case = pkg.cases.hydrostatic_box(n=6)
+    case.fluid["x"][3] = np.nan
+    dev = device_api.device_buffers(case)
+    with pytest.raises(device_api.LsmpsError) as e:
+        ctx.build_neighbor_lists(dev, case.params)
+    assert e.value.status == pkg.abi.NON_FINITE
+
+
+def test_overloaded_and_out_of_grid_cells(pkg, device_api, ctx, oracle):
+    """Particles outside the grid are clamped into edge cells
+    (neighbor_search.cu:36-46); an edge cell holding more candidates than the
+    shared-memory stage takes the exact global-memory path.  Rows must still
+    match the oracle bit for bit."""
+    rng = np.random.default_rng(11)
+    case = pkg.cases.hydrostatic_box(n=10, l0=0.01)
+    n = case.n_fluid
+    # pile 1500 particles just outside the low x face (clamped into cells at ix = 0)
+    k = 1500
+    extra = {c: np.asarray(v) for c, v in case.fluid.items()}
+    ox = case.params.grid.origin[0]
+    add = {"x": ox - 0.004 - rng.random(k) * 0.002, "y": 0.02 + rng.random(k) * 0.004,
+           "z": 0.02 + rng.random(k) * 0.004}
+    fluid = {}
+    for c, v in extra.items():
+        if c in add:
+            fluid[c] = np.concatenate([v, add[c]])
+        else:
+            fluid[c] = np.concatenate([v, np.zeros(k, dtype=v.dtype)])
+    big = type(case)(case.name, case.l0, fluid, case.walls, case.params)
+    dev, host = both(pkg, device_api, big, max_fluid_neighbors=2048, max_wall_neighbors=256)
+    ctx.build_neighbor_lists(dev, big.params)
+    oracle.build_neighbor_lists(host, big.params)
+    for which in ("fluid", "wall"):
+        go, gi = dev.csr_rows(which)
+        ho, hi = host.csr_rows(which)
+        assert np.array_equal(go, ho) and np.array_equal(gi, hi)
+    assert n + k == big.n_fluid
+
+
+def test_cell_list_random_keys_stable(pkg, device_api, ctx, oracle):
+    """Radix passes over many digits: random positions on a large grid."""
+    rng = np.random.default_rng(5)
+    n = 300_000
+    grid = pkg.abi.Grid()
+    grid.origin[:] = (0.0, 0.0, 0.0)
+    grid.cell_size = 0.01
+    grid.dims[:] = (180, 160, 150)  # 4.32M cells: 23-bit keys, 3 radix passes
+    x, y, z = (rng.random(n) * d * 0.01 for d in (180, 160, 150))
+    import torch
+
+    t = {c: torch.from_numpy(v).cuda() for c, v in zip("xyz", (x, y, z))}
+    ncell = 180 * 160 * 150
+    out = {k: torch.zeros(n if k in ("cell_ids", "sorted_indices") else ncell, dtype=torch.int32, device="cuda")
+           for k in ("cell_ids", "sorted_indices", "cell_begin", "cell_end")}
+    cv = pkg.abi.Cells()
+    cv.particle_count, cv.cell_count = n, ncell
+    for k, v in out.items():
+        setattr(cv, k, v.data_ptr())
+    ctx.build_cell_list(t["x"].data_ptr(), t["y"].data_ptr(), t["z"].data_ptr(), n, grid, cv)
+    host = {k: np.zeros(v.numel(), np.int32) for k, v in out.items()}
+    hv = pkg.abi.Cells()
+    hv.particle_count, hv.cell_count = n, ncell
+    for k, v in host.items():
+        setattr(hv, k, v.ctypes.data)
+    assert oracle.build_cell_list(x, y, z, grid, hv) == 0
+    for k in out:
+        assert np.array_equal(out[k].cpu().numpy(), host[k]), k
