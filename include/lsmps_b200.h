@@ -264,7 +264,8 @@ typedef struct lsmps_ctx lsmps_ctx;
 lsmps_status lsmps_ctx_create(int device, lsmps_ctx** out);
 void lsmps_ctx_destroy(lsmps_ctx* ctx);
 /* Queue all further work of this context on `stream` (a cudaStream_t; NULL =
- * the context's own non-blocking stream). */
+ * the legacy default stream).  A new context starts on its own non-blocking
+ * stream. */
 lsmps_status lsmps_ctx_set_stream(lsmps_ctx* ctx, void* stream);
 void* lsmps_ctx_stream(lsmps_ctx* ctx);
 lsmps_status lsmps_ctx_set_precision(lsmps_ctx* ctx, int precision);

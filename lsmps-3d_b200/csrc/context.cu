@@ -125,7 +125,9 @@ void lsmps_ctx_destroy(lsmps_ctx* ctx) {
 
 lsmps_status lsmps_ctx_set_stream(lsmps_ctx* ctx, void* stream) {
   if (!ctx) return LSMPS_INVALID_ARGUMENT;
-  ctx->stream = stream ? static_cast<cudaStream_t>(stream) : ctx->own_stream;
+  // NULL selects the legacy default stream, so work orders with other users
+  // of that stream (for example a framework's default stream).
+  ctx->stream = static_cast<cudaStream_t>(stream);
   return LSMPS_OK;
 }
 

@@ -2,9 +2,8 @@
 
 Integer outputs (sorted cell ids, sorted indices, cell ranges, CSR offsets
 and rows in their native order, surface labels) must be bit-exact.  Floating
-outputs are compared per element as |gpu - oracle| / max(|oracle|, floor)
-where floor = 1e-6 * max|oracle| of that output; the plain (FP64) form must
-stay within PLAIN_RTOL.  The two sides differ only in operation order (FMA
+outputs are compared with the metric of rel_err below; the plain (FP64) form must stay within
+PLAIN_RTOL.  The two sides differ only in operation order (FMA
 contraction, multiply-by-reciprocal) and, for the moment inverse, in the
 factorisation route (L^-T L^-1 versus substitution against identity columns),
 so the bound is set by rounding times the moment matrices' conditioning.
@@ -20,13 +19,21 @@ pytestmark = pytest.mark.gpu
 PLAIN_RTOL = 1e-9
 
 
-def rel_err(g, o, floor_frac=1e-6):
+def rel_err(g, o, floor_frac=1e-3):
+    """max(normwise, elementwise) relative error: normwise = max|g-o| / max|o|;
+    elementwise = max |g-o|/|o| over the entries with |o| >= floor_frac max|o|
+    (entries that cancel to near zero are covered by the normwise term)."""
     g = np.asarray(g, dtype=np.float64)
     o = np.asarray(o, dtype=np.float64)
     if o.size == 0:
         return 0.0
-    floor = floor_frac * max(float(np.max(np.abs(o))), 1e-300)
-    return float(np.max(np.abs(g - o) / np.maximum(np.abs(o), floor)))
+    scale = float(np.max(np.abs(o)))
+    if scale == 0.0:
+        return float(np.max(np.abs(g)))
+    d = np.abs(g - o)
+    big = np.abs(o) >= floor_frac * scale
+    elem = float(np.max(d[big] / np.abs(o[big]))) if big.any() else 0.0
+    return max(float(np.max(d)) / scale, elem)
 
 
 def both(pkg, device_api, case_or_kat, kat=False, **kw):
