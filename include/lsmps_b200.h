@@ -281,6 +281,16 @@ lsmps_status lsmps_ctx_synchronize(lsmps_ctx* ctx);
 uint64_t lsmps_ctx_required(lsmps_ctx* ctx);
 /* Number of kernel launches this context has queued since creation. */
 uint64_t lsmps_ctx_launch_count(lsmps_ctx* ctx);
+/* Per-kernel device timing (no counterpart in the reference, which has no
+ * tracing): while on, every launch is bracketed by CUDA events.  Turning it
+ * on clears the records. */
+lsmps_status lsmps_ctx_set_profiling(lsmps_ctx* ctx, int on);
+/* Waits for the stream, aggregates the records by kernel name in order of
+ * first launch, writes the names '\n'-separated into `names`, the summed
+ * milliseconds and launch counts into the arrays, clears the records and
+ * returns the number of entries (-1 on error). */
+int lsmps_ctx_profile_report(lsmps_ctx* ctx, char* names, size_t names_len, double* total_ms,
+                             uint64_t* launches, int max_entries);
 const char* lsmps_ctx_last_error(lsmps_ctx* ctx);
 const char* lsmps_status_string(int status);
 /* SimulationConfig defaults (include/lsmps3d/core/config.hpp:12-60). */

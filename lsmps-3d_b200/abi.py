@@ -231,6 +231,8 @@ _SIGNATURES = {
     "lsmps_ctx_synchronize": (c_int, [c_void_p]),
     "lsmps_ctx_required": (c_uint64, [c_void_p]),
     "lsmps_ctx_launch_count": (c_uint64, [c_void_p]),
+    "lsmps_ctx_set_profiling": (c_int, [c_void_p, c_int]),
+    "lsmps_ctx_profile_report": (c_int, [c_void_p, ctypes.c_char_p, c_size_t, P(c_double), P(c_uint64), c_int]),
     "lsmps_ctx_last_error": (c_char_p, [c_void_p]),
     "lsmps_status_string": (c_char_p, [c_int]),
     "lsmps_params_default": (None, [P(Params)]),

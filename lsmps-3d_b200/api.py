@@ -89,6 +89,21 @@ class Context:
     def synchronize(self) -> None:
         self.check(_lib.lsmps_ctx_synchronize(self.h))
 
+    def set_profiling(self, on: bool) -> None:
+        self.check(_lib.lsmps_ctx_set_profiling(self.h, 1 if on else 0))
+
+    def profile_report(self, max_entries: int = 64) -> list[tuple[str, float, int]]:
+        """(kernel name, total ms, launches) per kernel since profiling was
+        switched on; clears the records."""
+        names = ctypes.create_string_buffer(8192)
+        ms = (ctypes.c_double * max_entries)()
+        cnt = (ctypes.c_uint64 * max_entries)()
+        n = _lib.lsmps_ctx_profile_report(self.h, names, len(names), ms, cnt, max_entries)
+        if n < 0:
+            raise LsmpsError(abi.CUDA_ERROR, "profile report failed")
+        keys = names.value.decode().split("\n")[:n]
+        return [(keys[i], float(ms[i]), int(cnt[i])) for i in range(n)]
+
     @property
     def required(self) -> int:
         return int(_lib.lsmps_ctx_required(self.h))

@@ -8,6 +8,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <string>
+#include <vector>
 
 #include "lsmps_b200.h"
 
@@ -100,6 +101,15 @@ struct lsmps_ctx {
   unsigned long long launches = 0;
   unsigned long long required = 0;
   std::string last_error;
+  // Per-launch CUDA events while profiling is on (lsmps_ctx_set_profiling).
+  struct ProfileRecord {
+    const char* name;
+    cudaEvent_t start;
+    cudaEvent_t stop;
+  };
+  bool profiling = false;
+  std::vector<ProfileRecord> profile;
+  size_t profile_used = 0;
 };
 
 namespace lsmps {
@@ -132,12 +142,21 @@ lsmps_status begin_call(lsmps_ctx* ctx);
 lsmps_status end_call(lsmps_ctx* ctx, lsmps_status st);
 lsmps_status fold_status(lsmps_ctx* ctx);
 
+// Event pair for the next profiled launch (grown on demand, reused across steps).
+lsmps_ctx::ProfileRecord* profile_slot(lsmps_ctx* ctx, const char* name);
+
 template <typename Kernel, typename... Args>
-inline void launch(lsmps_ctx* ctx, Kernel kernel, dim3 grid, dim3 block, size_t smem, Args... args) {
+inline void launch_named(lsmps_ctx* ctx, const char* name, Kernel kernel, dim3 grid, dim3 block, size_t smem,
+                         Args... args) {
   if (grid.x == 0 || grid.y == 0 || grid.z == 0) return;
+  lsmps_ctx::ProfileRecord* rec = ctx->profiling ? profile_slot(ctx, name) : nullptr;
+  if (rec) cudaEventRecord(rec->start, ctx->stream);
   kernel<<<grid, block, smem, ctx->stream>>>(args...);
+  if (rec) cudaEventRecord(rec->stop, ctx->stream);
   ++ctx->launches;
 }
+
+#define launch(ctx, kernel, ...) launch_named(ctx, #kernel, kernel, __VA_ARGS__)
 
 // Scan helpers (scan.cu).  Exclusive scan of n int32 values into out (may
 // alias in); values and partial sums are accumulated in 64 bits and any

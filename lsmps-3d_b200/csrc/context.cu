@@ -73,6 +73,20 @@ lsmps_status fold_status(lsmps_ctx* ctx) {
   return LSMPS_OK;
 }
 
+lsmps_ctx::ProfileRecord* profile_slot(lsmps_ctx* ctx, const char* name) {
+  if (ctx->profile_used == ctx->profile.size()) {
+    lsmps_ctx::ProfileRecord r{name, nullptr, nullptr};
+    if (cudaEventCreate(&r.start) != cudaSuccess || cudaEventCreate(&r.stop) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    ctx->profile.push_back(r);
+  }
+  lsmps_ctx::ProfileRecord* r = &ctx->profile[ctx->profile_used++];
+  r->name = name;
+  return r;
+}
+
 lsmps_status end_call(lsmps_ctx* ctx, lsmps_status st) {
   if (st != LSMPS_OK) return st;
   const lsmps_status ls = check_launch(ctx, "kernel launch");
@@ -116,6 +130,10 @@ lsmps_status lsmps_ctx_create(int device, lsmps_ctx** out) {
 void lsmps_ctx_destroy(lsmps_ctx* ctx) {
   if (!ctx) return;
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (auto& r : ctx->profile) {
+    cudaEventDestroy(r.start);
+    cudaEventDestroy(r.stop);
+  }
   if (ctx->scratch) cudaFree(ctx->scratch);
   if (ctx->d_status) cudaFree(ctx->d_status);
   if (ctx->h_status) cudaFreeHost(ctx->h_status);
@@ -165,6 +183,57 @@ lsmps_status lsmps_ctx_synchronize(lsmps_ctx* ctx) {
 }
 
 uint64_t lsmps_ctx_required(lsmps_ctx* ctx) { return ctx ? ctx->required : 0; }
+
+lsmps_status lsmps_ctx_set_profiling(lsmps_ctx* ctx, int on) {
+  if (!ctx) return LSMPS_INVALID_ARGUMENT;
+  ctx->profiling = on != 0;
+  ctx->profile_used = 0;
+  return LSMPS_OK;
+}
+
+int lsmps_ctx_profile_report(lsmps_ctx* ctx, char* names, size_t names_len, double* total_ms, uint64_t* launches,
+                             int max_entries) {
+  if (!ctx || max_entries < 0) return -1;
+  if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+    cudaGetLastError();
+    return -1;
+  }
+  std::vector<std::string> keys;
+  std::vector<double> ms;
+  std::vector<uint64_t> cnt;
+  for (size_t k = 0; k < ctx->profile_used; ++k) {
+    const auto& r = ctx->profile[k];
+    float t = 0.0f;
+    if (cudaEventElapsedTime(&t, r.start, r.stop) != cudaSuccess) {
+      cudaGetLastError();
+      continue;
+    }
+    size_t e = 0;
+    while (e < keys.size() && keys[e] != r.name) ++e;
+    if (e == keys.size()) {
+      keys.emplace_back(r.name);
+      ms.push_back(0.0);
+      cnt.push_back(0);
+    }
+    ms[e] += t;
+    ++cnt[e];
+  }
+  ctx->profile_used = 0;
+  const int n = static_cast<int>(keys.size() < static_cast<size_t>(max_entries) ? keys.size() : max_entries);
+  std::string joined;
+  for (int e = 0; e < n; ++e) {
+    if (total_ms) total_ms[e] = ms[e];
+    if (launches) launches[e] = cnt[e];
+    joined += keys[e];
+    joined += '\n';
+  }
+  if (names && names_len) {
+    const size_t m = joined.size() < names_len - 1 ? joined.size() : names_len - 1;
+    std::memcpy(names, joined.data(), m);
+    names[m] = '\0';
+  }
+  return n;
+}
 
 uint64_t lsmps_ctx_launch_count(lsmps_ctx* ctx) { return ctx ? ctx->launches : 0; }
 

@@ -121,14 +121,16 @@ __global__ void __launch_bounds__(kThreads) shifting_kernel(GatherArgs a, double
     const double dx = xi - fx[j], dy = yi - fy[j], dz = zi - fz[j];
     const double d = sqrt(dx * dx + dy * dy + dz * dz);
     if (d <= 0.0 || d >= dmin) continue;
-    const double inv_d = 1.0 / d;
-    const double push = scale * (dmin - d) * inv_d;
-    shx = fma(push, dx, shx);
-    shy = fma(push, dy, shy);
-    shz = fma(push, dz, shz);
-    nx = fma(dx, inv_d, nx);
-    ny = fma(dy, inv_d, ny);
-    nz = fma(dz, inv_d, nz);
+    // The reference's exact expressions (pressure_correction.cu:318-324): for
+    // stacked particles the summed unit vectors nearly cancel, so the
+    // projection below amplifies any change of operation order.
+    const double push = scale * (dmin - d) / d;
+    shx += push * dx;
+    shy += push * dy;
+    shz += push * dz;
+    nx += dx / d;
+    ny += dy / d;
+    nz += dz / d;
   }
   const index_t we = a.wo[i + 1];
   for (index_t o = a.wo[i]; o < we; ++o) {

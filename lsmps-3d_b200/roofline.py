@@ -1,0 +1,67 @@
+"""Algorithmic (compulsory) bytes of one LSMPS step and of each kernel.
+
+Every array a stage must read or write is counted once per stage, from the
+run's actual N_f (fluid), N_w (wall), K_f / K_w (CSR entries) and C (cells);
+S is the size of the floating type (8 for FP64 storage).  Neighbour gathers
+(positions of j) are counted once per array, i.e. perfect cache reuse: the
+model is the floor a kernel can reach, and achieved/peak compares a kernel
+with that floor.
+"""
+
+from __future__ import annotations
+
+
+def step_terms(nf: int, nw: int, kf: int, kw: int, c: int, s: int = 8) -> dict[str, int]:
+    """Per-stage compulsory bytes of one benchmark step (provision -> PPE ->
+    correction -> neighbour rebuild -> surface labels, moments built once)."""
+    k = kf + kw
+    pos = 3 * s * (nf + nw)
+    t = {}
+    # cell lists: positions, (id, index) write, one sort read+write of keys and
+    # values, cell begin/end
+    t["cells"] = sum(3 * s * n + 8 * n + 16 * n + 8 * c for n in (nf, nw))
+    # CSR count + write: positions, cell data, offsets, rows
+    t["csr"] = pos + 4 * (nf + nw) + 16 * c + 8 * (nf + 1) + 4 * k
+    t["surface"] = 8 * nf + 4 * k + pos + 3 * s * nw + 4 * nf + (4 * nf + 4 * nf + 4 * kf + 3 * s * nf)
+    moment_kind = 8 * nf + 4 * k + pos + 3 * s * nw + 81 * s * nf + 2 * s * nf
+    t["moment"] = 2 * moment_kind
+    t["provision"] = 8 * nf + 4 * k + pos + pos + 81 * s * nf + 6 * s * nf + 3 * s * nw
+    t["ppe"] = (4 * (nf + 1) + 8 * nf + 4 * k + pos + pos + 4 * nf + 2 * 81 * s * nf + 3 * s * nw
+                + (4 + s) * (nf + kf) + 3 * s * nf)
+    t["gradient"] = 8 * nf + 4 * k + pos + s * nf + 3 * s * nw + 81 * s * nf + 3 * s * nf
+    t["shifting"] = 8 * nf + 4 * k + pos + 3 * s * nw + 4 * nf + 3 * s * nf
+    t["update"] = nf * (2 * 3 * s + 2 * 3 * s + 3 * 3 * s + 4)
+    t["anti_penetration"] = 8 * nf + 4 * kw + 6 * s * nw + 2 * 6 * s * nf
+    t["smoothing"] = 8 * nf + 4 * kf + 3 * s * nf + 3 * s * nf + 4 * nf + 3 * s * nf + 6 * s * nf
+    return t
+
+
+def step_bytes(nf: int, nw: int, kf: int, kw: int, c: int, s: int = 8) -> int:
+    return sum(step_terms(nf, nw, kf, kw, c, s).values())
+
+
+def kernel_bytes(nf: int, nw: int, kf: int, kw: int, c: int, s: int = 8) -> dict[str, int]:
+    """Algorithmic bytes per launch of the library's kernels (names as the
+    profiler reports them).  CSR kernels run once per table, so their table
+    sizes are summed over both launches and reported per launch on average."""
+    k = kf + kw
+    pos_f = 3 * s * nf
+    pos_w = 3 * s * nw
+    out = {}
+    # moment_kernel<9> builds velocity-A and pressure-A in one pass over the rows
+    out["moment_kernel<9>"] = (16 * nf + 4 * k + pos_f + pos_w + pos_w + 2 * (81 * s * nf + 2 * s * nf + 4 * nf))
+    out["laplacian_kernel"] = 16 * nf + 4 * k + 2 * (pos_f + pos_w) + 81 * s * nf + 3 * s * nf
+    out["ppe_kernel"] = (16 * nf + 4 * k + 2 * (pos_f + pos_w) + pos_w + 2 * 81 * s * nf + 4 * nf
+                         + (4 + s) * (nf + kf) + 3 * s * nf + 4 * (nf + 1))
+    out["gradient_kernel"] = 16 * nf + 4 * k + pos_f + pos_w + pos_w + s * nf + 81 * s * nf + 3 * s * nf + 4 * nf
+    out["shifting_kernel"] = 16 * nf + 4 * k + pos_f + pos_w + pos_w + 4 * nf + 3 * s * nf
+    out["smooth_kernel"] = 8 * nf + 4 * kf + pos_f + 3 * s * nf + 4 * nf + 3 * s * nf
+    out["classify_kernel"] = 16 * nf + 4 * k + pos_f + pos_w + pos_w + 4 * nf
+    out["expand_kernel"] = 8 * nf + 4 * kf + pos_f + 4 * nf
+    # count + write, averaged over the fluid and wall tables
+    out["csr_kernel<false>"] = (2 * pos_f + pos_w + 2 * 8 * c + 2 * 4 * nf + 4 * (nf + nw) + 2 * 4 * nf) // 2
+    out["csr_kernel<true>"] = (2 * pos_f + pos_w + 2 * 8 * c + 2 * 4 * nf + 4 * (nf + nw) + 2 * 4 * nf + 4 * k) // 2
+    out["update_kernel"] = nf * (2 * 3 * s + 2 * 3 * s + 3 * 3 * s + 4)
+    out["anti_penetration_kernel"] = 8 * nf + 4 * kw + 6 * s * nw + 2 * 6 * s * nf
+    out["copy_kernel"] = 6 * s * nf
+    return out

@@ -50,3 +50,28 @@ def buffers_from(pkg, alloc, kat):
 
 def rows(off, idx, n):
     return [sorted(int(v) for v in idx[off[i]:off[i + 1]]) for i in range(n)]
+
+
+def rel_err(g, o, floor_frac=1e-3, scale=None):
+    """max(normwise, elementwise) relative error of g against o.
+    normwise = max|g-o| / scale, scale = max|o| unless given (pass the
+    magnitude of the whole vector field for one of its components);
+    elementwise = max |g-o|/|o| over entries with |o| >= floor_frac * scale
+    (entries that cancel to near zero are covered by the normwise term)."""
+    g = np.asarray(g, dtype=np.float64)
+    o = np.asarray(o, dtype=np.float64)
+    if o.size == 0:
+        return 0.0
+    s = float(np.max(np.abs(o))) if scale is None else float(scale)
+    if s == 0.0:
+        return float(np.max(np.abs(g)))
+    d = np.abs(g - o)
+    big = np.abs(o) >= floor_frac * s
+    elem = float(np.max(d[big] / np.abs(o[big]))) if big.any() else 0.0
+    return max(float(np.max(d)) / s, elem)
+
+
+def vec_err(g: dict, o: dict, comps):
+    """rel_err of each component against the scale of the whole vector."""
+    scale = max(float(np.max(np.abs(np.asarray(o[c])))) if np.asarray(o[c]).size else 0.0 for c in comps)
+    return {c: rel_err(g[c], o[c], scale=scale if scale > 0 else None) for c in comps}
