@@ -71,7 +71,11 @@ def rel_err(g, o, floor_frac=1e-3, scale=None):
     return max(float(np.max(d)) / s, elem)
 
 
-def vec_err(g: dict, o: dict, comps):
-    """rel_err of each component against the scale of the whole vector."""
-    scale = max(float(np.max(np.abs(np.asarray(o[c])))) if np.asarray(o[c]).size else 0.0 for c in comps)
+def vec_err(g: dict, o: dict, comps, extra_scale: dict | None = None):
+    """rel_err of each component against the scale of the whole vector (and
+    of `extra_scale`'s same-named arrays, e.g. the operands of a cancellation)."""
+    arrays = [np.asarray(o[c]) for c in comps]
+    if extra_scale is not None:
+        arrays += [np.asarray(extra_scale[c]) for c in comps if c in extra_scale]
+    scale = max(float(np.max(np.abs(a))) if a.size else 0.0 for a in arrays)
     return {c: rel_err(g[c], o[c], scale=scale if scale > 0 else None) for c in comps}
