@@ -51,6 +51,21 @@ __device__ __forceinline__ double correction_weight(double distance, double supp
   return (distance >= support_radius || distance <= 0.0) ? 0.0 : 1.0 - distance / support_radius;
 }
 
+// The same weights with the division by r_e replaced by a multiplication with
+// 1/r_e (one rounding instead of an IEEE division sequence on the FP64 pipe).
+// The value differs from the reference's by at most one ulp of d/r_e; a
+// distance within that ulp of r_e may get weight 0 instead of ~1e-16.  Used by
+// the operator kernels, whose outputs are compared within a tolerance; the
+// label kernel keeps the reference's exact expressions.
+__device__ __forceinline__ double lin_weight_mul(double distance, double inv_re) {
+  const double w = 1.0 - distance * inv_re;
+  return w > 0.0 ? w : 0.0;
+}
+
+__device__ __forceinline__ double correction_weight_mul(double distance, double inv_re) {
+  return distance <= 0.0 ? 0.0 : lin_weight_mul(distance, inv_re);
+}
+
 // Type-A quadratic basis of the r_e-scaled offset with the multiply-by-inverse
 // form of explicit_update.cu:128-146 (ppe_matrix.cu:155-173 and
 // pressure_correction.cu:138-156 are the same).
@@ -110,6 +125,11 @@ struct lsmps_ctx {
   bool profiling = false;
   std::vector<ProfileRecord> profile;
   size_t profile_used = 0;
+  // 32-byte neighbour records (packed.cuh): two fluid and three wall arrays.
+  double4* pack_fluid[2] = {nullptr, nullptr};
+  double4* pack_wall[3] = {nullptr, nullptr, nullptr};
+  size_t pack_fluid_cap = 0;
+  size_t pack_wall_cap = 0;
 };
 
 namespace lsmps {
@@ -133,6 +153,10 @@ class Scratch {
  private:
   lsmps_ctx* ctx_;
 };
+
+// Grow the pack arrays to hold nf fluid and nw wall records (outside stream
+// capture; returns false if that is impossible).
+bool ensure_packs(lsmps_ctx* ctx, size_t nf, size_t nw);
 
 lsmps_status fail(lsmps_ctx* ctx, lsmps_status st, const char* what);
 lsmps_status check_launch(lsmps_ctx* ctx, const char* what);

@@ -26,6 +26,41 @@ bool Scratch::reserve(size_t bytes) {
   return true;
 }
 
+bool ensure_packs(lsmps_ctx* ctx, size_t nf, size_t nw) {
+  if (nf <= ctx->pack_fluid_cap && nw <= ctx->pack_wall_cap) return true;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  cudaStreamIsCapturing(ctx->stream, &cap);
+  if (cap != cudaStreamCaptureStatusNone) return false;
+  cudaStreamSynchronize(ctx->stream);
+  if (nf > ctx->pack_fluid_cap) {
+    for (auto& p : ctx->pack_fluid) {
+      if (p) cudaFree(p);
+      p = nullptr;
+    }
+    ctx->pack_fluid_cap = 0;
+    for (auto& p : ctx->pack_fluid)
+      if (cudaMalloc(&p, nf * sizeof(double4)) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+      }
+    ctx->pack_fluid_cap = nf;
+  }
+  if (nw > ctx->pack_wall_cap) {
+    for (auto& p : ctx->pack_wall) {
+      if (p) cudaFree(p);
+      p = nullptr;
+    }
+    ctx->pack_wall_cap = 0;
+    for (auto& p : ctx->pack_wall)
+      if (cudaMalloc(&p, nw * sizeof(double4)) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+      }
+    ctx->pack_wall_cap = nw;
+  }
+  return true;
+}
+
 lsmps_status fail(lsmps_ctx* ctx, lsmps_status st, const char* what) {
   if (ctx) ctx->last_error = what;
   return st;
@@ -135,6 +170,10 @@ void lsmps_ctx_destroy(lsmps_ctx* ctx) {
     cudaEventDestroy(r.stop);
   }
   if (ctx->scratch) cudaFree(ctx->scratch);
+  for (auto p : ctx->pack_fluid)
+    if (p) cudaFree(p);
+  for (auto p : ctx->pack_wall)
+    if (p) cudaFree(p);
   if (ctx->d_status) cudaFree(ctx->d_status);
   if (ctx->h_status) cudaFreeHost(ctx->h_status);
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
@@ -172,6 +211,7 @@ lsmps_status lsmps_ctx_reserve(lsmps_ctx* ctx, size_t fluid_capacity, size_t wal
   if (s2 > need) need = s2;
   Scratch s(ctx);
   if (!s.reserve(need)) return fail(ctx, LSMPS_CUDA_ERROR, "scratch allocation failed");
+  if (!ensure_packs(ctx, fluid_capacity, wall_capacity)) return fail(ctx, LSMPS_CUDA_ERROR, "pack allocation failed");
   return LSMPS_OK;
 }
 

@@ -4,6 +4,7 @@
 // LSMPS pressure gradient, particle shifting, velocity/position update,
 // wall anti-penetration and velocity smoothing.
 #include "impl.cuh"
+#include "packed.cuh"
 
 namespace lsmps {
 namespace {
@@ -64,7 +65,7 @@ __global__ void __launch_bounds__(kThreads) gradient_kernel(GatherArgs a, const 
   for (index_t o = a.fo[i]; o < fe; ++o) {
     const index_t j = a.fi[o];
     const double dx = fx[j] - xi, dy = fy[j] - yi, dz = fz[j] - zi;
-    const double w = correction_weight(sqrt(dx * dx + dy * dy + dz * dz), re);
+    const double w = correction_weight_mul(sqrt(dx * dx + dy * dy + dz * dz), inv_re);
     if (w <= 0.0) continue;
     basis_a_mul(dx, dy, dz, inv_re, b);
     const double dp = pressure[j] - pi;
@@ -75,7 +76,7 @@ __global__ void __launch_bounds__(kThreads) gradient_kernel(GatherArgs a, const 
   for (index_t o = a.wo[i]; o < we; ++o) {
     const index_t j = a.wi[o];
     const double dx = a.walls.x[j] - xi, dy = a.walls.y[j] - yi, dz = a.walls.z[j] - zi;
-    const double w = wall_scale * correction_weight(sqrt(dx * dx + dy * dy + dz * dz), re);
+    const double w = wall_scale * correction_weight_mul(sqrt(dx * dx + dy * dy + dz * dz), inv_re);
     if (w <= 0.0) continue;
     const double nx = a.walls.normal_x[j], ny = a.walls.normal_y[j], nz = a.walls.normal_z[j];
     double q[9];
@@ -234,48 +235,50 @@ __global__ void __launch_bounds__(kThreads) anti_penetration_kernel(lsmps_fluid 
   }
 }
 
-// smooth_velocity_kernel, pressure_correction.cu:446-504
-__global__ void __launch_bounds__(kThreads) smooth_kernel(lsmps_fluid f, const index_t* __restrict__ fo,
+// smooth_velocity_kernel, pressure_correction.cu:446-504, on neighbour records
+// fp = {x, y, z, 0} and fv = {vx, vy, vz, label} (packed.cuh).
+__global__ void __launch_bounds__(kThreads) smooth_kernel(index_t n, const double4* __restrict__ fp,
+                                                          const double4* __restrict__ fv,
+                                                          const index_t* __restrict__ fo,
                                                           const index_t* __restrict__ fi, double re, double strength,
                                                           double* ox, double* oy, double* oz) {
   const index_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= static_cast<index_t>(f.count)) return;
-  const double* __restrict__ vx = f.vx;
-  const double* __restrict__ vy = f.vy;
-  const double* __restrict__ vz = f.vz;
-  if (strength <= 0.0 || is_splash(f.surface_type, i)) {
-    ox[i] = vx[i];
-    oy[i] = vy[i];
-    oz[i] = vz[i];
+  if (i >= n) return;
+  const double inv_re = 1.0 / re;
+  constexpr double kSplash = static_cast<double>(LSMPS_SURFACE_SPLASH);
+  const double4 ui = ld4(fv, i);
+  if (strength <= 0.0 || ui.w == kSplash) {
+    ox[i] = ui.x;
+    oy[i] = ui.y;
+    oz[i] = ui.z;
     return;
   }
-  const double* __restrict__ fx = f.x;
-  const double* __restrict__ fy = f.y;
-  const double* __restrict__ fz = f.z;
-  const double xi = fx[i], yi = fy[i], zi = fz[i];
+  const double4 pi = ld4(fp, i);
   double ws = 0.0, ax = 0.0, ay = 0.0, az = 0.0;
   const index_t fe = fo[i + 1];
   for (index_t o = fo[i]; o < fe; ++o) {
     const index_t j = fi[o];
-    if (is_splash(f.surface_type, j)) continue;
-    const double dx = fx[j] - xi, dy = fy[j] - yi, dz = fz[j] - zi;
-    const double w = correction_weight(sqrt(dx * dx + dy * dy + dz * dz), re);
+    const double4 u = ld4(fv, j);
+    if (u.w == kSplash) continue;
+    const double4 q = ld4(fp, j);
+    const double dx = q.x - pi.x, dy = q.y - pi.y, dz = q.z - pi.z;
+    const double w = correction_weight_mul(sqrt(dx * dx + dy * dy + dz * dz), inv_re);
     if (w <= 0.0) continue;
     ws += w;
-    ax = fma(w, vx[j], ax);
-    ay = fma(w, vy[j], ay);
-    az = fma(w, vz[j], az);
+    ax = fma(w, u.x, ax);
+    ay = fma(w, u.y, ay);
+    az = fma(w, u.z, az);
   }
   if (ws <= 0.0) {
-    ox[i] = vx[i];
-    oy[i] = vy[i];
-    oz[i] = vz[i];
+    ox[i] = ui.x;
+    oy[i] = ui.y;
+    oz[i] = ui.z;
     return;
   }
   const double alpha = strength < 0.0 ? 0.0 : (strength > 1.0 ? 1.0 : strength);
-  ox[i] = (1.0 - alpha) * vx[i] + alpha * ax / ws;
-  oy[i] = (1.0 - alpha) * vy[i] + alpha * ay / ws;
-  oz[i] = (1.0 - alpha) * vz[i] + alpha * az / ws;
+  ox[i] = (1.0 - alpha) * ui.x + alpha * ax / ws;
+  oy[i] = (1.0 - alpha) * ui.y + alpha * ay / ws;
+  oz[i] = (1.0 - alpha) * ui.z + alpha * az / ws;
 }
 
 // copy_smoothed_velocity_kernel, pressure_correction.cu:506-515
@@ -377,24 +380,233 @@ lsmps_status smooth_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const lsmps_csr& 
   if (st) return st;
   if ((st = check_vector(ctx, f, sm, "Velocity smoothing workspace is too small"))) return st;
   if (f.count == 0) return LSMPS_OK;
-  launch(ctx, smooth_kernel, dim3(div_up(static_cast<long long>(f.count), kThreads)), dim3(kThreads), 0, f,
-         static_cast<const index_t*>(fn.offsets), static_cast<const index_t*>(fn.indices), p.support_radius,
-         p.velocity_smoothing_strength, sm.x, sm.y, sm.z);
+  if (!ensure_packs(ctx, f.count, 0)) return fail(ctx, LSMPS_CUDA_ERROR, "pack allocation failed");
+  pack4(ctx, f.x, f.y, f.z, nullptr, f.count, ctx->pack_fluid[0]);
+  pack4_label(ctx, f.vx, f.vy, f.vz, f.surface_type, f.count, ctx->pack_fluid[1]);
+  launch(ctx, smooth_kernel, dim3(div_up(static_cast<long long>(f.count), kThreads)), dim3(kThreads), 0,
+         static_cast<index_t>(f.count), static_cast<const double4*>(ctx->pack_fluid[0]),
+         static_cast<const double4*>(ctx->pack_fluid[1]), static_cast<const index_t*>(fn.offsets),
+         static_cast<const index_t*>(fn.indices), p.support_radius, p.velocity_smoothing_strength, sm.x, sm.y, sm.z);
   launch(ctx, copy_kernel, dim3(pointwise_blocks(ctx, f.count)), dim3(256), 0, static_cast<index_t>(f.count),
          static_cast<const double*>(sm.x), static_cast<const double*>(sm.y), static_cast<const double*>(sm.z), f.vx,
          f.vy, f.vz);
   return check_launch(ctx, "velocity smoothing");
 }
 
+namespace {
+
+// clamp_fluid_pressure_kernel + compute_pressure_gradient_kernel +
+// compute_particle_shifting_kernel in one pass over the rows.  All three read
+// the pre-update neighbourhood only.  The clamp is applied to every pressure
+// read (a neighbour's slot may or may not be clamped yet when it is read; both
+// give the same clamped value), and each thread writes its own clamped value.
+// The shifting offsets x_i - x_j are the exact negations of x_j - x_i, so the
+// outputs are bitwise those of the separate kernels.
+__global__ void __launch_bounds__(kThreads) gradient_shifting_kernel(GatherArgs a, double* pressure,
+                                                                     double* fluid_pressure,
+                                                                     const double* __restrict__ pinv, double re,
+                                                                     double wall_scale, double* gx, double* gy,
+                                                                     double* gz, double* sx_out, double* sy_out,
+                                                                     double* sz_out) {
+  const index_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= static_cast<index_t>(a.fluid.count)) return;
+  const double praw = pressure[i];
+  const double pi = praw < 0.0 ? 0.0 : praw;
+  pressure[i] = pi;
+  if (fluid_pressure != nullptr && fluid_pressure != pressure) fluid_pressure[i] = pi;
+  const bool splash = is_splash(a.fluid.surface_type, i);
+  const bool do_grad = !splash;
+  const bool do_shift = !(a.p.ps_displacement_scale <= 0.0 || splash);
+  if (!do_grad && !do_shift) {
+    gx[i] = gy[i] = gz[i] = 0.0;
+    sx_out[i] = sy_out[i] = sz_out[i] = 0.0;
+    return;
+  }
+  const double* __restrict__ fx = a.fluid.x;
+  const double* __restrict__ fy = a.fluid.y;
+  const double* __restrict__ fz = a.fluid.z;
+  const double xi = fx[i], yi = fy[i], zi = fz[i];
+  const double inv_re = 1.0 / re;
+  const double dmin = a.p.ps_min_distance_ratio * a.p.particle_spacing;
+  const double scale = a.p.ps_displacement_scale;
+  double rhs[9], b[9];
+#pragma unroll
+  for (int r = 0; r < 9; ++r) rhs[r] = 0.0;
+  double shx = 0.0, shy = 0.0, shz = 0.0, nx = 0.0, ny = 0.0, nz = 0.0;
+  const index_t fe = a.fo[i + 1];
+  for (index_t o = a.fo[i]; o < fe; ++o) {
+    const index_t j = a.fi[o];
+    const double dx = fx[j] - xi, dy = fy[j] - yi, dz = fz[j] - zi;
+    const double d = sqrt(dx * dx + dy * dy + dz * dz);
+    if (do_grad) {
+      const double w = correction_weight_mul(d, inv_re);
+      if (w > 0.0) {
+        basis_a_mul(dx, dy, dz, inv_re, b);
+        const double pj = pressure[j];
+        const double dp = (pj < 0.0 ? 0.0 : pj) - pi;
+#pragma unroll
+        for (int r = 0; r < 9; ++r) rhs[r] = fma(w * b[r], dp, rhs[r]);
+      }
+    }
+    if (do_shift && d > 0.0 && d < dmin) {
+      const double ex = -dx, ey = -dy, ez = -dz;
+      const double push = scale * (dmin - d) / d;
+      shx += push * ex;
+      shy += push * ey;
+      shz += push * ez;
+      nx += ex / d;
+      ny += ey / d;
+      nz += ez / d;
+    }
+  }
+  const index_t we = a.wo[i + 1];
+  for (index_t o = a.wo[i]; o < we; ++o) {
+    const index_t j = a.wi[o];
+    const double dx = a.walls.x[j] - xi, dy = a.walls.y[j] - yi, dz = a.walls.z[j] - zi;
+    const double d = sqrt(dx * dx + dy * dy + dz * dz);
+    const double wnx = a.walls.normal_x[j], wny = a.walls.normal_y[j], wnz = a.walls.normal_z[j];
+    if (do_grad) {
+      const double w = wall_scale * correction_weight_mul(d, inv_re);
+      if (w > 0.0) {
+        double q[9];
+        neumann_a(dx, dy, dz, wnx, wny, wnz, inv_re, q);
+        const double ng = a.p.gravity[0] * wnx + a.p.gravity[1] * wny + a.p.gravity[2] * wnz;
+        const double wr = re * a.p.density * ng;
+#pragma unroll
+        for (int r = 0; r < 9; ++r) rhs[r] = fma(w * q[r], wr, rhs[r]);
+      }
+    }
+    if (do_shift && d > 0.0 && d < dmin) {
+      const double push = scale * (dmin - d);
+      shx = fma(push, wnx, shx);
+      shy = fma(push, wny, shy);
+      shz = fma(push, wnz, shz);
+    }
+  }
+  if (do_grad) {
+    const double* __restrict__ inv = pinv + static_cast<size_t>(i) * 81;
+    double c0 = 0.0, c1 = 0.0, c2 = 0.0;
+#pragma unroll
+    for (int col = 0; col < 9; ++col) {
+      c0 = fma(inv[0 + col * 9], rhs[col], c0);
+      c1 = fma(inv[1 + col * 9], rhs[col], c1);
+      c2 = fma(inv[2 + col * 9], rhs[col], c2);
+    }
+    gx[i] = c0 * inv_re;
+    gy[i] = c1 * inv_re;
+    gz[i] = c2 * inv_re;
+  } else {
+    gx[i] = gy[i] = gz[i] = 0.0;
+  }
+  if (do_shift) {
+    if (is_surface(a.fluid.surface_type, i)) {
+      const double nn = sqrt(nx * nx + ny * ny + nz * nz);
+      if (nn > 0.0) {
+        nx /= nn;
+        ny /= nn;
+        nz /= nn;
+        const double nc = shx * nx + shy * ny + shz * nz;
+        shx -= nc * nx;
+        shy -= nc * ny;
+        shz -= nc * nz;
+      }
+    }
+    const double smax = a.p.ps_max_displacement_ratio * a.p.particle_spacing;
+    const double sn = sqrt(shx * shx + shy * shy + shz * shz);
+    if (sn > smax && sn > 0.0) {
+      const double sc = smax / sn;
+      shx *= sc;
+      shy *= sc;
+      shz *= sc;
+    }
+    sx_out[i] = shx;
+    sy_out[i] = shy;
+    sz_out[i] = shz;
+  } else {
+    sx_out[i] = sy_out[i] = sz_out[i] = 0.0;
+  }
+}
+
+// update_velocity_position_kernel followed by anti_penetration_kernel for the
+// same particle: the anti-penetration pass reads only the particle's own
+// updated state and the walls, so running it right after the update in the
+// same thread gives the same result as the two reference kernels.
+__global__ void __launch_bounds__(kThreads) update_anti_penetration_kernel(
+    lsmps_fluid f, lsmps_walls w, const index_t* __restrict__ wo, const index_t* __restrict__ wi,
+    const double* __restrict__ tx, const double* __restrict__ ty, const double* __restrict__ tz, double dt,
+    double density, const double* __restrict__ gx, const double* __restrict__ gy, const double* __restrict__ gz,
+    const double* __restrict__ sx, const double* __restrict__ sy, const double* __restrict__ sz, double clearance) {
+  const index_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= static_cast<index_t>(f.count)) return;
+  const bool splash = is_splash(f.surface_type, i);
+  const double ox = f.vx[i], oy = f.vy[i], oz = f.vz[i];
+  double vx = tx[i], vy = ty[i], vz = tz[i];
+  if (!splash) {
+    const double ps = dt / density;
+    vx -= ps * gx[i];
+    vy -= ps * gy[i];
+    vz -= ps * gz[i];
+  }
+  double x = f.x[i], y = f.y[i], z = f.z[i];
+  x += 0.5 * dt * (ox + vx) + sx[i];
+  y += 0.5 * dt * (oy + vy) + sy[i];
+  z += 0.5 * dt * (oz + vz) + sz[i];
+  if (clearance > 0.0) {
+    const index_t we = wo[i + 1];
+    for (index_t o = wo[i]; o < we; ++o) {
+      const index_t j = wi[o];
+      const double nx = w.normal_x[j], ny = w.normal_y[j], nz = w.normal_z[j];
+      const double sd = (x - w.x[j]) * nx + (y - w.y[j]) * ny + (z - w.z[j]) * nz;
+      if (sd >= clearance) continue;
+      const double c = clearance - sd;
+      x += c * nx;
+      y += c * ny;
+      z += c * nz;
+      const double nv = vx * nx + vy * ny + vz * nz;
+      if (nv < 0.0) {
+        vx -= nv * nx;
+        vy -= nv * ny;
+        vz -= nv * nz;
+      }
+    }
+  }
+  f.x[i] = x;
+  f.y[i] = y;
+  f.z[i] = z;
+  f.vx[i] = vx;
+  f.vy[i] = vy;
+  f.vz[i] = vz;
+}
+
+}  // namespace
+
 lsmps_status pressure_correction_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const lsmps_walls& w,
                                       const lsmps_csr& fn, const lsmps_csr& wn, const lsmps_fluid& t,
                                       double* pressure, const lsmps_params& p, const lsmps_moment& pm,
                                       const lsmps_vector& g, const lsmps_vector& s, const lsmps_vector& sm) {
-  lsmps_status st = clamp_pressure_impl(ctx, f, pressure);
-  if (!st) st = pressure_gradient_impl(ctx, f, w, fn, wn, pressure, p, pm, g);
-  if (!st) st = particle_shifting_impl(ctx, f, w, fn, wn, p, s);
-  if (!st) st = update_impl(ctx, f, t, p, g, s);
-  if (!st) st = anti_penetration_impl(ctx, f, w, wn, p);
+  lsmps_status st = check_fluid(ctx, f);
+  if (st) return st;
+  if (f.count > 0 && !pressure) return fail(ctx, LSMPS_INVALID_ARGUMENT, "Pressure correction requires a pressure array");
+  if ((st = check_vector(ctx, f, g, "Pressure gradient workspace is too small"))) return st;
+  if ((st = check_vector(ctx, f, s, "PS displacement workspace is too small"))) return st;
+  if (t.count < f.count || (f.count && (!t.vx || !t.vy || !t.vz)))
+    return fail(ctx, LSMPS_INVALID_ARGUMENT, "Pressure correction temporary velocity target is too small");
+  if (pm.kind != LSMPS_MOMENT_PRESSURE_WALL_NEUMANN_A || pm.matrix_size != 9 || pm.particle_count < f.count)
+    return fail(ctx, LSMPS_NOT_PREPARED, "Pressure correction requires a prepared pressure Type-A moment matrix");
+  if (f.count == 0) return LSMPS_OK;
+  if (!pm.inverse_matrices) return fail(ctx, LSMPS_INVALID_ARGUMENT, "pressure inverse buffer missing");
+  GatherArgs a{f, w, fn.offsets, fn.indices, wn.offsets, wn.indices, p};
+  const int blocks = div_up(static_cast<long long>(f.count), kThreads);
+  launch(ctx, gradient_shifting_kernel, dim3(blocks), dim3(kThreads), 0, a, pressure, f.pressure,
+         static_cast<const double*>(pm.inverse_matrices), pm.support_radius, pm.wall_weight_scale, g.x, g.y, g.z,
+         s.x, s.y, s.z);
+  launch(ctx, update_anti_penetration_kernel, dim3(blocks), dim3(kThreads), 0, f, w,
+         static_cast<const index_t*>(wn.offsets), static_cast<const index_t*>(wn.indices),
+         static_cast<const double*>(t.vx), static_cast<const double*>(t.vy), static_cast<const double*>(t.vz),
+         p.time_step, p.density, static_cast<const double*>(g.x), static_cast<const double*>(g.y),
+         static_cast<const double*>(g.z), static_cast<const double*>(s.x), static_cast<const double*>(s.y),
+         static_cast<const double*>(s.z), p.wall_clearance_ratio * p.particle_spacing);
+  st = check_launch(ctx, "gradient/shifting, update/anti-penetration");
   if (!st) st = smooth_impl(ctx, f, fn, p, sm);
   return st;
 }

@@ -15,6 +15,7 @@
 // triangular factor, and X = L^-T L^-1, then stored column-major and
 // symmetric like the reference's inverse_matrices.
 #include <cmath>
+#include <utility>
 
 #include "impl.cuh"
 
@@ -46,8 +47,8 @@ struct MomentArgs {
   double inv_re;
   double lambda;
   double wall_scale;
-  int nkinds;
-  KindOut kinds[kMaxKinds];
+  KindOut k0;  // first kind (boundary given by the kernel's B0)
+  KindOut k1;  // second kind when the kernel's B1 >= 0
   DeviceStatus* status;
 };
 
@@ -96,28 +97,39 @@ __device__ __forceinline__ void add_outer(double (&m)[N * (N + 1) / 2], const do
   }
 }
 
+// Column J of the lower Cholesky factor, in place.  J is a template argument
+// so that every index into the register array is a compile-time constant
+// even though sqrt() keeps the compiler from unrolling a loop over columns.
+template <int N, int J>
+__device__ __forceinline__ void cholesky_column(double (&a)[N * (N + 1) / 2], int& info) {
+  double s = a[tri(J, J)];
+#pragma unroll
+  for (int k = 0; k < J; ++k) s = fma(-a[tri(J, k)], a[tri(J, k)], s);
+  if (!(s > 0.0) && info == 0) info = J + 1;
+  const double ljj = sqrt(s);
+  a[tri(J, J)] = ljj;
+  const double inv = 1.0 / ljj;
+#pragma unroll
+  for (int i = J + 1; i < N; ++i) {
+    double t = a[tri(i, J)];
+#pragma unroll
+    for (int k = 0; k < J; ++k) t = fma(-a[tri(i, k)], a[tri(J, k)], t);
+    a[tri(i, J)] = t * inv;
+  }
+}
+
+template <int N, int... J>
+__device__ __forceinline__ void cholesky_columns(double (&a)[N * (N + 1) / 2], int& info,
+                                                 std::integer_sequence<int, J...>) {
+  (cholesky_column<N, J>(a, info), ...);
+}
+
 // Lower Cholesky in place; returns 0 or the 1-based order of the first
 // non-positive pivot (the potrf info convention).
 template <int N>
 __device__ __forceinline__ int cholesky(double (&a)[N * (N + 1) / 2]) {
   int info = 0;
-#pragma unroll
-  for (int j = 0; j < N; ++j) {
-    double s = a[tri(j, j)];
-#pragma unroll
-    for (int k = 0; k < j; ++k) s = fma(-a[tri(j, k)], a[tri(j, k)], s);
-    if (!(s > 0.0) && info == 0) info = j + 1;
-    const double ljj = sqrt(s);
-    a[tri(j, j)] = ljj;
-    const double inv = 1.0 / ljj;
-#pragma unroll
-    for (int i = j + 1; i < N; ++i) {
-      double t = a[tri(i, j)];
-#pragma unroll
-      for (int k = 0; k < j; ++k) t = fma(-a[tri(i, k)], a[tri(j, k)], t);
-      a[tri(i, j)] = t * inv;
-    }
-  }
+  cholesky_columns<N>(a, info, std::make_integer_sequence<int, N>{});
   return info;
 }
 
@@ -155,14 +167,60 @@ __device__ __forceinline__ void store_inverse(const double (&t)[N * (N + 1) / 2]
   }
 }
 
-template <int N>
+// Adds the wall term of boundary kind B (0 none, 1 Dirichlet sample,
+// 2 pressure Neumann) to m, regularises, inverts and stores one kind.
+template <int N, int B>
+__device__ __forceinline__ void finish_kind(double (&m)[N * (N + 1) / 2], const MomentArgs& a, const KindOut& ko,
+                                            index_t i, double xi, double yi, double zi) {
+  double b[N];
+  if (B != 0) {
+    const index_t we = a.wo[i + 1];
+    for (index_t o = a.wo[i]; o < we; ++o) {
+      const index_t j = a.wi[o];
+      const double dx = a.walls.x[j] - xi, dy = a.walls.y[j] - yi, dz = a.walls.z[j] - zi;
+      const double d2 = dx * dx + dy * dy + dz * dz;
+      if (d2 <= 0.0) continue;
+      const double w = a.wall_scale * (1.0 - sqrt(d2) * a.inv_re);
+      if (w <= 0.0) continue;
+      if (B == 2) {
+        neumann<N>(dx, dy, dz, a.walls.normal_x[j], a.walls.normal_y[j], a.walls.normal_z[j], a.inv_re, b);
+      } else {
+        basis<N>(dx, dy, dz, a.inv_re, b);
+      }
+      add_outer<N>(m, b, w);
+    }
+  }
+  // trace and regularisation, moment_matrix.cu:297-308
+  double trace = 0.0;
+#pragma unroll
+  for (int r = 0; r < N; ++r) trace += m[tri(r, r)];
+  const double reg = a.lambda * (trace > 0.0 ? trace / static_cast<double>(N) : 1.0);
+#pragma unroll
+  for (int r = 0; r < N; ++r) m[tri(r, r)] += reg;
+  const int info = cholesky<N>(m);
+  double* out = ko.inverse + static_cast<size_t>(i) * N * N;
+  if (info == 0) {
+    invert_lower<N>(m);
+    store_inverse<N>(m, out);
+  } else {
+    for (int e = 0; e < N * N; ++e) out[e] = __longlong_as_double(0x7ff8000000000000LL);
+    atomicAdd(&a.status->non_spd, 1u);
+    raise_flag(a.status, kFlagNonSpd);
+  }
+  ko.trace[i] = trace;
+  ko.reg[i] = reg;
+  ko.info[i] = info;
+}
+
+// One or two kinds (B1 < 0: one) from one pass over the fluid row.
+template <int N, int B0, int B1>
 __global__ void __launch_bounds__(kMomentThreads) moment_kernel(MomentArgs a) {
   constexpr int E = N * (N + 1) / 2;
-  extern __shared__ double s_fluid[];  // [E][kMomentThreads] when nkinds > 1
+  extern __shared__ double s_fluid[];  // [E][kMomentThreads] when two kinds share the fluid sum
   const index_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (blockIdx.x == 0 && threadIdx.x == 0) {
-    for (int k = 0; k < a.nkinds; ++k)
-      if (a.kinds[k].count) atomicAdd(a.kinds[k].count, 1);
+    if (a.k0.count) atomicAdd(a.k0.count, 1);
+    if (B1 >= 0 && a.k1.count) atomicAdd(a.k1.count, 1);
   }
   if (i >= static_cast<index_t>(a.fluid.count)) return;
   const double* __restrict__ fx = a.fluid.x;
@@ -184,53 +242,15 @@ __global__ void __launch_bounds__(kMomentThreads) moment_kernel(MomentArgs a) {
     basis<N>(dx, dy, dz, a.inv_re, b);
     add_outer<N>(m, b, w);
   }
-  if (a.nkinds > 1) {
+  if (B1 >= 0) {
 #pragma unroll
     for (int e = 0; e < E; ++e) s_fluid[e * kMomentThreads + threadIdx.x] = m[e];
   }
-  const index_t wb = a.wo[i], we = a.wo[i + 1];
-  for (int k = 0; k < a.nkinds; ++k) {
-    const KindOut ko = a.kinds[k];
-    if (k > 0) {
+  finish_kind<N, B0>(m, a, a.k0, i, xi, yi, zi);
+  if (B1 >= 0) {
 #pragma unroll
-      for (int e = 0; e < E; ++e) m[e] = s_fluid[e * kMomentThreads + threadIdx.x];
-    }
-    if (ko.boundary != 0) {
-      for (index_t o = wb; o < we; ++o) {
-        const index_t j = a.wi[o];
-        const double dx = a.walls.x[j] - xi, dy = a.walls.y[j] - yi, dz = a.walls.z[j] - zi;
-        const double d2 = dx * dx + dy * dy + dz * dz;
-        if (d2 <= 0.0) continue;
-        const double w = a.wall_scale * (1.0 - sqrt(d2) * a.inv_re);
-        if (w <= 0.0) continue;
-        if (ko.boundary == 2) {
-          neumann<N>(dx, dy, dz, a.walls.normal_x[j], a.walls.normal_y[j], a.walls.normal_z[j], a.inv_re, b);
-        } else {
-          basis<N>(dx, dy, dz, a.inv_re, b);
-        }
-        add_outer<N>(m, b, w);
-      }
-    }
-    // trace and regularisation, moment_matrix.cu:297-308
-    double trace = 0.0;
-#pragma unroll
-    for (int r = 0; r < N; ++r) trace += m[tri(r, r)];
-    const double reg = a.lambda * (trace > 0.0 ? trace / static_cast<double>(N) : 1.0);
-#pragma unroll
-    for (int r = 0; r < N; ++r) m[tri(r, r)] += reg;
-    const int info = cholesky<N>(m);
-    double* out = ko.inverse + static_cast<size_t>(i) * N * N;
-    if (info == 0) {
-      invert_lower<N>(m);
-      store_inverse<N>(m, out);
-    } else {
-      for (int e = 0; e < N * N; ++e) out[e] = __longlong_as_double(0x7ff8000000000000LL);
-      atomicAdd(&a.status->non_spd, 1u);
-      raise_flag(a.status, kFlagNonSpd);
-    }
-    ko.trace[i] = trace;
-    ko.reg[i] = reg;
-    ko.info[i] = info;
+    for (int e = 0; e < E; ++e) m[e] = s_fluid[e * kMomentThreads + threadIdx.x];
+    finish_kind<N, (B1 < 0 ? 0 : B1)>(m, a, a.k1, i, xi, yi, zi);
   }
 }
 
@@ -269,9 +289,8 @@ lsmps_status prepare_moments_impl(lsmps_ctx* ctx, const lsmps_fluid& fluid, cons
   base.lambda = p.lsmps_regularization;
   base.wall_scale = p.lsmps_wall_weight_scale;
   base.status = ctx->d_status;
-  MomentArgs a9 = base;
-  a9.nkinds = 0;
   const index_t n = static_cast<index_t>(fluid.count);
+  int velocity_a = -1, pressure_a = -1;
   for (int k = 0; k < count; ++k) {
     const lsmps_moment& mk = kinds[k];
     const bool type_b = mk.kind == LSMPS_MOMENT_PRESSURE_WALL_NEUMANN_B;
@@ -280,22 +299,33 @@ lsmps_status prepare_moments_impl(lsmps_ctx* ctx, const lsmps_fluid& fluid, cons
       return fail(ctx, LSMPS_INVALID_ARGUMENT, "Invalid Moment matrix cache");
     if (n && (!mk.inverse_matrices || !mk.moment_trace || !mk.regularization_added || !mk.info))
       return fail(ctx, LSMPS_INVALID_ARGUMENT, "Invalid Moment matrix cache buffers");
-    KindOut ko{boundary_of(mk.kind), mk.inverse_matrices, mk.moment_trace, mk.regularization_added, mk.info,
-               mk.inversion_count};
-    if (type_b) {
-      if (n == 0) continue;
-      MomentArgs ab = base;
-      ab.nkinds = 1;
-      ab.kinds[0] = ko;
-      launch(ctx, moment_kernel<10>, dim3(div_up(n, kMomentThreads)), dim3(kMomentThreads), 0, ab);
-    } else {
-      if (a9.nkinds == kMaxKinds) return fail(ctx, LSMPS_INVALID_ARGUMENT, "a Type-A kind is listed twice");
-      a9.kinds[a9.nkinds++] = ko;
-    }
+    if (mk.kind == LSMPS_MOMENT_VELOCITY_WALL_DIRICHLET_A && velocity_a < 0) velocity_a = k;
+    if (mk.kind == LSMPS_MOMENT_PRESSURE_WALL_NEUMANN_A && pressure_a < 0) pressure_a = k;
   }
-  if (a9.nkinds && n) {
-    const size_t smem = a9.nkinds > 1 ? sizeof(double) * 45 * kMomentThreads : 0;
-    launch(ctx, moment_kernel<9>, dim3(div_up(n, kMomentThreads)), dim3(kMomentThreads), smem, a9);
+  if (n == 0) return LSMPS_OK;
+  auto out_of = [](const lsmps_moment& mk) {
+    return KindOut{boundary_of(mk.kind), mk.inverse_matrices, mk.moment_trace, mk.regularization_added, mk.info,
+                   mk.inversion_count};
+  };
+  const dim3 grid(div_up(n, kMomentThreads)), block(kMomentThreads);
+  const bool fused = velocity_a >= 0 && pressure_a >= 0;
+  if (fused) {
+    // The step's two kinds share the fluid sum: one pass over the rows.
+    MomentArgs a = base;
+    a.k0 = out_of(kinds[velocity_a]);
+    a.k1 = out_of(kinds[pressure_a]);
+    launch(ctx, moment_kernel<9, 1, 2>, grid, block, sizeof(double) * 45 * kMomentThreads, a);
+  }
+  for (int k = 0; k < count; ++k) {
+    if (fused && (k == velocity_a || k == pressure_a)) continue;
+    MomentArgs a = base;
+    a.k0 = out_of(kinds[k]);
+    switch (kinds[k].kind) {
+      case LSMPS_MOMENT_VELOCITY_WALL_DIRICHLET_A: launch(ctx, moment_kernel<9, 1, -1>, grid, block, 0, a); break;
+      case LSMPS_MOMENT_PRESSURE_WALL_NEUMANN_A: launch(ctx, moment_kernel<9, 2, -1>, grid, block, 0, a); break;
+      case LSMPS_MOMENT_PRESSURE_WALL_NEUMANN_B: launch(ctx, moment_kernel<10, 2, -1>, grid, block, 0, a); break;
+      default: launch(ctx, moment_kernel<9, 0, -1>, grid, block, 0, a); break;
+    }
   }
   return check_launch(ctx, "moment matrices");
 }

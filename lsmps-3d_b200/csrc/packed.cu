@@ -1,0 +1,39 @@
+// packed.cu - streaming pack kernels for 32-byte neighbour records.
+#include "packed.cuh"
+
+namespace lsmps {
+
+__global__ void pack4_kernel(const double* __restrict__ a, const double* __restrict__ b,
+                             const double* __restrict__ c, const double* __restrict__ d, index_t n,
+                             double4* __restrict__ out) {
+  for (index_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    out[i] = make_double4(a[i], b[i], c[i], d ? d[i] : 0.0);
+}
+
+__global__ void pack4_label_kernel(const double* __restrict__ a, const double* __restrict__ b,
+                                   const double* __restrict__ c, const int32_t* __restrict__ label, index_t n,
+                                   double4* __restrict__ out) {
+  for (index_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    out[i] = make_double4(a[i], b[i], c[i], label ? static_cast<double>(label[i]) : 0.0);
+}
+
+int stream_blocks(lsmps_ctx* ctx, size_t n) {
+  const long long b = div_up(static_cast<long long>(n), 256);
+  const long long cap = static_cast<long long>(ctx->sm_count) * 8;
+  return static_cast<int>(b < 1 ? 1 : (b < cap ? b : cap));
+}
+
+void pack4(lsmps_ctx* ctx, const double* a, const double* b, const double* c, const double* d, size_t n,
+           double4* out) {
+  if (n == 0) return;
+  launch(ctx, pack4_kernel, dim3(stream_blocks(ctx, n)), dim3(256), 0, a, b, c, d, static_cast<index_t>(n), out);
+}
+
+void pack4_label(lsmps_ctx* ctx, const double* a, const double* b, const double* c, const int32_t* label, size_t n,
+                 double4* out) {
+  if (n == 0) return;
+  launch(ctx, pack4_label_kernel, dim3(stream_blocks(ctx, n)), dim3(256), 0, a, b, c, label,
+         static_cast<index_t>(n), out);
+}
+
+}  // namespace lsmps

@@ -1,0 +1,36 @@
+// packed.cuh - 32-byte neighbour records.
+//
+// Gather kernels read, for every CSR entry, several FP64 fields of the
+// neighbour (x, y, z and one more: pressure, a velocity component, a label).
+// Read from the SoA arrays each field is a separate 8-byte access in a
+// different cache sector; packed as one double4 {x, y, z, aux} the record is
+// one aligned 32-byte sector.  The packs are built by small streaming kernels
+// from the caller's SoA arrays into context scratch before a gather kernel
+// runs; the SoA arrays stay the interface.
+#pragma once
+
+#include "common.cuh"
+
+namespace lsmps {
+
+// {a[i], b[i], c[i], d ? d[i] : 0}
+__global__ void pack4_kernel(const double* __restrict__ a, const double* __restrict__ b,
+                             const double* __restrict__ c, const double* __restrict__ d, index_t n,
+                             double4* __restrict__ out);
+
+// {a[i], b[i], c[i], (double)label[i]} (label may be null -> 0)
+__global__ void pack4_label_kernel(const double* __restrict__ a, const double* __restrict__ b,
+                                   const double* __restrict__ c, const int32_t* __restrict__ label, index_t n,
+                                   double4* __restrict__ out);
+
+int stream_blocks(lsmps_ctx* ctx, size_t n);
+
+// Queue a pack of three (or four) SoA arrays into out[n].
+void pack4(lsmps_ctx* ctx, const double* a, const double* b, const double* c, const double* d, size_t n,
+           double4* out);
+void pack4_label(lsmps_ctx* ctx, const double* a, const double* b, const double* c, const int32_t* label, size_t n,
+                 double4* out);
+
+__device__ __forceinline__ double4 ld4(const double4* __restrict__ p, index_t j) { return __ldg(p + j); }
+
+}  // namespace lsmps

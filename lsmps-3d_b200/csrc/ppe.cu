@@ -106,7 +106,7 @@ __global__ void __launch_bounds__(kThreads) ppe_kernel(PpeArgs a) {
   for (index_t o = nb; o < ne; ++o) {
     const index_t j = a.fi[o];
     const double dx = fx[j] - xi, dy = fy[j] - yi, dz = fz[j] - zi;
-    const double w = lin_weight(sqrt(dx * dx + dy * dy + dz * dz), a.re);
+    const double w = lin_weight_mul(sqrt(dx * dx + dy * dy + dz * dz), a.inv_re);
     double off = 0.0;
     if (w > 0.0) {
       basis_a_mul(dx, dy, dz, a.inv_re, b);
@@ -122,7 +122,7 @@ __global__ void __launch_bounds__(kThreads) ppe_kernel(PpeArgs a) {
   for (index_t o = a.wo[i]; o < we; ++o) {
     const index_t j = a.wi[o];
     const double dx = a.walls.x[j] - xi, dy = a.walls.y[j] - yi, dz = a.walls.z[j] - zi;
-    const double bw = lin_weight(sqrt(dx * dx + dy * dy + dz * dz), a.re);
+    const double bw = lin_weight_mul(sqrt(dx * dx + dy * dy + dz * dz), a.inv_re);
     if (bw <= 0.0) continue;
     basis_a_mul(dx, dy, dz, a.inv_re, b);
     acc_rhs(b, a.vwall_scale * bw, a.twx[j] - uxi, a.twy[j] - uyi, a.twz[j] - uzi, rx, ry, rz);

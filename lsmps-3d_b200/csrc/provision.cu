@@ -4,15 +4,21 @@
 // (:178-248), combine_explicit_velocity_kernel (:250-270) and
 // combine_explicit_wall_velocity_kernel (:272-284).
 #include "impl.cuh"
+#include "packed.cuh"
 
 namespace lsmps {
 namespace {
 
 constexpr int kThreads = 128;
 
+// Neighbour records: fp = {x, y, z, 0}, fv = {vx, vy, vz, 0} per fluid
+// particle, wp / wv the same for walls (packed.cuh).
 struct LaplacianArgs {
-  lsmps_fluid fluid;
-  lsmps_walls walls;
+  index_t n;
+  const double4* fp;
+  const double4* fv;
+  const double4* wp;
+  const double4* wv;
   const index_t* fo;
   const index_t* fi;
   const index_t* wo;
@@ -53,35 +59,33 @@ __device__ __forceinline__ double lap_from(const double* __restrict__ inv, const
 
 __global__ void __launch_bounds__(kThreads) laplacian_kernel(LaplacianArgs a) {
   const index_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= static_cast<index_t>(a.fluid.count)) return;
-  const double* __restrict__ fx = a.fluid.x;
-  const double* __restrict__ fy = a.fluid.y;
-  const double* __restrict__ fz = a.fluid.z;
-  const double* __restrict__ vx = a.fluid.vx;
-  const double* __restrict__ vy = a.fluid.vy;
-  const double* __restrict__ vz = a.fluid.vz;
-  const double xi = fx[i], yi = fy[i], zi = fz[i];
-  const double uxi = vx[i], uyi = vy[i], uzi = vz[i];
+  if (i >= a.n) return;
+  const double4 pi = ld4(a.fp, i);
+  const double4 ui = ld4(a.fv, i);
   double rx[9], ry[9], rz[9], b[9];
 #pragma unroll
   for (int r = 0; r < 9; ++r) rx[r] = ry[r] = rz[r] = 0.0;
   const index_t fe = a.fo[i + 1];
   for (index_t o = a.fo[i]; o < fe; ++o) {
     const index_t j = a.fi[o];
-    const double dx = fx[j] - xi, dy = fy[j] - yi, dz = fz[j] - zi;
-    const double w = lin_weight(sqrt(dx * dx + dy * dy + dz * dz), a.re);
+    const double4 q = ld4(a.fp, j);
+    const double4 u = ld4(a.fv, j);
+    const double dx = q.x - pi.x, dy = q.y - pi.y, dz = q.z - pi.z;
+    const double w = lin_weight_mul(sqrt(dx * dx + dy * dy + dz * dz), a.inv_re);
     if (w <= 0.0) continue;
     basis_a_mul(dx, dy, dz, a.inv_re, b);
-    acc_rhs(b, w, vx[j] - uxi, vy[j] - uyi, vz[j] - uzi, rx, ry, rz);
+    acc_rhs(b, w, u.x - ui.x, u.y - ui.y, u.z - ui.z, rx, ry, rz);
   }
   const index_t we = a.wo[i + 1];
   for (index_t o = a.wo[i]; o < we; ++o) {
     const index_t j = a.wi[o];
-    const double dx = a.walls.x[j] - xi, dy = a.walls.y[j] - yi, dz = a.walls.z[j] - zi;
-    const double w = a.wall_scale * lin_weight(sqrt(dx * dx + dy * dy + dz * dz), a.re);
+    const double4 q = ld4(a.wp, j);
+    const double4 u = ld4(a.wv, j);
+    const double dx = q.x - pi.x, dy = q.y - pi.y, dz = q.z - pi.z;
+    const double w = a.wall_scale * lin_weight_mul(sqrt(dx * dx + dy * dy + dz * dz), a.inv_re);
     if (w <= 0.0) continue;
     basis_a_mul(dx, dy, dz, a.inv_re, b);
-    acc_rhs(b, w, a.walls.vx[j] - uxi, a.walls.vy[j] - uyi, a.walls.vz[j] - uzi, rx, ry, rz);
+    acc_rhs(b, w, u.x - ui.x, u.y - ui.y, u.z - ui.z, rx, ry, rz);
   }
   const double* inv = a.inverse + static_cast<size_t>(i) * 81;
   a.lx[i] = lap_from(inv, rx, a.re);
@@ -132,8 +136,15 @@ lsmps_status velocity_laplacian_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const
   if (f.count == 0) return LSMPS_OK;
   if (!vm.inverse_matrices || !lap.x || !lap.y || !lap.z || !f.vx || !f.vy || !f.vz)
     return fail(ctx, LSMPS_INVALID_ARGUMENT, "Provision buffers missing");
-  LaplacianArgs a{f, w, fn.offsets, fn.indices, wn.offsets, wn.indices, vm.inverse_matrices, vm.support_radius,
-                  1.0 / vm.support_radius, vm.wall_weight_scale, lap.x, lap.y, lap.z};
+  if (w.count > 0 && (!w.vx || !w.vy || !w.vz)) return fail(ctx, LSMPS_INVALID_ARGUMENT, "wall velocity missing");
+  if (!ensure_packs(ctx, f.count, w.count)) return fail(ctx, LSMPS_CUDA_ERROR, "pack allocation failed");
+  pack4(ctx, f.x, f.y, f.z, nullptr, f.count, ctx->pack_fluid[0]);
+  pack4(ctx, f.vx, f.vy, f.vz, nullptr, f.count, ctx->pack_fluid[1]);
+  pack4(ctx, w.x, w.y, w.z, nullptr, w.count, ctx->pack_wall[0]);
+  pack4(ctx, w.vx, w.vy, w.vz, nullptr, w.count, ctx->pack_wall[1]);
+  LaplacianArgs a{static_cast<index_t>(f.count), ctx->pack_fluid[0], ctx->pack_fluid[1], ctx->pack_wall[0],
+                  ctx->pack_wall[1], fn.offsets, fn.indices, wn.offsets, wn.indices, vm.inverse_matrices,
+                  vm.support_radius, 1.0 / vm.support_radius, vm.wall_weight_scale, lap.x, lap.y, lap.z};
   launch(ctx, laplacian_kernel, dim3(div_up(static_cast<long long>(f.count), kThreads)), dim3(kThreads), 0, a);
   return check_launch(ctx, "velocity laplacian");
 }
