@@ -31,6 +31,12 @@ void pack4(lsmps_ctx* ctx, const double* a, const double* b, const double* c, co
 void pack4_label(lsmps_ctx* ctx, const double* a, const double* b, const double* c, const int32_t* label, size_t n,
                  double4* out);
 
-__device__ __forceinline__ double4 ld4(const double4* __restrict__ p, index_t j) { return __ldg(p + j); }
+// One record through the read-only path: two 16-byte loads of one sector.
+__device__ __forceinline__ double4 ld4(const double4* __restrict__ p, index_t j) {
+  const double2* q = reinterpret_cast<const double2*>(p + j);
+  const double2 a = __ldg(q);
+  const double2 b = __ldg(q + 1);
+  return make_double4(a.x, a.y, b.x, b.y);
+}
 
 }  // namespace lsmps
