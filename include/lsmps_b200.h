@@ -281,6 +281,22 @@ lsmps_status lsmps_ctx_synchronize(lsmps_ctx* ctx);
 uint64_t lsmps_ctx_required(lsmps_ctx* ctx);
 /* Number of kernel launches this context has queued since creation. */
 uint64_t lsmps_ctx_launch_count(lsmps_ctx* ctx);
+/* Launch-shape knobs (no counterpart in the reference, whose kernels all use
+ * one thread per particle in 128-thread blocks).  Values are indices into each
+ * knob's variant list. */
+typedef enum lsmps_knob {
+  /* moment kernel register budget: 0 = compiler's choice, 1 = capped for 8
+   * blocks per SM (default) */
+  LSMPS_KNOB_MOMENT_OCCUPANCY = 0,
+  /* lanes cooperating on one PPE row: 0 -> 1 (default), 1 -> 4, 2 -> 8,
+   * 3 -> 16 */
+  LSMPS_KNOB_PPE_LANES = 1,
+  LSMPS_KNOB_COUNT = 2
+} lsmps_knob;
+lsmps_status lsmps_ctx_set_knob(lsmps_ctx* ctx, int knob, int value);
+int lsmps_ctx_knob(lsmps_ctx* ctx, int knob);
+/* Number of variants of a knob (0 for an unknown knob). */
+int lsmps_knob_variants(int knob);
 /* Per-kernel device timing (no counterpart in the reference, which has no
  * tracing): while on, every launch is bracketed by CUDA events.  Turning it
  * on clears the records. */

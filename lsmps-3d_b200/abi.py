@@ -39,6 +39,11 @@ STATUS_NAMES = {
 PRECISION_PLAIN = 0
 PRECISION_MIXED = 1
 
+# Launch-shape knobs (lsmps_knob).
+KNOB_MOMENT_OCCUPANCY = 0
+KNOB_PPE_LANES = 1
+KNOB_COUNT = 2
+
 # Surface labels, include/lsmps3d/surface/surface_type.cuh:5-10.
 INNER, NEAR_SURFACE, SURFACE, SPLASH = 0, 1, 2, 3
 
@@ -232,6 +237,9 @@ _SIGNATURES = {
     "lsmps_ctx_required": (c_uint64, [c_void_p]),
     "lsmps_ctx_launch_count": (c_uint64, [c_void_p]),
     "lsmps_ctx_set_profiling": (c_int, [c_void_p, c_int]),
+    "lsmps_ctx_set_knob": (c_int, [c_void_p, c_int, c_int]),
+    "lsmps_ctx_knob": (c_int, [c_void_p, c_int]),
+    "lsmps_knob_variants": (c_int, [c_int]),
     "lsmps_ctx_profile_report": (c_int, [c_void_p, ctypes.c_char_p, c_size_t, P(c_double), P(c_uint64), c_int]),
     "lsmps_ctx_last_error": (c_char_p, [c_void_p]),
     "lsmps_status_string": (c_char_p, [c_int]),

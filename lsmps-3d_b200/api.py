@@ -92,6 +92,12 @@ class Context:
     def set_profiling(self, on: bool) -> None:
         self.check(_lib.lsmps_ctx_set_profiling(self.h, 1 if on else 0))
 
+    def set_knob(self, knob: int, value: int) -> None:
+        self.check(_lib.lsmps_ctx_set_knob(self.h, knob, value))
+
+    def knob(self, knob: int) -> int:
+        return int(_lib.lsmps_ctx_knob(self.h, knob))
+
     def profile_report(self, max_entries: int = 64) -> list[tuple[str, float, int]]:
         """(kernel name, total ms, launches) per kernel since profiling was
         switched on; clears the records."""

@@ -125,6 +125,8 @@ struct lsmps_ctx {
   bool profiling = false;
   std::vector<ProfileRecord> profile;
   size_t profile_used = 0;
+  // Launch-shape knobs (lsmps_knob).
+  int knob[LSMPS_KNOB_COUNT] = {1, 0};
   // 32-byte neighbour records (packed.cuh): two fluid and three wall arrays.
   double4* pack_fluid[2] = {nullptr, nullptr};
   double4* pack_wall[3] = {nullptr, nullptr, nullptr};

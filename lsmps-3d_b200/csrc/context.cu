@@ -224,6 +224,26 @@ lsmps_status lsmps_ctx_synchronize(lsmps_ctx* ctx) {
 
 uint64_t lsmps_ctx_required(lsmps_ctx* ctx) { return ctx ? ctx->required : 0; }
 
+int lsmps_knob_variants(int knob) {
+  switch (knob) {
+    case LSMPS_KNOB_MOMENT_OCCUPANCY: return 2;
+    case LSMPS_KNOB_PPE_LANES: return 1;
+    default: return 0;
+  }
+}
+
+lsmps_status lsmps_ctx_set_knob(lsmps_ctx* ctx, int knob, int value) {
+  if (!ctx || knob < 0 || knob >= LSMPS_KNOB_COUNT || value < 0 || value >= lsmps_knob_variants(knob))
+    return LSMPS_INVALID_ARGUMENT;
+  ctx->knob[knob] = value;
+  return LSMPS_OK;
+}
+
+int lsmps_ctx_knob(lsmps_ctx* ctx, int knob) {
+  if (!ctx || knob < 0 || knob >= LSMPS_KNOB_COUNT) return -1;
+  return ctx->knob[knob];
+}
+
 lsmps_status lsmps_ctx_set_profiling(lsmps_ctx* ctx, int on) {
   if (!ctx) return LSMPS_INVALID_ARGUMENT;
   ctx->profiling = on != 0;

@@ -18,6 +18,7 @@
 #include <utility>
 
 #include "impl.cuh"
+#include "packed.cuh"
 
 namespace lsmps {
 namespace {
@@ -254,6 +255,223 @@ __global__ void __launch_bounds__(kMomentThreads) moment_kernel(MomentArgs a) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Type-A through monomial sums.
+//
+// Every entry of sum_j w b b^T with b = (sx, sy, sz, sx^2, sy^2, sz^2, sx sy,
+// sy sz, sz sx) is a weighted sum of one monomial of degree 2, 3 or 4 in
+// (sx, sy, sz), and the 45 lower-triangle entries share 31 distinct
+// monomials (6 + 10 + 15).  The hot loop accumulates those 31 sums
+// (10 products and 31 FMAs per neighbour instead of 18 products and 45 FMAs)
+// and the 45 entries are expanded once per particle.  Wall Dirichlet samples
+// use the same basis and go into the same sums; the wall Neumann vectors have
+// no such structure and are added to the expanded entries.
+// ---------------------------------------------------------------------------
+constexpr int kMonomials = 31;
+
+// Exponent of axis (0 x, 1 y, 2 z) in Type-A basis entry r.
+__host__ __device__ constexpr int basis_exponent(int r, int axis) {
+  return r < 3 ? (r == axis ? 1 : 0)
+       : r == 3 ? (axis == 0 ? 2 : 0)
+       : r == 4 ? (axis == 1 ? 2 : 0)
+       : r == 5 ? (axis == 2 ? 2 : 0)
+       : r == 6 ? (axis == 0 || axis == 1 ? 1 : 0)
+       : r == 7 ? (axis == 1 || axis == 2 ? 1 : 0)
+                : (axis == 2 || axis == 0 ? 1 : 0);
+}
+
+// Slot of the monomial x^a y^b z^c in the 31 sums (layout of acc_monomials).
+__host__ __device__ constexpr int monomial_slot(int a, int b, int c) {
+  const int code = a * 25 + b * 5 + c;
+  switch (code) {
+    case 50: return 0;   // xx
+    case 10: return 1;   // yy
+    case 2: return 2;    // zz
+    case 30: return 3;   // xy
+    case 6: return 4;    // yz
+    case 26: return 5;   // zx
+    case 75: return 6;   // xxx
+    case 15: return 7;   // yyy
+    case 3: return 8;    // zzz
+    case 55: return 9;   // xxy
+    case 51: return 10;  // xxz
+    case 35: return 11;  // xyy
+    case 11: return 12;  // yyz
+    case 27: return 13;  // xzz
+    case 7: return 14;   // yzz
+    case 31: return 15;  // xyz
+    case 100: return 16; // xxxx
+    case 20: return 17;  // yyyy
+    case 4: return 18;   // zzzz
+    case 80: return 19;  // xxxy
+    case 76: return 20;  // xxxz
+    case 40: return 21;  // xyyy
+    case 16: return 22;  // yyyz
+    case 28: return 23;  // xzzz
+    case 8: return 24;   // yzzz
+    case 60: return 25;  // xxyy
+    case 12: return 26;  // yyzz
+    case 52: return 27;  // xxzz
+    case 56: return 28;  // xxyz
+    case 36: return 29;  // xyyz
+    case 32: return 30;  // xyzz
+    default: return -1;
+  }
+}
+
+__host__ __device__ constexpr int entry_slot(int r, int c) {
+  return monomial_slot(basis_exponent(r, 0) + basis_exponent(c, 0), basis_exponent(r, 1) + basis_exponent(c, 1),
+                       basis_exponent(r, 2) + basis_exponent(c, 2));
+}
+
+__device__ __forceinline__ void acc_monomials(double (&s)[kMonomials], double sx, double sy, double sz, double w) {
+  const double qxx = sx * sx, qyy = sy * sy, qzz = sz * sz;
+  const double qxy = sx * sy, qyz = sy * sz, qzx = sz * sx;
+  const double wxx = w * qxx, wyy = w * qyy, wzz = w * qzz, wxy = w * qxy;
+  s[0] = fma(w, qxx, s[0]);
+  s[1] = fma(w, qyy, s[1]);
+  s[2] = fma(w, qzz, s[2]);
+  s[3] = fma(w, qxy, s[3]);
+  s[4] = fma(w, qyz, s[4]);
+  s[5] = fma(w, qzx, s[5]);
+  s[6] = fma(wxx, sx, s[6]);
+  s[7] = fma(wyy, sy, s[7]);
+  s[8] = fma(wzz, sz, s[8]);
+  s[9] = fma(wxx, sy, s[9]);
+  s[10] = fma(wxx, sz, s[10]);
+  s[11] = fma(wyy, sx, s[11]);
+  s[12] = fma(wyy, sz, s[12]);
+  s[13] = fma(wzz, sx, s[13]);
+  s[14] = fma(wzz, sy, s[14]);
+  s[15] = fma(wxy, sz, s[15]);
+  s[16] = fma(wxx, qxx, s[16]);
+  s[17] = fma(wyy, qyy, s[17]);
+  s[18] = fma(wzz, qzz, s[18]);
+  s[19] = fma(wxx, qxy, s[19]);
+  s[20] = fma(wxx, qzx, s[20]);
+  s[21] = fma(wyy, qxy, s[21]);
+  s[22] = fma(wyy, qyz, s[22]);
+  s[23] = fma(wzz, qzx, s[23]);
+  s[24] = fma(wzz, qyz, s[24]);
+  s[25] = fma(wxx, qyy, s[25]);
+  s[26] = fma(wyy, qzz, s[26]);
+  s[27] = fma(wzz, qxx, s[27]);
+  s[28] = fma(wxx, qyz, s[28]);
+  s[29] = fma(wyy, qzx, s[29]);
+  s[30] = fma(wzz, qxy, s[30]);
+}
+
+struct MomentPackedArgs {
+  index_t n;
+  const double4* fp;  // {x, y, z, -} fluid
+  const double4* wp;  // {x, y, z, -} walls
+  const double4* wn;  // {nx, ny, nz, -} walls
+  const index_t* fo;
+  const index_t* fi;
+  const index_t* wo;
+  const index_t* wi;
+  double inv_re;
+  double lambda;
+  double wall_scale;
+  KindOut k0;
+  KindOut k1;
+  DeviceStatus* status;
+};
+
+template <int B>
+__device__ __forceinline__ void finish_a(double (&s)[kMonomials], const MomentPackedArgs& a, const KindOut& ko,
+                                         index_t i, const double4& pi) {
+  const index_t wb = a.wo[i], we = a.wo[i + 1];
+  if (B == 1) {
+    for (index_t o = wb; o < we; ++o) {
+      const double4 q = ld4(a.wp, a.wi[o]);
+      const double dx = q.x - pi.x, dy = q.y - pi.y, dz = q.z - pi.z;
+      const double d2 = dx * dx + dy * dy + dz * dz;
+      if (d2 <= 0.0) continue;
+      const double w = a.wall_scale * (1.0 - sqrt(d2) * a.inv_re);
+      if (w <= 0.0) continue;
+      acc_monomials(s, dx * a.inv_re, dy * a.inv_re, dz * a.inv_re, w);
+    }
+  }
+  double m[45];
+#pragma unroll
+  for (int r = 0; r < 9; ++r) {
+#pragma unroll
+    for (int c = 0; c <= r; ++c) m[tri(r, c)] = s[entry_slot(r, c)];
+  }
+  if (B == 2) {
+    double q9[9];
+    for (index_t o = wb; o < we; ++o) {
+      const index_t j = a.wi[o];
+      const double4 q = ld4(a.wp, j);
+      const double dx = q.x - pi.x, dy = q.y - pi.y, dz = q.z - pi.z;
+      const double d2 = dx * dx + dy * dy + dz * dz;
+      if (d2 <= 0.0) continue;
+      const double w = a.wall_scale * (1.0 - sqrt(d2) * a.inv_re);
+      if (w <= 0.0) continue;
+      const double4 nrm = ld4(a.wn, j);
+      neumann<9>(dx, dy, dz, nrm.x, nrm.y, nrm.z, a.inv_re, q9);
+      add_outer<9>(m, q9, w);
+    }
+  }
+  double trace = 0.0;
+#pragma unroll
+  for (int r = 0; r < 9; ++r) trace += m[tri(r, r)];
+  const double reg = a.lambda * (trace > 0.0 ? trace / 9.0 : 1.0);
+#pragma unroll
+  for (int r = 0; r < 9; ++r) m[tri(r, r)] += reg;
+  const int info = cholesky<9>(m);
+  double* out = ko.inverse + static_cast<size_t>(i) * 81;
+  if (info == 0) {
+    invert_lower<9>(m);
+    store_inverse<9>(m, out);
+  } else {
+    for (int e = 0; e < 81; ++e) out[e] = __longlong_as_double(0x7ff8000000000000LL);
+    atomicAdd(&a.status->non_spd, 1u);
+    raise_flag(a.status, kFlagNonSpd);
+  }
+  ko.trace[i] = trace;
+  ko.reg[i] = reg;
+  ko.info[i] = info;
+}
+
+// Type-A kinds B0 (and B1 >= 0) from one pass over the fluid row.  MinBlocks
+// is the register budget variant (LSMPS_KNOB_MOMENT_OCCUPANCY).
+template <int B0, int B1, int MinBlocks>
+__global__ void __launch_bounds__(kMomentThreads, MinBlocks) moment_a_kernel(MomentPackedArgs a) {
+  extern __shared__ double s_mono[];  // [kMonomials][kMomentThreads] when B1 >= 0
+  const index_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (a.k0.count) atomicAdd(a.k0.count, 1);
+    if (B1 >= 0 && a.k1.count) atomicAdd(a.k1.count, 1);
+  }
+  if (i >= a.n) return;
+  const double4 pi = ld4(a.fp, i);
+  double s[kMonomials];
+#pragma unroll
+  for (int e = 0; e < kMonomials; ++e) s[e] = 0.0;
+  const index_t fe = a.fo[i + 1];
+  for (index_t o = a.fo[i]; o < fe; ++o) {
+    const double4 q = ld4(a.fp, a.fi[o]);
+    const double dx = q.x - pi.x, dy = q.y - pi.y, dz = q.z - pi.z;
+    const double d2 = dx * dx + dy * dy + dz * dz;
+    if (d2 <= 0.0) continue;
+    const double w = 1.0 - sqrt(d2) * a.inv_re;
+    if (w <= 0.0) continue;
+    acc_monomials(s, dx * a.inv_re, dy * a.inv_re, dz * a.inv_re, w);
+  }
+  if (B1 >= 0) {
+#pragma unroll
+    for (int e = 0; e < kMonomials; ++e) s_mono[e * kMomentThreads + threadIdx.x] = s[e];
+  }
+  finish_a<B0>(s, a, a.k0, i, pi);
+  if (B1 >= 0) {
+#pragma unroll
+    for (int e = 0; e < kMonomials; ++e) s[e] = s_mono[e * kMomentThreads + threadIdx.x];
+    finish_a<(B1 < 0 ? 0 : B1)>(s, a, a.k1, i, pi);
+  }
+}
+
 // make_matrix_request, moment_matrix.cu:494-538: boundary of each kind.
 int boundary_of(int kind) {
   switch (kind) {
@@ -308,23 +526,46 @@ lsmps_status prepare_moments_impl(lsmps_ctx* ctx, const lsmps_fluid& fluid, cons
                    mk.inversion_count};
   };
   const dim3 grid(div_up(n, kMomentThreads)), block(kMomentThreads);
+  if (!ensure_packs(ctx, fluid.count, walls.count)) return fail(ctx, LSMPS_CUDA_ERROR, "pack allocation failed");
+  pack4(ctx, fluid.x, fluid.y, fluid.z, nullptr, fluid.count, ctx->pack_fluid[0]);
+  pack4(ctx, walls.x, walls.y, walls.z, nullptr, walls.count, ctx->pack_wall[0]);
+  pack4(ctx, walls.normal_x, walls.normal_y, walls.normal_z, nullptr, walls.count, ctx->pack_wall[2]);
+  MomentPackedArgs pa{n, ctx->pack_fluid[0], ctx->pack_wall[0], ctx->pack_wall[2], fn.offsets, fn.indices,
+                      wn.offsets, wn.indices, base.inv_re, base.lambda, base.wall_scale, KindOut{}, KindOut{},
+                      ctx->d_status};
   const bool fused = velocity_a >= 0 && pressure_a >= 0;
+  const bool capped = ctx->knob[LSMPS_KNOB_MOMENT_OCCUPANCY] == 1;
   if (fused) {
-    // The step's two kinds share the fluid sum: one pass over the rows.
-    MomentArgs a = base;
+    // The step's two kinds share the fluid sums: one pass over the rows.
+    MomentPackedArgs a = pa;
     a.k0 = out_of(kinds[velocity_a]);
     a.k1 = out_of(kinds[pressure_a]);
-    launch(ctx, moment_kernel<9, 1, 2>, grid, block, sizeof(double) * 45 * kMomentThreads, a);
+    const size_t smem = sizeof(double) * kMonomials * kMomentThreads;
+    if (capped)
+      launch_named(ctx, "moment_a_kernel<V,P>", moment_a_kernel<1, 2, 8>, grid, block, smem, a);
+    else
+      launch_named(ctx, "moment_a_kernel<V,P>", moment_a_kernel<1, 2, 1>, grid, block, smem, a);
   }
   for (int k = 0; k < count; ++k) {
     if (fused && (k == velocity_a || k == pressure_a)) continue;
-    MomentArgs a = base;
+    MomentPackedArgs a = pa;
     a.k0 = out_of(kinds[k]);
     switch (kinds[k].kind) {
-      case LSMPS_MOMENT_VELOCITY_WALL_DIRICHLET_A: launch(ctx, moment_kernel<9, 1, -1>, grid, block, 0, a); break;
-      case LSMPS_MOMENT_PRESSURE_WALL_NEUMANN_A: launch(ctx, moment_kernel<9, 2, -1>, grid, block, 0, a); break;
-      case LSMPS_MOMENT_PRESSURE_WALL_NEUMANN_B: launch(ctx, moment_kernel<10, 2, -1>, grid, block, 0, a); break;
-      default: launch(ctx, moment_kernel<9, 0, -1>, grid, block, 0, a); break;
+      case LSMPS_MOMENT_VELOCITY_WALL_DIRICHLET_A:
+        launch_named(ctx, "moment_a_kernel<V>", moment_a_kernel<1, -1, 1>, grid, block, 0, a);
+        break;
+      case LSMPS_MOMENT_PRESSURE_WALL_NEUMANN_A:
+        launch_named(ctx, "moment_a_kernel<P>", moment_a_kernel<2, -1, 1>, grid, block, 0, a);
+        break;
+      case LSMPS_MOMENT_PRESSURE_WALL_NEUMANN_B: {
+        MomentArgs b = base;
+        b.k0 = a.k0;
+        launch_named(ctx, "moment_kernel<B>", moment_kernel<10, 2, -1>, grid, block, 0, b);
+        break;
+      }
+      default:
+        launch_named(ctx, "moment_a_kernel<F>", moment_a_kernel<0, -1, 1>, grid, block, 0, a);
+        break;
     }
   }
   return check_launch(ctx, "moment matrices");
