@@ -322,6 +322,37 @@ lsmps_status lsmps_build_cell_list(lsmps_ctx* ctx, const double* x, const double
                                    const double* z, size_t count, const lsmps_grid* grid,
                                    const lsmps_cells* cells);
 
+/* The same cell list, bit-identical to lsmps_build_cell_list's, from a call
+ * that allocates no memory and needs no context.  No counterpart in the
+ * reference, whose build_cell_list sorts through Thrust's allocator.
+ *
+ * For callers that must not allocate device memory while they run: a process
+ * whose device memory is all handed out by its own pool allocator, or a loop
+ * that must not meet the device-wide synchronisation of cudaFree.  The
+ * context entry point grows its scratch with cudaMalloc on demand; this one
+ * sorts in a fixed scratch array compiled into the library (about 4.1 MiB of
+ * device memory per device, loaded with the library's device code).
+ *
+ * - count above LSMPS_NOALLOC_MAX_PARTICLES returns LSMPS_CAPACITY_EXCEEDED
+ *   before any device work; other argument errors return
+ *   LSMPS_INVALID_ARGUMENT (LSMPS_INDEX_OVERFLOW for more than 2^31-1 cells).
+ * - Runs on the calling thread's current device, on `stream` (a
+ *   cudaStream_t; NULL is the legacy default stream), and waits for it before
+ *   returning.  A NaN or infinite coordinate returns LSMPS_NON_FINITE.
+ * - The first call on a device does its set-up: it looks up the scratch
+ *   array's device address, which makes the CUDA runtime load the library's
+ *   device code on that device.  Make that first call before capturing any
+ *   stream.
+ * - Nothing has to be zeroed beforehand: each call clears its own status
+ *   word and writes every scratch entry before reading it.
+ * - There is one scratch array per device, so two calls in flight at once on
+ *   one device would race on it.  Calls are therefore serialised per device
+ *   by a lock held until the call's kernels finish: a second host thread
+ *   calling on the same device waits.  (Each process has its own array.) */
+#define LSMPS_NOALLOC_MAX_PARTICLES 524288
+lsmps_status lsmps_build_cell_list_noalloc(void* stream, const double* x, const double* y, const double* z,
+                                           size_t count, const lsmps_grid* grid, const lsmps_cells* cells);
+
 /* build_neighbor_lists(...), neighbor_search.cuh:18-24.  Rows follow the
  * reference traversal order (27 cells dz -> dy -> dx, ascending sorted
  * position inside each cell); fluid rows exclude the particle itself. */

@@ -44,6 +44,9 @@ KNOB_MOMENT_OCCUPANCY = 0
 KNOB_PPE_LANES = 1
 KNOB_COUNT = 2
 
+# Particle limit of lsmps_build_cell_list_noalloc (its fixed scratch).
+NOALLOC_MAX_PARTICLES = 524288
+
 # Surface labels, include/lsmps3d/surface/surface_type.cuh:5-10.
 INNER, NEAR_SURFACE, SURFACE, SPLASH = 0, 1, 2, 3
 
@@ -245,6 +248,7 @@ _SIGNATURES = {
     "lsmps_status_string": (c_char_p, [c_int]),
     "lsmps_params_default": (None, [P(Params)]),
     "lsmps_build_cell_list": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, P(Grid), P(Cells)]),
+    "lsmps_build_cell_list_noalloc": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, P(Grid), P(Cells)]),
     "lsmps_build_neighbor_lists": (c_int, [c_void_p, P(Fluid), P(Walls), P(Params), P(Cells), P(Cells), P(Csr), P(Csr)]),
     "lsmps_reference_number_density": (c_double, [c_double, c_double]),
     "lsmps_classify_surface": (c_int, [c_void_p, P(Fluid), P(Walls), P(Csr), P(Csr), P(Params), P(SurfaceDiagnostics)]),

@@ -12,17 +12,10 @@
 #include <climits>
 #include <cmath>
 
-#include "common.cuh"
+#include "cells.cuh"
 
 namespace lsmps {
 namespace {
-
-constexpr int kRadixBits = 8;
-constexpr int kRadixBins = 1 << kRadixBits;
-constexpr int kSortThreads = 256;
-constexpr int kSortWarps = kSortThreads / kWarp;
-constexpr int kSortItems = 16;
-constexpr int kSortTile = kSortThreads * kSortItems;
 
 // clamp_cell_index, neighbor_search.cu:36-46, with the float-to-int
 // conversion of an out-of-range or NaN value made explicit.
@@ -38,6 +31,8 @@ __device__ __forceinline__ index_t cell_coord(double coordinate, double origin, 
   if (f >= static_cast<double>(dim)) return dim - 1;
   return static_cast<index_t>(f);
 }
+
+}  // namespace
 
 // assign_cells_kernel (neighbor_search.cu:61-73) fused with the cell-range
 // reset of reset_cell_ranges_kernel (:75-83).
@@ -148,8 +143,6 @@ int key_bits(long long ncell) {
   while ((1LL << bits) < ncell) ++bits;
   return bits;
 }
-
-}  // namespace
 
 lsmps_status validate_grid(lsmps_ctx* ctx, const lsmps_grid& grid) {
   if (!(grid.cell_size > 0.0) || grid.dims[0] <= 0 || grid.dims[1] <= 0 || grid.dims[2] <= 0)
