@@ -288,7 +288,7 @@ typedef enum lsmps_knob {
   /* moment kernel register budget: 0 = compiler's choice, 1 = capped for 8
    * blocks per SM (default) */
   LSMPS_KNOB_MOMENT_OCCUPANCY = 0,
-  /* lanes cooperating on one PPE row: 0 -> 1 (default), 1 -> 4, 2 -> 8,
+  /* lanes cooperating on one PPE row: 0 -> 1, 1 -> 4, 2 -> 8 (default),
    * 3 -> 16 */
   LSMPS_KNOB_PPE_LANES = 1,
   LSMPS_KNOB_COUNT = 2

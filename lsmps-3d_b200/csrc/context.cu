@@ -227,7 +227,7 @@ uint64_t lsmps_ctx_required(lsmps_ctx* ctx) { return ctx ? ctx->required : 0; }
 int lsmps_knob_variants(int knob) {
   switch (knob) {
     case LSMPS_KNOB_MOMENT_OCCUPANCY: return 2;
-    case LSMPS_KNOB_PPE_LANES: return 1;
+    case LSMPS_KNOB_PPE_LANES: return 4;
     default: return 0;
   }
 }

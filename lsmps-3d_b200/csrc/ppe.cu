@@ -141,6 +141,112 @@ __global__ void __launch_bounds__(kThreads) ppe_kernel(PpeArgs a) {
   if (a.wall_rhs_out) a.wall_rhs_out[i] = wall_rhs;
 }
 
+// Sum over the G lanes of a row group (G a power of two dividing 32); every
+// lane of the group ends with the total.  `mask` names the group's lanes
+// only, since other groups of the warp may have left.
+template <int G>
+__device__ __forceinline__ double group_sum(double v, unsigned mask) {
+#pragma unroll
+  for (int d = G / 2; d > 0; d >>= 1) v += __shfl_xor_sync(mask, v, d);
+  return v;
+}
+
+// The same row with G lanes per particle: lane l takes the neighbours
+// nb + l, nb + l + G, ..., so the G lanes write G consecutive (col, val)
+// slots per round and issue G independent gathers.  The partial sums (the
+// diagonal, the 27 divergence moments and the wall Neumann term) are added
+// across the group with shuffles; lane 0 finishes the row.  The sums are
+// associated differently from the one-lane kernel (rounding-level change).
+template <int G>
+__global__ void __launch_bounds__(kThreads) ppe_lanes_kernel(PpeArgs a) {
+  const index_t i = (blockIdx.x * blockDim.x + threadIdx.x) / G;
+  const int l = threadIdx.x & (G - 1);
+  const index_t n = static_cast<index_t>(a.fluid.count);
+  // Whole groups leave together, so the shuffles below see full groups.
+  if (i >= n) return;
+  const index_t nb = a.fo[i], ne = a.fo[i + 1];
+  const index_t row = i + nb;
+  if (l == 0) {
+    a.row_offsets[i] = row;
+    if (i + 1 == n) a.row_offsets[n] = n + ne;
+  }
+  const int type = a.fluid.surface_type ? a.fluid.surface_type[i] : LSMPS_SURFACE_INNER;
+  if (type == LSMPS_SURFACE_SURFACE || type == LSMPS_SURFACE_SPLASH) {
+    for (index_t o = nb + l; o < ne; o += G) {
+      a.col[row + 1 + o - nb] = a.fi[o];
+      a.val[row + 1 + o - nb] = 0.0;
+    }
+    if (l == 0) {
+      a.col[row] = i;
+      a.val[row] = 1.0;
+      a.rhs[i] = 0.0;
+      a.divergence[i] = 0.0;
+      if (a.wall_rhs_out) a.wall_rhs_out[i] = 0.0;
+    }
+    return;
+  }
+  const double* __restrict__ fx = a.fluid.x;
+  const double* __restrict__ fy = a.fluid.y;
+  const double* __restrict__ fz = a.fluid.z;
+  const double xi = fx[i], yi = fy[i], zi = fz[i];
+  const double* __restrict__ pinv = a.pinv + static_cast<size_t>(i) * 81;
+  double L[9];
+#pragma unroll
+  for (int col = 0; col < 9; ++col) L[col] = pinv[3 + col * 9] + pinv[4 + col * 9] + pinv[5 + col * 9];
+  const double uxi = a.tvx[i], uyi = a.tvy[i], uzi = a.tvz[i];
+  const double scale = 2.0 / (a.re * a.re * a.density);
+  double rx[9], ry[9], rz[9], b[9];
+#pragma unroll
+  for (int r = 0; r < 9; ++r) rx[r] = ry[r] = rz[r] = 0.0;
+  double diag = 0.0;
+  for (index_t o = nb + l; o < ne; o += G) {
+    const index_t j = a.fi[o];
+    const double dx = fx[j] - xi, dy = fy[j] - yi, dz = fz[j] - zi;
+    const double w = lin_weight_mul(sqrt(dx * dx + dy * dy + dz * dz), a.inv_re);
+    double off = 0.0;
+    if (w > 0.0) {
+      basis_a_mul(dx, dy, dz, a.inv_re, b);
+      off = w * dot9(L, b) * scale;
+      diag -= off;
+      acc_rhs(b, w, a.tvx[j] - uxi, a.tvy[j] - uyi, a.tvz[j] - uzi, rx, ry, rz);
+    }
+    a.col[row + 1 + o - nb] = j;
+    a.val[row + 1 + o - nb] = off;
+  }
+  double wall_rhs = 0.0;
+  const index_t we = a.wo[i + 1];
+  for (index_t o = a.wo[i] + l; o < we; o += G) {
+    const index_t j = a.wi[o];
+    const double dx = a.walls.x[j] - xi, dy = a.walls.y[j] - yi, dz = a.walls.z[j] - zi;
+    const double bw = lin_weight_mul(sqrt(dx * dx + dy * dy + dz * dz), a.inv_re);
+    if (bw <= 0.0) continue;
+    basis_a_mul(dx, dy, dz, a.inv_re, b);
+    acc_rhs(b, a.vwall_scale * bw, a.twx[j] - uxi, a.twy[j] - uyi, a.twz[j] - uzi, rx, ry, rz);
+    const double nx = a.walls.normal_x[j], ny = a.walls.normal_y[j], nz = a.walls.normal_z[j];
+    const double ng = a.gx * nx + a.gy * ny + a.gz * nz;
+    double q[9];
+    neumann_a(dx, dy, dz, nx, ny, nz, a.inv_re, q);
+    wall_rhs += 2.0 * a.pwall_scale * bw * ng * dot9(L, q) * a.inv_re;
+  }
+  const unsigned mask = ((G == 32) ? 0xffffffffu : ((1u << G) - 1u)) << ((threadIdx.x & (kWarp - 1)) & ~(G - 1));
+  diag = group_sum<G>(diag, mask);
+  wall_rhs = group_sum<G>(wall_rhs, mask);
+#pragma unroll
+  for (int r = 0; r < 9; ++r) {
+    rx[r] = group_sum<G>(rx[r], mask);
+    ry[r] = group_sum<G>(ry[r], mask);
+    rz[r] = group_sum<G>(rz[r], mask);
+  }
+  if (l != 0) return;
+  const double* __restrict__ vinv = a.vinv + static_cast<size_t>(i) * 81;
+  const double div = (coeff_row(vinv, rx, 0) + coeff_row(vinv, ry, 1) + coeff_row(vinv, rz, 2)) * a.inv_re;
+  a.col[row] = i;
+  a.val[row] = diag;
+  a.divergence[i] = div;
+  a.rhs[i] = div / a.dt - wall_rhs;
+  if (a.wall_rhs_out) a.wall_rhs_out[i] = wall_rhs;
+}
+
 }  // namespace
 
 lsmps_status assemble_ppe_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const lsmps_walls& w, const lsmps_params& p,
@@ -191,7 +297,13 @@ lsmps_status assemble_ppe_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const lsmps
   a.rhs = ws.rhs;
   a.divergence = ws.divergence;
   a.wall_rhs_out = ws.pressure_laplacian;
-  launch(ctx, ppe_kernel, dim3(div_up(static_cast<long long>(f.count), kThreads)), dim3(kThreads), 0, a);
+  const long long rows = static_cast<long long>(f.count);
+  switch (ctx->knob[LSMPS_KNOB_PPE_LANES]) {
+    case 1: launch(ctx, ppe_lanes_kernel<4>, dim3(div_up(rows * 4, kThreads)), dim3(kThreads), 0, a); break;
+    case 2: launch(ctx, ppe_lanes_kernel<8>, dim3(div_up(rows * 8, kThreads)), dim3(kThreads), 0, a); break;
+    case 3: launch(ctx, ppe_lanes_kernel<16>, dim3(div_up(rows * 16, kThreads)), dim3(kThreads), 0, a); break;
+    default: launch(ctx, ppe_kernel, dim3(div_up(rows, kThreads)), dim3(kThreads), 0, a); break;
+  }
   return check_launch(ctx, "PPE assembly");
 }
 

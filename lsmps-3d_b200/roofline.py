@@ -41,27 +41,35 @@ def step_bytes(nf: int, nw: int, kf: int, kw: int, c: int, s: int = 8) -> int:
 
 
 def kernel_bytes(nf: int, nw: int, kf: int, kw: int, c: int, s: int = 8) -> dict[str, int]:
-    """Algorithmic bytes per launch of the library's kernels (names as the
-    profiler reports them).  CSR kernels run once per table, so their table
-    sizes are summed over both launches and reported per launch on average."""
+    """Algorithmic bytes per launch of the step's kernels (names as the
+    library's profiler reports them): every array the kernel must read or
+    write counted once, neighbour gathers included once per array.  The two
+    CSR kernels run once per table (fluid, wall); their figure is the mean of
+    the two launches."""
     k = kf + kw
     pos_f = 3 * s * nf
     pos_w = 3 * s * nw
+    rows = 8 * (nf + 1) + 4 * k  # fluid and wall CSR offsets + indices
     out = {}
-    # moment_kernel<9> builds velocity-A and pressure-A in one pass over the rows
-    out["moment_kernel<9>"] = (16 * nf + 4 * k + pos_f + pos_w + pos_w + 2 * (81 * s * nf + 2 * s * nf + 4 * nf))
-    out["laplacian_kernel"] = 16 * nf + 4 * k + 2 * (pos_f + pos_w) + 81 * s * nf + 3 * s * nf
-    out["ppe_kernel"] = (16 * nf + 4 * k + 2 * (pos_f + pos_w) + pos_w + 2 * 81 * s * nf + 4 * nf
-                         + (4 + s) * (nf + kf) + 3 * s * nf + 4 * (nf + 1))
-    out["gradient_kernel"] = 16 * nf + 4 * k + pos_f + pos_w + pos_w + s * nf + 81 * s * nf + 3 * s * nf + 4 * nf
-    out["shifting_kernel"] = 16 * nf + 4 * k + pos_f + pos_w + pos_w + 4 * nf + 3 * s * nf
-    out["smooth_kernel"] = 8 * nf + 4 * kf + pos_f + 3 * s * nf + 4 * nf + 3 * s * nf
-    out["classify_kernel"] = 16 * nf + 4 * k + pos_f + pos_w + pos_w + 4 * nf
-    out["expand_kernel"] = 8 * nf + 4 * kf + pos_f + 4 * nf
-    # count + write, averaged over the fluid and wall tables
-    out["csr_kernel<false>"] = (2 * pos_f + pos_w + 2 * 8 * c + 2 * 4 * nf + 4 * (nf + nw) + 2 * 4 * nf) // 2
-    out["csr_kernel<true>"] = (2 * pos_f + pos_w + 2 * 8 * c + 2 * 4 * nf + 4 * (nf + nw) + 2 * 4 * nf + 4 * k) // 2
-    out["update_kernel"] = nf * (2 * 3 * s + 2 * 3 * s + 3 * 3 * s + 4)
-    out["anti_penetration_kernel"] = 8 * nf + 4 * kw + 6 * s * nw + 2 * 6 * s * nf
-    out["copy_kernel"] = 6 * s * nf
+    moment_kind_out = (81 * s + 2 * s + 4) * nf  # inverse, trace, regularisation, info
+    moment_in = rows + pos_f + 2 * pos_w  # wall positions + normals
+    out["moment_a_kernel<V,P>"] = moment_in + 2 * moment_kind_out
+    out["moment_a_kernel<V>"] = out["moment_a_kernel<P>"] = moment_in + moment_kind_out
+    out["laplacian_kernel"] = rows + 2 * pos_f + 2 * pos_w + 81 * s * nf + 3 * s * nf
+    ppe = (rows + 2 * pos_f + 4 * nf + 3 * pos_w + 2 * 81 * s * nf
+           + 4 * (nf + 1) + (4 + s) * (nf + kf) + 3 * s * nf)
+    for name in ("ppe_kernel", "ppe_lanes_kernel<4>", "ppe_lanes_kernel<8>", "ppe_lanes_kernel<16>"):
+        out[name] = ppe
+    out["gradient_shifting_kernel"] = (rows + 4 * nf + pos_f + 3 * s * nf + 2 * pos_w + 81 * s * nf
+                                       + 6 * s * nf)
+    out["update_anti_penetration_kernel"] = (4 * (nf + 1) + 4 * kw + 4 * nf + 2 * pos_f + 3 * pos_f
+                                             + 2 * pos_w + 2 * pos_f)
+    out["smooth_kernel"] = 4 * (nf + 1) + 4 * kf + 2 * pos_f + 4 * nf + pos_f
+    out["copy_kernel"] = 2 * pos_f
+    out["classify_kernel"] = rows + pos_f + 2 * pos_w + 4 * nf
+    out["expand_kernel"] = 4 * (nf + 1) + 4 * kf + 8 * nf
+    count_fluid = 2 * pos_f + 8 * c + 4 * nf + 4 * nf
+    count_wall = pos_f + pos_w + 8 * c + 4 * nw + 4 * nf
+    out["csr_kernel<false>"] = (count_fluid + count_wall) // 2
+    out["csr_kernel<true>"] = (count_fluid + count_wall + 8 * nf + 4 * k) // 2
     return out

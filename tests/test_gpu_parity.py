@@ -238,6 +238,63 @@ def test_full_step_matches_oracle(pkg, device_api, ctx, oracle, name, kw):
             assert e < 1e-7, (comp, e)
 
 
+KNOB_VARIANTS = [(0, 0), (0, 1), (1, 0), (1, 1), (1, 2), (1, 3)]
+
+
+@pytest.mark.parametrize("knob,value", KNOB_VARIANTS, ids=[f"knob{k}={v}" for k, v in KNOB_VARIANTS])
+def test_launch_variants_match_oracle(pkg, device_api, oracle, knob, value):
+    """Every launch-shape variant (lsmps_knob) computes the oracle's moments
+    and PPE system: splash case, so Dirichlet rows and Splash particles are
+    in it."""
+    case = pkg.cases.CASES["splash"](nx=40, ny=10, nz=40, l0=0.0025)
+    p = case.params
+    dev, host = both(pkg, device_api, case)
+    c = device_api.Context(0)
+    try:
+        c.set_knob(knob, value)
+        assert c.knob(knob) == value
+        c.build_neighbor_lists(dev, p)
+        c.classify_surface(dev, p)
+        c.prepare_moments(dev, p, [0, 1])
+        c.provision(dev, p)
+        c.assemble_ppe(dev, p)
+    finally:
+        c.close()
+    assert oracle.build_neighbor_lists(host, p)[0] == 0
+    assert oracle.classify_surface(host, p) == 0
+    assert np.array_equal(dev.numpy("fluid")["surface_type"], host.fluid["surface_type"])
+    for kind in (0, 1):
+        assert oracle.prepare_moment(host, p, kind) == 0
+        gm = {k: dev.alloc.to_numpy(v) for k, v in dev.moments[kind].items()}
+        hm = host.moments[kind]
+        assert np.array_equal(gm["info"], hm["info"])
+        ok = hm["info"] == 0
+        gi = gm["inverse_matrices"].reshape(-1, 81)[ok]
+        hi = hm["inverse_matrices"].reshape(-1, 81)[ok]
+        assert (np.max(np.abs(gi - hi), axis=1) / np.max(np.abs(hi), axis=1)).max() < 1e-7
+    oracle.provision(host, p)
+    oracle.assemble_ppe(host, p)
+    g = dev.numpy("ppe")
+    nnz = int(host.ppe["row_offsets"][-1])
+    assert np.array_equal(g["row_offsets"], host.ppe["row_offsets"])
+    assert np.array_equal(g["col_indices"][:nnz], host.ppe["col_indices"][:nnz])
+    for k in ("values", "rhs", "divergence", "pressure_laplacian"):
+        a, b = (g[k][:nnz], host.ppe[k][:nnz]) if k == "values" else (g[k], host.ppe[k])
+        assert rel_err(a, b) < 1e-7, k
+
+
+def test_knob_arguments_checked(device_api):
+    c = device_api.Context(0)
+    try:
+        with pytest.raises(device_api.LsmpsError):
+            c.set_knob(1, 4)
+        with pytest.raises(device_api.LsmpsError):
+            c.set_knob(7, 0)
+        assert c.knob(0) == 1 and c.knob(1) == 2
+    finally:
+        c.close()
+
+
 def test_deterministic_repeat(pkg, device_api, ctx):
     case = pkg.cases.dam_break(nx=16, ny=8, nz=16, l0=0.005)
     outs = []
