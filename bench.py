@@ -34,10 +34,13 @@ sys.path.insert(0, ROOT)
 import __graft_entry__ as graft_entry  # noqa: E402
 
 METRIC = "particles/s per LSMPS step, mixed vs plain FP64 on 1 B200 at stated error; HBM %"
+KNOB_NAMES = {0: "moment_occupancy", 1: "ppe_lanes"}
 WORKLOADS = {
     "splash": ("splash", {}, "splash dam break 200x50x200 (2M fluid, l0=0.0025 m, 5% splash, 3 wall layers)"),
     "dam_break": ("dam_break", {}, "dam break 100x50x100 (500k fluid, l0=0.005 m, jitter 0.05 l0, 3 wall layers)"),
     "hydrostatic": ("hydrostatic", {}, "hydrostatic box 20^3 (8k fluid, l0=0.01 m, 3 wall layers)"),
+    "batched": ("batched", {}, "64 independent boxes, fluid counts log-uniform in [8k, 200k] (seed 7), hydrostatic "
+                               "or dam-break layout by seeded coin flip, 3 wall layers, l0=0.005 m"),
 }
 
 
@@ -50,6 +53,10 @@ def parse_args():
     ap.add_argument("--workload", choices=list(WORKLOADS), default="splash")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--kappa-threshold", type=float, default=None,
+                    help="mixed form: condition-estimate threshold of the FP64 route (library default if omitted)")
+    ap.add_argument("--precision", choices=["both", "plain", "mixed"], default="both",
+                    help="forms to time; the last one timed is the headline (mixed when both)")
     return ap.parse_args()
 
 
@@ -173,6 +180,8 @@ def run_ours(args, world, rank, local):
     with torch.cuda.stream(stream):
         dev = api.device_buffers(case, device=device)
         ctx = api.Context(local)
+        if args.kappa_threshold is not None:
+            ctx.set_condition_threshold(args.kappa_threshold)
         ctx.reserve(case.n_fluid, case.n_wall, case.n_cells)
         state = dev.step_state(p)
 
@@ -199,25 +208,43 @@ def run_ours(args, world, rank, local):
             return e0.elapsed_time(e1) / k, ctx.launch_count - launches0
 
         results = {}
-        forms = [("plain", pkg.abi.PRECISION_PLAIN)]
+        forms = [("plain", pkg.abi.PRECISION_PLAIN), ("mixed", pkg.abi.PRECISION_MIXED)]
+        if args.precision != "both":
+            forms = [f for f in forms if f[0] == args.precision]
         for form, prec in forms:
             ctx.set_precision(prec)
+            ctx.reserve(case.n_fluid, case.n_wall, case.n_cells)
             reset()
+            fallbacks0 = ctx.fp64_fallbacks
             for _ in range(args.warmup):
                 ctx.step(dev, p, state)
+            # the project autotuner picks the launch-shape knobs on this state
+            # (it runs only stages that are pure functions of the state)
+            tuned = ctx.autotune(dev, p, repeats=3, state=state)
+            ctx.synchronize()
             with ClockSampler(local) as sampler:
                 ms, launches = timed_steps(args.steps)
             clocks = sampler.summary()
             ms_max = max_over_ranks(world, ms, device)
             kf = int(dev.fluid_neighbors["offsets"][case.n_fluid].item())
             kw_ = int(dev.wall_neighbors["offsets"][case.n_fluid].item())
+            fallbacks = (ctx.fp64_fallbacks - fallbacks0) / max(1, args.warmup + args.steps)
             # per-kernel device time of the same steps (events around each launch)
             ctx.set_profiling(True)
             for _ in range(2):
                 ctx.step(dev, p, state)
             prof = ctx.profile_report()
             ctx.set_profiling(False)
-            results[form] = dict(ms=ms_max, launches=launches // args.steps, clocks=clocks, kf=kf, kw=kw_, prof=prof)
+            results[form] = dict(ms=ms_max, launches=launches // args.steps, clocks=clocks, kf=kf, kw=kw_, prof=prof,
+                                 fallbacks=fallbacks,
+                                 autotune={KNOB_NAMES[k]: v for k, (v, _) in tuned.items()})
+
+        # error of the mixed step against the plain FP64 step from the same
+        # state, at full size (the parity tests pin the plain form to the FP64
+        # oracle)
+        error = None
+        if len(forms) == 2:
+            error = mixed_error(pkg, torch, ctx, dev, case, p, state, reset)
 
         # end to end through the C ABI with host buffers: pinned inputs copied
         # in and the step's particle state copied back inside the timed region
@@ -261,6 +288,7 @@ def run_ours(args, world, rank, local):
 
     head_form = forms[-1][0]
     h = results[head_form]
+    peak_s, _ = peaks()
     peak, peak_kind = peaks()
     kb = roofline.kernel_bytes(case.n_fluid, case.n_wall, h["kf"], h["kw"], case.n_cells)
     top = max(h["prof"], key=lambda e: e[1]) if h["prof"] else ("", 0.0, 1)
@@ -281,7 +309,7 @@ def run_ours(args, world, rank, local):
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f64" if head_form == "plain" else "f32+f64",
+        "dtype": "f64" if head_form == "plain" else "f32+f64 (mixed)",
         "data": "synthetic",
         "config": {
             "workload": desc,
@@ -307,12 +335,164 @@ def run_ours(args, world, rank, local):
             "step_bytes_model": step_b,
             "step_hbm_frac": step_b / (h["ms"] * 1e-3) / 1e9 / peak,
         },
+        "forms": {
+            f: {"value": world * case.n_fluid / (r["ms"] * 1e-3), "ms_per_step": r["ms"],
+                "fp64_fallbacks_per_step": r["fallbacks"], "autotune": r["autotune"],
+                "step_hbm_frac": roofline.step_bytes(case.n_fluid, case.n_wall, r["kf"], r["kw"], case.n_cells)
+                / (r["ms"] * 1e-3) / 1e9 / peak_s,
+                "kernels": [{"name": n, "ms_per_step": ms / 2, "launches_per_step": c // 2}
+                            for n, ms, c in r["prof"]]}
+            for f, r in results.items()},
+        "mixed_over_plain": (results["plain"]["ms"] / results["mixed"]["ms"]) if len(results) == 2 else None,
+        "error": error,
         "kernels": [{"name": n, "ms_per_step": ms / 2, "launches_per_step": c // 2} for n, ms, c in h["prof"]],
         "gpu_launches": h["launches"] * args.steps,
         "clocks": h["clocks"],
         "e2e": e2e,
     }
     return out, case
+
+
+def run_batched(args, world, rank, local):
+    """64 independent boxes: one captured CUDA graph of the mixed step over 8
+    worker streams (the project autotuner sets each worker's knobs) against
+    the same boxes stepped one after another in the plain FP64 form without a
+    graph."""
+    import torch
+
+    pkg = graft_entry.load_package()
+    from importlib import import_module
+
+    import_module("lsmps3d_b200.build").build_all()
+    api = import_module("lsmps3d_b200.api")
+    device = torch.device(f"cuda:{local}")
+    torch.cuda.set_device(device)
+    boxes = pkg.cases.batched_boxes()
+    setup_stream = torch.cuda.Stream(device)
+    bufs = []
+    with torch.cuda.stream(setup_stream):
+        ctx = api.Context(local)
+        for case in boxes:
+            b = api.device_buffers(case, device=device)
+            ctx.build_neighbor_lists(b, case.params)
+            ctx.classify_surface(b, case.params)
+            bufs.append((b, case.params, b.step_state(case.params)))
+        # sequential plain FP64 steps, one box after another, no graph
+        ctx.set_precision(pkg.abi.PRECISION_PLAIN)
+        ctx.set_synchronous(False)
+        ctx.reserve(max(c.n_fluid for c in boxes), max(c.n_wall for c in boxes), max(c.n_cells for c in boxes))
+        for b, p, st in bufs:
+            ctx.step(b, p, st)
+        ctx.synchronize()
+        torch.cuda.synchronize(device)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(setup_stream)
+        for b, p, st in bufs:
+            ctx.step(b, p, st)
+        e1.record(setup_stream)
+        ctx.synchronize()
+        torch.cuda.synchronize(device)
+        seq_ms = e0.elapsed_time(e1)
+        ctx.close()
+    n_total = sum(c.n_fluid for c in boxes)
+    batch = api.Batch(local, streams=8)
+    for b, p, _ in bufs:
+        batch.add(b, p)
+    batch.capture(precision=pkg.abi.PRECISION_MIXED, autotune_repeats=2)
+    stream = torch.cuda.ExternalStream(batch.stream, device=device)
+    for _ in range(args.warmup):
+        batch.launch()
+    batch.synchronize()
+    barrier(world)
+    torch.cuda.synchronize(device)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as sampler:
+        e0.record(stream)
+        for _ in range(args.steps):
+            batch.launch()
+        e1.record(stream)
+        batch.synchronize()
+        torch.cuda.synchronize(device)
+    ms = max_over_ranks(world, e0.elapsed_time(e1) / args.steps, device)
+    batch.close()
+    value = world * n_total / (ms * 1e-3)
+    return {
+        "metric": METRIC,
+        "value": value,
+        "unit": "particles/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32+f64 (mixed)",
+        "data": "synthetic",
+        "config": {"workload": WORKLOADS["batched"][2], "boxes": len(boxes), "n_fluid_total": n_total,
+                   "n_wall_total": sum(c.n_wall for c in boxes), "graph_streams": 8,
+                   "precision": "mixed (graph) vs plain (sequential)",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "sequential_plain": {"value": n_total / (seq_ms * 1e-3), "ms_per_pass": seq_ms,
+                             "what": "the same 64 boxes stepped one after another with lsmps_step in the plain "
+                                     "FP64 form, no graph"},
+        "graph_over_sequential": seq_ms / ms,
+        "clocks": sampler.summary(),
+        "e2e": None,
+        "gpu_launches": None,
+    }
+
+
+def mixed_error(pkg, torch, ctx, dev, case, p, state, reset):
+    """One plain and one mixed step from the same state; row-normwise PPE
+    coefficient error and normwise errors of the other outputs, on the
+    device."""
+    def run(prec):
+        ctx.set_precision(prec)
+        reset()
+        ctx.step(dev, p, state)
+        ctx.synchronize()
+        out = {k: v.clone() for k, v in dev.ppe.items() if k in ("values", "rhs", "divergence", "pressure_laplacian")}
+        out["row_offsets"] = dev.ppe["row_offsets"].clone()
+        for k in ("x", "y", "z", "vx", "vy", "vz", "pressure"):
+            out["f_" + k] = dev.fluid[k].clone()
+        for k in ("x", "y", "z"):
+            out["g_" + k] = dev.pressure_gradient[k].clone()
+            out["l_" + k] = dev.velocity_laplacian[k].clone()
+        return out
+
+    ref = run(pkg.abi.PRECISION_PLAIN)
+    mix = run(pkg.abi.PRECISION_MIXED)
+    ctx.set_precision(pkg.abi.PRECISION_MIXED)
+    off = ref["row_offsets"].long()
+    n = off.numel() - 1
+    nnz = int(off[-1].item())
+    lengths = off[1:] - off[:-1]
+    row = torch.repeat_interleave(torch.arange(n, device=off.device), lengths)
+    d = (mix["values"][:nnz] - ref["values"][:nnz]).abs()
+    a = ref["values"][:nnz].abs()
+    dmax = torch.zeros(n, dtype=d.dtype, device=d.device).scatter_reduce(0, row, d, "amax")
+    amax = torch.zeros(n, dtype=d.dtype, device=d.device).scatter_reduce(0, row, a, "amax")
+    coef = float(torch.where(amax > 0, dmax / torch.where(amax > 0, amax, torch.ones_like(amax)), dmax).max())
+
+    def norm_err(keys):
+        num = max(float((mix[k] - ref[k]).abs().max()) for k in keys)
+        den = max(float(ref[k].abs().max()) for k in keys)
+        return num / den if den > 0 else num
+
+    del row, d, a
+    return {
+        "reference": "this library's plain FP64 step from the same state (the plain form is held to the FP64 "
+                     "oracle within 1e-9 by the parity tests)",
+        "ppe_coefficients_max_rel_rowwise": coef,
+        "ppe_rhs_rel": norm_err(["rhs"]),
+        "ppe_divergence_rel": norm_err(["divergence"]),
+        "pressure_gradient_rel": norm_err(["g_x", "g_y", "g_z"]),
+        "velocity_laplacian_rel": norm_err(["l_x", "l_y", "l_z"]),
+        "velocity_rel": norm_err(["f_vx", "f_vy", "f_vz"]),
+        "position_rel": norm_err(["f_x", "f_y", "f_z"]),
+        "target": "PPE coefficients <= 1e-5 (row-normwise)",
+    }
 
 
 def cpu_baseline(case_kind: str):
@@ -354,6 +534,8 @@ def run_reference(args, world, rank, local):
 
     kind, kw, desc = WORKLOADS[args.workload]
     base = {"metric": METRIC, "unit": "particles/s", "impl": "reference", "higher_is_better": True}
+    if kind == "batched":
+        return dict(impl="reference", unavailable="the reference steps one box per process; it has no batched form")
     if not ref_mod.available():
         return dict(impl="reference", unavailable="oracle/_ref/libref_lsmps.so was not built (needs the reference sources)")
     case = pkg.cases.CASES[kind](**kw)
@@ -398,6 +580,15 @@ def main():
     if args.impl == "reference":
         if rank == 0:
             print(json.dumps(run_reference(args, world, rank, local)), flush=True)
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+        return
+    if args.workload == "batched":
+        out = run_batched(args, world, rank, local)
+        if rank == 0:
+            print(json.dumps(out), flush=True)
         if world > 1:
             import torch.distributed as dist
 

@@ -281,9 +281,18 @@ lsmps_status lsmps_ctx_synchronize(lsmps_ctx* ctx);
 uint64_t lsmps_ctx_required(lsmps_ctx* ctx);
 /* Number of kernel launches this context has queued since creation. */
 uint64_t lsmps_ctx_launch_count(lsmps_ctx* ctx);
+/* Mixed form (no counterpart in the reference, which has one precision):
+ * moment matrices whose FP32 Cholesky factor failed or whose condition
+ * estimate (max L_ii / min L_ii)^2 exceeded the threshold are factorised in
+ * FP64 instead.  The threshold defaults to 1e4 (one FP64 refinement of an
+ * FP32 factor leaves a relative error of about (kappa 2^-24)^2: ~4e-7 at 1e4,
+ * ~4e-3 at 1e6); the count accumulates over the context's life (read back at
+ * each status fold). */
+lsmps_status lsmps_ctx_set_condition_threshold(lsmps_ctx* ctx, double threshold);
+uint64_t lsmps_ctx_fp64_fallbacks(lsmps_ctx* ctx);
 /* Launch-shape knobs (no counterpart in the reference, whose kernels all use
  * one thread per particle in 128-thread blocks).  Values are indices into each
- * knob's variant list. */
+ * knob's variant list; lsmps_autotune() picks them by timing. */
 typedef enum lsmps_knob {
   /* moment kernel register budget: 0 = compiler's choice, 1 = capped for 8
    * blocks per SM (default) */
@@ -297,6 +306,16 @@ lsmps_status lsmps_ctx_set_knob(lsmps_ctx* ctx, int knob, int value);
 int lsmps_ctx_knob(lsmps_ctx* ctx, int knob);
 /* Number of variants of a knob (0 for an unknown knob). */
 int lsmps_knob_variants(int knob);
+/* Project autotuner (no counterpart in the reference): times every variant of
+ * every knob on the caller's state with CUDA events (`repeats` timed launches
+ * after one untimed launch each) and leaves the fastest set on the context.
+ * Only stages that are pure functions of the state are run (the moment stage
+ * and the PPE assembly), so the simulation does not advance; the state's
+ * temporary velocity should hold u* (it does after any lsmps_step).  If
+ * best_ms is not NULL it receives LSMPS_KNOB_COUNT mean times (ms) of the
+ * chosen variants.  Synchronous. */
+lsmps_status lsmps_autotune(lsmps_ctx* ctx, const lsmps_params* params, const lsmps_step_state* state,
+                            int repeats, double* best_ms);
 /* Per-kernel device timing (no counterpart in the reference, which has no
  * tracing): while on, every launch is bracketed by CUDA events.  Turning it
  * on clears the records. */
@@ -481,6 +500,78 @@ lsmps_status lsmps_pressure_correction(lsmps_ctx* ctx, const lsmps_fluid* fluid,
  * `pressure` -> neighbour rebuild -> surface labels.  Uses the context's
  * precision mode. */
 lsmps_status lsmps_step(lsmps_ctx* ctx, const lsmps_params* params, const lsmps_step_state* state);
+
+/* ------------------------------------------------------------------------- */
+/* Batched boxes in one CUDA graph (no counterpart in the reference)          */
+/* ------------------------------------------------------------------------- */
+/* Many independent boxes (each its own params and step state, of any size)
+ * stepped by one captured CUDA graph.  The batch owns `streams` worker
+ * streams, each with its own context; box b runs on stream b mod streams, so
+ * boxes on different streams overlap on the GPU.
+ *   create -> add every box -> capture(precision) -> launch (repeatedly) ->
+ *   synchronize (folds every worker context's device status) -> destroy.
+ * capture reserves each worker context for its largest box, optionally runs
+ * lsmps_autotune on that box (autotune_repeats > 0; 0 keeps the defaults),
+ * then records one lsmps_step per box between a fork and a join on the
+ * batch's origin stream.  Each launch advances every box by one step; the
+ * boxes' buffers must stay valid and keep their sizes while the graph
+ * exists. */
+typedef struct lsmps_batch lsmps_batch;
+lsmps_status lsmps_batch_create(int device, int streams, lsmps_batch** out);
+void lsmps_batch_destroy(lsmps_batch* batch);
+lsmps_status lsmps_batch_add(lsmps_batch* batch, const lsmps_params* params, const lsmps_step_state* state);
+int lsmps_batch_size(lsmps_batch* batch);
+lsmps_status lsmps_batch_capture(lsmps_batch* batch, int precision, int autotune_repeats);
+/* stream: where the graph is launched (NULL: the batch's origin stream). */
+lsmps_status lsmps_batch_launch(lsmps_batch* batch, void* stream);
+lsmps_status lsmps_batch_synchronize(lsmps_batch* batch);
+void* lsmps_batch_stream(lsmps_batch* batch);
+const char* lsmps_batch_last_error(lsmps_batch* batch);
+
+/* ------------------------------------------------------------------------- */
+/* Differentiable operators (no counterpart in the reference)                */
+/* ------------------------------------------------------------------------- */
+/* Outputs of lsmps_operators_forward, or (to lsmps_operators_backward) the
+ * cotangents dL/d(output) of a loss L.  Per fluid particle, over its fluid CSR
+ * row, with the fluid-only Type-A moment matrix (kind FLUID_ONLY_A):
+ *   grad_*      LSMPS gradient of the scalar field f
+ *   laplacian   LSMPS Laplacian of f (2/r_e^2 times rows 3..5)
+ *   divergence  LSMPS divergence of the vector field v
+ *   ppe_*       optional fluid-only PPE rows in the reference's layout
+ *               (diagonal first, then the CSR row; ppe_matrix.cu:243-370
+ *               without wall terms): row_offsets[count + 1], col_indices and
+ *               values[count + K]; ppe_rhs = divergence / dt.
+ * Any pointer may be NULL: the output is not written (forward) or its
+ * cotangent is zero (backward; ppe_row_offsets / ppe_col_indices are not
+ * read). */
+typedef struct lsmps_operator_out {
+  size_t count;
+  double* grad_x;
+  double* grad_y;
+  double* grad_z;
+  double* laplacian;
+  double* divergence;
+  int32_t* ppe_row_offsets;
+  int32_t* ppe_col_indices;
+  double* ppe_values;
+  double* ppe_rhs;
+} lsmps_operator_out;
+
+/* fluid: positions (x, y, z, count; other fields unused); fn: its fluid CSR
+ * (the topology is an input: it is held fixed under differentiation).  If
+ * inverse_out is not NULL it receives the count x 81 inverses (column-major),
+ * which lsmps_operators_backward can reuse instead of recomputing them. */
+lsmps_status lsmps_operators_forward(lsmps_ctx* ctx, const lsmps_fluid* fluid, const lsmps_csr* fn,
+                                     const lsmps_params* params, const double* f, const lsmps_vector* v,
+                                     const lsmps_operator_out* out, double* inverse_out);
+/* Gradients of L with respect to f (f_bar), v (v_bar) and the positions
+ * (x_bar), each optional (NULL: not computed) and overwritten.  inverse: the
+ * forward's inverse_out, or NULL to recompute the inverses from the positions
+ * (the memory-lean choice: nothing of the forward has to be kept). */
+lsmps_status lsmps_operators_backward(lsmps_ctx* ctx, const lsmps_fluid* fluid, const lsmps_csr* fn,
+                                      const lsmps_params* params, const double* f, const lsmps_vector* v,
+                                      const lsmps_operator_out* cotangent, const double* inverse, double* f_bar,
+                                      const lsmps_vector* v_bar, const lsmps_vector* x_bar);
 
 #ifdef __cplusplus
 }

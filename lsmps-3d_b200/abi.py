@@ -172,6 +172,14 @@ class Params(Structure):
     ]
 
 
+class OperatorOut(Structure):
+    _fields_ = [("count", c_size_t)] + [
+        (n, c_void_p)
+        for n in ("grad_x", "grad_y", "grad_z", "laplacian", "divergence", "ppe_row_offsets", "ppe_col_indices",
+                  "ppe_values", "ppe_rhs")
+    ]
+
+
 class StepState(Structure):
     _fields_ = [
         ("fluid", Fluid),
@@ -240,9 +248,12 @@ _SIGNATURES = {
     "lsmps_ctx_required": (c_uint64, [c_void_p]),
     "lsmps_ctx_launch_count": (c_uint64, [c_void_p]),
     "lsmps_ctx_set_profiling": (c_int, [c_void_p, c_int]),
+    "lsmps_ctx_set_condition_threshold": (c_int, [c_void_p, c_double]),
+    "lsmps_ctx_fp64_fallbacks": (c_uint64, [c_void_p]),
     "lsmps_ctx_set_knob": (c_int, [c_void_p, c_int, c_int]),
     "lsmps_ctx_knob": (c_int, [c_void_p, c_int]),
     "lsmps_knob_variants": (c_int, [c_int]),
+    "lsmps_autotune": (c_int, [c_void_p, P(Params), P(StepState), c_int, P(c_double)]),
     "lsmps_ctx_profile_report": (c_int, [c_void_p, ctypes.c_char_p, c_size_t, P(c_double), P(c_uint64), c_int]),
     "lsmps_ctx_last_error": (c_char_p, [c_void_p]),
     "lsmps_status_string": (c_char_p, [c_int]),
@@ -287,6 +298,19 @@ _SIGNATURES = {
         ],
     ),
     "lsmps_step": (c_int, [c_void_p, P(Params), P(StepState)]),
+    "lsmps_batch_create": (c_int, [c_int, c_int, P(c_void_p)]),
+    "lsmps_batch_destroy": (None, [c_void_p]),
+    "lsmps_batch_add": (c_int, [c_void_p, P(Params), P(StepState)]),
+    "lsmps_batch_size": (c_int, [c_void_p]),
+    "lsmps_batch_capture": (c_int, [c_void_p, c_int, c_int]),
+    "lsmps_batch_launch": (c_int, [c_void_p, c_void_p]),
+    "lsmps_batch_synchronize": (c_int, [c_void_p]),
+    "lsmps_batch_stream": (c_void_p, [c_void_p]),
+    "lsmps_batch_last_error": (c_char_p, [c_void_p]),
+    "lsmps_operators_forward": (c_int, [c_void_p, P(Fluid), P(Csr), P(Params), c_void_p, P(Vector), P(OperatorOut),
+                                        c_void_p]),
+    "lsmps_operators_backward": (c_int, [c_void_p, P(Fluid), P(Csr), P(Params), c_void_p, P(Vector), P(OperatorOut),
+                                         c_void_p, c_void_p, P(Vector), P(Vector)]),
 }
 
 

@@ -98,6 +98,24 @@ class Context:
     def knob(self, knob: int) -> int:
         return int(_lib.lsmps_ctx_knob(self.h, knob))
 
+    def autotune(self, b: StepBuffers, params: abi.Params, repeats: int = 3,
+                 state: abi.StepState | None = None) -> dict[int, tuple[int, float]]:
+        """lsmps_autotune on this state; returns {knob: (chosen variant, mean ms)}."""
+        s = state if state is not None else b.step_state(params)
+        ms = (ctypes.c_double * abi.KNOB_COUNT)()
+        self.check(_lib.lsmps_autotune(self.h, r(params), r(s), repeats, ms))
+        return {k: (self.knob(k), float(ms[k])) for k in range(abi.KNOB_COUNT)}
+
+    def set_condition_threshold(self, threshold: float) -> None:
+        """Mixed form: condition estimate above which a moment matrix is
+        factorised in FP64 (default 1e4)."""
+        self.check(_lib.lsmps_ctx_set_condition_threshold(self.h, float(threshold)))
+
+    @property
+    def fp64_fallbacks(self) -> int:
+        """Mixed form: moment matrices factorised in FP64 so far."""
+        return int(_lib.lsmps_ctx_fp64_fallbacks(self.h))
+
     def profile_report(self, max_entries: int = 64) -> list[tuple[str, float, int]]:
         """(kernel name, total ms, launches) per kernel since profiling was
         switched on; clears the records."""
@@ -167,6 +185,54 @@ class Context:
     def step(self, b: StepBuffers, params: abi.Params, state: abi.StepState | None = None) -> None:
         s = state if state is not None else b.step_state(params)
         self.check(_lib.lsmps_step(self.h, r(params), r(s)))
+
+
+class Batch:
+    """Independent boxes stepped by one captured CUDA graph (lsmps_batch_*).
+    Keeps the boxes' StepBuffers, params and step states alive while the
+    graph exists."""
+
+    def __init__(self, device: int = 0, streams: int = 8):
+        h = ctypes.c_void_p()
+        st = _lib.lsmps_batch_create(device, streams, ctypes.byref(h))
+        if st != abi.OK:
+            raise LsmpsError(st, "lsmps_batch_create failed")
+        self.h = h
+        self.boxes = []
+
+    def check(self, st: int) -> None:
+        if st != abi.OK:
+            msg = _lib.lsmps_batch_last_error(self.h)
+            raise LsmpsError(st, msg.decode() if msg else "")
+
+    def add(self, b: StepBuffers, params: abi.Params) -> None:
+        state = b.step_state(params)
+        self.boxes.append((b, params, state))
+        self.check(_lib.lsmps_batch_add(self.h, r(params), r(state)))
+
+    def capture(self, precision: int = abi.PRECISION_MIXED, autotune_repeats: int = 0) -> None:
+        self.check(_lib.lsmps_batch_capture(self.h, precision, autotune_repeats))
+
+    def launch(self, stream_handle: int | None = None) -> None:
+        self.check(_lib.lsmps_batch_launch(self.h, ctypes.c_void_p(stream_handle) if stream_handle else None))
+
+    def synchronize(self) -> None:
+        self.check(_lib.lsmps_batch_synchronize(self.h))
+
+    @property
+    def stream(self) -> int:
+        return int(_lib.lsmps_batch_stream(self.h) or 0)
+
+    def close(self):
+        if getattr(self, "h", None):
+            _lib.lsmps_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def device_buffers(case, max_fluid_neighbors: int = 256, max_wall_neighbors: int = 256, device="cuda") -> StepBuffers:

@@ -245,7 +245,7 @@ def splash_dam_break(nx: int = 200, ny: int = 50, nz: int = 200, l0: float = 0.0
     return case
 
 
-def lattice_box(n: int = 64, l0: float = 0.01, jitter: float = 0.1, seed: int = 4, layers: int = 3) -> Case:
+def lattice_box(n: int = 64, l0: float = 0.01, jitter: float = 0.1, seed: int = 40, layers: int = 3) -> Case:
     """n^3 jittered lattice inside a closed-bottom tank (adjoint check case)."""
     fx, fy, fz = fluid_block(n, n, n, l0)
     m = fx.shape[0]
@@ -254,6 +254,28 @@ def lattice_box(n: int = 64, l0: float = 0.01, jitter: float = 0.1, seed: int = 
     walls = _tank_walls_fast(n, n, n + 4, l0, layers)
     return _make_case(f"lattice_{n}^3", l0, fx + d[:, 0], fy + d[:, 1], fz + d[:, 2], walls, n * l0,
                       meta={"jitter": jitter, "seed": seed})
+
+
+def batched_boxes(count: int = 64, seed: int = 7, n_min: int = 8_000, n_max: int = 200_000,
+                  l0: float = 0.005) -> list[Case]:
+    """The batched workload: `count` independent boxes whose fluid counts are
+    drawn log-uniform in [n_min, n_max] (seeded); each box is a hydrostatic
+    cube (side round(N^(1/3))) or a dam-break block (2:1:2, ny =
+    round((N/4)^(1/3))) by a seeded coin flip, with 3 wall layers and
+    r_e = 3.1 l0."""
+    u = uniform01(seed, 2 * count)
+    boxes = []
+    for b in range(count):
+        target = float(np.exp(np.log(n_min) + u[2 * b] * (np.log(n_max) - np.log(n_min))))
+        if u[2 * b + 1] < 0.5:
+            side = max(4, int(round(target ** (1.0 / 3.0))))
+            c = hydrostatic_box(n=side, l0=l0)
+        else:
+            ny = max(2, int(round((target / 4.0) ** (1.0 / 3.0))))
+            c = dam_break(nx=2 * ny, ny=ny, nz=2 * ny, l0=l0, seed=seed * 1000 + b)
+        c.name = f"box{b}_{c.name}"
+        boxes.append(c)
+    return boxes
 
 
 CASES = {

@@ -30,6 +30,8 @@ struct DeviceStatus {
   unsigned int flags;
   unsigned int non_spd;
   unsigned long long required;
+  unsigned int fallbacks;  // mixed form: moment matrices factorised in FP64
+  unsigned int pad;
 };
 
 __device__ __forceinline__ void raise_flag(DeviceStatus* s, unsigned f) { atomicOr(&s->flags, f); }
@@ -115,6 +117,7 @@ struct lsmps_ctx {
   size_t scratch_used = 0;
   unsigned long long launches = 0;
   unsigned long long required = 0;
+  unsigned long long fallbacks = 0;
   std::string last_error;
   // Per-launch CUDA events while profiling is on (lsmps_ctx_set_profiling).
   struct ProfileRecord {
@@ -132,6 +135,28 @@ struct lsmps_ctx {
   double4* pack_wall[3] = {nullptr, nullptr, nullptr};
   size_t pack_fluid_cap = 0;
   size_t pack_wall_cap = 0;
+  // Mixed form (LSMPS_PRECISION_MIXED): per fluid particle the 31 FP64 fluid
+  // moment sums ([31][n]) and the compact FP32 operator rows of the velocity
+  // and pressure inverses ([n][36]: Laplacian row, then rows 0, 1, 2).
+  double* mixed_sums = nullptr;
+  float* mixed_rows[2] = {nullptr, nullptr};
+  double* mixed_rows64[2] = {nullptr, nullptr};  // rows of matrices factorised in FP64
+  uint8_t* mixed_flag[2] = {nullptr, nullptr};   // 1: the particle's rows are in mixed_rows64
+  size_t mixed_cap = 0;
+  // Condition-estimate threshold above which a moment matrix is factorised
+  // in FP64 in the mixed form.  One FP64 refinement of an FP32 factor leaves
+  // a relative error of about (kappa u)^2 (u = 2^-24): ~4e-7 at 1e4, ~4e-3 at
+  // 1e6.
+  double kappa_threshold = 1.0e4;
+  // Operator forward/backward pair (adjoint.cu): fluid-only inverse, its
+  // trace / regularisation / info, and the backward's per-particle stash.
+  double* adj_inverse = nullptr;
+  double* adj_trace = nullptr;
+  double* adj_reg = nullptr;
+  int32_t* adj_info = nullptr;
+  int32_t* adj_count = nullptr;
+  double* adj_stash = nullptr;
+  size_t adj_cap = 0;
 };
 
 namespace lsmps {
@@ -159,6 +184,12 @@ class Scratch {
 // Grow the pack arrays to hold nf fluid and nw wall records (outside stream
 // capture; returns false if that is impossible).
 bool ensure_packs(lsmps_ctx* ctx, size_t nf, size_t nw);
+// Grow the mixed-form arrays to nf fluid particles (outside stream capture).
+bool ensure_mixed(lsmps_ctx* ctx, size_t nf);
+void free_mixed(lsmps_ctx* ctx);
+// Grow / free the operator pair's scratch (adjoint.cu).
+bool ensure_adjoint(lsmps_ctx* ctx, size_t n);
+void free_adjoint(lsmps_ctx* ctx);
 
 lsmps_status fail(lsmps_ctx* ctx, lsmps_status st, const char* what);
 lsmps_status check_launch(lsmps_ctx* ctx, const char* what);

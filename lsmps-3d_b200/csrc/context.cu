@@ -2,7 +2,7 @@
 #include <cstring>
 #include <new>
 
-#include "common.cuh"
+#include "impl.cuh"
 
 namespace lsmps {
 
@@ -23,6 +23,42 @@ bool Scratch::reserve(size_t bytes) {
     return false;
   }
   ctx_->scratch_bytes = grown;
+  return true;
+}
+
+void free_mixed(lsmps_ctx* ctx) {
+  if (ctx->mixed_sums) cudaFree(ctx->mixed_sums);
+  ctx->mixed_sums = nullptr;
+  for (int k = 0; k < 2; ++k) {
+    if (ctx->mixed_rows[k]) cudaFree(ctx->mixed_rows[k]);
+    if (ctx->mixed_rows64[k]) cudaFree(ctx->mixed_rows64[k]);
+    if (ctx->mixed_flag[k]) cudaFree(ctx->mixed_flag[k]);
+    ctx->mixed_rows[k] = nullptr;
+    ctx->mixed_rows64[k] = nullptr;
+    ctx->mixed_flag[k] = nullptr;
+  }
+  ctx->mixed_cap = 0;
+}
+
+bool ensure_mixed(lsmps_ctx* ctx, size_t nf) {
+  if (nf <= ctx->mixed_cap) return true;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  cudaStreamIsCapturing(ctx->stream, &cap);
+  if (cap != cudaStreamCaptureStatusNone) return false;
+  cudaStreamSynchronize(ctx->stream);
+  free_mixed(ctx);
+  bool ok = cudaMalloc(&ctx->mixed_sums, nf * 31 * sizeof(double)) == cudaSuccess;
+  for (int k = 0; k < 2 && ok; ++k) {
+    ok = cudaMalloc(&ctx->mixed_rows[k], nf * 36 * sizeof(float)) == cudaSuccess &&
+         cudaMalloc(&ctx->mixed_rows64[k], nf * 36 * sizeof(double)) == cudaSuccess &&
+         cudaMalloc(&ctx->mixed_flag[k], nf) == cudaSuccess;
+  }
+  if (!ok) {
+    cudaGetLastError();
+    free_mixed(ctx);
+    return false;
+  }
+  ctx->mixed_cap = nf;
   return true;
 }
 
@@ -92,6 +128,7 @@ lsmps_status fold_status(lsmps_ctx* ctx) {
   }
   const DeviceStatus s = *ctx->h_status;
   cudaMemsetAsync(ctx->d_status, 0, sizeof(DeviceStatus), ctx->stream);
+  ctx->fallbacks += s.fallbacks;
   if (s.flags & kFlagNonFinite) {
     ctx->last_error = "non-finite particle coordinate";
     return LSMPS_NON_FINITE;
@@ -174,6 +211,8 @@ void lsmps_ctx_destroy(lsmps_ctx* ctx) {
     if (p) cudaFree(p);
   for (auto p : ctx->pack_wall)
     if (p) cudaFree(p);
+  free_mixed(ctx);
+  free_adjoint(ctx);
   if (ctx->d_status) cudaFree(ctx->d_status);
   if (ctx->h_status) cudaFreeHost(ctx->h_status);
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
@@ -209,9 +248,14 @@ lsmps_status lsmps_ctx_reserve(lsmps_ctx* ctx, size_t fluid_capacity, size_t wal
   size_t need = cell_list_scratch_bytes(n, cell_capacity);
   const size_t s2 = scan_scratch_bytes(fluid_capacity + 1) + 4096;
   if (s2 > need) need = s2;
+  // what lsmps_step's neighbour rebuild takes, so that a step can be captured
+  const size_t s3 = neighbor_scratch_bytes(fluid_capacity, wall_capacity, cell_capacity);
+  if (s3 > need) need = s3;
   Scratch s(ctx);
   if (!s.reserve(need)) return fail(ctx, LSMPS_CUDA_ERROR, "scratch allocation failed");
   if (!ensure_packs(ctx, fluid_capacity, wall_capacity)) return fail(ctx, LSMPS_CUDA_ERROR, "pack allocation failed");
+  if (ctx->precision == LSMPS_PRECISION_MIXED && !ensure_mixed(ctx, fluid_capacity))
+    return fail(ctx, LSMPS_CUDA_ERROR, "mixed-form allocation failed");
   return LSMPS_OK;
 }
 
@@ -223,6 +267,14 @@ lsmps_status lsmps_ctx_synchronize(lsmps_ctx* ctx) {
 }
 
 uint64_t lsmps_ctx_required(lsmps_ctx* ctx) { return ctx ? ctx->required : 0; }
+
+uint64_t lsmps_ctx_fp64_fallbacks(lsmps_ctx* ctx) { return ctx ? ctx->fallbacks : 0; }
+
+lsmps_status lsmps_ctx_set_condition_threshold(lsmps_ctx* ctx, double threshold) {
+  if (!ctx || !(threshold >= 1.0)) return LSMPS_INVALID_ARGUMENT;
+  ctx->kappa_threshold = threshold;
+  return LSMPS_OK;
+}
 
 int lsmps_knob_variants(int knob) {
   switch (knob) {

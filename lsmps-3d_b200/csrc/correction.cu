@@ -4,6 +4,7 @@
 // LSMPS pressure gradient, particle shifting, velocity/position update,
 // wall anti-penetration and velocity smoothing.
 #include "impl.cuh"
+#include "mixed.cuh"
 #include "packed.cuh"
 
 namespace lsmps {
@@ -402,9 +403,15 @@ namespace {
 // give the same clamped value), and each thread writes its own clamped value.
 // The shifting offsets x_i - x_j are the exact negations of x_j - x_i, so the
 // outputs are bitwise those of the separate kernels.
+//
+// Mixed (the mixed form): the FP64 gradient sums are contracted with rows
+// 0..2 of the pressure operator rows (FP32, or FP64 for FP64-route
+// particles) instead of the full inverse.
+template <bool Mixed>
 __global__ void __launch_bounds__(kThreads) gradient_shifting_kernel(GatherArgs a, double* pressure,
                                                                      double* fluid_pressure,
-                                                                     const double* __restrict__ pinv, double re,
+                                                                     const double* __restrict__ pinv,
+                                                                     MixedRows prows, double re,
                                                                      double wall_scale, double* gx, double* gy,
                                                                      double* gz, double* sx_out, double* sy_out,
                                                                      double* sz_out) {
@@ -483,7 +490,21 @@ __global__ void __launch_bounds__(kThreads) gradient_shifting_kernel(GatherArgs 
       shz = fma(push, wnz, shz);
     }
   }
-  if (do_grad) {
+  if (do_grad && Mixed) {
+    double g[9], c0 = 0.0, c1 = 0.0, c2 = 0.0;
+    load_row9(prows, i, 1, g);
+#pragma unroll
+    for (int col = 0; col < 9; ++col) c0 = fma(g[col], rhs[col], c0);
+    load_row9(prows, i, 2, g);
+#pragma unroll
+    for (int col = 0; col < 9; ++col) c1 = fma(g[col], rhs[col], c1);
+    load_row9(prows, i, 3, g);
+#pragma unroll
+    for (int col = 0; col < 9; ++col) c2 = fma(g[col], rhs[col], c2);
+    gx[i] = c0 * inv_re;
+    gy[i] = c1 * inv_re;
+    gz[i] = c2 * inv_re;
+  } else if (do_grad) {
     const double* __restrict__ inv = pinv + static_cast<size_t>(i) * 81;
     double c0 = 0.0, c1 = 0.0, c2 = 0.0;
 #pragma unroll
@@ -583,7 +604,8 @@ __global__ void __launch_bounds__(kThreads) update_anti_penetration_kernel(
 lsmps_status pressure_correction_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const lsmps_walls& w,
                                       const lsmps_csr& fn, const lsmps_csr& wn, const lsmps_fluid& t,
                                       double* pressure, const lsmps_params& p, const lsmps_moment& pm,
-                                      const lsmps_vector& g, const lsmps_vector& s, const lsmps_vector& sm) {
+                                      const lsmps_vector& g, const lsmps_vector& s, const lsmps_vector& sm,
+                                      bool mixed) {
   lsmps_status st = check_fluid(ctx, f);
   if (st) return st;
   if (f.count > 0 && !pressure) return fail(ctx, LSMPS_INVALID_ARGUMENT, "Pressure correction requires a pressure array");
@@ -594,12 +616,20 @@ lsmps_status pressure_correction_impl(lsmps_ctx* ctx, const lsmps_fluid& f, cons
   if (pm.kind != LSMPS_MOMENT_PRESSURE_WALL_NEUMANN_A || pm.matrix_size != 9 || pm.particle_count < f.count)
     return fail(ctx, LSMPS_NOT_PREPARED, "Pressure correction requires a prepared pressure Type-A moment matrix");
   if (f.count == 0) return LSMPS_OK;
-  if (!pm.inverse_matrices) return fail(ctx, LSMPS_INVALID_ARGUMENT, "pressure inverse buffer missing");
   GatherArgs a{f, w, fn.offsets, fn.indices, wn.offsets, wn.indices, p};
   const int blocks = div_up(static_cast<long long>(f.count), kThreads);
-  launch(ctx, gradient_shifting_kernel, dim3(blocks), dim3(kThreads), 0, a, pressure, f.pressure,
-         static_cast<const double*>(pm.inverse_matrices), pm.support_radius, pm.wall_weight_scale, g.x, g.y, g.z,
-         s.x, s.y, s.z);
+  if (mixed) {
+    if (!ctx->mixed_rows[1] || ctx->mixed_cap < f.count)
+      return fail(ctx, LSMPS_NOT_PREPARED, "mixed pressure operator rows were not prepared");
+    launch(ctx, gradient_shifting_kernel<true>, dim3(blocks), dim3(kThreads), 0, a, pressure, f.pressure,
+           static_cast<const double*>(nullptr), mixed_rows_of(ctx, 1), pm.support_radius,
+           pm.wall_weight_scale, g.x, g.y, g.z, s.x, s.y, s.z);
+  } else {
+    if (!pm.inverse_matrices) return fail(ctx, LSMPS_INVALID_ARGUMENT, "pressure inverse buffer missing");
+    launch(ctx, gradient_shifting_kernel<false>, dim3(blocks), dim3(kThreads), 0, a, pressure, f.pressure,
+           static_cast<const double*>(pm.inverse_matrices), MixedRows{},
+           pm.support_radius, pm.wall_weight_scale, g.x, g.y, g.z, s.x, s.y, s.z);
+  }
   launch(ctx, update_anti_penetration_kernel, dim3(blocks), dim3(kThreads), 0, f, w,
          static_cast<const index_t*>(wn.offsets), static_cast<const index_t*>(wn.indices),
          static_cast<const double*>(t.vx), static_cast<const double*>(t.vy), static_cast<const double*>(t.vz),

@@ -14,9 +14,21 @@ lsmps_status classify_surface_impl(lsmps_ctx* ctx, const lsmps_fluid& fluid, con
 lsmps_status prepare_moments_impl(lsmps_ctx* ctx, const lsmps_fluid& fluid, const lsmps_walls& walls,
                                   const lsmps_csr& fn, const lsmps_csr& wn, const lsmps_params& p,
                                   const lsmps_moment* kinds, int count);
+// Mixed form of the step's moment stage: compact FP32 operator rows of the
+// velocity and pressure Type-A inverses in ctx->mixed_rows (the views get
+// trace, regularisation, info and inversion_count; their inverse_matrices
+// are not written).
+lsmps_status mixed_step_moments_impl(lsmps_ctx* ctx, const lsmps_fluid& fluid, const lsmps_walls& walls,
+                                     const lsmps_csr& fn, const lsmps_csr& wn, const lsmps_params& p,
+                                     const lsmps_moment& vm, const lsmps_moment& pm);
 lsmps_status velocity_laplacian_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const lsmps_walls& w,
                                      const lsmps_csr& fn, const lsmps_csr& wn, const lsmps_moment& vm,
                                      const lsmps_vector& lap);
+// Mixed form (after mixed_step_moments_impl in the same step: reads the
+// position packs it left and ctx->mixed_rows).
+lsmps_status velocity_laplacian_mixed_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const lsmps_walls& w,
+                                           const lsmps_csr& fn, const lsmps_csr& wn, const lsmps_moment& vm,
+                                           const lsmps_vector& lap);
 lsmps_status temporary_velocity_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const lsmps_params& p,
                                      const lsmps_vector& lap, const lsmps_fluid& t);
 lsmps_status temporary_wall_velocity_impl(lsmps_ctx* ctx, const lsmps_walls& w, const lsmps_params& p,
@@ -25,10 +37,15 @@ lsmps_status assemble_ppe_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const lsmps
                                const lsmps_csr& fn, const lsmps_csr& wn, const lsmps_fluid& tv,
                                const lsmps_walls& tw, const lsmps_moment& vm, const lsmps_moment& pm,
                                const lsmps_ppe& ws);
+lsmps_status assemble_ppe_mixed_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const lsmps_walls& w,
+                                     const lsmps_params& p, const lsmps_csr& fn, const lsmps_csr& wn,
+                                     const lsmps_fluid& tv, const lsmps_walls& tw, const lsmps_moment& vm,
+                                     const lsmps_moment& pm, const lsmps_ppe& ws);
 lsmps_status pressure_correction_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const lsmps_walls& w,
                                       const lsmps_csr& fn, const lsmps_csr& wn, const lsmps_fluid& t,
                                       double* pressure, const lsmps_params& p, const lsmps_moment& pm,
-                                      const lsmps_vector& g, const lsmps_vector& s, const lsmps_vector& sm);
+                                      const lsmps_vector& g, const lsmps_vector& s, const lsmps_vector& sm,
+                                      bool mixed = false);
 lsmps_status build_neighbor_lists_impl(lsmps_ctx* ctx, Scratch& scratch, const lsmps_fluid& fluid,
                                        const lsmps_walls& walls, const lsmps_params& p,
                                        const lsmps_cells& fc, const lsmps_cells& wc, const lsmps_csr& fn,

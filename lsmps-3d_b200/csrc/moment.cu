@@ -101,34 +101,36 @@ __device__ __forceinline__ void add_outer(double (&m)[N * (N + 1) / 2], const do
 // Column J of the lower Cholesky factor, in place.  J is a template argument
 // so that every index into the register array is a compile-time constant
 // even though sqrt() keeps the compiler from unrolling a loop over columns.
-template <int N, int J>
-__device__ __forceinline__ void cholesky_column(double (&a)[N * (N + 1) / 2], int& info) {
-  double s = a[tri(J, J)];
+// T is double for the plain form and float for the mixed form's first
+// factorisation.
+template <int N, int J, typename T>
+__device__ __forceinline__ void cholesky_column(T (&a)[N * (N + 1) / 2], int& info) {
+  T s = a[tri(J, J)];
 #pragma unroll
   for (int k = 0; k < J; ++k) s = fma(-a[tri(J, k)], a[tri(J, k)], s);
-  if (!(s > 0.0) && info == 0) info = J + 1;
-  const double ljj = sqrt(s);
+  if (!(s > T(0)) && info == 0) info = J + 1;
+  const T ljj = sqrt(s);
   a[tri(J, J)] = ljj;
-  const double inv = 1.0 / ljj;
+  const T inv = T(1) / ljj;
 #pragma unroll
   for (int i = J + 1; i < N; ++i) {
-    double t = a[tri(i, J)];
+    T t = a[tri(i, J)];
 #pragma unroll
     for (int k = 0; k < J; ++k) t = fma(-a[tri(i, k)], a[tri(J, k)], t);
     a[tri(i, J)] = t * inv;
   }
 }
 
-template <int N, int... J>
-__device__ __forceinline__ void cholesky_columns(double (&a)[N * (N + 1) / 2], int& info,
+template <int N, typename T, int... J>
+__device__ __forceinline__ void cholesky_columns(T (&a)[N * (N + 1) / 2], int& info,
                                                  std::integer_sequence<int, J...>) {
   (cholesky_column<N, J>(a, info), ...);
 }
 
 // Lower Cholesky in place; returns 0 or the 1-based order of the first
 // non-positive pivot (the potrf info convention).
-template <int N>
-__device__ __forceinline__ int cholesky(double (&a)[N * (N + 1) / 2]) {
+template <int N, typename T>
+__device__ __forceinline__ int cholesky(T (&a)[N * (N + 1) / 2]) {
   int info = 0;
   cholesky_columns<N>(a, info, std::make_integer_sequence<int, N>{});
   return info;
@@ -324,10 +326,11 @@ __host__ __device__ constexpr int entry_slot(int r, int c) {
                        basis_exponent(r, 2) + basis_exponent(c, 2));
 }
 
-__device__ __forceinline__ void acc_monomials(double (&s)[kMonomials], double sx, double sy, double sz, double w) {
-  const double qxx = sx * sx, qyy = sy * sy, qzz = sz * sz;
-  const double qxy = sx * sy, qyz = sy * sz, qzx = sz * sx;
-  const double wxx = w * qxx, wyy = w * qyy, wzz = w * qzz, wxy = w * qxy;
+template <typename T>
+__device__ __forceinline__ void acc_monomials(T (&s)[kMonomials], T sx, T sy, T sz, T w) {
+  const T qxx = sx * sx, qyy = sy * sy, qzz = sz * sz;
+  const T qxy = sx * sy, qyz = sy * sz, qzx = sz * sx;
+  const T wxx = w * qxx, wyy = w * qyy, wzz = w * qzz, wxy = w * qxy;
   s[0] = fma(w, qxx, s[0]);
   s[1] = fma(w, qyy, s[1]);
   s[2] = fma(w, qzz, s[2]);
@@ -472,6 +475,326 @@ __global__ void __launch_bounds__(kMomentThreads, MinBlocks) moment_a_kernel(Mom
   }
 }
 
+// ---------------------------------------------------------------------------
+// Mixed form (LSMPS_PRECISION_MIXED).
+//
+// Stage 1 (moment_sums_kernel): the 31 fluid monomial sums of each particle.
+// Each neighbour's r_e-scaled offset and weight are formed in FP32 from the
+// FP64 coordinate difference, its 31 weighted monomials are formed in FP32,
+// and each is added into its sum with Kahan's compensated summation (an FP32
+// sum and an FP32 running compensation), so the summation adds no error
+// beyond O(n u^2) to the rounding of the terms themselves.  The totals
+// (sum minus compensation, in FP64) go to the context's mixed_sums array,
+// monomial-major.
+//
+// Stage 2 (moment_rows_kernel, one thread per particle and kind): the kind's
+// wall term (FP64; walls are few), trace and regularisation as in the plain
+// form, then an FP32 Cholesky factorisation.  The operator rows the step
+// consumes are y = M^-1 u for u = e3 + e4 + e5 (the Laplacian row) and
+// u = e0, e1, e2 (the gradient rows; M^-1 is symmetric, so rows equal
+// columns): each is solved with the FP32 factor and refined once in FP64,
+// y1 = y0 + M^-1_f32 (u - M y0) with the residual u - M y0 formed against the
+// FP64 matrix.  A matrix whose FP32 factorisation fails, or whose condition
+// estimate (max L_ii / min L_ii)^2 exceeds the context's threshold (1e4 by
+// default: ill-conditioned Surface and Splash particles), is factorised and
+// solved in FP64 instead and counted in DeviceStatus::fallbacks.  The rows
+// are stored as FP32, 36 per particle: [Laplacian row, row 0, row 1, row 2].
+// With Full, all nine columns are solved and the full FP64 inverse is
+// written to the moment view (lsmps_prepare_moments in the mixed form).
+
+constexpr int kSumThreads = 128;
+constexpr int kRowThreads = 64;
+
+struct MixedSumArgs {
+  index_t n;
+  const double4* fp;
+  const index_t* fo;
+  const index_t* fi;
+  double inv_re;
+  double* sums;
+};
+
+// Kahan step for the 31 weighted monomials of one neighbour (the same
+// products as acc_monomials).
+__device__ __forceinline__ void kahan_monomials(float (&s)[kMonomials], float (&c)[kMonomials], float sx, float sy,
+                                                float sz, float w) {
+  float t[kMonomials];
+#pragma unroll
+  for (int e = 0; e < kMonomials; ++e) t[e] = 0.0f;
+  acc_monomials(t, sx, sy, sz, w);
+#pragma unroll
+  for (int e = 0; e < kMonomials; ++e) {
+    const float y = t[e] - c[e];
+    const float u = s[e] + y;
+    c[e] = (u - s[e]) - y;
+    s[e] = u;
+  }
+}
+
+__global__ void __launch_bounds__(kSumThreads) moment_sums_kernel(MixedSumArgs a) {
+  const index_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.n) return;
+  const double4 pi = ld4(a.fp, i);
+  float sum[kMonomials], comp[kMonomials];
+#pragma unroll
+  for (int e = 0; e < kMonomials; ++e) sum[e] = comp[e] = 0.0f;
+  const index_t fb = a.fo[i], fe = a.fo[i + 1];
+  for (index_t o = fb; o < fe; ++o) {
+    const double4 q = ld4(a.fp, a.fi[o]);
+    const float sx = static_cast<float>((q.x - pi.x) * a.inv_re);
+    const float sy = static_cast<float>((q.y - pi.y) * a.inv_re);
+    const float sz = static_cast<float>((q.z - pi.z) * a.inv_re);
+    const float d2 = sx * sx + sy * sy + sz * sz;
+    if (d2 > 0.0f) {
+      const float w = 1.0f - sqrtf(d2);
+      if (w > 0.0f) kahan_monomials(sum, comp, sx, sy, sz, w);
+    }
+  }
+  const size_t n = static_cast<size_t>(a.n);
+#pragma unroll
+  for (int e = 0; e < kMonomials; ++e) a.sums[e * n + i] = static_cast<double>(sum[e]) - static_cast<double>(comp[e]);
+}
+
+struct MixedRowArgs {
+  index_t n;
+  const double* sums;
+  const double4* fp;
+  const double4* wp;
+  const double4* wn;
+  const index_t* fo;
+  const index_t* fi;
+  const index_t* wo;
+  const index_t* wi;
+  double inv_re;
+  double lambda;
+  double wall_scale;
+  double kappa_threshold;
+  KindOut k[2];       // velocity Dirichlet-A, pressure Neumann-A
+  float* rows[2];     // compact FP32 rows per kind (unless Full)
+  double* rows64[2];  // compact FP64 rows of the FP64-route particles (unless Full)
+  uint8_t* flag[2];   // 1 where rows64 holds the particle's rows (unless Full)
+  DeviceStatus* status;
+};
+
+// v <- L^-T L^-1 v with the packed lower factor and its reciprocal diagonal.
+template <typename T>
+__device__ __forceinline__ void chol_solve(const T (&l)[45], const T (&dinv)[9], T (&v)[9]) {
+#pragma unroll
+  for (int r = 0; r < 9; ++r) {
+    T t = v[r];
+#pragma unroll
+    for (int k = 0; k < r; ++k) t = fma(-l[tri(r, k)], v[k], t);
+    v[r] = t * dinv[r];
+  }
+#pragma unroll
+  for (int r = 8; r >= 0; --r) {
+    T t = v[r];
+#pragma unroll
+    for (int k = r + 1; k < 9; ++k) t = fma(-l[tri(k, r)], v[k], t);
+    v[r] = t * dinv[r];
+  }
+}
+
+// Target t of the row set: t = 0 the Laplacian row (e3 + e4 + e5), t = 1..3
+// rows 0..2; with Full, t = 0..8 is e_t.
+template <bool Full>
+__device__ __forceinline__ double target(int t, int r) {
+  if (Full) return r == t ? 1.0 : 0.0;
+  if (t == 0) return (r >= 3 && r <= 5) ? 1.0 : 0.0;
+  return r == t - 1 ? 1.0 : 0.0;
+}
+
+template <bool Full>
+__device__ __forceinline__ void store_target(const MixedRowArgs& a, int kind, index_t i, int t, const double (&y)[9],
+                                             bool fp64) {
+  if (Full) {
+    double* out = a.k[kind].inverse + static_cast<size_t>(i) * 81;
+#pragma unroll
+    for (int r = 0; r < 9; ++r) {
+      if (r < t) continue;
+      out[r + t * 9] = y[r];
+      out[t + r * 9] = y[r];
+    }
+  } else if (fp64) {
+    double* out = a.rows64[kind] + static_cast<size_t>(i) * 36 + t * 9;
+#pragma unroll
+    for (int r = 0; r < 9; ++r) out[r] = y[r];
+  } else {
+    float* out = a.rows[kind] + static_cast<size_t>(i) * 36 + t * 9;
+#pragma unroll
+    for (int r = 0; r < 9; ++r) out[r] = static_cast<float>(y[r]);
+  }
+}
+
+// The kind's matrix from the 31 fluid monomial totals s: the wall term (FP64;
+// Dirichlet into s, Neumann as q q^T), expanded into the thread's column of
+// shared memory m[e * kRowThreads], then trace and regularisation
+// (moment_matrix.cu:286-308).  Returns the trace; *reg gets the shift.
+__device__ __forceinline__ double assemble_kind(const MixedRowArgs& a, int kind, index_t i, const double4& pi,
+                                                double (&s)[kMonomials], double* m, double* reg) {
+  const index_t wb = a.wo[i], we = a.wo[i + 1];
+  if (kind == 0) {
+    for (index_t o = wb; o < we; ++o) {
+      const double4 q = ld4(a.wp, a.wi[o]);
+      const double dx = q.x - pi.x, dy = q.y - pi.y, dz = q.z - pi.z;
+      const double d2 = dx * dx + dy * dy + dz * dz;
+      if (d2 <= 0.0) continue;
+      const double w = a.wall_scale * (1.0 - sqrt(d2) * a.inv_re);
+      if (w <= 0.0) continue;
+      acc_monomials(s, dx * a.inv_re, dy * a.inv_re, dz * a.inv_re, w);
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < 9; ++r) {
+#pragma unroll
+    for (int c = 0; c <= r; ++c) m[tri(r, c) * kRowThreads] = s[entry_slot(r, c)];
+  }
+  if (kind == 1) {
+    double q9[9];
+    for (index_t o = wb; o < we; ++o) {
+      const index_t j = a.wi[o];
+      const double4 q = ld4(a.wp, j);
+      const double dx = q.x - pi.x, dy = q.y - pi.y, dz = q.z - pi.z;
+      const double d2 = dx * dx + dy * dy + dz * dz;
+      if (d2 <= 0.0) continue;
+      const double w = a.wall_scale * (1.0 - sqrt(d2) * a.inv_re);
+      if (w <= 0.0) continue;
+      const double4 nrm = ld4(a.wn, j);
+      neumann<9>(dx, dy, dz, nrm.x, nrm.y, nrm.z, a.inv_re, q9);
+#pragma unroll
+      for (int r = 0; r < 9; ++r) {
+        const double wr = w * q9[r];
+#pragma unroll
+        for (int c = 0; c <= r; ++c) m[tri(r, c) * kRowThreads] = fma(wr, q9[c], m[tri(r, c) * kRowThreads]);
+      }
+    }
+  }
+  double trace = 0.0;
+#pragma unroll
+  for (int r = 0; r < 9; ++r) trace += m[tri(r, r) * kRowThreads];
+  *reg = a.lambda * (trace > 0.0 ? trace / 9.0 : 1.0);
+#pragma unroll
+  for (int r = 0; r < 9; ++r) m[tri(r, r) * kRowThreads] += *reg;
+  return trace;
+}
+
+template <bool Full>
+__global__ void __launch_bounds__(kRowThreads, 6) moment_rows_kernel(MixedRowArgs a) {
+  __shared__ double s_m[45 * kRowThreads];
+  const int kind = blockIdx.y;
+  const index_t i = blockIdx.x * kRowThreads + threadIdx.x;
+  if (blockIdx.x == 0 && threadIdx.x == 0 && a.k[kind].count) atomicAdd(a.k[kind].count, 1);
+  if (i >= a.n) return;
+  double* m = s_m + threadIdx.x;  // entry e at m[e * kRowThreads]
+  const size_t n = static_cast<size_t>(a.n);
+  const double4 pi = ld4(a.fp, i);
+  const KindOut& ko = a.k[kind];
+  constexpr int kTargets = Full ? 9 : 4;
+  double reg = 0.0, trace = 0.0;
+  {
+    double s[kMonomials];
+#pragma unroll
+    for (int e = 0; e < kMonomials; ++e) s[e] = a.sums[e * n + i];
+    trace = assemble_kind(a, kind, i, pi, s, m, &reg);
+  }
+  float l[45];
+#pragma unroll
+  for (int e = 0; e < 45; ++e) l[e] = static_cast<float>(m[e * kRowThreads]);
+  int info = cholesky<9>(l);
+  bool fp64 = info != 0;
+  float dinv[9];
+  if (!fp64) {
+    float lo = l[tri(0, 0)], hi = lo;
+#pragma unroll
+    for (int r = 1; r < 9; ++r) {
+      lo = fminf(lo, l[tri(r, r)]);
+      hi = fmaxf(hi, l[tri(r, r)]);
+    }
+    const double ratio = static_cast<double>(hi) / static_cast<double>(lo);
+    fp64 = ratio * ratio > a.kappa_threshold;
+#pragma unroll
+    for (int r = 0; r < 9; ++r) dinv[r] = 1.0f / l[tri(r, r)];
+  }
+  if (!fp64) {
+    for (int t = 0; t < kTargets; ++t) {
+      float y0[9];
+#pragma unroll
+      for (int r = 0; r < 9; ++r) y0[r] = static_cast<float>(target<Full>(t, r));
+      chol_solve(l, dinv, y0);
+      // one refinement step: residual against the FP64 matrix, correction
+      // through the FP32 factor
+      float d[9];
+#pragma unroll
+      for (int r = 0; r < 9; ++r) {
+        double res = target<Full>(t, r);
+#pragma unroll
+        for (int c = 0; c < 9; ++c) {
+          const int e = r >= c ? tri(r, c) : tri(c, r);
+          res = fma(-m[e * kRowThreads], static_cast<double>(y0[c]), res);
+        }
+        d[r] = static_cast<float>(res);
+      }
+      chol_solve(l, dinv, d);
+      double y[9];
+#pragma unroll
+      for (int r = 0; r < 9; ++r) y[r] = static_cast<double>(y0[r]) + static_cast<double>(d[r]);
+      store_target<Full>(a, kind, i, t, y, false);
+    }
+    ko.trace[i] = trace;
+    ko.reg[i] = reg;
+    ko.info[i] = 0;
+    if (!Full) a.flag[kind][i] = 0;
+    return;
+  }
+  // FP64 route: the matrix is re-assembled in FP64 from the particle's rows
+  // (the FP32-rounded terms can leave a nearly rank-deficient matrix
+  // indefinite) and factorised in FP64, as in the plain form.
+  atomicAdd(&a.status->fallbacks, 1u);
+  {
+    double s[kMonomials];
+#pragma unroll
+    for (int e = 0; e < kMonomials; ++e) s[e] = 0.0;
+    const index_t fe = a.fo[i + 1];
+    for (index_t o = a.fo[i]; o < fe; ++o) {
+      const double4 q = ld4(a.fp, a.fi[o]);
+      const double dx = q.x - pi.x, dy = q.y - pi.y, dz = q.z - pi.z;
+      const double d2 = dx * dx + dy * dy + dz * dz;
+      if (d2 <= 0.0) continue;
+      const double w = 1.0 - sqrt(d2) * a.inv_re;
+      if (w <= 0.0) continue;
+      acc_monomials(s, dx * a.inv_re, dy * a.inv_re, dz * a.inv_re, w);
+    }
+    trace = assemble_kind(a, kind, i, pi, s, m, &reg);
+  }
+  ko.trace[i] = trace;
+  ko.reg[i] = reg;
+  if (!Full) a.flag[kind][i] = 1;
+  double l64[45];
+#pragma unroll
+  for (int e = 0; e < 45; ++e) l64[e] = m[e * kRowThreads];
+  info = cholesky<9>(l64);
+  ko.info[i] = info;
+  if (info != 0) {
+    double nan9[9];
+#pragma unroll
+    for (int r = 0; r < 9; ++r) nan9[r] = __longlong_as_double(0x7ff8000000000000LL);
+    for (int t = 0; t < kTargets; ++t) store_target<Full>(a, kind, i, t, nan9, true);
+    atomicAdd(&a.status->non_spd, 1u);
+    raise_flag(a.status, kFlagNonSpd);
+    return;
+  }
+  double dinv64[9];
+#pragma unroll
+  for (int r = 0; r < 9; ++r) dinv64[r] = 1.0 / l64[tri(r, r)];
+  for (int t = 0; t < kTargets; ++t) {
+    double y[9];
+#pragma unroll
+    for (int r = 0; r < 9; ++r) y[r] = target<Full>(t, r);
+    chol_solve(l64, dinv64, y);
+    store_target<Full>(a, kind, i, t, y, true);
+  }
+}
+
 // make_matrix_request, moment_matrix.cu:494-538: boundary of each kind.
 int boundary_of(int kind) {
   switch (kind) {
@@ -482,7 +805,72 @@ int boundary_of(int kind) {
   }
 }
 
+// Queue the two mixed-form stages for the velocity (kv) and pressure (kp)
+// Type-A kinds; positions are already packed into ctx->pack_fluid[0] and the
+// wall packs.
+lsmps_status launch_mixed(lsmps_ctx* ctx, index_t n, const lsmps_csr& fn, const lsmps_csr& wn,
+                          const lsmps_params& p, const KindOut& kv, const KindOut& kp, bool full) {
+  if (!ensure_mixed(ctx, static_cast<size_t>(n))) return fail(ctx, LSMPS_CUDA_ERROR, "mixed-form allocation failed");
+  const double inv_re = 1.0 / p.support_radius;
+  MixedSumArgs sa{n, ctx->pack_fluid[0], fn.offsets, fn.indices, inv_re, ctx->mixed_sums};
+  launch(ctx, moment_sums_kernel, dim3(div_up(n, kSumThreads)), dim3(kSumThreads), 0, sa);
+  MixedRowArgs ra{};
+  ra.n = n;
+  ra.sums = ctx->mixed_sums;
+  ra.fp = ctx->pack_fluid[0];
+  ra.wp = ctx->pack_wall[0];
+  ra.wn = ctx->pack_wall[2];
+  ra.wo = wn.offsets;
+  ra.wi = wn.indices;
+  ra.inv_re = inv_re;
+  ra.lambda = p.lsmps_regularization;
+  ra.wall_scale = p.lsmps_wall_weight_scale;
+  ra.kappa_threshold = ctx->kappa_threshold;
+  ra.k[0] = kv;
+  ra.k[1] = kp;
+  ra.fo = fn.offsets;
+  ra.fi = fn.indices;
+  for (int k = 0; k < 2; ++k) {
+    ra.rows[k] = ctx->mixed_rows[k];
+    ra.rows64[k] = ctx->mixed_rows64[k];
+    ra.flag[k] = ctx->mixed_flag[k];
+  }
+  ra.status = ctx->d_status;
+  const dim3 grid(div_up(n, kRowThreads), 2);
+  if (full)
+    launch(ctx, moment_rows_kernel<true>, grid, dim3(kRowThreads), 0, ra);
+  else
+    launch(ctx, moment_rows_kernel<false>, grid, dim3(kRowThreads), 0, ra);
+  return LSMPS_OK;
+}
+
 }  // namespace
+
+lsmps_status mixed_step_moments_impl(lsmps_ctx* ctx, const lsmps_fluid& fluid, const lsmps_walls& walls,
+                                     const lsmps_csr& fn, const lsmps_csr& wn, const lsmps_params& p,
+                                     const lsmps_moment& vm, const lsmps_moment& pm) {
+  if (!(p.support_radius > 0.0)) return fail(ctx, LSMPS_INVALID_ARGUMENT, "Moment support radius must be positive");
+  if (vm.kind != LSMPS_MOMENT_VELOCITY_WALL_DIRICHLET_A || pm.kind != LSMPS_MOMENT_PRESSURE_WALL_NEUMANN_A ||
+      vm.matrix_size != 9 || pm.matrix_size != 9 || vm.particle_count < fluid.count ||
+      pm.particle_count < fluid.count)
+    return fail(ctx, LSMPS_INVALID_ARGUMENT, "Invalid Moment matrix cache");
+  if (fluid.count > fn.particle_count || fluid.count > wn.particle_count)
+    return fail(ctx, LSMPS_INVALID_ARGUMENT, "Moment matrix neighbor lists are smaller than fluid particle count");
+  const index_t n = static_cast<index_t>(fluid.count);
+  if (n == 0) return LSMPS_OK;
+  if (!vm.moment_trace || !vm.regularization_added || !vm.info || !pm.moment_trace || !pm.regularization_added ||
+      !pm.info)
+    return fail(ctx, LSMPS_INVALID_ARGUMENT, "Invalid Moment matrix cache buffers");
+  if (!ensure_packs(ctx, fluid.count, walls.count)) return fail(ctx, LSMPS_CUDA_ERROR, "pack allocation failed");
+  pack4(ctx, fluid.x, fluid.y, fluid.z, nullptr, fluid.count, ctx->pack_fluid[0]);
+  pack4(ctx, walls.x, walls.y, walls.z, nullptr, walls.count, ctx->pack_wall[0]);
+  pack4(ctx, walls.normal_x, walls.normal_y, walls.normal_z, nullptr, walls.count, ctx->pack_wall[2]);
+  const KindOut kv{1, vm.inverse_matrices, vm.moment_trace, vm.regularization_added, vm.info, vm.inversion_count};
+  const KindOut kp{2, pm.inverse_matrices, pm.moment_trace, pm.regularization_added, pm.info, pm.inversion_count};
+  lsmps_status st = launch_mixed(ctx, n, fn, wn, p, kv, kp, false);
+  if (st) return st;
+  return check_launch(ctx, "mixed moment rows");
+}
 
 lsmps_status prepare_moments_impl(lsmps_ctx* ctx, const lsmps_fluid& fluid, const lsmps_walls& walls,
                                   const lsmps_csr& fn, const lsmps_csr& wn, const lsmps_params& p,
@@ -535,7 +923,12 @@ lsmps_status prepare_moments_impl(lsmps_ctx* ctx, const lsmps_fluid& fluid, cons
                       ctx->d_status};
   const bool fused = velocity_a >= 0 && pressure_a >= 0;
   const bool capped = ctx->knob[LSMPS_KNOB_MOMENT_OCCUPANCY] == 1;
-  if (fused) {
+  if (fused && ctx->precision == LSMPS_PRECISION_MIXED) {
+    // Mixed form: FP32 assembly and factorisation with FP64 refinement; the
+    // full inverse is written (FP64) for the caller's views.
+    lsmps_status st = launch_mixed(ctx, n, fn, wn, p, out_of(kinds[velocity_a]), out_of(kinds[pressure_a]), true);
+    if (st) return st;
+  } else if (fused) {
     // The step's two kinds share the fluid sums: one pass over the rows.
     MomentPackedArgs a = pa;
     a.k0 = out_of(kinds[velocity_a]);

@@ -6,6 +6,7 @@
 // neighbour in CSR order (columns unsorted).  Surface and Splash rows are
 // Dirichlet rows: diagonal 1, neighbour slots 0, rhs 0 (:124-131, :262-276).
 #include "impl.cuh"
+#include "mixed.cuh"
 
 namespace lsmps {
 namespace {
@@ -40,6 +41,10 @@ struct PpeArgs {
   double* rhs;
   double* divergence;
   double* wall_rhs_out;  // pressure_laplacian (holds the wall Neumann term, :367-369)
+  // Mixed form: operator rows [Laplacian row, rows 0..2] per particle of the
+  // velocity and pressure inverses, in place of vinv / pinv.
+  MixedRows vrows;
+  MixedRows prows;
 };
 
 __device__ __forceinline__ double dot9(const double a[9], const double b[9]) {
@@ -157,7 +162,13 @@ __device__ __forceinline__ double group_sum(double v, unsigned mask) {
 // diagonal, the 27 divergence moments and the wall Neumann term) are added
 // across the group with shuffles; lane 0 finishes the row.  The sums are
 // associated differently from the one-lane kernel (rounding-level change).
-template <int G>
+//
+// Mixed (the mixed form): the pressure Laplacian row L comes from the
+// pressure operator rows and the divergence rows from the velocity operator
+// rows (FP32, or FP64 for FP64-route particles); geometry, coefficients, the
+// diagonal (minus the sum of the off-diagonal values) and the RHS sums stay
+// FP64.
+template <int G, bool Mixed>
 __global__ void __launch_bounds__(kThreads) ppe_lanes_kernel(PpeArgs a) {
   const index_t i = (blockIdx.x * blockDim.x + threadIdx.x) / G;
   const int l = threadIdx.x & (G - 1);
@@ -189,10 +200,14 @@ __global__ void __launch_bounds__(kThreads) ppe_lanes_kernel(PpeArgs a) {
   const double* __restrict__ fy = a.fluid.y;
   const double* __restrict__ fz = a.fluid.z;
   const double xi = fx[i], yi = fy[i], zi = fz[i];
-  const double* __restrict__ pinv = a.pinv + static_cast<size_t>(i) * 81;
   double L[9];
+  if (Mixed) {
+    load_row9(a.prows, i, 0, L);
+  } else {
+    const double* __restrict__ pinv = a.pinv + static_cast<size_t>(i) * 81;
 #pragma unroll
-  for (int col = 0; col < 9; ++col) L[col] = pinv[3 + col * 9] + pinv[4 + col * 9] + pinv[5 + col * 9];
+    for (int col = 0; col < 9; ++col) L[col] = pinv[3 + col * 9] + pinv[4 + col * 9] + pinv[5 + col * 9];
+  }
   const double uxi = a.tvx[i], uyi = a.tvy[i], uzi = a.tvz[i];
   const double scale = 2.0 / (a.re * a.re * a.density);
   double rx[9], ry[9], rz[9], b[9];
@@ -238,8 +253,23 @@ __global__ void __launch_bounds__(kThreads) ppe_lanes_kernel(PpeArgs a) {
     rz[r] = group_sum<G>(rz[r], mask);
   }
   if (l != 0) return;
-  const double* __restrict__ vinv = a.vinv + static_cast<size_t>(i) * 81;
-  const double div = (coeff_row(vinv, rx, 0) + coeff_row(vinv, ry, 1) + coeff_row(vinv, rz, 2)) * a.inv_re;
+  double div;
+  if (Mixed) {
+    double g[9], c0 = 0.0, c1 = 0.0, c2 = 0.0;
+    load_row9(a.vrows, i, 1, g);
+#pragma unroll
+    for (int col = 0; col < 9; ++col) c0 = fma(g[col], rx[col], c0);
+    load_row9(a.vrows, i, 2, g);
+#pragma unroll
+    for (int col = 0; col < 9; ++col) c1 = fma(g[col], ry[col], c1);
+    load_row9(a.vrows, i, 3, g);
+#pragma unroll
+    for (int col = 0; col < 9; ++col) c2 = fma(g[col], rz[col], c2);
+    div = (c0 + c1 + c2) * a.inv_re;
+  } else {
+    const double* __restrict__ vinv = a.vinv + static_cast<size_t>(i) * 81;
+    div = (coeff_row(vinv, rx, 0) + coeff_row(vinv, ry, 1) + coeff_row(vinv, rz, 2)) * a.inv_re;
+  }
   a.col[row] = i;
   a.val[row] = diag;
   a.divergence[i] = div;
@@ -299,12 +329,66 @@ lsmps_status assemble_ppe_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const lsmps
   a.wall_rhs_out = ws.pressure_laplacian;
   const long long rows = static_cast<long long>(f.count);
   switch (ctx->knob[LSMPS_KNOB_PPE_LANES]) {
-    case 1: launch(ctx, ppe_lanes_kernel<4>, dim3(div_up(rows * 4, kThreads)), dim3(kThreads), 0, a); break;
-    case 2: launch(ctx, ppe_lanes_kernel<8>, dim3(div_up(rows * 8, kThreads)), dim3(kThreads), 0, a); break;
-    case 3: launch(ctx, ppe_lanes_kernel<16>, dim3(div_up(rows * 16, kThreads)), dim3(kThreads), 0, a); break;
+    case 1: launch_named(ctx, "ppe_lanes_kernel<4, false>", ppe_lanes_kernel<4, false>, dim3(div_up(rows * 4, kThreads)), dim3(kThreads), 0, a); break;
+    case 2: launch_named(ctx, "ppe_lanes_kernel<8, false>", ppe_lanes_kernel<8, false>, dim3(div_up(rows * 8, kThreads)), dim3(kThreads), 0, a); break;
+    case 3: launch_named(ctx, "ppe_lanes_kernel<16, false>", ppe_lanes_kernel<16, false>, dim3(div_up(rows * 16, kThreads)), dim3(kThreads), 0, a); break;
     default: launch(ctx, ppe_kernel, dim3(div_up(rows, kThreads)), dim3(kThreads), 0, a); break;
   }
   return check_launch(ctx, "PPE assembly");
+}
+
+lsmps_status assemble_ppe_mixed_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const lsmps_walls& w,
+                                     const lsmps_params& p, const lsmps_csr& fn, const lsmps_csr& wn,
+                                     const lsmps_fluid& tv, const lsmps_walls& tw, const lsmps_moment& vm,
+                                     const lsmps_moment& pm, const lsmps_ppe& ws) {
+  if (ws.matrix.rows < f.count || ws.matrix.cols < f.count || ws.matrix.nnz < f.count + fn.neighbor_count)
+    return fail(ctx, LSMPS_INVALID_ARGUMENT, "PPE matrix workspace is smaller than the requested fluid system");
+  if (f.count == 0) return LSMPS_OK;
+  if (!ws.matrix.row_offsets || !ws.matrix.col_indices || !ws.matrix.values || !ws.rhs || !ws.divergence ||
+      !tv.vx || !tv.vy || !tv.vz)
+    return fail(ctx, LSMPS_INVALID_ARGUMENT, "PPE workspace requires matrix, rhs, divergence and velocity buffers");
+  if (tw.count > 0 && (!tw.vx || !tw.vy || !tw.vz))
+    return fail(ctx, LSMPS_INVALID_ARGUMENT, "PPE RHS assembly requires temporary wall velocity buffers");
+  if (!ctx->mixed_rows[0] || !ctx->mixed_rows[1] || ctx->mixed_cap < f.count)
+    return fail(ctx, LSMPS_NOT_PREPARED, "mixed operator rows were not prepared");
+  PpeArgs a{};
+  a.fluid = f;
+  a.walls = w;
+  a.fo = fn.offsets;
+  a.fi = fn.indices;
+  a.wo = wn.offsets;
+  a.wi = wn.indices;
+  a.tvx = tv.vx;
+  a.tvy = tv.vy;
+  a.tvz = tv.vz;
+  a.twx = tw.vx;
+  a.twy = tw.vy;
+  a.twz = tw.vz;
+  a.vrows = mixed_rows_of(ctx, 0);
+  a.prows = mixed_rows_of(ctx, 1);
+  a.re = pm.support_radius;
+  a.inv_re = 1.0 / pm.support_radius;
+  a.vwall_scale = vm.wall_weight_scale;
+  a.pwall_scale = pm.wall_weight_scale;
+  a.density = p.density;
+  a.dt = p.time_step;
+  a.gx = p.gravity[0];
+  a.gy = p.gravity[1];
+  a.gz = p.gravity[2];
+  a.row_offsets = ws.matrix.row_offsets;
+  a.col = ws.matrix.col_indices;
+  a.val = ws.matrix.values;
+  a.rhs = ws.rhs;
+  a.divergence = ws.divergence;
+  a.wall_rhs_out = ws.pressure_laplacian;
+  const long long rows = static_cast<long long>(f.count);
+  switch (ctx->knob[LSMPS_KNOB_PPE_LANES]) {
+    case 0:
+    case 1: launch_named(ctx, "ppe_lanes_kernel<4, true>", ppe_lanes_kernel<4, true>, dim3(div_up(rows * 4, kThreads)), dim3(kThreads), 0, a); break;
+    case 3: launch_named(ctx, "ppe_lanes_kernel<16, true>", ppe_lanes_kernel<16, true>, dim3(div_up(rows * 16, kThreads)), dim3(kThreads), 0, a); break;
+    default: launch_named(ctx, "ppe_lanes_kernel<8, true>", ppe_lanes_kernel<8, true>, dim3(div_up(rows * 8, kThreads)), dim3(kThreads), 0, a); break;
+  }
+  return check_launch(ctx, "PPE assembly (mixed)");
 }
 
 }  // namespace lsmps

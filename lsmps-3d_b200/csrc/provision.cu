@@ -4,6 +4,7 @@
 // (:178-248), combine_explicit_velocity_kernel (:250-270) and
 // combine_explicit_wall_velocity_kernel (:272-284).
 #include "impl.cuh"
+#include "mixed.cuh"
 #include "packed.cuh"
 
 namespace lsmps {
@@ -57,7 +58,11 @@ __device__ __forceinline__ double lap_from(const double* __restrict__ inv, const
   return 2.0 * second / (re * re);
 }
 
-__global__ void __launch_bounds__(kThreads) laplacian_kernel(LaplacianArgs a) {
+// Mixed (the mixed form): the inverse is replaced by the particle's
+// Laplacian row from the mixed-form operator rows (FP32, or FP64 for the
+// FP64-route particles); the sums are the same FP64 sums.
+template <bool Mixed>
+__global__ void __launch_bounds__(kThreads) laplacian_kernel(LaplacianArgs a, MixedRows rows) {
   const index_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= a.n) return;
   const double4 pi = ld4(a.fp, i);
@@ -87,10 +92,26 @@ __global__ void __launch_bounds__(kThreads) laplacian_kernel(LaplacianArgs a) {
     basis_a_mul(dx, dy, dz, a.inv_re, b);
     acc_rhs(b, w, u.x - ui.x, u.y - ui.y, u.z - ui.z, rx, ry, rz);
   }
-  const double* inv = a.inverse + static_cast<size_t>(i) * 81;
-  a.lx[i] = lap_from(inv, rx, a.re);
-  a.ly[i] = lap_from(inv, ry, a.re);
-  a.lz[i] = lap_from(inv, rz, a.re);
+  if (Mixed) {
+    double l[9];
+    load_row9(rows, i, 0, l);
+    double cx = 0.0, cy = 0.0, cz = 0.0;
+#pragma unroll
+    for (int r = 0; r < 9; ++r) {
+      cx = fma(l[r], rx[r], cx);
+      cy = fma(l[r], ry[r], cy);
+      cz = fma(l[r], rz[r], cz);
+    }
+    const double scale = 2.0 / (a.re * a.re);
+    a.lx[i] = scale * cx;
+    a.ly[i] = scale * cy;
+    a.lz[i] = scale * cz;
+  } else {
+    const double* inv = a.inverse + static_cast<size_t>(i) * 81;
+    a.lx[i] = lap_from(inv, rx, a.re);
+    a.ly[i] = lap_from(inv, ry, a.re);
+    a.lz[i] = lap_from(inv, rz, a.re);
+  }
 }
 
 // combine_explicit_velocity_kernel, explicit_update.cu:250-270
@@ -127,6 +148,28 @@ int pointwise_blocks(lsmps_ctx* ctx, size_t n) {
 
 }  // namespace
 
+lsmps_status velocity_laplacian_mixed_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const lsmps_walls& w,
+                                           const lsmps_csr& fn, const lsmps_csr& wn, const lsmps_moment& vm,
+                                           const lsmps_vector& lap) {
+  if (lap.count < f.count) return fail(ctx, LSMPS_INVALID_ARGUMENT, "Provision laplacian workspace is too small");
+  if (f.count == 0) return LSMPS_OK;
+  if (!lap.x || !lap.y || !lap.z || !f.vx || !f.vy || !f.vz)
+    return fail(ctx, LSMPS_INVALID_ARGUMENT, "Provision buffers missing");
+  if (w.count > 0 && (!w.vx || !w.vy || !w.vz)) return fail(ctx, LSMPS_INVALID_ARGUMENT, "wall velocity missing");
+  if (!ctx->mixed_rows[0] || ctx->mixed_cap < f.count)
+    return fail(ctx, LSMPS_NOT_PREPARED, "mixed velocity operator rows were not prepared");
+  if (!ensure_packs(ctx, f.count, w.count)) return fail(ctx, LSMPS_CUDA_ERROR, "pack allocation failed");
+  pack4(ctx, f.vx, f.vy, f.vz, nullptr, f.count, ctx->pack_fluid[1]);
+  pack4(ctx, w.vx, w.vy, w.vz, nullptr, w.count, ctx->pack_wall[1]);
+  // fluid and wall positions are still packed from the moment stage
+  LaplacianArgs a{static_cast<index_t>(f.count), ctx->pack_fluid[0], ctx->pack_fluid[1], ctx->pack_wall[0],
+                  ctx->pack_wall[1], fn.offsets, fn.indices, wn.offsets, wn.indices, nullptr,
+                  vm.support_radius, 1.0 / vm.support_radius, vm.wall_weight_scale, lap.x, lap.y, lap.z};
+  launch(ctx, laplacian_kernel<true>, dim3(div_up(static_cast<long long>(f.count), kThreads)), dim3(kThreads), 0, a,
+         mixed_rows_of(ctx, 0));
+  return check_launch(ctx, "velocity laplacian (mixed)");
+}
+
 lsmps_status velocity_laplacian_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const lsmps_walls& w,
                                      const lsmps_csr& fn, const lsmps_csr& wn, const lsmps_moment& vm,
                                      const lsmps_vector& lap) {
@@ -145,7 +188,8 @@ lsmps_status velocity_laplacian_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const
   LaplacianArgs a{static_cast<index_t>(f.count), ctx->pack_fluid[0], ctx->pack_fluid[1], ctx->pack_wall[0],
                   ctx->pack_wall[1], fn.offsets, fn.indices, wn.offsets, wn.indices, vm.inverse_matrices,
                   vm.support_radius, 1.0 / vm.support_radius, vm.wall_weight_scale, lap.x, lap.y, lap.z};
-  launch(ctx, laplacian_kernel, dim3(div_up(static_cast<long long>(f.count), kThreads)), dim3(kThreads), 0, a);
+  launch(ctx, laplacian_kernel<false>, dim3(div_up(static_cast<long long>(f.count), kThreads)), dim3(kThreads), 0, a,
+         MixedRows{});
   return check_launch(ctx, "velocity laplacian");
 }
 

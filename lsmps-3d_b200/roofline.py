@@ -56,12 +56,21 @@ def kernel_bytes(nf: int, nw: int, kf: int, kw: int, c: int, s: int = 8) -> dict
     out["moment_a_kernel<V,P>"] = moment_in + 2 * moment_kind_out
     out["moment_a_kernel<V>"] = out["moment_a_kernel<P>"] = moment_in + moment_kind_out
     out["laplacian_kernel"] = rows + 2 * pos_f + 2 * pos_w + 81 * s * nf + 3 * s * nf
-    ppe = (rows + 2 * pos_f + 4 * nf + 3 * pos_w + 2 * 81 * s * nf
-           + 4 * (nf + 1) + (4 + s) * (nf + kf) + 3 * s * nf)
-    for name in ("ppe_kernel", "ppe_lanes_kernel<4>", "ppe_lanes_kernel<8>", "ppe_lanes_kernel<16>"):
-        out[name] = ppe
-    out["gradient_shifting_kernel"] = (rows + 4 * nf + pos_f + 3 * s * nf + 2 * pos_w + 81 * s * nf
-                                       + 6 * s * nf)
+    ppe_common = rows + 2 * pos_f + 4 * nf + 3 * pos_w + 4 * (nf + 1) + (4 + s) * (nf + kf) + 3 * s * nf
+    out["ppe_kernel"] = ppe_common + 2 * 81 * s * nf
+    for g in (4, 8, 16):
+        out[f"ppe_lanes_kernel<{g}, false>"] = ppe_common + 2 * 81 * s * nf
+        # mixed form: the pressure Laplacian row and the three velocity rows, FP32
+        out[f"ppe_lanes_kernel<{g}, true>"] = ppe_common + 36 * 4 * nf
+    grad_common = rows + 4 * nf + pos_f + 3 * s * nf + 2 * pos_w + 6 * s * nf
+    out["gradient_shifting_kernel<false>"] = grad_common + 81 * s * nf
+    out["gradient_shifting_kernel<true>"] = grad_common + 27 * 4 * nf
+    # mixed-form moment stages: FP32 assembly into FP64 monomial totals, then
+    # per kind the FP32 factorisation, refinement and the 36-float rows
+    out["moment_sums_kernel"] = 4 * (nf + 1) + 4 * kf + pos_f + 31 * 8 * nf
+    out["moment_rows_kernel<false>"] = (2 * 31 * 8 * nf + 2 * (4 * (nf + 1) + 4 * kw + pos_f + 2 * pos_w)
+                                        + 2 * (36 * 4 + 2 * s + 4) * nf)
+    out["laplacian_mixed_kernel"] = rows + 2 * pos_f + 2 * pos_w + 9 * 4 * nf + 3 * s * nf
     out["update_anti_penetration_kernel"] = (4 * (nf + 1) + 4 * kw + 4 * nf + 2 * pos_f + 3 * pos_f
                                              + 2 * pos_w + 2 * pos_f)
     out["smooth_kernel"] = 4 * (nf + 1) + 4 * kf + 2 * pos_f + 4 * nf + pos_f

@@ -79,3 +79,26 @@ def vec_err(g: dict, o: dict, comps, extra_scale: dict | None = None):
         arrays += [np.asarray(extra_scale[c]) for c in comps if c in extra_scale]
     scale = max(float(np.max(np.abs(a))) if a.size else 0.0 for a in arrays)
     return {c: rel_err(g[c], o[c], scale=scale if scale > 0 else None) for c in comps}
+
+
+def row_rel_err(values, ref_values, row_offsets):
+    """Row-normwise relative error of a CSR matrix against a reference with
+    the same pattern: max over rows of max_j |a_ij - r_ij| / max_j |r_ij|
+    (rows whose reference is all zero are compared absolutely).  This is the
+    "max relative error in PPE coefficients" the mixed form is held to: each
+    coefficient's error measured against the size of its own row."""
+    v = np.asarray(values, dtype=np.float64)
+    r = np.asarray(ref_values, dtype=np.float64)
+    off = np.asarray(row_offsets, dtype=np.int64)
+    n = off.size - 1
+    if n <= 0:
+        return 0.0
+    d = np.abs(v[: off[-1]] - r[: off[-1]])
+    a = np.abs(r[: off[-1]])
+    lengths = np.diff(off)
+    nz = lengths > 0
+    starts = off[:-1][nz]
+    dmax = np.maximum.reduceat(d, starts)
+    amax = np.maximum.reduceat(a, starts)
+    per_row = np.where(amax > 0, dmax / np.where(amax > 0, amax, 1.0), dmax)
+    return float(per_row.max()) if per_row.size else 0.0

@@ -59,11 +59,11 @@ def test_host_only_entry_points(lib, pkg):
 
 STRUCTS = ["lsmps_fluid", "lsmps_walls", "lsmps_grid", "lsmps_cells", "lsmps_csr", "lsmps_vector",
            "lsmps_surface_diagnostics", "lsmps_moment", "lsmps_csr_matrix", "lsmps_ppe", "lsmps_params",
-           "lsmps_step_state"]
+           "lsmps_step_state", "lsmps_operator_out"]
 PY = {"lsmps_fluid": "Fluid", "lsmps_walls": "Walls", "lsmps_grid": "Grid", "lsmps_cells": "Cells",
       "lsmps_csr": "Csr", "lsmps_vector": "Vector", "lsmps_surface_diagnostics": "SurfaceDiagnostics",
       "lsmps_moment": "Moment", "lsmps_csr_matrix": "CsrMatrix", "lsmps_ppe": "Ppe", "lsmps_params": "Params",
-      "lsmps_step_state": "StepState"}
+      "lsmps_step_state": "StepState", "lsmps_operator_out": "OperatorOut"}
 
 
 def test_struct_layout_matches_header(pkg, tmp_path):

@@ -283,6 +283,32 @@ def test_launch_variants_match_oracle(pkg, device_api, oracle, knob, value):
         assert rel_err(a, b) < 1e-7, k
 
 
+def test_autotune_leaves_state_and_picks_valid_variants(pkg, device_api):
+    case = pkg.cases.dam_break(nx=24, ny=12, nz=24, l0=0.005)
+    p = case.params
+    dev = device_api.device_buffers(case)
+    c = device_api.Context(0)
+    try:
+        c.build_neighbor_lists(dev, p)
+        c.classify_surface(dev, p)
+        c.step(dev, p)
+        before = {k: v.copy() for k, v in dev.numpy("fluid").items()}
+        rows_before = dev.csr_rows("fluid")
+        for prec in (pkg.abi.PRECISION_PLAIN, pkg.abi.PRECISION_MIXED):
+            c.set_precision(prec)
+            tuned = c.autotune(dev, p, repeats=2)
+            lib = device_api._lib
+            for k, (v, ms) in tuned.items():
+                assert 0 <= v < lib.lsmps_knob_variants(k) and ms > 0.0
+        after = dev.numpy("fluid")
+        for k in before:
+            assert np.array_equal(before[k], after[k]), k
+        ro, ri = dev.csr_rows("fluid")
+        assert np.array_equal(ro, rows_before[0]) and np.array_equal(ri, rows_before[1])
+    finally:
+        c.close()
+
+
 def test_knob_arguments_checked(device_api):
     c = device_api.Context(0)
     try:
