@@ -257,11 +257,18 @@ __global__ void __launch_bounds__(kThreads) smooth_kernel(index_t n, const doubl
   const double4 pi = ld4(fp, i);
   double ws = 0.0, ax = 0.0, ay = 0.0, az = 0.0;
   const index_t fe = fo[i + 1];
-  for (index_t o = fo[i]; o < fe; ++o) {
-    const index_t j = fi[o];
-    const double4 u = ld4(fv, j);
+  index_t o = fo[i];
+  index_t jn = o < fe ? fi[o] : i;
+  double4 un = ld4(fv, jn), qn = ld4(fp, jn);
+  for (; o < fe; ++o) {
+    // the next neighbour's records are loaded while this one is summed
+    const double4 u = un, q = qn;
+    if (o + 1 < fe) {
+      jn = fi[o + 1];
+      un = ld4(fv, jn);
+      qn = ld4(fp, jn);
+    }
     if (u.w == kSplash) continue;
-    const double4 q = ld4(fp, j);
     const double dx = q.x - pi.x, dy = q.y - pi.y, dz = q.z - pi.z;
     const double w = correction_weight_mul(sqrt(dx * dx + dy * dy + dz * dz), inv_re);
     if (w <= 0.0) continue;

@@ -453,9 +453,13 @@ __global__ void __launch_bounds__(kMomentThreads, MinBlocks) moment_a_kernel(Mom
   double s[kMonomials];
 #pragma unroll
   for (int e = 0; e < kMonomials; ++e) s[e] = 0.0;
+  // The next neighbour's record is loaded while this one is accumulated.
   const index_t fe = a.fo[i + 1];
-  for (index_t o = a.fo[i]; o < fe; ++o) {
-    const double4 q = ld4(a.fp, a.fi[o]);
+  index_t o = a.fo[i];
+  double4 qn = o < fe ? ld4(a.fp, a.fi[o]) : pi;
+  for (; o < fe; ++o) {
+    const double4 q = qn;
+    if (o + 1 < fe) qn = ld4(a.fp, a.fi[o + 1]);
     const double dx = q.x - pi.x, dy = q.y - pi.y, dz = q.z - pi.z;
     const double d2 = dx * dx + dy * dy + dz * dz;
     if (d2 <= 0.0) continue;
@@ -539,8 +543,10 @@ __global__ void __launch_bounds__(kSumThreads) moment_sums_kernel(MixedSumArgs a
 #pragma unroll
   for (int e = 0; e < kMonomials; ++e) sum[e] = comp[e] = 0.0f;
   const index_t fb = a.fo[i], fe = a.fo[i + 1];
+  double4 qn = fb < fe ? ld4(a.fp, a.fi[fb]) : pi;
   for (index_t o = fb; o < fe; ++o) {
-    const double4 q = ld4(a.fp, a.fi[o]);
+    const double4 q = qn;
+    if (o + 1 < fe) qn = ld4(a.fp, a.fi[o + 1]);
     const float sx = static_cast<float>((q.x - pi.x) * a.inv_re);
     const float sy = static_cast<float>((q.y - pi.y) * a.inv_re);
     const float sz = static_cast<float>((q.z - pi.z) * a.inv_re);

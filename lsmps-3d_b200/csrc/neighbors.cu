@@ -10,7 +10,10 @@
 // memory once, as cell-relative FP32 coordinates, and every warp then tests
 // its home particles against the staged set 32 candidates at a time.  The
 // accepted candidates of one warp step are compacted with a ballot, so a row
-// comes out in exactly the reference's traversal order.
+// comes out in exactly the reference's traversal order.  The count pass keeps
+// the ballots (one 32-bit mask per 32 staged candidates and home particle);
+// after the scan the write pass re-stages only the candidate indices and
+// replays the masks, so the distance tests run once per table.
 //
 // Exactness: the FP32 distance is only a screen.  With coordinates scaled by
 // 1/h and re-centred on the home cell, every component is at most 2 in
@@ -34,6 +37,7 @@ constexpr int kCsrWarps = kCsrThreads / kWarp;
 constexpr int kStageCap = 1024;
 constexpr float kScreenMargin = 1.0e-4f;
 constexpr float kFarLimit = 2.0f;
+constexpr int kMaskWords = kStageCap / 32;
 
 struct CsrArgs {
   const double* fx;
@@ -59,6 +63,10 @@ struct CsrArgs {
   index_t* indices;
   unsigned long long capacity;
   const index_t* total;  // write pass: offsets[N]
+  // Per home particle, one 32-bit accept mask per 32 staged candidates
+  // (bits[i * kMaskWords + chunk]); written by the count pass, replayed by the
+  // write pass.
+  unsigned* bits;
   DeviceStatus* status;
 };
 
@@ -128,18 +136,44 @@ __global__ void __launch_bounds__(kCsrThreads) csr_kernel(CsrArgs a) {
         while (s_pre[t + 1] <= k) ++t;
         const index_t j = a.src_sorted[s_cb[t] + (k - s_pre[t])];
         s_idx[k] = j;
-        s_rel[k] = make_float4(to_rel(a.sx[j], ccx, a.inv_h), to_rel(a.sy[j], ccy, a.inv_h),
-                               to_rel(a.sz[j], ccz, a.inv_h), 0.0f);
+        if (!kWrite)
+          s_rel[k] = make_float4(to_rel(a.sx[j], ccx, a.inv_h), to_rel(a.sy[j], ccy, a.inv_h),
+                                 to_rel(a.sz[j], ccz, a.inv_h), 0.0f);
       }
     }
     __syncthreads();
     for (index_t h = hb + warp; h < he; h += kCsrWarps) {
       const index_t i = a.home_sorted[h];
-      const double xi = a.fx[i], yi = a.fy[i], zi = a.fz[i];
       index_t out = 0;
       if (kWrite) out = a.offsets[i];
       index_t count = 0;
+      if (staged && kWrite) {
+        // Replay the count pass's accept masks: lane c holds chunk c's mask,
+        // an exclusive warp scan of the popcounts gives each chunk's base.
+        const int chunks = (nc + kWarp - 1) / kWarp;
+        const unsigned word = lane < chunks ? a.bits[static_cast<size_t>(i) * kMaskWords + lane] : 0u;
+        const int pc = __popc(word);
+        int incl = pc;
+#pragma unroll
+        for (int d = 1; d < kWarp; d <<= 1) {
+          const int t = __shfl_up_sync(0xffffffffu, incl, d);
+          if (lane >= d) incl += t;
+        }
+        const int base_mine = incl - pc;
+        for (int c = 0; c < chunks; ++c) {
+          const unsigned m = __shfl_sync(0xffffffffu, word, c);
+          const int cb = __shfl_sync(0xffffffffu, base_mine, c);
+          if ((m >> lane) & 1u) {
+            const unsigned long long pos =
+                static_cast<unsigned long long>(out) + cb + __popc(m & lanemask_lt);
+            if (pos < a.capacity) a.indices[pos] = s_idx[c * kWarp + lane];
+          }
+        }
+        continue;
+      }
+      const double xi = a.fx[i], yi = a.fy[i], zi = a.fz[i];
       if (staged) {
+        unsigned my_mask = 0u;  // lane c keeps chunk c's accept mask
         const float rx = to_rel(xi, ccx, a.inv_h), ry = to_rel(yi, ccy, a.inv_h), rz = to_rel(zi, ccz, a.inv_h);
         for (index_t base = 0; base < nc; base += kWarp) {
           const index_t k = base + lane;
@@ -159,16 +193,10 @@ __global__ void __launch_bounds__(kCsrThreads) csr_kernel(CsrArgs a) {
             }
           }
           const unsigned m = __ballot_sync(0xffffffffu, pass);
-          if (kWrite) {
-            if (pass) {
-              const unsigned long long pos = static_cast<unsigned long long>(out) + __popc(m & lanemask_lt);
-              if (pos < a.capacity) a.indices[pos] = j;
-            }
-            out += __popc(m);
-          } else {
-            count += __popc(m);
-          }
+          if (lane == base / kWarp) my_mask = m;
+          count += __popc(m);
         }
+        if (lane < (nc + kWarp - 1) / kWarp) a.bits[static_cast<size_t>(i) * kMaskWords + lane] = my_mask;
       } else {
         // More candidates than the stage holds (overloaded edge cells):
         // exact tests straight from global memory, same order.
@@ -204,7 +232,8 @@ __global__ void __launch_bounds__(kCsrThreads) csr_kernel(CsrArgs a) {
 
 lsmps_status one_neighbor_list(lsmps_ctx* ctx, Scratch& scratch, const lsmps_fluid& fluid, const double* sx,
                                const double* sy, const double* sz, const lsmps_cells& home, const lsmps_cells& src,
-                               const lsmps_grid& grid, double radius, bool exclude_self, const lsmps_csr& out) {
+                               const lsmps_grid& grid, double radius, bool exclude_self, const lsmps_csr& out,
+                               unsigned* bits) {
   if (fluid.count > out.particle_count || !out.offsets)
     return fail(ctx, LSMPS_INVALID_ARGUMENT, "Neighbor list particle capacity is smaller than fluid count");
   const size_t n = fluid.count;
@@ -233,6 +262,7 @@ lsmps_status one_neighbor_list(lsmps_ctx* ctx, Scratch& scratch, const lsmps_flu
   a.indices = out.indices;
   a.capacity = out.neighbor_count;
   a.total = out.offsets + n;
+  a.bits = bits;
   a.status = ctx->d_status;
   const int blocks = static_cast<int>(std::min<long long>(a.ncell, static_cast<long long>(ctx->sm_count) * 16));
   if (n) launch(ctx, csr_kernel<false>, dim3(blocks), dim3(kCsrThreads), 0, a);
@@ -246,7 +276,8 @@ lsmps_status one_neighbor_list(lsmps_ctx* ctx, Scratch& scratch, const lsmps_flu
 
 size_t neighbor_scratch_bytes(size_t n_fluid, size_t n_wall, size_t ncell) {
   const size_t nmax = n_fluid > n_wall ? n_fluid : n_wall;
-  return 2 * cell_list_scratch_bytes(nmax, ncell) + 2 * scan_scratch_bytes(n_fluid + 1) + 4096;
+  return 2 * cell_list_scratch_bytes(nmax, ncell) + 2 * scan_scratch_bytes(n_fluid + 1) +
+         n_fluid * kMaskWords * sizeof(unsigned) + 4096;
 }
 
 lsmps_status build_neighbor_lists_impl(lsmps_ctx* ctx, Scratch& scratch, const lsmps_fluid& fluid,
@@ -256,12 +287,15 @@ lsmps_status build_neighbor_lists_impl(lsmps_ctx* ctx, Scratch& scratch, const l
   if (!(radius > 0.0)) return fail(ctx, LSMPS_INVALID_ARGUMENT, "Neighbor search radius must be positive");
   if (radius > p.grid.cell_size)
     return fail(ctx, LSMPS_INVALID_ARGUMENT, "Neighbor search currently requires radius <= cell_size");
+  unsigned* bits = scratch.take<unsigned>(fluid.count * kMaskWords + 1);
+  if (!bits) return fail(ctx, LSMPS_CUDA_ERROR, "neighbour scratch exhausted");
   lsmps_status st = build_cell_list_impl(ctx, scratch, fluid.x, fluid.y, fluid.z, fluid.count, p.grid, fc);
   if (!st) st = build_cell_list_impl(ctx, scratch, walls.x, walls.y, walls.z, walls.count, p.grid, wc);
+  // the two tables run one after the other on the stream and share the masks
   if (!st)
-    st = one_neighbor_list(ctx, scratch, fluid, fluid.x, fluid.y, fluid.z, fc, fc, p.grid, radius, true, fn);
+    st = one_neighbor_list(ctx, scratch, fluid, fluid.x, fluid.y, fluid.z, fc, fc, p.grid, radius, true, fn, bits);
   if (!st)
-    st = one_neighbor_list(ctx, scratch, fluid, walls.x, walls.y, walls.z, fc, wc, p.grid, radius, false, wn);
+    st = one_neighbor_list(ctx, scratch, fluid, walls.x, walls.y, walls.z, fc, wc, p.grid, radius, false, wn, bits);
   return st;
 }
 

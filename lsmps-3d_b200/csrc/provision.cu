@@ -71,10 +71,17 @@ __global__ void __launch_bounds__(kThreads) laplacian_kernel(LaplacianArgs a, Mi
 #pragma unroll
   for (int r = 0; r < 9; ++r) rx[r] = ry[r] = rz[r] = 0.0;
   const index_t fe = a.fo[i + 1];
-  for (index_t o = a.fo[i]; o < fe; ++o) {
-    const index_t j = a.fi[o];
-    const double4 q = ld4(a.fp, j);
-    const double4 u = ld4(a.fv, j);
+  index_t o = a.fo[i];
+  index_t jn = o < fe ? a.fi[o] : i;
+  double4 qn = ld4(a.fp, jn), un = ld4(a.fv, jn);
+  for (; o < fe; ++o) {
+    // the next neighbour's records are loaded while this one is summed
+    const double4 q = qn, u = un;
+    if (o + 1 < fe) {
+      jn = a.fi[o + 1];
+      qn = ld4(a.fp, jn);
+      un = ld4(a.fv, jn);
+    }
     const double dx = q.x - pi.x, dy = q.y - pi.y, dz = q.z - pi.z;
     const double w = lin_weight_mul(sqrt(dx * dx + dy * dy + dz * dz), a.inv_re);
     if (w <= 0.0) continue;
