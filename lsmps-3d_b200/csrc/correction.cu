@@ -40,6 +40,11 @@ struct GatherArgs {
   const index_t* wo;
   const index_t* wi;
   lsmps_params p;
+  // 32-byte records of the fused gradient/shifting kernel: fluid
+  // {x, y, z, pressure}, walls {x, y, z, -} and {nx, ny, nz, -}.
+  const double4* fpp = nullptr;
+  const double4* wp = nullptr;
+  const double4* wn = nullptr;
 };
 
 // compute_pressure_gradient_kernel, pressure_correction.cu:200-276
@@ -436,10 +441,8 @@ __global__ void __launch_bounds__(kThreads) gradient_shifting_kernel(GatherArgs 
     sx_out[i] = sy_out[i] = sz_out[i] = 0.0;
     return;
   }
-  const double* __restrict__ fx = a.fluid.x;
-  const double* __restrict__ fy = a.fluid.y;
-  const double* __restrict__ fz = a.fluid.z;
-  const double xi = fx[i], yi = fy[i], zi = fz[i];
+  const double4 own = ld4(a.fpp, i);
+  const double xi = own.x, yi = own.y, zi = own.z;
   const double inv_re = 1.0 / re;
   const double dmin = a.p.ps_min_distance_ratio * a.p.particle_spacing;
   const double scale = a.p.ps_displacement_scale;
@@ -447,16 +450,22 @@ __global__ void __launch_bounds__(kThreads) gradient_shifting_kernel(GatherArgs 
 #pragma unroll
   for (int r = 0; r < 9; ++r) rhs[r] = 0.0;
   double shx = 0.0, shy = 0.0, shz = 0.0, nx = 0.0, ny = 0.0, nz = 0.0;
+  // {x, y, z, raw pressure} of the neighbours, packed before the launch (the
+  // clamp is applied on read, as for every pressure this kernel reads); the
+  // next record is loaded while this one is used.
   const index_t fe = a.fo[i + 1];
-  for (index_t o = a.fo[i]; o < fe; ++o) {
-    const index_t j = a.fi[o];
-    const double dx = fx[j] - xi, dy = fy[j] - yi, dz = fz[j] - zi;
+  index_t o = a.fo[i];
+  double4 qn = ld4(a.fpp, o < fe ? a.fi[o] : i);
+  for (; o < fe; ++o) {
+    const double4 q = qn;
+    if (o + 1 < fe) qn = ld4(a.fpp, a.fi[o + 1]);
+    const double dx = q.x - xi, dy = q.y - yi, dz = q.z - zi;
     const double d = sqrt(dx * dx + dy * dy + dz * dz);
     if (do_grad) {
       const double w = correction_weight_mul(d, inv_re);
       if (w > 0.0) {
         basis_a_mul(dx, dy, dz, inv_re, b);
-        const double pj = pressure[j];
+        const double pj = q.w;
         const double dp = (pj < 0.0 ? 0.0 : pj) - pi;
 #pragma unroll
         for (int r = 0; r < 9; ++r) rhs[r] = fma(w * b[r], dp, rhs[r]);
@@ -476,9 +485,10 @@ __global__ void __launch_bounds__(kThreads) gradient_shifting_kernel(GatherArgs 
   const index_t we = a.wo[i + 1];
   for (index_t o = a.wo[i]; o < we; ++o) {
     const index_t j = a.wi[o];
-    const double dx = a.walls.x[j] - xi, dy = a.walls.y[j] - yi, dz = a.walls.z[j] - zi;
+    const double4 q = ld4(a.wp, j), nrm = ld4(a.wn, j);
+    const double dx = q.x - xi, dy = q.y - yi, dz = q.z - zi;
     const double d = sqrt(dx * dx + dy * dy + dz * dz);
-    const double wnx = a.walls.normal_x[j], wny = a.walls.normal_y[j], wnz = a.walls.normal_z[j];
+    const double wnx = nrm.x, wny = nrm.y, wnz = nrm.z;
     if (do_grad) {
       const double w = wall_scale * correction_weight_mul(d, inv_re);
       if (w > 0.0) {
@@ -624,6 +634,13 @@ lsmps_status pressure_correction_impl(lsmps_ctx* ctx, const lsmps_fluid& f, cons
     return fail(ctx, LSMPS_NOT_PREPARED, "Pressure correction requires a prepared pressure Type-A moment matrix");
   if (f.count == 0) return LSMPS_OK;
   GatherArgs a{f, w, fn.offsets, fn.indices, wn.offsets, wn.indices, p};
+  if (!ensure_packs(ctx, f.count, w.count)) return fail(ctx, LSMPS_CUDA_ERROR, "pack allocation failed");
+  pack4(ctx, f.x, f.y, f.z, pressure, f.count, ctx->pack_fluid[0]);
+  pack4(ctx, w.x, w.y, w.z, nullptr, w.count, ctx->pack_wall[0]);
+  pack4(ctx, w.normal_x, w.normal_y, w.normal_z, nullptr, w.count, ctx->pack_wall[2]);
+  a.fpp = ctx->pack_fluid[0];
+  a.wp = ctx->pack_wall[0];
+  a.wn = ctx->pack_wall[2];
   const int blocks = div_up(static_cast<long long>(f.count), kThreads);
   if (mixed) {
     if (!ctx->mixed_rows[1] || ctx->mixed_cap < f.count)

@@ -601,6 +601,31 @@ __device__ __forceinline__ void chol_solve(const T (&l)[45], const T (&dinv)[9],
   }
 }
 
+// The same for G right-hand sides at once (independent chains interleaved).
+template <typename T, int G>
+__device__ __forceinline__ void chol_solve_group(const T (&l)[45], const T (&dinv)[9], T (&v)[G][9]) {
+#pragma unroll
+  for (int r = 0; r < 9; ++r) {
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+      T t = v[g][r];
+#pragma unroll
+      for (int k = 0; k < r; ++k) t = fma(-l[tri(r, k)], v[g][k], t);
+      v[g][r] = t * dinv[r];
+    }
+  }
+#pragma unroll
+  for (int r = 8; r >= 0; --r) {
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+      T t = v[g][r];
+#pragma unroll
+      for (int k = r + 1; k < 9; ++k) t = fma(-l[tri(k, r)], v[g][k], t);
+      v[g][r] = t * dinv[r];
+    }
+  }
+}
+
 // Target t of the row set: t = 0 the Laplacian row (e3 + e4 + e5), t = 1..3
 // rows 0..2; with Full, t = 0..8 is e_t.
 template <bool Full>
@@ -722,29 +747,43 @@ __global__ void __launch_bounds__(kRowThreads, 6) moment_rows_kernel(MixedRowArg
     for (int r = 0; r < 9; ++r) dinv[r] = 1.0f / l[tri(r, r)];
   }
   if (!fp64) {
-    for (int t = 0; t < kTargets; ++t) {
-      float y0[9];
+    // The targets are solved in groups of kGroup so that their independent
+    // substitution chains interleave.
+    constexpr int kGroup = Full ? 3 : 2;  // divides kTargets
+    static_assert(kTargets % kGroup == 0, "target groups must tile the targets");
+    for (int t0 = 0; t0 < kTargets; t0 += kGroup) {
+      float y0[kGroup][9], d[kGroup][9];
 #pragma unroll
-      for (int r = 0; r < 9; ++r) y0[r] = static_cast<float>(target<Full>(t, r));
-      chol_solve(l, dinv, y0);
-      // one refinement step: residual against the FP64 matrix, correction
-      // through the FP32 factor
-      float d[9];
+      for (int g = 0; g < kGroup; ++g) {
+#pragma unroll
+        for (int r = 0; r < 9; ++r) y0[g][r] = static_cast<float>(target<Full>(t0 + g, r));
+      }
+      chol_solve_group(l, dinv, y0);
+      // one refinement step: residual against the FP64 matrix (each entry
+      // read once for the group), correction through the FP32 factor
 #pragma unroll
       for (int r = 0; r < 9; ++r) {
-        double res = target<Full>(t, r);
+        double res[kGroup];
+#pragma unroll
+        for (int g = 0; g < kGroup; ++g) res[g] = target<Full>(t0 + g, r);
 #pragma unroll
         for (int c = 0; c < 9; ++c) {
           const int e = r >= c ? tri(r, c) : tri(c, r);
-          res = fma(-m[e * kRowThreads], static_cast<double>(y0[c]), res);
-        }
-        d[r] = static_cast<float>(res);
-      }
-      chol_solve(l, dinv, d);
-      double y[9];
+          const double mv = m[e * kRowThreads];
 #pragma unroll
-      for (int r = 0; r < 9; ++r) y[r] = static_cast<double>(y0[r]) + static_cast<double>(d[r]);
-      store_target<Full>(a, kind, i, t, y, false);
+          for (int g = 0; g < kGroup; ++g) res[g] = fma(-mv, static_cast<double>(y0[g][c]), res[g]);
+        }
+#pragma unroll
+        for (int g = 0; g < kGroup; ++g) d[g][r] = static_cast<float>(res[g]);
+      }
+      chol_solve_group(l, dinv, d);
+#pragma unroll
+      for (int g = 0; g < kGroup; ++g) {
+        double y[9];
+#pragma unroll
+        for (int r = 0; r < 9; ++r) y[r] = static_cast<double>(y0[g][r]) + static_cast<double>(d[g][r]);
+        store_target<Full>(a, kind, i, t0 + g, y, false);
+      }
     }
     ko.trace[i] = trace;
     ko.reg[i] = reg;

@@ -7,6 +7,7 @@
 // Dirichlet rows: diagonal 1, neighbour slots 0, rhs 0 (:124-131, :262-276).
 #include "impl.cuh"
 #include "mixed.cuh"
+#include "packed.cuh"
 
 namespace lsmps {
 namespace {
@@ -45,6 +46,14 @@ struct PpeArgs {
   // velocity and pressure inverses, in place of vinv / pinv.
   MixedRows vrows;
   MixedRows prows;
+  // 32-byte neighbour records (packed.cuh) for the lane kernels: fluid
+  // {x, y, z, -} and {u*x, u*y, u*z, -}; walls {x, y, z, -},
+  // {u*x, u*y, u*z, -} and {nx, ny, nz, -}.
+  const double4* fp;
+  const double4* fu;
+  const double4* wp;
+  const double4* wu;
+  const double4* wn;
 };
 
 __device__ __forceinline__ double dot9(const double a[9], const double b[9]) {
@@ -169,7 +178,7 @@ __device__ __forceinline__ double group_sum(double v, unsigned mask) {
 // diagonal (minus the sum of the off-diagonal values) and the RHS sums stay
 // FP64.
 template <int G, bool Mixed>
-__global__ void __launch_bounds__(kThreads) ppe_lanes_kernel(PpeArgs a) {
+__global__ void __launch_bounds__(kThreads, 4) ppe_lanes_kernel(PpeArgs a) {
   const index_t i = (blockIdx.x * blockDim.x + threadIdx.x) / G;
   const int l = threadIdx.x & (G - 1);
   const index_t n = static_cast<index_t>(a.fluid.count);
@@ -196,10 +205,8 @@ __global__ void __launch_bounds__(kThreads) ppe_lanes_kernel(PpeArgs a) {
     }
     return;
   }
-  const double* __restrict__ fx = a.fluid.x;
-  const double* __restrict__ fy = a.fluid.y;
-  const double* __restrict__ fz = a.fluid.z;
-  const double xi = fx[i], yi = fy[i], zi = fz[i];
+  const double4 pi = ld4(a.fp, i);
+  const double xi = pi.x, yi = pi.y, zi = pi.z;
   double L[9];
   if (Mixed) {
     load_row9(a.prows, i, 0, L);
@@ -214,16 +221,26 @@ __global__ void __launch_bounds__(kThreads) ppe_lanes_kernel(PpeArgs a) {
 #pragma unroll
   for (int r = 0; r < 9; ++r) rx[r] = ry[r] = rz[r] = 0.0;
   double diag = 0.0;
-  for (index_t o = nb + l; o < ne; o += G) {
-    const index_t j = a.fi[o];
-    const double dx = fx[j] - xi, dy = fy[j] - yi, dz = fz[j] - zi;
+  // Each lane loads its next neighbour's records while it works on this one.
+  index_t o = nb + l;
+  index_t jn = o < ne ? a.fi[o] : i;
+  double4 qn = ld4(a.fp, jn), un = ld4(a.fu, jn);
+  for (; o < ne; o += G) {
+    const index_t j = jn;
+    const double4 q = qn, u = un;
+    if (o + G < ne) {
+      jn = a.fi[o + G];
+      qn = ld4(a.fp, jn);
+      un = ld4(a.fu, jn);
+    }
+    const double dx = q.x - xi, dy = q.y - yi, dz = q.z - zi;
     const double w = lin_weight_mul(sqrt(dx * dx + dy * dy + dz * dz), a.inv_re);
     double off = 0.0;
     if (w > 0.0) {
       basis_a_mul(dx, dy, dz, a.inv_re, b);
       off = w * dot9(L, b) * scale;
       diag -= off;
-      acc_rhs(b, w, a.tvx[j] - uxi, a.tvy[j] - uyi, a.tvz[j] - uzi, rx, ry, rz);
+      acc_rhs(b, w, u.x - uxi, u.y - uyi, u.z - uzi, rx, ry, rz);
     }
     a.col[row + 1 + o - nb] = j;
     a.val[row + 1 + o - nb] = off;
@@ -232,16 +249,17 @@ __global__ void __launch_bounds__(kThreads) ppe_lanes_kernel(PpeArgs a) {
   const index_t we = a.wo[i + 1];
   for (index_t o = a.wo[i] + l; o < we; o += G) {
     const index_t j = a.wi[o];
-    const double dx = a.walls.x[j] - xi, dy = a.walls.y[j] - yi, dz = a.walls.z[j] - zi;
+    const double4 q = ld4(a.wp, j), u = ld4(a.wu, j), nrm = ld4(a.wn, j);
+    const double dx = q.x - xi, dy = q.y - yi, dz = q.z - zi;
     const double bw = lin_weight_mul(sqrt(dx * dx + dy * dy + dz * dz), a.inv_re);
     if (bw <= 0.0) continue;
     basis_a_mul(dx, dy, dz, a.inv_re, b);
-    acc_rhs(b, a.vwall_scale * bw, a.twx[j] - uxi, a.twy[j] - uyi, a.twz[j] - uzi, rx, ry, rz);
-    const double nx = a.walls.normal_x[j], ny = a.walls.normal_y[j], nz = a.walls.normal_z[j];
+    acc_rhs(b, a.vwall_scale * bw, u.x - uxi, u.y - uyi, u.z - uzi, rx, ry, rz);
+    const double nx = nrm.x, ny = nrm.y, nz = nrm.z;
     const double ng = a.gx * nx + a.gy * ny + a.gz * nz;
-    double q[9];
-    neumann_a(dx, dy, dz, nx, ny, nz, a.inv_re, q);
-    wall_rhs += 2.0 * a.pwall_scale * bw * ng * dot9(L, q) * a.inv_re;
+    double qn9[9];
+    neumann_a(dx, dy, dz, nx, ny, nz, a.inv_re, qn9);
+    wall_rhs += 2.0 * a.pwall_scale * bw * ng * dot9(L, qn9) * a.inv_re;
   }
   const unsigned mask = ((G == 32) ? 0xffffffffu : ((1u << G) - 1u)) << ((threadIdx.x & (kWarp - 1)) & ~(G - 1));
   diag = group_sum<G>(diag, mask);
@@ -275,6 +293,24 @@ __global__ void __launch_bounds__(kThreads) ppe_lanes_kernel(PpeArgs a) {
   a.divergence[i] = div;
   a.rhs[i] = div / a.dt - wall_rhs;
   if (a.wall_rhs_out) a.wall_rhs_out[i] = wall_rhs;
+}
+
+// Neighbour records of the lane kernels: positions and u* of the fluid,
+// positions, u* and normals of the walls.
+bool pack_ppe(lsmps_ctx* ctx, const lsmps_fluid& f, const lsmps_walls& w, const lsmps_fluid& tv,
+              const lsmps_walls& tw, PpeArgs& a) {
+  if (!ensure_packs(ctx, f.count, w.count)) return false;
+  pack4(ctx, f.x, f.y, f.z, nullptr, f.count, ctx->pack_fluid[0]);
+  pack4(ctx, tv.vx, tv.vy, tv.vz, nullptr, f.count, ctx->pack_fluid[1]);
+  pack4(ctx, w.x, w.y, w.z, nullptr, w.count, ctx->pack_wall[0]);
+  pack4(ctx, tw.vx, tw.vy, tw.vz, nullptr, w.count, ctx->pack_wall[1]);
+  pack4(ctx, w.normal_x, w.normal_y, w.normal_z, nullptr, w.count, ctx->pack_wall[2]);
+  a.fp = ctx->pack_fluid[0];
+  a.fu = ctx->pack_fluid[1];
+  a.wp = ctx->pack_wall[0];
+  a.wu = ctx->pack_wall[1];
+  a.wn = ctx->pack_wall[2];
+  return true;
 }
 
 }  // namespace
@@ -327,6 +363,8 @@ lsmps_status assemble_ppe_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const lsmps
   a.rhs = ws.rhs;
   a.divergence = ws.divergence;
   a.wall_rhs_out = ws.pressure_laplacian;
+  if (ctx->knob[LSMPS_KNOB_PPE_LANES] != 0 && !pack_ppe(ctx, f, w, tv, tw, a))
+    return fail(ctx, LSMPS_CUDA_ERROR, "pack allocation failed");
   const long long rows = static_cast<long long>(f.count);
   switch (ctx->knob[LSMPS_KNOB_PPE_LANES]) {
     case 1: launch_named(ctx, "ppe_lanes_kernel<4, false>", ppe_lanes_kernel<4, false>, dim3(div_up(rows * 4, kThreads)), dim3(kThreads), 0, a); break;
@@ -381,6 +419,7 @@ lsmps_status assemble_ppe_mixed_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const
   a.rhs = ws.rhs;
   a.divergence = ws.divergence;
   a.wall_rhs_out = ws.pressure_laplacian;
+  if (!pack_ppe(ctx, f, w, tv, tw, a)) return fail(ctx, LSMPS_CUDA_ERROR, "pack allocation failed");
   const long long rows = static_cast<long long>(f.count);
   switch (ctx->knob[LSMPS_KNOB_PPE_LANES]) {
     case 0:
