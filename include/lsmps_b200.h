@@ -297,7 +297,7 @@ typedef enum lsmps_knob {
   /* moment kernel register budget: 0 = compiler's choice, 1 = capped for 8
    * blocks per SM (default) */
   LSMPS_KNOB_MOMENT_OCCUPANCY = 0,
-  /* lanes cooperating on one PPE row: 0 -> 1, 1 -> 4, 2 -> 8 (default),
+  /* lanes cooperating on one PPE row: 0 -> 1, 1 -> 4 (default), 2 -> 8,
    * 3 -> 16 */
   LSMPS_KNOB_PPE_LANES = 1,
   LSMPS_KNOB_COUNT = 2

@@ -129,7 +129,7 @@ struct lsmps_ctx {
   std::vector<ProfileRecord> profile;
   size_t profile_used = 0;
   // Launch-shape knobs (lsmps_knob).
-  int knob[LSMPS_KNOB_COUNT] = {1, 2};
+  int knob[LSMPS_KNOB_COUNT] = {1, 1};
   // 32-byte neighbour records (packed.cuh): two fluid and three wall arrays.
   double4* pack_fluid[2] = {nullptr, nullptr};
   double4* pack_wall[3] = {nullptr, nullptr, nullptr};

@@ -142,6 +142,66 @@ __global__ void __launch_bounds__(kCsrThreads) csr_kernel(CsrArgs a) {
       }
     }
     __syncthreads();
+    if (!kWrite && staged) {
+      // Count pass over the staged set: each warp tests two home particles
+      // per staged chunk (one shared-memory read of the candidate for both).
+      for (index_t h = hb + 2 * warp; h < he; h += 2 * kCsrWarps) {
+        const bool two = h + 1 < he;
+        const index_t i0 = a.home_sorted[h];
+        const index_t i1 = two ? a.home_sorted[h + 1] : i0;
+        const double x0 = a.fx[i0], y0 = a.fy[i0], z0 = a.fz[i0];
+        const double x1 = a.fx[i1], y1 = a.fy[i1], z1 = a.fz[i1];
+        const float r0x = to_rel(x0, ccx, a.inv_h), r0y = to_rel(y0, ccy, a.inv_h), r0z = to_rel(z0, ccz, a.inv_h);
+        const float r1x = to_rel(x1, ccx, a.inv_h), r1y = to_rel(y1, ccy, a.inv_h), r1z = to_rel(z1, ccz, a.inv_h);
+        unsigned keep0 = 0u, keep1 = 0u;  // lane c keeps chunk c's masks
+        index_t count0 = 0, count1 = 0;
+        for (index_t base = 0; base < nc; base += kWarp) {
+          const index_t k = base + lane;
+          bool pass0 = false, pass1 = false;
+          if (k < nc) {
+            const index_t j = s_idx[k];
+            const float4 q = s_rel[k];
+            if (!(a.exclude_self && j == i0)) {
+              const float dx = r0x - q.x, dy = r0y - q.y, dz = r0z - q.z;
+              const float d2 = dx * dx + dy * dy + dz * dz;
+              if (d2 < a.lo2) {
+                pass0 = true;
+              } else if (!(d2 > a.hi2)) {  // near the boundary, or NaN (far)
+                pass0 = within_radius(x0, y0, z0, a.sx[j], a.sy[j], a.sz[j], a.r2);
+              }
+            }
+            if (two && !(a.exclude_self && j == i1)) {
+              const float dx = r1x - q.x, dy = r1y - q.y, dz = r1z - q.z;
+              const float d2 = dx * dx + dy * dy + dz * dz;
+              if (d2 < a.lo2) {
+                pass1 = true;
+              } else if (!(d2 > a.hi2)) {
+                pass1 = within_radius(x1, y1, z1, a.sx[j], a.sy[j], a.sz[j], a.r2);
+              }
+            }
+          }
+          const unsigned m0 = __ballot_sync(0xffffffffu, pass0);
+          const unsigned m1 = __ballot_sync(0xffffffffu, pass1);
+          if (lane == base / kWarp) {
+            keep0 = m0;
+            keep1 = m1;
+          }
+          count0 += __popc(m0);
+          count1 += __popc(m1);
+        }
+        const int chunks = (nc + kWarp - 1) / kWarp;
+        if (lane < chunks) {
+          a.bits[static_cast<size_t>(i0) * kMaskWords + lane] = keep0;
+          if (two) a.bits[static_cast<size_t>(i1) * kMaskWords + lane] = keep1;
+        }
+        if (lane == 0) {
+          a.offsets[i0] = count0;
+          if (two) a.offsets[i1] = count1;
+        }
+      }
+      __syncthreads();
+      continue;
+    }
     for (index_t h = hb + warp; h < he; h += kCsrWarps) {
       const index_t i = a.home_sorted[h];
       index_t out = 0;

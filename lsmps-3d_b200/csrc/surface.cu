@@ -9,6 +9,7 @@
 #include <cmath>
 
 #include "impl.cuh"
+#include "packed.cuh"
 
 namespace lsmps {
 namespace {
@@ -66,30 +67,36 @@ struct SurfaceArgs {
   lsmps_params p;
   double n0;
   lsmps_surface_diagnostics diag;
+  // 32-byte records (packed.cuh): fluid {x, y, z, -}, walls {x, y, z, -} and
+  // {nx, ny, nz, -}.
+  const double4* fp;
+  const double4* wp;
+  const double4* wn;
 };
 
 __global__ void __launch_bounds__(kSurfaceThreads) classify_kernel(SurfaceArgs a) {
   const index_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= static_cast<index_t>(a.fluid.count)) return;
-  const double* __restrict__ fx = a.fluid.x;
-  const double* __restrict__ fy = a.fluid.y;
-  const double* __restrict__ fz = a.fluid.z;
   const index_t fb = a.fo[i], fe = a.fo[i + 1];
   const index_t wb = a.wo[i], we = a.wo[i + 1];
   const index_t fcount = fe - fb, wcount = we - wb;
   const index_t cls = a.p.include_wall_neighbors ? fcount + wcount : fcount;
   const double re = a.p.support_radius;
-  const double px = fx[i], py = fy[i], pz = fz[i];
+  const double4 own = ld4(a.fp, i);
+  const double px = own.x, py = own.y, pz = own.z;
   double nd = 0.0, sx = 0.0, sy = 0.0, sz = 0.0;
   int weighted = 0;
+  // the next neighbour's record is loaded while this one is accumulated
+  double4 qn = ld4(a.fp, fb < fe ? a.fi[fb] : i);
   for (index_t o = fb; o < fe; ++o) {
-    const index_t j = a.fi[o];
-    accumulate(fx[j] - px, fy[j] - py, fz[j] - pz, re, nd, sx, sy, sz, weighted);
+    const double4 q = qn;
+    if (o + 1 < fe) qn = ld4(a.fp, a.fi[o + 1]);
+    accumulate(q.x - px, q.y - py, q.z - pz, re, nd, sx, sy, sz, weighted);
   }
   if (a.p.include_wall_neighbors) {
     for (index_t o = wb; o < we; ++o) {
-      const index_t j = a.wi[o];
-      accumulate(a.walls.x[j] - px, a.walls.y[j] - py, a.walls.z[j] - pz, re, nd, sx, sy, sz, weighted);
+      const double4 q = ld4(a.wp, a.wi[o]);
+      accumulate(q.x - px, q.y - py, q.z - pz, re, nd, sx, sy, sz, weighted);
     }
   }
   double aniso = 0.0;
@@ -104,12 +111,14 @@ __global__ void __launch_bounds__(kSurfaceThreads) classify_kernel(SurfaceArgs a
     basis.count = 0;
     for (index_t o = wb; o < we; ++o) {
       const index_t j = a.wi[o];
-      const double dx = a.walls.x[j] - px, dy = a.walls.y[j] - py, dz = a.walls.z[j] - pz;
+      const double4 q = ld4(a.wp, j);
+      const double dx = q.x - px, dy = q.y - py, dz = q.z - pz;
       const double d2 = dx * dx + dy * dy + dz * dz;
       if (d2 <= 0.0) continue;
       const double d = sqrt(d2);
       if (lin_weight(d, re) <= 0.0) continue;
-      const double nx = a.walls.normal_x[j], ny = a.walls.normal_y[j], nz = a.walls.normal_z[j];
+      const double4 nrm = ld4(a.wn, j);
+      const double nx = nrm.x, ny = nrm.y, nz = nrm.z;
       const double nl2 = nx * nx + ny * ny + nz * nz;
       if (nl2 <= 0.0) continue;
       const double inv = safe_rsqrt(nl2);
@@ -161,18 +170,19 @@ __global__ void __launch_bounds__(kSurfaceThreads) classify_kernel(SurfaceArgs a
 
 // expand_near_surface_kernel, surface_detection.cu:322-348.  Only Inner rows
 // are written and only Surface labels are read, so the pass is race-free.
-__global__ void __launch_bounds__(kSurfaceThreads) expand_kernel(const double* __restrict__ fx,
-                                                                 const double* __restrict__ fy,
-                                                                 const double* __restrict__ fz, int32_t* type,
+// Reads the 4-byte label of each neighbour first; positions are read only
+// for the (few) Surface neighbours.
+__global__ void __launch_bounds__(kSurfaceThreads) expand_kernel(const double4* __restrict__ fp, int32_t* type,
                                                                  index_t n, const index_t* __restrict__ fo,
                                                                  const index_t* __restrict__ fi, double r2) {
   const index_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n || type[i] != LSMPS_SURFACE_INNER) return;
-  const double px = fx[i], py = fy[i], pz = fz[i];
+  const double4 own = ld4(fp, i);
   for (index_t o = fo[i]; o < fo[i + 1]; ++o) {
     const index_t j = fi[o];
     if (type[j] != LSMPS_SURFACE_SURFACE) continue;
-    const double dx = fx[j] - px, dy = fy[j] - py, dz = fz[j] - pz;
+    const double4 q = ld4(fp, j);
+    const double dx = q.x - own.x, dy = q.y - own.y, dz = q.z - own.z;
     if (dx * dx + dy * dy + dz * dz <= r2) {
       type[i] = LSMPS_SURFACE_NEAR_SURFACE;
       return;
@@ -220,13 +230,21 @@ lsmps_status classify_surface_impl(lsmps_ctx* ctx, const lsmps_fluid& fluid, con
   a.p = p;
   a.n0 = n0;
   if (diag) a.diag = *diag;
+  if (!ensure_packs(ctx, fluid.count, walls.count)) return fail(ctx, LSMPS_CUDA_ERROR, "pack allocation failed");
+  pack4(ctx, fluid.x, fluid.y, fluid.z, nullptr, fluid.count, ctx->pack_fluid[0]);
+  pack4(ctx, walls.x, walls.y, walls.z, nullptr, walls.count, ctx->pack_wall[0]);
+  pack4(ctx, walls.normal_x, walls.normal_y, walls.normal_z, nullptr, walls.count, ctx->pack_wall[2]);
+  a.fp = ctx->pack_fluid[0];
+  a.wp = ctx->pack_wall[0];
+  a.wn = ctx->pack_wall[2];
   const index_t n = static_cast<index_t>(fluid.count);
   launch(ctx, classify_kernel, dim3(div_up(n, kSurfaceThreads)), dim3(kSurfaceThreads), 0, a);
-  if (p.near_surface_radius > 0.0)
+  if (p.near_surface_radius > 0.0) {
     launch(ctx, expand_kernel, dim3(div_up(n, kSurfaceThreads)), dim3(kSurfaceThreads), 0,
-           static_cast<const double*>(fluid.x), static_cast<const double*>(fluid.y),
-           static_cast<const double*>(fluid.z), fluid.surface_type, n, static_cast<const index_t*>(fn.offsets),
-           static_cast<const index_t*>(fn.indices), p.near_surface_radius * p.near_surface_radius);
+           static_cast<const double4*>(ctx->pack_fluid[0]), fluid.surface_type, n,
+           static_cast<const index_t*>(fn.offsets), static_cast<const index_t*>(fn.indices),
+           p.near_surface_radius * p.near_surface_radius);
+  }
   return check_launch(ctx, "surface classification");
 }
 

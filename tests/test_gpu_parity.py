@@ -316,7 +316,7 @@ def test_knob_arguments_checked(device_api):
             c.set_knob(1, 4)
         with pytest.raises(device_api.LsmpsError):
             c.set_knob(7, 0)
-        assert c.knob(0) == 1 and c.knob(1) == 2
+        assert c.knob(0) == 1 and c.knob(1) == 1
     finally:
         c.close()
 
