@@ -53,6 +53,7 @@ def parse_args():
     ap.add_argument("--workload", choices=list(WORKLOADS), default="splash")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default launch-shape knobs")
     ap.add_argument("--kappa-threshold", type=float, default=None,
                     help="mixed form: condition-estimate threshold of the FP64 route (library default if omitted)")
     ap.add_argument("--precision", choices=["both", "plain", "mixed"], default="both",
@@ -151,6 +152,23 @@ def max_over_ranks(world, value: float, device) -> float:
     return float(t.item())
 
 
+def measured_traffic(kernel: str, n_fluid: int):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary of the
+    500k dam break (profiles/), scaled to this workload by fluid-particle
+    count (the kernels' traffic grows in proportion); None if not captured."""
+    import glob
+
+    for path in sorted(glob.glob(os.path.join(ROOT, "profiles", "dram_traffic_*.json"))):
+        with open(path) as fh:
+            d = json.load(fh)
+        k = d.get("kernels", {}).get(kernel)
+        if k:
+            return (k["dram_bytes_per_fluid_particle"] * n_fluid,
+                    f"{os.path.basename(path)}: ncu dram__bytes_read+write at {d['n_fluid']} fluid particles, "
+                    f"scaled by fluid count")
+    return None, None
+
+
 def peaks() -> tuple[float, str]:
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -220,7 +238,10 @@ def run_ours(args, world, rank, local):
                 ctx.step(dev, p, state)
             # the project autotuner picks the launch-shape knobs on this state
             # (it runs only stages that are pure functions of the state)
-            tuned = ctx.autotune(dev, p, repeats=3, state=state)
+            if args.no_autotune:
+                tuned = {k: (ctx.knob(k), 0.0) for k in range(pkg.abi.KNOB_COUNT)}
+            else:
+                tuned = ctx.autotune(dev, p, repeats=3, state=state)
             ctx.synchronize()
             with ClockSampler(local) as sampler:
                 ms, launches = timed_steps(args.steps)
@@ -297,6 +318,7 @@ def run_ours(args, world, rank, local):
     avg_ms = top_ms / max(top_n, 1)
     alg = kb.get(top_name)
     achieved = alg / (avg_ms * 1e-3) / 1e9 if alg and avg_ms > 0 else None
+    traffic, traffic_source = measured_traffic(top_name, case.n_fluid)
     step_b = roofline.step_bytes(case.n_fluid, case.n_wall, h["kf"], h["kw"], case.n_cells)
     out = {
         "metric": METRIC,
@@ -331,7 +353,9 @@ def run_ours(args, world, rank, local):
             "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
             "unit": "GB/s",
             "frac": achieved / peak if achieved else None,
-            "traffic": None,
+            "traffic": traffic,
+            "traffic_source": traffic_source,
+            "algorithmic_bytes": alg,
             "step_bytes_model": step_b,
             "step_hbm_frac": step_b / (h["ms"] * 1e-3) / 1e9 / peak,
         },

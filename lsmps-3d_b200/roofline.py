@@ -55,7 +55,9 @@ def kernel_bytes(nf: int, nw: int, kf: int, kw: int, c: int, s: int = 8) -> dict
     moment_in = rows + pos_f + 2 * pos_w  # wall positions + normals
     out["moment_a_kernel<V,P>"] = moment_in + 2 * moment_kind_out
     out["moment_a_kernel<V>"] = out["moment_a_kernel<P>"] = moment_in + moment_kind_out
-    out["laplacian_kernel"] = rows + 2 * pos_f + 2 * pos_w + 81 * s * nf + 3 * s * nf
+    lap = rows + 2 * pos_f + 2 * pos_w + 3 * s * nf
+    out["laplacian_kernel<false>"] = lap + 81 * s * nf
+    out["laplacian_kernel<true>"] = lap + 9 * 4 * nf  # the FP32 Laplacian row
     ppe_common = rows + 2 * pos_f + 4 * nf + 3 * pos_w + 4 * (nf + 1) + (4 + s) * (nf + kf) + 3 * s * nf
     out["ppe_kernel"] = ppe_common + 2 * 81 * s * nf
     for g in (4, 8, 16):
@@ -70,7 +72,6 @@ def kernel_bytes(nf: int, nw: int, kf: int, kw: int, c: int, s: int = 8) -> dict
     out["moment_sums_kernel"] = 4 * (nf + 1) + 4 * kf + pos_f + 31 * 8 * nf
     out["moment_rows_kernel<false>"] = (2 * 31 * 8 * nf + 2 * (4 * (nf + 1) + 4 * kw + pos_f + 2 * pos_w)
                                         + 2 * (36 * 4 + 2 * s + 4) * nf)
-    out["laplacian_mixed_kernel"] = rows + 2 * pos_f + 2 * pos_w + 9 * 4 * nf + 3 * s * nf
     out["update_anti_penetration_kernel"] = (4 * (nf + 1) + 4 * kw + 4 * nf + 2 * pos_f + 3 * pos_f
                                              + 2 * pos_w + 2 * pos_f)
     out["smooth_kernel"] = 4 * (nf + 1) + 4 * kf + 2 * pos_f + 4 * nf + pos_f
