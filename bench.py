@@ -34,7 +34,7 @@ sys.path.insert(0, ROOT)
 import __graft_entry__ as graft_entry  # noqa: E402
 
 METRIC = "particles/s per LSMPS step, mixed vs plain FP64 on 1 B200 at stated error; HBM %"
-KNOB_NAMES = {0: "moment_occupancy", 1: "ppe_lanes"}
+KNOB_NAMES = {0: "moment_occupancy", 1: "ppe_lanes", 2: "gather_lanes"}
 WORKLOADS = {
     "splash": ("splash", {}, "splash dam break 200x50x200 (2M fluid, l0=0.0025 m, 5% splash, 3 wall layers)"),
     "dam_break": ("dam_break", {}, "dam break 100x50x100 (500k fluid, l0=0.005 m, jitter 0.05 l0, 3 wall layers)"),

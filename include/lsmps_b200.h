@@ -300,7 +300,10 @@ typedef enum lsmps_knob {
   /* lanes cooperating on one PPE row: 0 -> 1, 1 -> 4 (default), 2 -> 8,
    * 3 -> 16 */
   LSMPS_KNOB_PPE_LANES = 1,
-  LSMPS_KNOB_COUNT = 2
+  /* lanes cooperating on one particle in the velocity-Laplacian and
+   * smoothing passes: 0 -> 1, 1 -> 2, 2 -> 4 (default) */
+  LSMPS_KNOB_GATHER_LANES = 2,
+  LSMPS_KNOB_COUNT = 3
 } lsmps_knob;
 lsmps_status lsmps_ctx_set_knob(lsmps_ctx* ctx, int knob, int value);
 int lsmps_ctx_knob(lsmps_ctx* ctx, int knob);

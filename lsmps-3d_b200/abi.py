@@ -42,7 +42,8 @@ PRECISION_MIXED = 1
 # Launch-shape knobs (lsmps_knob).
 KNOB_MOMENT_OCCUPANCY = 0
 KNOB_PPE_LANES = 1
-KNOB_COUNT = 2
+KNOB_GATHER_LANES = 2
+KNOB_COUNT = 3
 
 # Particle limit of lsmps_build_cell_list_noalloc (its fixed scratch).
 NOALLOC_MAX_PARTICLES = 524288

@@ -4,7 +4,8 @@
 // Only stages that are pure functions of the step state are timed, so tuning
 // never advances the simulation: the moment stage (its outputs are rebuilt
 // from the positions) for LSMPS_KNOB_MOMENT_OCCUPANCY and the PPE assembly
-// (rebuilt from u*, the moments and the CSR) for LSMPS_KNOB_PPE_LANES.  The
+// (rebuilt from u*, the moments and the CSR) for LSMPS_KNOB_PPE_LANES, the
+// velocity Laplacian (rebuilt from the velocities) for LSMPS_KNOB_GATHER_LANES.  The
 // state's temporary velocity must hold u* of the current positions (it does
 // after any lsmps_step or the provision entry points); its values only feed
 // the timed kernels' arithmetic, not their control flow.
@@ -81,11 +82,21 @@ extern "C" lsmps_status lsmps_autotune(lsmps_ctx* ctx, const lsmps_params* param
                              s->temporary_velocity, s->temporary_wall_velocity, s->velocity_moment,
                              s->pressure_moment, s->ppe);
   };
-  double ms[LSMPS_KNOB_COUNT] = {0.0, 0.0};
+  double ms[LSMPS_KNOB_COUNT] = {0.0, 0.0, 0.0};
   st = time_variants(ctx, LSMPS_KNOB_MOMENT_OCCUPANCY, repeats, moments, &ms[0]);
   // the PPE reads the moment outputs of the chosen variant
   if (!st) st = moments();
   if (!st) st = time_variants(ctx, LSMPS_KNOB_PPE_LANES, repeats, ppe, &ms[1]);
+  // the Laplacian pass stands for both passes this knob shapes (the smoothing
+  // pass writes the state, so it is not run here)
+  auto laplacian = [&]() -> lsmps_status {
+    if (mixed)
+      return velocity_laplacian_mixed_impl(ctx, s->fluid, s->walls, s->fluid_neighbors, s->wall_neighbors,
+                                           s->velocity_moment, s->velocity_laplacian);
+    return velocity_laplacian_impl(ctx, s->fluid, s->walls, s->fluid_neighbors, s->wall_neighbors,
+                                   s->velocity_moment, s->velocity_laplacian);
+  };
+  if (!st) st = time_variants(ctx, LSMPS_KNOB_GATHER_LANES, repeats, laplacian, &ms[2]);
   if (best_ms)
     for (int k = 0; k < LSMPS_KNOB_COUNT; ++k) best_ms[k] = ms[k];
   return end_call(ctx, st);

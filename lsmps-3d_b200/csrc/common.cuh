@@ -100,6 +100,22 @@ __device__ __forceinline__ void neumann_a(double dx, double dy, double dz, doubl
 
 inline int div_up(long long a, long long b) { return static_cast<int>((a + b - 1) / b); }
 
+// Lane groups: G consecutive lanes of a warp (G a power of two dividing 32)
+// share one particle.  group_mask names the calling thread's group only, so
+// the shuffles stay valid when other groups of the warp have left.
+template <int G>
+__device__ __forceinline__ unsigned group_mask() {
+  return ((G == 32) ? 0xffffffffu : ((1u << G) - 1u)) << ((threadIdx.x & (kWarp - 1)) & ~(G - 1));
+}
+
+// Sum over the lanes of a group; every lane of the group ends with the total.
+template <int G>
+__device__ __forceinline__ double group_sum(double v, unsigned mask) {
+#pragma unroll
+  for (int d = G / 2; d > 0; d >>= 1) v += __shfl_xor_sync(mask, v, d);
+  return v;
+}
+
 }  // namespace lsmps
 
 // Opaque context of the C ABI.
@@ -129,7 +145,7 @@ struct lsmps_ctx {
   std::vector<ProfileRecord> profile;
   size_t profile_used = 0;
   // Launch-shape knobs (lsmps_knob).
-  int knob[LSMPS_KNOB_COUNT] = {1, 1};
+  int knob[LSMPS_KNOB_COUNT] = {1, 1, 2};
   // 32-byte neighbour records (packed.cuh): two fluid and three wall arrays.
   double4* pack_fluid[2] = {nullptr, nullptr};
   double4* pack_wall[3] = {nullptr, nullptr, nullptr};

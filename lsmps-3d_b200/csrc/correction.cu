@@ -243,33 +243,39 @@ __global__ void __launch_bounds__(kThreads) anti_penetration_kernel(lsmps_fluid 
 
 // smooth_velocity_kernel, pressure_correction.cu:446-504, on neighbour records
 // fp = {x, y, z, 0} and fv = {vx, vy, vz, label} (packed.cuh).
+template <int G>
 __global__ void __launch_bounds__(kThreads) smooth_kernel(index_t n, const double4* __restrict__ fp,
                                                           const double4* __restrict__ fv,
                                                           const index_t* __restrict__ fo,
                                                           const index_t* __restrict__ fi, double re, double strength,
                                                           double* ox, double* oy, double* oz) {
-  const index_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  // G lanes per particle (lane l takes entries l, l + G, ...); the group
+  // leaves or continues as a whole.
+  const index_t i = (blockIdx.x * blockDim.x + threadIdx.x) / G;
+  const int l = threadIdx.x & (G - 1);
   if (i >= n) return;
   const double inv_re = 1.0 / re;
   constexpr double kSplash = static_cast<double>(LSMPS_SURFACE_SPLASH);
   const double4 ui = ld4(fv, i);
   if (strength <= 0.0 || ui.w == kSplash) {
-    ox[i] = ui.x;
-    oy[i] = ui.y;
-    oz[i] = ui.z;
+    if (l == 0) {
+      ox[i] = ui.x;
+      oy[i] = ui.y;
+      oz[i] = ui.z;
+    }
     return;
   }
   const double4 pi = ld4(fp, i);
   double ws = 0.0, ax = 0.0, ay = 0.0, az = 0.0;
   const index_t fe = fo[i + 1];
-  index_t o = fo[i];
+  index_t o = fo[i] + l;
   index_t jn = o < fe ? fi[o] : i;
   double4 un = ld4(fv, jn), qn = ld4(fp, jn);
-  for (; o < fe; ++o) {
+  for (; o < fe; o += G) {
     // the next neighbour's records are loaded while this one is summed
     const double4 u = un, q = qn;
-    if (o + 1 < fe) {
-      jn = fi[o + 1];
+    if (o + G < fe) {
+      jn = fi[o + G];
       un = ld4(fv, jn);
       qn = ld4(fp, jn);
     }
@@ -281,6 +287,14 @@ __global__ void __launch_bounds__(kThreads) smooth_kernel(index_t n, const doubl
     ax = fma(w, u.x, ax);
     ay = fma(w, u.y, ay);
     az = fma(w, u.z, az);
+  }
+  if (G > 1) {
+    const unsigned mask = group_mask<G>();
+    ws = group_sum<G>(ws, mask);
+    ax = group_sum<G>(ax, mask);
+    ay = group_sum<G>(ay, mask);
+    az = group_sum<G>(az, mask);
+    if (l != 0) return;
   }
   if (ws <= 0.0) {
     ox[i] = ui.x;
@@ -396,10 +410,26 @@ lsmps_status smooth_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const lsmps_csr& 
   if (!ensure_packs(ctx, f.count, 0)) return fail(ctx, LSMPS_CUDA_ERROR, "pack allocation failed");
   pack4(ctx, f.x, f.y, f.z, nullptr, f.count, ctx->pack_fluid[0]);
   pack4_label(ctx, f.vx, f.vy, f.vz, f.surface_type, f.count, ctx->pack_fluid[1]);
-  launch(ctx, smooth_kernel, dim3(div_up(static_cast<long long>(f.count), kThreads)), dim3(kThreads), 0,
-         static_cast<index_t>(f.count), static_cast<const double4*>(ctx->pack_fluid[0]),
-         static_cast<const double4*>(ctx->pack_fluid[1]), static_cast<const index_t*>(fn.offsets),
-         static_cast<const index_t*>(fn.indices), p.support_radius, p.velocity_smoothing_strength, sm.x, sm.y, sm.z);
+  const long long n = static_cast<long long>(f.count);
+  const double4* fp = ctx->pack_fluid[0];
+  const double4* fv = ctx->pack_fluid[1];
+  switch (ctx->knob[LSMPS_KNOB_GATHER_LANES]) {
+    case 1:
+      launch(ctx, smooth_kernel<2>, dim3(div_up(2 * n, kThreads)), dim3(kThreads), 0, static_cast<index_t>(n), fp, fv,
+             static_cast<const index_t*>(fn.offsets), static_cast<const index_t*>(fn.indices), p.support_radius,
+             p.velocity_smoothing_strength, sm.x, sm.y, sm.z);
+      break;
+    case 2:
+      launch(ctx, smooth_kernel<4>, dim3(div_up(4 * n, kThreads)), dim3(kThreads), 0, static_cast<index_t>(n), fp, fv,
+             static_cast<const index_t*>(fn.offsets), static_cast<const index_t*>(fn.indices), p.support_radius,
+             p.velocity_smoothing_strength, sm.x, sm.y, sm.z);
+      break;
+    default:
+      launch(ctx, smooth_kernel<1>, dim3(div_up(n, kThreads)), dim3(kThreads), 0, static_cast<index_t>(n), fp, fv,
+             static_cast<const index_t*>(fn.offsets), static_cast<const index_t*>(fn.indices), p.support_radius,
+             p.velocity_smoothing_strength, sm.x, sm.y, sm.z);
+      break;
+  }
   launch(ctx, copy_kernel, dim3(pointwise_blocks(ctx, f.count)), dim3(256), 0, static_cast<index_t>(f.count),
          static_cast<const double*>(sm.x), static_cast<const double*>(sm.y), static_cast<const double*>(sm.z), f.vx,
          f.vy, f.vz);

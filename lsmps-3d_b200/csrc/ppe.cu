@@ -155,16 +155,6 @@ __global__ void __launch_bounds__(kThreads) ppe_kernel(PpeArgs a) {
   if (a.wall_rhs_out) a.wall_rhs_out[i] = wall_rhs;
 }
 
-// Sum over the G lanes of a row group (G a power of two dividing 32); every
-// lane of the group ends with the total.  `mask` names the group's lanes
-// only, since other groups of the warp may have left.
-template <int G>
-__device__ __forceinline__ double group_sum(double v, unsigned mask) {
-#pragma unroll
-  for (int d = G / 2; d > 0; d >>= 1) v += __shfl_xor_sync(mask, v, d);
-  return v;
-}
-
 // The same row with G lanes per particle: lane l takes the neighbours
 // nb + l, nb + l + G, ..., so the G lanes write G consecutive (col, val)
 // slots per round and issue G independent gathers.  The partial sums (the
@@ -261,7 +251,7 @@ __global__ void __launch_bounds__(kThreads, 4) ppe_lanes_kernel(PpeArgs a) {
     neumann_a(dx, dy, dz, nx, ny, nz, a.inv_re, qn9);
     wall_rhs += 2.0 * a.pwall_scale * bw * ng * dot9(L, qn9) * a.inv_re;
   }
-  const unsigned mask = ((G == 32) ? 0xffffffffu : ((1u << G) - 1u)) << ((threadIdx.x & (kWarp - 1)) & ~(G - 1));
+  const unsigned mask = group_mask<G>();
   diag = group_sum<G>(diag, mask);
   wall_rhs = group_sum<G>(wall_rhs, mask);
 #pragma unroll

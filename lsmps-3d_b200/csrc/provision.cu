@@ -61,24 +61,29 @@ __device__ __forceinline__ double lap_from(const double* __restrict__ inv, const
 // Mixed (the mixed form): the inverse is replaced by the particle's
 // Laplacian row from the mixed-form operator rows (FP32, or FP64 for the
 // FP64-route particles); the sums are the same FP64 sums.
-template <bool Mixed>
+//
+// G lanes per particle (G = 1, 2, 4; LSMPS_KNOB_GATHER_LANES): lane l sums the
+// entries l, l + G, ... of both rows and the groups' partial sums are added
+// with shuffles (a rounding-level reassociation for G > 1).
+template <bool Mixed, int G>
 __global__ void __launch_bounds__(kThreads) laplacian_kernel(LaplacianArgs a, MixedRows rows) {
-  const index_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= a.n) return;
+  const index_t i = (blockIdx.x * blockDim.x + threadIdx.x) / G;
+  const int l = threadIdx.x & (G - 1);
+  if (i >= a.n) return;  // the whole group
   const double4 pi = ld4(a.fp, i);
   const double4 ui = ld4(a.fv, i);
   double rx[9], ry[9], rz[9], b[9];
 #pragma unroll
   for (int r = 0; r < 9; ++r) rx[r] = ry[r] = rz[r] = 0.0;
   const index_t fe = a.fo[i + 1];
-  index_t o = a.fo[i];
+  index_t o = a.fo[i] + l;
   index_t jn = o < fe ? a.fi[o] : i;
   double4 qn = ld4(a.fp, jn), un = ld4(a.fv, jn);
-  for (; o < fe; ++o) {
+  for (; o < fe; o += G) {
     // the next neighbour's records are loaded while this one is summed
     const double4 q = qn, u = un;
-    if (o + 1 < fe) {
-      jn = a.fi[o + 1];
+    if (o + G < fe) {
+      jn = a.fi[o + G];
       qn = ld4(a.fp, jn);
       un = ld4(a.fv, jn);
     }
@@ -89,7 +94,7 @@ __global__ void __launch_bounds__(kThreads) laplacian_kernel(LaplacianArgs a, Mi
     acc_rhs(b, w, u.x - ui.x, u.y - ui.y, u.z - ui.z, rx, ry, rz);
   }
   const index_t we = a.wo[i + 1];
-  for (index_t o = a.wo[i]; o < we; ++o) {
+  for (index_t o = a.wo[i] + l; o < we; o += G) {
     const index_t j = a.wi[o];
     const double4 q = ld4(a.wp, j);
     const double4 u = ld4(a.wv, j);
@@ -98,6 +103,16 @@ __global__ void __launch_bounds__(kThreads) laplacian_kernel(LaplacianArgs a, Mi
     if (w <= 0.0) continue;
     basis_a_mul(dx, dy, dz, a.inv_re, b);
     acc_rhs(b, w, u.x - ui.x, u.y - ui.y, u.z - ui.z, rx, ry, rz);
+  }
+  if (G > 1) {
+    const unsigned mask = group_mask<G>();
+#pragma unroll
+    for (int r = 0; r < 9; ++r) {
+      rx[r] = group_sum<G>(rx[r], mask);
+      ry[r] = group_sum<G>(ry[r], mask);
+      rz[r] = group_sum<G>(rz[r], mask);
+    }
+    if (l != 0) return;
   }
   if (Mixed) {
     double l[9];
@@ -147,6 +162,25 @@ __global__ void wall_combine_kernel(lsmps_walls w, lsmps_params p, double* tx, d
   }
 }
 
+template <bool Mixed>
+void launch_laplacian(lsmps_ctx* ctx, const LaplacianArgs& a, const MixedRows& rows) {
+  const long long n = a.n;
+  switch (ctx->knob[LSMPS_KNOB_GATHER_LANES]) {
+    case 1:
+      launch_named(ctx, Mixed ? "laplacian_kernel<true, 2>" : "laplacian_kernel<false, 2>", laplacian_kernel<Mixed, 2>,
+                   dim3(div_up(2 * n, kThreads)), dim3(kThreads), 0, a, rows);
+      break;
+    case 2:
+      launch_named(ctx, Mixed ? "laplacian_kernel<true, 4>" : "laplacian_kernel<false, 4>", laplacian_kernel<Mixed, 4>,
+                   dim3(div_up(4 * n, kThreads)), dim3(kThreads), 0, a, rows);
+      break;
+    default:
+      launch_named(ctx, Mixed ? "laplacian_kernel<true, 1>" : "laplacian_kernel<false, 1>", laplacian_kernel<Mixed, 1>,
+                   dim3(div_up(n, kThreads)), dim3(kThreads), 0, a, rows);
+      break;
+  }
+}
+
 int pointwise_blocks(lsmps_ctx* ctx, size_t n) {
   const long long b = div_up(static_cast<long long>(n), 256);
   const long long cap = static_cast<long long>(ctx->sm_count) * 8;
@@ -172,8 +206,7 @@ lsmps_status velocity_laplacian_mixed_impl(lsmps_ctx* ctx, const lsmps_fluid& f,
   LaplacianArgs a{static_cast<index_t>(f.count), ctx->pack_fluid[0], ctx->pack_fluid[1], ctx->pack_wall[0],
                   ctx->pack_wall[1], fn.offsets, fn.indices, wn.offsets, wn.indices, nullptr,
                   vm.support_radius, 1.0 / vm.support_radius, vm.wall_weight_scale, lap.x, lap.y, lap.z};
-  launch(ctx, laplacian_kernel<true>, dim3(div_up(static_cast<long long>(f.count), kThreads)), dim3(kThreads), 0, a,
-         mixed_rows_of(ctx, 0));
+  launch_laplacian<true>(ctx, a, mixed_rows_of(ctx, 0));
   return check_launch(ctx, "velocity laplacian (mixed)");
 }
 
@@ -195,8 +228,7 @@ lsmps_status velocity_laplacian_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const
   LaplacianArgs a{static_cast<index_t>(f.count), ctx->pack_fluid[0], ctx->pack_fluid[1], ctx->pack_wall[0],
                   ctx->pack_wall[1], fn.offsets, fn.indices, wn.offsets, wn.indices, vm.inverse_matrices,
                   vm.support_radius, 1.0 / vm.support_radius, vm.wall_weight_scale, lap.x, lap.y, lap.z};
-  launch(ctx, laplacian_kernel<false>, dim3(div_up(static_cast<long long>(f.count), kThreads)), dim3(kThreads), 0, a,
-         MixedRows{});
+  launch_laplacian<false>(ctx, a, MixedRows{});
   return check_launch(ctx, "velocity laplacian");
 }
 

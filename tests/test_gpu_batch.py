@@ -31,7 +31,9 @@ def test_graph_batch_matches_sequential_steps(pkg, device_api, precision):
     try:
         for b, p in bufs:
             batch.add(b, p)
-        batch.capture(precision=precision, autotune_repeats=1)
+        # default launch shapes, as in the solo steps (the autotuner may pick
+        # lane counts that reassociate sums at the rounding level)
+        batch.capture(precision=precision, autotune_repeats=0)
         batch.launch()
         batch.synchronize()
     finally:

@@ -238,7 +238,7 @@ def test_full_step_matches_oracle(pkg, device_api, ctx, oracle, name, kw):
             assert e < 1e-7, (comp, e)
 
 
-KNOB_VARIANTS = [(0, 0), (0, 1), (1, 0), (1, 1), (1, 2), (1, 3)]
+KNOB_VARIANTS = [(0, 0), (0, 1), (1, 0), (1, 1), (1, 2), (1, 3), (2, 0), (2, 1), (2, 2)]
 
 
 @pytest.mark.parametrize("knob,value", KNOB_VARIANTS, ids=[f"knob{k}={v}" for k, v in KNOB_VARIANTS])
@@ -309,14 +309,43 @@ def test_autotune_leaves_state_and_picks_valid_variants(pkg, device_api):
         c.close()
 
 
+@pytest.mark.parametrize("lanes", [1, 2], ids=["gather2", "gather4"])
+def test_gather_lanes_step_matches_oracle(pkg, device_api, oracle, lanes):
+    """The lane-parallel velocity-Laplacian and smoothing passes against the
+    oracle's step, on a moving fluid (so both passes do real work)."""
+    case = pkg.cases.CASES["dam_break"](nx=24, ny=12, nz=24, l0=0.005)
+    f = case.fluid
+    f["vx"] = 0.1 * np.sin(f["x"] / 0.12)
+    f["vy"] = 0.1 * np.cos(f["y"] / 0.12)
+    f["vz"] = 0.1 * f["z"] / 0.12
+    p = case.params
+    dev, host = both(pkg, device_api, case)
+    c = device_api.Context(0)
+    try:
+        c.set_knob(pkg.abi.KNOB_GATHER_LANES, lanes)
+        c.build_neighbor_lists(dev, p)
+        c.classify_surface(dev, p)
+        c.step(dev, p)
+    finally:
+        c.close()
+    oracle.build_neighbor_lists(host, p)
+    oracle.classify_surface(host, p)
+    assert oracle.step(host, p)[0] == 0
+    lap = vec_err(dev.numpy("velocity_laplacian"), host.numpy("velocity_laplacian"), ("x", "y", "z"))
+    g = dev.numpy("fluid")
+    state = {**vec_err(g, host.fluid, ("x", "y", "z")), **vec_err(g, host.fluid, ("vx", "vy", "vz"))}
+    for k, e in {**lap, **state}.items():
+        assert e < PLAIN_RTOL, (k, e)
+
+
 def test_knob_arguments_checked(device_api):
     c = device_api.Context(0)
     try:
         with pytest.raises(device_api.LsmpsError):
-            c.set_knob(1, 4)
+            c.set_knob(2, 3)
         with pytest.raises(device_api.LsmpsError):
             c.set_knob(7, 0)
-        assert c.knob(0) == 1 and c.knob(1) == 1
+        assert c.knob(0) == 1 and c.knob(1) == 1 and c.knob(2) == 2
     finally:
         c.close()
 
