@@ -294,8 +294,9 @@ uint64_t lsmps_ctx_fp64_fallbacks(lsmps_ctx* ctx);
  * one thread per particle in 128-thread blocks).  Values are indices into each
  * knob's variant list; lsmps_autotune() picks them by timing. */
 typedef enum lsmps_knob {
-  /* moment kernel register budget: 0 = compiler's choice, 1 = capped for 8
-   * blocks per SM (default) */
+  /* plain-form moment kernel: 0 = compiler's register choice, 1 = capped for
+   * 8 blocks per SM (default), 2 = the two kinds on two warps sharing each
+   * row */
   LSMPS_KNOB_MOMENT_OCCUPANCY = 0,
   /* lanes cooperating on one PPE row: 0 -> 1, 1 -> 4 (default), 2 -> 8,
    * 3 -> 16 */

@@ -278,7 +278,7 @@ lsmps_status lsmps_ctx_set_condition_threshold(lsmps_ctx* ctx, double threshold)
 
 int lsmps_knob_variants(int knob) {
   switch (knob) {
-    case LSMPS_KNOB_MOMENT_OCCUPANCY: return 2;
+    case LSMPS_KNOB_MOMENT_OCCUPANCY: return 3;
     case LSMPS_KNOB_PPE_LANES: return 4;
     case LSMPS_KNOB_GATHER_LANES: return 3;
     default: return 0;

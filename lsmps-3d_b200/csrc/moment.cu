@@ -479,6 +479,52 @@ __global__ void __launch_bounds__(kMomentThreads, MinBlocks) moment_a_kernel(Mom
   }
 }
 
+// The velocity and pressure kinds with the two warps of a 64-thread block
+// sharing 32 particles: warp h sums the even (h = 0) or odd (h = 1) entries of
+// each row, the halves are exchanged through shared memory, then warp 0
+// finishes the velocity kind and warp 1 the pressure kind, so neither the
+// row sum nor the two factorisations run twice in one thread and no warp
+// diverges between the kinds (LSMPS_KNOB_MOMENT_OCCUPANCY variant 2).
+__global__ void __launch_bounds__(2 * kWarp, 8) moment_a_split_kernel(MomentPackedArgs a) {
+  __shared__ double s_half[2][kMonomials][kWarp];
+  const int lane = threadIdx.x & (kWarp - 1), half = threadIdx.x >> 5;
+  const index_t i = blockIdx.x * kWarp + lane;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (a.k0.count) atomicAdd(a.k0.count, 1);
+    if (a.k1.count) atomicAdd(a.k1.count, 1);
+  }
+  const bool live = i < a.n;
+  const double4 pi = live ? ld4(a.fp, i) : make_double4(0.0, 0.0, 0.0, 0.0);
+  double s[kMonomials];
+#pragma unroll
+  for (int e = 0; e < kMonomials; ++e) s[e] = 0.0;
+  if (live) {
+    const index_t fe = a.fo[i + 1];
+    index_t o = a.fo[i] + half;
+    double4 qn = o < fe ? ld4(a.fp, a.fi[o]) : pi;
+    for (; o < fe; o += 2) {
+      const double4 q = qn;
+      if (o + 2 < fe) qn = ld4(a.fp, a.fi[o + 2]);
+      const double dx = q.x - pi.x, dy = q.y - pi.y, dz = q.z - pi.z;
+      const double d2 = dx * dx + dy * dy + dz * dz;
+      if (d2 <= 0.0) continue;
+      const double w = 1.0 - sqrt(d2) * a.inv_re;
+      if (w <= 0.0) continue;
+      acc_monomials(s, dx * a.inv_re, dy * a.inv_re, dz * a.inv_re, w);
+    }
+  }
+#pragma unroll
+  for (int e = 0; e < kMonomials; ++e) s_half[half][e][lane] = s[e];
+  __syncthreads();
+  if (!live) return;
+#pragma unroll
+  for (int e = 0; e < kMonomials; ++e) s[e] = s_half[0][e][lane] + s_half[1][e][lane];
+  if (half == 0)
+    finish_a<1>(s, a, a.k0, i, pi);
+  else
+    finish_a<2>(s, a, a.k1, i, pi);
+}
+
 // ---------------------------------------------------------------------------
 // Mixed form (LSMPS_PRECISION_MIXED).
 //
@@ -709,25 +755,15 @@ __device__ __forceinline__ double assemble_kind(const MixedRowArgs& a, int kind,
   return trace;
 }
 
+// Stage 2 of one particle and kind from its fluid monomial totals s (the
+// thread's column of shared memory m holds the kind's matrix).
 template <bool Full>
-__global__ void __launch_bounds__(kRowThreads, 6) moment_rows_kernel(MixedRowArgs a) {
-  __shared__ double s_m[45 * kRowThreads];
-  const int kind = blockIdx.y;
-  const index_t i = blockIdx.x * kRowThreads + threadIdx.x;
-  if (blockIdx.x == 0 && threadIdx.x == 0 && a.k[kind].count) atomicAdd(a.k[kind].count, 1);
-  if (i >= a.n) return;
-  double* m = s_m + threadIdx.x;  // entry e at m[e * kRowThreads]
-  const size_t n = static_cast<size_t>(a.n);
-  const double4 pi = ld4(a.fp, i);
+__device__ __forceinline__ void mixed_rows_of_particle(const MixedRowArgs& a, int kind, index_t i, const double4& pi,
+                                                       double (&s)[kMonomials], double* m) {
   const KindOut& ko = a.k[kind];
   constexpr int kTargets = Full ? 9 : 4;
   double reg = 0.0, trace = 0.0;
-  {
-    double s[kMonomials];
-#pragma unroll
-    for (int e = 0; e < kMonomials; ++e) s[e] = a.sums[e * n + i];
-    trace = assemble_kind(a, kind, i, pi, s, m, &reg);
-  }
+  trace = assemble_kind(a, kind, i, pi, s, m, &reg);
   float l[45];
 #pragma unroll
   for (int e = 0; e < 45; ++e) l[e] = static_cast<float>(m[e * kRowThreads]);
@@ -840,6 +876,67 @@ __global__ void __launch_bounds__(kRowThreads, 6) moment_rows_kernel(MixedRowArg
   }
 }
 
+template <bool Full>
+__global__ void __launch_bounds__(kRowThreads, 6) moment_rows_kernel(MixedRowArgs a) {
+  __shared__ double s_m[45 * kRowThreads];
+  const int kind = blockIdx.y;
+  const index_t i = blockIdx.x * kRowThreads + threadIdx.x;
+  if (blockIdx.x == 0 && threadIdx.x == 0 && a.k[kind].count) atomicAdd(a.k[kind].count, 1);
+  if (i >= a.n) return;
+  const size_t n = static_cast<size_t>(a.n);
+  double s[kMonomials];
+#pragma unroll
+  for (int e = 0; e < kMonomials; ++e) s[e] = a.sums[e * n + i];
+  mixed_rows_of_particle<Full>(a, kind, i, ld4(a.fp, i), s, s_m + threadIdx.x);
+}
+
+// Both stages in one kernel (the step's path): the two warps of a 64-thread
+// block share 32 particles, each warp sums the even or odd entries of their
+// rows (Kahan-compensated FP32), the halves meet in shared memory as FP64
+// totals, then warp 0 finishes the velocity kind and warp 1 the pressure kind.
+template <bool Full>
+__global__ void __launch_bounds__(kRowThreads, 6) moment_mixed_split_kernel(MixedSumArgs sa, MixedRowArgs a) {
+  static_assert(kRowThreads == 2 * kWarp, "two warps per block");
+  __shared__ double s_m[45 * kRowThreads];
+  __shared__ double s_half[2][kMonomials][kWarp];
+  const int lane = threadIdx.x & (kWarp - 1), half = threadIdx.x >> 5;
+  const index_t i = blockIdx.x * kWarp + lane;
+  if (blockIdx.x == 0 && lane == 0 && a.k[half].count) atomicAdd(a.k[half].count, 1);
+  const bool live = i < a.n;
+  const double4 pi = live ? ld4(a.fp, i) : make_double4(0.0, 0.0, 0.0, 0.0);
+  {
+    float sum[kMonomials], comp[kMonomials];
+#pragma unroll
+    for (int e = 0; e < kMonomials; ++e) sum[e] = comp[e] = 0.0f;
+    if (live) {
+      const index_t fe = sa.fo[i + 1];
+      index_t o = sa.fo[i] + half;
+      double4 qn = o < fe ? ld4(sa.fp, sa.fi[o]) : pi;
+      for (; o < fe; o += 2) {
+        const double4 q = qn;
+        if (o + 2 < fe) qn = ld4(sa.fp, sa.fi[o + 2]);
+        const float sx = static_cast<float>((q.x - pi.x) * sa.inv_re);
+        const float sy = static_cast<float>((q.y - pi.y) * sa.inv_re);
+        const float sz = static_cast<float>((q.z - pi.z) * sa.inv_re);
+        const float d2 = sx * sx + sy * sy + sz * sz;
+        if (d2 > 0.0f) {
+          const float w = 1.0f - sqrtf(d2);
+          if (w > 0.0f) kahan_monomials(sum, comp, sx, sy, sz, w);
+        }
+      }
+    }
+#pragma unroll
+    for (int e = 0; e < kMonomials; ++e)
+      s_half[half][e][lane] = static_cast<double>(sum[e]) - static_cast<double>(comp[e]);
+  }
+  __syncthreads();
+  if (!live) return;
+  double s[kMonomials];
+#pragma unroll
+  for (int e = 0; e < kMonomials; ++e) s[e] = s_half[0][e][lane] + s_half[1][e][lane];
+  mixed_rows_of_particle<Full>(a, half, i, pi, s, s_m + threadIdx.x);
+}
+
 // make_matrix_request, moment_matrix.cu:494-538: boundary of each kind.
 int boundary_of(int kind) {
   switch (kind) {
@@ -858,7 +955,7 @@ lsmps_status launch_mixed(lsmps_ctx* ctx, index_t n, const lsmps_csr& fn, const 
   if (!ensure_mixed(ctx, static_cast<size_t>(n))) return fail(ctx, LSMPS_CUDA_ERROR, "mixed-form allocation failed");
   const double inv_re = 1.0 / p.support_radius;
   MixedSumArgs sa{n, ctx->pack_fluid[0], fn.offsets, fn.indices, inv_re, ctx->mixed_sums};
-  launch(ctx, moment_sums_kernel, dim3(div_up(n, kSumThreads)), dim3(kSumThreads), 0, sa);
+  const bool split = ctx->knob[LSMPS_KNOB_MOMENT_OCCUPANCY] == 2;
   MixedRowArgs ra{};
   ra.n = n;
   ra.sums = ctx->mixed_sums;
@@ -881,6 +978,15 @@ lsmps_status launch_mixed(lsmps_ctx* ctx, index_t n, const lsmps_csr& fn, const 
     ra.flag[k] = ctx->mixed_flag[k];
   }
   ra.status = ctx->d_status;
+  if (split) {
+    // one kernel: row halves on two warps, one kind per warp
+    if (full)
+      launch(ctx, moment_mixed_split_kernel<true>, dim3(div_up(n, kWarp)), dim3(kRowThreads), 0, sa, ra);
+    else
+      launch(ctx, moment_mixed_split_kernel<false>, dim3(div_up(n, kWarp)), dim3(kRowThreads), 0, sa, ra);
+    return LSMPS_OK;
+  }
+  launch(ctx, moment_sums_kernel, dim3(div_up(n, kSumThreads)), dim3(kSumThreads), 0, sa);
   const dim3 grid(div_up(n, kRowThreads), 2);
   if (full)
     launch(ctx, moment_rows_kernel<true>, grid, dim3(kRowThreads), 0, ra);
@@ -968,6 +1074,7 @@ lsmps_status prepare_moments_impl(lsmps_ctx* ctx, const lsmps_fluid& fluid, cons
                       ctx->d_status};
   const bool fused = velocity_a >= 0 && pressure_a >= 0;
   const bool capped = ctx->knob[LSMPS_KNOB_MOMENT_OCCUPANCY] == 1;
+  const bool split = ctx->knob[LSMPS_KNOB_MOMENT_OCCUPANCY] == 2;
   if (fused && ctx->precision == LSMPS_PRECISION_MIXED) {
     // Mixed form: FP32 assembly and factorisation with FP64 refinement; the
     // full inverse is written (FP64) for the caller's views.
@@ -979,7 +1086,9 @@ lsmps_status prepare_moments_impl(lsmps_ctx* ctx, const lsmps_fluid& fluid, cons
     a.k0 = out_of(kinds[velocity_a]);
     a.k1 = out_of(kinds[pressure_a]);
     const size_t smem = sizeof(double) * kMonomials * kMomentThreads;
-    if (capped)
+    if (split)
+      launch_named(ctx, "moment_a_split_kernel", moment_a_split_kernel, dim3(div_up(n, kWarp)), dim3(2 * kWarp), 0, a);
+    else if (capped)
       launch_named(ctx, "moment_a_kernel<V,P>", moment_a_kernel<1, 2, 8>, grid, block, smem, a);
     else
       launch_named(ctx, "moment_a_kernel<V,P>", moment_a_kernel<1, 2, 1>, grid, block, smem, a);

@@ -53,9 +53,12 @@ def kernel_bytes(nf: int, nw: int, kf: int, kw: int, c: int, s: int = 8) -> dict
     out = {}
     moment_kind_out = (81 * s + 2 * s + 4) * nf  # inverse, trace, regularisation, info
     moment_in = rows + pos_f + 2 * pos_w  # wall positions + normals
-    out["moment_a_kernel<V,P>"] = moment_in + 2 * moment_kind_out
+    out["moment_a_kernel<V,P>"] = out["moment_a_split_kernel"] = moment_in + 2 * moment_kind_out
     out["moment_a_kernel<V>"] = out["moment_a_kernel<P>"] = moment_in + moment_kind_out
     lap = rows + 2 * pos_f + 2 * pos_w + 3 * s * nf
+    # the two mixed stages in one kernel (row halves on two warps)
+    out["moment_mixed_split_kernel<false>"] = (4 * (nf + 1) + 4 * kf + pos_f + 2 * (4 * (nf + 1) + 4 * kw + 2 * pos_w)
+                                               + 2 * (36 * 4 + 2 * s + 4) * nf)
     out["laplacian_kernel<false>"] = lap + 81 * s * nf
     out["laplacian_kernel<true>"] = lap + 9 * 4 * nf  # the FP32 Laplacian row
     ppe_common = rows + 2 * pos_f + 4 * nf + 3 * pos_w + 4 * (nf + 1) + (4 + s) * (nf + kf) + 3 * s * nf

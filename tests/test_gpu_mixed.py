@@ -64,15 +64,17 @@ def _swirl(case):
     return case
 
 
+@pytest.mark.parametrize("moment_variant", [1, 2], ids=["two_kernels", "split_warps"])
 @pytest.mark.parametrize("threshold", [1e6, 1e4], ids=["kappa1e6", "kappa1e4"])
 @pytest.mark.parametrize("name,kw", CASES, ids=[c[0] for c in CASES])
-def test_mixed_step_against_fp64_oracle(pkg, device_api, oracle, name, kw, threshold):
+def test_mixed_step_against_fp64_oracle(pkg, device_api, oracle, name, kw, threshold, moment_variant):
     case = _swirl(pkg.cases.CASES[name](**kw))
     p = case.params
     dev, host = _both(pkg, case)
     c = device_api.Context(0, precision=pkg.abi.PRECISION_MIXED)
     try:
         c.set_condition_threshold(threshold)
+        c.set_knob(pkg.abi.KNOB_MOMENT_OCCUPANCY, moment_variant)
         c.build_neighbor_lists(dev, p)
         c.classify_surface(dev, p)
         c.step(dev, p)
@@ -125,8 +127,9 @@ def test_mixed_step_against_fp64_oracle(pkg, device_api, oracle, name, kw, thres
         assert fallbacks > 0  # ill-conditioned Surface/Splash matrices took the FP64 route
 
 
+@pytest.mark.parametrize("moment_variant", [1, 2], ids=["two_kernels", "split_warps"])
 @pytest.mark.parametrize("name,kw", CASES, ids=[c[0] for c in CASES])
-def test_mixed_moment_inverse_against_fp64_oracle(pkg, device_api, oracle, name, kw):
+def test_mixed_moment_inverse_against_fp64_oracle(pkg, device_api, oracle, name, kw, moment_variant):
     """lsmps_prepare_moments in the mixed form writes the full inverse (all
     nine columns refined once in FP64).  Per-particle normwise error against
     the oracle's FP64 inverse, by condition number band."""
@@ -135,6 +138,7 @@ def test_mixed_moment_inverse_against_fp64_oracle(pkg, device_api, oracle, name,
     dev, host = _both(pkg, case)
     c = device_api.Context(0, precision=pkg.abi.PRECISION_MIXED)
     try:
+        c.set_knob(pkg.abi.KNOB_MOMENT_OCCUPANCY, moment_variant)
         c.build_neighbor_lists(dev, p)
         c.prepare_moments(dev, p, [0, 1])
     finally:

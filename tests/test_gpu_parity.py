@@ -238,7 +238,7 @@ def test_full_step_matches_oracle(pkg, device_api, ctx, oracle, name, kw):
             assert e < 1e-7, (comp, e)
 
 
-KNOB_VARIANTS = [(0, 0), (0, 1), (1, 0), (1, 1), (1, 2), (1, 3), (2, 0), (2, 1), (2, 2)]
+KNOB_VARIANTS = [(0, 0), (0, 1), (0, 2), (1, 0), (1, 1), (1, 2), (1, 3), (2, 0), (2, 1), (2, 2)]
 
 
 @pytest.mark.parametrize("knob,value", KNOB_VARIANTS, ids=[f"knob{k}={v}" for k, v in KNOB_VARIANTS])
