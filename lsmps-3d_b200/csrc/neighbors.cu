@@ -24,6 +24,7 @@
 // particle outside the +-2 window (clamped into an edge cell), is decided by
 // the reference's own FP64 test dx*dx + dy*dy + dz*dz <= r^2
 // (neighbor_search.cu:48-59).  The neighbour sets are therefore the FP64 ones.
+#include <algorithm>
 #include <climits>
 #include <cmath>
 
@@ -67,8 +68,21 @@ struct CsrArgs {
   // (bits[i * kMaskWords + chunk]); written by the count pass, replayed by the
   // write pass.
   unsigned* bits;
+  // Source positions in cell-sorted order (src_pos[k] = position of
+  // src_sorted[k]), so that staging a cell reads one contiguous range.
+  const double4* src_pos;
   DeviceStatus* status;
 };
+
+// src_pos[k] = {x, y, z, 0} of particle sorted[k].
+__global__ void sorted_positions_kernel(const double* __restrict__ x, const double* __restrict__ y,
+                                        const double* __restrict__ z, const index_t* __restrict__ sorted, index_t n,
+                                        double4* __restrict__ out) {
+  for (index_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const index_t j = sorted[k];
+    out[k] = make_double4(x[j], y[j], z[j], 0.0);
+  }
+}
 
 __device__ __forceinline__ bool within_radius(double ax, double ay, double az, double bx, double by, double bz,
                                               double r2) {
@@ -134,11 +148,12 @@ __global__ void __launch_bounds__(kCsrThreads) csr_kernel(CsrArgs a) {
       for (index_t k = threadIdx.x; k < nc; k += kCsrThreads) {
         int t = 0;
         while (s_pre[t + 1] <= k) ++t;
-        const index_t j = a.src_sorted[s_cb[t] + (k - s_pre[t])];
-        s_idx[k] = j;
-        if (!kWrite)
-          s_rel[k] = make_float4(to_rel(a.sx[j], ccx, a.inv_h), to_rel(a.sy[j], ccy, a.inv_h),
-                                 to_rel(a.sz[j], ccz, a.inv_h), 0.0f);
+        const index_t pos = s_cb[t] + (k - s_pre[t]);
+        s_idx[k] = a.src_sorted[pos];
+        if (!kWrite) {
+          const double4 q = a.src_pos[pos];
+          s_rel[k] = make_float4(to_rel(q.x, ccx, a.inv_h), to_rel(q.y, ccy, a.inv_h), to_rel(q.z, ccz, a.inv_h), 0.0f);
+        }
       }
     }
     __syncthreads();
@@ -293,7 +308,7 @@ __global__ void __launch_bounds__(kCsrThreads) csr_kernel(CsrArgs a) {
 lsmps_status one_neighbor_list(lsmps_ctx* ctx, Scratch& scratch, const lsmps_fluid& fluid, const double* sx,
                                const double* sy, const double* sz, const lsmps_cells& home, const lsmps_cells& src,
                                const lsmps_grid& grid, double radius, bool exclude_self, const lsmps_csr& out,
-                               unsigned* bits) {
+                               size_t n_src, unsigned* bits, double4* src_pos) {
   if (fluid.count > out.particle_count || !out.offsets)
     return fail(ctx, LSMPS_INVALID_ARGUMENT, "Neighbor list particle capacity is smaller than fluid count");
   const size_t n = fluid.count;
@@ -323,7 +338,18 @@ lsmps_status one_neighbor_list(lsmps_ctx* ctx, Scratch& scratch, const lsmps_flu
   a.capacity = out.neighbor_count;
   a.total = out.offsets + n;
   a.bits = bits;
+  a.src_pos = src_pos;
   a.status = ctx->d_status;
+  // n_src is the source set's particle count (the cell list holds that many
+  // sorted entries; its particle_count is only a capacity)
+  if (n_src > src.particle_count)
+    return fail(ctx, LSMPS_INVALID_ARGUMENT, "Cell list particle capacity is smaller than particle count");
+  if (n_src > 0) {
+    const int pb = static_cast<int>(std::min<long long>(div_up(static_cast<long long>(n_src), 256),
+                                                        static_cast<long long>(ctx->sm_count) * 8));
+    launch(ctx, sorted_positions_kernel, dim3(pb), dim3(256), 0, sx, sy, sz,
+           static_cast<const index_t*>(src.sorted_indices), static_cast<index_t>(n_src), src_pos);
+  }
   const int blocks = static_cast<int>(std::min<long long>(a.ncell, static_cast<long long>(ctx->sm_count) * 16));
   if (n) launch(ctx, csr_kernel<false>, dim3(blocks), dim3(kCsrThreads), 0, a);
   lsmps_status st = exclusive_scan_i32(ctx, scratch, out.offsets, out.offsets, n, nullptr, out.offsets + n);
@@ -337,7 +363,7 @@ lsmps_status one_neighbor_list(lsmps_ctx* ctx, Scratch& scratch, const lsmps_flu
 size_t neighbor_scratch_bytes(size_t n_fluid, size_t n_wall, size_t ncell) {
   const size_t nmax = n_fluid > n_wall ? n_fluid : n_wall;
   return 2 * cell_list_scratch_bytes(nmax, ncell) + 2 * scan_scratch_bytes(n_fluid + 1) +
-         n_fluid * kMaskWords * sizeof(unsigned) + 4096;
+         n_fluid * kMaskWords * sizeof(unsigned) + nmax * sizeof(double4) + 4096;
 }
 
 lsmps_status build_neighbor_lists_impl(lsmps_ctx* ctx, Scratch& scratch, const lsmps_fluid& fluid,
@@ -348,14 +374,17 @@ lsmps_status build_neighbor_lists_impl(lsmps_ctx* ctx, Scratch& scratch, const l
   if (radius > p.grid.cell_size)
     return fail(ctx, LSMPS_INVALID_ARGUMENT, "Neighbor search currently requires radius <= cell_size");
   unsigned* bits = scratch.take<unsigned>(fluid.count * kMaskWords + 1);
-  if (!bits) return fail(ctx, LSMPS_CUDA_ERROR, "neighbour scratch exhausted");
+  double4* src_pos = scratch.take<double4>(std::max(fluid.count, walls.count) + 1);
+  if (!bits || !src_pos) return fail(ctx, LSMPS_CUDA_ERROR, "neighbour scratch exhausted");
   lsmps_status st = build_cell_list_impl(ctx, scratch, fluid.x, fluid.y, fluid.z, fluid.count, p.grid, fc);
   if (!st) st = build_cell_list_impl(ctx, scratch, walls.x, walls.y, walls.z, walls.count, p.grid, wc);
   // the two tables run one after the other on the stream and share the masks
   if (!st)
-    st = one_neighbor_list(ctx, scratch, fluid, fluid.x, fluid.y, fluid.z, fc, fc, p.grid, radius, true, fn, bits);
+    st = one_neighbor_list(ctx, scratch, fluid, fluid.x, fluid.y, fluid.z, fc, fc, p.grid, radius, true, fn,
+                           fluid.count, bits, src_pos);
   if (!st)
-    st = one_neighbor_list(ctx, scratch, fluid, walls.x, walls.y, walls.z, fc, wc, p.grid, radius, false, wn, bits);
+    st = one_neighbor_list(ctx, scratch, fluid, walls.x, walls.y, walls.z, fc, wc, p.grid, radius, false, wn,
+                           walls.count, bits, src_pos);
   return st;
 }
 

@@ -171,23 +171,31 @@ __global__ void __launch_bounds__(kSurfaceThreads) classify_kernel(SurfaceArgs a
 // expand_near_surface_kernel, surface_detection.cu:322-348.  Only Inner rows
 // are written and only Surface labels are read, so the pass is race-free.
 // Reads the 4-byte label of each neighbour first; positions are read only
-// for the (few) Surface neighbours.
+// for the (few) Surface neighbours.  kExpandLanes lanes share a row (lane l
+// takes entries l, l + kExpandLanes, ...); the answer is whether any lane
+// found a Surface neighbour within r_ns, which does not depend on the order.
+constexpr int kExpandLanes = 4;
+
 __global__ void __launch_bounds__(kSurfaceThreads) expand_kernel(const double4* __restrict__ fp, int32_t* type,
                                                                  index_t n, const index_t* __restrict__ fo,
                                                                  const index_t* __restrict__ fi, double r2) {
-  const index_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n || type[i] != LSMPS_SURFACE_INNER) return;
+  const index_t i = (blockIdx.x * blockDim.x + threadIdx.x) / kExpandLanes;
+  const int l = threadIdx.x & (kExpandLanes - 1);
+  if (i >= n || type[i] != LSMPS_SURFACE_INNER) return;  // the whole group
   const double4 own = ld4(fp, i);
-  for (index_t o = fo[i]; o < fo[i + 1]; ++o) {
+  bool near = false;
+  const index_t fe = fo[i + 1];
+  for (index_t o = fo[i] + l; o < fe && !near; o += kExpandLanes) {
     const index_t j = fi[o];
     if (type[j] != LSMPS_SURFACE_SURFACE) continue;
     const double4 q = ld4(fp, j);
     const double dx = q.x - own.x, dy = q.y - own.y, dz = q.z - own.z;
-    if (dx * dx + dy * dy + dz * dz <= r2) {
-      type[i] = LSMPS_SURFACE_NEAR_SURFACE;
-      return;
-    }
+    near = dx * dx + dy * dy + dz * dz <= r2;
   }
+  // Only Inner rows are written and only Surface labels are read, so the
+  // in-place update is race-free.
+  const unsigned hit = __ballot_sync(group_mask<kExpandLanes>(), near);
+  if (l == 0 && hit != 0u) type[i] = LSMPS_SURFACE_NEAR_SURFACE;
 }
 
 }  // namespace
@@ -240,7 +248,8 @@ lsmps_status classify_surface_impl(lsmps_ctx* ctx, const lsmps_fluid& fluid, con
   const index_t n = static_cast<index_t>(fluid.count);
   launch(ctx, classify_kernel, dim3(div_up(n, kSurfaceThreads)), dim3(kSurfaceThreads), 0, a);
   if (p.near_surface_radius > 0.0) {
-    launch(ctx, expand_kernel, dim3(div_up(n, kSurfaceThreads)), dim3(kSurfaceThreads), 0,
+    launch(ctx, expand_kernel, dim3(div_up(static_cast<long long>(n) * kExpandLanes, kSurfaceThreads)),
+           dim3(kSurfaceThreads), 0,
            static_cast<const double4*>(ctx->pack_fluid[0]), fluid.surface_type, n,
            static_cast<const index_t*>(fn.offsets), static_cast<const index_t*>(fn.indices),
            p.near_surface_radius * p.near_surface_radius);
