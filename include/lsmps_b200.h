@@ -401,6 +401,19 @@ lsmps_status lsmps_classify_surface(lsmps_ctx* ctx, const lsmps_fluid* fluid,
                                     const lsmps_csr* wall_neighbors, const lsmps_params* params,
                                     const lsmps_surface_diagnostics* diagnostics);
 
+/* compute_virtual_light_diagnostics(...), surface_detection.cuh:38-43
+ * (src/surface/surface_detection.cu:350-475, 555-578).  For each fluid
+ * particle, how many of the reference's 14 fixed light directions (the six
+ * axes and eight diagonals in the coordinate planes) stay open: a direction
+ * is blocked when a fluid neighbour (and, with include_wall_neighbors, a wall
+ * neighbour) within the support radius lies inside the cone of
+ * virtual_light_cone_cosine around it.  open_direction_count[i] gets the
+ * count, open_fraction[i] the count / 14; either may be NULL, not both. */
+lsmps_status lsmps_virtual_light(lsmps_ctx* ctx, const lsmps_fluid* fluid, const lsmps_walls* walls,
+                                 const lsmps_csr* fluid_neighbors, const lsmps_csr* wall_neighbors,
+                                 const lsmps_params* params, int32_t* open_direction_count,
+                                 double* open_fraction);
+
 /* ------------------------------------------------------------------------- */
 /* Moment matrices: include/lsmps3d/moment_matrix/moment_matrix.cuh          */
 /* ------------------------------------------------------------------------- */

@@ -264,6 +264,7 @@ _SIGNATURES = {
     "lsmps_build_neighbor_lists": (c_int, [c_void_p, P(Fluid), P(Walls), P(Params), P(Cells), P(Cells), P(Csr), P(Csr)]),
     "lsmps_reference_number_density": (c_double, [c_double, c_double]),
     "lsmps_classify_surface": (c_int, [c_void_p, P(Fluid), P(Walls), P(Csr), P(Csr), P(Params), P(SurfaceDiagnostics)]),
+    "lsmps_virtual_light": (c_int, [c_void_p, P(Fluid), P(Walls), P(Csr), P(Csr), P(Params), c_void_p, c_void_p]),
     "lsmps_prepare_moments": (c_int, [c_void_p, P(Fluid), P(Walls), P(Csr), P(Csr), P(Params), P(Moment), c_int]),
     "lsmps_velocity_laplacian": (c_int, [c_void_p, P(Fluid), P(Walls), P(Csr), P(Csr), P(Moment), P(Vector)]),
     "lsmps_temporary_velocity": (c_int, [c_void_p, P(Fluid), P(Params), P(Vector), P(Fluid)]),

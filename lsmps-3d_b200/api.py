@@ -150,6 +150,14 @@ class Context:
             self.h, r(b.fluid_view()), r(b.walls_view()), r(b.csr_view("fluid")), r(b.csr_view("wall")),
             r(params), r(diagnostics) if diagnostics is not None else None))
 
+    def virtual_light(self, b: StepBuffers, params: abi.Params, open_count_ptr: int | None,
+                      open_fraction_ptr: int | None) -> None:
+        """compute_virtual_light_diagnostics (surface_detection.cu:555-578): open-direction count
+        (int32) and fraction (float64) per fluid particle into caller-owned device buffers."""
+        self.check(_lib.lsmps_virtual_light(
+            self.h, r(b.fluid_view()), r(b.walls_view()), r(b.csr_view("fluid")), r(b.csr_view("wall")),
+            r(params), open_count_ptr, open_fraction_ptr))
+
     def prepare_moments(self, b: StepBuffers, params: abi.Params, kinds) -> None:
         b.params_for_moment = params
         arr = (abi.Moment * len(kinds))(*[b.moment_view(k) for k in kinds])

@@ -11,6 +11,9 @@ double reference_number_density(double l0, double re);
 lsmps_status classify_surface_impl(lsmps_ctx* ctx, const lsmps_fluid& fluid, const lsmps_walls& walls,
                                    const lsmps_csr& fn, const lsmps_csr& wn, const lsmps_params& p,
                                    const lsmps_surface_diagnostics* diag);
+lsmps_status virtual_light_impl(lsmps_ctx* ctx, const lsmps_fluid& fluid, const lsmps_walls& walls,
+                                const lsmps_csr& fn, const lsmps_csr& wn, const lsmps_params& p,
+                                int32_t* open_count, double* open_fraction);
 lsmps_status prepare_moments_impl(lsmps_ctx* ctx, const lsmps_fluid& fluid, const lsmps_walls& walls,
                                   const lsmps_csr& fn, const lsmps_csr& wn, const lsmps_params& p,
                                   const lsmps_moment* kinds, int count);

@@ -198,7 +198,105 @@ __global__ void __launch_bounds__(kSurfaceThreads) expand_kernel(const double4* 
   if (l == 0 && hit != 0u) type[i] = LSMPS_SURFACE_NEAR_SURFACE;
 }
 
+// Virtual-light openness, virtual_light_kernel (surface_detection.cu:445-475).
+// The 14 light directions of virtual_light_direction (:350-382): the six axes,
+// then (±1, ±1, 0)/√2 in the order ++, +-, -+, --, then (1, 0, ±1)/√2 and
+// (0, 1, ±1)/√2.  A direction is blocked when some neighbour within the
+// support radius has (d · dir)/|d| >= cone cosine.
+//
+// The reference walks the neighbour rows once per direction (14 passes); here
+// each neighbour is read once and tested against all 14 directions, and the
+// blocked directions are kept as a 14-bit mask.  Whether a direction is
+// blocked does not depend on the order in which neighbours are tested, so
+// kLightLanes lanes share a row and OR their masks.  The projection is the
+// reference's expression, (dx·ux + dy·uy + dz·uz)·rsqrt(d²), term for term.
+constexpr int kLightDirections = 14;
+constexpr int kLightLanes = 4;
+
+__device__ __forceinline__ void light_direction(int k, double& ux, double& uy, double& uz) {
+  constexpr double s = 0.7071067811865475;
+  const double axis[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+  const double diag[8][3] = {{s, s, 0}, {s, -s, 0}, {-s, s, 0}, {-s, -s, 0},
+                             {s, 0, s}, {s, 0, -s}, {0, s, s},  {0, s, -s}};
+  const double* u = k < 6 ? axis[k] : diag[k - 6];
+  ux = u[0];
+  uy = u[1];
+  uz = u[2];
+}
+
+__device__ __forceinline__ unsigned blocked_directions(double dx, double dy, double dz, double re2, double cone) {
+  const double d2 = dx * dx + dy * dy + dz * dz;
+  if (d2 <= 0.0 || d2 > re2) return 0u;
+  const double inv = safe_rsqrt(d2);
+  unsigned mask = 0u;
+#pragma unroll
+  for (int k = 0; k < kLightDirections; ++k) {
+    double ux, uy, uz;
+    light_direction(k, ux, uy, uz);
+    const double projection = (dx * ux + dy * uy + dz * uz) * inv;
+    if (projection >= cone) mask |= 1u << k;
+  }
+  return mask;
+}
+
+__global__ void __launch_bounds__(kSurfaceThreads)
+    virtual_light_kernel(const double4* __restrict__ fp, const double4* __restrict__ wp, index_t n,
+                         const index_t* __restrict__ fo, const index_t* __restrict__ fi,
+                         const index_t* __restrict__ wo, const index_t* __restrict__ wi, int include_walls,
+                         double re2, double cone, int32_t* open_count, double* open_fraction) {
+  const index_t i = (blockIdx.x * blockDim.x + threadIdx.x) / kLightLanes;
+  const int l = threadIdx.x & (kLightLanes - 1);
+  if (i >= n) return;  // the whole group
+  const double4 own = ld4(fp, i);
+  constexpr unsigned kAll = (1u << kLightDirections) - 1u;
+  unsigned blocked = 0u;
+  const index_t fe = fo[i + 1];
+  for (index_t o = fo[i] + l; o < fe && blocked != kAll; o += kLightLanes) {
+    const double4 q = ld4(fp, fi[o]);
+    blocked |= blocked_directions(q.x - own.x, q.y - own.y, q.z - own.z, re2, cone);
+  }
+  if (include_walls) {
+    const index_t we = wo[i + 1];
+    for (index_t o = wo[i] + l; o < we && blocked != kAll; o += kLightLanes) {
+      const double4 q = ld4(wp, wi[o]);
+      blocked |= blocked_directions(q.x - own.x, q.y - own.y, q.z - own.z, re2, cone);
+    }
+  }
+  blocked = __reduce_or_sync(group_mask<kLightLanes>(), blocked);
+  if (l != 0) return;
+  const int open = kLightDirections - __popc(blocked);
+  if (open_count) open_count[i] = open;
+  if (open_fraction) open_fraction[i] = static_cast<double>(open) / static_cast<double>(kLightDirections);
+}
+
 }  // namespace
+
+lsmps_status virtual_light_impl(lsmps_ctx* ctx, const lsmps_fluid& fluid, const lsmps_walls& walls,
+                                const lsmps_csr& fn, const lsmps_csr& wn, const lsmps_params& p,
+                                int32_t* open_count, double* open_fraction) {
+  // validate_surface_inputs and the checks of compute_virtual_light_diagnostics,
+  // surface_detection.cu:477-492, 555-578.
+  if (!(p.support_radius > 0.0))
+    return fail(ctx, LSMPS_INVALID_ARGUMENT, "Surface detection support radius must be positive");
+  if (fluid.count > fn.particle_count || fluid.count > wn.particle_count)
+    return fail(ctx, LSMPS_INVALID_ARGUMENT, "Surface detection neighbor lists are smaller than fluid particle count");
+  if (!(p.virtual_light_cone_cosine >= -1.0 && p.virtual_light_cone_cosine <= 1.0))
+    return fail(ctx, LSMPS_INVALID_ARGUMENT, "Virtual light cone cosine must be in [-1, 1]");
+  if (!open_count && !open_fraction)
+    return fail(ctx, LSMPS_INVALID_ARGUMENT, "Virtual light diagnostics require at least one output buffer");
+  if (fluid.count == 0) return LSMPS_OK;
+  if (!ensure_packs(ctx, fluid.count, walls.count)) return fail(ctx, LSMPS_CUDA_ERROR, "pack allocation failed");
+  pack4(ctx, fluid.x, fluid.y, fluid.z, nullptr, fluid.count, ctx->pack_fluid[0]);
+  pack4(ctx, walls.x, walls.y, walls.z, nullptr, walls.count, ctx->pack_wall[0]);
+  const index_t n = static_cast<index_t>(fluid.count);
+  launch(ctx, virtual_light_kernel, dim3(div_up(static_cast<long long>(n) * kLightLanes, kSurfaceThreads)),
+         dim3(kSurfaceThreads), 0, static_cast<const double4*>(ctx->pack_fluid[0]),
+         static_cast<const double4*>(ctx->pack_wall[0]), n, static_cast<const index_t*>(fn.offsets),
+         static_cast<const index_t*>(fn.indices), static_cast<const index_t*>(wn.offsets),
+         static_cast<const index_t*>(wn.indices), p.include_wall_neighbors ? 1 : 0,
+         p.support_radius * p.support_radius, p.virtual_light_cone_cosine, open_count, open_fraction);
+  return check_launch(ctx, "virtual light diagnostics");
+}
 
 // compute_uniform_reference_number_density, surface_detection.cu:494-520.
 double reference_number_density(double l0, double re) {
@@ -273,5 +371,17 @@ extern "C" lsmps_status lsmps_classify_surface(lsmps_ctx* ctx, const lsmps_fluid
   lsmps_status st = begin_call(ctx);
   if (st) return st;
   st = classify_surface_impl(ctx, *fluid, *walls, *fluid_neighbors, *wall_neighbors, *params, diagnostics);
+  return end_call(ctx, st);
+}
+
+extern "C" lsmps_status lsmps_virtual_light(lsmps_ctx* ctx, const lsmps_fluid* fluid, const lsmps_walls* walls,
+                                            const lsmps_csr* fluid_neighbors, const lsmps_csr* wall_neighbors,
+                                            const lsmps_params* params, int32_t* open_direction_count,
+                                            double* open_fraction) {
+  if (!ctx || !fluid || !walls || !fluid_neighbors || !wall_neighbors || !params) return LSMPS_INVALID_ARGUMENT;
+  lsmps_status st = begin_call(ctx);
+  if (st) return st;
+  st = virtual_light_impl(ctx, *fluid, *walls, *fluid_neighbors, *wall_neighbors, *params, open_direction_count,
+                          open_fraction);
   return end_call(ctx, st);
 }

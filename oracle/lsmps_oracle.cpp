@@ -1037,6 +1037,57 @@ int oracle_classify_surface(const lsmps_fluid* f, const lsmps_walls* w, const ls
   return LSMPS_OK;
 }
 
+// compute_virtual_light_diagnostics, surface_detection.cu:555-578, with
+// virtual_light_kernel (:445-475): for each of the 14 directions of
+// virtual_light_direction (:350-382), one pass over the fluid row and, when
+// the fluid row did not block it and walls are included, one over the wall
+// row (fluid_neighbor_blocks_light :384-412, wall_neighbor_blocks_light
+// :414-443).  The projection is computed without contraction here; the
+// device computes the same expression with the compiler's FMA contraction,
+// so the two can differ only for a neighbour whose projection lies within a
+// few ulp of the cone cosine.
+int oracle_virtual_light(const lsmps_fluid* f, const lsmps_walls* w, const lsmps_csr* fn,
+                         const lsmps_csr* wn, const lsmps_params* p, int32_t* open_count,
+                         double* open_fraction) {
+  if (p->support_radius <= 0.0) return LSMPS_INVALID_ARGUMENT;
+  if (!(p->virtual_light_cone_cosine >= -1.0 && p->virtual_light_cone_cosine <= 1.0))
+    return LSMPS_INVALID_ARGUMENT;
+  if (!open_count && !open_fraction) return LSMPS_INVALID_ARGUMENT;
+  constexpr double s = 0.7071067811865475;
+  static const double dirs[14][3] = {{1, 0, 0},  {-1, 0, 0}, {0, 1, 0},  {0, -1, 0}, {0, 0, 1},
+                                     {0, 0, -1}, {s, s, 0},  {s, -s, 0}, {-s, s, 0}, {-s, -s, 0},
+                                     {s, 0, s},  {s, 0, -s}, {0, s, s},  {0, s, -s}};
+  const double re2 = p->support_radius * p->support_radius;
+  const double cone = p->virtual_light_cone_cosine;
+  const int64_t count = static_cast<int64_t>(f->count);
+  auto row_blocks = [&](size_t i, const double* sx, const double* sy, const double* sz,
+                        const lsmps_csr* nb, const double* dir) {
+    const double px = f->x[i], py = f->y[i], pz = f->z[i];
+    for (index_t o = nb->offsets[i]; o < nb->offsets[i + 1]; ++o) {
+      const index_t j = nb->indices[o];
+      const double dx = sx[j] - px, dy = sy[j] - py, dz = sz[j] - pz;
+      const double d2 = dx * dx + dy * dy + dz * dz;
+      if (d2 <= 0.0 || d2 > re2) continue;
+      const double projection = (dx * dir[0] + dy * dir[1] + dz * dir[2]) * safe_rsqrt(d2);
+      if (projection >= cone) return true;
+    }
+    return false;
+  };
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int64_t i = 0; i < count; ++i) {
+    int open = 0;
+    for (int k = 0; k < 14; ++k) {
+      bool blocked = row_blocks(static_cast<size_t>(i), f->x, f->y, f->z, fn, dirs[k]);
+      if (!blocked && p->include_wall_neighbors)
+        blocked = row_blocks(static_cast<size_t>(i), w->x, w->y, w->z, wn, dirs[k]);
+      if (!blocked) ++open;
+    }
+    if (open_count) open_count[i] = open;
+    if (open_fraction) open_fraction[i] = static_cast<double>(open) / 14.0;
+  }
+  return LSMPS_OK;
+}
+
 int oracle_prepare_moment(const lsmps_fluid* f, const lsmps_walls* w, const lsmps_csr* fn,
                           const lsmps_csr* wn, const lsmps_params* p, const lsmps_moment* out) {
   return prepare_moment(f, w, fn, wn, p, out);

@@ -51,6 +51,8 @@ def lib(abi):
         "oracle_reference_number_density": (c_double, [c_double, c_double]),
         "oracle_classify_surface": (c_int, [P(abi.Fluid), P(abi.Walls), P(abi.Csr), P(abi.Csr), P(abi.Params),
                                             P(abi.SurfaceDiagnostics)]),
+        "oracle_virtual_light": (c_int, [P(abi.Fluid), P(abi.Walls), P(abi.Csr), P(abi.Csr), P(abi.Params),
+                                         c_void_p, c_void_p]),
         "oracle_prepare_moment": (c_int, [P(abi.Fluid), P(abi.Walls), P(abi.Csr), P(abi.Csr), P(abi.Params),
                                           P(abi.Moment)]),
         "oracle_velocity_laplacian": (c_int, [P(abi.Fluid), P(abi.Walls), P(abi.Csr), P(abi.Csr), P(abi.Moment),
@@ -114,6 +116,13 @@ class Oracle:
     def classify_surface(self, b, params, diag=None) -> int:
         return self.L.oracle_classify_surface(r(b.fluid_view()), r(b.walls_view()), r(b.csr_view("fluid")),
                                               r(b.csr_view("wall")), r(params), r(diag) if diag is not None else None)
+
+    def virtual_light(self, b, params, open_count=None, open_fraction=None) -> int:
+        """open_count: int32 array, open_fraction: float64 array (numpy), either may be None."""
+        return self.L.oracle_virtual_light(
+            r(b.fluid_view()), r(b.walls_view()), r(b.csr_view("fluid")), r(b.csr_view("wall")), r(params),
+            open_count.ctypes.data if open_count is not None else None,
+            open_fraction.ctypes.data if open_fraction is not None else None)
 
     def prepare_moment(self, b, params, kind) -> int:
         b.params_for_moment = params

@@ -308,4 +308,23 @@ int ref_download_correction(void* handle, const lsmps_vector* gradient, const ls
   return 0;
 }
 
+// compute_virtual_light_diagnostics on the current geometry (after
+// ref_rebuild); the open-direction counts and fractions into host arrays.
+int ref_virtual_light(void* handle, int32_t* open_count, double* open_fraction) {
+  auto* h = static_cast<Harness*>(handle);
+  auto v = h->workspace->view();
+  const size_t n = v.fluid.count;
+  int* d_count = nullptr;
+  real* d_fraction = nullptr;
+  LSMPS3D_CUDA_CHECK(cudaMalloc(&d_count, (n ? n : 1) * sizeof(int)));
+  LSMPS3D_CUDA_CHECK(cudaMalloc(&d_fraction, (n ? n : 1) * sizeof(real)));
+  compute_virtual_light_diagnostics(v.fluid, v.walls, v.fluid_neighbors, v.wall_neighbors, h->config,
+                                    VirtualLightDiagnosticsView{d_count, d_fraction});
+  down(open_count, d_count, n);
+  down(open_fraction, d_fraction, n);
+  cudaFree(d_count);
+  cudaFree(d_fraction);
+  return 0;
+}
+
 }  // extern "C"

@@ -49,6 +49,7 @@ def lib(abi):
         "ref_download_temporary": (c_int, [c_void_p, P(abi.Fluid), P(abi.Walls)]),
         "ref_download_ppe": (c_longlong, [c_void_p, P(abi.Ppe), c_size_t]),
         "ref_download_correction": (c_int, [c_void_p, P(abi.Vector), P(abi.Vector)]),
+        "ref_virtual_light": (c_int, [c_void_p, c_void_p, c_void_p]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -130,3 +131,13 @@ class ReferencePath:
         self.L.ref_download_fluid(self.h, ctypes.byref(b.fluid_view()))
         self.L.ref_download_correction(self.h, ctypes.byref(b.vector_view(b.pressure_gradient)),
                                        ctypes.byref(b.vector_view(b.ps_displacement)))
+
+    def virtual_light(self):
+        """compute_virtual_light_diagnostics of the reference on its current geometry:
+        (open_direction_count int32[N], open_fraction float64[N])."""
+        import numpy as np
+        n = self.b.n_fluid
+        count = np.zeros(n, dtype=np.int32)
+        frac = np.zeros(n, dtype=np.float64)
+        self.L.ref_virtual_light(self.h, count.ctypes.data, frac.ctypes.data)
+        return count, frac

@@ -68,6 +68,9 @@ def main():
             "max_fluid_neighbors": 6,
             "max_wall_neighbors": 4,
             "expected_labels_at": {"0": 1, "1": 2, "6": 3, "7": 0},
+            "virtual_light_source": "tests/unit/smoke_surface_detection.cu:238-264",
+            "expected_open_count_greater": [1, 0],
+            "expected_open_fraction_above": {"6": 0.99},
         },
         "moment_matrix": {
             "source": "tests/unit/smoke_moment_matrix.cu:11-132",

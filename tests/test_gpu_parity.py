@@ -159,6 +159,35 @@ def test_csr_bit_exact_native_order(pipeline):
         assert np.array_equal(gi, hi), which
 
 
+@pytest.mark.parametrize("walls", [1, 0], ids=["with_walls", "fluid_only"])
+def test_virtual_light_matches_oracle(pkg, device_api, pipeline, ctx, oracle, walls):
+    # Open-direction counts are integers: bit-exact.  (The oracle evaluates
+    # the projection without FMA contraction; only a neighbour within a few
+    # ulp of the cone would tell the two apart, and the seeded cases have none.)
+    import torch
+
+    case, dev, host = pipeline
+    p = type(case.params).from_buffer_copy(case.params)
+    p.include_wall_neighbors = walls
+    n = case.n_fluid
+    count = torch.full((n,), -1, dtype=torch.int32, device="cuda")
+    frac = torch.full((n,), -1.0, dtype=torch.float64, device="cuda")
+    ctx.virtual_light(dev, p, count.data_ptr(), frac.data_ptr())
+    hc = np.zeros(n, np.int32)
+    hf = np.zeros(n, np.float64)
+    assert oracle.virtual_light(host, p, hc, hf) == 0
+    gc = count.cpu().numpy()
+    assert np.array_equal(gc, hc), np.flatnonzero(gc != hc)[:10]
+    assert np.array_equal(frac.cpu().numpy(), hf)
+    print(f"{case.name} walls={walls}: open directions histogram {np.bincount(gc, minlength=15).tolist()}")
+    # count only
+    c2 = torch.zeros((n,), dtype=torch.int32, device="cuda")
+    ctx.virtual_light(dev, p, c2.data_ptr(), None)
+    assert torch.equal(c2, count)
+    with pytest.raises(device_api.LsmpsError):
+        ctx.virtual_light(dev, p, None, None)
+
+
 def test_pipeline_stages_match_oracle(pkg, pipeline, ctx, oracle):
     case, dev, host = pipeline
     p = case.params

@@ -59,6 +59,16 @@ def test_stages_against_reference_cuda(pkg, device_api, name, kw):
         assert np.array_equal(gi, hi), which
     assert np.array_equal(dev.numpy("fluid")["surface_type"], host.fluid["surface_type"])
 
+    # virtual-light diagnostic on the same geometry: integer counts, bit-exact
+    import torch
+
+    rc, rf = ref.virtual_light()
+    gc = torch.zeros(case.n_fluid, dtype=torch.int32, device="cuda")
+    gf = torch.zeros(case.n_fluid, dtype=torch.float64, device="cuda")
+    ctx.virtual_light(dev, p, gc.data_ptr(), gf.data_ptr())
+    assert np.array_equal(gc.cpu().numpy(), rc)
+    assert np.array_equal(gf.cpu().numpy(), rf)
+
     # provision (moments of this generation + u*)
     ref.provision()
     ref.fetch_moments(p)

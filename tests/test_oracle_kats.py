@@ -64,6 +64,61 @@ def test_surface_detection_kat(pkg, oracle, kats):
     assert diag_arrays["air_open_ratio"][1] > 0 and diag_arrays["air_anisotropy"][1] > 0
 
 
+def test_virtual_light_kat(pkg, oracle, kats):
+    # smoke_surface_detection.cu:238-264: the particle at the edge of the
+    # cluster sees more open directions than the centre one, and the isolated
+    # particle 6 sees (almost) all of them.
+    k = kats["surface_detection"]
+    b = buffers_from(pkg, pkg.buffers.NumpyAlloc(), k)
+    p = params_from(pkg, k)
+    assert oracle.build_neighbor_lists(b, p)[0] == 0
+    count = np.zeros(8, np.int32)
+    frac = np.zeros(8, np.float64)
+    assert oracle.virtual_light(b, p, count, frac) == 0
+    hi, lo = k["expected_open_count_greater"]
+    assert count[hi] > count[lo], count.tolist()
+    for i, above in k["expected_open_fraction_above"].items():
+        assert frac[int(i)] > above
+    assert np.array_equal(frac, count / 14.0)
+    # either output alone, and neither (an argument error, surface_detection.cu:567-570)
+    c2 = np.full(8, -1, np.int32)
+    assert oracle.virtual_light(b, p, c2, None) == 0 and np.array_equal(c2, count)
+    assert oracle.virtual_light(b, p, None, None) == pkg.abi.INVALID_ARGUMENT
+    p.virtual_light_cone_cosine = 1.5
+    assert oracle.virtual_light(b, p, count, None) == pkg.abi.INVALID_ARGUMENT
+
+
+def test_virtual_light_lattice(pkg, oracle):
+    # On a cubic lattice with r_e > sqrt(2) l0 every one of the 14 directions
+    # has a neighbour exactly on it (projection 1), so an interior particle is
+    # closed; an isolated particle is open in all 14.  Walls only close
+    # directions when include_wall_neighbors is set.
+    l0 = 1.0
+    pts = [(ix, iy, iz) for iz in range(5) for iy in range(5) for ix in range(5)]
+    pts.append((20.0, 20.0, 20.0))
+    k = {"fluid": {"x": [q[0] * l0 for q in pts], "y": [q[1] * l0 for q in pts], "z": [q[2] * l0 for q in pts]},
+         "walls": {"x": [2.0], "y": [2.0], "z": [-1.0]},
+         "grid": {"origin": [-2.0, -2.0, -2.0], "cell_size": 1.5, "dims": [16, 16, 16]},
+         "params": {"support_radius": 1.5, "particle_spacing": l0, "virtual_light_cone_cosine": 0.8660254,
+                    "include_wall_neighbors": 1},
+         "max_fluid_neighbors": 32, "max_wall_neighbors": 4}
+    b = buffers_from(pkg, pkg.buffers.NumpyAlloc(), k)
+    p = params_from(pkg, k)
+    assert oracle.build_neighbor_lists(b, p)[0] == 0
+    n = len(pts)
+    count = np.zeros(n, np.int32)
+    assert oracle.virtual_light(b, p, count, None) == 0
+    centre = pts.index((2, 2, 2))
+    bottom = pts.index((2, 2, 0))
+    assert count[centre] == 0
+    assert count[n - 1] == 14
+    with_wall = int(count[bottom])
+    p.include_wall_neighbors = 0
+    assert oracle.virtual_light(b, p, count, None) == 0
+    # the wall below closes -z (direction 5) and nothing else near it
+    assert int(count[bottom]) == with_wall + 1
+
+
 def _moment_case(pkg, k):
     b = buffers_from(pkg, pkg.buffers.NumpyAlloc(), k)
     p = params_from(pkg, k)
