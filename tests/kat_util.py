@@ -102,3 +102,35 @@ def row_rel_err(values, ref_values, row_offsets):
     amax = np.maximum.reduceat(a, starts)
     per_row = np.where(amax > 0, dmax / np.where(amax > 0, amax, 1.0), dmax)
     return float(per_row.max()) if per_row.size else 0.0
+
+
+LIGHT_DIRECTIONS = np.array(
+    [[1, 0, 0], [-1, 0, 0], [0, 1, 0], [0, -1, 0], [0, 0, 1], [0, 0, -1]]
+    + [[a * 0.7071067811865475, b * 0.7071067811865475, 0] for a, b in ((1, 1), (1, -1), (-1, 1), (-1, -1))]
+    + [[0.7071067811865475, 0, 0.7071067811865475], [0.7071067811865475, 0, -0.7071067811865475],
+       [0, 0.7071067811865475, 0.7071067811865475], [0, 0.7071067811865475, -0.7071067811865475]])
+
+
+def light_ties(b, params, eps=1e-12):
+    """Per fluid particle, how many of the 14 virtual-light directions have a
+    neighbour whose projection lies within eps of the cone cosine.  Such a
+    direction's open/blocked answer depends on the last bits of the
+    projection (FMA contraction, the device rsqrt), so the CPU oracle and the
+    device may differ there by up to that many directions."""
+    n = b.n_fluid
+    ties = np.zeros((n, 14), dtype=bool)
+    re2 = params.support_radius ** 2
+    rows = [("fluid", b.fluid)]
+    if params.include_wall_neighbors:
+        rows.append(("wall", b.walls))
+    for which, src in rows:
+        off, idx = b.csr_rows(which)
+        owner = np.repeat(np.arange(n), np.diff(off[: n + 1]))
+        idx = idx[: len(owner)]
+        d = np.stack([src[c][idx] - b.fluid[c][owner] for c in ("x", "y", "z")], 1)
+        d2 = (d * d).sum(1)
+        ok = (d2 > 0) & (d2 <= re2)
+        proj = (d[ok] @ LIGHT_DIRECTIONS.T) / np.sqrt(d2[ok])[:, None]
+        near = np.abs(proj - params.virtual_light_cone_cosine) <= eps
+        np.logical_or.at(ties, owner[ok], near)
+    return ties.sum(1)

@@ -12,7 +12,7 @@ so the bound is set by rounding times the moment matrices' conditioning.
 import numpy as np
 import pytest
 
-from kat_util import buffers_from, params_from, rel_err, rows, vec_err
+from kat_util import buffers_from, light_ties, params_from, rel_err, rows, vec_err
 
 pytestmark = pytest.mark.gpu
 
@@ -161,9 +161,14 @@ def test_csr_bit_exact_native_order(pipeline):
 
 @pytest.mark.parametrize("walls", [1, 0], ids=["with_walls", "fluid_only"])
 def test_virtual_light_matches_oracle(pkg, device_api, pipeline, ctx, oracle, walls):
-    # Open-direction counts are integers: bit-exact.  (The oracle evaluates
-    # the projection without FMA contraction; only a neighbour within a few
-    # ulp of the cone would tell the two apart, and the seeded cases have none.)
+    # Open-direction counts are integers: bit-exact, except where a
+    # neighbour's projection lies within 1e-12 of the cone cosine (lattice
+    # vectors at exactly 30 degrees to a light direction): there the answer
+    # depends on the projection's last bits, which the oracle (no FMA
+    # contraction, 1/sqrt) need not share with the device (the reference's own
+    # expression and rsqrt; bit-exact against the reference in
+    # test_gpu_reference.py).  Such particles may differ by at most their
+    # number of tied directions.
     import torch
 
     case, dev, host = pipeline
@@ -177,8 +182,13 @@ def test_virtual_light_matches_oracle(pkg, device_api, pipeline, ctx, oracle, wa
     hf = np.zeros(n, np.float64)
     assert oracle.virtual_light(host, p, hc, hf) == 0
     gc = count.cpu().numpy()
-    assert np.array_equal(gc, hc), np.flatnonzero(gc != hc)[:10]
-    assert np.array_equal(frac.cpu().numpy(), hf)
+    ties = light_ties(host, p)
+    clear = ties == 0
+    assert np.array_equal(gc[clear], hc[clear]), np.flatnonzero(clear & (gc != hc))[:10]
+    assert np.all(np.abs(gc - hc) <= ties)
+    print(f"{case.name} walls={walls}: {int((~clear).sum())} particles with a tied direction, "
+          f"{int((gc != hc).sum())} differ from the oracle")
+    assert np.array_equal(frac.cpu().numpy(), gc / 14.0)
     print(f"{case.name} walls={walls}: open directions histogram {np.bincount(gc, minlength=15).tolist()}")
     # count only
     c2 = torch.zeros((n,), dtype=torch.int32, device="cuda")
