@@ -462,6 +462,47 @@ lsmps_status lsmps_assemble_ppe(lsmps_ctx* ctx, const lsmps_fluid* fluid,
                                 const lsmps_moment* pressure_moment, const lsmps_ppe* workspace);
 
 /* ------------------------------------------------------------------------- */
+/* PPE solve: AmgxPpeSolver::solve, include/lsmps3d/ppe/ppe_matrix.cuh:88-110 */
+/* ------------------------------------------------------------------------- */
+/* The reference solves the assembled system with AMGX (src/ppe/ppe_matrix.cu:
+ * 586-679; a third-party library, used only when found at build time) in
+ * AMGX's GMRES configuration (:604-610).  lsmps_solve_ppe solves it on the
+ * device with restarted GMRES (Saad & Schultz), keeping the reference's
+ * semantics: initial guess zero, stop at max_iters or when the residual's L2
+ * norm reaches tolerance x the initial one, then clamp negative values to
+ * zero (:662).  Works on any square CSR matrix (row_offsets[rows] entries
+ * used; nnz is not read). */
+enum {
+  LSMPS_CONVERGENCE_RELATIVE_INITIAL = 0, /* AMGX "RELATIVE_INI": |r| <= tol |r0| */
+  LSMPS_CONVERGENCE_ABSOLUTE = 1          /* AMGX "ABSOLUTE": |r| <= tol */
+};
+enum {
+  LSMPS_PRECONDITIONER_NONE = 0,  /* AMGX "NOSOLVER" (the reference's configuration) */
+  LSMPS_PRECONDITIONER_JACOBI = 1 /* right preconditioning with diag(A) */
+};
+typedef struct lsmps_solver_options {
+  int32_t max_iters;         /* total Arnoldi steps over all restarts; 100 */
+  int32_t restart;           /* Krylov dimension per cycle, 1..64; 20 */
+  double tolerance;          /* 1e-6 */
+  int32_t convergence;       /* LSMPS_CONVERGENCE_* */
+  int32_t preconditioner;    /* LSMPS_PRECONDITIONER_* */
+  int32_t clamp_negative;    /* 1: pressure = max(pressure, 0) afterwards */
+  int32_t use_initial_guess; /* 0: start from zero, as the reference */
+} lsmps_solver_options;
+typedef struct lsmps_solver_report {
+  int32_t iterations;      /* Arnoldi steps taken */
+  int32_t converged;       /* 1 if the final true residual met the criterion */
+  double initial_residual; /* |b - A x0| */
+  double final_residual;   /* |b - A x| before the clamp */
+} lsmps_solver_report;
+void lsmps_solver_options_default(lsmps_solver_options* options);
+/* options may be NULL (defaults); report may be NULL.  Not capturable in a
+ * CUDA graph: each Arnoldi step reads 17 bytes back to the host. */
+lsmps_status lsmps_solve_ppe(lsmps_ctx* ctx, const lsmps_csr_matrix* matrix, const double* rhs,
+                             double* pressure, const lsmps_solver_options* options,
+                             lsmps_solver_report* report);
+
+/* ------------------------------------------------------------------------- */
 /* Pressure correction: include/lsmps3d/correction/pressure_correction.cuh   */
 /* ------------------------------------------------------------------------- */
 /* clamp_particle_pressure(...), pressure_correction.cuh:91. */

@@ -146,6 +146,33 @@ class Ppe(Structure):
     ]
 
 
+class SolverOptions(Structure):
+    _fields_ = [
+        ("max_iters", c_int32),
+        ("restart", c_int32),
+        ("tolerance", c_double),
+        ("convergence", c_int32),
+        ("preconditioner", c_int32),
+        ("clamp_negative", c_int32),
+        ("use_initial_guess", c_int32),
+    ]
+
+
+class SolverReport(Structure):
+    _fields_ = [
+        ("iterations", c_int32),
+        ("converged", c_int32),
+        ("initial_residual", c_double),
+        ("final_residual", c_double),
+    ]
+
+
+CONVERGENCE_RELATIVE_INITIAL = 0
+CONVERGENCE_ABSOLUTE = 1
+PRECONDITIONER_NONE = 0
+PRECONDITIONER_JACOBI = 1
+
+
 class Params(Structure):
     _fields_ = [
         ("particle_spacing", c_double),
@@ -200,6 +227,13 @@ class StepState(Structure):
         ("smoothed_velocity", Vector),
         ("pressure", c_void_p),
     ]
+
+
+def default_solver_options() -> SolverOptions:
+    """lsmps_solver_options_default: AMGX's GMRES configuration of the
+    reference (src/ppe/ppe_matrix.cu:604-610) with AMGX's restart length 20."""
+    return SolverOptions(max_iters=100, restart=20, tolerance=1e-6, convergence=CONVERGENCE_RELATIVE_INITIAL,
+                         preconditioner=PRECONDITIONER_NONE, clamp_negative=1, use_initial_guess=0)
 
 
 def default_params() -> Params:
@@ -273,6 +307,8 @@ _SIGNATURES = {
         c_int,
         [c_void_p, P(Fluid), P(Walls), P(Params), P(Csr), P(Csr), P(Fluid), P(Walls), P(Moment), P(Moment), P(Ppe)],
     ),
+    "lsmps_solver_options_default": (None, [P(SolverOptions)]),
+    "lsmps_solve_ppe": (c_int, [c_void_p, P(CsrMatrix), c_void_p, c_void_p, P(SolverOptions), P(SolverReport)]),
     "lsmps_clamp_particle_pressure": (c_int, [c_void_p, P(Fluid), c_void_p]),
     "lsmps_pressure_gradient": (
         c_int,

@@ -190,6 +190,20 @@ class Context:
             r(b.vector_view(b.pressure_gradient)), r(b.vector_view(b.ps_displacement)),
             r(b.vector_view(b.smoothed_velocity))))
 
+    def solve_csr(self, matrix: abi.CsrMatrix, rhs_ptr: int, x_ptr: int,
+                  options: abi.SolverOptions | None = None) -> abi.SolverReport:
+        """lsmps_solve_ppe on any square device CSR system (AmgxPpeSolver::solve,
+        src/ppe/ppe_matrix.cu:586-679): restarted GMRES from zero, then the clamp."""
+        rep = abi.SolverReport()
+        self.check(_lib.lsmps_solve_ppe(self.h, r(matrix), ctypes.c_void_p(rhs_ptr), ctypes.c_void_p(x_ptr),
+                                        r(options) if options is not None else None, r(rep)))
+        return rep
+
+    def solve_ppe(self, b: StepBuffers, options: abi.SolverOptions | None = None) -> abi.SolverReport:
+        """Solve the assembled PPE rows of `b` into b.ppe["pressure"]."""
+        v = b.ppe_view()
+        return self.solve_csr(v.matrix, v.rhs, v.pressure, options)
+
     def step(self, b: StepBuffers, params: abi.Params, state: abi.StepState | None = None) -> None:
         s = state if state is not None else b.step_state(params)
         self.check(_lib.lsmps_step(self.h, r(params), r(s)))

@@ -4,6 +4,12 @@
 // function, and the AmgxPpeSolver front end.
 #include "lsmps3d/ppe/ppe_matrix.cuh"
 
+#include <cstdlib>
+#include <filesystem>
+#include <fstream>
+#include <iostream>
+#include <sstream>
+#include <string>
 #include <utility>
 
 #include "dropin.hpp"
@@ -151,9 +157,93 @@ void assemble_ppe_matrix_and_rhs(const FluidParticleSoA& fluid, const WallPartic
   dropin::check(lsmps_assemble_ppe(dropin::context(), &f, &w, &p, &fn, &wn, &tv, &tw, &vm, &pm, &ws));
 }
 
-// AmgxPpeSolver (ppe_matrix.cu:553-679).  AMGX is a third-party library that
-// this build does not link; the front end behaves as the reference's build
-// without LSMPS3D_ENABLE_AMGX: not available, and solve() reports that.
+// AmgxPpeSolver (ppe_matrix.cu:553-679).  The reference hands the system to
+// AMGX; here lsmps_solve_ppe runs the same method on the device (restarted
+// GMRES from a zero initial guess, then the clamp of negative pressures)
+// without the host round trip of the CSR.  The configuration file, when one
+// is given and exists, is read in AMGX's JSON form for the settings that
+// method has: the outer solver must be GMRES; max_iters, tolerance,
+// gmres_n_restart, convergence (RELATIVE_INI or ABSOLUTE) and the
+// preconditioner's solver (NOSOLVER, or BLOCK_JACOBI / JACOBI_L1 for
+// diagonal scaling) are honoured.  Without a file the settings are the
+// reference's built-in configuration (:604-610).
+namespace {
+
+std::string read_text(const std::filesystem::path& path) {
+  std::ifstream in(path);
+  std::ostringstream text;
+  text << in.rdbuf();
+  return text.str();
+}
+
+// Position just after `"key"` and the following ':' (npos if absent).
+size_t value_of(const std::string& text, const std::string& key, size_t from = 0) {
+  const size_t k = text.find("\"" + key + "\"", from);
+  if (k == std::string::npos) return std::string::npos;
+  const size_t colon = text.find(':', k + key.size() + 2);
+  return colon == std::string::npos ? std::string::npos : colon + 1;
+}
+
+bool number_of(const std::string& text, const std::string& key, double& out) {
+  const size_t v = value_of(text, key);
+  if (v == std::string::npos) return false;
+  char* end = nullptr;
+  const double d = std::strtod(text.c_str() + v, &end);
+  if (end == text.c_str() + v) return false;
+  out = d;
+  return true;
+}
+
+// The string value that starts at v (after blanks); empty for other values.
+std::string string_at(const std::string& text, size_t v) {
+  if (v == std::string::npos) return {};
+  const size_t a = text.find_first_not_of(" \t\r\n", v);
+  if (a == std::string::npos || text[a] != '"') return {};
+  const size_t b = a == std::string::npos ? a : text.find('"', a + 1);
+  return b == std::string::npos ? std::string() : text.substr(a + 1, b - a - 1);
+}
+
+lsmps_solver_options options_from(const std::filesystem::path& path) {
+  lsmps_solver_options o;
+  lsmps_solver_options_default(&o);
+  std::error_code ec;
+  if (path.empty() || !std::filesystem::exists(path, ec)) return o;
+  const std::string text = read_text(path);
+  // The outer solver: the "solver" value that is not the preconditioner's.
+  const size_t pre = value_of(text, "preconditioner");
+  std::string outer;
+  for (size_t at = 0;;) {
+    const size_t v = value_of(text, "solver", at);
+    if (v == std::string::npos) break;
+    const std::string name = string_at(text, v);
+    const bool in_preconditioner = pre != std::string::npos && v > pre && text.find('}', pre) > v;
+    if (!name.empty() && !in_preconditioner) outer = name;
+    at = v;
+  }
+  if (outer != "GMRES") dropin::fail("PPE solver configuration " + path.string() + " must use GMRES");
+  double d = 0.0;
+  if (number_of(text, "max_iters", d)) o.max_iters = static_cast<int32_t>(d);
+  if (number_of(text, "tolerance", d)) o.tolerance = d;
+  if (number_of(text, "gmres_n_restart", d)) o.restart = static_cast<int32_t>(d);
+  const std::string convergence = string_at(text, value_of(text, "convergence"));
+  if (convergence == "ABSOLUTE") {
+    o.convergence = LSMPS_CONVERGENCE_ABSOLUTE;
+  } else if (!convergence.empty() && convergence != "RELATIVE_INI" && convergence != "RELATIVE_INI_CORE") {
+    dropin::fail("unsupported PPE solver convergence " + convergence);
+  }
+  if (pre != std::string::npos) {
+    const std::string name = string_at(text, value_of(text, "solver", pre));
+    if (name == "BLOCK_JACOBI" || name == "JACOBI_L1") {
+      o.preconditioner = LSMPS_PRECONDITIONER_JACOBI;
+    } else if (!name.empty() && name != "NOSOLVER") {
+      dropin::fail("unsupported PPE preconditioner " + name);
+    }
+  }
+  return o;
+}
+
+}  // namespace
+
 struct AmgxPpeSolver::Impl {
   Impl(std::filesystem::path path, bool stats) : config_path(std::move(path)), print_solve_stats(stats) {}
   std::filesystem::path config_path;
@@ -167,7 +257,7 @@ AmgxPpeSolver::~AmgxPpeSolver() = default;
 AmgxPpeSolver::AmgxPpeSolver(AmgxPpeSolver&&) noexcept = default;
 AmgxPpeSolver& AmgxPpeSolver::operator=(AmgxPpeSolver&&) noexcept = default;
 
-bool AmgxPpeSolver::is_available() noexcept { return false; }
+bool AmgxPpeSolver::is_available() noexcept { return true; }
 
 const std::filesystem::path& AmgxPpeSolver::config_path() const noexcept { return impl_->config_path; }
 
@@ -176,9 +266,15 @@ void AmgxPpeSolver::solve(const CsrMatrixView& matrix, const real* rhs, real* pr
   if (matrix.rows != matrix.cols || matrix.row_offsets == nullptr || matrix.col_indices == nullptr ||
       matrix.values == nullptr || rhs == nullptr || pressure == nullptr)
     dropin::fail("AMGX PPE solve requires a square CSR matrix, rhs, and solution buffer");
-  dropin::fail(
-      "AMGX support is not enabled in this build. Configure with AMGX headers and library available to use "
-      "AmgxPpeSolver.");
+  const lsmps_solver_options options = options_from(impl_->config_path);
+  const lsmps_csr_matrix a{matrix.rows, matrix.cols, matrix.nnz, matrix.row_offsets, matrix.col_indices,
+                           matrix.values};
+  lsmps_solver_report report{};
+  dropin::check(lsmps_solve_ppe(dropin::context(), &a, rhs, pressure, &options, &report));
+  if (impl_->print_solve_stats)
+    std::cout << "PPE GMRES(" << options.restart << "): " << report.iterations << " iterations, residual "
+              << report.initial_residual << " -> " << report.final_residual
+              << (report.converged ? " (converged)" : " (not converged)") << std::endl;
 }
 
 }  // namespace lsmps3d

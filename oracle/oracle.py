@@ -74,6 +74,8 @@ def lib(abi):
                                                c_void_p, P(abi.Params), P(abi.Moment), P(abi.Vector),
                                                P(abi.Vector), P(abi.Vector)]),
         "oracle_step": (c_int, [P(abi.Params), P(abi.StepState), P(c_uint64)]),
+        "oracle_solve_ppe": (c_int, [P(abi.CsrMatrix), c_void_p, c_void_p, P(abi.SolverOptions),
+                                     P(abi.SolverReport)]),
         "oracle_max_threads": (c_int, []),
     }
     for name, (res, args) in sig.items():
@@ -160,3 +162,11 @@ class Oracle:
         req = (c_uint64 * 2)()
         st = self.L.oracle_step(r(params), r(b.step_state(params)), req)
         return st, (int(req[0]), int(req[1]))
+
+    def solve_ppe(self, row_offsets, col_indices, values, rhs, x, options):
+        """GMRES on a host CSR system (numpy arrays); returns (status, SolverReport)."""
+        A = self.abi.CsrMatrix(len(row_offsets) - 1, len(row_offsets) - 1, len(values), row_offsets.ctypes.data,
+                               col_indices.ctypes.data, values.ctypes.data)
+        rep = self.abi.SolverReport()
+        st = self.L.oracle_solve_ppe(r(A), rhs.ctypes.data, x.ctypes.data, r(options), r(rep))
+        return st, rep

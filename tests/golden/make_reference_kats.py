@@ -96,6 +96,13 @@ def main():
             "tolerance": 2.0e-3,
             "expected_workspace_bytes": (27 + 2) * 3 * 8,
         },
+        "ppe_solve": {
+            "source": "tests/unit/smoke_ppe_matrix.cu:52-117",
+            "row_offsets": [0, 2, 4], "col_indices": [0, 1, 0, 1], "values": [4.0, -1.0, -1.0, 4.0],
+            "rhs": [3.0, 3.0], "expected": [1.0, 1.0],
+            "negated_rhs": [-3.0, -3.0], "expected_negated_clamped": [0.0, 0.0],
+            "tolerance": 2.0e-5,
+        },
         "ppe": {
             "source": "tests/unit/smoke_ppe_matrix.cu:119-286",
             "fluid": {"x": x, "y": y, "z": z, "vx": list(x), "vy": [2.0 * b for b in y], "vz": [3.0 * c for c in z]},

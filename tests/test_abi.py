@@ -57,13 +57,22 @@ def test_host_only_entry_points(lib, pkg):
             assert a == b, name
 
 
+def test_solver_options_default(lib, pkg):
+    o = pkg.abi.SolverOptions()
+    lib.lsmps_solver_options_default(ctypes.byref(o))
+    d = pkg.abi.default_solver_options()
+    for name, _ in pkg.abi.SolverOptions._fields_:
+        assert getattr(o, name) == getattr(d, name), name
+
+
 STRUCTS = ["lsmps_fluid", "lsmps_walls", "lsmps_grid", "lsmps_cells", "lsmps_csr", "lsmps_vector",
            "lsmps_surface_diagnostics", "lsmps_moment", "lsmps_csr_matrix", "lsmps_ppe", "lsmps_params",
-           "lsmps_step_state", "lsmps_operator_out"]
+           "lsmps_step_state", "lsmps_operator_out", "lsmps_solver_options", "lsmps_solver_report"]
 PY = {"lsmps_fluid": "Fluid", "lsmps_walls": "Walls", "lsmps_grid": "Grid", "lsmps_cells": "Cells",
       "lsmps_csr": "Csr", "lsmps_vector": "Vector", "lsmps_surface_diagnostics": "SurfaceDiagnostics",
       "lsmps_moment": "Moment", "lsmps_csr_matrix": "CsrMatrix", "lsmps_ppe": "Ppe", "lsmps_params": "Params",
-      "lsmps_step_state": "StepState", "lsmps_operator_out": "OperatorOut"}
+      "lsmps_step_state": "StepState", "lsmps_operator_out": "OperatorOut",
+      "lsmps_solver_options": "SolverOptions", "lsmps_solver_report": "SolverReport"}
 
 
 def test_struct_layout_matches_header(pkg, tmp_path):
