@@ -10,6 +10,11 @@ a 1.0 x 0.25 x 0.5 m tank with 3 wall layers, 5% of the fluid lifted into the
 10 l0 above the free surface (seeded synthetic input).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload splash|dam_break|hydrostatic|batched|virtual_light|ppe_solve]
+
+virtual_light and ppe_solve time one stage outside the step (the
+virtual-light diagnostic; the PPE solve with the reference's AMGX settings)
+on the splash workload's state after one step.
 
 N > 1 runs under torchrun: every rank runs an independent replica (the path
 does not shard; there is no data-path collective) and value = N x particles /
@@ -41,6 +46,14 @@ WORKLOADS = {
     "hydrostatic": ("hydrostatic", {}, "hydrostatic box 20^3 (8k fluid, l0=0.01 m, 3 wall layers)"),
     "batched": ("batched", {}, "64 independent boxes, fluid counts log-uniform in [8k, 200k] (seed 7), hydrostatic "
                                "or dam-break layout by seeded coin flip, 3 wall layers, l0=0.005 m"),
+    # Stages outside the step, on the geometry of the splash workload after one step.
+    "virtual_light": ("splash", {}, "virtual-light diagnostic on the splash dam break 200x50x200 (2M fluid)"),
+    "ppe_solve": ("splash", {}, "PPE solve (GMRES(20), 100 iterations, 1e-6 relative, from zero: the reference's AMGX "
+                                "configuration) of the splash dam break 200x50x200 (2M rows)"),
+}
+STAGE_METRICS = {
+    "virtual_light": "particles/s of the virtual-light diagnostic (compute_virtual_light_diagnostics) on 1 B200",
+    "ppe_solve": "PPE solves/s (AmgxPpeSolver::solve semantics) on 1 B200",
 }
 
 
@@ -467,6 +480,117 @@ def run_batched(args, world, rank, local):
     }
 
 
+def run_stage(args, world, rank, local):
+    """A stage outside the benchmark step, on the state one plain step leaves:
+    the virtual-light diagnostic (lsmps_virtual_light) or the PPE solve
+    (lsmps_solve_ppe on the step's assembled rows, from zero each time)."""
+    import torch
+
+    pkg = graft_entry.load_package()
+    from importlib import import_module
+
+    import_module("lsmps3d_b200.build").build_all()
+    api = import_module("lsmps3d_b200.api")
+    roofline = import_module("lsmps3d_b200.roofline")
+    device = torch.device(f"cuda:{local}")
+    kind, kw, desc = WORKLOADS[args.workload]
+    case = pkg.cases.CASES[kind](**kw)
+    p = case.params
+    stream = torch.cuda.Stream(device)
+    n = case.n_fluid
+    with torch.cuda.stream(stream):
+        dev = api.device_buffers(case, device=device)
+        ctx = api.Context(local)
+        ctx.reserve(case.n_fluid, case.n_wall, case.n_cells)
+        state = dev.step_state(p)
+        ctx.build_neighbor_lists(dev, p)
+        ctx.classify_surface(dev, p)
+        ctx.step(dev, p, state)
+        kf = int(dev.fluid_neighbors["offsets"][n].item())
+        kw_ = int(dev.wall_neighbors["offsets"][n].item())
+        nnz = int(dev.ppe["row_offsets"][n].item())
+        if args.workload == "virtual_light":
+            count = torch.empty(n, dtype=torch.int32, device=device)
+            frac = torch.empty(n, dtype=torch.float64, device=device)
+
+            def call():
+                ctx.virtual_light(dev, p, count.data_ptr(), frac.data_ptr())
+        else:
+            x = torch.empty(n, dtype=torch.float64, device=device)
+            v = dev.ppe_view()
+            opt = pkg.abi.default_solver_options()
+            reports = []
+
+            def call():
+                reports.append(ctx.solve_csr(v.matrix, v.rhs, x.data_ptr(), opt))
+        for _ in range(args.warmup):
+            call()
+        ctx.synchronize()
+        barrier(world)
+        torch.cuda.synchronize(device)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        launches0 = ctx.launch_count
+        with ClockSampler(local) as sampler:
+            e0.record(stream)
+            for _ in range(args.steps):
+                call()
+            e1.record(stream)
+            ctx.synchronize()
+            torch.cuda.synchronize(device)
+        launches = ctx.launch_count - launches0
+        ms = max_over_ranks(world, e0.elapsed_time(e1) / args.steps, device)
+        ctx.set_profiling(True)
+        call()
+        prof = ctx.profile_report()
+        ctx.set_profiling(False)
+        ctx.close()
+    peak, peak_kind = peaks()
+    if args.workload == "virtual_light":
+        kb = roofline.kernel_bytes(n, case.n_wall, kf, kw_, case.n_cells)
+        value, unit = world * n / (ms * 1e-3), "particles/s"
+        extra = {}
+    else:
+        kb = roofline.solve_kernel_bytes(n, nnz, restart=opt.restart)
+        value, unit = world / (ms * 1e-3), "solves/s"
+        r = reports[-1]
+        extra = {"solver": {"iterations": r.iterations, "converged": bool(r.converged),
+                            "residual_reduction": r.final_residual / r.initial_residual if r.initial_residual else 0.0,
+                            "ms_per_iteration": ms / max(r.iterations, 1), "rows": n, "nnz": nnz}}
+    top_name, top_ms, top_n = max(prof, key=lambda e: e[1])
+    avg_ms = top_ms / max(top_n, 1)
+    alg = kb.get(top_name)
+    achieved = alg / (avg_ms * 1e-3) / 1e9 if alg else None
+    traffic, traffic_source = measured_traffic(top_name, n)
+    out = {
+        "metric": STAGE_METRICS[args.workload],
+        "value": value,
+        "unit": unit,
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": desc, "n_fluid": n, "n_wall": case.n_wall, "csr_fluid_entries": kf,
+                   "csr_wall_entries": kw_, "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "l2": "inputs larger than the 126 MB L2 (no flush needed)"},
+        "roofline": {"bound": "hbm", "kernel": top_name,
+                     "kernel_share": top_ms / (sum(e[1] for e in prof) or 1.0), "achieved": achieved, "peak": peak,
+                     "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                     else "fallback", "unit": "GB/s", "frac": achieved / peak if achieved else None,
+                     "traffic": traffic, "traffic_source": traffic_source, "algorithmic_bytes": alg},
+        "kernels": [{"name": k, "ms": t, "launches": c} for k, t, c in prof],
+        "gpu_launches": launches,
+        "clocks": sampler.summary(),
+        "e2e": None,
+    }
+    out.update(extra)
+    return out
+
+
 def mixed_error(pkg, torch, ctx, dev, case, p, state, reset):
     """One plain and one mixed step from the same state; row-normwise PPE
     coefficient error and normwise errors of the other outputs, on the
@@ -560,6 +684,9 @@ def run_reference(args, world, rank, local):
     base = {"metric": METRIC, "unit": "particles/s", "impl": "reference", "higher_is_better": True}
     if kind == "batched":
         return dict(impl="reference", unavailable="the reference steps one box per process; it has no batched form")
+    if args.workload == "ppe_solve":
+        return dict(impl="reference", unavailable="the reference solves the PPE with AMGX, a third-party library that "
+                                                  "is not installed here; its build without AMGX has no solve")
     if not ref_mod.available():
         return dict(impl="reference", unavailable="oracle/_ref/libref_lsmps.so was not built (needs the reference sources)")
     case = pkg.cases.CASES[kind](**kw)
@@ -568,10 +695,18 @@ def run_reference(args, world, rank, local):
     b.load_case(case)
     ref = ref_mod.ReferencePath(pkg.abi, case, b)
     ref.rebuild()
-    if args.warmup:
-        ref.steps(args.warmup)
-    with ClockSampler(local) as sampler:
-        ms = ref.steps(args.steps)
+    if args.workload == "virtual_light":
+        base["metric"] = STAGE_METRICS["virtual_light"]
+        ref.steps(1)  # the same state as our arm: one step after the first rebuild
+        if args.warmup:
+            ref.virtual_light_steps(args.warmup)
+        with ClockSampler(local) as sampler:
+            ms = ref.virtual_light_steps(args.steps)
+    else:
+        if args.warmup:
+            ref.steps(args.warmup)
+        with ClockSampler(local) as sampler:
+            ms = ref.steps(args.steps)
     clocks = sampler.summary()
     ref.close()
     mean_ms = sum(ms) / len(ms)
@@ -604,6 +739,15 @@ def main():
     if args.impl == "reference":
         if rank == 0:
             print(json.dumps(run_reference(args, world, rank, local)), flush=True)
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+        return
+    if args.workload in STAGE_METRICS:
+        out = run_stage(args, world, rank, local)
+        if rank == 0:
+            print(json.dumps(out), flush=True)
         if world > 1:
             import torch.distributed as dist
 

@@ -551,6 +551,43 @@ lsmps_status lsmps_pressure_correction(lsmps_ctx* ctx, const lsmps_fluid* fluid,
                                        const lsmps_vector* smoothed_velocity);
 
 /* ------------------------------------------------------------------------- */
+/* Time-step control on the device (simulation_driver.cu:110-143, 337-338;    */
+/* SimulationTimeManager, include/lsmps3d/core/time_step.hpp)                */
+/* ------------------------------------------------------------------------- */
+/* TimeStepLimits (time_step.hpp:9-18) without the output interval (output
+ * scheduling is host I/O). */
+typedef struct lsmps_time_limits {
+  double min_time_step;
+  double max_time_step;
+  double growth_factor;   /* >= 1 */
+  double cfl;
+  double particle_spacing;
+  double final_time;
+} lsmps_time_limits;
+/* The time manager's state, kept in DEVICE memory by the caller. */
+typedef struct lsmps_time_state {
+  double current_time;
+  double time_step;      /* dt of the step just advanced (the config's time_step) */
+  double cfl_time_step;
+  double max_velocity;   /* largest finite |u| at the start of the step */
+  uint64_t step_index;
+} lsmps_time_state;
+/* SimulationTimeManager::reset (time_step.cpp:85-94): time 0, time step
+ * clamped to [min, max].  Host-only; copy the result to device memory. */
+void lsmps_time_state_init(const lsmps_time_limits* limits, double time_step, lsmps_time_state* host_state);
+/* max_velocity (the largest finite |u| over the fluid) followed by
+ * SimulationTimeManager::advance (time_step.cpp:104-132) on *device_state:
+ * dt = clamp(min(dt_prev * growth, cfl * l0 / |u|max), min, max), cut to the
+ * remaining time; time += dt.  No host round trip (capturable). */
+lsmps_status lsmps_advance_time(lsmps_ctx* ctx, const lsmps_fluid* fluid, const lsmps_time_limits* limits,
+                                lsmps_time_state* device_state);
+/* While set, every kernel of the step that uses the time step (u* combine,
+ * PPE right-hand side, velocity/position update) reads it from this device
+ * address (e.g. &device_state->time_step) instead of lsmps_params.time_step;
+ * NULL restores lsmps_params.time_step. */
+lsmps_status lsmps_ctx_set_device_time_step(lsmps_ctx* ctx, const double* device_time_step);
+
+/* ------------------------------------------------------------------------- */
 /* Whole step (src/app/simulation_driver.cu:346-383 minus the solve and I/O) */
 /* ------------------------------------------------------------------------- */
 /* One time step on the state's buffers: moments (velocity and pressure

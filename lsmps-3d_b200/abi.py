@@ -167,6 +167,16 @@ class SolverReport(Structure):
     ]
 
 
+class TimeLimits(Structure):
+    _fields_ = [(n, c_double) for n in ("min_time_step", "max_time_step", "growth_factor", "cfl", "particle_spacing",
+                                       "final_time")]
+
+
+class TimeState(Structure):
+    _fields_ = [("current_time", c_double), ("time_step", c_double), ("cfl_time_step", c_double),
+                ("max_velocity", c_double), ("step_index", c_uint64)]
+
+
 CONVERGENCE_RELATIVE_INITIAL = 0
 CONVERGENCE_ABSOLUTE = 1
 PRECONDITIONER_NONE = 0
@@ -307,6 +317,9 @@ _SIGNATURES = {
         c_int,
         [c_void_p, P(Fluid), P(Walls), P(Params), P(Csr), P(Csr), P(Fluid), P(Walls), P(Moment), P(Moment), P(Ppe)],
     ),
+    "lsmps_time_state_init": (None, [P(TimeLimits), c_double, P(TimeState)]),
+    "lsmps_advance_time": (c_int, [c_void_p, P(Fluid), P(TimeLimits), c_void_p]),
+    "lsmps_ctx_set_device_time_step": (c_int, [c_void_p, c_void_p]),
     "lsmps_solver_options_default": (None, [P(SolverOptions)]),
     "lsmps_solve_ppe": (c_int, [c_void_p, P(CsrMatrix), c_void_p, c_void_p, P(SolverOptions), P(SolverReport)]),
     "lsmps_clamp_particle_pressure": (c_int, [c_void_p, P(Fluid), c_void_p]),

@@ -204,6 +204,15 @@ class Context:
         v = b.ppe_view()
         return self.solve_csr(v.matrix, v.rhs, v.pressure, options)
 
+    def advance_time(self, b: StepBuffers, limits: abi.TimeLimits, state_ptr: int) -> None:
+        """max |u| and SimulationTimeManager::advance on the device state at state_ptr
+        (an abi.TimeState in device memory)."""
+        self.check(_lib.lsmps_advance_time(self.h, r(b.fluid_view()), r(limits), ctypes.c_void_p(state_ptr)))
+
+    def set_device_time_step(self, ptr: int | None) -> None:
+        """Kernels read dt from this device address (None: from the params)."""
+        self.check(_lib.lsmps_ctx_set_device_time_step(self.h, ctypes.c_void_p(ptr) if ptr else None))
+
     def step(self, b: StepBuffers, params: abi.Params, state: abi.StepState | None = None) -> None:
         s = state if state is not None else b.step_state(params)
         self.check(_lib.lsmps_step(self.h, r(params), r(s)))

@@ -146,6 +146,10 @@ struct lsmps_ctx {
   size_t profile_used = 0;
   // Launch-shape knobs (lsmps_knob).
   int knob[LSMPS_KNOB_COUNT] = {1, 1, 2};
+  // Device-resident time step read by the kernels that use dt (provision
+  // combine, PPE right-hand side, velocity/position update) instead of
+  // lsmps_params::time_step, while set (lsmps_ctx_set_device_time_step).
+  const double* device_dt = nullptr;
   // 32-byte neighbour records (packed.cuh): two fluid and three wall arrays.
   double4* pack_fluid[2] = {nullptr, nullptr};
   double4* pack_wall[3] = {nullptr, nullptr, nullptr};

@@ -176,10 +176,12 @@ __global__ void __launch_bounds__(kThreads) shifting_kernel(GatherArgs a, double
 
 // update_velocity_position_kernel, pressure_correction.cu:369-402
 __global__ void update_kernel(lsmps_fluid f, const double* __restrict__ tx, const double* __restrict__ ty,
-                              const double* __restrict__ tz, double dt, double density,
+                              const double* __restrict__ tz, double dt_host, const double* __restrict__ dtp,
+                              double density,
                               const double* __restrict__ gx, const double* __restrict__ gy,
                               const double* __restrict__ gz, const double* __restrict__ sx,
                               const double* __restrict__ sy, const double* __restrict__ sz) {
+  const double dt = dtp ? *dtp : dt_host;
   for (index_t i = blockIdx.x * blockDim.x + threadIdx.x; i < static_cast<index_t>(f.count);
        i += gridDim.x * blockDim.x) {
     const bool splash = is_splash(f.surface_type, i);
@@ -386,7 +388,7 @@ lsmps_status update_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const lsmps_fluid
   if (f.count == 0) return LSMPS_OK;
   launch(ctx, update_kernel, dim3(pointwise_blocks(ctx, f.count)), dim3(256), 0, f,
          static_cast<const double*>(t.vx), static_cast<const double*>(t.vy), static_cast<const double*>(t.vz),
-         p.time_step, p.density, static_cast<const double*>(g.x), static_cast<const double*>(g.y),
+         p.time_step, ctx->device_dt, p.density, static_cast<const double*>(g.x), static_cast<const double*>(g.y),
          static_cast<const double*>(g.z), static_cast<const double*>(s.x), static_cast<const double*>(s.y),
          static_cast<const double*>(s.z));
   return check_launch(ctx, "velocity/position update");
@@ -601,11 +603,12 @@ __global__ void __launch_bounds__(kThreads) gradient_shifting_kernel(GatherArgs 
 // same thread gives the same result as the two reference kernels.
 __global__ void __launch_bounds__(kThreads) update_anti_penetration_kernel(
     lsmps_fluid f, lsmps_walls w, const index_t* __restrict__ wo, const index_t* __restrict__ wi,
-    const double* __restrict__ tx, const double* __restrict__ ty, const double* __restrict__ tz, double dt,
-    double density, const double* __restrict__ gx, const double* __restrict__ gy, const double* __restrict__ gz,
+    const double* __restrict__ tx, const double* __restrict__ ty, const double* __restrict__ tz, double dt_host,
+    const double* __restrict__ dtp, double density, const double* __restrict__ gx, const double* __restrict__ gy, const double* __restrict__ gz,
     const double* __restrict__ sx, const double* __restrict__ sy, const double* __restrict__ sz, double clearance) {
   const index_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= static_cast<index_t>(f.count)) return;
+  const double dt = dtp ? *dtp : dt_host;
   const bool splash = is_splash(f.surface_type, i);
   const double ox = f.vx[i], oy = f.vy[i], oz = f.vz[i];
   double vx = tx[i], vy = ty[i], vz = tz[i];
@@ -687,7 +690,7 @@ lsmps_status pressure_correction_impl(lsmps_ctx* ctx, const lsmps_fluid& f, cons
   launch(ctx, update_anti_penetration_kernel, dim3(blocks), dim3(kThreads), 0, f, w,
          static_cast<const index_t*>(wn.offsets), static_cast<const index_t*>(wn.indices),
          static_cast<const double*>(t.vx), static_cast<const double*>(t.vy), static_cast<const double*>(t.vz),
-         p.time_step, p.density, static_cast<const double*>(g.x), static_cast<const double*>(g.y),
+         p.time_step, ctx->device_dt, p.density, static_cast<const double*>(g.x), static_cast<const double*>(g.y),
          static_cast<const double*>(g.z), static_cast<const double*>(s.x), static_cast<const double*>(s.y),
          static_cast<const double*>(s.z), p.wall_clearance_ratio * p.particle_spacing);
   st = check_launch(ctx, "gradient/shifting, update/anti-penetration");

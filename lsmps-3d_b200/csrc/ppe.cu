@@ -35,6 +35,7 @@ struct PpeArgs {
   double pwall_scale;
   double density;
   double dt;
+  const double* dt_dev;  // device time step (overrides dt when set)
   double gx, gy, gz;
   index_t* row_offsets;
   index_t* col;
@@ -151,7 +152,7 @@ __global__ void __launch_bounds__(kThreads) ppe_kernel(PpeArgs a) {
   a.col[row] = i;
   a.val[row] = diag;
   a.divergence[i] = div;
-  a.rhs[i] = div / a.dt - wall_rhs;
+  a.rhs[i] = div / (a.dt_dev ? *a.dt_dev : a.dt) - wall_rhs;
   if (a.wall_rhs_out) a.wall_rhs_out[i] = wall_rhs;
 }
 
@@ -281,7 +282,7 @@ __global__ void __launch_bounds__(kThreads, 4) ppe_lanes_kernel(PpeArgs a) {
   a.col[row] = i;
   a.val[row] = diag;
   a.divergence[i] = div;
-  a.rhs[i] = div / a.dt - wall_rhs;
+  a.rhs[i] = div / (a.dt_dev ? *a.dt_dev : a.dt) - wall_rhs;
   if (a.wall_rhs_out) a.wall_rhs_out[i] = wall_rhs;
 }
 
@@ -344,6 +345,7 @@ lsmps_status assemble_ppe_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const lsmps
   a.pwall_scale = pm.wall_weight_scale;
   a.density = p.density;
   a.dt = p.time_step;
+  a.dt_dev = ctx->device_dt;
   a.gx = p.gravity[0];
   a.gy = p.gravity[1];
   a.gz = p.gravity[2];
@@ -400,6 +402,7 @@ lsmps_status assemble_ppe_mixed_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const
   a.pwall_scale = pm.wall_weight_scale;
   a.density = p.density;
   a.dt = p.time_step;
+  a.dt_dev = ctx->device_dt;
   a.gx = p.gravity[0];
   a.gy = p.gravity[1];
   a.gz = p.gravity[2];

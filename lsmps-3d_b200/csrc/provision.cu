@@ -139,12 +139,12 @@ __global__ void __launch_bounds__(kThreads) laplacian_kernel(LaplacianArgs a, Mi
 // combine_explicit_velocity_kernel, explicit_update.cu:250-270
 __global__ void combine_kernel(lsmps_fluid f, lsmps_params p, const double* __restrict__ lx,
                                const double* __restrict__ ly, const double* __restrict__ lz, double* tx, double* ty,
-                               double* tz) {
+                               double* tz, const double* __restrict__ dtp) {
+  const double dt = dtp ? *dtp : p.time_step;
   for (index_t i = blockIdx.x * blockDim.x + threadIdx.x; i < static_cast<index_t>(f.count);
        i += gridDim.x * blockDim.x) {
     const bool splash = f.surface_type != nullptr && f.surface_type[i] == LSMPS_SURFACE_SPLASH;
     const double nu = splash ? 0.0 : p.kinematic_viscosity;
-    const double dt = p.time_step;
     tx[i] = f.vx[i] + dt * (nu * lx[i] + p.gravity[0]);
     ty[i] = f.vy[i] + dt * (nu * ly[i] + p.gravity[1]);
     tz[i] = f.vz[i] + dt * (nu * lz[i] + p.gravity[2]);
@@ -152,10 +152,11 @@ __global__ void combine_kernel(lsmps_fluid f, lsmps_params p, const double* __re
 }
 
 // combine_explicit_wall_velocity_kernel, explicit_update.cu:272-284
-__global__ void wall_combine_kernel(lsmps_walls w, lsmps_params p, double* tx, double* ty, double* tz) {
+__global__ void wall_combine_kernel(lsmps_walls w, lsmps_params p, double* tx, double* ty, double* tz,
+                                    const double* __restrict__ dtp) {
+  const double dt = dtp ? *dtp : p.time_step;
   for (index_t i = blockIdx.x * blockDim.x + threadIdx.x; i < static_cast<index_t>(w.count);
        i += gridDim.x * blockDim.x) {
-    const double dt = p.time_step;
     tx[i] = w.vx[i] + dt * p.gravity[0];
     ty[i] = w.vy[i] + dt * p.gravity[1];
     tz[i] = w.vz[i] + dt * p.gravity[2];
@@ -240,7 +241,7 @@ lsmps_status temporary_velocity_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const
   if (!t.vx || !t.vy || !t.vz) return fail(ctx, LSMPS_INVALID_ARGUMENT, "temporary velocity requires vx/vy/vz");
   launch(ctx, combine_kernel, dim3(pointwise_blocks(ctx, f.count)), dim3(256), 0, f, p,
          static_cast<const double*>(lap.x), static_cast<const double*>(lap.y), static_cast<const double*>(lap.z),
-         t.vx, t.vy, t.vz);
+         t.vx, t.vy, t.vz, ctx->device_dt);
   return check_launch(ctx, "temporary velocity");
 }
 
@@ -250,7 +251,8 @@ lsmps_status temporary_wall_velocity_impl(lsmps_ctx* ctx, const lsmps_walls& w, 
     return fail(ctx, LSMPS_INVALID_ARGUMENT, "Provision temporary wall velocity target is smaller than wall particle count");
   if (w.count == 0) return LSMPS_OK;
   if (!t.vx || !t.vy || !t.vz) return fail(ctx, LSMPS_INVALID_ARGUMENT, "temporary wall velocity requires vx/vy/vz");
-  launch(ctx, wall_combine_kernel, dim3(pointwise_blocks(ctx, w.count)), dim3(256), 0, w, p, t.vx, t.vy, t.vz);
+  launch(ctx, wall_combine_kernel, dim3(pointwise_blocks(ctx, w.count)), dim3(256), 0, w, p, t.vx, t.vy, t.vz,
+         ctx->device_dt);
   return check_launch(ctx, "temporary wall velocity");
 }
 

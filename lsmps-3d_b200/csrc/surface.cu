@@ -249,20 +249,31 @@ __global__ void __launch_bounds__(kSurfaceThreads)
   if (i >= n) return;  // the whole group
   const double4 own = ld4(fp, i);
   constexpr unsigned kAll = (1u << kLightDirections) - 1u;
+  const unsigned gm = group_mask<kLightLanes>();
   unsigned blocked = 0u;
+  // The group walks the row kLightLanes entries at a time and merges its
+  // masks after each round, so it stops as soon as all 14 directions are
+  // blocked (every lane runs the same rounds).
   const index_t fe = fo[i + 1];
-  for (index_t o = fo[i] + l; o < fe && blocked != kAll; o += kLightLanes) {
-    const double4 q = ld4(fp, fi[o]);
-    blocked |= blocked_directions(q.x - own.x, q.y - own.y, q.z - own.z, re2, cone);
+  for (index_t base = fo[i]; base < fe && blocked != kAll; base += kLightLanes) {
+    const index_t o = base + l;
+    if (o < fe) {
+      const double4 q = ld4(fp, fi[o]);
+      blocked |= blocked_directions(q.x - own.x, q.y - own.y, q.z - own.z, re2, cone);
+    }
+    blocked = __reduce_or_sync(gm, blocked);
   }
   if (include_walls) {
     const index_t we = wo[i + 1];
-    for (index_t o = wo[i] + l; o < we && blocked != kAll; o += kLightLanes) {
-      const double4 q = ld4(wp, wi[o]);
-      blocked |= blocked_directions(q.x - own.x, q.y - own.y, q.z - own.z, re2, cone);
+    for (index_t base = wo[i]; base < we && blocked != kAll; base += kLightLanes) {
+      const index_t o = base + l;
+      if (o < we) {
+        const double4 q = ld4(wp, wi[o]);
+        blocked |= blocked_directions(q.x - own.x, q.y - own.y, q.z - own.z, re2, cone);
+      }
+      blocked = __reduce_or_sync(gm, blocked);
     }
   }
-  blocked = __reduce_or_sync(group_mask<kLightLanes>(), blocked);
   if (l != 0) return;
   const int open = kLightDirections - __popc(blocked);
   if (open_count) open_count[i] = open;

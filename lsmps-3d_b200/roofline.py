@@ -85,4 +85,24 @@ def kernel_bytes(nf: int, nw: int, kf: int, kw: int, c: int, s: int = 8) -> dict
     count_wall = pos_f + pos_w + 8 * c + 4 * nw + 4 * nf
     out["csr_kernel<false>"] = (count_fluid + count_wall) // 2
     out["csr_kernel<true>"] = (count_fluid + count_wall + 8 * nf + 4 * k) // 2
+    # virtual-light diagnostic (not in the step): rows, positions, count + fraction
+    out["virtual_light_kernel"] = rows + pos_f + pos_w + (4 + s) * nf
     return out
+
+
+def solve_kernel_bytes(rows: int, nnz: int, restart: int = 20, s: int = 8) -> dict[str, int]:
+    """Algorithmic bytes per launch of the PPE solve's kernels (csrc/solve.cu)
+    on a system of `rows` rows and `nnz` stored entries: the SpMV reads the
+    row offsets, the (column, value) pairs, the input vector once and writes
+    the output; the Gram-Schmidt passes stream the basis vectors they use (on
+    average half the restart length plus one per pass)."""
+    vec = s * rows
+    avg_basis = (restart + 1) / 2.0
+    return {
+        "spmv_kernel<kSpmvLanes>": 4 * (rows + 1) + (4 + s) * nnz + 2 * vec,
+        "dots_kernel": int(vec * (avg_basis + 1)),
+        "update_kernel": int(vec * (avg_basis + 2)),
+        "scale_kernel": 2 * vec,
+        "correct_kernel": int(vec * (restart + 2)),
+        "residual_kernel": 2 * vec,
+    }

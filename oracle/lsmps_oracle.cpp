@@ -1306,6 +1306,29 @@ int oracle_solve_ppe(const lsmps_csr_matrix* A, const double* b, double* x, cons
   return LSMPS_OK;
 }
 
+// max_velocity (src/app/simulation_driver.cu:110-143: the largest finite
+// sqrt(vx^2 + vy^2 + vz^2), 0 for no fluid) followed by
+// SimulationTimeManager::advance (src/core/time_step.cpp:104-132), on a host
+// copy of the time state.
+int oracle_advance_time(const lsmps_fluid* f, const lsmps_time_limits* lim, lsmps_time_state* st) {
+  double umax = 0.0;
+  for (size_t i = 0; i < f->count; ++i) {
+    const double v = std::sqrt(f->vx[i] * f->vx[i] + f->vy[i] * f->vy[i] + f->vz[i] * f->vz[i]);
+    if (std::isfinite(v)) umax = std::max(umax, v);
+  }
+  const double cfl_dt =
+      (!(umax > 0.0) || !std::isfinite(umax)) ? lim->max_time_step : lim->cfl * lim->particle_spacing / umax;
+  double dt = std::clamp(std::min(st->time_step * lim->growth_factor, cfl_dt), lim->min_time_step, lim->max_time_step);
+  const double remaining = lim->final_time - st->current_time;
+  if (remaining > 0.0 && dt > remaining) dt = remaining;
+  st->current_time += dt;
+  st->time_step = dt;
+  st->cfl_time_step = cfl_dt;
+  st->max_velocity = umax;
+  st->step_index += 1;
+  return LSMPS_OK;
+}
+
 int oracle_max_threads() {
 #ifdef _OPENMP
   return omp_get_max_threads();

@@ -76,6 +76,7 @@ def lib(abi):
         "oracle_step": (c_int, [P(abi.Params), P(abi.StepState), P(c_uint64)]),
         "oracle_solve_ppe": (c_int, [P(abi.CsrMatrix), c_void_p, c_void_p, P(abi.SolverOptions),
                                      P(abi.SolverReport)]),
+        "oracle_advance_time": (c_int, [P(abi.Fluid), P(abi.TimeLimits), P(abi.TimeState)]),
         "oracle_max_threads": (c_int, []),
     }
     for name, (res, args) in sig.items():
@@ -170,3 +171,7 @@ class Oracle:
         rep = self.abi.SolverReport()
         st = self.L.oracle_solve_ppe(r(A), rhs.ctypes.data, x.ctypes.data, r(options), r(rep))
         return st, rep
+
+    def advance_time(self, b, limits, state) -> int:
+        """max |u| and the time manager's advance on a host TimeState (in place)."""
+        return self.L.oracle_advance_time(r(b.fluid_view()), r(limits), r(state))

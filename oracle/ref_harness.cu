@@ -327,4 +327,28 @@ int ref_virtual_light(void* handle, int32_t* open_count, double* open_fraction) 
   return 0;
 }
 
+// `steps` timed calls of compute_virtual_light_diagnostics on the current
+// geometry; per-call device times (ms, CUDA events on the legacy default
+// stream) into ms[].
+int ref_virtual_light_steps(void* handle, int steps, float* ms) {
+  auto* h = static_cast<Harness*>(handle);
+  auto v = h->workspace->view();
+  const size_t n = v.fluid.count;
+  int* d_count = nullptr;
+  real* d_fraction = nullptr;
+  LSMPS3D_CUDA_CHECK(cudaMalloc(&d_count, (n ? n : 1) * sizeof(int)));
+  LSMPS3D_CUDA_CHECK(cudaMalloc(&d_fraction, (n ? n : 1) * sizeof(real)));
+  for (int s = 0; s < steps; ++s) {
+    cudaEventRecord(h->e0, 0);
+    compute_virtual_light_diagnostics(v.fluid, v.walls, v.fluid_neighbors, v.wall_neighbors, h->config,
+                                      VirtualLightDiagnosticsView{d_count, d_fraction});
+    cudaEventRecord(h->e1, 0);
+    cudaEventSynchronize(h->e1);
+    if (ms) cudaEventElapsedTime(&ms[s], h->e0, h->e1);
+  }
+  cudaFree(d_count);
+  cudaFree(d_fraction);
+  return 0;
+}
+
 }  // extern "C"

@@ -50,6 +50,7 @@ def lib(abi):
         "ref_download_ppe": (c_longlong, [c_void_p, P(abi.Ppe), c_size_t]),
         "ref_download_correction": (c_int, [c_void_p, P(abi.Vector), P(abi.Vector)]),
         "ref_virtual_light": (c_int, [c_void_p, c_void_p, c_void_p]),
+        "ref_virtual_light_steps": (c_int, [c_void_p, c_int, P(c_float)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -141,3 +142,9 @@ class ReferencePath:
         frac = np.zeros(n, dtype=np.float64)
         self.L.ref_virtual_light(self.h, count.ctypes.data, frac.ctypes.data)
         return count, frac
+
+    def virtual_light_steps(self, n: int) -> list[float]:
+        """n timed calls of the reference's compute_virtual_light_diagnostics (ms each)."""
+        ms = (c_float * n)()
+        self.L.ref_virtual_light_steps(self.h, n, ms)
+        return [float(ms[i]) for i in range(n)]

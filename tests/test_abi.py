@@ -65,14 +65,25 @@ def test_solver_options_default(lib, pkg):
         assert getattr(o, name) == getattr(d, name), name
 
 
+def test_time_state_init(lib, pkg):
+    lim = pkg.abi.TimeLimits(min_time_step=1e-6, max_time_step=1e-3, growth_factor=1.05, cfl=0.2,
+                             particle_spacing=0.01, final_time=1.0)
+    st = pkg.abi.TimeState()
+    for dt, want in ((1e-4, 1e-4), (1.0, 1e-3), (1e-9, 1e-6)):
+        lib.lsmps_time_state_init(ctypes.byref(lim), dt, ctypes.byref(st))
+        assert st.time_step == want and st.current_time == 0.0 and st.step_index == 0
+
+
 STRUCTS = ["lsmps_fluid", "lsmps_walls", "lsmps_grid", "lsmps_cells", "lsmps_csr", "lsmps_vector",
            "lsmps_surface_diagnostics", "lsmps_moment", "lsmps_csr_matrix", "lsmps_ppe", "lsmps_params",
-           "lsmps_step_state", "lsmps_operator_out", "lsmps_solver_options", "lsmps_solver_report"]
+           "lsmps_step_state", "lsmps_operator_out", "lsmps_solver_options", "lsmps_solver_report",
+           "lsmps_time_limits", "lsmps_time_state"]
 PY = {"lsmps_fluid": "Fluid", "lsmps_walls": "Walls", "lsmps_grid": "Grid", "lsmps_cells": "Cells",
       "lsmps_csr": "Csr", "lsmps_vector": "Vector", "lsmps_surface_diagnostics": "SurfaceDiagnostics",
       "lsmps_moment": "Moment", "lsmps_csr_matrix": "CsrMatrix", "lsmps_ppe": "Ppe", "lsmps_params": "Params",
       "lsmps_step_state": "StepState", "lsmps_operator_out": "OperatorOut",
-      "lsmps_solver_options": "SolverOptions", "lsmps_solver_report": "SolverReport"}
+      "lsmps_solver_options": "SolverOptions", "lsmps_solver_report": "SolverReport",
+      "lsmps_time_limits": "TimeLimits", "lsmps_time_state": "TimeState"}
 
 
 def test_struct_layout_matches_header(pkg, tmp_path):
