@@ -64,6 +64,9 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=list(WORKLOADS), default="splash")
+    ap.add_argument("--stage-case", choices=["splash", "dam_break"], default="splash",
+                    help="state the virtual_light / ppe_solve workloads run on (dam_break: the 500k case, for "
+                         "profiler captures)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch-shape knobs")
@@ -494,6 +497,10 @@ def run_stage(args, world, rank, local):
     roofline = import_module("lsmps3d_b200.roofline")
     device = torch.device(f"cuda:{local}")
     kind, kw, desc = WORKLOADS[args.workload]
+    if args.stage_case != "splash":
+        kind, kw = args.stage_case, WORKLOADS[args.stage_case][1]
+        desc = desc.replace("splash dam break 200x50x200 (2M fluid)", WORKLOADS[args.stage_case][2]).replace(
+            "splash dam break 200x50x200 (2M rows)", WORKLOADS[args.stage_case][2])
     case = pkg.cases.CASES[kind](**kw)
     p = case.params
     stream = torch.cuda.Stream(device)

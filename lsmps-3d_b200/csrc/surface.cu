@@ -213,29 +213,34 @@ __global__ void __launch_bounds__(kSurfaceThreads) expand_kernel(const double4* 
 constexpr int kLightDirections = 14;
 constexpr int kLightLanes = 4;
 
-__device__ __forceinline__ void light_direction(int k, double& ux, double& uy, double& uz) {
-  constexpr double s = 0.7071067811865475;
-  const double axis[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
-  const double diag[8][3] = {{s, s, 0}, {s, -s, 0}, {-s, s, 0}, {-s, -s, 0},
-                             {s, 0, s}, {s, 0, -s}, {0, s, s},  {0, s, -s}};
-  const double* u = k < 6 ? axis[k] : diag[k - 6];
-  ux = u[0];
-  uy = u[1];
-  uz = u[2];
-}
-
+// The projections of virtual_light_direction's 14 unit vectors, each the
+// reference's (dx ux + dy uy + dz uz) * rsqrt(d2) with the terms whose
+// component is 0 left out: x*1 = x, x*(-1) = -x and adding x*0 = ±0 are
+// exact, so for finite offsets the values are bit-identical to the full
+// expression, while the FP64 pipe (this kernel's bound) does about half the
+// work.  The two-term sums keep the reference's operand order, so the
+// compiler contracts them into the same FMA as the three-term form.
 __device__ __forceinline__ unsigned blocked_directions(double dx, double dy, double dz, double re2, double cone) {
   const double d2 = dx * dx + dy * dy + dz * dz;
   if (d2 <= 0.0 || d2 > re2) return 0u;
   const double inv = safe_rsqrt(d2);
+  constexpr double s = 0.7071067811865475;
+  const double px = dx * inv, py = dy * inv, pz = dz * inv;
   unsigned mask = 0u;
-#pragma unroll
-  for (int k = 0; k < kLightDirections; ++k) {
-    double ux, uy, uz;
-    light_direction(k, ux, uy, uz);
-    const double projection = (dx * ux + dy * uy + dz * uz) * inv;
-    if (projection >= cone) mask |= 1u << k;
-  }
+  mask |= (px >= cone) ? 1u << 0 : 0u;
+  mask |= (-px >= cone) ? 1u << 1 : 0u;
+  mask |= (py >= cone) ? 1u << 2 : 0u;
+  mask |= (-py >= cone) ? 1u << 3 : 0u;
+  mask |= (pz >= cone) ? 1u << 4 : 0u;
+  mask |= (-pz >= cone) ? 1u << 5 : 0u;
+  mask |= ((dx * s + dy * s) * inv >= cone) ? 1u << 6 : 0u;
+  mask |= ((dx * s + dy * -s) * inv >= cone) ? 1u << 7 : 0u;
+  mask |= ((dx * -s + dy * s) * inv >= cone) ? 1u << 8 : 0u;
+  mask |= ((dx * -s + dy * -s) * inv >= cone) ? 1u << 9 : 0u;
+  mask |= ((dx * s + dz * s) * inv >= cone) ? 1u << 10 : 0u;
+  mask |= ((dx * s + dz * -s) * inv >= cone) ? 1u << 11 : 0u;
+  mask |= ((dy * s + dz * s) * inv >= cone) ? 1u << 12 : 0u;
+  mask |= ((dy * s + dz * -s) * inv >= cone) ? 1u << 13 : 0u;
   return mask;
 }
 
