@@ -451,7 +451,11 @@ namespace {
 // Mixed (the mixed form): the FP64 gradient sums are contracted with rows
 // 0..2 of the pressure operator rows (FP32, or FP64 for FP64-route
 // particles) instead of the full inverse.
-template <bool Mixed>
+//
+// G lanes share a particle (G = 1, 2, 4: LSMPS_KNOB_GATHER_LANES): lane l
+// takes row entries l, l + G, ...; the 15 partial sums are combined with
+// shuffles and lane 0 finishes the particle.
+template <bool Mixed, int G>
 __global__ void __launch_bounds__(kThreads) gradient_shifting_kernel(GatherArgs a, double* pressure,
                                                                      double* fluid_pressure,
                                                                      const double* __restrict__ pinv,
@@ -459,18 +463,24 @@ __global__ void __launch_bounds__(kThreads) gradient_shifting_kernel(GatherArgs 
                                                                      double wall_scale, double* gx, double* gy,
                                                                      double* gz, double* sx_out, double* sy_out,
                                                                      double* sz_out) {
-  const index_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= static_cast<index_t>(a.fluid.count)) return;
+  const long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const index_t i = static_cast<index_t>(t / G);
+  const int l = static_cast<int>(t % G);
+  if (i >= static_cast<index_t>(a.fluid.count)) return;  // the whole group
   const double praw = pressure[i];
   const double pi = praw < 0.0 ? 0.0 : praw;
-  pressure[i] = pi;
-  if (fluid_pressure != nullptr && fluid_pressure != pressure) fluid_pressure[i] = pi;
+  if (l == 0) {
+    pressure[i] = pi;
+    if (fluid_pressure != nullptr && fluid_pressure != pressure) fluid_pressure[i] = pi;
+  }
   const bool splash = is_splash(a.fluid.surface_type, i);
   const bool do_grad = !splash;
   const bool do_shift = !(a.p.ps_displacement_scale <= 0.0 || splash);
   if (!do_grad && !do_shift) {
-    gx[i] = gy[i] = gz[i] = 0.0;
-    sx_out[i] = sy_out[i] = sz_out[i] = 0.0;
+    if (l == 0) {
+      gx[i] = gy[i] = gz[i] = 0.0;
+      sx_out[i] = sy_out[i] = sz_out[i] = 0.0;
+    }
     return;
   }
   const double4 own = ld4(a.fpp, i);
@@ -486,11 +496,11 @@ __global__ void __launch_bounds__(kThreads) gradient_shifting_kernel(GatherArgs 
   // clamp is applied on read, as for every pressure this kernel reads); the
   // next record is loaded while this one is used.
   const index_t fe = a.fo[i + 1];
-  index_t o = a.fo[i];
+  index_t o = a.fo[i] + l;
   double4 qn = ld4(a.fpp, o < fe ? a.fi[o] : i);
-  for (; o < fe; ++o) {
+  for (; o < fe; o += G) {
     const double4 q = qn;
-    if (o + 1 < fe) qn = ld4(a.fpp, a.fi[o + 1]);
+    if (o + G < fe) qn = ld4(a.fpp, a.fi[o + G]);
     const double dx = q.x - xi, dy = q.y - yi, dz = q.z - zi;
     const double d = sqrt(dx * dx + dy * dy + dz * dz);
     if (do_grad) {
@@ -515,7 +525,7 @@ __global__ void __launch_bounds__(kThreads) gradient_shifting_kernel(GatherArgs 
     }
   }
   const index_t we = a.wo[i + 1];
-  for (index_t o = a.wo[i]; o < we; ++o) {
+  for (index_t o = a.wo[i] + l; o < we; o += G) {
     const index_t j = a.wi[o];
     const double4 q = ld4(a.wp, j), nrm = ld4(a.wn, j);
     const double dx = q.x - xi, dy = q.y - yi, dz = q.z - zi;
@@ -538,6 +548,18 @@ __global__ void __launch_bounds__(kThreads) gradient_shifting_kernel(GatherArgs 
       shy = fma(push, wny, shy);
       shz = fma(push, wnz, shz);
     }
+  }
+  if (G > 1) {
+    const unsigned gm = group_mask<G>();
+#pragma unroll
+    for (int r = 0; r < 9; ++r) rhs[r] = group_sum<G>(rhs[r], gm);
+    shx = group_sum<G>(shx, gm);
+    shy = group_sum<G>(shy, gm);
+    shz = group_sum<G>(shz, gm);
+    nx = group_sum<G>(nx, gm);
+    ny = group_sum<G>(ny, gm);
+    nz = group_sum<G>(nz, gm);
+    if (l != 0) return;
   }
   if (do_grad && Mixed) {
     double g[9], c0 = 0.0, c1 = 0.0, c2 = 0.0;
@@ -649,6 +671,30 @@ __global__ void __launch_bounds__(kThreads) update_anti_penetration_kernel(
   f.vz[i] = vz;
 }
 
+// gradient_shifting_kernel with the context's lane count (LSMPS_KNOB_GATHER_LANES).
+template <bool Mixed>
+void launch_gradient_shifting(lsmps_ctx* ctx, size_t count, const GatherArgs& a, double* pressure,
+                              double* fluid_pressure, const double* pinv, const MixedRows& rows, double re,
+                              double wall_scale, const lsmps_vector& g, const lsmps_vector& s) {
+  const long long n = static_cast<long long>(count);
+  switch (ctx->knob[LSMPS_KNOB_GATHER_LANES]) {
+    case 1:
+      launch_named(ctx, Mixed ? "gradient_shifting_kernel<true, 2>" : "gradient_shifting_kernel<false, 2>",
+                   gradient_shifting_kernel<Mixed, 2>, dim3(div_up(2 * n, kThreads)), dim3(kThreads), 0, a, pressure,
+                   fluid_pressure, pinv, rows, re, wall_scale, g.x, g.y, g.z, s.x, s.y, s.z);
+      break;
+    case 2:
+      launch_named(ctx, Mixed ? "gradient_shifting_kernel<true, 4>" : "gradient_shifting_kernel<false, 4>",
+                   gradient_shifting_kernel<Mixed, 4>, dim3(div_up(4 * n, kThreads)), dim3(kThreads), 0, a, pressure,
+                   fluid_pressure, pinv, rows, re, wall_scale, g.x, g.y, g.z, s.x, s.y, s.z);
+      break;
+    default:
+      launch_named(ctx, Mixed ? "gradient_shifting_kernel<true, 1>" : "gradient_shifting_kernel<false, 1>",
+                   gradient_shifting_kernel<Mixed, 1>, dim3(div_up(n, kThreads)), dim3(kThreads), 0, a, pressure,
+                   fluid_pressure, pinv, rows, re, wall_scale, g.x, g.y, g.z, s.x, s.y, s.z);
+  }
+}
+
 }  // namespace
 
 lsmps_status pressure_correction_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const lsmps_walls& w,
@@ -678,14 +724,12 @@ lsmps_status pressure_correction_impl(lsmps_ctx* ctx, const lsmps_fluid& f, cons
   if (mixed) {
     if (!ctx->mixed_rows[1] || ctx->mixed_cap < f.count)
       return fail(ctx, LSMPS_NOT_PREPARED, "mixed pressure operator rows were not prepared");
-    launch(ctx, gradient_shifting_kernel<true>, dim3(blocks), dim3(kThreads), 0, a, pressure, f.pressure,
-           static_cast<const double*>(nullptr), mixed_rows_of(ctx, 1), pm.support_radius,
-           pm.wall_weight_scale, g.x, g.y, g.z, s.x, s.y, s.z);
+    launch_gradient_shifting<true>(ctx, f.count, a, pressure, f.pressure, nullptr, mixed_rows_of(ctx, 1),
+                                   pm.support_radius, pm.wall_weight_scale, g, s);
   } else {
     if (!pm.inverse_matrices) return fail(ctx, LSMPS_INVALID_ARGUMENT, "pressure inverse buffer missing");
-    launch(ctx, gradient_shifting_kernel<false>, dim3(blocks), dim3(kThreads), 0, a, pressure, f.pressure,
-           static_cast<const double*>(pm.inverse_matrices), MixedRows{},
-           pm.support_radius, pm.wall_weight_scale, g.x, g.y, g.z, s.x, s.y, s.z);
+    launch_gradient_shifting<false>(ctx, f.count, a, pressure, f.pressure, pm.inverse_matrices, MixedRows{},
+                                    pm.support_radius, pm.wall_weight_scale, g, s);
   }
   launch(ctx, update_anti_penetration_kernel, dim3(blocks), dim3(kThreads), 0, f, w,
          static_cast<const index_t*>(wn.offsets), static_cast<const index_t*>(wn.indices),

@@ -79,6 +79,12 @@ def kernel_bytes(nf: int, nw: int, kf: int, kw: int, c: int, s: int = 8) -> dict
                                              + 2 * pos_w + 2 * pos_f)
     out["smooth_kernel"] = 4 * (nf + 1) + 4 * kf + 2 * pos_f + 4 * nf + pos_f
     out["copy_kernel"] = 2 * pos_f
+    # lane-parallel variants (LSMPS_KNOB_GATHER_LANES) move the same bytes
+    for g in (1, 2, 4):
+        for m in ("false", "true"):
+            out[f"laplacian_kernel<{m}, {g}>"] = out[f"laplacian_kernel<{m}>"]
+            out[f"gradient_shifting_kernel<{m}, {g}>"] = out[f"gradient_shifting_kernel<{m}>"]
+        out[f"smooth_kernel<{g}>"] = out["smooth_kernel"]
     out["classify_kernel"] = rows + pos_f + 2 * pos_w + 4 * nf
     out["expand_kernel"] = 4 * (nf + 1) + 4 * kf + 8 * nf
     count_fluid = 2 * pos_f + 8 * c + 4 * nf + 4 * nf
