@@ -301,8 +301,8 @@ typedef enum lsmps_knob {
   /* lanes cooperating on one PPE row: 0 -> 1, 1 -> 4 (default), 2 -> 8,
    * 3 -> 16 */
   LSMPS_KNOB_PPE_LANES = 1,
-  /* lanes cooperating on one particle in the velocity-Laplacian and
-   * smoothing passes: 0 -> 1, 1 -> 2, 2 -> 4 (default) */
+  /* lanes cooperating on one particle in the velocity-Laplacian, pressure
+   * gradient/shifting and smoothing passes: 0 -> 1, 1 -> 2, 2 -> 4 (default) */
   LSMPS_KNOB_GATHER_LANES = 2,
   LSMPS_KNOB_COUNT = 3
 } lsmps_knob;

@@ -5,7 +5,9 @@
 // never advances the simulation: the moment stage (its outputs are rebuilt
 // from the positions) for LSMPS_KNOB_MOMENT_OCCUPANCY and the PPE assembly
 // (rebuilt from u*, the moments and the CSR) for LSMPS_KNOB_PPE_LANES, the
-// velocity Laplacian (rebuilt from the velocities) for LSMPS_KNOB_GATHER_LANES.  The
+// velocity Laplacian, gradient/shifting and smoothing gathers (their outputs are
+// rebuilt from the state; the smoothing result is not copied back) for
+// LSMPS_KNOB_GATHER_LANES.  The
 // state's temporary velocity must hold u* of the current positions (it does
 // after any lsmps_step or the provision entry points); its values only feed
 // the timed kernels' arithmetic, not their control flow.
@@ -87,16 +89,22 @@ extern "C" lsmps_status lsmps_autotune(lsmps_ctx* ctx, const lsmps_params* param
   // the PPE reads the moment outputs of the chosen variant
   if (!st) st = moments();
   if (!st) st = time_variants(ctx, LSMPS_KNOB_PPE_LANES, repeats, ppe, &ms[1]);
-  // the Laplacian pass stands for both passes this knob shapes (the smoothing
-  // pass writes the state, so it is not run here)
-  auto laplacian = [&]() -> lsmps_status {
-    if (mixed)
-      return velocity_laplacian_mixed_impl(ctx, s->fluid, s->walls, s->fluid_neighbors, s->wall_neighbors,
-                                           s->velocity_moment, s->velocity_laplacian);
-    return velocity_laplacian_impl(ctx, s->fluid, s->walls, s->fluid_neighbors, s->wall_neighbors,
-                                   s->velocity_moment, s->velocity_laplacian);
+  // The three passes this knob shapes: the velocity Laplacian, the pressure
+  // gradient + shifting pass (it writes only its vectors and clamps the
+  // pressure, as the step does) and the smoothing pass without its copy back
+  // into the velocities.
+  auto gathers = [&]() -> lsmps_status {
+    lsmps_status r = mixed ? velocity_laplacian_mixed_impl(ctx, s->fluid, s->walls, s->fluid_neighbors,
+                                                           s->wall_neighbors, s->velocity_moment, s->velocity_laplacian)
+                           : velocity_laplacian_impl(ctx, s->fluid, s->walls, s->fluid_neighbors, s->wall_neighbors,
+                                                     s->velocity_moment, s->velocity_laplacian);
+    if (!r && s->pressure)
+      r = gradient_shifting_stage(ctx, s->fluid, s->walls, s->fluid_neighbors, s->wall_neighbors, s->pressure,
+                                  *params, s->pressure_moment, s->pressure_gradient, s->ps_displacement, mixed);
+    if (!r) r = smooth_impl(ctx, s->fluid, s->fluid_neighbors, *params, s->smoothed_velocity, false);
+    return r;
   };
-  if (!st) st = time_variants(ctx, LSMPS_KNOB_GATHER_LANES, repeats, laplacian, &ms[2]);
+  if (!st) st = time_variants(ctx, LSMPS_KNOB_GATHER_LANES, repeats, gathers, &ms[2]);
   if (best_ms)
     for (int k = 0; k < LSMPS_KNOB_COUNT; ++k) best_ms[k] = ms[k];
   return end_call(ctx, st);

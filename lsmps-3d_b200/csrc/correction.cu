@@ -404,7 +404,7 @@ lsmps_status anti_penetration_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const l
 }
 
 lsmps_status smooth_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const lsmps_csr& fn, const lsmps_params& p,
-                         const lsmps_vector& sm) {
+                         const lsmps_vector& sm, bool copy_back) {
   lsmps_status st = check_fluid(ctx, f);
   if (st) return st;
   if ((st = check_vector(ctx, f, sm, "Velocity smoothing workspace is too small"))) return st;
@@ -432,9 +432,10 @@ lsmps_status smooth_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const lsmps_csr& 
              p.velocity_smoothing_strength, sm.x, sm.y, sm.z);
       break;
   }
-  launch(ctx, copy_kernel, dim3(pointwise_blocks(ctx, f.count)), dim3(256), 0, static_cast<index_t>(f.count),
-         static_cast<const double*>(sm.x), static_cast<const double*>(sm.y), static_cast<const double*>(sm.z), f.vx,
-         f.vy, f.vz);
+  if (copy_back)
+    launch(ctx, copy_kernel, dim3(pointwise_blocks(ctx, f.count)), dim3(256), 0, static_cast<index_t>(f.count),
+           static_cast<const double*>(sm.x), static_cast<const double*>(sm.y), static_cast<const double*>(sm.z), f.vx,
+           f.vy, f.vz);
   return check_launch(ctx, "velocity smoothing");
 }
 
@@ -697,6 +698,36 @@ void launch_gradient_shifting(lsmps_ctx* ctx, size_t count, const GatherArgs& a,
 
 }  // namespace
 
+// Pressure clamp, LSMPS pressure gradient and particle shifting in one pass
+// (the first half of the fused correction; also run alone by the autotuner:
+// it writes only the gradient and shift vectors and the clamped pressure,
+// which the step clamps anyway).
+lsmps_status gradient_shifting_stage(lsmps_ctx* ctx, const lsmps_fluid& f, const lsmps_walls& w,
+                                     const lsmps_csr& fn, const lsmps_csr& wn, double* pressure,
+                                     const lsmps_params& p, const lsmps_moment& pm, const lsmps_vector& g,
+                                     const lsmps_vector& s, bool mixed) {
+  if (f.count == 0) return LSMPS_OK;
+  GatherArgs a{f, w, fn.offsets, fn.indices, wn.offsets, wn.indices, p};
+  if (!ensure_packs(ctx, f.count, w.count)) return fail(ctx, LSMPS_CUDA_ERROR, "pack allocation failed");
+  pack4(ctx, f.x, f.y, f.z, pressure, f.count, ctx->pack_fluid[0]);
+  pack4(ctx, w.x, w.y, w.z, nullptr, w.count, ctx->pack_wall[0]);
+  pack4(ctx, w.normal_x, w.normal_y, w.normal_z, nullptr, w.count, ctx->pack_wall[2]);
+  a.fpp = ctx->pack_fluid[0];
+  a.wp = ctx->pack_wall[0];
+  a.wn = ctx->pack_wall[2];
+  if (mixed) {
+    if (!ctx->mixed_rows[1] || ctx->mixed_cap < f.count)
+      return fail(ctx, LSMPS_NOT_PREPARED, "mixed pressure operator rows were not prepared");
+    launch_gradient_shifting<true>(ctx, f.count, a, pressure, f.pressure, nullptr, mixed_rows_of(ctx, 1),
+                                   pm.support_radius, pm.wall_weight_scale, g, s);
+  } else {
+    if (!pm.inverse_matrices) return fail(ctx, LSMPS_INVALID_ARGUMENT, "pressure inverse buffer missing");
+    launch_gradient_shifting<false>(ctx, f.count, a, pressure, f.pressure, pm.inverse_matrices, MixedRows{},
+                                    pm.support_radius, pm.wall_weight_scale, g, s);
+  }
+  return check_launch(ctx, "gradient/shifting");
+}
+
 lsmps_status pressure_correction_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const lsmps_walls& w,
                                       const lsmps_csr& fn, const lsmps_csr& wn, const lsmps_fluid& t,
                                       double* pressure, const lsmps_params& p, const lsmps_moment& pm,
@@ -712,25 +743,9 @@ lsmps_status pressure_correction_impl(lsmps_ctx* ctx, const lsmps_fluid& f, cons
   if (pm.kind != LSMPS_MOMENT_PRESSURE_WALL_NEUMANN_A || pm.matrix_size != 9 || pm.particle_count < f.count)
     return fail(ctx, LSMPS_NOT_PREPARED, "Pressure correction requires a prepared pressure Type-A moment matrix");
   if (f.count == 0) return LSMPS_OK;
-  GatherArgs a{f, w, fn.offsets, fn.indices, wn.offsets, wn.indices, p};
-  if (!ensure_packs(ctx, f.count, w.count)) return fail(ctx, LSMPS_CUDA_ERROR, "pack allocation failed");
-  pack4(ctx, f.x, f.y, f.z, pressure, f.count, ctx->pack_fluid[0]);
-  pack4(ctx, w.x, w.y, w.z, nullptr, w.count, ctx->pack_wall[0]);
-  pack4(ctx, w.normal_x, w.normal_y, w.normal_z, nullptr, w.count, ctx->pack_wall[2]);
-  a.fpp = ctx->pack_fluid[0];
-  a.wp = ctx->pack_wall[0];
-  a.wn = ctx->pack_wall[2];
+  st = gradient_shifting_stage(ctx, f, w, fn, wn, pressure, p, pm, g, s, mixed);
+  if (st) return st;
   const int blocks = div_up(static_cast<long long>(f.count), kThreads);
-  if (mixed) {
-    if (!ctx->mixed_rows[1] || ctx->mixed_cap < f.count)
-      return fail(ctx, LSMPS_NOT_PREPARED, "mixed pressure operator rows were not prepared");
-    launch_gradient_shifting<true>(ctx, f.count, a, pressure, f.pressure, nullptr, mixed_rows_of(ctx, 1),
-                                   pm.support_radius, pm.wall_weight_scale, g, s);
-  } else {
-    if (!pm.inverse_matrices) return fail(ctx, LSMPS_INVALID_ARGUMENT, "pressure inverse buffer missing");
-    launch_gradient_shifting<false>(ctx, f.count, a, pressure, f.pressure, pm.inverse_matrices, MixedRows{},
-                                    pm.support_radius, pm.wall_weight_scale, g, s);
-  }
   launch(ctx, update_anti_penetration_kernel, dim3(blocks), dim3(kThreads), 0, f, w,
          static_cast<const index_t*>(wn.offsets), static_cast<const index_t*>(wn.indices),
          static_cast<const double*>(t.vx), static_cast<const double*>(t.vy), static_cast<const double*>(t.vz),
@@ -738,7 +753,7 @@ lsmps_status pressure_correction_impl(lsmps_ctx* ctx, const lsmps_fluid& f, cons
          static_cast<const double*>(g.z), static_cast<const double*>(s.x), static_cast<const double*>(s.y),
          static_cast<const double*>(s.z), p.wall_clearance_ratio * p.particle_spacing);
   st = check_launch(ctx, "gradient/shifting, update/anti-penetration");
-  if (!st) st = smooth_impl(ctx, f, fn, p, sm);
+  if (!st) st = smooth_impl(ctx, f, fn, p, sm, true);
   return st;
 }
 
@@ -790,7 +805,7 @@ lsmps_status lsmps_anti_penetration(lsmps_ctx* ctx, const lsmps_fluid* fluid, co
 lsmps_status lsmps_smooth_particle_velocity(lsmps_ctx* ctx, const lsmps_fluid* fluid, const lsmps_csr* fn,
                                             const lsmps_params* params, const lsmps_vector* sm) {
   if (!ctx || !fluid || !fn || !params || !sm) return LSMPS_INVALID_ARGUMENT;
-  LSMPS_API_BODY(smooth_impl(ctx, *fluid, *fn, *params, *sm));
+  LSMPS_API_BODY(smooth_impl(ctx, *fluid, *fn, *params, *sm, true));
 }
 
 lsmps_status lsmps_pressure_correction(lsmps_ctx* ctx, const lsmps_fluid* fluid, const lsmps_walls* walls,

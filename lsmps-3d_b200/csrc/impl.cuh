@@ -44,6 +44,15 @@ lsmps_status assemble_ppe_mixed_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const
                                      const lsmps_params& p, const lsmps_csr& fn, const lsmps_csr& wn,
                                      const lsmps_fluid& tv, const lsmps_walls& tw, const lsmps_moment& vm,
                                      const lsmps_moment& pm, const lsmps_ppe& ws);
+// Pressure clamp + gradient + particle shifting (the first half of the fused
+// correction), and the velocity smoothing pass (copy_back = false leaves the
+// smoothed velocity in `sm` only).
+lsmps_status gradient_shifting_stage(lsmps_ctx* ctx, const lsmps_fluid& f, const lsmps_walls& w,
+                                     const lsmps_csr& fn, const lsmps_csr& wn, double* pressure,
+                                     const lsmps_params& p, const lsmps_moment& pm, const lsmps_vector& g,
+                                     const lsmps_vector& s, bool mixed);
+lsmps_status smooth_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const lsmps_csr& fn, const lsmps_params& p,
+                         const lsmps_vector& sm, bool copy_back);
 lsmps_status pressure_correction_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const lsmps_walls& w,
                                       const lsmps_csr& fn, const lsmps_csr& wn, const lsmps_fluid& t,
                                       double* pressure, const lsmps_params& p, const lsmps_moment& pm,

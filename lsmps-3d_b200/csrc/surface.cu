@@ -86,21 +86,12 @@ __global__ void __launch_bounds__(kSurfaceThreads) classify_kernel(SurfaceArgs a
   const double px = own.x, py = own.y, pz = own.z;
   double nd = 0.0, sx = 0.0, sy = 0.0, sz = 0.0;
   int weighted = 0;
-  // The sums run in row order (the labels depend on their rounding), so the
-  // loads are overlapped instead: the records of the next kAhead neighbours
-  // are in flight while one is accumulated.
-  constexpr int kAhead = 4;
-  double4 ring[kAhead];
-#pragma unroll
-  for (int k = 0; k < kAhead; ++k) ring[k] = ld4(a.fp, fb + k < fe ? a.fi[fb + k] : i);
-  for (index_t o = fb; o < fe; o += kAhead) {
-#pragma unroll
-    for (int k = 0; k < kAhead; ++k) {
-      if (o + k >= fe) break;
-      const double4 q = ring[k];
-      if (o + k + kAhead < fe) ring[k] = ld4(a.fp, a.fi[o + k + kAhead]);
-      accumulate(q.x - px, q.y - py, q.z - pz, re, nd, sx, sy, sz, weighted);
-    }
+  // the next neighbour's record is loaded while this one is accumulated
+  double4 qn = ld4(a.fp, fb < fe ? a.fi[fb] : i);
+  for (index_t o = fb; o < fe; ++o) {
+    const double4 q = qn;
+    if (o + 1 < fe) qn = ld4(a.fp, a.fi[o + 1]);
+    accumulate(q.x - px, q.y - py, q.z - pz, re, nd, sx, sy, sz, weighted);
   }
   if (a.p.include_wall_neighbors) {
     for (index_t o = wb; o < we; ++o) {
