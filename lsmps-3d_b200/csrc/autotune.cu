@@ -90,21 +90,37 @@ extern "C" lsmps_status lsmps_autotune(lsmps_ctx* ctx, const lsmps_params* param
   if (!st) st = moments();
   if (!st) st = time_variants(ctx, LSMPS_KNOB_PPE_LANES, repeats, ppe, &ms[1]);
   // The three passes this knob shapes: the velocity Laplacian, the pressure
-  // gradient + shifting pass (it writes only its vectors and clamps the
-  // pressure, as the step does) and the smoothing pass without its copy back
-  // into the velocities.
+  // gradient + shifting pass (on a copy of the pressure, which it clamps in
+  // place) and the smoothing pass without its copy back into the velocities.
+  double* pressure_copy = nullptr;
+  if (!st && s->pressure && s->fluid.count) {
+    if (cudaMalloc(&pressure_copy, s->fluid.count * sizeof(double)) != cudaSuccess) {
+      cudaGetLastError();
+      pressure_copy = nullptr;
+      st = fail(ctx, LSMPS_CUDA_ERROR, "autotune pressure copy allocation failed");
+    } else {
+      cudaMemcpyAsync(pressure_copy, s->pressure, s->fluid.count * sizeof(double), cudaMemcpyDeviceToDevice,
+                      ctx->stream);
+    }
+  }
+  lsmps_fluid fluid_copy = s->fluid;
+  fluid_copy.pressure = pressure_copy;
   auto gathers = [&]() -> lsmps_status {
     lsmps_status r = mixed ? velocity_laplacian_mixed_impl(ctx, s->fluid, s->walls, s->fluid_neighbors,
                                                            s->wall_neighbors, s->velocity_moment, s->velocity_laplacian)
                            : velocity_laplacian_impl(ctx, s->fluid, s->walls, s->fluid_neighbors, s->wall_neighbors,
                                                      s->velocity_moment, s->velocity_laplacian);
-    if (!r && s->pressure)
-      r = gradient_shifting_stage(ctx, s->fluid, s->walls, s->fluid_neighbors, s->wall_neighbors, s->pressure,
+    if (!r && pressure_copy)
+      r = gradient_shifting_stage(ctx, fluid_copy, s->walls, s->fluid_neighbors, s->wall_neighbors, pressure_copy,
                                   *params, s->pressure_moment, s->pressure_gradient, s->ps_displacement, mixed);
     if (!r) r = smooth_impl(ctx, s->fluid, s->fluid_neighbors, *params, s->smoothed_velocity, false);
     return r;
   };
   if (!st) st = time_variants(ctx, LSMPS_KNOB_GATHER_LANES, repeats, gathers, &ms[2]);
+  if (pressure_copy) {
+    cudaStreamSynchronize(ctx->stream);
+    cudaFree(pressure_copy);
+  }
   if (best_ms)
     for (int k = 0; k < LSMPS_KNOB_COUNT; ++k) best_ms[k] = ms[k];
   return end_call(ctx, st);
