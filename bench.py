@@ -70,6 +70,9 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch-shape knobs")
+    ap.add_argument("--knobs", default=None,
+                    help="comma-separated launch-shape knob values (moment variant, PPE lanes, gather lanes) to use "
+                         "instead of autotuning, e.g. 2,1,1 (what the autotuner picks at 2M)")
     ap.add_argument("--kappa-threshold", type=float, default=None,
                     help="mixed form: condition-estimate threshold of the FP64 route (library default if omitted)")
     ap.add_argument("--precision", choices=["both", "plain", "mixed"], default="both",
@@ -254,7 +257,11 @@ def run_ours(args, world, rank, local):
                 ctx.step(dev, p, state)
             # the project autotuner picks the launch-shape knobs on this state
             # (it runs only stages that are pure functions of the state)
-            if args.no_autotune:
+            if args.knobs:
+                for k, v in enumerate(int(x) for x in args.knobs.split(",")):
+                    ctx.set_knob(k, v)
+                tuned = {k: (ctx.knob(k), 0.0) for k in range(pkg.abi.KNOB_COUNT)}
+            elif args.no_autotune:
                 tuned = {k: (ctx.knob(k), 0.0) for k in range(pkg.abi.KNOB_COUNT)}
             else:
                 tuned = ctx.autotune(dev, p, repeats=3, state=state)
