@@ -253,15 +253,14 @@ def run_ours(args, world, rank, local):
             ctx.reserve(case.n_fluid, case.n_wall, case.n_cells)
             reset()
             fallbacks0 = ctx.fp64_fallbacks
+            if args.knobs:  # fixed knobs apply from the first step on
+                for k, v in enumerate(int(x) for x in args.knobs.split(",")):
+                    ctx.set_knob(k, v)
             for _ in range(args.warmup):
                 ctx.step(dev, p, state)
             # the project autotuner picks the launch-shape knobs on this state
             # (it runs only stages that are pure functions of the state)
-            if args.knobs:
-                for k, v in enumerate(int(x) for x in args.knobs.split(",")):
-                    ctx.set_knob(k, v)
-                tuned = {k: (ctx.knob(k), 0.0) for k in range(pkg.abi.KNOB_COUNT)}
-            elif args.no_autotune:
+            if args.knobs or args.no_autotune:
                 tuned = {k: (ctx.knob(k), 0.0) for k in range(pkg.abi.KNOB_COUNT)}
             else:
                 tuned = ctx.autotune(dev, p, repeats=3, state=state)
