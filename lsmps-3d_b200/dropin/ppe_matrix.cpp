@@ -257,7 +257,12 @@ AmgxPpeSolver::~AmgxPpeSolver() = default;
 AmgxPpeSolver::AmgxPpeSolver(AmgxPpeSolver&&) noexcept = default;
 AmgxPpeSolver& AmgxPpeSolver::operator=(AmgxPpeSolver&&) noexcept = default;
 
-bool AmgxPpeSolver::is_available() noexcept { return true; }
+// LSMPS_DROPIN_SOLVER=off reproduces the reference's build without AMGX (no
+// solve available), e.g. to compare its diagnostic programs output for output.
+bool AmgxPpeSolver::is_available() noexcept {
+  const char* v = std::getenv("LSMPS_DROPIN_SOLVER");
+  return v == nullptr || std::string(v) != "off";
+}
 
 const std::filesystem::path& AmgxPpeSolver::config_path() const noexcept { return impl_->config_path; }
 
@@ -266,6 +271,10 @@ void AmgxPpeSolver::solve(const CsrMatrixView& matrix, const real* rhs, real* pr
   if (matrix.rows != matrix.cols || matrix.row_offsets == nullptr || matrix.col_indices == nullptr ||
       matrix.values == nullptr || rhs == nullptr || pressure == nullptr)
     dropin::fail("AMGX PPE solve requires a square CSR matrix, rhs, and solution buffer");
+  if (!is_available())
+    dropin::fail(
+        "AMGX support is not enabled in this build. Configure with AMGX headers and library available to use "
+        "AmgxPpeSolver.");
   const lsmps_solver_options options = options_from(impl_->config_path);
   const lsmps_csr_matrix a{matrix.rows, matrix.cols, matrix.nnz, matrix.row_offsets, matrix.col_indices,
                            matrix.values};

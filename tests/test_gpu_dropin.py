@@ -83,3 +83,122 @@ def test_dropin_error_convention(case, message, workdir):
     r = run(CHECKS, workdir, case, env=env)
     assert r.returncode == 0, r.stdout + r.stderr
     assert r.stdout.strip() == f"caught: {message}"
+
+
+# --- the reference's diagnostic programs -------------------------------------
+
+def parse_vtk(path):
+    """Point fields of a legacy ASCII VTK file written by the reference's
+    LegacyVtkWriter: {name: array} (vectors as (n, 3)), plus "POINTS"."""
+    import numpy as np
+
+    tok = open(path).read().split()
+    fields, i = {}, 0
+    n = None
+    while i < len(tok):
+        t = tok[i]
+        if t == "POINTS":
+            n = int(tok[i + 1])
+            fields["POINTS"] = np.array(tok[i + 3:i + 3 + 3 * n], dtype=float).reshape(n, 3)
+            i += 3 + 3 * n
+        elif t == "SCALARS":
+            name = tok[i + 1]
+            start = i + 6  # SCALARS name type 1 LOOKUP_TABLE default
+            fields[name] = np.array(tok[start:start + n], dtype=float)
+            i = start + n
+        elif t == "VECTORS":
+            name = tok[i + 1]
+            fields[name] = np.array(tok[i + 3:i + 3 + 3 * n], dtype=float).reshape(n, 3)
+            i += 3 + 3 * n
+        else:
+            i += 1
+    return fields
+
+
+def parse_csv(path):
+    import csv
+
+    with open(path) as f:
+        rows = list(csv.reader(f))
+    return rows[0], rows[1:]
+
+
+def compare_outputs(ref_dir, our_dir, skip_fields=(), rtol=1e-6):
+    """Every CSV and VTK file the reference build wrote, field by field:
+    integer-valued columns exactly, real ones within rtol of the field's scale
+    (the files carry 9 significant digits)."""
+    import numpy as np
+
+    worst = {}
+    files = sorted(p.relative_to(ref_dir) for p in ref_dir.rglob("*") if p.suffix in (".csv", ".vtk"))
+    assert files, "the reference build wrote no output"
+    for rel in files:
+        a, b = ref_dir / rel, our_dir / rel
+        assert b.exists(), rel
+        if rel.suffix == ".csv":
+            ha, ra = parse_csv(a)
+            hb, rb = parse_csv(b)
+            assert ha == hb and len(ra) == len(rb), rel
+            for c, name in enumerate(ha):
+                col_a = [r[c] for r in ra]
+                col_b = [r[c] for r in rb]
+                try:
+                    va, vb = np.array(col_a, float), np.array(col_b, float)
+                except ValueError:  # names (surface_type_name, expected_surface)
+                    assert col_a == col_b, (rel, name)
+                    continue
+                if np.all(va == np.round(va)) and "count" in name or name in ("particle_id", "surface_type"):
+                    assert np.array_equal(va, vb), (rel, name)
+                scale = max(np.max(np.abs(va)), 1e-300)
+                worst[f"{rel}:{name}"] = float(np.max(np.abs(va - vb)) / scale)
+        else:
+            fa, fb = parse_vtk(a), parse_vtk(b)
+            assert sorted(fa) == sorted(fb), rel
+            for name in fa:
+                if name in skip_fields:
+                    continue
+                va, vb = fa[name], fb[name]
+                if name in ("surface_type", "fluid_neighbor_count", "wall_neighbor_count", "ppe_matrix_row_nnz"):
+                    assert np.array_equal(va, vb), (rel, name)
+                scale = max(np.max(np.abs(va)), 1e-300)
+                worst[f"{rel}:{name}"] = float(np.max(np.abs(va - vb)) / scale)
+    bad = {k: v for k, v in worst.items() if v > rtol}
+    return worst, bad
+
+
+def test_complex_surface_diagnostics_program(workdir):
+    # Five surface-detection cases (inclined plane, sine wave, droplet,
+    # cylinder, stepped box): labels, counts, densities, anisotropies and
+    # normals written by the reference's own program, through the drop-in.
+    ref_out, our_out = workdir / "complex_ref", workdir / "complex_dropin"
+    r = run(os.path.join(UNIT, "reference", "complex_surface_diagnostics"), workdir, "all", str(ref_out))
+    assert r.returncode == 0, r.stderr
+    g = run(os.path.join(UNIT, "dropin", "complex_surface_diagnostics"), workdir, "all", str(our_out))
+    assert g.returncode == 0, g.stderr
+    assert g.stdout.replace(str(our_out), "@") == r.stdout.replace(str(ref_out), "@")
+    worst, bad = compare_outputs(ref_out, our_out, rtol=1e-7)
+    print(f"complex surface diagnostics: {len(worst)} fields, worst relative difference "
+          f"{max(worst.values()):.2e}")
+    assert not bad, bad
+
+
+def test_hydrostatic_surface_diagnostics_program(workdir):
+    # Neighbours, labels, moments, provision, PPE rows and the pressure
+    # operators of a half-full hydrostatic box.  The reference here has no
+    # AMGX, so its program skips the solve: the drop-in runs with its solver
+    # switched off (LSMPS_DROPIN_SOLVER=off) to take the same branch.
+    ref_out, our_out = workdir / "hydro_ref", workdir / "hydro_dropin"
+    r = run(os.path.join(UNIT, "reference", "hydrostatic_surface_diagnostics"), workdir, str(ref_out))
+    assert r.returncode == 0, r.stderr
+    env = dict(os.environ, LSMPS_DROPIN_SOLVER="off")
+    g = run(os.path.join(UNIT, "dropin", "hydrostatic_surface_diagnostics"), workdir, str(our_out), env=env)
+    assert g.returncode == 0, g.stderr
+    worst, bad = compare_outputs(ref_out, our_out, rtol=1e-6)
+    print(f"hydrostatic diagnostics: {len(worst)} fields, worst relative difference {max(worst.values()):.2e}")
+    for k in sorted(worst, key=worst.get)[-5:]:
+        print(f"  {k}: {worst[k]:.2e}")
+    assert not bad, bad
+    # and with the device solve (the drop-in's AmgxPpeSolver)
+    g = run(os.path.join(UNIT, "dropin", "hydrostatic_surface_diagnostics"), workdir, str(workdir / "hydro_solve"))
+    assert g.returncode == 0, g.stderr
+    print("\n".join(line for line in g.stdout.splitlines() if "PPE" in line))
