@@ -208,3 +208,105 @@ def test_hydrostatic_surface_diagnostics_program(workdir):
     g = run(os.path.join(UNIT, "dropin", "hydrostatic_surface_diagnostics"), workdir, str(workdir / "hydro_solve"))
     assert g.returncode == 0, g.stderr
     print("\n".join(line for line in g.stdout.splitlines() if "PPE" in line))
+
+
+# --- the reference's simulation driver ---------------------------------------
+
+def _write_driver_inputs(pkg, d, out_dir, final_time=2.0e-3):
+    """A small jittered dam break (24 x 12 x 24 fluid, 3 wall layers) as the
+    driver's CSV inputs and INI configuration (docs/implementation_notes.md:
+    100-122 format; every double written in full precision)."""
+    import numpy as np
+
+    case = pkg.cases.CASES["dam_break"](nx=24, ny=12, nz=24, l0=0.005)
+    p = case.params
+    f, w = case.fluid, case.walls
+    with open(d / "fluid.csv", "w") as fh:
+        fh.write("x,y,z,vx,vy,vz\n")
+        for row in zip(*(np.asarray(f[k], float) for k in ("x", "y", "z", "vx", "vy", "vz"))):
+            fh.write(",".join(repr(float(v)) for v in row) + "\n")
+    with open(d / "walls.csv", "w") as fh:
+        fh.write("x,y,z,vx,vy,vz,normal_x,normal_y,normal_z\n")
+        for row in zip(*(np.asarray(w[k], float) for k in ("x", "y", "z", "vx", "vy", "vz", "normal_x",
+                                                               "normal_y", "normal_z"))):
+            fh.write(",".join(repr(float(v)) for v in row) + "\n")
+    r = repr
+    ini = f"""[geometry]
+particle_spacing={r(p.particle_spacing)}
+support_radius={r(p.support_radius)}
+near_surface_radius={r(p.near_surface_radius)}
+cell_size={r(p.support_radius)}
+
+[simulation]
+time_step=1e-4
+min_time_step=1e-6
+max_time_step=2e-4
+time_step_growth_factor=1.05
+final_time={r(final_time)}
+output_interval=1e-3
+density={r(p.density)}
+kinematic_viscosity={r(p.kinematic_viscosity)}
+gravity_x={r(p.gravity[0])}
+gravity_y={r(p.gravity[1])}
+gravity_z={r(p.gravity[2])}
+
+[surface]
+splash_neighbor_threshold={p.splash_neighbor_threshold}
+number_density_ratio_threshold={r(p.number_density_ratio_threshold)}
+air_open_ratio_threshold={r(p.air_open_ratio_threshold)}
+air_anisotropy_threshold={r(p.air_anisotropy_threshold)}
+include_wall_neighbors={'true' if p.include_wall_neighbors else 'false'}
+wall_normal_independence_threshold={r(p.wall_normal_independence_threshold)}
+
+[lsmps]
+regularization={r(p.lsmps_regularization)}
+wall_weight_scale={r(p.lsmps_wall_weight_scale)}
+
+[correction]
+ps_displacement_scale={r(p.ps_displacement_scale)}
+ps_min_distance_ratio={r(p.ps_min_distance_ratio)}
+ps_max_displacement_ratio={r(p.ps_max_displacement_ratio)}
+wall_clearance_ratio={r(p.wall_clearance_ratio)}
+velocity_smoothing_strength={r(p.velocity_smoothing_strength)}
+
+[files]
+fluid_particle_file={d / 'fluid.csv'}
+wall_particle_file={d / 'walls.csv'}
+output_directory={out_dir}
+vtk_file_prefix=dam_break
+amgx_config_path={d / 'configs' / 'amgx_ppe.json'}
+"""
+    path = out_dir.parent / (out_dir.name + ".ini")
+    path.write_text(ini)
+    return path, case
+
+
+def test_reference_driver_program(pkg, workdir):
+    # The reference's whole time loop (src/app/simulation_driver.cu: CFL time
+    # step, provision, PPE assembly, [solve], correction, rebuild, labels, VTK
+    # output) built against the drop-in, against the same program built from
+    # the reference's modules.  With the solve off on both sides (the
+    # reference here has no AMGX), every VTK file the two write must agree:
+    # labels exactly, the real fields to 1e-9 of their scale after 10 steps.
+    ref_ini, _ = _write_driver_inputs(pkg, workdir, workdir / "drv_ref")
+    our_ini, _ = _write_driver_inputs(pkg, workdir, workdir / "drv_dropin")
+    r = run(os.path.join(UNIT, "reference", "lsmps3d_driver"), workdir, str(ref_ini))
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    env = dict(os.environ, LSMPS_DROPIN_SOLVER="off")
+    g = run(os.path.join(UNIT, "dropin", "lsmps3d_driver"), workdir, str(our_ini), env=env)
+    assert g.returncode == 0, g.stdout[-2000:] + g.stderr[-2000:]
+    worst, bad = compare_outputs(workdir / "drv_ref", workdir / "drv_dropin", rtol=1e-9)
+    print(f"driver outputs: {len(worst)} fields, worst relative difference {max(worst.values()):.2e}")
+    for k in sorted(worst, key=worst.get)[-4:]:
+        print(f"  {k}: {worst[k]:.2e}")
+    assert not bad, bad
+    # The same loop with the device PPE solve (the drop-in's AmgxPpeSolver).
+    sol_ini, _ = _write_driver_inputs(pkg, workdir, workdir / "drv_solve")
+    g = run(os.path.join(UNIT, "dropin", "lsmps3d_driver"), workdir, str(sol_ini))
+    assert g.returncode == 0, g.stdout[-2000:] + g.stderr[-2000:]
+    import numpy as np
+
+    last = sorted((workdir / "drv_solve").rglob("*.vtk"))
+    fields = parse_vtk([p for p in last if "wall" not in p.name][-1])
+    assert np.all(np.isfinite(fields["pressure"])) and fields["pressure"].max() > 0.0
+    print(f"with the device solve: final pressure max {fields['pressure'].max():.3e}")
