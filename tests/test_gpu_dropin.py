@@ -287,7 +287,8 @@ def test_reference_driver_program(pkg, workdir):
     # output) built against the drop-in, against the same program built from
     # the reference's modules.  With the solve off on both sides (the
     # reference here has no AMGX), every VTK file the two write must agree:
-    # labels exactly, the real fields to 1e-9 of their scale after 10 steps.
+    # labels exactly, the real fields to 1e-9 of their scale (14 steps; the
+    # outputs are written with 9 significant digits).
     ref_ini, _ = _write_driver_inputs(pkg, workdir, workdir / "drv_ref")
     our_ini, _ = _write_driver_inputs(pkg, workdir, workdir / "drv_dropin")
     r = run(os.path.join(UNIT, "reference", "lsmps3d_driver"), workdir, str(ref_ini))
