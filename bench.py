@@ -10,7 +10,7 @@ a 1.0 x 0.25 x 0.5 m tank with 3 wall layers, 5% of the fluid lifted into the
 10 l0 above the free surface (seeded synthetic input).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload splash|dam_break|hydrostatic|batched|virtual_light|ppe_solve]
+                  [--workload splash|dam_break|hydrostatic|batched|splash_shuffled|virtual_light|ppe_solve]
 
 virtual_light and ppe_solve time one stage outside the step (the
 virtual-light diagnostic; the PPE solve with the reference's AMGX settings)
@@ -47,6 +47,8 @@ WORKLOADS = {
     "batched": ("batched", {}, "64 independent boxes, fluid counts log-uniform in [8k, 200k] (seed 7), hydrostatic "
                                "or dam-break layout by seeded coin flip, 3 wall layers, l0=0.005 m"),
     # Stages outside the step, on the geometry of the splash workload after one step.
+    "splash_shuffled": ("splash_shuffled", {}, "splash dam break 200x50x200 (2M fluid) with the fluid numbered in a "
+                                               "seeded random order, stepped before and after lsmps_reorder_fluid"),
     "virtual_light": ("splash", {}, "virtual-light diagnostic on the splash dam break 200x50x200 (2M fluid)"),
     "ppe_solve": ("splash", {}, "PPE solve (GMRES(20), 100 iterations, 1e-6 relative, from zero: the reference's AMGX "
                                 "configuration) of the splash dam break 200x50x200 (2M rows)"),
@@ -489,6 +491,87 @@ def run_batched(args, world, rank, local):
     }
 
 
+def run_reorder(args, world, rank, local):
+    """The splash step on input whose fluid numbering does not follow space,
+    then after one lsmps_reorder_fluid (renumbering in cell order) and a
+    neighbour rebuild; plain form, default knobs."""
+    import torch
+
+    pkg = graft_entry.load_package()
+    from importlib import import_module
+
+    import_module("lsmps3d_b200.build").build_all()
+    api = import_module("lsmps3d_b200.api")
+    device = torch.device(f"cuda:{local}")
+    kind, kw, desc = WORKLOADS[args.workload]
+    case = pkg.cases.CASES[kind](**kw)
+    p = case.params
+    stream = torch.cuda.Stream(device)
+    out = {}
+    with torch.cuda.stream(stream):
+        dev = api.device_buffers(case, device=device)
+        ctx = api.Context(local)
+        ctx.reserve(case.n_fluid, case.n_wall, case.n_cells)
+        state = dev.step_state(p)
+        ctx.build_neighbor_lists(dev, p)
+        ctx.classify_surface(dev, p)
+        ctx.set_synchronous(False)
+
+        def timed(k):
+            for _ in range(args.warmup):
+                ctx.step(dev, p, state)
+            ctx.synchronize()
+            barrier(world)
+            torch.cuda.synchronize(device)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            launches0 = ctx.launch_count
+            e0.record(stream)
+            for _ in range(k):
+                ctx.step(dev, p, state)
+            e1.record(stream)
+            ctx.synchronize()
+            torch.cuda.synchronize(device)
+            return max_over_ranks(world, e0.elapsed_time(e1) / k, device), ctx.launch_count - launches0
+
+        with ClockSampler(local) as s0:
+            ms_shuffled, _ = timed(args.steps)
+        ctx.set_synchronous(True)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ctx.reorder_fluid(dev)
+        ctx.build_neighbor_lists(dev, p)
+        e1.record(stream)
+        torch.cuda.synchronize(device)
+        ms_reorder = e0.elapsed_time(e1)
+        ctx.set_synchronous(False)
+        with ClockSampler(local) as s1:
+            ms_sorted, launches = timed(args.steps)
+        ctx.close()
+    n = case.n_fluid
+    return {
+        "metric": METRIC,
+        "value": world * n / (ms_sorted * 1e-3),
+        "unit": "particles/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_sorted,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": desc, "n_fluid": n, "n_wall": case.n_wall, "precision": "plain",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "without_reorder": {"value": world * n / (ms_shuffled * 1e-3), "ms_per_step": ms_shuffled,
+                            "clocks": s0.summary()},
+        "reorder_and_rebuild_ms": ms_reorder,
+        "gpu_launches": launches,
+        "clocks": s1.summary(),
+        "e2e": None,
+    }
+
+
 def run_stage(args, world, rank, local):
     """A stage outside the benchmark step, on the state one plain step leaves:
     the virtual-light diagnostic (lsmps_virtual_light) or the PPE solve
@@ -697,6 +780,9 @@ def run_reference(args, world, rank, local):
     base = {"metric": METRIC, "unit": "particles/s", "impl": "reference", "higher_is_better": True}
     if kind == "batched":
         return dict(impl="reference", unavailable="the reference steps one box per process; it has no batched form")
+    if args.workload == "splash_shuffled":
+        return dict(impl="reference", unavailable="the reference has no renumbering; its step on this input is the "
+                                                  "splash workload's step (its cost does not depend on numbering here)")
     if args.workload == "ppe_solve":
         return dict(impl="reference", unavailable="the reference solves the PPE with AMGX, a third-party library that "
                                                   "is not installed here; its build without AMGX has no solve")
@@ -757,8 +843,8 @@ def main():
 
             dist.destroy_process_group()
         return
-    if args.workload in STAGE_METRICS:
-        out = run_stage(args, world, rank, local)
+    if args.workload in STAGE_METRICS or args.workload == "splash_shuffled":
+        out = (run_stage if args.workload in STAGE_METRICS else run_reorder)(args, world, rank, local)
         if rank == 0:
             print(json.dumps(out), flush=True)
         if world > 1:

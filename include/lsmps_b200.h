@@ -376,6 +376,21 @@ lsmps_status lsmps_build_cell_list(lsmps_ctx* ctx, const double* x, const double
 lsmps_status lsmps_build_cell_list_noalloc(void* stream, const double* x, const double* y, const double* z,
                                            size_t count, const lsmps_grid* grid, const lsmps_cells* cells);
 
+/* Renumbers the fluid particles in the order of fluid_cells (cell id
+ * ascending, stable), as last built for the current positions (by
+ * lsmps_build_neighbor_lists or lsmps_step): x, y, z, vx, vy, vz, pressure
+ * and surface_type are permuted in place and, when permutation is not NULL,
+ * permutation[k] receives the previous index of the particle now at k (a
+ * device array of fluid->count).  No counterpart in the reference; it keeps
+ * the gathers of later steps local when the input numbering does not follow
+ * space.  Afterwards the neighbour lists (and anything else the caller keeps
+ * per fluid particle) are stale: rebuild them with lsmps_build_neighbor_lists
+ * before the next step.  The rebuilt rows list the same neighbours in the same
+ * order, so the next step's results are the renumbered results of the step
+ * without renumbering, bit for bit. */
+lsmps_status lsmps_reorder_fluid(lsmps_ctx* ctx, const lsmps_fluid* fluid, const lsmps_cells* fluid_cells,
+                                 int32_t* permutation);
+
 /* build_neighbor_lists(...), neighbor_search.cuh:18-24.  Rows follow the
  * reference traversal order (27 cells dz -> dy -> dx, ascending sorted
  * position inside each cell); fluid rows exclude the particle itself. */

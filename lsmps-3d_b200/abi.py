@@ -306,6 +306,7 @@ _SIGNATURES = {
     "lsmps_build_cell_list": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, P(Grid), P(Cells)]),
     "lsmps_build_cell_list_noalloc": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, P(Grid), P(Cells)]),
     "lsmps_build_neighbor_lists": (c_int, [c_void_p, P(Fluid), P(Walls), P(Params), P(Cells), P(Cells), P(Csr), P(Csr)]),
+    "lsmps_reorder_fluid": (c_int, [c_void_p, P(Fluid), P(Cells), c_void_p]),
     "lsmps_reference_number_density": (c_double, [c_double, c_double]),
     "lsmps_classify_surface": (c_int, [c_void_p, P(Fluid), P(Walls), P(Csr), P(Csr), P(Params), P(SurfaceDiagnostics)]),
     "lsmps_virtual_light": (c_int, [c_void_p, P(Fluid), P(Walls), P(Csr), P(Csr), P(Params), c_void_p, c_void_p]),

@@ -145,6 +145,12 @@ class Context:
             self.h, r(b.fluid_view()), r(b.walls_view()), r(params), r(b.cells_view("fluid")),
             r(b.cells_view("wall")), r(b.csr_view("fluid")), r(b.csr_view("wall"))))
 
+    def reorder_fluid(self, b: StepBuffers, permutation_ptr: int | None = None) -> None:
+        """Renumber the fluid of `b` in its fluid cell-list order (lsmps_reorder_fluid); the
+        neighbour lists must be rebuilt afterwards."""
+        self.check(_lib.lsmps_reorder_fluid(self.h, r(b.fluid_view()), r(b.cells_view("fluid")),
+                                            ctypes.c_void_p(permutation_ptr) if permutation_ptr else None))
+
     def classify_surface(self, b: StepBuffers, params: abi.Params, diagnostics: abi.SurfaceDiagnostics | None = None):
         self.check(_lib.lsmps_classify_surface(
             self.h, r(b.fluid_view()), r(b.walls_view()), r(b.csr_view("fluid")), r(b.csr_view("wall")),

@@ -278,9 +278,31 @@ def batched_boxes(count: int = 64, seed: int = 7, n_min: int = 8_000, n_max: int
     return boxes
 
 
+def shuffled(case: Case, seed: int = 11) -> Case:
+    """The same particles with the fluid numbered in a seeded random order
+    (input whose numbering does not follow space)."""
+    n = case.n_fluid
+    perm = np.argsort(uniform01(seed, n), kind="stable")
+    fluid = {k: np.ascontiguousarray(np.asarray(v)[perm]) for k, v in case.fluid.items()}
+    meta = dict(case.meta, shuffle_seed=seed)
+    return Case(case.name + "_shuffled", case.l0, fluid, case.walls, case.params, meta)
+
+
+def splash_shuffled(**kw) -> Case:
+    """splash_dam_break with the fluid numbered in a seeded random order."""
+    return shuffled(splash_dam_break(**kw))
+
+
+def dam_break_shuffled(**kw) -> Case:
+    """dam_break with the fluid numbered in a seeded random order."""
+    return shuffled(dam_break(**kw))
+
+
 CASES = {
     "hydrostatic": hydrostatic_box,
     "dam_break": dam_break,
     "splash": splash_dam_break,
     "lattice": lattice_box,
+    "splash_shuffled": splash_shuffled,
+    "dam_break_shuffled": dam_break_shuffled,
 }
