@@ -780,9 +780,6 @@ def run_reference(args, world, rank, local):
     base = {"metric": METRIC, "unit": "particles/s", "impl": "reference", "higher_is_better": True}
     if kind == "batched":
         return dict(impl="reference", unavailable="the reference steps one box per process; it has no batched form")
-    if args.workload == "splash_shuffled":
-        return dict(impl="reference", unavailable="the reference has no renumbering; its step on this input is the "
-                                                  "splash workload's step (its cost does not depend on numbering here)")
     if args.workload == "ppe_solve":
         return dict(impl="reference", unavailable="the reference solves the PPE with AMGX, a third-party library that "
                                                   "is not installed here; its build without AMGX has no solve")
