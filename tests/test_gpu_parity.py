@@ -125,6 +125,8 @@ CASES = [
     ("hydrostatic", dict(n=20, l0=0.01)),
     ("dam_break", dict(nx=24, ny=12, nz=24, l0=0.005)),
     ("splash", dict(nx=40, ny=10, nz=40, l0=0.0025)),
+    # the same dam break with the fluid numbered in random order
+    ("dam_break_shuffled", dict(nx=24, ny=12, nz=24, l0=0.005)),
 ]
 
 

@@ -21,6 +21,7 @@ def test_reordered_step_equals_renumbered_step(pkg, device_api):
     ctx.build_neighbor_lists(a, p)
     ctx.classify_surface(a, p)
     before = a.numpy("fluid")
+    ao, ai = a.csr_rows("fluid")  # the rows the step starts from
     ctx.step(a, p)
     fa = a.numpy("fluid")
     # B: renumber in cell order, rebuild the rows, step
@@ -38,7 +39,6 @@ def test_reordered_step_equals_renumbered_step(pkg, device_api):
     ctx.build_neighbor_lists(b, p)
     cells = b.numpy("fluid_cells")
     assert np.array_equal(cells["sorted_indices"], np.arange(case.n_fluid))
-    ao, ai = a.csr_rows("fluid")
     bo, bi = b.csr_rows("fluid")
     inv = np.empty_like(perm)
     inv[perm] = np.arange(case.n_fluid)
