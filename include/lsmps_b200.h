@@ -289,6 +289,11 @@ uint64_t lsmps_ctx_launch_count(lsmps_ctx* ctx);
  * ~4e-3 at 1e6); the count accumulates over the context's life (read back at
  * each status fold). */
 lsmps_status lsmps_ctx_set_condition_threshold(lsmps_ctx* ctx, double threshold);
+/* lsmps_step's gather kernels visit the fluid in the order of the state's
+ * fluid cell list (particles of one cell on adjacent threads, sharing their
+ * neighbours' records in cache) when this context built that list last
+ * (1, the default), or in index order (0).  Results are identical either way. */
+lsmps_status lsmps_ctx_set_cell_order(lsmps_ctx* ctx, int on);
 uint64_t lsmps_ctx_fp64_fallbacks(lsmps_ctx* ctx);
 /* Launch-shape knobs (no counterpart in the reference, whose kernels all use
  * one thread per particle in 128-thread blocks).  Values are indices into each

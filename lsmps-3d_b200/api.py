@@ -106,6 +106,10 @@ class Context:
         self.check(_lib.lsmps_autotune(self.h, r(params), r(s), repeats, ms))
         return {k: (self.knob(k), float(ms[k])) for k in range(abi.KNOB_COUNT)}
 
+    def set_cell_order(self, on: bool) -> None:
+        """lsmps_step visits the fluid in cell order (default) or index order."""
+        self.check(_lib.lsmps_ctx_set_cell_order(self.h, 1 if on else 0))
+
     def set_condition_threshold(self, threshold: float) -> None:
         """Mixed form: condition estimate above which a moment matrix is
         factorised in FP64 (default 1e4)."""

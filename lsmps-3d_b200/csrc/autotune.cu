@@ -68,6 +68,10 @@ extern "C" lsmps_status lsmps_autotune(lsmps_ctx* ctx, const lsmps_params* param
   lsmps_status st = begin_call(ctx);
   if (st) return st;
   const bool mixed = ctx->precision == LSMPS_PRECISION_MIXED;
+  // time the kernels in the order lsmps_step will visit the fluid
+  if (ctx->cell_order && s->fluid.count > 0 && s->fluid_cells.sorted_indices == ctx->built_order &&
+      ctx->built_order_count == s->fluid.count)
+    ctx->order = s->fluid_cells.sorted_indices;
   auto moments = [&]() -> lsmps_status {
     if (mixed)
       return mixed_step_moments_impl(ctx, s->fluid, s->walls, s->fluid_neighbors, s->wall_neighbors, *params,
@@ -121,6 +125,7 @@ extern "C" lsmps_status lsmps_autotune(lsmps_ctx* ctx, const lsmps_params* param
     cudaStreamSynchronize(ctx->stream);
     cudaFree(pressure_copy);
   }
+  ctx->order = nullptr;
   if (best_ms)
     for (int k = 0; k < LSMPS_KNOB_COUNT; ++k) best_ms[k] = ms[k];
   return end_call(ctx, st);

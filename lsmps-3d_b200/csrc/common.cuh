@@ -108,6 +108,12 @@ __device__ __forceinline__ unsigned group_mask() {
   return ((G == 32) ? 0xffffffffu : ((1u << G) - 1u)) << ((threadIdx.x & (kWarp - 1)) & ~(G - 1));
 }
 
+// The particle a thread (or lane group) visits: its index in the context's
+// visiting order (lsmps_ctx::order), or the index itself.
+__device__ __forceinline__ index_t visit(const int32_t* __restrict__ order, index_t t) {
+  return order ? order[t] : t;
+}
+
 // Sum over the lanes of a group; every lane of the group ends with the total.
 template <int G>
 __device__ __forceinline__ double group_sum(double v, unsigned mask) {
@@ -150,6 +156,17 @@ struct lsmps_ctx {
   // combine, PPE right-hand side, velocity/position update) instead of
   // lsmps_params::time_step, while set (lsmps_ctx_set_device_time_step).
   const double* device_dt = nullptr;
+  // Order in which the per-particle gather kernels of lsmps_step visit the
+  // fluid (the fluid cell list's sorted indices: particles of one cell on
+  // adjacent threads, so their neighbour records are shared in cache), or
+  // NULL for index order.  Visiting order changes no result.
+  const int32_t* order = nullptr;
+  bool cell_order = true;
+  // The fluid cell list this context built last (lsmps_build_neighbor_lists
+  // or a step's rebuild): only such a list, known to hold a permutation of
+  // the fluid, is used as a visiting order.
+  const int32_t* built_order = nullptr;
+  size_t built_order_count = 0;
   // 32-byte neighbour records (packed.cuh): two fluid and three wall arrays.
   double4* pack_fluid[2] = {nullptr, nullptr};
   double4* pack_wall[3] = {nullptr, nullptr, nullptr};

@@ -45,6 +45,7 @@ struct GatherArgs {
   const double4* fpp = nullptr;
   const double4* wp = nullptr;
   const double4* wn = nullptr;
+  const int32_t* order = nullptr;  // visiting order of the fused kernel (lsmps_ctx::order) or NULL
 };
 
 // compute_pressure_gradient_kernel, pressure_correction.cu:200-276
@@ -250,12 +251,14 @@ __global__ void __launch_bounds__(kThreads) smooth_kernel(index_t n, const doubl
                                                           const double4* __restrict__ fv,
                                                           const index_t* __restrict__ fo,
                                                           const index_t* __restrict__ fi, double re, double strength,
-                                                          double* ox, double* oy, double* oz) {
+                                                          double* ox, double* oy, double* oz,
+                                                          const int32_t* __restrict__ order) {
   // G lanes per particle (lane l takes entries l, l + G, ...); the group
   // leaves or continues as a whole.
-  const index_t i = (blockIdx.x * blockDim.x + threadIdx.x) / G;
+  const index_t t = (blockIdx.x * blockDim.x + threadIdx.x) / G;
   const int l = threadIdx.x & (G - 1);
-  if (i >= n) return;
+  if (t >= n) return;
+  const index_t i = visit(order, t);
   const double inv_re = 1.0 / re;
   constexpr double kSplash = static_cast<double>(LSMPS_SURFACE_SPLASH);
   const double4 ui = ld4(fv, i);
@@ -419,17 +422,17 @@ lsmps_status smooth_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const lsmps_csr& 
     case 1:
       launch(ctx, smooth_kernel<2>, dim3(div_up(2 * n, kThreads)), dim3(kThreads), 0, static_cast<index_t>(n), fp, fv,
              static_cast<const index_t*>(fn.offsets), static_cast<const index_t*>(fn.indices), p.support_radius,
-             p.velocity_smoothing_strength, sm.x, sm.y, sm.z);
+             p.velocity_smoothing_strength, sm.x, sm.y, sm.z, ctx->order);
       break;
     case 2:
       launch(ctx, smooth_kernel<4>, dim3(div_up(4 * n, kThreads)), dim3(kThreads), 0, static_cast<index_t>(n), fp, fv,
              static_cast<const index_t*>(fn.offsets), static_cast<const index_t*>(fn.indices), p.support_radius,
-             p.velocity_smoothing_strength, sm.x, sm.y, sm.z);
+             p.velocity_smoothing_strength, sm.x, sm.y, sm.z, ctx->order);
       break;
     default:
       launch(ctx, smooth_kernel<1>, dim3(div_up(n, kThreads)), dim3(kThreads), 0, static_cast<index_t>(n), fp, fv,
              static_cast<const index_t*>(fn.offsets), static_cast<const index_t*>(fn.indices), p.support_radius,
-             p.velocity_smoothing_strength, sm.x, sm.y, sm.z);
+             p.velocity_smoothing_strength, sm.x, sm.y, sm.z, ctx->order);
       break;
   }
   if (copy_back)
@@ -464,10 +467,11 @@ __global__ void __launch_bounds__(kThreads) gradient_shifting_kernel(GatherArgs 
                                                                      double wall_scale, double* gx, double* gy,
                                                                      double* gz, double* sx_out, double* sy_out,
                                                                      double* sz_out) {
-  const long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
-  const index_t i = static_cast<index_t>(t / G);
-  const int l = static_cast<int>(t % G);
-  if (i >= static_cast<index_t>(a.fluid.count)) return;  // the whole group
+  const long long tt = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const index_t t = static_cast<index_t>(tt / G);
+  const int l = static_cast<int>(tt % G);
+  if (t >= static_cast<index_t>(a.fluid.count)) return;  // the whole group
+  const index_t i = visit(a.order, t);
   const double praw = pressure[i];
   const double pi = praw < 0.0 ? 0.0 : praw;
   if (l == 0) {
@@ -715,6 +719,7 @@ lsmps_status gradient_shifting_stage(lsmps_ctx* ctx, const lsmps_fluid& f, const
   a.fpp = ctx->pack_fluid[0];
   a.wp = ctx->pack_wall[0];
   a.wn = ctx->pack_wall[2];
+  a.order = ctx->order;
   if (mixed) {
     if (!ctx->mixed_rows[1] || ctx->mixed_cap < f.count)
       return fail(ctx, LSMPS_NOT_PREPARED, "mixed pressure operator rows were not prepared");

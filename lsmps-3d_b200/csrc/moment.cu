@@ -379,6 +379,7 @@ struct MomentPackedArgs {
   KindOut k0;
   KindOut k1;
   DeviceStatus* status;
+  const int32_t* order;  // visiting order (lsmps_ctx::order) or NULL
 };
 
 template <int B>
@@ -443,12 +444,13 @@ __device__ __forceinline__ void finish_a(double (&s)[kMonomials], const MomentPa
 template <int B0, int B1, int MinBlocks>
 __global__ void __launch_bounds__(kMomentThreads, MinBlocks) moment_a_kernel(MomentPackedArgs a) {
   extern __shared__ double s_mono[];  // [kMonomials][kMomentThreads] when B1 >= 0
-  const index_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  const index_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     if (a.k0.count) atomicAdd(a.k0.count, 1);
     if (B1 >= 0 && a.k1.count) atomicAdd(a.k1.count, 1);
   }
-  if (i >= a.n) return;
+  if (t >= a.n) return;
+  const index_t i = visit(a.order, t);
   const double4 pi = ld4(a.fp, i);
   double s[kMonomials];
 #pragma unroll
@@ -488,12 +490,13 @@ __global__ void __launch_bounds__(kMomentThreads, MinBlocks) moment_a_kernel(Mom
 __global__ void __launch_bounds__(2 * kWarp, 8) moment_a_split_kernel(MomentPackedArgs a) {
   __shared__ double s_half[2][kMonomials][kWarp];
   const int lane = threadIdx.x & (kWarp - 1), half = threadIdx.x >> 5;
-  const index_t i = blockIdx.x * kWarp + lane;
+  const index_t t = blockIdx.x * kWarp + lane;
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     if (a.k0.count) atomicAdd(a.k0.count, 1);
     if (a.k1.count) atomicAdd(a.k1.count, 1);
   }
-  const bool live = i < a.n;
+  const bool live = t < a.n;
+  const index_t i = live ? visit(a.order, t) : 0;
   const double4 pi = live ? ld4(a.fp, i) : make_double4(0.0, 0.0, 0.0, 0.0);
   double s[kMonomials];
 #pragma unroll
@@ -1071,7 +1074,7 @@ lsmps_status prepare_moments_impl(lsmps_ctx* ctx, const lsmps_fluid& fluid, cons
   pack4(ctx, walls.normal_x, walls.normal_y, walls.normal_z, nullptr, walls.count, ctx->pack_wall[2]);
   MomentPackedArgs pa{n, ctx->pack_fluid[0], ctx->pack_wall[0], ctx->pack_wall[2], fn.offsets, fn.indices,
                       wn.offsets, wn.indices, base.inv_re, base.lambda, base.wall_scale, KindOut{}, KindOut{},
-                      ctx->d_status};
+                      ctx->d_status, ctx->order};
   const bool fused = velocity_a >= 0 && pressure_a >= 0;
   const bool capped = ctx->knob[LSMPS_KNOB_MOMENT_OCCUPANCY] == 1;
   const bool split = ctx->knob[LSMPS_KNOB_MOMENT_OCCUPANCY] == 2;

@@ -376,7 +376,12 @@ lsmps_status build_neighbor_lists_impl(lsmps_ctx* ctx, Scratch& scratch, const l
   unsigned* bits = scratch.take<unsigned>(fluid.count * kMaskWords + 1);
   double4* src_pos = scratch.take<double4>(std::max(fluid.count, walls.count) + 1);
   if (!bits || !src_pos) return fail(ctx, LSMPS_CUDA_ERROR, "neighbour scratch exhausted");
+  ctx->built_order = nullptr;
   lsmps_status st = build_cell_list_impl(ctx, scratch, fluid.x, fluid.y, fluid.z, fluid.count, p.grid, fc);
+  if (!st) {
+    ctx->built_order = fc.sorted_indices;
+    ctx->built_order_count = fluid.count;
+  }
   if (!st) st = build_cell_list_impl(ctx, scratch, walls.x, walls.y, walls.z, walls.count, p.grid, wc);
   // the two tables run one after the other on the stream and share the masks
   if (!st)

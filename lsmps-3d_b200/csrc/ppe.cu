@@ -55,6 +55,7 @@ struct PpeArgs {
   const double4* wp;
   const double4* wu;
   const double4* wn;
+  const int32_t* order;  // visiting order of the lane kernel (lsmps_ctx::order) or NULL
 };
 
 __device__ __forceinline__ double dot9(const double a[9], const double b[9]) {
@@ -170,11 +171,12 @@ __global__ void __launch_bounds__(kThreads) ppe_kernel(PpeArgs a) {
 // FP64.
 template <int G, bool Mixed>
 __global__ void __launch_bounds__(kThreads, 4) ppe_lanes_kernel(PpeArgs a) {
-  const index_t i = (blockIdx.x * blockDim.x + threadIdx.x) / G;
+  const index_t t = (blockIdx.x * blockDim.x + threadIdx.x) / G;
   const int l = threadIdx.x & (G - 1);
   const index_t n = static_cast<index_t>(a.fluid.count);
   // Whole groups leave together, so the shuffles below see full groups.
-  if (i >= n) return;
+  if (t >= n) return;
+  const index_t i = visit(a.order, t);
   const index_t nb = a.fo[i], ne = a.fo[i + 1];
   const index_t row = i + nb;
   if (l == 0) {
@@ -350,6 +352,7 @@ lsmps_status assemble_ppe_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const lsmps
   a.gy = p.gravity[1];
   a.gz = p.gravity[2];
   a.row_offsets = ws.matrix.row_offsets;
+  a.order = ctx->order;
   a.col = ws.matrix.col_indices;
   a.val = ws.matrix.values;
   a.rhs = ws.rhs;
@@ -407,6 +410,7 @@ lsmps_status assemble_ppe_mixed_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const
   a.gy = p.gravity[1];
   a.gz = p.gravity[2];
   a.row_offsets = ws.matrix.row_offsets;
+  a.order = ctx->order;
   a.col = ws.matrix.col_indices;
   a.val = ws.matrix.values;
   a.rhs = ws.rhs;

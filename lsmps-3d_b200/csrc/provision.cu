@@ -31,6 +31,7 @@ struct LaplacianArgs {
   double* lx;
   double* ly;
   double* lz;
+  const int32_t* order;  // visiting order (lsmps_ctx::order) or NULL
 };
 
 // accumulate_velocity_rhs, explicit_update.cu:148-162
@@ -67,9 +68,10 @@ __device__ __forceinline__ double lap_from(const double* __restrict__ inv, const
 // with shuffles (a rounding-level reassociation for G > 1).
 template <bool Mixed, int G>
 __global__ void __launch_bounds__(kThreads) laplacian_kernel(LaplacianArgs a, MixedRows rows) {
-  const index_t i = (blockIdx.x * blockDim.x + threadIdx.x) / G;
+  const index_t t = (blockIdx.x * blockDim.x + threadIdx.x) / G;
   const int l = threadIdx.x & (G - 1);
-  if (i >= a.n) return;  // the whole group
+  if (t >= a.n) return;  // the whole group
+  const index_t i = visit(a.order, t);
   const double4 pi = ld4(a.fp, i);
   const double4 ui = ld4(a.fv, i);
   double rx[9], ry[9], rz[9], b[9];
@@ -206,7 +208,8 @@ lsmps_status velocity_laplacian_mixed_impl(lsmps_ctx* ctx, const lsmps_fluid& f,
   // fluid and wall positions are still packed from the moment stage
   LaplacianArgs a{static_cast<index_t>(f.count), ctx->pack_fluid[0], ctx->pack_fluid[1], ctx->pack_wall[0],
                   ctx->pack_wall[1], fn.offsets, fn.indices, wn.offsets, wn.indices, nullptr,
-                  vm.support_radius, 1.0 / vm.support_radius, vm.wall_weight_scale, lap.x, lap.y, lap.z};
+                  vm.support_radius, 1.0 / vm.support_radius, vm.wall_weight_scale, lap.x, lap.y, lap.z,
+                  ctx->order};
   launch_laplacian<true>(ctx, a, mixed_rows_of(ctx, 0));
   return check_launch(ctx, "velocity laplacian (mixed)");
 }
@@ -228,7 +231,8 @@ lsmps_status velocity_laplacian_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const
   pack4(ctx, w.vx, w.vy, w.vz, nullptr, w.count, ctx->pack_wall[1]);
   LaplacianArgs a{static_cast<index_t>(f.count), ctx->pack_fluid[0], ctx->pack_fluid[1], ctx->pack_wall[0],
                   ctx->pack_wall[1], fn.offsets, fn.indices, wn.offsets, wn.indices, vm.inverse_matrices,
-                  vm.support_radius, 1.0 / vm.support_radius, vm.wall_weight_scale, lap.x, lap.y, lap.z};
+                  vm.support_radius, 1.0 / vm.support_radius, vm.wall_weight_scale, lap.x, lap.y, lap.z,
+                  ctx->order};
   launch_laplacian<false>(ctx, a, MixedRows{});
   return check_launch(ctx, "velocity laplacian");
 }

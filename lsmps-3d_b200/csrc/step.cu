@@ -15,6 +15,14 @@ extern "C" lsmps_status lsmps_step(lsmps_ctx* ctx, const lsmps_params* params, c
   Scratch scratch(ctx);
   if (!scratch.reserve(neighbor_scratch_bytes(s->fluid.count, s->walls.count, s->fluid_cells.cell_count)))
     return fail(ctx, LSMPS_CUDA_ERROR, "scratch allocation failed (reserve before graph capture)");
+  // The gather kernels visit the fluid in cell order: the fluid cell list of
+  // the state, when this context built it last (every step ends by
+  // rebuilding it; the caller builds it before the first step), so it is
+  // known to be a permutation of the fluid.  The labels after the rebuild use
+  // the rebuilt list.  The visiting order changes no result.
+  if (ctx->cell_order && s->fluid.count > 0 && s->fluid_cells.sorted_indices == ctx->built_order &&
+      ctx->built_order_count == s->fluid.count)
+    ctx->order = s->fluid_cells.sorted_indices;
   // The driver prepares the moment caches once per geometry generation; the
   // geometry changes every step, so every step builds them once.
   const bool mixed = ctx->precision == LSMPS_PRECISION_MIXED;
@@ -52,5 +60,6 @@ extern "C" lsmps_status lsmps_step(lsmps_ctx* ctx, const lsmps_params* params, c
                                    s->fluid_neighbors, s->wall_neighbors);
   if (!st)
     st = classify_surface_impl(ctx, s->fluid, s->walls, s->fluid_neighbors, s->wall_neighbors, *params, nullptr);
+  ctx->order = nullptr;
   return end_call(ctx, st);
 }

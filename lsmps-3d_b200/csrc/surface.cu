@@ -72,11 +72,13 @@ struct SurfaceArgs {
   const double4* fp;
   const double4* wp;
   const double4* wn;
+  const int32_t* order;  // visiting order (lsmps_ctx::order) or NULL
 };
 
 __global__ void __launch_bounds__(kSurfaceThreads) classify_kernel(SurfaceArgs a) {
-  const index_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= static_cast<index_t>(a.fluid.count)) return;
+  const index_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= static_cast<index_t>(a.fluid.count)) return;
+  const index_t i = visit(a.order, t);
   const index_t fb = a.fo[i], fe = a.fo[i + 1];
   const index_t wb = a.wo[i], we = a.wo[i + 1];
   const index_t fcount = fe - fb, wcount = we - wb;
@@ -359,6 +361,7 @@ lsmps_status classify_surface_impl(lsmps_ctx* ctx, const lsmps_fluid& fluid, con
   a.fp = ctx->pack_fluid[0];
   a.wp = ctx->pack_wall[0];
   a.wn = ctx->pack_wall[2];
+  a.order = ctx->order;
   const index_t n = static_cast<index_t>(fluid.count);
   launch(ctx, classify_kernel, dim3(div_up(n, kSurfaceThreads)), dim3(kSurfaceThreads), 0, a);
   if (p.near_surface_radius > 0.0) {

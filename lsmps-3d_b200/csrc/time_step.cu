@@ -139,3 +139,9 @@ extern "C" lsmps_status lsmps_ctx_set_device_time_step(lsmps_ctx* ctx, const dou
   ctx->device_dt = device_time_step;
   return LSMPS_OK;
 }
+
+extern "C" lsmps_status lsmps_ctx_set_cell_order(lsmps_ctx* ctx, int on) {
+  if (!ctx) return LSMPS_INVALID_ARGUMENT;
+  ctx->cell_order = on != 0;
+  return LSMPS_OK;
+}

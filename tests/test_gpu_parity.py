@@ -379,6 +379,33 @@ def test_gather_lanes_step_matches_oracle(pkg, device_api, oracle, lanes):
         assert e < PLAIN_RTOL, (k, e)
 
 
+@pytest.mark.parametrize("precision", [0, 1], ids=["plain", "mixed"])
+def test_cell_visiting_order_changes_no_result(pkg, device_api, precision):
+    # lsmps_step visits the fluid in cell order when the context built the
+    # state's cell list; every output must equal the index-order step's, bit
+    # for bit (on the randomly numbered dam break, where the two orders differ most).
+    case = pkg.cases.CASES["dam_break_shuffled"](nx=24, ny=12, nz=24, l0=0.005)
+    p = case.params
+    out = []
+    for cell_order in (False, True):
+        c = device_api.Context(0)
+        c.set_precision(precision)
+        c.set_cell_order(cell_order)
+        dev = device_api.device_buffers(case)
+        c.build_neighbor_lists(dev, p)
+        c.classify_surface(dev, p)
+        for _ in range(2):
+            c.step(dev, p)
+        snap = {f"fluid.{k}": v for k, v in dev.numpy("fluid").items()}
+        snap.update({f"ppe.{k}": v for k, v in dev.numpy("ppe").items()})
+        for name in ("pressure_gradient", "ps_displacement", "velocity_laplacian"):
+            snap.update({f"{name}.{k}": v for k, v in dev.numpy(name).items()})
+        out.append(snap)
+        c.close()
+    for k in out[0]:
+        assert np.array_equal(out[0][k], out[1][k]), k
+
+
 def test_knob_arguments_checked(device_api):
     c = device_api.Context(0)
     try:
