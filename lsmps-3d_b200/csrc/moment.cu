@@ -564,7 +564,8 @@ struct MixedSumArgs {
   const index_t* fo;
   const index_t* fi;
   double inv_re;
-  double* sums;
+  double* sums;          // [kMonomials][n], by visiting position
+  const int32_t* order;  // visiting order (lsmps_ctx::order) or NULL
 };
 
 // Kahan step for the 31 weighted monomials of one neighbour (the same
@@ -585,8 +586,9 @@ __device__ __forceinline__ void kahan_monomials(float (&s)[kMonomials], float (&
 }
 
 __global__ void __launch_bounds__(kSumThreads) moment_sums_kernel(MixedSumArgs a) {
-  const index_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= a.n) return;
+  const index_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= a.n) return;
+  const index_t i = visit(a.order, t);
   const double4 pi = ld4(a.fp, i);
   float sum[kMonomials], comp[kMonomials];
 #pragma unroll
@@ -607,7 +609,7 @@ __global__ void __launch_bounds__(kSumThreads) moment_sums_kernel(MixedSumArgs a
   }
   const size_t n = static_cast<size_t>(a.n);
 #pragma unroll
-  for (int e = 0; e < kMonomials; ++e) a.sums[e * n + i] = static_cast<double>(sum[e]) - static_cast<double>(comp[e]);
+  for (int e = 0; e < kMonomials; ++e) a.sums[e * n + t] = static_cast<double>(sum[e]) - static_cast<double>(comp[e]);
 }
 
 struct MixedRowArgs {
@@ -629,6 +631,7 @@ struct MixedRowArgs {
   double* rows64[2];  // compact FP64 rows of the FP64-route particles (unless Full)
   uint8_t* flag[2];   // 1 where rows64 holds the particle's rows (unless Full)
   DeviceStatus* status;
+  const int32_t* order;  // visiting order (the sums are stored by visiting position) or NULL
 };
 
 // v <- L^-T L^-1 v with the packed lower factor and its reciprocal diagonal.
@@ -883,13 +886,14 @@ template <bool Full>
 __global__ void __launch_bounds__(kRowThreads, 6) moment_rows_kernel(MixedRowArgs a) {
   __shared__ double s_m[45 * kRowThreads];
   const int kind = blockIdx.y;
-  const index_t i = blockIdx.x * kRowThreads + threadIdx.x;
+  const index_t t = blockIdx.x * kRowThreads + threadIdx.x;
   if (blockIdx.x == 0 && threadIdx.x == 0 && a.k[kind].count) atomicAdd(a.k[kind].count, 1);
-  if (i >= a.n) return;
+  if (t >= a.n) return;
+  const index_t i = visit(a.order, t);
   const size_t n = static_cast<size_t>(a.n);
   double s[kMonomials];
 #pragma unroll
-  for (int e = 0; e < kMonomials; ++e) s[e] = a.sums[e * n + i];
+  for (int e = 0; e < kMonomials; ++e) s[e] = a.sums[e * n + t];
   mixed_rows_of_particle<Full>(a, kind, i, ld4(a.fp, i), s, s_m + threadIdx.x);
 }
 
@@ -903,9 +907,10 @@ __global__ void __launch_bounds__(kRowThreads, 6) moment_mixed_split_kernel(Mixe
   __shared__ double s_m[45 * kRowThreads];
   __shared__ double s_half[2][kMonomials][kWarp];
   const int lane = threadIdx.x & (kWarp - 1), half = threadIdx.x >> 5;
-  const index_t i = blockIdx.x * kWarp + lane;
+  const index_t t = blockIdx.x * kWarp + lane;
   if (blockIdx.x == 0 && lane == 0 && a.k[half].count) atomicAdd(a.k[half].count, 1);
-  const bool live = i < a.n;
+  const bool live = t < a.n;
+  const index_t i = live ? visit(a.order, t) : 0;
   const double4 pi = live ? ld4(a.fp, i) : make_double4(0.0, 0.0, 0.0, 0.0);
   {
     float sum[kMonomials], comp[kMonomials];
@@ -957,7 +962,7 @@ lsmps_status launch_mixed(lsmps_ctx* ctx, index_t n, const lsmps_csr& fn, const 
                           const lsmps_params& p, const KindOut& kv, const KindOut& kp, bool full) {
   if (!ensure_mixed(ctx, static_cast<size_t>(n))) return fail(ctx, LSMPS_CUDA_ERROR, "mixed-form allocation failed");
   const double inv_re = 1.0 / p.support_radius;
-  MixedSumArgs sa{n, ctx->pack_fluid[0], fn.offsets, fn.indices, inv_re, ctx->mixed_sums};
+  MixedSumArgs sa{n, ctx->pack_fluid[0], fn.offsets, fn.indices, inv_re, ctx->mixed_sums, ctx->order};
   const bool split = ctx->knob[LSMPS_KNOB_MOMENT_OCCUPANCY] == 2;
   MixedRowArgs ra{};
   ra.n = n;
@@ -981,6 +986,7 @@ lsmps_status launch_mixed(lsmps_ctx* ctx, index_t n, const lsmps_csr& fn, const 
     ra.flag[k] = ctx->mixed_flag[k];
   }
   ra.status = ctx->d_status;
+  ra.order = ctx->order;
   if (split) {
     // one kernel: row halves on two warps, one kind per warp
     if (full)
