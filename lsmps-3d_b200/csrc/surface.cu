@@ -180,10 +180,13 @@ constexpr int kExpandLanes = 4;
 
 __global__ void __launch_bounds__(kSurfaceThreads) expand_kernel(const double4* __restrict__ fp, int32_t* type,
                                                                  index_t n, const index_t* __restrict__ fo,
-                                                                 const index_t* __restrict__ fi, double r2) {
-  const index_t i = (blockIdx.x * blockDim.x + threadIdx.x) / kExpandLanes;
+                                                                 const index_t* __restrict__ fi, double r2,
+                                                                 const int32_t* __restrict__ order) {
+  const index_t t = (blockIdx.x * blockDim.x + threadIdx.x) / kExpandLanes;
   const int l = threadIdx.x & (kExpandLanes - 1);
-  if (i >= n || type[i] != LSMPS_SURFACE_INNER) return;  // the whole group
+  if (t >= n) return;  // the whole group
+  const index_t i = visit(order, t);
+  if (type[i] != LSMPS_SURFACE_INNER) return;
   const double4 own = ld4(fp, i);
   bool near = false;
   const index_t fe = fo[i + 1];
@@ -369,7 +372,7 @@ lsmps_status classify_surface_impl(lsmps_ctx* ctx, const lsmps_fluid& fluid, con
            dim3(kSurfaceThreads), 0,
            static_cast<const double4*>(ctx->pack_fluid[0]), fluid.surface_type, n,
            static_cast<const index_t*>(fn.offsets), static_cast<const index_t*>(fn.indices),
-           p.near_surface_radius * p.near_surface_radius);
+           p.near_surface_radius * p.near_surface_radius, static_cast<const int32_t*>(ctx->order));
   }
   return check_launch(ctx, "surface classification");
 }
