@@ -39,12 +39,6 @@ constexpr int kStageCap = 1024;
 constexpr float kScreenMargin = 1.0e-4f;
 constexpr float kFarLimit = 2.0f;
 constexpr int kMaskWords = kStageCap / 32;
-// A staged chunk of 32 candidates is skipped for a pair of home particles
-// when the distance from each of them to the chunk's bounding box (FP32,
-// cell-relative) exceeds (r/h)^2 by this much: far more than the FP32
-// rounding of the box corners and of the screened distances, so no
-// candidate within r is ever skipped.
-constexpr float kChunkMargin = 1.0e-3f;
 
 struct CsrArgs {
   const double* fx;
@@ -107,11 +101,6 @@ template <bool kWrite>
 __global__ void __launch_bounds__(kCsrThreads) csr_kernel(CsrArgs a) {
   __shared__ float4 s_rel[kStageCap];
   __shared__ index_t s_idx[kStageCap];
-  // count pass: per staged chunk of 32 candidates, the bounding box of their
-  // cell-relative coordinates ({min x, min y, min z, -}, {max x, ...});
-  // a chunk holding a far (NaN-coded) candidate gets an unbounded box
-  __shared__ float4 s_lo[kMaskWords];
-  __shared__ float4 s_hi[kMaskWords];
   __shared__ index_t s_cb[27];
   __shared__ index_t s_cnt[27];
   __shared__ index_t s_pre[28];
@@ -169,31 +158,8 @@ __global__ void __launch_bounds__(kCsrThreads) csr_kernel(CsrArgs a) {
     }
     __syncthreads();
     if (!kWrite && staged) {
-      // chunk bounding boxes (one warp per chunk)
-      for (int c = warp; c * kWarp < nc; c += kCsrWarps) {
-        const index_t k = c * kWarp + lane;
-        float4 q = k < nc ? s_rel[k] : s_rel[c * kWarp];  // pad with the chunk's first candidate
-        const bool far = isnan(q.x) || isnan(q.y) || isnan(q.z);
-        float lx = q.x, ly = q.y, lz = q.z, hx = q.x, hy = q.y, hz = q.z;
-#pragma unroll
-        for (int d = 16; d > 0; d >>= 1) {
-          lx = fminf(lx, __shfl_xor_sync(0xffffffffu, lx, d));
-          ly = fminf(ly, __shfl_xor_sync(0xffffffffu, ly, d));
-          lz = fminf(lz, __shfl_xor_sync(0xffffffffu, lz, d));
-          hx = fmaxf(hx, __shfl_xor_sync(0xffffffffu, hx, d));
-          hy = fmaxf(hy, __shfl_xor_sync(0xffffffffu, hy, d));
-          hz = fmaxf(hz, __shfl_xor_sync(0xffffffffu, hz, d));
-        }
-        const bool any_far = __any_sync(0xffffffffu, far);
-        if (lane == 0) {
-          s_lo[c] = any_far ? make_float4(-INFINITY, -INFINITY, -INFINITY, 0.0f) : make_float4(lx, ly, lz, 0.0f);
-          s_hi[c] = any_far ? make_float4(INFINITY, INFINITY, INFINITY, 0.0f) : make_float4(hx, hy, hz, 0.0f);
-        }
-      }
-      __syncthreads();
       // Count pass over the staged set: each warp tests two home particles
-      // per staged chunk (one shared-memory read of the candidate for both);
-      // a chunk whose box is out of reach of both is skipped (its masks are 0).
+      // per staged chunk (one shared-memory read of the candidate for both).
       for (index_t h = hb + 2 * warp; h < he; h += 2 * kCsrWarps) {
         const bool two = h + 1 < he;
         const index_t i0 = a.home_sorted[h];
@@ -204,26 +170,8 @@ __global__ void __launch_bounds__(kCsrThreads) csr_kernel(CsrArgs a) {
         const float r1x = to_rel(x1, ccx, a.inv_h), r1y = to_rel(y1, ccy, a.inv_h), r1z = to_rel(z1, ccz, a.inv_h);
         unsigned keep0 = 0u, keep1 = 0u;  // lane c keeps chunk c's masks
         index_t count0 = 0, count1 = 0;
-        const float skip2 = a.hi2 + kChunkMargin;
         for (index_t base = 0; base < nc; base += kWarp) {
           const index_t k = base + lane;
-          {
-            // squared distance from each home particle to the chunk's box
-            // (NaN for a far home particle: never skipped)
-            const float4 lo = s_lo[base / kWarp], hi = s_hi[base / kWarp];
-            const float ex0 = fmaxf(fmaxf(lo.x - r0x, r0x - hi.x), 0.0f);
-            const float ey0 = fmaxf(fmaxf(lo.y - r0y, r0y - hi.y), 0.0f);
-            const float ez0 = fmaxf(fmaxf(lo.z - r0z, r0z - hi.z), 0.0f);
-            const float ex1 = fmaxf(fmaxf(lo.x - r1x, r1x - hi.x), 0.0f);
-            const float ey1 = fmaxf(fmaxf(lo.y - r1y, r1y - hi.y), 0.0f);
-            const float ez1 = fmaxf(fmaxf(lo.z - r1z, r1z - hi.z), 0.0f);
-            const bool out0 = ex0 * ex0 + ey0 * ey0 + ez0 * ez0 > skip2 && !isnan(r0x + r0y + r0z);
-            const bool out1 = ex1 * ex1 + ey1 * ey1 + ez1 * ez1 > skip2 && !isnan(r1x + r1y + r1z);
-            if (out0 && out1) {  // uniform across the warp
-              if (lane == base / kWarp) keep0 = keep1 = 0u;
-              continue;
-            }
-          }
           bool pass0 = false, pass1 = false;
           if (k < nc) {
             const index_t j = s_idx[k];
