@@ -4,16 +4,17 @@
 // exclusive scan :319-320, host capacity check :323-328, write kernel
 // :238-253).
 //
-// Layout of the work: one block per home cell.  The block stages the
-// candidate set of the 27 surrounding source cells (in the reference's
-// dz -> dy -> dx order, ascending sorted position inside a cell) into shared
-// memory once, as cell-relative FP32 coordinates, and every warp then tests
-// its home particles against the staged set 32 candidates at a time.  The
-// accepted candidates of one warp step are compacted with a ballot, so a row
-// comes out in exactly the reference's traversal order.  The count pass keeps
-// the ballots (one 32-bit mask per 32 staged candidates and home particle);
-// after the scan the write pass re-stages only the candidate indices and
-// replays the masks, so the distance tests run once per table.
+// Layout of the work.  A home cell's candidates are the particles of the 27
+// surrounding source cells in the reference's dz -> dy -> dx order, ascending
+// sorted position inside a cell (its "sequence").  The count pass gives each
+// home cell one warp and each home particle one lane: the warp stages the
+// sequence in shared memory as cell-relative FP32 coordinates and every lane
+// tests its particle against all of it through broadcast loads, keeping one
+// 32-bit accept mask per 32 candidates.  After the scan of the counts, the
+// write pass gives each home cell a block, stages the candidate indices and
+// replays the masks, one warp per particle, compacting each 32-candidate
+// chunk with a popcount: rows come out in exactly the reference's traversal
+// order and the distance tests run once per table.
 //
 // Exactness: the FP32 distance is only a screen.  With coordinates scaled by
 // 1/h and re-centred on the home cell, every component is at most 2 in
@@ -39,6 +40,9 @@ constexpr int kStageCap = 1024;
 constexpr float kScreenMargin = 1.0e-4f;
 constexpr float kFarLimit = 2.0f;
 constexpr int kMaskWords = kStageCap / 32;
+constexpr int kCountWarps = 2;               // warps (home cells) per block of the count pass
+constexpr int kMaskStride = kMaskWords + 1;  // padded row of the count pass's mask transpose
+constexpr float kSentinel = 1.0e18f;         // far enough that d^2 stays finite and rejected
 
 struct CsrArgs {
   const double* fx;
@@ -97,9 +101,167 @@ __device__ __forceinline__ float to_rel(double v, double centre, double inv_h) {
   return fabsf(r) <= kFarLimit ? r : __int_as_float(0x7fc00000);  // NaN forces the exact test
 }
 
-template <bool kWrite>
-__global__ void __launch_bounds__(kCsrThreads) csr_kernel(CsrArgs a) {
-  __shared__ float4 s_rel[kStageCap];
+__device__ __forceinline__ index_t warp_sum(index_t v) {
+  for (int d = 16; d > 0; d >>= 1) v += __shfl_xor_sync(0xffffffffu, v, d);
+  return v;
+}
+
+// Count pass: one warp per home cell, one lane per home particle.  The warp
+// stages its 27-cell candidate sequence (cell-relative FP32 coordinates, the
+// candidate's cell-sorted position in .w) in shared memory, padded to whole
+// 32-candidate chunks with far sentinels; every lane then walks the sequence
+// with broadcast loads, so one shared-memory read serves the whole cell's
+// particles and each candidate costs a lane a handful of FP32 instructions.
+// Bit b of chunk c of a lane's mask is the candidate at sequence position
+// 32c + b, the numbering the write pass replays.  In the fluid table the
+// home cell is the centre source cell, so a particle's own bit sits at
+// sequence position (start of the centre cell) + (its sorted position in the
+// home cell) and is cleared after the tests (the reference skips j == i).
+__global__ void __launch_bounds__(kCountWarps * kWarp) csr_count_kernel(CsrArgs a) {
+  __shared__ float4 s_rel[kCountWarps][kStageCap];
+  __shared__ unsigned s_mask[kCountWarps][kWarp * kMaskStride];
+  __shared__ index_t s_cb[kCountWarps][27];
+  __shared__ index_t s_pre[kCountWarps][28];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  float4* rel = s_rel[w];
+  unsigned* msk = s_mask[w];
+  index_t* cb = s_cb[w];
+  index_t* pre = s_pre[w];
+  const int dimx = a.grid.dims[0], dimy = a.grid.dims[1], dimz = a.grid.dims[2];
+  for (index_t c = blockIdx.x * kCountWarps + w; c < a.ncell; c += gridDim.x * kCountWarps) {
+    const index_t hb = a.home_begin[c];
+    if (hb < 0) continue;  // uniform across the warp
+    const index_t he = a.home_end[c];
+    const int cx = c % dimx;
+    const int cy = (c / dimx) % dimy;
+    const int cz = c / (dimx * dimy);
+    index_t b = -1, n = 0;
+    if (lane < 27) {
+      const int nz = cz + lane / 9 - 1, ny = cy + (lane / 3) % 3 - 1, nx = cx + lane % 3 - 1;
+      if (nz >= 0 && nz < dimz && ny >= 0 && ny < dimy && nx >= 0 && nx < dimx) {
+        const index_t cell = (nz * dimy + ny) * dimx + nx;
+        b = a.src_begin[cell];
+        const index_t e = a.src_end[cell];
+        if (b >= 0 && e >= 0) n = e - b;
+      }
+    }
+    index_t incl = n;
+#pragma unroll
+    for (int d = 1; d < kWarp; d <<= 1) {
+      const index_t t = __shfl_up_sync(0xffffffffu, incl, d);
+      if (lane >= d) incl += t;
+    }
+    const index_t nc = __shfl_sync(0xffffffffu, incl, 31);
+    if (lane < 27) {
+      cb[lane] = b;
+      pre[lane] = incl - n;
+    }
+    if (lane == 0) pre[27] = nc;
+    __syncwarp();
+    if (nc > kStageCap) {
+      // More candidates than the stage holds (overloaded edge cells): exact
+      // tests straight from global memory; only the count is needed here.
+      for (index_t h = hb; h < he; ++h) {
+        const index_t i = a.home_sorted[h];
+        const double xi = a.fx[i], yi = a.fy[i], zi = a.fz[i];
+        index_t count = 0;
+        for (int t = 0; t < 27; ++t) {
+          const index_t b0 = cb[t], cnt = pre[t + 1] - pre[t];
+          for (index_t k = lane; k < cnt; k += kWarp) {
+            const index_t j = a.src_sorted[b0 + k];
+            if (!(a.exclude_self && j == i) && within_radius(xi, yi, zi, a.sx[j], a.sy[j], a.sz[j], a.r2)) ++count;
+          }
+        }
+        count = warp_sum(count);
+        if (lane == 0) a.offsets[i] = count;
+      }
+      __syncwarp();
+      continue;
+    }
+    const double ccx = a.grid.origin[0] + (cx + 0.5) * a.grid.cell_size;
+    const double ccy = a.grid.origin[1] + (cy + 0.5) * a.grid.cell_size;
+    const double ccz = a.grid.origin[2] + (cz + 0.5) * a.grid.cell_size;
+    const int chunks = static_cast<int>((nc + kWarp - 1) / kWarp);
+    {
+      int t = 0;  // each lane's source cell only moves forward
+      for (index_t k = lane; k < chunks * kWarp; k += kWarp) {
+        float4 v = make_float4(kSentinel, kSentinel, kSentinel, __int_as_float(-1));
+        if (k < nc) {
+          while (pre[t + 1] <= k) ++t;
+          const index_t pos = cb[t] + (k - pre[t]);
+          const double4 q = a.src_pos[pos];
+          v = make_float4(to_rel(q.x, ccx, a.inv_h), to_rel(q.y, ccy, a.inv_h), to_rel(q.z, ccz, a.inv_h),
+                          __int_as_float(pos));
+        }
+        rel[k] = v;
+      }
+    }
+    __syncwarp();
+    const index_t self_base = pre[13];
+    for (index_t h0 = hb; h0 < he; h0 += kWarp) {
+      const index_t h = h0 + lane;
+      const bool live = h < he;
+      index_t i = 0;
+      double xi = 0.0, yi = 0.0, zi = 0.0;
+      // idle lanes sit far from every candidate and from the sentinels
+      float rx = -kSentinel, ry = -kSentinel, rz = -kSentinel;
+      int self_chunk = -1;
+      unsigned self_bit = 0u;
+      if (live) {
+        i = a.home_sorted[h];
+        xi = a.fx[i];
+        yi = a.fy[i];
+        zi = a.fz[i];
+        rx = to_rel(xi, ccx, a.inv_h);
+        ry = to_rel(yi, ccy, a.inv_h);
+        rz = to_rel(zi, ccz, a.inv_h);
+        if (a.exclude_self) {
+          const index_t k = self_base + (h - hb);
+          self_chunk = static_cast<int>(k >> 5);
+          self_bit = 1u << (k & 31);
+        }
+      }
+      index_t count = 0;
+      for (int ch = 0; ch < chunks; ++ch) {
+        const float4* q = rel + ch * kWarp;
+        unsigned lo = 0u, near = 0u;
+#pragma unroll
+        for (int bit = 0; bit < kWarp; ++bit) {
+          const float4 v = q[bit];
+          const float dx = rx - v.x, dy = ry - v.y, dz = rz - v.z;
+          const float d2 = dx * dx + dy * dy + dz * dz;
+          if (d2 < a.lo2) lo |= 1u << bit;
+          if (!(d2 > a.hi2)) near |= 1u << bit;  // near the boundary, or NaN (outside the window)
+        }
+        for (unsigned amb = near & ~lo; amb; amb &= amb - 1) {
+          const int bit = __ffs(amb) - 1;
+          const int pos = __float_as_int(q[bit].w);
+          if (pos >= 0) {
+            const double4 s = a.src_pos[pos];
+            if (within_radius(xi, yi, zi, s.x, s.y, s.z, a.r2)) lo |= 1u << bit;
+          }
+        }
+        if (ch == self_chunk) lo &= ~self_bit;
+        count += __popc(lo);
+        msk[lane * kMaskStride + ch] = lo;
+      }
+      __syncwarp();
+      const int nlive = static_cast<int>(min(static_cast<index_t>(kWarp), he - h0));
+      for (int p = 0; p < nlive; ++p) {
+        const index_t ip = __shfl_sync(0xffffffffu, i, p);
+        if (lane < chunks) a.bits[static_cast<size_t>(ip) * kMaskWords + lane] = msk[p * kMaskStride + lane];
+      }
+      if (live) a.offsets[i] = count;
+      __syncwarp();
+    }
+  }
+}
+
+// Write pass: one block per home cell; the block stages the candidate indices
+// of the 27-cell sequence, then each warp takes one home particle and replays
+// its accept masks into the row (an exclusive scan of the chunk popcounts
+// gives each chunk's base), so rows come out in the reference's order.
+__global__ void __launch_bounds__(kCsrThreads) csr_write_kernel(CsrArgs a) {
   __shared__ index_t s_idx[kStageCap];
   __shared__ index_t s_cb[27];
   __shared__ index_t s_cnt[27];
@@ -107,7 +269,7 @@ __global__ void __launch_bounds__(kCsrThreads) csr_kernel(CsrArgs a) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const unsigned lanemask_lt = (1u << lane) - 1u;
   const int dimx = a.grid.dims[0], dimy = a.grid.dims[1], dimz = a.grid.dims[2];
-  if (kWrite && blockIdx.x == 0 && threadIdx.x == 0 && static_cast<unsigned long long>(*a.total) > a.capacity)
+  if (blockIdx.x == 0 && threadIdx.x == 0 && static_cast<unsigned long long>(*a.total) > a.capacity)
     record_required(a.status, static_cast<unsigned long long>(*a.total));
   for (index_t c = blockIdx.x; c < a.ncell; c += gridDim.x) {
     const index_t hb = a.home_begin[c];
@@ -140,91 +302,19 @@ __global__ void __launch_bounds__(kCsrThreads) csr_kernel(CsrArgs a) {
     }
     __syncthreads();
     const index_t nc = s_pre[27];
-    const double ccx = a.grid.origin[0] + (cx + 0.5) * a.grid.cell_size;
-    const double ccy = a.grid.origin[1] + (cy + 0.5) * a.grid.cell_size;
-    const double ccz = a.grid.origin[2] + (cz + 0.5) * a.grid.cell_size;
     const bool staged = nc <= kStageCap;
     if (staged) {
+      int t = 0;  // each thread's source cell only moves forward
       for (index_t k = threadIdx.x; k < nc; k += kCsrThreads) {
-        int t = 0;
         while (s_pre[t + 1] <= k) ++t;
-        const index_t pos = s_cb[t] + (k - s_pre[t]);
-        s_idx[k] = a.src_sorted[pos];
-        if (!kWrite) {
-          const double4 q = a.src_pos[pos];
-          s_rel[k] = make_float4(to_rel(q.x, ccx, a.inv_h), to_rel(q.y, ccy, a.inv_h), to_rel(q.z, ccz, a.inv_h), 0.0f);
-        }
+        s_idx[k] = a.src_sorted[s_cb[t] + (k - s_pre[t])];
       }
     }
     __syncthreads();
-    if (!kWrite && staged) {
-      // Count pass over the staged set: each warp tests two home particles
-      // per staged chunk (one shared-memory read of the candidate for both).
-      for (index_t h = hb + 2 * warp; h < he; h += 2 * kCsrWarps) {
-        const bool two = h + 1 < he;
-        const index_t i0 = a.home_sorted[h];
-        const index_t i1 = two ? a.home_sorted[h + 1] : i0;
-        const double x0 = a.fx[i0], y0 = a.fy[i0], z0 = a.fz[i0];
-        const double x1 = a.fx[i1], y1 = a.fy[i1], z1 = a.fz[i1];
-        const float r0x = to_rel(x0, ccx, a.inv_h), r0y = to_rel(y0, ccy, a.inv_h), r0z = to_rel(z0, ccz, a.inv_h);
-        const float r1x = to_rel(x1, ccx, a.inv_h), r1y = to_rel(y1, ccy, a.inv_h), r1z = to_rel(z1, ccz, a.inv_h);
-        unsigned keep0 = 0u, keep1 = 0u;  // lane c keeps chunk c's masks
-        index_t count0 = 0, count1 = 0;
-        for (index_t base = 0; base < nc; base += kWarp) {
-          const index_t k = base + lane;
-          bool pass0 = false, pass1 = false;
-          if (k < nc) {
-            const index_t j = s_idx[k];
-            const float4 q = s_rel[k];
-            if (!(a.exclude_self && j == i0)) {
-              const float dx = r0x - q.x, dy = r0y - q.y, dz = r0z - q.z;
-              const float d2 = dx * dx + dy * dy + dz * dz;
-              if (d2 < a.lo2) {
-                pass0 = true;
-              } else if (!(d2 > a.hi2)) {  // near the boundary, or NaN (far)
-                pass0 = within_radius(x0, y0, z0, a.sx[j], a.sy[j], a.sz[j], a.r2);
-              }
-            }
-            if (two && !(a.exclude_self && j == i1)) {
-              const float dx = r1x - q.x, dy = r1y - q.y, dz = r1z - q.z;
-              const float d2 = dx * dx + dy * dy + dz * dz;
-              if (d2 < a.lo2) {
-                pass1 = true;
-              } else if (!(d2 > a.hi2)) {
-                pass1 = within_radius(x1, y1, z1, a.sx[j], a.sy[j], a.sz[j], a.r2);
-              }
-            }
-          }
-          const unsigned m0 = __ballot_sync(0xffffffffu, pass0);
-          const unsigned m1 = __ballot_sync(0xffffffffu, pass1);
-          if (lane == base / kWarp) {
-            keep0 = m0;
-            keep1 = m1;
-          }
-          count0 += __popc(m0);
-          count1 += __popc(m1);
-        }
-        const int chunks = (nc + kWarp - 1) / kWarp;
-        if (lane < chunks) {
-          a.bits[static_cast<size_t>(i0) * kMaskWords + lane] = keep0;
-          if (two) a.bits[static_cast<size_t>(i1) * kMaskWords + lane] = keep1;
-        }
-        if (lane == 0) {
-          a.offsets[i0] = count0;
-          if (two) a.offsets[i1] = count1;
-        }
-      }
-      __syncthreads();
-      continue;
-    }
     for (index_t h = hb + warp; h < he; h += kCsrWarps) {
       const index_t i = a.home_sorted[h];
-      index_t out = 0;
-      if (kWrite) out = a.offsets[i];
-      index_t count = 0;
-      if (staged && kWrite) {
-        // Replay the count pass's accept masks: lane c holds chunk c's mask,
-        // an exclusive warp scan of the popcounts gives each chunk's base.
+      index_t out = a.offsets[i];
+      if (staged) {
         const int chunks = (nc + kWarp - 1) / kWarp;
         const unsigned word = lane < chunks ? a.bits[static_cast<size_t>(i) * kMaskWords + lane] : 0u;
         const int pc = __popc(word);
@@ -235,71 +325,38 @@ __global__ void __launch_bounds__(kCsrThreads) csr_kernel(CsrArgs a) {
           if (lane >= d) incl += t;
         }
         const int base_mine = incl - pc;
-        for (int c = 0; c < chunks; ++c) {
-          const unsigned m = __shfl_sync(0xffffffffu, word, c);
-          const int cb = __shfl_sync(0xffffffffu, base_mine, c);
+        for (int ch = 0; ch < chunks; ++ch) {
+          const unsigned m = __shfl_sync(0xffffffffu, word, ch);
+          const int cbase = __shfl_sync(0xffffffffu, base_mine, ch);
           if ((m >> lane) & 1u) {
-            const unsigned long long pos =
-                static_cast<unsigned long long>(out) + cb + __popc(m & lanemask_lt);
-            if (pos < a.capacity) a.indices[pos] = s_idx[c * kWarp + lane];
+            const unsigned long long pos = static_cast<unsigned long long>(out) + cbase + __popc(m & lanemask_lt);
+            if (pos < a.capacity) a.indices[pos] = s_idx[ch * kWarp + lane];
           }
         }
         continue;
       }
+      // More candidates than the stage holds (overloaded edge cells): exact
+      // tests straight from global memory, same order.
       const double xi = a.fx[i], yi = a.fy[i], zi = a.fz[i];
-      if (staged) {
-        unsigned my_mask = 0u;  // lane c keeps chunk c's accept mask
-        const float rx = to_rel(xi, ccx, a.inv_h), ry = to_rel(yi, ccy, a.inv_h), rz = to_rel(zi, ccz, a.inv_h);
-        for (index_t base = 0; base < nc; base += kWarp) {
+      for (int t = 0; t < 27; ++t) {
+        const index_t cnt = s_cnt[t];
+        const index_t b = s_cb[t];
+        for (index_t base = 0; base < cnt; base += kWarp) {
           const index_t k = base + lane;
           bool pass = false;
           index_t j = 0;
-          if (k < nc) {
-            j = s_idx[k];
-            if (!(a.exclude_self && j == i)) {
-              const float4 q = s_rel[k];
-              const float dx = rx - q.x, dy = ry - q.y, dz = rz - q.z;
-              const float d2 = dx * dx + dy * dy + dz * dz;
-              if (d2 < a.lo2) {
-                pass = true;
-              } else if (!(d2 > a.hi2)) {  // near the boundary, or NaN (far)
-                pass = within_radius(xi, yi, zi, a.sx[j], a.sy[j], a.sz[j], a.r2);
-              }
-            }
+          if (k < cnt) {
+            j = a.src_sorted[b + k];
+            if (!(a.exclude_self && j == i)) pass = within_radius(xi, yi, zi, a.sx[j], a.sy[j], a.sz[j], a.r2);
           }
           const unsigned m = __ballot_sync(0xffffffffu, pass);
-          if (lane == base / kWarp) my_mask = m;
-          count += __popc(m);
-        }
-        if (lane < (nc + kWarp - 1) / kWarp) a.bits[static_cast<size_t>(i) * kMaskWords + lane] = my_mask;
-      } else {
-        // More candidates than the stage holds (overloaded edge cells):
-        // exact tests straight from global memory, same order.
-        for (int t = 0; t < 27; ++t) {
-          const index_t cnt = s_cnt[t];
-          const index_t b = s_cb[t];
-          for (index_t base = 0; base < cnt; base += kWarp) {
-            const index_t k = base + lane;
-            bool pass = false;
-            index_t j = 0;
-            if (k < cnt) {
-              j = a.src_sorted[b + k];
-              if (!(a.exclude_self && j == i)) pass = within_radius(xi, yi, zi, a.sx[j], a.sy[j], a.sz[j], a.r2);
-            }
-            const unsigned m = __ballot_sync(0xffffffffu, pass);
-            if (kWrite) {
-              if (pass) {
-                const unsigned long long pos = static_cast<unsigned long long>(out) + __popc(m & lanemask_lt);
-                if (pos < a.capacity) a.indices[pos] = j;
-              }
-              out += __popc(m);
-            } else {
-              count += __popc(m);
-            }
+          if (pass) {
+            const unsigned long long pos = static_cast<unsigned long long>(out) + __popc(m & lanemask_lt);
+            if (pos < a.capacity) a.indices[pos] = j;
           }
+          out += __popc(m);
         }
       }
-      if (!kWrite && lane == 0) a.offsets[i] = count;
     }
     __syncthreads();
   }
@@ -333,6 +390,10 @@ lsmps_status one_neighbor_list(lsmps_ctx* ctx, Scratch& scratch, const lsmps_flu
   a.hi2 = static_cast<float>(r2n) + kScreenMargin;
   a.ncell = static_cast<index_t>(static_cast<long long>(grid.dims[0]) * grid.dims[1] * grid.dims[2]);
   a.exclude_self = exclude_self ? 1 : 0;
+  // the count pass finds a particle's own bit through the home cell's place
+  // in the source list, so the self-excluding table must use one cell list
+  if (exclude_self && (home.sorted_indices != src.sorted_indices || home.cell_begin != src.cell_begin))
+    return fail(ctx, LSMPS_INVALID_ARGUMENT, "self-excluding neighbour table needs one cell list");
   a.offsets = out.offsets;
   a.indices = out.indices;
   a.capacity = out.neighbor_count;
@@ -350,11 +411,13 @@ lsmps_status one_neighbor_list(lsmps_ctx* ctx, Scratch& scratch, const lsmps_flu
     launch(ctx, sorted_positions_kernel, dim3(pb), dim3(256), 0, sx, sy, sz,
            static_cast<const index_t*>(src.sorted_indices), static_cast<index_t>(n_src), src_pos);
   }
-  const int blocks = static_cast<int>(std::min<long long>(a.ncell, static_cast<long long>(ctx->sm_count) * 16));
-  if (n) launch(ctx, csr_kernel<false>, dim3(blocks), dim3(kCsrThreads), 0, a);
+  const int count_blocks = static_cast<int>(
+      std::min<long long>(div_up(static_cast<long long>(a.ncell), kCountWarps), static_cast<long long>(ctx->sm_count) * 20));
+  if (n) launch(ctx, csr_count_kernel, dim3(count_blocks), dim3(kCountWarps * kWarp), 0, a);
   lsmps_status st = exclusive_scan_i32(ctx, scratch, out.offsets, out.offsets, n, nullptr, out.offsets + n);
   if (st) return st;
-  if (n) launch(ctx, csr_kernel<true>, dim3(blocks), dim3(kCsrThreads), 0, a);
+  const int blocks = static_cast<int>(std::min<long long>(a.ncell, static_cast<long long>(ctx->sm_count) * 16));
+  if (n) launch(ctx, csr_write_kernel, dim3(blocks), dim3(kCsrThreads), 0, a);
   return check_launch(ctx, "neighbour list");
 }
 

@@ -89,8 +89,8 @@ def kernel_bytes(nf: int, nw: int, kf: int, kw: int, c: int, s: int = 8) -> dict
     out["expand_kernel"] = 4 * (nf + 1) + 4 * kf + 8 * nf
     count_fluid = 2 * pos_f + 8 * c + 4 * nf + 4 * nf
     count_wall = pos_f + pos_w + 8 * c + 4 * nw + 4 * nf
-    out["csr_kernel<false>"] = (count_fluid + count_wall) // 2
-    out["csr_kernel<true>"] = (count_fluid + count_wall + 8 * nf + 4 * k) // 2
+    out["csr_count_kernel"] = (count_fluid + count_wall) // 2
+    out["csr_write_kernel"] = (count_fluid + count_wall + 8 * nf + 4 * k) // 2
     # virtual-light diagnostic (not in the step): rows, positions, count + fraction
     out["virtual_light_kernel"] = rows + pos_f + pos_w + (4 + s) * nf
     return out
