@@ -43,6 +43,7 @@ constexpr int kMaskWords = kStageCap / 32;
 constexpr int kCountWarps = 2;               // warps (home cells) per block of the count pass
 constexpr int kMaskStride = kMaskWords + 1;  // padded row of the count pass's mask transpose
 constexpr float kSentinel = 1.0e18f;         // far enough that d^2 stays finite and rejected
+constexpr int kStageBatch = 8;               // candidate loads in flight per lane while staging
 
 struct CsrArgs {
   const double* fx;
@@ -183,17 +184,32 @@ __global__ void __launch_bounds__(kCountWarps * kWarp) csr_count_kernel(CsrArgs 
     const double ccz = a.grid.origin[2] + (cz + 0.5) * a.grid.cell_size;
     const int chunks = static_cast<int>((nc + kWarp - 1) / kWarp);
     {
+      // kStageBatch loads in flight per lane: the staging is a chain of L2
+      // round trips otherwise
       int t = 0;  // each lane's source cell only moves forward
-      for (index_t k = lane; k < chunks * kWarp; k += kWarp) {
-        float4 v = make_float4(kSentinel, kSentinel, kSentinel, __int_as_float(-1));
-        if (k < nc) {
-          while (pre[t + 1] <= k) ++t;
-          const index_t pos = cb[t] + (k - pre[t]);
-          const double4 q = a.src_pos[pos];
-          v = make_float4(to_rel(q.x, ccx, a.inv_h), to_rel(q.y, ccy, a.inv_h), to_rel(q.z, ccz, a.inv_h),
-                          __int_as_float(pos));
+      for (index_t k0 = lane; k0 < chunks * kWarp; k0 += kStageBatch * kWarp) {
+        index_t pos[kStageBatch];
+        double4 q[kStageBatch];
+#pragma unroll
+        for (int u = 0; u < kStageBatch; ++u) {
+          const index_t k = k0 + u * kWarp;
+          pos[u] = -1;
+          if (k < nc) {
+            while (pre[t + 1] <= k) ++t;
+            pos[u] = cb[t] + (k - pre[t]);
+          }
         }
-        rel[k] = v;
+#pragma unroll
+        for (int u = 0; u < kStageBatch; ++u)
+          if (pos[u] >= 0) q[u] = a.src_pos[pos[u]];
+#pragma unroll
+        for (int u = 0; u < kStageBatch; ++u) {
+          const index_t k = k0 + u * kWarp;
+          if (k >= chunks * kWarp) break;
+          rel[k] = pos[u] >= 0 ? make_float4(to_rel(q[u].x, ccx, a.inv_h), to_rel(q[u].y, ccy, a.inv_h),
+                                             to_rel(q[u].z, ccz, a.inv_h), __int_as_float(pos[u]))
+                               : make_float4(kSentinel, kSentinel, kSentinel, __int_as_float(-1));
+        }
       }
     }
     __syncwarp();
