@@ -18,12 +18,13 @@
 //
 // Exactness: the FP32 distance is only a screen.  With coordinates scaled by
 // 1/h and re-centred on the home cell, every component is at most 2 in
-// magnitude for particles inside the grid, and the FP32 squared distance
-// differs from the exact one by less than 384 * 2^-24 < 2.3e-5.  A candidate
-// is accepted or rejected from FP32 only when it is more than
-// kScreenMargin = 1e-4 away from (r/h)^2; everything closer, and every
-// particle outside the +-2 window (clamped into an edge cell), is decided by
-// the reference's own FP64 test dx*dx + dy*dy + dz*dz <= r^2
+// magnitude for particles inside the grid, and the FP32 value of
+// e = d^2 - lo2 (lo2 = (r/h)^2 - kScreenMargin, formed by three fused
+// multiply-adds on the FP32 differences) is within a few hundred 2^-24 of the
+// exact one, far inside kScreenMargin = 1e-4.  A candidate is accepted from
+// FP32 when e < 0 and rejected when e >= 2 kScreenMargin; everything between,
+// and every particle outside the +-2 window (clamped into an edge cell), is
+// decided by the reference's own FP64 test dx*dx + dy*dy + dz*dz <= r^2
 // (neighbor_search.cu:48-59).  The neighbour sets are therefore the FP64 ones.
 #include <algorithm>
 #include <climits>
@@ -61,8 +62,8 @@ struct CsrArgs {
   lsmps_grid grid;
   double r2;
   double inv_h;
-  float lo2;
-  float hi2;
+  float lo2;   // (r/h)^2 - kScreenMargin
+  float band;  // a little over 2 kScreenMargin: FP32 rejects only e >= band
   index_t ncell;
   int exclude_self;
   index_t* offsets;  // count pass: per-particle counts; write pass: row offsets
@@ -102,17 +103,39 @@ __device__ __forceinline__ float to_rel(double v, double centre, double inv_h) {
   return fabsf(r) <= kFarLimit ? r : __int_as_float(0x7fc00000);  // NaN forces the exact test
 }
 
+// Two FP32 lanes in one 64-bit register (the first in the low half) and the
+// packed FP32 arithmetic of sm_100 on them: one instruction per pair.
+__device__ __forceinline__ unsigned long long pack2(float lo, float hi) {
+  return (static_cast<unsigned long long>(__float_as_uint(hi)) << 32) | __float_as_uint(lo);
+}
+__device__ __forceinline__ unsigned long long sub2(unsigned long long a, unsigned long long b) {
+  unsigned long long d;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ unsigned long long fma2(unsigned long long a, unsigned long long b, unsigned long long c) {
+  unsigned long long d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+// (acc << 1) | sign bit of the FP32 value in v's low (kHigh: high) half.
+template <bool kHigh>
+__device__ __forceinline__ unsigned shift_in_sign(unsigned acc, unsigned long long v) {
+  return __funnelshift_l(static_cast<unsigned>(kHigh ? v >> 32 : v), acc, 1);
+}
+
 __device__ __forceinline__ index_t warp_sum(index_t v) {
   for (int d = 16; d > 0; d >>= 1) v += __shfl_xor_sync(0xffffffffu, v, d);
   return v;
 }
 
 // Count pass: one warp per home cell, one lane per home particle.  The warp
-// stages its 27-cell candidate sequence (cell-relative FP32 coordinates, the
-// candidate's cell-sorted position in .w) in shared memory, padded to whole
-// 32-candidate chunks with far sentinels; every lane then walks the sequence
-// with broadcast loads, so one shared-memory read serves the whole cell's
-// particles and each candidate costs a lane a handful of FP32 instructions.
+// stages its 27-cell candidate sequence (cell-relative FP32 coordinates and
+// the candidate's cell-sorted position) in shared memory, padded to whole
+// 32-candidate chunks with far sentinels and laid out by candidate pairs
+// ({x0, x1, y0, y1}, {z0, z1, pos0, pos1}), so that every lane walks the
+// sequence with broadcast loads and tests two candidates per packed FP32
+// instruction; the sign of e = d^2 - lo2 is shifted straight into the mask.
 // Bit b of chunk c of a lane's mask is the candidate at sequence position
 // 32c + b, the numbering the write pass replays.  In the fluid table the
 // home cell is the centre source cell, so a particle's own bit sits at
@@ -121,11 +144,14 @@ __device__ __forceinline__ index_t warp_sum(index_t v) {
 __global__ void __launch_bounds__(kCountWarps * kWarp) csr_count_kernel(CsrArgs a) {
   __shared__ float4 s_rel[kCountWarps][kStageCap];
   __shared__ unsigned s_mask[kCountWarps][kWarp * kMaskStride];
+  __shared__ unsigned s_far[kCountWarps][kMaskWords];  // per chunk: candidates outside the window
   __shared__ index_t s_cb[kCountWarps][27];
   __shared__ index_t s_pre[kCountWarps][28];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   float4* rel = s_rel[w];
+  float* relf = reinterpret_cast<float*>(rel);
   unsigned* msk = s_mask[w];
+  unsigned* far = s_far[w];
   index_t* cb = s_cb[w];
   index_t* pre = s_pre[w];
   const int dimx = a.grid.dims[0], dimy = a.grid.dims[1], dimz = a.grid.dims[2];
@@ -205,10 +231,20 @@ __global__ void __launch_bounds__(kCountWarps * kWarp) csr_count_kernel(CsrArgs 
 #pragma unroll
         for (int u = 0; u < kStageBatch; ++u) {
           const index_t k = k0 + u * kWarp;
-          if (k >= chunks * kWarp) break;
-          rel[k] = pos[u] >= 0 ? make_float4(to_rel(q[u].x, ccx, a.inv_h), to_rel(q[u].y, ccy, a.inv_h),
-                                             to_rel(q[u].z, ccz, a.inv_h), __int_as_float(pos[u]))
-                               : make_float4(kSentinel, kSentinel, kSentinel, __int_as_float(-1));
+          if (k >= chunks * kWarp) break;  // uniform: the lanes of one u share a chunk
+          float x = kSentinel, y = kSentinel, z = kSentinel;
+          if (pos[u] >= 0) {
+            x = to_rel(q[u].x, ccx, a.inv_h);
+            y = to_rel(q[u].y, ccy, a.inv_h);
+            z = to_rel(q[u].z, ccz, a.inv_h);
+          }
+          float* slot = relf + (k >> 1) * 8 + (k & 1);
+          slot[0] = x;
+          slot[2] = y;
+          slot[4] = z;
+          slot[6] = __int_as_float(static_cast<int>(pos[u]));
+          const unsigned outside = __ballot_sync(0xffffffffu, isnan(x) || isnan(y) || isnan(z));
+          if (lane == 0) far[k >> 5] = outside;
         }
       }
     }
@@ -223,6 +259,7 @@ __global__ void __launch_bounds__(kCountWarps * kWarp) csr_count_kernel(CsrArgs 
       float rx = -kSentinel, ry = -kSentinel, rz = -kSentinel;
       int self_chunk = -1;
       unsigned self_bit = 0u;
+      bool home_far = false;
       if (live) {
         i = a.home_sorted[h];
         xi = a.fx[i];
@@ -231,31 +268,45 @@ __global__ void __launch_bounds__(kCountWarps * kWarp) csr_count_kernel(CsrArgs 
         rx = to_rel(xi, ccx, a.inv_h);
         ry = to_rel(yi, ccy, a.inv_h);
         rz = to_rel(zi, ccz, a.inv_h);
+        home_far = isnan(rx) || isnan(ry) || isnan(rz);
         if (a.exclude_self) {
           const index_t k = self_base + (h - hb);
           self_chunk = static_cast<int>(k >> 5);
           self_bit = 1u << (k & 31);
         }
       }
+      const unsigned long long rxx = pack2(rx, rx), ryy = pack2(ry, ry), rzz = pack2(rz, rz);
+      const unsigned long long nlo = pack2(-a.lo2, -a.lo2), band = pack2(a.band, a.band);
       index_t count = 0;
       for (int ch = 0; ch < chunks; ++ch) {
-        const float4* q = rel + ch * kWarp;
+        const ulonglong2* q = reinterpret_cast<const ulonglong2*>(rel + ch * kWarp);
+        // bit 31 - b: candidate b accepted from FP32 (e < 0) / not rejected (e < band)
         unsigned lo = 0u, near = 0u;
 #pragma unroll
-        for (int bit = 0; bit < kWarp; ++bit) {
-          const float4 v = q[bit];
-          const float dx = rx - v.x, dy = ry - v.y, dz = rz - v.z;
-          const float d2 = dx * dx + dy * dy + dz * dz;
-          if (d2 < a.lo2) lo |= 1u << bit;
-          if (!(d2 > a.hi2)) near |= 1u << bit;  // near the boundary, or NaN (outside the window)
+        for (int pr = 0; pr < kWarp / 2; ++pr) {
+          const ulonglong2 xy = q[2 * pr], zp = q[2 * pr + 1];
+          const unsigned long long dx = sub2(rxx, xy.x), dy = sub2(ryy, xy.y), dz = sub2(rzz, zp.x);
+          unsigned long long e = fma2(dx, dx, nlo);
+          e = fma2(dy, dy, e);
+          e = fma2(dz, dz, e);
+          const unsigned long long f = sub2(e, band);
+          lo = shift_in_sign<true>(shift_in_sign<false>(lo, e), e);
+          near = shift_in_sign<true>(shift_in_sign<false>(near, f), f);
         }
-        for (unsigned amb = near & ~lo; amb; amb &= amb - 1) {
+        lo = __brev(lo);
+        near = __brev(near);
+        // between the thresholds, or a coordinate outside the window: FP64
+        unsigned amb = (near & ~lo) | far[ch];
+        if (home_far) amb = ~0u;
+        for (; amb; amb &= amb - 1) {
           const int bit = __ffs(amb) - 1;
-          const int pos = __float_as_int(q[bit].w);
+          const int pos = __float_as_int(relf[ch * kWarp * 4 + (bit >> 1) * 8 + 6 + (bit & 1)]);
+          bool in = false;
           if (pos >= 0) {
-            const double4 s = a.src_pos[pos];
-            if (within_radius(xi, yi, zi, s.x, s.y, s.z, a.r2)) lo |= 1u << bit;
+            const double4 sp = a.src_pos[pos];
+            in = within_radius(xi, yi, zi, sp.x, sp.y, sp.z, a.r2);
           }
+          lo = in ? (lo | (1u << bit)) : (lo & ~(1u << bit));
         }
         if (ch == self_chunk) lo &= ~self_bit;
         count += __popc(lo);
@@ -403,7 +454,7 @@ lsmps_status one_neighbor_list(lsmps_ctx* ctx, Scratch& scratch, const lsmps_flu
   a.inv_h = 1.0 / grid.cell_size;
   const double r2n = a.r2 * a.inv_h * a.inv_h;
   a.lo2 = static_cast<float>(r2n) - kScreenMargin;
-  a.hi2 = static_cast<float>(r2n) + kScreenMargin;
+  a.band = 2.0f * kScreenMargin * 1.001f;
   a.ncell = static_cast<index_t>(static_cast<long long>(grid.dims[0]) * grid.dims[1] * grid.dims[2]);
   a.exclude_self = exclude_self ? 1 : 0;
   // the count pass finds a particle's own bit through the home cell's place

@@ -60,13 +60,24 @@ index_t clamp_cell_index(double coordinate, double origin, double cell_size, ind
   return index;
 }
 
-// neighbor_search.cu:48-59
+// neighbor_search.cu:48-59.  The reference evaluates dx*dx + dy*dy + dz*dz
+// <= r^2 on the device, where nvcc contracts the sum into fused
+// multiply-adds; for pairs within rounding of r (an unjittered lattice whose
+// spacing divides r) the contracted and the twice-rounded sums decide
+// differently, so the oracle states the contracted form explicitly:
+// fma(dz, dz, fma(dx, dx, dy * dy)), the one of the six orders that
+// reproduces the reference's CUDA path on such a lattice pair for pair
+// (tests/test_gpu_parity.py, test_csr_pairs_at_the_radius).
 bool within_radius(double ax, double ay, double az, double bx, double by, double bz,
                    double radius_squared) {
   const double dx = ax - bx;
   const double dy = ay - by;
   const double dz = az - bz;
-  return dx * dx + dy * dy + dz * dz <= radius_squared;
+  // the two sums differ by a few units in the last place (no cancellation:
+  // squares), so the fused one is only needed close to r^2
+  const double twice = dx * dx + dy * dy + dz * dz;
+  if (std::fabs(twice - radius_squared) > 1e-12 * radius_squared) return twice <= radius_squared;
+  return std::fma(dz, dz, std::fma(dx, dx, dy * dy)) <= radius_squared;
 }
 
 // build_cell_list_impl, neighbor_search.cu:255-292: assign cells (:61-73),

@@ -9,6 +9,9 @@ factorisation route (L^-T L^-1 versus substitution against identity columns),
 so the bound is set by rounding times the moment matrices' conditioning.
 """
 
+import os
+import sys
+
 import numpy as np
 import pytest
 
@@ -484,6 +487,44 @@ def test_overloaded_and_out_of_grid_cells(pkg, device_api, ctx, oracle):
         ho, hi = host.csr_rows(which)
         assert np.array_equal(go, ho) and np.array_equal(gi, hi)
     assert n + k == big.n_fluid
+
+
+@pytest.mark.parametrize("radius_l0", [2.0, 3.0, 6.0 ** 0.5])
+def test_csr_pairs_at_the_radius(pkg, device_api, ctx, oracle, radius_l0):
+    """An unjittered lattice with the support radius equal to a lattice
+    distance (2 l0, 3 l0 = |(2,2,1)| l0, sqrt(6) l0 = |(2,1,1)| l0): many
+    pairs lie within rounding of r, where the FP32 screen must hand over to
+    the reference's FP64 test.  Rows must match the oracle, and the
+    reference's own CUDA path where it is built, bit for bit."""
+    case = pkg.cases.hydrostatic_box(n=12, l0=0.01)
+    p = case.params
+    p.support_radius = radius_l0 * case.l0
+    p.grid.cell_size = p.support_radius
+    pkg.cases.derive_grid(p, [case.fluid["x"], case.walls["x"]], [case.fluid["y"], case.walls["y"]],
+                          [case.fluid["z"], case.walls["z"]])
+    dev, host = both(pkg, device_api, case, max_fluid_neighbors=256, max_wall_neighbors=256)
+    ctx.build_neighbor_lists(dev, p)
+    oracle.build_neighbor_lists(host, p)
+    for which in ("fluid", "wall"):
+        go, gi = dev.csr_rows(which)
+        ho, hi = host.csr_rows(which)
+        assert np.array_equal(go, ho) and np.array_equal(gi, hi), which
+    # the reference's own CUDA path decides the ties the same way (its device
+    # distance test contracts into fused multiply-adds, as the oracle states)
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle"))
+    import reference as ref_mod
+
+    if ref_mod.available():
+        rb = pkg.buffers.StepBuffers(pkg.buffers.NumpyAlloc(), case.n_fluid, case.n_wall, case.n_cells,
+                                     max_fluid_neighbors=256, max_wall_neighbors=256)
+        rb.load_case(case)
+        ref = ref_mod.ReferencePath(pkg.abi, case, rb, 256, 256)
+        ref.rebuild()
+        ref.fetch_geometry()
+        for which in ("fluid", "wall"):
+            go, gi = dev.csr_rows(which)
+            ro, ri = rb.csr_rows(which)
+            assert np.array_equal(go, ro) and np.array_equal(gi, ri), ("reference", which)
 
 
 def test_cell_list_random_keys_stable(pkg, device_api, ctx, oracle):
