@@ -324,6 +324,25 @@ __global__ void __launch_bounds__(kCountWarps * kWarp) csr_count_kernel(CsrArgs 
   }
 }
 
+// Position of the n-th (from 0) set bit of w, n < popc(w): two halving steps
+// down to a byte, then a table of the set-bit positions of every byte.
+__device__ __forceinline__ int nth_set_bit(unsigned w, int n, const unsigned char* nth) {
+  int pos = 0;
+  int c = __popc(w & 0xffffu);
+  if (n >= c) {
+    n -= c;
+    w >>= 16;
+    pos = 16;
+  }
+  c = __popc(w & 0xffu);
+  if (n >= c) {
+    n -= c;
+    w >>= 8;
+    pos += 8;
+  }
+  return pos + nth[(w & 0xffu) * 8 + (n & 7)];
+}
+
 // Write pass: one block per home cell; the block stages the candidate indices
 // of the 27-cell sequence, then each warp takes one home particle and replays
 // its accept masks into the row (an exclusive scan of the chunk popcounts
@@ -333,9 +352,18 @@ __global__ void __launch_bounds__(kCsrThreads) csr_write_kernel(CsrArgs a) {
   __shared__ index_t s_cb[27];
   __shared__ index_t s_cnt[27];
   __shared__ index_t s_pre[28];
+  __shared__ int s_list[kCsrWarps][kWarp];
+  __shared__ unsigned char s_nth[256 * 8];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const unsigned lanemask_lt = (1u << lane) - 1u;
   const int dimx = a.grid.dims[0], dimy = a.grid.dims[1], dimz = a.grid.dims[2];
+  for (int b = threadIdx.x; b < 256; b += kCsrThreads) {
+    int k = 0;
+    for (int bit = 0; bit < 8; ++bit)
+      if ((b >> bit) & 1) s_nth[b * 8 + k++] = static_cast<unsigned char>(bit);
+    for (; k < 8; ++k) s_nth[b * 8 + k] = 0;
+  }
+  __syncthreads();
   if (blockIdx.x == 0 && threadIdx.x == 0 && static_cast<unsigned long long>(*a.total) > a.capacity)
     record_required(a.status, static_cast<unsigned long long>(*a.total));
   for (index_t c = blockIdx.x; c < a.ncell; c += gridDim.x) {
@@ -392,14 +420,28 @@ __global__ void __launch_bounds__(kCsrThreads) csr_write_kernel(CsrArgs a) {
           if (lane >= d) incl += t;
         }
         const int base_mine = incl - pc;
-        for (int ch = 0; ch < chunks; ++ch) {
+        const int total = __shfl_sync(0xffffffffu, incl, kWarp - 1);
+        // the non-empty chunks in order, so an entry finds its chunk by rank
+        const unsigned nonempty = __ballot_sync(0xffffffffu, pc > 0);
+        if (pc > 0) s_list[warp][__popc(nonempty & lanemask_lt)] = lane;
+        __syncwarp();
+        // 32 consecutive row entries per round, one per lane: coalesced stores
+        for (int r0 = 0; r0 < total; r0 += kWarp) {
+          const bool starts_here = pc > 0 && base_mine >= r0 && base_mine < r0 + kWarp;
+          const unsigned starts = __reduce_or_sync(0xffffffffu, starts_here ? 1u << (base_mine - r0) : 0u);
+          const int before = __popc(__ballot_sync(0xffffffffu, pc > 0 && base_mine < r0));
+          const int e = r0 + lane;
+          const int rank = before + __popc(starts & (0xffffffffu >> (kWarp - 1 - lane))) - 1;
+          const int ch = s_list[warp][min(max(rank, 0), kWarp - 1)];
           const unsigned m = __shfl_sync(0xffffffffu, word, ch);
           const int cbase = __shfl_sync(0xffffffffu, base_mine, ch);
-          if ((m >> lane) & 1u) {
-            const unsigned long long pos = static_cast<unsigned long long>(out) + cbase + __popc(m & lanemask_lt);
-            if (pos < a.capacity) a.indices[pos] = s_idx[ch * kWarp + lane];
+          if (e < total) {
+            const unsigned long long pos = static_cast<unsigned long long>(out) + e;
+            const int bit = nth_set_bit(m, e - cbase, s_nth);
+            if (pos < a.capacity) a.indices[pos] = s_idx[ch * kWarp + bit];
           }
         }
+        __syncwarp();
         continue;
       }
       // More candidates than the stage holds (overloaded edge cells): exact
