@@ -373,27 +373,29 @@ __global__ void __launch_bounds__(kCsrThreads) csr_write_kernel(CsrArgs a) {
     const int cx = c % dimx;
     const int cy = (c / dimx) % dimy;
     const int cz = c / (dimx * dimy);
-    if (threadIdx.x < 27) {
-      const int t = threadIdx.x;
-      const int nz = cz + t / 9 - 1, ny = cy + (t / 3) % 3 - 1, nx = cx + t % 3 - 1;
+    if (warp == 0) {  // the 27 source cells and their starts, one warp scan
       index_t b = -1, n = 0;
-      if (nz >= 0 && nz < dimz && ny >= 0 && ny < dimy && nx >= 0 && nx < dimx) {
-        const index_t cell = (nz * dimy + ny) * dimx + nx;
-        b = a.src_begin[cell];
-        const index_t e = a.src_end[cell];
-        if (b >= 0 && e >= 0) n = e - b;
+      if (lane < 27) {
+        const int nz = cz + lane / 9 - 1, ny = cy + (lane / 3) % 3 - 1, nx = cx + lane % 3 - 1;
+        if (nz >= 0 && nz < dimz && ny >= 0 && ny < dimy && nx >= 0 && nx < dimx) {
+          const index_t cell = (nz * dimy + ny) * dimx + nx;
+          b = a.src_begin[cell];
+          const index_t e = a.src_end[cell];
+          if (b >= 0 && e >= 0) n = e - b;
+        }
       }
-      s_cb[t] = b;
-      s_cnt[t] = n;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      index_t run = 0;
-      for (int t = 0; t < 27; ++t) {
-        s_pre[t] = run;
-        run += s_cnt[t];
+      index_t incl = n;
+#pragma unroll
+      for (int d = 1; d < kWarp; d <<= 1) {
+        const index_t t = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= d) incl += t;
       }
-      s_pre[27] = run;
+      if (lane < 27) {
+        s_cb[lane] = b;
+        s_cnt[lane] = n;
+        s_pre[lane] = incl - n;
+      }
+      if (lane == kWarp - 1) s_pre[27] = incl;
     }
     __syncthreads();
     const index_t nc = s_pre[27];
