@@ -42,7 +42,6 @@ constexpr float kScreenMargin = 1.0e-4f;
 constexpr float kFarLimit = 2.0f;
 constexpr int kMaskWords = kStageCap / 32;
 constexpr int kCountWarps = 2;               // warps (home cells) per block of the count pass
-constexpr int kMaskStride = kMaskWords + 1;  // padded row of the count pass's mask transpose
 constexpr float kSentinel = 1.0e18f;         // far enough that d^2 stays finite and rejected
 constexpr int kStageBatch = 8;               // candidate loads in flight per lane while staging
 
@@ -143,14 +142,12 @@ __device__ __forceinline__ index_t warp_sum(index_t v) {
 // home cell) and is cleared after the tests (the reference skips j == i).
 __global__ void __launch_bounds__(kCountWarps * kWarp) csr_count_kernel(CsrArgs a) {
   __shared__ float4 s_rel[kCountWarps][kStageCap];
-  __shared__ unsigned s_mask[kCountWarps][kWarp * kMaskStride];
   __shared__ unsigned s_far[kCountWarps][kMaskWords];  // per chunk: candidates outside the window
   __shared__ index_t s_cb[kCountWarps][27];
   __shared__ index_t s_pre[kCountWarps][28];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   float4* rel = s_rel[w];
   float* relf = reinterpret_cast<float*>(rel);
-  unsigned* msk = s_mask[w];
   unsigned* far = s_far[w];
   index_t* cb = s_cb[w];
   index_t* pre = s_pre[w];
@@ -310,16 +307,11 @@ __global__ void __launch_bounds__(kCountWarps * kWarp) csr_count_kernel(CsrArgs 
         }
         if (ch == self_chunk) lo &= ~self_bit;
         count += __popc(lo);
-        msk[lane * kMaskStride + ch] = lo;
-      }
-      __syncwarp();
-      const int nlive = static_cast<int>(min(static_cast<index_t>(kWarp), he - h0));
-      for (int p = 0; p < nlive; ++p) {
-        const index_t ip = __shfl_sync(0xffffffffu, i, p);
-        if (lane < chunks) a.bits[static_cast<size_t>(ip) * kMaskWords + lane] = msk[p * kMaskStride + lane];
+        // each lane fills its own particle's 128-byte mask line over the
+        // chunks; the partial writes merge in L2
+        if (live) a.bits[static_cast<size_t>(i) * kMaskWords + ch] = lo;
       }
       if (live) a.offsets[i] = count;
-      __syncwarp();
     }
   }
 }
