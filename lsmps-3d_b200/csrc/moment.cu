@@ -17,6 +17,7 @@
 #include <cmath>
 #include <utility>
 
+#include "f32x2.cuh"
 #include "impl.cuh"
 #include "packed.cuh"
 
@@ -585,14 +586,58 @@ __device__ __forceinline__ void kahan_monomials(float (&s)[kMonomials], float (&
   }
 }
 
+// The 31 weighted monomials as 16 packed pairs: pair p holds monomial
+// sum_pair_lo(p) in its low half and sum_pair_hi(p) in its high half (-1:
+// unused).  Every product is the scalar one of acc_monomials (one rounding of
+// a two-factor product; wxx = w qxx etc.), two per instruction.
+__host__ __device__ constexpr int sum_pair_lo(int p) {
+  constexpr int lo[16] = {0, 2, 4, 6, 8, 9, 10, 13, 16, 18, 19, 20, 28, 24, 25, 27};
+  return lo[p];
+}
+__host__ __device__ constexpr int sum_pair_hi(int p) {
+  constexpr int hi[16] = {1, 3, 5, 7, 15, 11, 12, 14, 17, 30, 21, 29, 22, 23, 26, -1};
+  return hi[p];
+}
+
+__device__ __forceinline__ void monomial_pairs(f32x2 (&t)[16], float sx, float sy, float sz, float w) {
+  const f32x2 xy = pack2(sx, sy);
+  const f32x2 q1 = mul2(xy, xy);                          // qxx, qyy
+  const f32x2 q2 = mul2(pack2(sz, sx), pack2(sz, sy));    // qzz, qxy
+  const f32x2 q3 = mul2(pack2(sy, sz), pack2(sz, sx));    // qyz, qzx
+  const f32x2 ww = pack2(w, w);
+  const f32x2 w1 = mul2(ww, q1);                          // wxx, wyy
+  const f32x2 w2 = mul2(ww, q2);                          // wzz, wxy
+  const f32x2 w3 = mul2(ww, q3);                          // w qyz, w qzx
+  const float wzz = low_half(w2);
+  const f32x2 zz = pack2(wzz, wzz);
+  t[0] = w1;
+  t[1] = w2;
+  t[2] = w3;
+  t[3] = mul2(w1, xy);                                    // wxx x, wyy y
+  t[4] = mul2(w2, pack2(sz, sz));                         // wzz z, wxy z
+  t[5] = mul2(w1, pack2(sy, sx));                         // wxx y, wyy x
+  t[6] = mul2(w1, pack2(sz, sz));                         // wxx z, wyy z
+  t[7] = mul2(zz, xy);                                    // wzz x, wzz y
+  t[8] = mul2(w1, q1);                                    // wxx qxx, wyy qyy
+  t[9] = mul2(zz, q2);                                    // wzz qzz, wzz qxy
+  const float qxy = high_half(q2), qzx = high_half(q3), qyz = low_half(q3);
+  t[10] = mul2(w1, pack2(qxy, qxy));                      // wxx qxy, wyy qxy
+  t[11] = mul2(w1, pack2(qzx, qzx));                      // wxx qzx, wyy qzx
+  t[12] = mul2(w1, pack2(qyz, qyz));                      // wxx qyz, wyy qyz
+  t[13] = mul2(zz, q3);                                   // wzz qyz, wzz qzx
+  t[14] = mul2(w1, pack2(high_half(q1), low_half(q2)));   // wxx qyy, wyy qzz
+  t[15] = pack2(wzz * low_half(q1), 0.0f);                // wzz qxx
+}
+
 __global__ void __launch_bounds__(kSumThreads) moment_sums_kernel(MixedSumArgs a) {
   const index_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= a.n) return;
   const index_t i = visit(a.order, t);
   const double4 pi = ld4(a.fp, i);
-  float sum[kMonomials], comp[kMonomials];
+  // Kahan sums and compensations, two monomials per register pair
+  f32x2 sum[16], comp[16];
 #pragma unroll
-  for (int e = 0; e < kMonomials; ++e) sum[e] = comp[e] = 0.0f;
+  for (int p = 0; p < 16; ++p) sum[p] = comp[p] = 0ull;
   const index_t fb = a.fo[i], fe = a.fo[i + 1];
   double4 qn = fb < fe ? ld4(a.fp, a.fi[fb]) : pi;
   for (index_t o = fb; o < fe; ++o) {
@@ -604,12 +649,27 @@ __global__ void __launch_bounds__(kSumThreads) moment_sums_kernel(MixedSumArgs a
     const float d2 = sx * sx + sy * sy + sz * sz;
     if (d2 > 0.0f) {
       const float w = 1.0f - sqrtf(d2);
-      if (w > 0.0f) kahan_monomials(sum, comp, sx, sy, sz, w);
+      if (w > 0.0f) {
+        f32x2 tm[16];
+        monomial_pairs(tm, sx, sy, sz, w);
+#pragma unroll
+        for (int p = 0; p < 16; ++p) {
+          const f32x2 y = sub2(tm[p], comp[p]);
+          const f32x2 u = add2(sum[p], y);
+          comp[p] = sub2(sub2(u, sum[p]), y);
+          sum[p] = u;
+        }
+      }
     }
   }
   const size_t n = static_cast<size_t>(a.n);
 #pragma unroll
-  for (int e = 0; e < kMonomials; ++e) a.sums[e * n + t] = static_cast<double>(sum[e]) - static_cast<double>(comp[e]);
+  for (int p = 0; p < 16; ++p) {
+    a.sums[sum_pair_lo(p) * n + t] = static_cast<double>(low_half(sum[p])) - static_cast<double>(low_half(comp[p]));
+    if (sum_pair_hi(p) >= 0)
+      a.sums[sum_pair_hi(p) * n + t] =
+          static_cast<double>(high_half(sum[p])) - static_cast<double>(high_half(comp[p]));
+  }
 }
 
 struct MixedRowArgs {

@@ -30,6 +30,7 @@
 #include <climits>
 #include <cmath>
 
+#include "f32x2.cuh"
 #include "impl.cuh"
 
 namespace lsmps {
@@ -102,21 +103,6 @@ __device__ __forceinline__ float to_rel(double v, double centre, double inv_h) {
   return fabsf(r) <= kFarLimit ? r : __int_as_float(0x7fc00000);  // NaN forces the exact test
 }
 
-// Two FP32 lanes in one 64-bit register (the first in the low half) and the
-// packed FP32 arithmetic of sm_100 on them: one instruction per pair.
-__device__ __forceinline__ unsigned long long pack2(float lo, float hi) {
-  return (static_cast<unsigned long long>(__float_as_uint(hi)) << 32) | __float_as_uint(lo);
-}
-__device__ __forceinline__ unsigned long long sub2(unsigned long long a, unsigned long long b) {
-  unsigned long long d;
-  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-  return d;
-}
-__device__ __forceinline__ unsigned long long fma2(unsigned long long a, unsigned long long b, unsigned long long c) {
-  unsigned long long d;
-  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
-  return d;
-}
 // (acc << 1) | sign bit of the FP32 value in v's low (kHigh: high) half.
 template <bool kHigh>
 __device__ __forceinline__ unsigned shift_in_sign(unsigned acc, unsigned long long v) {
