@@ -71,6 +71,7 @@ extern "C" lsmps_status lsmps_batch_create(int device, int streams, lsmps_batch*
       b->ctxs.push_back(ctx);
       lsmps_ctx_set_stream(ctx, st);
       lsmps_ctx_set_synchronous(ctx, 0);
+      ctx->csr_cell_blocks = true;
     }
   }
   if (!ok) {

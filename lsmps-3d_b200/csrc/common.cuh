@@ -167,6 +167,11 @@ struct lsmps_ctx {
   // the fluid, is used as a visiting order.
   const int32_t* built_order = nullptr;
   size_t built_order_count = 0;
+  // CSR count pass shape: false = warp per home cell, lane per home particle
+  // (the fastest on a GPU the build has to itself); true = block per home
+  // cell, warp per two home particles, which leaves the streams of a batched
+  // graph running beside it faster (set for batch worker contexts).
+  bool csr_cell_blocks = false;
   // 32-byte neighbour records (packed.cuh): two fluid and three wall arrays.
   double4* pack_fluid[2] = {nullptr, nullptr};
   double4* pack_wall[3] = {nullptr, nullptr, nullptr};

@@ -302,6 +302,143 @@ __global__ void __launch_bounds__(kCountWarps * kWarp) csr_count_kernel(CsrArgs 
   }
 }
 
+// The count pass in the shape the batched graphs use (lsmps_ctx::
+// csr_cell_blocks): one block per home cell stages the sequence once as
+// cell-relative FP32 coordinates (candidate index in s_idx), and each warp
+// tests two home particles per staged 32-candidate chunk, one candidate per
+// lane, with ballots into the same accept masks as csr_count_kernel.  The
+// same screen (accept below lo2, FP64 test up to lo2 + band or for NaN).
+__global__ void __launch_bounds__(kCsrThreads) csr_count_cell_kernel(CsrArgs a) {
+  __shared__ float4 s_rel[kStageCap];
+  __shared__ index_t s_idx[kStageCap];
+  __shared__ index_t s_cb[27];
+  __shared__ index_t s_cnt[27];
+  __shared__ index_t s_pre[28];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int dimx = a.grid.dims[0], dimy = a.grid.dims[1], dimz = a.grid.dims[2];
+  const float hi2 = a.lo2 + a.band;
+  for (index_t c = blockIdx.x; c < a.ncell; c += gridDim.x) {
+    const index_t hb = a.home_begin[c];
+    if (hb < 0) continue;  // uniform across the block
+    const index_t he = a.home_end[c];
+    const int cx = c % dimx;
+    const int cy = (c / dimx) % dimy;
+    const int cz = c / (dimx * dimy);
+    if (warp == 0) {  // the 27 source cells and their starts, one warp scan
+      index_t b = -1, n = 0;
+      if (lane < 27) {
+        const int nz = cz + lane / 9 - 1, ny = cy + (lane / 3) % 3 - 1, nx = cx + lane % 3 - 1;
+        if (nz >= 0 && nz < dimz && ny >= 0 && ny < dimy && nx >= 0 && nx < dimx) {
+          const index_t cell = (nz * dimy + ny) * dimx + nx;
+          b = a.src_begin[cell];
+          const index_t e = a.src_end[cell];
+          if (b >= 0 && e >= 0) n = e - b;
+        }
+      }
+      index_t incl = n;
+#pragma unroll
+      for (int d = 1; d < kWarp; d <<= 1) {
+        const index_t t = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= d) incl += t;
+      }
+      if (lane < 27) {
+        s_cb[lane] = b;
+        s_cnt[lane] = n;
+        s_pre[lane] = incl - n;
+      }
+      if (lane == kWarp - 1) s_pre[27] = incl;
+    }
+    __syncthreads();
+    const index_t nc = s_pre[27];
+    const double ccx = a.grid.origin[0] + (cx + 0.5) * a.grid.cell_size;
+    const double ccy = a.grid.origin[1] + (cy + 0.5) * a.grid.cell_size;
+    const double ccz = a.grid.origin[2] + (cz + 0.5) * a.grid.cell_size;
+    if (nc <= kStageCap) {
+      int t = 0;  // each thread's source cell only moves forward
+      for (index_t k = threadIdx.x; k < nc; k += kCsrThreads) {
+        while (s_pre[t + 1] <= k) ++t;
+        const index_t pos = s_cb[t] + (k - s_pre[t]);
+        s_idx[k] = a.src_sorted[pos];
+        const double4 q = a.src_pos[pos];
+        s_rel[k] = make_float4(to_rel(q.x, ccx, a.inv_h), to_rel(q.y, ccy, a.inv_h), to_rel(q.z, ccz, a.inv_h), 0.0f);
+      }
+      __syncthreads();
+      for (index_t h = hb + 2 * warp; h < he; h += 2 * kCsrWarps) {
+        const bool two = h + 1 < he;
+        const index_t i0 = a.home_sorted[h];
+        const index_t i1 = two ? a.home_sorted[h + 1] : i0;
+        const double x0 = a.fx[i0], y0 = a.fy[i0], z0 = a.fz[i0];
+        const double x1 = a.fx[i1], y1 = a.fy[i1], z1 = a.fz[i1];
+        const float r0x = to_rel(x0, ccx, a.inv_h), r0y = to_rel(y0, ccy, a.inv_h), r0z = to_rel(z0, ccz, a.inv_h);
+        const float r1x = to_rel(x1, ccx, a.inv_h), r1y = to_rel(y1, ccy, a.inv_h), r1z = to_rel(z1, ccz, a.inv_h);
+        unsigned keep0 = 0u, keep1 = 0u;  // lane c keeps chunk c's masks
+        index_t count0 = 0, count1 = 0;
+        for (index_t base = 0; base < nc; base += kWarp) {
+          const index_t k = base + lane;
+          bool pass0 = false, pass1 = false;
+          if (k < nc) {
+            const index_t j = s_idx[k];
+            const float4 q = s_rel[k];
+            if (!(a.exclude_self && j == i0)) {
+              const float dx = r0x - q.x, dy = r0y - q.y, dz = r0z - q.z;
+              const float d2 = dx * dx + dy * dy + dz * dz;
+              if (d2 < a.lo2) {
+                pass0 = true;
+              } else if (!(d2 > hi2)) {  // near the boundary, or NaN (outside the window)
+                pass0 = within_radius(x0, y0, z0, a.sx[j], a.sy[j], a.sz[j], a.r2);
+              }
+            }
+            if (two && !(a.exclude_self && j == i1)) {
+              const float dx = r1x - q.x, dy = r1y - q.y, dz = r1z - q.z;
+              const float d2 = dx * dx + dy * dy + dz * dz;
+              if (d2 < a.lo2) {
+                pass1 = true;
+              } else if (!(d2 > hi2)) {
+                pass1 = within_radius(x1, y1, z1, a.sx[j], a.sy[j], a.sz[j], a.r2);
+              }
+            }
+          }
+          const unsigned m0 = __ballot_sync(0xffffffffu, pass0);
+          const unsigned m1 = __ballot_sync(0xffffffffu, pass1);
+          if (lane == base / kWarp) {
+            keep0 = m0;
+            keep1 = m1;
+          }
+          count0 += __popc(m0);
+          count1 += __popc(m1);
+        }
+        const int chunks = static_cast<int>((nc + kWarp - 1) / kWarp);
+        if (lane < chunks) {
+          a.bits[static_cast<size_t>(i0) * kMaskWords + lane] = keep0;
+          if (two) a.bits[static_cast<size_t>(i1) * kMaskWords + lane] = keep1;
+        }
+        if (lane == 0) {
+          a.offsets[i0] = count0;
+          if (two) a.offsets[i1] = count1;
+        }
+      }
+    } else {
+      // More candidates than the stage holds: exact tests from global memory
+      // (count only; the write pass keeps the order).
+      for (index_t h = hb + warp; h < he; h += kCsrWarps) {
+        const index_t i = a.home_sorted[h];
+        const double xi = a.fx[i], yi = a.fy[i], zi = a.fz[i];
+        index_t count = 0;
+        for (int t = 0; t < 27; ++t) {
+          const index_t b0 = s_cb[t], cnt = s_cnt[t];
+          for (index_t k = lane; k < cnt; k += kWarp) {
+            const index_t j = a.src_sorted[b0 + k];
+            if (!(a.exclude_self && j == i) && within_radius(xi, yi, zi, a.sx[j], a.sy[j], a.sz[j], a.r2)) ++count;
+          }
+        }
+        count = warp_sum(count);
+        if (lane == 0) a.offsets[i] = count;
+      }
+    }
+    __syncthreads();
+  }
+}
+
 // Position of the n-th (from 0) set bit of w, n < popc(w): two halving steps
 // down to a byte, then a table of the set-bit positions of every byte.
 __device__ __forceinline__ int nth_set_bit(unsigned w, int n, const unsigned char* nth) {
@@ -502,7 +639,12 @@ lsmps_status one_neighbor_list(lsmps_ctx* ctx, Scratch& scratch, const lsmps_flu
   }
   const int count_blocks = static_cast<int>(
       std::min<long long>(div_up(static_cast<long long>(a.ncell), kCountWarps), static_cast<long long>(ctx->sm_count) * 20));
-  if (n) launch(ctx, csr_count_kernel, dim3(count_blocks), dim3(kCountWarps * kWarp), 0, a);
+  if (n && ctx->csr_cell_blocks)
+    launch(ctx, csr_count_cell_kernel,
+           dim3(static_cast<int>(std::min<long long>(a.ncell, static_cast<long long>(ctx->sm_count) * 16))),
+           dim3(kCsrThreads), 0, a);
+  else if (n)
+    launch(ctx, csr_count_kernel, dim3(count_blocks), dim3(kCountWarps * kWarp), 0, a);
   lsmps_status st = exclusive_scan_i32(ctx, scratch, out.offsets, out.offsets, n, nullptr, out.offsets + n);
   if (st) return st;
   const int blocks = static_cast<int>(std::min<long long>(a.ncell, static_cast<long long>(ctx->sm_count) * 16));
