@@ -503,9 +503,13 @@ __global__ void __launch_bounds__(kThreads) gradient_shifting_kernel(GatherArgs 
   const index_t fe = a.fo[i + 1];
   index_t o = a.fo[i] + l;
   double4 qn = ld4(a.fpp, o < fe ? a.fi[o] : i);
+  index_t jnn = o + G < fe ? a.fi[o + G] : i;  // the index after the next
   for (; o < fe; o += G) {
     const double4 q = qn;
-    if (o + G < fe) qn = ld4(a.fpp, a.fi[o + G]);
+    if (o + G < fe) {
+      qn = ld4(a.fpp, jnn);
+      if (o + 2 * G < fe) jnn = a.fi[o + 2 * G];
+    }
     const double dx = q.x - xi, dy = q.y - yi, dz = q.z - zi;
     const double d = sqrt(dx * dx + dy * dy + dz * dz);
     if (do_grad) {

@@ -506,9 +506,13 @@ __global__ void __launch_bounds__(2 * kWarp, 8) moment_a_split_kernel(MomentPack
     const index_t fe = a.fo[i + 1];
     index_t o = a.fo[i] + half;
     double4 qn = o < fe ? ld4(a.fp, a.fi[o]) : pi;
+    index_t jnn = o + 2 < fe ? a.fi[o + 2] : i;  // the index after the next
     for (; o < fe; o += 2) {
       const double4 q = qn;
-      if (o + 2 < fe) qn = ld4(a.fp, a.fi[o + 2]);
+      if (o + 2 < fe) {
+        qn = ld4(a.fp, jnn);
+        if (o + 4 < fe) jnn = a.fi[o + 4];
+      }
       const double dx = q.x - pi.x, dy = q.y - pi.y, dz = q.z - pi.z;
       const double d2 = dx * dx + dy * dy + dz * dz;
       if (d2 <= 0.0) continue;
@@ -640,9 +644,13 @@ __global__ void __launch_bounds__(kSumThreads) moment_sums_kernel(MixedSumArgs a
   for (int p = 0; p < 16; ++p) sum[p] = comp[p] = 0ull;
   const index_t fb = a.fo[i], fe = a.fo[i + 1];
   double4 qn = fb < fe ? ld4(a.fp, a.fi[fb]) : pi;
+  index_t jnn = fb + 1 < fe ? a.fi[fb + 1] : i;  // the index after the next
   for (index_t o = fb; o < fe; ++o) {
     const double4 q = qn;
-    if (o + 1 < fe) qn = ld4(a.fp, a.fi[o + 1]);
+    if (o + 1 < fe) {
+      qn = ld4(a.fp, jnn);
+      if (o + 2 < fe) jnn = a.fi[o + 2];
+    }
     const float sx = static_cast<float>((q.x - pi.x) * a.inv_re);
     const float sy = static_cast<float>((q.y - pi.y) * a.inv_re);
     const float sz = static_cast<float>((q.z - pi.z) * a.inv_re);

@@ -214,17 +214,20 @@ __global__ void __launch_bounds__(kThreads, 4) ppe_lanes_kernel(PpeArgs a) {
 #pragma unroll
   for (int r = 0; r < 9; ++r) rx[r] = ry[r] = rz[r] = 0.0;
   double diag = 0.0;
-  // Each lane loads its next neighbour's records while it works on this one.
+  // Each lane loads its next neighbour's records, and the index after that,
+  // while it works on this one.
   index_t o = nb + l;
   index_t jn = o < ne ? a.fi[o] : i;
+  index_t jnn = o + G < ne ? a.fi[o + G] : i;
   double4 qn = ld4(a.fp, jn), un = ld4(a.fu, jn);
   for (; o < ne; o += G) {
     const index_t j = jn;
     const double4 q = qn, u = un;
     if (o + G < ne) {
-      jn = a.fi[o + G];
+      jn = jnn;
       qn = ld4(a.fp, jn);
       un = ld4(a.fu, jn);
+      if (o + 2 * G < ne) jnn = a.fi[o + 2 * G];
     }
     const double dx = q.x - xi, dy = q.y - yi, dz = q.z - zi;
     const double w = lin_weight_mul(sqrt(dx * dx + dy * dy + dz * dz), a.inv_re);

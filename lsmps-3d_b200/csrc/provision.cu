@@ -67,7 +67,7 @@ __device__ __forceinline__ double lap_from(const double* __restrict__ inv, const
 // entries l, l + G, ... of both rows and the groups' partial sums are added
 // with shuffles (a rounding-level reassociation for G > 1).
 template <bool Mixed, int G>
-__global__ void __launch_bounds__(kThreads) laplacian_kernel(LaplacianArgs a, MixedRows rows) {
+__global__ void __launch_bounds__(kThreads, 4) laplacian_kernel(LaplacianArgs a, MixedRows rows) {
   const index_t t = (blockIdx.x * blockDim.x + threadIdx.x) / G;
   const int l = threadIdx.x & (G - 1);
   if (t >= a.n) return;  // the whole group
@@ -80,14 +80,17 @@ __global__ void __launch_bounds__(kThreads) laplacian_kernel(LaplacianArgs a, Mi
   const index_t fe = a.fo[i + 1];
   index_t o = a.fo[i] + l;
   index_t jn = o < fe ? a.fi[o] : i;
+  index_t jnn = o + G < fe ? a.fi[o + G] : i;
   double4 qn = ld4(a.fp, jn), un = ld4(a.fv, jn);
   for (; o < fe; o += G) {
-    // the next neighbour's records are loaded while this one is summed
+    // the next neighbour's records, and the index after that, are loaded
+    // while this one is summed
     const double4 q = qn, u = un;
     if (o + G < fe) {
-      jn = a.fi[o + G];
+      jn = jnn;
       qn = ld4(a.fp, jn);
       un = ld4(a.fv, jn);
+      if (o + 2 * G < fe) jnn = a.fi[o + 2 * G];
     }
     const double dx = q.x - pi.x, dy = q.y - pi.y, dz = q.z - pi.z;
     const double w = lin_weight_mul(sqrt(dx * dx + dy * dy + dz * dz), a.inv_re);

@@ -90,9 +90,13 @@ __global__ void __launch_bounds__(kSurfaceThreads) classify_kernel(SurfaceArgs a
   int weighted = 0;
   // the next neighbour's record is loaded while this one is accumulated
   double4 qn = ld4(a.fp, fb < fe ? a.fi[fb] : i);
+  index_t jnn = fb + 1 < fe ? a.fi[fb + 1] : i;  // the index after the next
   for (index_t o = fb; o < fe; ++o) {
     const double4 q = qn;
-    if (o + 1 < fe) qn = ld4(a.fp, a.fi[o + 1]);
+    if (o + 1 < fe) {
+      qn = ld4(a.fp, jnn);
+      if (o + 2 < fe) jnn = a.fi[o + 2];
+    }
     accumulate(q.x - px, q.y - py, q.z - pz, re, nd, sx, sy, sz, weighted);
   }
   if (a.p.include_wall_neighbors) {
