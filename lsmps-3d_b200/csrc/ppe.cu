@@ -200,14 +200,23 @@ __global__ void __launch_bounds__(kThreads, 4) ppe_lanes_kernel(PpeArgs a) {
   }
   const double4 pi = ld4(a.fp, i);
   const double xi = pi.x, yi = pi.y, zi = pi.z;
-  double L[9];
-  if (Mixed) {
-    load_row9(a.prows, i, 0, L);
-  } else {
-    const double* __restrict__ pinv = a.pinv + static_cast<size_t>(i) * 81;
+  // The pressure Laplacian row, once per group in shared memory: read by
+  // broadcast in every neighbour's dot product, it holds no registers.
+  __shared__ double s_L[kThreads / G][9];
+  double* L = s_L[threadIdx.x / G];
+  if (l == 0) {
+    double Lr[9];
+    if (Mixed) {
+      load_row9(a.prows, i, 0, Lr);
+    } else {
+      const double* __restrict__ pinv = a.pinv + static_cast<size_t>(i) * 81;
 #pragma unroll
-    for (int col = 0; col < 9; ++col) L[col] = pinv[3 + col * 9] + pinv[4 + col * 9] + pinv[5 + col * 9];
+      for (int col = 0; col < 9; ++col) Lr[col] = pinv[3 + col * 9] + pinv[4 + col * 9] + pinv[5 + col * 9];
+    }
+#pragma unroll
+    for (int col = 0; col < 9; ++col) L[col] = Lr[col];
   }
+  __syncwarp(group_mask<G>());
   const double uxi = a.tvx[i], uyi = a.tvy[i], uzi = a.tvz[i];
   const double scale = 2.0 / (a.re * a.re * a.density);
   double rx[9], ry[9], rz[9], b[9];
