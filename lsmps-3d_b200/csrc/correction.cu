@@ -460,7 +460,7 @@ namespace {
 // takes row entries l, l + G, ...; the 15 partial sums are combined with
 // shuffles and lane 0 finishes the particle.
 template <bool Mixed, int G>
-__global__ void __launch_bounds__(kThreads) gradient_shifting_kernel(GatherArgs a, double* pressure,
+__global__ void __launch_bounds__(kThreads, 6) gradient_shifting_kernel(GatherArgs a, double* pressure,
                                                                      double* fluid_pressure,
                                                                      const double* __restrict__ pinv,
                                                                      MixedRows prows, double re,

@@ -47,7 +47,7 @@ struct LaplacianArgs {
 // entries l, l + G, ... of both rows and the groups' partial sums are added
 // with shuffles (a rounding-level reassociation for G > 1).
 template <bool Mixed, int G>
-__global__ void __launch_bounds__(kThreads, 4) laplacian_kernel(LaplacianArgs a, MixedRows rows) {
+__global__ void __launch_bounds__(kThreads, 5) laplacian_kernel(LaplacianArgs a, MixedRows rows) {
   const index_t t = (blockIdx.x * blockDim.x + threadIdx.x) / G;
   const int l = threadIdx.x & (G - 1);
   if (t >= a.n) return;  // the whole group
