@@ -76,6 +76,19 @@ __device__ __forceinline__ void acc_rhs(const double b[9], double w, double ux, 
   }
 }
 
+// (Gx . b) ux + (Gy . b) uy + (Gz . b) uz for one neighbour.
+__device__ __forceinline__ double div_term(const double gx[9], const double gy[9], const double gz[9],
+                                           const double b[9], double ux, double uy, double uz) {
+  double cx = 0.0, cy = 0.0, cz = 0.0;
+#pragma unroll
+  for (int r = 0; r < 9; ++r) {
+    cx = fma(gx[r], b[r], cx);
+    cy = fma(gy[r], b[r], cy);
+    cz = fma(gz[r], b[r], cz);
+  }
+  return fma(cx, ux, fma(cy, uy, cz * uz));
+}
+
 __device__ __forceinline__ double coeff_row(const double* __restrict__ inv, const double rhs[9], int row) {
   double c = 0.0;
 #pragma unroll
@@ -219,9 +232,25 @@ __global__ void __launch_bounds__(kThreads, 4) ppe_lanes_kernel(PpeArgs a) {
   __syncwarp(group_mask<G>());
   const double uxi = a.tvx[i], uyi = a.tvy[i], uzi = a.tvz[i];
   const double scale = 2.0 / (a.re * a.re * a.density);
-  double rx[9], ry[9], rz[9], b[9];
+  // The velocity gradient rows (rows 0..2 of the velocity inverse, or the
+  // mixed-form rows 1..3) are applied to each neighbour's basis vector:
+  // sum_j w_j sum_c (G_c . b_j) du_c,j equals sum_c G_c . sum_j w_j b_j du_c,j
+  // up to rounding, with one accumulator instead of 27.
+  double gx[9], gy[9], gz[9], b[9];
+  if (Mixed) {
+    load_row9(a.vrows, i, 1, gx);
+    load_row9(a.vrows, i, 2, gy);
+    load_row9(a.vrows, i, 3, gz);
+  } else {
+    const double* __restrict__ vinv = a.vinv + static_cast<size_t>(i) * 81;
 #pragma unroll
-  for (int r = 0; r < 9; ++r) rx[r] = ry[r] = rz[r] = 0.0;
+    for (int col = 0; col < 9; ++col) {
+      gx[col] = vinv[0 + col * 9];
+      gy[col] = vinv[1 + col * 9];
+      gz[col] = vinv[2 + col * 9];
+    }
+  }
+  double dsum = 0.0;
   double diag = 0.0;
   // Each lane loads its next neighbour's records, and the index after that,
   // while it works on this one.
@@ -245,7 +274,7 @@ __global__ void __launch_bounds__(kThreads, 4) ppe_lanes_kernel(PpeArgs a) {
       basis_a_mul(dx, dy, dz, a.inv_re, b);
       off = w * dot9(L, b) * scale;
       diag -= off;
-      acc_rhs(b, w, u.x - uxi, u.y - uyi, u.z - uzi, rx, ry, rz);
+      dsum = fma(w, div_term(gx, gy, gz, b, u.x - uxi, u.y - uyi, u.z - uzi), dsum);
     }
     a.col[row + 1 + o - nb] = j;
     a.val[row + 1 + o - nb] = off;
@@ -259,7 +288,7 @@ __global__ void __launch_bounds__(kThreads, 4) ppe_lanes_kernel(PpeArgs a) {
     const double bw = lin_weight_mul(sqrt(dx * dx + dy * dy + dz * dz), a.inv_re);
     if (bw <= 0.0) continue;
     basis_a_mul(dx, dy, dz, a.inv_re, b);
-    acc_rhs(b, a.vwall_scale * bw, u.x - uxi, u.y - uyi, u.z - uzi, rx, ry, rz);
+    dsum = fma(a.vwall_scale * bw, div_term(gx, gy, gz, b, u.x - uxi, u.y - uyi, u.z - uzi), dsum);
     const double nx = nrm.x, ny = nrm.y, nz = nrm.z;
     const double ng = a.gx * nx + a.gy * ny + a.gz * nz;
     double qn9[9];
@@ -269,30 +298,9 @@ __global__ void __launch_bounds__(kThreads, 4) ppe_lanes_kernel(PpeArgs a) {
   const unsigned mask = group_mask<G>();
   diag = group_sum<G>(diag, mask);
   wall_rhs = group_sum<G>(wall_rhs, mask);
-#pragma unroll
-  for (int r = 0; r < 9; ++r) {
-    rx[r] = group_sum<G>(rx[r], mask);
-    ry[r] = group_sum<G>(ry[r], mask);
-    rz[r] = group_sum<G>(rz[r], mask);
-  }
+  dsum = group_sum<G>(dsum, mask);
   if (l != 0) return;
-  double div;
-  if (Mixed) {
-    double g[9], c0 = 0.0, c1 = 0.0, c2 = 0.0;
-    load_row9(a.vrows, i, 1, g);
-#pragma unroll
-    for (int col = 0; col < 9; ++col) c0 = fma(g[col], rx[col], c0);
-    load_row9(a.vrows, i, 2, g);
-#pragma unroll
-    for (int col = 0; col < 9; ++col) c1 = fma(g[col], ry[col], c1);
-    load_row9(a.vrows, i, 3, g);
-#pragma unroll
-    for (int col = 0; col < 9; ++col) c2 = fma(g[col], rz[col], c2);
-    div = (c0 + c1 + c2) * a.inv_re;
-  } else {
-    const double* __restrict__ vinv = a.vinv + static_cast<size_t>(i) * 81;
-    div = (coeff_row(vinv, rx, 0) + coeff_row(vinv, ry, 1) + coeff_row(vinv, rz, 2)) * a.inv_re;
-  }
+  const double div = dsum * a.inv_re;
   a.col[row] = i;
   a.val[row] = diag;
   a.divergence[i] = div;
