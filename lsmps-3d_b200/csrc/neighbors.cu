@@ -118,7 +118,9 @@ __device__ __forceinline__ index_t warp_sum(index_t v) {
 // stages its 27-cell candidate sequence (cell-relative FP32 coordinates and
 // the candidate's cell-sorted position) in shared memory, padded to whole
 // 32-candidate chunks with far sentinels and laid out by candidate pairs
-// ({x0, x1, y0, y1}, {z0, z1, pos0, pos1}), so that every lane walks the
+// ({x0, x1, y0, y1} and {z0, z1}: 12 bytes per candidate, so that more warps
+// fit an SM; the rare FP64 test finds a candidate's sorted position from the
+// cell starts), so that every lane walks the
 // sequence with broadcast loads and tests two candidates per packed FP32
 // instruction; the sign of e = d^2 - lo2 is shifted straight into the mask.
 // Bit b of chunk c of a lane's mask is the candidate at sequence position
@@ -127,13 +129,14 @@ __device__ __forceinline__ index_t warp_sum(index_t v) {
 // sequence position (start of the centre cell) + (its sorted position in the
 // home cell) and is cleared after the tests (the reference skips j == i).
 __global__ void __launch_bounds__(kCountWarps * kWarp) csr_count_kernel(CsrArgs a) {
-  __shared__ float4 s_rel[kCountWarps][kStageCap];
+  __shared__ float4 s_xy[kCountWarps][kStageCap / 2];  // pair p: {x_2p, x_2p+1, y_2p, y_2p+1}
+  __shared__ float2 s_z[kCountWarps][kStageCap / 2];   // pair p: {z_2p, z_2p+1}
   __shared__ unsigned s_far[kCountWarps][kMaskWords];  // per chunk: candidates outside the window
   __shared__ index_t s_cb[kCountWarps][27];
   __shared__ index_t s_pre[kCountWarps][28];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  float4* rel = s_rel[w];
-  float* relf = reinterpret_cast<float*>(rel);
+  float4* sxy = s_xy[w];
+  float2* sz = s_z[w];
   unsigned* far = s_far[w];
   index_t* cb = s_cb[w];
   index_t* pre = s_pre[w];
@@ -221,11 +224,10 @@ __global__ void __launch_bounds__(kCountWarps * kWarp) csr_count_kernel(CsrArgs 
             y = to_rel(q[u].y, ccy, a.inv_h);
             z = to_rel(q[u].z, ccz, a.inv_h);
           }
-          float* slot = relf + (k >> 1) * 8 + (k & 1);
-          slot[0] = x;
-          slot[2] = y;
-          slot[4] = z;
-          slot[6] = __int_as_float(static_cast<int>(pos[u]));
+          float* xy = reinterpret_cast<float*>(sxy + (k >> 1)) + (k & 1);
+          xy[0] = x;
+          xy[2] = y;
+          reinterpret_cast<float*>(sz + (k >> 1))[k & 1] = z;
           const unsigned outside = __ballot_sync(0xffffffffu, isnan(x) || isnan(y) || isnan(z));
           if (lane == 0) far[k >> 5] = outside;
         }
@@ -262,13 +264,14 @@ __global__ void __launch_bounds__(kCountWarps * kWarp) csr_count_kernel(CsrArgs 
       const unsigned long long nlo = pack2(-a.lo2, -a.lo2), band = pack2(a.band, a.band);
       index_t count = 0;
       for (int ch = 0; ch < chunks; ++ch) {
-        const ulonglong2* q = reinterpret_cast<const ulonglong2*>(rel + ch * kWarp);
+        const ulonglong2* qxy = reinterpret_cast<const ulonglong2*>(sxy + ch * (kWarp / 2));
+        const unsigned long long* qz = reinterpret_cast<const unsigned long long*>(sz + ch * (kWarp / 2));
         // bit 31 - b: candidate b accepted from FP32 (e < 0) / not rejected (e < band)
         unsigned lo = 0u, near = 0u;
 #pragma unroll
         for (int pr = 0; pr < kWarp / 2; ++pr) {
-          const ulonglong2 xy = q[2 * pr], zp = q[2 * pr + 1];
-          const unsigned long long dx = sub2(rxx, xy.x), dy = sub2(ryy, xy.y), dz = sub2(rzz, zp.x);
+          const ulonglong2 xy = qxy[pr];
+          const unsigned long long dx = sub2(rxx, xy.x), dy = sub2(ryy, xy.y), dz = sub2(rzz, qz[pr]);
           unsigned long long e = fma2(dx, dx, nlo);
           e = fma2(dy, dy, e);
           e = fma2(dz, dz, e);
@@ -283,7 +286,13 @@ __global__ void __launch_bounds__(kCountWarps * kWarp) csr_count_kernel(CsrArgs 
         if (home_far) amb = ~0u;
         for (; amb; amb &= amb - 1) {
           const int bit = __ffs(amb) - 1;
-          const int pos = __float_as_int(relf[ch * kWarp * 4 + (bit >> 1) * 8 + 6 + (bit & 1)]);
+          const index_t k = static_cast<index_t>(ch) * kWarp + bit;
+          index_t pos = -1;
+          if (k < nc) {
+            int t = 0;
+            while (pre[t + 1] <= k) ++t;
+            pos = cb[t] + (k - pre[t]);
+          }
           bool in = false;
           if (pos >= 0) {
             const double4 sp = a.src_pos[pos];
