@@ -25,7 +25,6 @@ namespace lsmps {
 namespace {
 
 constexpr int kMomentThreads = 64;
-constexpr int kMaxKinds = 3;
 
 __host__ __device__ constexpr int tri(int r, int c) { return r * (r + 1) / 2 + c; }
 
