@@ -175,10 +175,16 @@ def test_forward_and_adjoint_match_fp64_autograd(pkg, device_api):
     vr = [torch.from_numpy(a.copy()).requires_grad_(True) for a in v_np]
     ref = torch_operators(xr, fr, vr, ops.off, ops.idx, ops.p)
     assert np.array_equal(out["ppe_row_offsets"].cpu().numpy()[:-1], (np.arange(ops.n) + ops.off[:-1]))
+    # v is divergence-free (each component is constant along its own axis), so
+    # the divergence and the PPE rhs are discretization noise about 1e-3 of
+    # the velocity-gradient scale 2 pi / L; their errors are measured against
+    # that scale, the others against their own maximum.
+    grad_scale = 2.0 * np.pi / (64 * case.l0)
+    floor = {"divergence": grad_scale, "ppe_rhs": grad_scale / ops.p.time_step}
     for k, r in ref.items():
         g = out[k].cpu().numpy()
         rn = r.detach().numpy()
-        err = np.max(np.abs(g - rn)) / max(np.max(np.abs(rn)), 1e-300)
+        err = np.max(np.abs(g - rn)) / max(np.max(np.abs(rn)), floor.get(k, 0.0), 1e-300)
         print(f"\nforward {k}: {err:.2e}")
         assert err < FORWARD_RTOL, (k, err)
     loss = sum((cot[k].cpu() * r).sum() for k, r in ref.items())
