@@ -82,8 +82,12 @@ __global__ void __launch_bounds__(kScanThreads) hist_scan_kernel(index_t* __rest
 }
 
 // Per-device set-up, done once under the device's lock: the address of
-// g_scratch on that device (looking it up makes the runtime load this file's
-// device code there) and the SM count for the grid sizes.
+// g_scratch on that device and the SM count for the grid sizes.  Each .cu
+// file of the library is its own device module, and under lazy module loading
+// (the CUDA runtime's default) a module is loaded on first use, which can
+// allocate device memory.  Looking up g_scratch loads this file's module;
+// querying the attributes of the sort kernels compiled in cells.cu loads
+// that module too, so that no later call (count = 0 included) loads code.
 constexpr int kMaxDevices = 64;
 struct DeviceSlot {
   std::mutex lock;
@@ -96,6 +100,15 @@ lsmps_status set_up(DeviceSlot& slot, int device) {
   if (slot.scratch) return LSMPS_OK;
   void* p = nullptr;
   if (cudaGetSymbolAddress(&p, g_scratch) != cudaSuccess || !p) return LSMPS_CUDA_ERROR;
+  const void* kernels[] = {reinterpret_cast<const void*>(hash_kernel),
+                           reinterpret_cast<const void*>(radix_hist_kernel),
+                           reinterpret_cast<const void*>(radix_scatter_kernel),
+                           reinterpret_cast<const void*>(ranges_kernel),
+                           reinterpret_cast<const void*>(hist_scan_kernel)};
+  for (const void* k : kernels) {
+    cudaFuncAttributes attr;
+    if (cudaFuncGetAttributes(&attr, k) != cudaSuccess) return LSMPS_CUDA_ERROR;
+  }
   int sms = 0;
   if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess || sms <= 0)
     return LSMPS_CUDA_ERROR;
@@ -125,6 +138,9 @@ extern "C" lsmps_status lsmps_build_cell_list_noalloc(void* stream_handle, const
       (count && (!cells->cell_ids || !cells->sorted_indices || !x || !y || !z)))
     return LSMPS_INVALID_ARGUMENT;
 
+  // An error left pending by earlier work of the caller is not this call's:
+  // report it without clearing it and without queuing anything.
+  if (cudaPeekAtLastError() != cudaSuccess) return LSMPS_CUDA_ERROR;
   int device = 0;
   if (cudaGetDevice(&device) != cudaSuccess) return LSMPS_CUDA_ERROR;
   if (device < 0 || device >= kMaxDevices) return LSMPS_INVALID_ARGUMENT;
@@ -167,11 +183,13 @@ extern "C" lsmps_status lsmps_build_cell_list_noalloc(void* stream_handle, const
     const int range_blocks = static_cast<int>(std::min<long long>(div_up(n, 256), slot.sm_count * 8LL));
     ranges_kernel<<<range_blocks, 256, 0, stream>>>(cells->cell_ids, n, cells->cell_begin, cells->cell_end);
   }
-  if (cudaGetLastError() != cudaSuccess) return LSMPS_CUDA_ERROR;
   DeviceStatus h{};
-  if (cudaMemcpyAsync(&h, status, sizeof(DeviceStatus), cudaMemcpyDeviceToHost, stream) != cudaSuccess)
-    return LSMPS_CUDA_ERROR;
-  if (cudaStreamSynchronize(stream) != cudaSuccess) return LSMPS_CUDA_ERROR;
+  bool failed = cudaGetLastError() != cudaSuccess;
+  if (!failed)
+    failed = cudaMemcpyAsync(&h, status, sizeof(DeviceStatus), cudaMemcpyDeviceToHost, stream) != cudaSuccess;
+  // Always wait for what was queued before the lock is released: the next
+  // call on this device reuses the same scratch.
+  if (cudaStreamSynchronize(stream) != cudaSuccess || failed) return LSMPS_CUDA_ERROR;
   if (h.flags & kFlagNonFinite) return LSMPS_NON_FINITE;
   return LSMPS_OK;
 }
