@@ -368,9 +368,13 @@ lsmps_status lsmps_build_cell_list(lsmps_ctx* ctx, const double* x, const double
  *   cudaStream_t; NULL is the legacy default stream), and waits for it before
  *   returning.  A NaN or infinite coordinate returns LSMPS_NON_FINITE.
  * - The first call on a device does its set-up: it looks up the scratch
- *   array's device address, which makes the CUDA runtime load the library's
- *   device code on that device.  Make that first call before capturing any
- *   stream.
+ *   array's device address and loads the device code of the sort kernels on
+ *   that device (the CUDA runtime loads code lazily by default, and loading
+ *   can allocate), so later calls load nothing.  Make that first call (any
+ *   count, 0 included) before capturing any stream.
+ * - An error already pending on the calling thread (from earlier CUDA work)
+ *   is reported as LSMPS_CUDA_ERROR without being cleared and without any
+ *   device work queued.
  * - Nothing has to be zeroed beforehand: each call clears its own status
  *   word and writes every scratch entry before reading it.
  * - There is one scratch array per device, so two calls in flight at once on
@@ -687,6 +691,15 @@ lsmps_status lsmps_operators_backward(lsmps_ctx* ctx, const lsmps_fluid* fluid, 
                                       const lsmps_params* params, const double* f, const lsmps_vector* v,
                                       const lsmps_operator_out* cotangent, const double* inverse, double* f_bar,
                                       const lsmps_vector* v_bar, const lsmps_vector* x_bar);
+/* Form of lsmps_operators_backward (no counterpart in the reference).
+ * 0 (default): deterministic -- the CSR is transposed (entries sorted stably
+ * by neighbour) and every particle gathers the terms of its own row and of
+ * the rows that list it in a fixed order, with no atomics; repeated calls give
+ * the same bits.  Costs a sort of the K entries and 20 bytes of scratch per
+ * entry.  1: each row scatters its terms into its neighbours with FP64
+ * atomics (no transpose; the sums' order, and so the last bits, may vary
+ * between calls). */
+lsmps_status lsmps_ctx_set_adjoint_atomic(lsmps_ctx* ctx, int on);
 
 #ifdef __cplusplus
 }

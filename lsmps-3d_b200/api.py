@@ -110,6 +110,11 @@ class Context:
         """lsmps_step visits the fluid in cell order (default) or index order."""
         self.check(_lib.lsmps_ctx_set_cell_order(self.h, 1 if on else 0))
 
+    def set_adjoint_atomic(self, on: bool) -> None:
+        """Operator backward: scatter with FP64 atomics (True) or the
+        deterministic transpose + gather (False, the default)."""
+        self.check(_lib.lsmps_ctx_set_adjoint_atomic(self.h, 1 if on else 0))
+
     def set_condition_threshold(self, threshold: float) -> None:
         """Mixed form: condition estimate above which a moment matrix is
         factorised in FP64 (default 1e4)."""

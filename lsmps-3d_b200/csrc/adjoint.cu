@@ -31,8 +31,19 @@
 //
 // The backward recomputes M_i^-1 from the positions (no stored inverse is
 // needed) unless the caller passes the inverse the forward wrote.
-// Scatter to neighbours uses FP64 atomics (result order-dependent at the
-// rounding level).
+//
+// Each CSR entry (i, j) contributes to the cotangents of both its owner i and
+// its neighbour j.  The default backward is deterministic: after the
+// per-particle stash pass it builds the transpose of the CSR (entries sorted
+// stably by neighbour, so each particle's incoming entries are in ascending
+// entry order) and every particle gathers its own row's terms and its
+// incoming entries' terms in a fixed order, with no atomics: repeated runs
+// give the same bits.  lsmps_ctx_set_adjoint_atomic(ctx, 1) selects the
+// scatter form instead (FP64 atomics into the neighbours; no transpose, but
+// the result depends on the atomics' order at the rounding level).
+#include <algorithm>
+
+#include "cells.cuh"
 #include "impl.cuh"
 #include "packed.cuh"
 
@@ -251,76 +262,116 @@ __global__ void __launch_bounds__(kThreads) ops_adjoint_rows_kernel(OpsArgs a) {
   st[91] = trace > 0.0 ? 1.0 : 0.0;
 }
 
+// Terms of one CSR entry of owner i (stash st, position pi, field values
+// phii) with neighbour j: tphi[p] is added to phibar_p[j] and taken from
+// phibar_p[i], g is added to xbar[j] and taken from xbar[i].  ab is the
+// entry's PPE cotangent (c (abar_ij - abar_ii)), rho_reg the owner's
+// regularisation factor.  False for an entry with zero weight or distance.
+__device__ __forceinline__ bool pair_terms(const OpsArgs& a, const double* __restrict__ st, const double4& pi,
+                                           const double phii[4], index_t j, double ab, double rho_reg,
+                                           double tphi[4], double g[3]) {
+  const double4 q = ld4(a.fp, j);
+  const double dx = q.x - pi.x, dy = q.y - pi.y, dz = q.z - pi.z;
+  const double dist = sqrt(dx * dx + dy * dy + dz * dz);
+  const double w = lin_weight(dist, a.re);
+  if (w <= 0.0 || dist <= 0.0) return false;
+  double b[9], s[3], beta[9];
+  basis_div(dx, dy, dz, a.inv_re, b, s);
+  double alpha = 0.0;
+#pragma unroll
+  for (int k = 0; k < 9; ++k) beta[k] = 0.0;
+  const double* phi[4] = {a.f, a.vx, a.vy, a.vz};
+#pragma unroll
+  for (int p = 0; p < 4; ++p) {
+    const double* rb = st + 9 * p;
+    const double* y = st + 36 + 9 * p;
+    const double rbb = dot9(rb, b);
+    const double e = (phi[p][j] - phii[p]) - dot9(b, y);
+    alpha = fma(rbb, e, alpha);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) beta[k] = fma(w, rb[k] * e - rbb * y[k], beta[k]);
+    tphi[p] = w * rbb;
+  }
+  if (a.bar.ppe_values != nullptr) {
+    const double* hh = st + 72;
+    const double* l = st + 81;
+    const double lb = dot9(l, b), hb = dot9(hh, b);
+    alpha += ab * lb - hb * lb;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) beta[k] += ab * w * l[k] - w * (lb * hh[k] + hb * l[k]);
+  }
+  if (rho_reg != 0.0) {
+    alpha -= rho_reg * dot9(b, b);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) beta[k] -= rho_reg * 2.0 * w * b[k];
+  }
+  // dL/dd = (-alpha d/|d| + J_b(s)^T beta) / r_e
+  const double inv_d = 1.0 / dist;
+  g[0] = (-alpha * dx * inv_d + beta[0] + 2.0 * s[0] * beta[3] + s[1] * beta[6] + s[2] * beta[8]) * a.inv_re;
+  g[1] = (-alpha * dy * inv_d + beta[1] + 2.0 * s[1] * beta[4] + s[0] * beta[6] + s[2] * beta[7]) * a.inv_re;
+  g[2] = (-alpha * dz * inv_d + beta[2] + 2.0 * s[2] * beta[5] + s[1] * beta[7] + s[0] * beta[8]) * a.inv_re;
+  return true;
+}
+
+// The owner-side quantities of particle i that pair_terms needs.
+struct OwnerTerms {
+  double4 pi;
+  const double* st;
+  double phii[4];
+  index_t nb;
+  index_t row;
+  double diag_bar;
+  double rho_reg;
+};
+
+__device__ __forceinline__ OwnerTerms owner_terms(const OpsArgs& a, index_t i) {
+  OwnerTerms t;
+  t.pi = ld4(a.fp, i);
+  t.st = a.stash + static_cast<size_t>(i) * kStash;
+  t.phii[0] = a.f[i];
+  t.phii[1] = a.vx[i];
+  t.phii[2] = a.vy[i];
+  t.phii[3] = a.vz[i];
+  t.nb = a.fo[i];
+  t.row = i + t.nb;
+  t.diag_bar = a.bar.ppe_values != nullptr ? a.bar.ppe_values[t.row] : 0.0;
+  t.rho_reg = t.st[91] != 0.0 ? t.st[90] * a.lambda / 9.0 : 0.0;
+  return t;
+}
+
+// PPE cotangent of entry o of the owner's row.
+__device__ __forceinline__ double entry_ab(const OpsArgs& a, const OwnerTerms& t, index_t o) {
+  return a.bar.ppe_values != nullptr ? a.ppe_scale * (a.bar.ppe_values[t.row + 1 + o - t.nb] - t.diag_bar) : 0.0;
+}
+
+// Scatter form (lsmps_ctx_set_adjoint_atomic): each owner adds its entries'
+// terms into its neighbours with FP64 atomics.
 __global__ void __launch_bounds__(kThreads) ops_adjoint_scatter_kernel(OpsArgs a) {
   const index_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= a.n) return;
-  const double4 pi = ld4(a.fp, i);
-  const double* __restrict__ st = a.stash + static_cast<size_t>(i) * kStash;
-  const double* phi[4] = {a.f, a.vx, a.vy, a.vz};
+  const OwnerTerms t = owner_terms(a, i);
   double* phibar[4] = {a.fbar, a.vbar[0], a.vbar[1], a.vbar[2]};
-  const double phii[4] = {a.f[i], a.vx[i], a.vy[i], a.vz[i]};
-  const bool ppe = a.bar.ppe_values != nullptr;
-  const index_t nb = a.fo[i], ne = a.fo[i + 1];
-  const index_t row = i + nb;
-  const double diag_bar = ppe ? a.bar.ppe_values[row] : 0.0;
-  const double rho_reg = st[91] != 0.0 ? st[90] * a.lambda / 9.0 : 0.0;
+  const index_t ne = a.fo[i + 1];
   double own_x = 0.0, own_y = 0.0, own_z = 0.0;
   double own_phi[4] = {0.0, 0.0, 0.0, 0.0};
-  double b[9], s[3], beta[9];
-  for (index_t o = nb; o < ne; ++o) {
+  for (index_t o = t.nb; o < ne; ++o) {
     const index_t j = a.fi[o];
-    const double4 q = ld4(a.fp, j);
-    const double dx = q.x - pi.x, dy = q.y - pi.y, dz = q.z - pi.z;
-    const double dist = sqrt(dx * dx + dy * dy + dz * dz);
-    const double w = lin_weight(dist, a.re);
-    if (w <= 0.0 || dist <= 0.0) continue;
-    basis_div(dx, dy, dz, a.inv_re, b, s);
-    double alpha = 0.0;
+    double tphi[4], g[3];
+    if (!pair_terms(a, t.st, t.pi, t.phii, j, entry_ab(a, t, o), t.rho_reg, tphi, g)) continue;
 #pragma unroll
-    for (int k = 0; k < 9; ++k) beta[k] = 0.0;
-#pragma unroll
-    for (int p = 0; p < 4; ++p) {
-      const double* rb = st + 9 * p;
-      const double* y = st + 36 + 9 * p;
-      const double rbb = dot9(rb, b);
-      const double e = (phi[p][j] - phii[p]) - dot9(b, y);
-      alpha = fma(rbb, e, alpha);
-#pragma unroll
-      for (int k = 0; k < 9; ++k) beta[k] = fma(w, rb[k] * e - rbb * y[k], beta[k]);
-      // field cotangents
-      const double tphi = w * rbb;
+    for (int p = 0; p < 4; ++p)
       if (phibar[p]) {
-        atomicAdd(&phibar[p][j], tphi);
-        own_phi[p] -= tphi;
+        atomicAdd(&phibar[p][j], tphi[p]);
+        own_phi[p] -= tphi[p];
       }
-    }
-    if (ppe) {
-      const double* hh = st + 72;
-      const double* l = st + 81;
-      const double ab = a.ppe_scale * (a.bar.ppe_values[row + 1 + o - nb] - diag_bar);
-      const double lb = dot9(l, b), hb = dot9(hh, b);
-      alpha += ab * lb - hb * lb;
-#pragma unroll
-      for (int k = 0; k < 9; ++k) beta[k] += ab * w * l[k] - w * (lb * hh[k] + hb * l[k]);
-    }
-    if (rho_reg != 0.0) {
-      alpha -= rho_reg * dot9(b, b);
-#pragma unroll
-      for (int k = 0; k < 9; ++k) beta[k] -= rho_reg * 2.0 * w * b[k];
-    }
-    // dL/dd = (-alpha d/|d| + J_b(s)^T beta) / r_e
-    const double inv_d = 1.0 / dist;
-    const double gx = (-alpha * dx * inv_d + beta[0] + 2.0 * s[0] * beta[3] + s[1] * beta[6] + s[2] * beta[8]) * a.inv_re;
-    const double gy = (-alpha * dy * inv_d + beta[1] + 2.0 * s[1] * beta[4] + s[0] * beta[6] + s[2] * beta[7]) * a.inv_re;
-    const double gz = (-alpha * dz * inv_d + beta[2] + 2.0 * s[2] * beta[5] + s[1] * beta[7] + s[0] * beta[8]) * a.inv_re;
     if (a.xbar[0]) {
-      atomicAdd(&a.xbar[0][j], gx);
-      atomicAdd(&a.xbar[1][j], gy);
-      atomicAdd(&a.xbar[2][j], gz);
+      atomicAdd(&a.xbar[0][j], g[0]);
+      atomicAdd(&a.xbar[1][j], g[1]);
+      atomicAdd(&a.xbar[2][j], g[2]);
     }
-    own_x -= gx;
-    own_y -= gy;
-    own_z -= gz;
+    own_x -= g[0];
+    own_y -= g[1];
+    own_z -= g[2];
   }
   if (a.xbar[0]) {
     atomicAdd(&a.xbar[0][i], own_x);
@@ -330,6 +381,74 @@ __global__ void __launch_bounds__(kThreads) ops_adjoint_scatter_kernel(OpsArgs a
 #pragma unroll
   for (int p = 0; p < 4; ++p)
     if (phibar[p]) atomicAdd(&phibar[p][i], own_phi[p]);
+}
+
+// Transpose of the CSR, step 1: for every entry o of row i, key = its
+// neighbour (indices outside [0, n) become the sentinel n), value = o, and
+// owner[o] = i.  Eight lanes per row.
+__global__ void __launch_bounds__(kThreads) transpose_keys_kernel(const index_t* __restrict__ fo,
+                                                                  const index_t* __restrict__ fi, index_t n,
+                                                                  index_t* __restrict__ keys,
+                                                                  index_t* __restrict__ vals,
+                                                                  index_t* __restrict__ owner) {
+  const index_t i = static_cast<index_t>((static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x) / 8);
+  const int lane = threadIdx.x & 7;
+  if (i >= n) return;
+  const index_t ne = fo[i + 1];
+  for (index_t o = fo[i] + lane; o < ne; o += 8) {
+    const index_t j = fi[o];
+    keys[o] = (j >= 0 && j < n) ? j : n;
+    vals[o] = o;
+    owner[o] = i;
+  }
+}
+
+// Deterministic form: particle j sums, in a fixed order, the terms of its
+// incoming entries (the transpose row [tb[j], te[j]) of entry offsets,
+// ascending) and then subtracts those of its own row, and writes its
+// cotangents (no atomics, no accumulation into the outputs).
+__global__ void __launch_bounds__(kThreads) ops_adjoint_gather_kernel(OpsArgs a, const index_t* __restrict__ tb,
+                                                                      const index_t* __restrict__ te,
+                                                                      const index_t* __restrict__ tsrc,
+                                                                      const index_t* __restrict__ owner) {
+  const index_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= a.n) return;
+  double acc_phi[4] = {0.0, 0.0, 0.0, 0.0};
+  double acc_x = 0.0, acc_y = 0.0, acc_z = 0.0;
+  const index_t b0 = tb[j], e0 = te[j];
+  if (b0 >= 0) {
+    for (index_t k = b0; k < e0; ++k) {
+      const index_t o = tsrc[k];
+      const OwnerTerms t = owner_terms(a, owner[o]);
+      double tphi[4], g[3];
+      if (!pair_terms(a, t.st, t.pi, t.phii, j, entry_ab(a, t, o), t.rho_reg, tphi, g)) continue;
+#pragma unroll
+      for (int p = 0; p < 4; ++p) acc_phi[p] += tphi[p];
+      acc_x += g[0];
+      acc_y += g[1];
+      acc_z += g[2];
+    }
+  }
+  const OwnerTerms t = owner_terms(a, j);
+  const index_t ne = a.fo[j + 1];
+  for (index_t o = t.nb; o < ne; ++o) {
+    double tphi[4], g[3];
+    if (!pair_terms(a, t.st, t.pi, t.phii, a.fi[o], entry_ab(a, t, o), t.rho_reg, tphi, g)) continue;
+#pragma unroll
+    for (int p = 0; p < 4; ++p) acc_phi[p] -= tphi[p];
+    acc_x -= g[0];
+    acc_y -= g[1];
+    acc_z -= g[2];
+  }
+  double* phibar[4] = {a.fbar, a.vbar[0], a.vbar[1], a.vbar[2]};
+#pragma unroll
+  for (int p = 0; p < 4; ++p)
+    if (phibar[p]) phibar[p][j] = acc_phi[p];
+  if (a.xbar[0]) {
+    a.xbar[0][j] = acc_x;
+    a.xbar[1][j] = acc_y;
+    a.xbar[2][j] = acc_z;
+  }
 }
 
 }  // namespace
@@ -406,6 +525,67 @@ lsmps_status moments(lsmps_ctx* ctx, const lsmps_fluid& fl, const lsmps_csr& fn,
   return st;
 }
 
+// The deterministic backward after the stash pass: the CSR's transpose by a
+// stable radix sort of the entries by neighbour (cells.cuh), its row ranges,
+// then the gather.  Reads the entry count back to size the sort (the call
+// allocates its scratch, so it is not made under stream capture anyway).
+lsmps_status transpose_and_gather(lsmps_ctx* ctx, const lsmps_csr& fn, const OpsArgs& a) {
+  const index_t n = a.n;
+  index_t total = 0;
+  if (cudaMemcpyAsync(&total, fn.offsets + n, sizeof(index_t), cudaMemcpyDeviceToHost, ctx->stream) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+    return fail(ctx, LSMPS_CUDA_ERROR, "reading the neighbour count failed");
+  if (total < 0 || static_cast<size_t>(total) > fn.neighbor_count)
+    return fail(ctx, LSMPS_INVALID_ARGUMENT, "neighbour table offsets exceed its capacity");
+  const size_t k = static_cast<size_t>(total);
+  const int tiles = total ? div_up(total, kSortTile) : 0;
+  const size_t hist_entries = static_cast<size_t>(tiles) * kRadixBins;
+  Scratch scratch(ctx);
+  const size_t bytes = 5 * (k * sizeof(index_t) + 256) + 2 * ((n + 1) * sizeof(index_t) + 256) +
+                       hist_entries * sizeof(index_t) + 256 + 4 * scan_scratch_bytes(hist_entries + 1) + 4096;
+  if (!scratch.reserve(bytes)) return fail(ctx, LSMPS_CUDA_ERROR, "adjoint transpose scratch allocation failed");
+  index_t* keys = scratch.take<index_t>(k + 1);
+  index_t* vals = scratch.take<index_t>(k + 1);
+  index_t* alt_keys = scratch.take<index_t>(k + 1);
+  index_t* alt_vals = scratch.take<index_t>(k + 1);
+  index_t* owner = scratch.take<index_t>(k + 1);
+  index_t* tb = scratch.take<index_t>(static_cast<size_t>(n) + 1);
+  index_t* te = scratch.take<index_t>(static_cast<size_t>(n) + 1);
+  index_t* hist = scratch.take<index_t>(hist_entries + 1);
+  if (!keys || !vals || !alt_keys || !alt_vals || !owner || !tb || !te || !hist)
+    return fail(ctx, LSMPS_CUDA_ERROR, "adjoint transpose scratch exhausted");
+  cudaMemsetAsync(tb, 0xff, (static_cast<size_t>(n) + 1) * sizeof(index_t), ctx->stream);
+  cudaMemsetAsync(te, 0xff, (static_cast<size_t>(n) + 1) * sizeof(index_t), ctx->stream);
+  if (total > 0) {
+    launch(ctx, transpose_keys_kernel, dim3(div_up(static_cast<long long>(n) * 8, kThreads)), dim3(kThreads), 0,
+           a.fo, a.fi, n, keys, vals, owner);
+    const int passes = (key_bits(static_cast<long long>(n) + 1) + kRadixBits - 1) / kRadixBits;
+    index_t *k0 = keys, *v0 = vals, *k1 = alt_keys, *v1 = alt_vals;
+    for (int p = 0; p < passes; ++p) {
+      const int shift = p * kRadixBits;
+      launch(ctx, radix_hist_kernel, dim3(tiles), dim3(kSortThreads), 0, static_cast<const index_t*>(k0), total,
+             shift, hist, tiles);
+      lsmps_status st = exclusive_scan_i32(ctx, scratch, hist, hist, hist_entries, nullptr, nullptr);
+      if (st) return st;
+      launch(ctx, radix_scatter_kernel, dim3(tiles), dim3(kSortThreads), 0, static_cast<const index_t*>(k0),
+             static_cast<const index_t*>(v0), k1, v1, total, shift, static_cast<const index_t*>(hist), tiles);
+      std::swap(k0, k1);
+      std::swap(v0, v1);
+    }
+    const int range_blocks = static_cast<int>(std::min<long long>(div_up(total, 256), ctx->sm_count * 8LL));
+    launch(ctx, ranges_kernel, dim3(range_blocks), dim3(256), 0, static_cast<const index_t*>(k0), total, tb, te);
+    launch(ctx, ops_adjoint_gather_kernel, dim3(div_up(n, kThreads)), dim3(kThreads), 0, a,
+           static_cast<const index_t*>(tb), static_cast<const index_t*>(te), static_cast<const index_t*>(v0),
+           static_cast<const index_t*>(owner));
+  } else {
+    launch(ctx, ops_adjoint_gather_kernel, dim3(div_up(n, kThreads)), dim3(kThreads), 0, a,
+           static_cast<const index_t*>(tb), static_cast<const index_t*>(te), static_cast<const index_t*>(vals),
+           static_cast<const index_t*>(owner));
+  }
+  return check_launch(ctx, "operators backward (transpose and gather)");
+}
+
 OpsArgs make_args(lsmps_ctx* ctx, const lsmps_fluid& fl, const lsmps_csr& fn, const lsmps_params& p, const double* f,
                   const lsmps_vector& v, const double* inverse) {
   OpsArgs a{};
@@ -471,15 +651,18 @@ extern "C" lsmps_status lsmps_operators_backward(lsmps_ctx* ctx, const lsmps_flu
     st = fail(ctx, LSMPS_CUDA_ERROR, "operator scratch allocation failed");
   if (st) return end_call(ctx, st);
   const size_t n = fluid->count;
-  // Gradients are accumulated: start from zero.
-  if (f_bar) cudaMemsetAsync(f_bar, 0, n * sizeof(double), ctx->stream);
-  const lsmps_vector* outs[2] = {v_bar, x_bar};
-  for (const lsmps_vector* o : outs)
-    if (o) {
-      cudaMemsetAsync(o->x, 0, n * sizeof(double), ctx->stream);
-      cudaMemsetAsync(o->y, 0, n * sizeof(double), ctx->stream);
-      cudaMemsetAsync(o->z, 0, n * sizeof(double), ctx->stream);
-    }
+  const bool atomic = ctx->adjoint_atomic;
+  if (atomic) {
+    // The scatter form accumulates into the gradients: start from zero.
+    if (f_bar) cudaMemsetAsync(f_bar, 0, n * sizeof(double), ctx->stream);
+    const lsmps_vector* outs[2] = {v_bar, x_bar};
+    for (const lsmps_vector* o : outs)
+      if (o) {
+        cudaMemsetAsync(o->x, 0, n * sizeof(double), ctx->stream);
+        cudaMemsetAsync(o->y, 0, n * sizeof(double), ctx->stream);
+        cudaMemsetAsync(o->z, 0, n * sizeof(double), ctx->stream);
+      }
+  }
   // The inverse is recomputed from the positions unless the caller kept the
   // forward's.
   if (!inverse) {
@@ -497,6 +680,17 @@ extern "C" lsmps_status lsmps_operators_backward(lsmps_ctx* ctx, const lsmps_flu
   a.xbar[1] = x_bar ? x_bar->y : nullptr;
   a.xbar[2] = x_bar ? x_bar->z : nullptr;
   launch(ctx, ops_adjoint_rows_kernel, dim3(div_up(a.n, kThreads)), dim3(kThreads), 0, a);
-  launch(ctx, ops_adjoint_scatter_kernel, dim3(div_up(a.n, kThreads)), dim3(kThreads), 0, a);
+  if (atomic) {
+    launch(ctx, ops_adjoint_scatter_kernel, dim3(div_up(a.n, kThreads)), dim3(kThreads), 0, a);
+  } else {
+    st = transpose_and_gather(ctx, *fn, a);
+    if (st) return end_call(ctx, st);
+  }
   return end_call(ctx, check_launch(ctx, "operators backward"));
+}
+
+extern "C" lsmps_status lsmps_ctx_set_adjoint_atomic(lsmps_ctx* ctx, int on) {
+  if (!ctx || (on != 0 && on != 1)) return LSMPS_INVALID_ARGUMENT;
+  ctx->adjoint_atomic = on != 0;
+  return LSMPS_OK;
 }

@@ -4,6 +4,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <cstdint>
 #include <cstdio>
@@ -199,6 +200,9 @@ struct lsmps_ctx {
   int32_t* adj_count = nullptr;
   double* adj_stash = nullptr;
   size_t adj_cap = 0;
+  // Backward form: false = transpose + gather (deterministic, the default),
+  // true = scatter with FP64 atomics (lsmps_ctx_set_adjoint_atomic).
+  bool adjoint_atomic = false;
 };
 
 namespace lsmps {
@@ -256,6 +260,16 @@ inline void launch_named(lsmps_ctx* ctx, const char* name, Kernel kernel, dim3 g
 }
 
 #define launch(ctx, kernel, ...) launch_named(ctx, #kernel, kernel, __VA_ARGS__)
+
+// NVTX range for the host-side span of one stage (what a timeline profiler
+// shows as the stage's launch window).  NVTX is header-only: with no tool
+// attached a push/pop costs a few nanoseconds.
+struct StageRange {
+  explicit StageRange(const char* name) { nvtxRangePushA(name); }
+  ~StageRange() { nvtxRangePop(); }
+  StageRange(const StageRange&) = delete;
+  StageRange& operator=(const StageRange&) = delete;
+};
 
 // Scan helpers (scan.cu).  Exclusive scan of n int32 values into out (may
 // alias in); values and partial sums are accumulated in 64 bits and any

@@ -252,3 +252,71 @@ def test_adjoint_against_finite_differences_64cubed(pkg, device_api):
             assert abs(fd - ad) <= FD_RTOL * max(abs(ad), 1e-3 * float(bar.abs().max())), (name, int(k), fd, ad)
     print(f"\nfinite differences: {checked} particles x 3 coordinates, worst relative error {worst:.2e}")
     assert checked >= 48
+
+
+def test_forward_is_bitwise_reproducible(pkg, device_api):
+    """The forward (and the fluid-only inverse it builds) has no atomics and
+    no reduction across threads: repeated calls on the same inputs must give
+    the same bits.  The torch FP64 restatement on the CPU is run twice as
+    well and its repeatability reported."""
+    import torch
+
+    case = pkg.cases.lattice_box(n=12, l0=0.01)
+    ops = Operators(pkg, device_api, case)
+    f_np, v_np = fields(pkg, case)
+    x = [torch.from_numpy(case.fluid[k].copy()).cuda() for k in ("x", "y", "z")]
+    f = torch.from_numpy(f_np).cuda()
+    v = [torch.from_numpy(a.copy()).cuda() for a in v_np]
+    runs = []
+    for _ in range(5):
+        out = ops.alloc_out()
+        inv = torch.full((ops.n * 81,), float("nan"), dtype=torch.float64, device="cuda")
+        st = ops.lib.lsmps_operators_forward(ops.ctx.h, ctypes.byref(ops._fluid(x)),
+                                             ctypes.byref(ops.dev.csr_view("fluid")), ctypes.byref(ops.p),
+                                             ctypes.c_void_p(f.data_ptr()), ctypes.byref(ops._vec(v)),
+                                             ctypes.byref(ops._out(out)), ctypes.c_void_p(inv.data_ptr()))
+        ops.ctx.check(st)
+        out["inverse"] = inv
+        runs.append({k: t.cpu().numpy() for k, t in out.items()})
+    for r in runs[1:]:
+        for k in r:
+            assert np.array_equal(r[k], runs[0][k]), k
+    xr = torch.from_numpy(np.stack([case.fluid[k] for k in ("x", "y", "z")], 1).copy())
+    fr = torch.from_numpy(f_np.copy())
+    vr = [torch.from_numpy(a.copy()) for a in v_np]
+    refs = [torch_operators(xr, fr, vr, ops.off, ops.idx, ops.p) for _ in range(3)]
+    moved = [k for k in refs[0] if any(not torch.equal(r[k], refs[0][k]) for r in refs[1:])]
+    print(f"\ntorch FP64 restatement: outputs that differ between identical runs: {moved}")
+
+
+def test_backward_deterministic_and_atomic_forms(pkg, device_api):
+    """The default backward (CSR transpose + gather, no atomics) gives the
+    same bits on repeated calls, and agrees with the scatter form (FP64
+    atomics) to rounding."""
+    import torch
+
+    case = pkg.cases.lattice_box(n=12, l0=0.01)
+    ops = Operators(pkg, device_api, case)
+    f_np, v_np = fields(pkg, case)
+    x = [torch.from_numpy(case.fluid[k].copy()).cuda() for k in ("x", "y", "z")]
+    f = torch.from_numpy(f_np).cuda()
+    v = [torch.from_numpy(a.copy()).cuda() for a in v_np]
+    cot = cotangents(pkg, ops)
+
+    def flat(res):
+        fbar, vbar, xbar = res
+        return [t.cpu().numpy() for t in [fbar, *vbar, *xbar]]
+
+    det = [flat(ops.backward(x, f, v, cot)) for _ in range(3)]
+    for r in det[1:]:
+        for a_, b_ in zip(r, det[0]):
+            assert np.array_equal(a_, b_)
+    ops.ctx.set_adjoint_atomic(True)
+    try:
+        atom = flat(ops.backward(x, f, v, cot))
+    finally:
+        ops.ctx.set_adjoint_atomic(False)
+    for name, a_, b_ in zip(["f", "vx", "vy", "vz", "xx", "xy", "xz"], atom, det[0]):
+        err = np.max(np.abs(a_ - b_)) / max(np.max(np.abs(b_)), 1e-300)
+        print(f"\natomic vs deterministic d/d{name}: {err:.2e}")
+        assert err < 1e-12, (name, err)
