@@ -315,8 +315,12 @@ def run_ours(args, world, rank, local):
                                   "once at set-up (same particles and work; the as-given lattice numbering is the "
                                   "headline value)"}
 
-        # end to end through the C ABI with host buffers: pinned inputs copied
-        # in and the step's particle state copied back inside the timed region
+        # end to end through the C ABI with host buffers: the particle state
+        # lives in pinned host memory; every step copies it in, steps, and
+        # copies the moved fluid state back into the same host buffers, which
+        # the next step copies in again.  So each step's inputs are the
+        # previous step's outputs, consistent with the neighbour tables and
+        # labels that step rebuilt on the device.
         e2e = None
         if not args.no_e2e:
             ctx.set_precision(forms[-1][1])
@@ -325,7 +329,7 @@ def run_ours(args, world, rank, local):
                         [("walls", k) for k in ("x", "y", "z", "vx", "vy", "vz", "normal_x", "normal_y", "normal_z")]
             fields_out = [("fluid", k) for k in ("x", "y", "z", "vx", "vy", "vz", "pressure", "surface_type")]
             host_in = {f: getattr(dev, f[0])[f[1]].detach().to("cpu").pin_memory() for f in fields_in}
-            host_out = {f: torch.empty_like(host_in[f]).pin_memory() for f in fields_out}
+            host_out = {f: host_in[f] for f in fields_out}
             h2d = sum(t.numel() * t.element_size() for t in host_in.values())
             d2h = sum(t.numel() * t.element_size() for t in host_out.values())
             k_e2e = max(1, min(args.steps, 5))

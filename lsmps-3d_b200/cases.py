@@ -245,6 +245,32 @@ def splash_dam_break(nx: int = 200, ny: int = 50, nz: int = 200, l0: float = 0.0
     return case
 
 
+def splash_scattered(nx: int = 200, ny: int = 50, nz: int = 200, l0: float = 0.0025, fraction: float = 0.05,
+                     seed: int = 3, layers: int = 3) -> Case:
+    """The splash dam break with the lifted particles scattered off the
+    lattice: the same seeded `fraction` of the fluid is placed uniformly over
+    the whole tank floor plan (x in [0, 2 nx l0], y in [0, 2 ny l0]) and
+    z = H + U(0, 10 l0) above the free surface H = nz l0 (stream seed + 100).
+    The lifted layer is then about a quarter of the bulk density with
+    Poisson-scattered gaps, so it holds sparse neighbourhoods (Splash
+    particles) and ill-conditioned moment matrices, which lifted particles
+    kept on lattice columns do not."""
+    fx, fy, fz = fluid_block(nx, ny, nz, l0)
+    n = fx.shape[0]
+    u = uniform01(seed, 2 * n).reshape(n, 2)
+    sel = u[:, 0] < fraction
+    m = int(sel.sum())
+    v = uniform01(seed + 100, 3 * m).reshape(m, 3)
+    height = nz * l0
+    fx, fy, fz = fx.copy(), fy.copy(), fz.copy()
+    fx[sel] = v[:, 0] * (2 * nx * l0)
+    fy[sel] = v[:, 1] * (2 * ny * l0)
+    fz[sel] = height + v[:, 2] * (10.0 * l0)
+    walls = _tank_walls_fast(2 * nx, ny * 2, nx, l0, layers)
+    return _make_case(f"splash_scattered_{nx}x{ny}x{nz}", l0, fx, fy, fz, walls, height,
+                      meta={"fraction": fraction, "seed": seed, "splash_count": m})
+
+
 def lattice_box(n: int = 64, l0: float = 0.01, jitter: float = 0.1, seed: int = 40, layers: int = 3) -> Case:
     """n^3 jittered lattice inside a closed-bottom tank (adjoint check case)."""
     fx, fy, fz = fluid_block(n, n, n, l0)
@@ -302,6 +328,7 @@ CASES = {
     "hydrostatic": hydrostatic_box,
     "dam_break": dam_break,
     "splash": splash_dam_break,
+    "splash_scattered": splash_scattered,
     "lattice": lattice_box,
     "splash_shuffled": splash_shuffled,
     "dam_break_shuffled": dam_break_shuffled,

@@ -745,6 +745,57 @@ __device__ __forceinline__ void chol_solve_group(const T (&l)[45], const T (&din
   }
 }
 
+// Estimate of ||M^-1||_1 from the FP32 factor by Hager's method with
+// Higham's refinements (N. J. Higham, "FORTRAN codes for estimating the
+// one-norm of a real or complex matrix", ACM TOMS 14 (1988); the iteration of
+// LAPACK's xLACN2): x = e/n; repeat y = M^-1 x, z = M^-T sign(y) (= M^-1
+// sign(y), M symmetric); stop when ||z||_inf <= z.x, else x = e_j at the
+// largest |z_j|.  At most two rounds here, and the result is raised to
+// Higham's alternative lower bound 2 ||M^-1 b||_1 / (3n) with
+// b_i = (-1)^i (1 + i/(n-1)).  A lower bound of ||M^-1||_1, usually within a
+// small factor of it.
+__device__ __forceinline__ float inverse_norm1_estimate(const float (&l)[45], const float (&dinv)[9]) {
+  float x[9], y[9], z[9];
+#pragma unroll
+  for (int r = 0; r < 9; ++r) x[r] = 1.0f / 9.0f;
+  float est = 0.0f;
+#pragma unroll 1
+  for (int round = 0; round < 2; ++round) {
+#pragma unroll
+    for (int r = 0; r < 9; ++r) y[r] = x[r];
+    chol_solve(l, dinv, y);
+    float ny = 0.0f;
+#pragma unroll
+    for (int r = 0; r < 9; ++r) ny += fabsf(y[r]);
+    if (round > 0 && ny <= est) break;
+    est = ny;
+#pragma unroll
+    for (int r = 0; r < 9; ++r) z[r] = y[r] >= 0.0f ? 1.0f : -1.0f;
+    chol_solve(l, dinv, z);
+    int jmax = 0;
+    float zmax = fabsf(z[0]), zx = z[0] * x[0];
+#pragma unroll
+    for (int r = 1; r < 9; ++r) {
+      zx = fmaf(z[r], x[r], zx);
+      if (fabsf(z[r]) > zmax) {
+        zmax = fabsf(z[r]);
+        jmax = r;
+      }
+    }
+    if (zmax <= zx) break;
+#pragma unroll
+    for (int r = 0; r < 9; ++r) x[r] = r == jmax ? 1.0f : 0.0f;
+  }
+#pragma unroll
+  for (int r = 0; r < 9; ++r) y[r] = ((r & 1) ? -1.0f : 1.0f) * (1.0f + static_cast<float>(r) / 8.0f);
+  chol_solve(l, dinv, y);
+  float alt = 0.0f;
+#pragma unroll
+  for (int r = 0; r < 9; ++r) alt += fabsf(y[r]);
+  alt *= 2.0f / 27.0f;
+  return fmaxf(est, alt);
+}
+
 // Target t of the row set: t = 0 the Laplacian row (e3 + e4 + e5), t = 1..3
 // rows 0..2; with Full, t = 0..8 is e_t.
 template <bool Full>
@@ -850,10 +901,23 @@ __device__ __forceinline__ void mixed_rows_of_particle(const MixedRowArgs& a, in
       lo = fminf(lo, l[tri(r, r)]);
       hi = fmaxf(hi, l[tri(r, r)]);
     }
-    const double ratio = static_cast<double>(hi) / static_cast<double>(lo);
-    fp64 = ratio * ratio > a.kappa_threshold;
 #pragma unroll
     for (int r = 0; r < 9; ++r) dinv[r] = 1.0f / l[tri(r, r)];
+    // Condition estimate: the larger of (max L_ii / min L_ii)^2 (a lower
+    // bound of kappa_2) and kappa_1 = ||M||_1 * est(||M^-1||_1).
+    const double ratio = static_cast<double>(hi) / static_cast<double>(lo);
+    double norm1 = 0.0;
+#pragma unroll
+    for (int c = 0; c < 9; ++c) {
+      double col = 0.0;
+#pragma unroll
+      for (int r = 0; r < 9; ++r) col += fabs(m[(r >= c ? tri(r, c) : tri(c, r)) * kRowThreads]);
+      norm1 = fmax(norm1, col);
+    }
+    const double kappa1 = norm1 * static_cast<double>(inverse_norm1_estimate(l, dinv));
+    const double kappa = fmax(ratio * ratio, kappa1);
+    // NaN (an overflowed estimate) also takes the FP64 route
+    fp64 = !(kappa <= a.kappa_threshold);
   }
   if (!fp64) {
     // The targets are solved in groups of kGroup so that their independent

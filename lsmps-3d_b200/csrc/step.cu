@@ -12,6 +12,7 @@ extern "C" lsmps_status lsmps_step(lsmps_ctx* ctx, const lsmps_params* params, c
   if (!ctx || !params || !s) return LSMPS_INVALID_ARGUMENT;
   lsmps_status st = begin_call(ctx);
   if (st) return st;
+  StageRange step_range("lsmps_step");
   Scratch scratch(ctx);
   if (!scratch.reserve(neighbor_scratch_bytes(s->fluid.count, s->walls.count, s->fluid_cells.cell_count)))
     return fail(ctx, LSMPS_CUDA_ERROR, "scratch allocation failed (reserve before graph capture)");
@@ -24,42 +25,55 @@ extern "C" lsmps_status lsmps_step(lsmps_ctx* ctx, const lsmps_params* params, c
       ctx->built_order_count == s->fluid.count)
     ctx->order = s->fluid_cells.sorted_indices;
   // The driver prepares the moment caches once per geometry generation; the
-  // geometry changes every step, so every step builds them once.
+  // geometry changes every step, so every step builds them once.  Each stage
+  // is an NVTX range.
   const bool mixed = ctx->precision == LSMPS_PRECISION_MIXED;
-  if (mixed) {
-    // FP32 assembly and factorisation with FP64 refinement; the consumers
-    // read the compact FP32 operator rows instead of the full inverses.
-    st = mixed_step_moments_impl(ctx, s->fluid, s->walls, s->fluid_neighbors, s->wall_neighbors, *params,
-                                 s->velocity_moment, s->pressure_moment);
-    if (!st)
-      st = velocity_laplacian_mixed_impl(ctx, s->fluid, s->walls, s->fluid_neighbors, s->wall_neighbors,
-                                         s->velocity_moment, s->velocity_laplacian);
-  } else {
-    const lsmps_moment kinds[2] = {s->velocity_moment, s->pressure_moment};
-    st = prepare_moments_impl(ctx, s->fluid, s->walls, s->fluid_neighbors, s->wall_neighbors, *params, kinds, 2);
-    if (!st)
-      st = velocity_laplacian_impl(ctx, s->fluid, s->walls, s->fluid_neighbors, s->wall_neighbors,
-                                   s->velocity_moment, s->velocity_laplacian);
+  {
+    StageRange range("lsmps moments + velocity Laplacian");
+    if (mixed) {
+      // FP32 assembly and factorisation with FP64 refinement; the consumers
+      // read the compact FP32 operator rows instead of the full inverses.
+      st = mixed_step_moments_impl(ctx, s->fluid, s->walls, s->fluid_neighbors, s->wall_neighbors, *params,
+                                   s->velocity_moment, s->pressure_moment);
+      if (!st)
+        st = velocity_laplacian_mixed_impl(ctx, s->fluid, s->walls, s->fluid_neighbors, s->wall_neighbors,
+                                           s->velocity_moment, s->velocity_laplacian);
+    } else {
+      const lsmps_moment kinds[2] = {s->velocity_moment, s->pressure_moment};
+      st = prepare_moments_impl(ctx, s->fluid, s->walls, s->fluid_neighbors, s->wall_neighbors, *params, kinds, 2);
+      if (!st)
+        st = velocity_laplacian_impl(ctx, s->fluid, s->walls, s->fluid_neighbors, s->wall_neighbors,
+                                     s->velocity_moment, s->velocity_laplacian);
+    }
   }
-  if (!st) st = temporary_velocity_impl(ctx, s->fluid, *params, s->velocity_laplacian, s->temporary_velocity);
-  if (!st) st = temporary_wall_velocity_impl(ctx, s->walls, *params, s->temporary_wall_velocity);
-  if (!st && mixed)
-    st = assemble_ppe_mixed_impl(ctx, s->fluid, s->walls, *params, s->fluid_neighbors, s->wall_neighbors,
-                                 s->temporary_velocity, s->temporary_wall_velocity, s->velocity_moment,
-                                 s->pressure_moment, s->ppe);
-  else if (!st)
-    st = assemble_ppe_impl(ctx, s->fluid, s->walls, *params, s->fluid_neighbors, s->wall_neighbors,
-                           s->temporary_velocity, s->temporary_wall_velocity, s->velocity_moment,
-                           s->pressure_moment, s->ppe);
-  if (!st)
-    st = pressure_correction_impl(ctx, s->fluid, s->walls, s->fluid_neighbors, s->wall_neighbors,
-                                  s->temporary_velocity, s->pressure, *params, s->pressure_moment,
-                                  s->pressure_gradient, s->ps_displacement, s->smoothed_velocity, mixed);
-  if (!st)
-    st = build_neighbor_lists_impl(ctx, scratch, s->fluid, s->walls, *params, s->fluid_cells, s->wall_cells,
-                                   s->fluid_neighbors, s->wall_neighbors);
-  if (!st)
-    st = classify_surface_impl(ctx, s->fluid, s->walls, s->fluid_neighbors, s->wall_neighbors, *params, nullptr);
+  {
+    StageRange range("lsmps provision + PPE rows");
+    if (!st) st = temporary_velocity_impl(ctx, s->fluid, *params, s->velocity_laplacian, s->temporary_velocity);
+    if (!st) st = temporary_wall_velocity_impl(ctx, s->walls, *params, s->temporary_wall_velocity);
+    if (!st && mixed)
+      st = assemble_ppe_mixed_impl(ctx, s->fluid, s->walls, *params, s->fluid_neighbors, s->wall_neighbors,
+                                   s->temporary_velocity, s->temporary_wall_velocity, s->velocity_moment,
+                                   s->pressure_moment, s->ppe);
+    else if (!st)
+      st = assemble_ppe_impl(ctx, s->fluid, s->walls, *params, s->fluid_neighbors, s->wall_neighbors,
+                             s->temporary_velocity, s->temporary_wall_velocity, s->velocity_moment,
+                             s->pressure_moment, s->ppe);
+  }
+  {
+    StageRange range("lsmps pressure correction");
+    if (!st)
+      st = pressure_correction_impl(ctx, s->fluid, s->walls, s->fluid_neighbors, s->wall_neighbors,
+                                    s->temporary_velocity, s->pressure, *params, s->pressure_moment,
+                                    s->pressure_gradient, s->ps_displacement, s->smoothed_velocity, mixed);
+  }
+  {
+    StageRange range("lsmps neighbour rebuild + labels");
+    if (!st)
+      st = build_neighbor_lists_impl(ctx, scratch, s->fluid, s->walls, *params, s->fluid_cells, s->wall_cells,
+                                     s->fluid_neighbors, s->wall_neighbors);
+    if (!st)
+      st = classify_surface_impl(ctx, s->fluid, s->walls, s->fluid_neighbors, s->wall_neighbors, *params, nullptr);
+  }
   ctx->order = nullptr;
   return end_call(ctx, st);
 }
