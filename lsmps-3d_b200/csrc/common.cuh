@@ -185,6 +185,12 @@ struct lsmps_ctx {
   float* mixed_rows[2] = {nullptr, nullptr};
   double* mixed_rows64[2] = {nullptr, nullptr};  // rows of matrices factorised in FP64
   uint8_t* mixed_flag[2] = {nullptr, nullptr};   // 1: the particle's rows are in mixed_rows64
+  // The particles whose rows are in mixed_rows64, per kind, listed by the
+  // step's moment stage (mixed_count[kind] entries, in no particular order):
+  // the FP32 consumer kernels skip them and an FP64 pass over the list
+  // finishes them.
+  int32_t* mixed_list[2] = {nullptr, nullptr};
+  unsigned int* mixed_count = nullptr;  // [4]
   size_t mixed_cap = 0;
   // Condition-estimate threshold above which a moment matrix is factorised
   // in FP64 in the mixed form.  One FP64 refinement of an FP32 factor leaves

@@ -29,10 +29,14 @@ bool Scratch::reserve(size_t bytes) {
 void free_mixed(lsmps_ctx* ctx) {
   if (ctx->mixed_sums) cudaFree(ctx->mixed_sums);
   ctx->mixed_sums = nullptr;
+  if (ctx->mixed_count) cudaFree(ctx->mixed_count);
+  ctx->mixed_count = nullptr;
   for (int k = 0; k < 2; ++k) {
     if (ctx->mixed_rows[k]) cudaFree(ctx->mixed_rows[k]);
     if (ctx->mixed_rows64[k]) cudaFree(ctx->mixed_rows64[k]);
     if (ctx->mixed_flag[k]) cudaFree(ctx->mixed_flag[k]);
+    if (ctx->mixed_list[k]) cudaFree(ctx->mixed_list[k]);
+    ctx->mixed_list[k] = nullptr;
     ctx->mixed_rows[k] = nullptr;
     ctx->mixed_rows64[k] = nullptr;
     ctx->mixed_flag[k] = nullptr;
@@ -47,12 +51,15 @@ bool ensure_mixed(lsmps_ctx* ctx, size_t nf) {
   if (cap != cudaStreamCaptureStatusNone) return false;
   cudaStreamSynchronize(ctx->stream);
   free_mixed(ctx);
-  bool ok = cudaMalloc(&ctx->mixed_sums, nf * 31 * sizeof(double)) == cudaSuccess;
+  bool ok = cudaMalloc(&ctx->mixed_sums, nf * 31 * sizeof(double)) == cudaSuccess &&
+            cudaMalloc(&ctx->mixed_count, 4 * sizeof(unsigned int)) == cudaSuccess;
   for (int k = 0; k < 2 && ok; ++k) {
     ok = cudaMalloc(&ctx->mixed_rows[k], nf * 36 * sizeof(float)) == cudaSuccess &&
          cudaMalloc(&ctx->mixed_rows64[k], nf * 36 * sizeof(double)) == cudaSuccess &&
-         cudaMalloc(&ctx->mixed_flag[k], nf) == cudaSuccess;
+         cudaMalloc(&ctx->mixed_flag[k], nf) == cudaSuccess &&
+         cudaMalloc(&ctx->mixed_list[k], nf * sizeof(int32_t)) == cudaSuccess;
   }
+  if (ok) ok = cudaMemsetAsync(ctx->mixed_count, 0, 4 * sizeof(unsigned int), ctx->stream) == cudaSuccess;
   if (!ok) {
     cudaGetLastError();
     free_mixed(ctx);

@@ -444,6 +444,22 @@ lsmps_status smooth_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const lsmps_csr& 
 
 namespace {
 
+// Outputs of the gradient/shifting pass.
+struct GradShiftOut {
+  double* pressure;
+  double* fluid_pressure;
+  const double* pinv;
+  MixedRows prows;
+  double re;
+  double wall_scale;
+  double* gx;
+  double* gy;
+  double* gz;
+  double* sx;
+  double* sy;
+  double* sz;
+};
+
 // clamp_fluid_pressure_kernel + compute_pressure_gradient_kernel +
 // compute_particle_shifting_kernel in one pass over the rows.  All three read
 // the pre-update neighbourhood only.  The clamp is applied to every pressure
@@ -460,18 +476,14 @@ namespace {
 // takes row entries l, l + G, ...; the 15 partial sums are combined with
 // shuffles and lane 0 finishes the particle.
 template <bool Mixed, int G>
-__global__ void __launch_bounds__(kThreads, 6) gradient_shifting_kernel(GatherArgs a, double* pressure,
-                                                                     double* fluid_pressure,
-                                                                     const double* __restrict__ pinv,
-                                                                     MixedRows prows, double re,
-                                                                     double wall_scale, double* gx, double* gy,
-                                                                     double* gz, double* sx_out, double* sy_out,
-                                                                     double* sz_out) {
-  const long long tt = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
-  const index_t t = static_cast<index_t>(tt / G);
-  const int l = static_cast<int>(tt % G);
-  if (t >= static_cast<index_t>(a.fluid.count)) return;  // the whole group
-  const index_t i = visit(a.order, t);
+__device__ __forceinline__ void gradient_shifting_of(const GatherArgs& a, const GradShiftOut& out, index_t i,
+                                                     int l) {
+  double* pressure = out.pressure;
+  double* fluid_pressure = out.fluid_pressure;
+  const double* __restrict__ pinv = out.pinv;
+  const MixedRows& prows = out.prows;
+  const double re = out.re, wall_scale = out.wall_scale;
+  double *gx = out.gx, *gy = out.gy, *gz = out.gz, *sx_out = out.sx, *sy_out = out.sy, *sz_out = out.sz;
   const double praw = pressure[i];
   const double pi = praw < 0.0 ? 0.0 : praw;
   if (l == 0) {
@@ -628,6 +640,187 @@ __global__ void __launch_bounds__(kThreads, 6) gradient_shifting_kernel(GatherAr
   }
 }
 
+template <bool Mixed, int G>
+__global__ void __launch_bounds__(kThreads, 6) gradient_shifting_kernel(GatherArgs a, GradShiftOut out) {
+  const long long tt = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const index_t t = static_cast<index_t>(tt / G);
+  const int l = static_cast<int>(tt % G);
+  if (t >= static_cast<index_t>(a.fluid.count)) return;  // the whole group
+  gradient_shifting_of<Mixed, G>(a, out, visit(a.order, t), l);
+}
+
+// The FP64-route particles of the pressure kind (gradient_shifting_of<true,
+// G>, FP64 arithmetic); lane groups stride over the list.
+template <int G>
+__global__ void __launch_bounds__(kThreads, 6) gradient_shifting_list_kernel(GatherArgs a, GradShiftOut out) {
+  const index_t groups = static_cast<index_t>(gridDim.x * blockDim.x / G);
+  const int l = threadIdx.x & (G - 1);
+  const index_t count = static_cast<index_t>(*out.prows.count);
+  for (index_t t = static_cast<index_t>((blockIdx.x * blockDim.x + threadIdx.x) / G); t < count; t += groups)
+    gradient_shifting_of<true, G>(a, out, out.prows.list[t], l);
+}
+
+// Mixed form with FP32 arithmetic for the gradient: each neighbour's offset
+// is formed in FP64 and rounded once to FP32 (r_e-scaled); weight, basis and
+// the nine moment right-hand-side sums w b (p_j - p_i) are FP32 (each lane's
+// partial sums, added across the lane group in FP64), and the FP32 gradient
+// rows are applied in FP64.  Particle shifting keeps the reference's FP64
+// expressions: a pair is tested in FP32 first (|s|^2 against (d_min / r_e)^2
+// with a relative margin of 1e-5, far above the FP32 rounding of |s|^2) and
+// only pairs that pass are evaluated, and decided, in FP64.  Particles whose
+// pressure rows took the FP64 route are left to gradient_shifting_list_kernel.
+template <int G>
+__global__ void __launch_bounds__(kThreads, 6) gradient32_kernel(GatherArgs a, GradShiftOut out) {
+  const long long tt = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const index_t t = static_cast<index_t>(tt / G);
+  const int l = static_cast<int>(tt % G);
+  if (t >= static_cast<index_t>(a.fluid.count)) return;  // the whole group
+  const index_t i = visit(a.order, t);
+  if (out.prows.flag[i]) return;
+  const double praw = out.pressure[i];
+  const double pi = praw < 0.0 ? 0.0 : praw;
+  if (l == 0) {
+    out.pressure[i] = pi;
+    if (out.fluid_pressure != nullptr && out.fluid_pressure != out.pressure) out.fluid_pressure[i] = pi;
+  }
+  const bool splash = is_splash(a.fluid.surface_type, i);
+  const bool do_shift = !(a.p.ps_displacement_scale <= 0.0 || splash);
+  if (splash) {
+    if (l == 0) {
+      out.gx[i] = out.gy[i] = out.gz[i] = 0.0;
+      out.sx[i] = out.sy[i] = out.sz[i] = 0.0;
+    }
+    return;
+  }
+  const double4 own = ld4(a.fpp, i);
+  const double inv_re = 1.0 / out.re;
+  const float inv_re_f = static_cast<float>(inv_re);
+  const double dmin = a.p.ps_min_distance_ratio * a.p.particle_spacing;
+  const float dmin_s2 = static_cast<float>(dmin * inv_re * dmin * inv_re) * (1.0f + 1e-5f);
+  const double scale = a.p.ps_displacement_scale;
+  float rhs[9], b[9];
+#pragma unroll
+  for (int r = 0; r < 9; ++r) rhs[r] = 0.0f;
+  double shx = 0.0, shy = 0.0, shz = 0.0, nx = 0.0, ny = 0.0, nz = 0.0;
+  const index_t fe = a.fo[i + 1];
+  index_t o = a.fo[i] + l;
+  double4 qn = ld4(a.fpp, o < fe ? a.fi[o] : i);
+  index_t jnn = o + G < fe ? a.fi[o + G] : i;
+  for (; o < fe; o += G) {
+    const double4 q = qn;
+    if (o + G < fe) {
+      qn = ld4(a.fpp, jnn);
+      if (o + 2 * G < fe) jnn = a.fi[o + 2 * G];
+    }
+    const double dx = q.x - own.x, dy = q.y - own.y, dz = q.z - own.z;
+    const float w = basis_f32(dx, dy, dz, inv_re_f, b);
+    const float s2 = b[3] + b[4] + b[5];
+    if (w > 0.0f && s2 > 0.0f) {
+      const double pj = q.w;
+      const float wdp = w * static_cast<float>((pj < 0.0 ? 0.0 : pj) - pi);
+#pragma unroll
+      for (int r = 0; r < 9; ++r) rhs[r] = fmaf(wdp, b[r], rhs[r]);
+    }
+    if (do_shift && s2 < dmin_s2) {
+      const double d = sqrt(dx * dx + dy * dy + dz * dz);
+      if (d > 0.0 && d < dmin) {
+        const double ex = -dx, ey = -dy, ez = -dz;
+        const double push = scale * (dmin - d) / d;
+        shx += push * ex;
+        shy += push * ey;
+        shz += push * ez;
+        nx += ex / d;
+        ny += ey / d;
+        nz += ez / d;
+      }
+    }
+  }
+  const float wscale = static_cast<float>(out.wall_scale);
+  const float wr = static_cast<float>(out.re * a.p.density);
+  const index_t we = a.wo[i + 1];
+  for (index_t o = a.wo[i] + l; o < we; o += G) {
+    const index_t j = a.wi[o];
+    const double4 q = ld4(a.wp, j), nrm = ld4(a.wn, j);
+    const double dx = q.x - own.x, dy = q.y - own.y, dz = q.z - own.z;
+    const float w = wscale * basis_f32(dx, dy, dz, inv_re_f, b);
+    const float s2 = b[3] + b[4] + b[5];
+    const float nxf = static_cast<float>(nrm.x), nyf = static_cast<float>(nrm.y), nzf = static_cast<float>(nrm.z);
+    if (w > 0.0f && s2 > 0.0f) {
+      // wall Neumann vector (moment_matrix.cu:177-201) of the scaled offset
+      const float q9[9] = {nxf, nyf, nzf, 2.0f * b[0] * nxf, 2.0f * b[1] * nyf, 2.0f * b[2] * nzf,
+                           fmaf(b[1], nxf, b[0] * nyf), fmaf(b[2], nyf, b[1] * nzf), fmaf(b[0], nzf, b[2] * nxf)};
+      const float ng = static_cast<float>(a.p.gravity[0] * nrm.x + a.p.gravity[1] * nrm.y + a.p.gravity[2] * nrm.z);
+      const float wq = w * wr * ng;
+#pragma unroll
+      for (int r = 0; r < 9; ++r) rhs[r] = fmaf(wq, q9[r], rhs[r]);
+    }
+    if (do_shift && s2 < dmin_s2) {
+      const double d = sqrt(dx * dx + dy * dy + dz * dz);
+      if (d > 0.0 && d < dmin) {
+        const double push = scale * (dmin - d);
+        shx = fma(push, nrm.x, shx);
+        shy = fma(push, nrm.y, shy);
+        shz = fma(push, nrm.z, shz);
+      }
+    }
+  }
+  double rd[9];
+#pragma unroll
+  for (int r = 0; r < 9; ++r) rd[r] = static_cast<double>(rhs[r]);
+  if (G > 1) {
+    const unsigned gm = group_mask<G>();
+#pragma unroll
+    for (int r = 0; r < 9; ++r) rd[r] = group_sum<G>(rd[r], gm);
+    shx = group_sum<G>(shx, gm);
+    shy = group_sum<G>(shy, gm);
+    shz = group_sum<G>(shz, gm);
+    nx = group_sum<G>(nx, gm);
+    ny = group_sum<G>(ny, gm);
+    nz = group_sum<G>(nz, gm);
+    if (l != 0) return;
+  }
+  {
+    const float* g = out.prows.f32 + static_cast<size_t>(i) * 36;
+    double c0 = 0.0, c1 = 0.0, c2 = 0.0;
+#pragma unroll
+    for (int col = 0; col < 9; ++col) {
+      c0 = fma(static_cast<double>(g[9 + col]), rd[col], c0);
+      c1 = fma(static_cast<double>(g[18 + col]), rd[col], c1);
+      c2 = fma(static_cast<double>(g[27 + col]), rd[col], c2);
+    }
+    out.gx[i] = c0 * inv_re;
+    out.gy[i] = c1 * inv_re;
+    out.gz[i] = c2 * inv_re;
+  }
+  if (do_shift) {
+    if (is_surface(a.fluid.surface_type, i)) {
+      const double nn = sqrt(nx * nx + ny * ny + nz * nz);
+      if (nn > 0.0) {
+        nx /= nn;
+        ny /= nn;
+        nz /= nn;
+        const double nc = shx * nx + shy * ny + shz * nz;
+        shx -= nc * nx;
+        shy -= nc * ny;
+        shz -= nc * nz;
+      }
+    }
+    const double smax = a.p.ps_max_displacement_ratio * a.p.particle_spacing;
+    const double sn = sqrt(shx * shx + shy * shy + shz * shz);
+    if (sn > smax && sn > 0.0) {
+      const double sc = smax / sn;
+      shx *= sc;
+      shy *= sc;
+      shz *= sc;
+    }
+    out.sx[i] = shx;
+    out.sy[i] = shy;
+    out.sz[i] = shz;
+  } else {
+    out.sx[i] = out.sy[i] = out.sz[i] = 0.0;
+  }
+}
+
 // update_velocity_position_kernel followed by anti_penetration_kernel for the
 // same particle: the anti-penetration pass reads only the particle's own
 // updated state and the walls, so running it right after the update in the
@@ -682,25 +875,45 @@ __global__ void __launch_bounds__(kThreads) update_anti_penetration_kernel(
 
 // gradient_shifting_kernel with the context's lane count (LSMPS_KNOB_GATHER_LANES).
 template <bool Mixed>
-void launch_gradient_shifting(lsmps_ctx* ctx, size_t count, const GatherArgs& a, double* pressure,
-                              double* fluid_pressure, const double* pinv, const MixedRows& rows, double re,
-                              double wall_scale, const lsmps_vector& g, const lsmps_vector& s) {
+void launch_gradient_shifting(lsmps_ctx* ctx, size_t count, const GatherArgs& a, const GradShiftOut& out) {
   const long long n = static_cast<long long>(count);
   switch (ctx->knob[LSMPS_KNOB_GATHER_LANES]) {
     case 1:
       launch_named(ctx, Mixed ? "gradient_shifting_kernel<true, 2>" : "gradient_shifting_kernel<false, 2>",
-                   gradient_shifting_kernel<Mixed, 2>, dim3(div_up(2 * n, kThreads)), dim3(kThreads), 0, a, pressure,
-                   fluid_pressure, pinv, rows, re, wall_scale, g.x, g.y, g.z, s.x, s.y, s.z);
+                   gradient_shifting_kernel<Mixed, 2>, dim3(div_up(2 * n, kThreads)), dim3(kThreads), 0, a, out);
       break;
     case 2:
       launch_named(ctx, Mixed ? "gradient_shifting_kernel<true, 4>" : "gradient_shifting_kernel<false, 4>",
-                   gradient_shifting_kernel<Mixed, 4>, dim3(div_up(4 * n, kThreads)), dim3(kThreads), 0, a, pressure,
-                   fluid_pressure, pinv, rows, re, wall_scale, g.x, g.y, g.z, s.x, s.y, s.z);
+                   gradient_shifting_kernel<Mixed, 4>, dim3(div_up(4 * n, kThreads)), dim3(kThreads), 0, a, out);
       break;
     default:
       launch_named(ctx, Mixed ? "gradient_shifting_kernel<true, 1>" : "gradient_shifting_kernel<false, 1>",
-                   gradient_shifting_kernel<Mixed, 1>, dim3(div_up(n, kThreads)), dim3(kThreads), 0, a, pressure,
-                   fluid_pressure, pinv, rows, re, wall_scale, g.x, g.y, g.z, s.x, s.y, s.z);
+                   gradient_shifting_kernel<Mixed, 1>, dim3(div_up(n, kThreads)), dim3(kThreads), 0, a, out);
+  }
+}
+
+// The mixed form: FP32 kernel, then the FP64-route particles.
+void launch_gradient32(lsmps_ctx* ctx, size_t count, const GatherArgs& a, const GradShiftOut& out) {
+  const long long n = static_cast<long long>(count);
+  const dim3 list_grid(static_cast<unsigned>(ctx->sm_count * 2));
+  switch (ctx->knob[LSMPS_KNOB_GATHER_LANES]) {
+    case 1:
+      launch_named(ctx, "gradient32_kernel<2>", gradient32_kernel<2>, dim3(div_up(2 * n, kThreads)), dim3(kThreads), 0,
+                   a, out);
+      launch_named(ctx, "gradient_shifting_list_kernel<2>", gradient_shifting_list_kernel<2>, list_grid,
+                   dim3(kThreads), 0, a, out);
+      break;
+    case 2:
+      launch_named(ctx, "gradient32_kernel<4>", gradient32_kernel<4>, dim3(div_up(4 * n, kThreads)), dim3(kThreads), 0,
+                   a, out);
+      launch_named(ctx, "gradient_shifting_list_kernel<4>", gradient_shifting_list_kernel<4>, list_grid,
+                   dim3(kThreads), 0, a, out);
+      break;
+    default:
+      launch_named(ctx, "gradient32_kernel<1>", gradient32_kernel<1>, dim3(div_up(n, kThreads)), dim3(kThreads), 0, a,
+                   out);
+      launch_named(ctx, "gradient_shifting_list_kernel<1>", gradient_shifting_list_kernel<1>, list_grid,
+                   dim3(kThreads), 0, a, out);
   }
 }
 
@@ -724,15 +937,17 @@ lsmps_status gradient_shifting_stage(lsmps_ctx* ctx, const lsmps_fluid& f, const
   a.wp = ctx->pack_wall[0];
   a.wn = ctx->pack_wall[2];
   a.order = ctx->order;
+  GradShiftOut out{pressure, f.pressure, nullptr, MixedRows{}, pm.support_radius, pm.wall_weight_scale,
+                   g.x, g.y, g.z, s.x, s.y, s.z};
   if (mixed) {
-    if (!ctx->mixed_rows[1] || ctx->mixed_cap < f.count)
+    if (!ctx->mixed_rows[1] || !ctx->mixed_count || ctx->mixed_cap < f.count)
       return fail(ctx, LSMPS_NOT_PREPARED, "mixed pressure operator rows were not prepared");
-    launch_gradient_shifting<true>(ctx, f.count, a, pressure, f.pressure, nullptr, mixed_rows_of(ctx, 1),
-                                   pm.support_radius, pm.wall_weight_scale, g, s);
+    out.prows = mixed_rows_of(ctx, 1);
+    launch_gradient32(ctx, f.count, a, out);
   } else {
     if (!pm.inverse_matrices) return fail(ctx, LSMPS_INVALID_ARGUMENT, "pressure inverse buffer missing");
-    launch_gradient_shifting<false>(ctx, f.count, a, pressure, f.pressure, pm.inverse_matrices, MixedRows{},
-                                    pm.support_radius, pm.wall_weight_scale, g, s);
+    out.pinv = pm.inverse_matrices;
+    launch_gradient_shifting<false>(ctx, f.count, a, out);
   }
   return check_launch(ctx, "gradient/shifting");
 }

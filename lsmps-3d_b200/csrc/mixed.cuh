@@ -15,13 +15,43 @@
 namespace lsmps {
 
 struct MixedRows {
-  const float* f32;      // [n][36]
-  const double* f64;     // [n][36], valid where flag[i] != 0
-  const uint8_t* flag;   // [n]
+  const float* f32;           // [n][36]
+  const double* f64;          // [n][36], valid where flag[i] != 0
+  const uint8_t* flag;        // [n]
+  const int32_t* list;        // the flagged particles, *count of them
+  const unsigned int* count;
 };
 
 inline MixedRows mixed_rows_of(const lsmps_ctx* ctx, int kind) {
-  return MixedRows{ctx->mixed_rows[kind], ctx->mixed_rows64[kind], ctx->mixed_flag[kind]};
+  return MixedRows{ctx->mixed_rows[kind], ctx->mixed_rows64[kind], ctx->mixed_flag[kind], ctx->mixed_list[kind],
+                   ctx->mixed_count ? ctx->mixed_count + kind : nullptr};
+}
+
+// FP32 geometry of one neighbour from the FP64 coordinate difference:
+// s = d / r_e rounded once to FP32, w = 1 - |s| (0 outside the support) and
+// the Type-A basis of s.  Returns w.
+__device__ __forceinline__ float basis_f32(double dx, double dy, double dz, float inv_re, float b[9]) {
+  const float sx = static_cast<float>(dx) * inv_re;
+  const float sy = static_cast<float>(dy) * inv_re;
+  const float sz = static_cast<float>(dz) * inv_re;
+  const float w = 1.0f - sqrtf(fmaf(sx, sx, fmaf(sy, sy, sz * sz)));
+  b[0] = sx;
+  b[1] = sy;
+  b[2] = sz;
+  b[3] = sx * sx;
+  b[4] = sy * sy;
+  b[5] = sz * sz;
+  b[6] = sx * sy;
+  b[7] = sy * sz;
+  b[8] = sz * sx;
+  return w > 0.0f ? w : 0.0f;
+}
+
+__device__ __forceinline__ float dot9f(const float a[9], const float b[9]) {
+  float v = a[0] * b[0];
+#pragma unroll
+  for (int k = 1; k < 9; ++k) v = fmaf(a[k], b[k], v);
+  return v;
 }
 
 // Row t (0..3) of particle i as doubles.

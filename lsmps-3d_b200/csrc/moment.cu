@@ -697,6 +697,8 @@ struct MixedRowArgs {
   float* rows[2];     // compact FP32 rows per kind (unless Full)
   double* rows64[2];  // compact FP64 rows of the FP64-route particles (unless Full)
   uint8_t* flag[2];   // 1 where rows64 holds the particle's rows (unless Full)
+  int32_t* list[2];   // the FP64-route particles, appended (unless Full)
+  unsigned int* count;
   DeviceStatus* status;
   const int32_t* order;  // visiting order (the sums are stored by visiting position) or NULL
 };
@@ -986,7 +988,10 @@ __device__ __forceinline__ void mixed_rows_of_particle(const MixedRowArgs& a, in
   }
   ko.trace[i] = trace;
   ko.reg[i] = reg;
-  if (!Full) a.flag[kind][i] = 1;
+  if (!Full) {
+    a.flag[kind][i] = 1;
+    a.list[kind][atomicAdd(&a.count[kind], 1u)] = i;
+  }
   double l64[45];
 #pragma unroll
   for (int e = 0; e < 45; ++e) l64[e] = m[e * kRowThreads];
@@ -1115,7 +1120,11 @@ lsmps_status launch_mixed(lsmps_ctx* ctx, index_t n, const lsmps_csr& fn, const 
     ra.rows[k] = ctx->mixed_rows[k];
     ra.rows64[k] = ctx->mixed_rows64[k];
     ra.flag[k] = ctx->mixed_flag[k];
+    ra.list[k] = ctx->mixed_list[k];
   }
+  ra.count = ctx->mixed_count;
+  // the lists of FP64-route particles start empty every time
+  cudaMemsetAsync(ctx->mixed_count, 0, 4 * sizeof(unsigned int), ctx->stream);
   ra.status = ctx->d_status;
   ra.order = ctx->order;
   if (split) {

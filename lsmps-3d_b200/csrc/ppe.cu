@@ -183,16 +183,11 @@ __global__ void __launch_bounds__(kThreads) ppe_kernel(PpeArgs a) {
 // diagonal (minus the sum of the off-diagonal values) and the RHS sums stay
 // FP64.
 template <int G, bool Mixed>
-__global__ void __launch_bounds__(kThreads, 4) ppe_lanes_kernel(PpeArgs a) {
-  const index_t t = (blockIdx.x * blockDim.x + threadIdx.x) / G;
-  const int l = threadIdx.x & (G - 1);
+__device__ __forceinline__ void ppe_row(const PpeArgs& a, index_t i, int l, bool write_offsets) {
   const index_t n = static_cast<index_t>(a.fluid.count);
-  // Whole groups leave together, so the shuffles below see full groups.
-  if (t >= n) return;
-  const index_t i = visit(a.order, t);
   const index_t nb = a.fo[i], ne = a.fo[i + 1];
   const index_t row = i + nb;
-  if (l == 0) {
+  if (l == 0 && write_offsets) {
     a.row_offsets[i] = row;
     if (i + 1 == n) a.row_offsets[n] = n + ne;
   }
@@ -308,6 +303,151 @@ __global__ void __launch_bounds__(kThreads, 4) ppe_lanes_kernel(PpeArgs a) {
   if (a.wall_rhs_out) a.wall_rhs_out[i] = wall_rhs;
 }
 
+template <int G, bool Mixed>
+__global__ void __launch_bounds__(kThreads, 4) ppe_lanes_kernel(PpeArgs a) {
+  const index_t t = (blockIdx.x * blockDim.x + threadIdx.x) / G;
+  const int l = threadIdx.x & (G - 1);
+  // Whole groups leave together, so the shuffles see full groups.
+  if (t >= static_cast<index_t>(a.fluid.count)) return;
+  ppe_row<G, Mixed>(a, visit(a.order, t), l, true);
+}
+
+// The mixed form with FP32 arithmetic; the particles whose rows took the
+// FP64 route get their row offsets here and their rows from ppe_list_kernel.
+//
+// FP32 arithmetic: each neighbour's offset is formed in FP64 and rounded
+// once to FP32 (r_e-scaled); distance, weight, basis, the coefficient
+// a_ij = 2 w (L . b) / (r_e^2 rho) and the divergence term are FP32, with the
+// FP32 operator rows; the diagonal (minus the sum of the stored off-diagonal
+// values), the divergence sum and the wall Neumann sum accumulate in FP64.
+template <int G>
+__device__ __forceinline__ void ppe_row32(const PpeArgs& a, index_t i, int l) {
+  const index_t n = static_cast<index_t>(a.fluid.count);
+  const index_t nb = a.fo[i], ne = a.fo[i + 1];
+  const index_t row = i + nb;
+  if (l == 0) {
+    a.row_offsets[i] = row;
+    if (i + 1 == n) a.row_offsets[n] = n + ne;
+  }
+  if (a.vrows.flag[i] | a.prows.flag[i]) return;  // FP64 rows: ppe_list_kernel
+  const int type = a.fluid.surface_type ? a.fluid.surface_type[i] : LSMPS_SURFACE_INNER;
+  if (type == LSMPS_SURFACE_SURFACE || type == LSMPS_SURFACE_SPLASH) {
+    for (index_t o = nb + l; o < ne; o += G) {
+      a.col[row + 1 + o - nb] = a.fi[o];
+      a.val[row + 1 + o - nb] = 0.0;
+    }
+    if (l == 0) {
+      a.col[row] = i;
+      a.val[row] = 1.0;
+      a.rhs[i] = 0.0;
+      a.divergence[i] = 0.0;
+      if (a.wall_rhs_out) a.wall_rhs_out[i] = 0.0;
+    }
+    return;
+  }
+  const double4 pi = ld4(a.fp, i);
+  // The group's four operator rows in shared memory (read by broadcast in
+  // every neighbour's dot products; they hold no registers): the pressure
+  // Laplacian row L, then the velocity gradient rows 0, 1, 2.  The stride of
+  // 40 floats keeps the 16-byte row reads of neighbouring groups on
+  // different banks.
+  __shared__ __align__(16) float s_rows[kThreads / G][40];
+  float* L = s_rows[threadIdx.x / G];
+  const float* gx = L + 9;
+  const float* gy = L + 18;
+  const float* gz = L + 27;
+  for (int c = l; c < 36; c += G)
+    L[c] = c < 9 ? a.prows.f32[static_cast<size_t>(i) * 36 + c] : a.vrows.f32[static_cast<size_t>(i) * 36 + c];
+  __syncwarp(group_mask<G>());
+  float b[9];
+  const double uxi = a.tvx[i], uyi = a.tvy[i], uzi = a.tvz[i];
+  const float inv_re = static_cast<float>(a.inv_re);
+  const float scale = static_cast<float>(2.0 / (a.re * a.re * a.density));
+  double dsum = 0.0, diag = 0.0;
+  index_t o = nb + l;
+  index_t jn = o < ne ? a.fi[o] : i;
+  index_t jnn = o + G < ne ? a.fi[o + G] : i;
+  double4 qn = ld4(a.fp, jn), un = ld4(a.fu, jn);
+  for (; o < ne; o += G) {
+    const index_t j = jn;
+    const double4 q = qn, u = un;
+    if (o + G < ne) {
+      jn = jnn;
+      qn = ld4(a.fp, jn);
+      un = ld4(a.fu, jn);
+      if (o + 2 * G < ne) jnn = a.fi[o + 2 * G];
+    }
+    const float w = basis_f32(q.x - pi.x, q.y - pi.y, q.z - pi.z, inv_re, b);
+    float off = 0.0f;
+    if (w > 0.0f) {
+      off = w * dot9f(L, b) * scale;
+      diag -= static_cast<double>(off);
+      const float dux = static_cast<float>(u.x - uxi), duy = static_cast<float>(u.y - uyi),
+                  duz = static_cast<float>(u.z - uzi);
+      const float cx = dot9f(gx, b), cy = dot9f(gy, b), cz = dot9f(gz, b);
+      dsum += static_cast<double>(w * fmaf(cx, dux, fmaf(cy, duy, cz * duz)));
+    }
+    a.col[row + 1 + o - nb] = j;
+    a.val[row + 1 + o - nb] = static_cast<double>(off);
+  }
+  double wall_rhs = 0.0;
+  const index_t we = a.wo[i + 1];
+  const float vws = static_cast<float>(a.vwall_scale);
+  const float pws = static_cast<float>(2.0 * a.pwall_scale);
+  for (index_t o = a.wo[i] + l; o < we; o += G) {
+    const index_t j = a.wi[o];
+    const double4 q = ld4(a.wp, j), u = ld4(a.wu, j), nrm = ld4(a.wn, j);
+    const float w = basis_f32(q.x - pi.x, q.y - pi.y, q.z - pi.z, inv_re, b);
+    if (w <= 0.0f) continue;
+    const float dux = static_cast<float>(u.x - uxi), duy = static_cast<float>(u.y - uyi),
+                duz = static_cast<float>(u.z - uzi);
+    const float cx = dot9f(gx, b), cy = dot9f(gy, b), cz = dot9f(gz, b);
+    dsum += static_cast<double>(vws * w * fmaf(cx, dux, fmaf(cy, duy, cz * duz)));
+    const float nx = static_cast<float>(nrm.x), ny = static_cast<float>(nrm.y), nz = static_cast<float>(nrm.z);
+    // wall Neumann vector (moment_matrix.cu:177-201) of the scaled offset
+    const float q9[9] = {nx, ny, nz, 2.0f * b[0] * nx, 2.0f * b[1] * ny, 2.0f * b[2] * nz,
+                         fmaf(b[1], nx, b[0] * ny), fmaf(b[2], ny, b[1] * nz), fmaf(b[0], nz, b[2] * nx)};
+    const double ng = a.gx * nrm.x + a.gy * nrm.y + a.gz * nrm.z;
+    wall_rhs += static_cast<double>(pws * w * dot9f(L, q9)) * ng * a.inv_re;
+  }
+  const unsigned mask = group_mask<G>();
+  diag = group_sum<G>(diag, mask);
+  wall_rhs = group_sum<G>(wall_rhs, mask);
+  dsum = group_sum<G>(dsum, mask);
+  if (l != 0) return;
+  const double div = dsum * a.inv_re;
+  a.col[row] = i;
+  a.val[row] = diag;
+  a.divergence[i] = div;
+  a.rhs[i] = div / (a.dt_dev ? *a.dt_dev : a.dt) - wall_rhs;
+  if (a.wall_rhs_out) a.wall_rhs_out[i] = wall_rhs;
+}
+
+template <int G>
+__global__ void __launch_bounds__(kThreads, 7) ppe32_kernel(PpeArgs a) {
+  const index_t t = (blockIdx.x * blockDim.x + threadIdx.x) / G;
+  const int l = threadIdx.x & (G - 1);
+  if (t >= static_cast<index_t>(a.fluid.count)) return;
+  ppe_row32<G>(a, visit(a.order, t), l);
+}
+
+// The rows of the FP64-route particles (FP64 arithmetic, ppe_row<G, true>):
+// first every particle of the velocity kind's list, then those of the
+// pressure kind's list that are not on the velocity kind's.  Lane groups
+// stride over the lists.
+template <int G>
+__global__ void __launch_bounds__(kThreads, 4) ppe_list_kernel(PpeArgs a) {
+  const index_t groups = static_cast<index_t>(gridDim.x * blockDim.x / G);
+  const index_t g0 = static_cast<index_t>((blockIdx.x * blockDim.x + threadIdx.x) / G);
+  const int l = threadIdx.x & (G - 1);
+  const index_t nv = static_cast<index_t>(*a.vrows.count), np = static_cast<index_t>(*a.prows.count);
+  for (index_t t = g0; t < nv + np; t += groups) {
+    const index_t i = t < nv ? a.vrows.list[t] : a.prows.list[t - nv];
+    if (t >= nv && a.vrows.flag[i]) continue;
+    ppe_row<G, true>(a, i, l, false);
+  }
+}
+
 // Neighbour records of the lane kernels: positions and u* of the fluid,
 // positions, u* and normals of the walls.
 bool pack_ppe(lsmps_ctx* ctx, const lsmps_fluid& f, const lsmps_walls& w, const lsmps_fluid& tv,
@@ -402,7 +542,7 @@ lsmps_status assemble_ppe_mixed_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const
     return fail(ctx, LSMPS_INVALID_ARGUMENT, "PPE workspace requires matrix, rhs, divergence and velocity buffers");
   if (tw.count > 0 && (!tw.vx || !tw.vy || !tw.vz))
     return fail(ctx, LSMPS_INVALID_ARGUMENT, "PPE RHS assembly requires temporary wall velocity buffers");
-  if (!ctx->mixed_rows[0] || !ctx->mixed_rows[1] || ctx->mixed_cap < f.count)
+  if (!ctx->mixed_rows[0] || !ctx->mixed_rows[1] || !ctx->mixed_count || ctx->mixed_cap < f.count)
     return fail(ctx, LSMPS_NOT_PREPARED, "mixed operator rows were not prepared");
   PpeArgs a{};
   a.fluid = f;
@@ -438,11 +578,21 @@ lsmps_status assemble_ppe_mixed_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const
   a.wall_rhs_out = ws.pressure_laplacian;
   if (!pack_ppe(ctx, f, w, tv, tw, a)) return fail(ctx, LSMPS_CUDA_ERROR, "pack allocation failed");
   const long long rows = static_cast<long long>(f.count);
+  const dim3 list_grid(static_cast<unsigned>(ctx->sm_count * 2));
   switch (ctx->knob[LSMPS_KNOB_PPE_LANES]) {
     case 0:
-    case 1: launch_named(ctx, "ppe_lanes_kernel<4, true>", ppe_lanes_kernel<4, true>, dim3(div_up(rows * 4, kThreads)), dim3(kThreads), 0, a); break;
-    case 3: launch_named(ctx, "ppe_lanes_kernel<16, true>", ppe_lanes_kernel<16, true>, dim3(div_up(rows * 16, kThreads)), dim3(kThreads), 0, a); break;
-    default: launch_named(ctx, "ppe_lanes_kernel<8, true>", ppe_lanes_kernel<8, true>, dim3(div_up(rows * 8, kThreads)), dim3(kThreads), 0, a); break;
+    case 1:
+      launch_named(ctx, "ppe32_kernel<4>", ppe32_kernel<4>, dim3(div_up(rows * 4, kThreads)), dim3(kThreads), 0, a);
+      launch_named(ctx, "ppe_list_kernel<4>", ppe_list_kernel<4>, list_grid, dim3(kThreads), 0, a);
+      break;
+    case 3:
+      launch_named(ctx, "ppe32_kernel<16>", ppe32_kernel<16>, dim3(div_up(rows * 16, kThreads)), dim3(kThreads), 0, a);
+      launch_named(ctx, "ppe_list_kernel<16>", ppe_list_kernel<16>, list_grid, dim3(kThreads), 0, a);
+      break;
+    default:
+      launch_named(ctx, "ppe32_kernel<8>", ppe32_kernel<8>, dim3(div_up(rows * 8, kThreads)), dim3(kThreads), 0, a);
+      launch_named(ctx, "ppe_list_kernel<8>", ppe_list_kernel<8>, list_grid, dim3(kThreads), 0, a);
+      break;
   }
   return check_launch(ctx, "PPE assembly (mixed)");
 }

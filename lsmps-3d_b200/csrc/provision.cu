@@ -47,11 +47,7 @@ struct LaplacianArgs {
 // entries l, l + G, ... of both rows and the groups' partial sums are added
 // with shuffles (a rounding-level reassociation for G > 1).
 template <bool Mixed, int G>
-__global__ void __launch_bounds__(kThreads, 5) laplacian_kernel(LaplacianArgs a, MixedRows rows) {
-  const index_t t = (blockIdx.x * blockDim.x + threadIdx.x) / G;
-  const int l = threadIdx.x & (G - 1);
-  if (t >= a.n) return;  // the whole group
-  const index_t i = visit(a.order, t);
+__device__ __forceinline__ void laplacian_of(const LaplacianArgs& a, const MixedRows& rows, index_t i, int l) {
   const double4 pi = ld4(a.fp, i);
   const double4 ui = ld4(a.fv, i);
   // The particle's Laplacian row L (the sum of the inverse's rows 3..5, or
@@ -125,6 +121,92 @@ __global__ void __launch_bounds__(kThreads, 5) laplacian_kernel(LaplacianArgs a,
   a.lz[i] = scale * cz;
 }
 
+template <bool Mixed, int G>
+__global__ void __launch_bounds__(kThreads, 5) laplacian_kernel(LaplacianArgs a, MixedRows rows) {
+  const index_t t = (blockIdx.x * blockDim.x + threadIdx.x) / G;
+  const int l = threadIdx.x & (G - 1);
+  if (t >= a.n) return;  // the whole group
+  laplacian_of<Mixed, G>(a, rows, visit(a.order, t), l);
+}
+
+// Mixed form with FP32 arithmetic: each neighbour's offset is formed in FP64
+// and rounded once to FP32 (r_e-scaled); distance, weight, basis and the
+// coefficient w (L . b) with the FP32 Laplacian row are FP32; the coefficient
+// times the FP64 velocity difference accumulates in FP64.  Particles whose
+// velocity rows took the FP64 route are left to laplacian_list_kernel.
+template <int G>
+__global__ void __launch_bounds__(kThreads, 8) laplacian32_kernel(LaplacianArgs a, MixedRows rows) {
+  const index_t t = (blockIdx.x * blockDim.x + threadIdx.x) / G;
+  const int l = threadIdx.x & (G - 1);
+  if (t >= a.n) return;  // the whole group
+  const index_t i = visit(a.order, t);
+  if (rows.flag[i]) return;
+  const double4 pi = ld4(a.fp, i);
+  const double4 ui = ld4(a.fv, i);
+  __shared__ float s_L[kThreads / G][12];
+  float* L = s_L[threadIdx.x / G];
+  for (int c = l; c < 9; c += G) L[c] = rows.f32[static_cast<size_t>(i) * 36 + c];
+  __syncwarp(group_mask<G>());
+  const float inv_re = static_cast<float>(a.inv_re);
+  float b[9];
+  double cx = 0.0, cy = 0.0, cz = 0.0;
+  const index_t fe = a.fo[i + 1];
+  index_t o = a.fo[i] + l;
+  index_t jn = o < fe ? a.fi[o] : i;
+  index_t jnn = o + G < fe ? a.fi[o + G] : i;
+  double4 qn = ld4(a.fp, jn), un = ld4(a.fv, jn);
+  for (; o < fe; o += G) {
+    const double4 q = qn, u = un;
+    if (o + G < fe) {
+      jn = jnn;
+      qn = ld4(a.fp, jn);
+      un = ld4(a.fv, jn);
+      if (o + 2 * G < fe) jnn = a.fi[o + 2 * G];
+    }
+    const float w = basis_f32(q.x - pi.x, q.y - pi.y, q.z - pi.z, inv_re, b);
+    if (w <= 0.0f) continue;
+    const double s = static_cast<double>(w * dot9f(L, b));
+    cx = fma(s, u.x - ui.x, cx);
+    cy = fma(s, u.y - ui.y, cy);
+    cz = fma(s, u.z - ui.z, cz);
+  }
+  const float wall_scale = static_cast<float>(a.wall_scale);
+  const index_t we = a.wo[i + 1];
+  for (index_t o = a.wo[i] + l; o < we; o += G) {
+    const index_t j = a.wi[o];
+    const double4 q = ld4(a.wp, j);
+    const double4 u = ld4(a.wv, j);
+    const float w = wall_scale * basis_f32(q.x - pi.x, q.y - pi.y, q.z - pi.z, inv_re, b);
+    if (w <= 0.0f) continue;
+    const double s = static_cast<double>(w * dot9f(L, b));
+    cx = fma(s, u.x - ui.x, cx);
+    cy = fma(s, u.y - ui.y, cy);
+    cz = fma(s, u.z - ui.z, cz);
+  }
+  if (G > 1) {
+    const unsigned mask = group_mask<G>();
+    cx = group_sum<G>(cx, mask);
+    cy = group_sum<G>(cy, mask);
+    cz = group_sum<G>(cz, mask);
+    if (l != 0) return;
+  }
+  const double scale = 2.0 / (a.re * a.re);
+  a.lx[i] = scale * cx;
+  a.ly[i] = scale * cy;
+  a.lz[i] = scale * cz;
+}
+
+// The FP64-route particles of the velocity kind (FP64 arithmetic,
+// laplacian_of<true, G>); lane groups stride over the list.
+template <int G>
+__global__ void __launch_bounds__(kThreads, 5) laplacian_list_kernel(LaplacianArgs a, MixedRows rows) {
+  const index_t groups = static_cast<index_t>(gridDim.x * blockDim.x / G);
+  const int l = threadIdx.x & (G - 1);
+  const index_t count = static_cast<index_t>(*rows.count);
+  for (index_t t = static_cast<index_t>((blockIdx.x * blockDim.x + threadIdx.x) / G); t < count; t += groups)
+    laplacian_of<true, G>(a, rows, rows.list[t], l);
+}
+
 // combine_explicit_velocity_kernel, explicit_update.cu:250-270
 __global__ void combine_kernel(lsmps_fluid f, lsmps_params p, const double* __restrict__ lx,
                                const double* __restrict__ ly, const double* __restrict__ lz, double* tx, double* ty,
@@ -187,7 +269,7 @@ lsmps_status velocity_laplacian_mixed_impl(lsmps_ctx* ctx, const lsmps_fluid& f,
   if (!lap.x || !lap.y || !lap.z || !f.vx || !f.vy || !f.vz)
     return fail(ctx, LSMPS_INVALID_ARGUMENT, "Provision buffers missing");
   if (w.count > 0 && (!w.vx || !w.vy || !w.vz)) return fail(ctx, LSMPS_INVALID_ARGUMENT, "wall velocity missing");
-  if (!ctx->mixed_rows[0] || ctx->mixed_cap < f.count)
+  if (!ctx->mixed_rows[0] || !ctx->mixed_count || ctx->mixed_cap < f.count)
     return fail(ctx, LSMPS_NOT_PREPARED, "mixed velocity operator rows were not prepared");
   if (!ensure_packs(ctx, f.count, w.count)) return fail(ctx, LSMPS_CUDA_ERROR, "pack allocation failed");
   pack4(ctx, f.vx, f.vy, f.vz, nullptr, f.count, ctx->pack_fluid[1]);
@@ -197,7 +279,26 @@ lsmps_status velocity_laplacian_mixed_impl(lsmps_ctx* ctx, const lsmps_fluid& f,
                   ctx->pack_wall[1], fn.offsets, fn.indices, wn.offsets, wn.indices, nullptr,
                   vm.support_radius, 1.0 / vm.support_radius, vm.wall_weight_scale, lap.x, lap.y, lap.z,
                   ctx->order};
-  launch_laplacian<true>(ctx, a, mixed_rows_of(ctx, 0));
+  const MixedRows rows = mixed_rows_of(ctx, 0);
+  const long long n = a.n;
+  const dim3 list_grid(static_cast<unsigned>(ctx->sm_count * 2));
+  switch (ctx->knob[LSMPS_KNOB_GATHER_LANES]) {
+    case 1:
+      launch_named(ctx, "laplacian32_kernel<2>", laplacian32_kernel<2>, dim3(div_up(2 * n, kThreads)), dim3(kThreads),
+                   0, a, rows);
+      launch_named(ctx, "laplacian_list_kernel<2>", laplacian_list_kernel<2>, list_grid, dim3(kThreads), 0, a, rows);
+      break;
+    case 2:
+      launch_named(ctx, "laplacian32_kernel<4>", laplacian32_kernel<4>, dim3(div_up(4 * n, kThreads)), dim3(kThreads),
+                   0, a, rows);
+      launch_named(ctx, "laplacian_list_kernel<4>", laplacian_list_kernel<4>, list_grid, dim3(kThreads), 0, a, rows);
+      break;
+    default:
+      launch_named(ctx, "laplacian32_kernel<1>", laplacian32_kernel<1>, dim3(div_up(n, kThreads)), dim3(kThreads), 0,
+                   a, rows);
+      launch_named(ctx, "laplacian_list_kernel<1>", laplacian_list_kernel<1>, list_grid, dim3(kThreads), 0, a, rows);
+      break;
+  }
   return check_launch(ctx, "velocity laplacian (mixed)");
 }
 

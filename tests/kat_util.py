@@ -81,6 +81,20 @@ def vec_err(g: dict, o: dict, comps, extra_scale: dict | None = None):
     return {c: rel_err(g[c], o[c], scale=scale if scale > 0 else None) for c in comps}
 
 
+def coef_rel_err(values, ref_values, floor_frac=1e-4):
+    """Per-coefficient relative error of a matrix's values against a
+    reference: max |a - r| / max(|r|, floor), floor = floor_frac times the
+    largest |r| (coefficients below the floor are measured against it)."""
+    v = np.asarray(values, dtype=np.float64)
+    r = np.asarray(ref_values, dtype=np.float64)
+    if r.size == 0:
+        return 0.0
+    floor = floor_frac * float(np.max(np.abs(r)))
+    if floor == 0.0:
+        return float(np.max(np.abs(v)))
+    return float(np.max(np.abs(v - r) / np.maximum(np.abs(r), floor)))
+
+
 def row_rel_err(values, ref_values, row_offsets):
     """Row-normwise relative error of a CSR matrix against a reference with
     the same pattern: max over rows of max_j |a_ij - r_ij| / max_j |r_ij|
