@@ -837,10 +837,12 @@ def mixed_error(pkg, torch, ctx, dev, case, p, state, reset, default_kappa):
         dmax = torch.zeros(n, dtype=d.dtype, device=d.device).scatter_reduce(0, row, d, "amax")
         rowwise = float(torch.where(amax > 0, dmax / torch.where(amax > 0, amax, torch.ones_like(amax)), dmax).max())
         per_coef = float((d / torch.clamp(a, min=floor)).max())
+        per_coef_2 = float((d / torch.clamp(a, min=100.0 * floor)).max())
         out["thresholds"][f"{kappa:.0e}"] = {
             "fp64_route_matrices": int(mix["fallbacks"]),
             "ppe_coefficients_max_rel_per_coefficient": per_coef,
             "ppe_coefficients_floor": f"|a_ij| below 1e-4 of the largest |a_ij| ({floor:.3e}) counts as that floor",
+            "ppe_coefficients_max_rel_per_coefficient_floor_1e-2": per_coef_2,
             "ppe_coefficients_max_rel_rowwise": rowwise,
             "ppe_rhs_rel": norm_err(mix, ["rhs"]),
             "ppe_divergence_rel": norm_err(mix, ["divergence"]),

@@ -694,7 +694,6 @@ __global__ void __launch_bounds__(kThreads, 6) gradient32_kernel(GatherArgs a, G
   }
   const double4 own = ld4(a.fpp, i);
   const double inv_re = 1.0 / out.re;
-  const float inv_re_f = static_cast<float>(inv_re);
   const double dmin = a.p.ps_min_distance_ratio * a.p.particle_spacing;
   const float dmin_s2 = static_cast<float>(dmin * inv_re * dmin * inv_re) * (1.0f + 1e-5f);
   const double scale = a.p.ps_displacement_scale;
@@ -713,7 +712,7 @@ __global__ void __launch_bounds__(kThreads, 6) gradient32_kernel(GatherArgs a, G
       if (o + 2 * G < fe) jnn = a.fi[o + 2 * G];
     }
     const double dx = q.x - own.x, dy = q.y - own.y, dz = q.z - own.z;
-    const float w = basis_f32(dx, dy, dz, inv_re_f, b);
+    const float w = basis_f32(dx, dy, dz, inv_re, b);
     const float s2 = b[3] + b[4] + b[5];
     if (w > 0.0f && s2 > 0.0f) {
       const double pj = q.w;
@@ -742,7 +741,7 @@ __global__ void __launch_bounds__(kThreads, 6) gradient32_kernel(GatherArgs a, G
     const index_t j = a.wi[o];
     const double4 q = ld4(a.wp, j), nrm = ld4(a.wn, j);
     const double dx = q.x - own.x, dy = q.y - own.y, dz = q.z - own.z;
-    const float w = wscale * basis_f32(dx, dy, dz, inv_re_f, b);
+    const float w = wscale * basis_f32(dx, dy, dz, inv_re, b);
     const float s2 = b[3] + b[4] + b[5];
     const float nxf = static_cast<float>(nrm.x), nyf = static_cast<float>(nrm.y), nzf = static_cast<float>(nrm.z);
     if (w > 0.0f && s2 > 0.0f) {

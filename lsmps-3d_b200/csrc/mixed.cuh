@@ -27,14 +27,21 @@ inline MixedRows mixed_rows_of(const lsmps_ctx* ctx, int kind) {
                    ctx->mixed_count ? ctx->mixed_count + kind : nullptr};
 }
 
-// FP32 geometry of one neighbour from the FP64 coordinate difference:
-// s = d / r_e rounded once to FP32, w = 1 - |s| (0 outside the support) and
-// the Type-A basis of s.  Returns w.
-__device__ __forceinline__ float basis_f32(double dx, double dy, double dz, float inv_re, float b[9]) {
-  const float sx = static_cast<float>(dx) * inv_re;
-  const float sy = static_cast<float>(dy) * inv_re;
-  const float sz = static_cast<float>(dz) * inv_re;
-  const float w = 1.0f - sqrtf(fmaf(sx, sx, fmaf(sy, sy, sz * sz)));
+// FP32 geometry of one neighbour from the FP64 coordinate difference d:
+// s = d / r_e rounded to FP32, the Type-A basis of s, and the weight
+// w = 1 - |s| (0 outside the support).  The weight is formed as
+// (1 - |s|^2) / (1 + |s|) with |s|^2 and 1 - |s|^2 in FP64: for a neighbour
+// near the edge of the support 1 - |s| cancels, and from FP32 components it
+// would carry an absolute error of ~1e-7, a large relative error of a small
+// weight (and of the PPE coefficient proportional to it); this form keeps the
+// weight's relative error near FP32 rounding.  Returns w.
+__device__ __forceinline__ float basis_f32(double dx, double dy, double dz, double inv_re, float b[9]) {
+  const float inv_re_f = static_cast<float>(inv_re);
+  const float sx = static_cast<float>(dx) * inv_re_f;
+  const float sy = static_cast<float>(dy) * inv_re_f;
+  const float sz = static_cast<float>(dz) * inv_re_f;
+  const double s2 = fma(dx, dx, fma(dy, dy, dz * dz)) * (inv_re * inv_re);
+  const float w = s2 < 1.0 ? __fdividef(static_cast<float>(1.0 - s2), 1.0f + sqrtf(static_cast<float>(s2))) : 0.0f;
   b[0] = sx;
   b[1] = sy;
   b[2] = sz;
@@ -44,7 +51,7 @@ __device__ __forceinline__ float basis_f32(double dx, double dy, double dz, floa
   b[6] = sx * sy;
   b[7] = sy * sz;
   b[8] = sz * sx;
-  return w > 0.0f ? w : 0.0f;
+  return w;
 }
 
 __device__ __forceinline__ float dot9f(const float a[9], const float b[9]) {

@@ -361,7 +361,6 @@ __device__ __forceinline__ void ppe_row32(const PpeArgs& a, index_t i, int l) {
   __syncwarp(group_mask<G>());
   float b[9];
   const double uxi = a.tvx[i], uyi = a.tvy[i], uzi = a.tvz[i];
-  const float inv_re = static_cast<float>(a.inv_re);
   const float scale = static_cast<float>(2.0 / (a.re * a.re * a.density));
   double dsum = 0.0, diag = 0.0;
   index_t o = nb + l;
@@ -377,7 +376,7 @@ __device__ __forceinline__ void ppe_row32(const PpeArgs& a, index_t i, int l) {
       un = ld4(a.fu, jn);
       if (o + 2 * G < ne) jnn = a.fi[o + 2 * G];
     }
-    const float w = basis_f32(q.x - pi.x, q.y - pi.y, q.z - pi.z, inv_re, b);
+    const float w = basis_f32(q.x - pi.x, q.y - pi.y, q.z - pi.z, a.inv_re, b);
     float off = 0.0f;
     if (w > 0.0f) {
       off = w * dot9f(L, b) * scale;
@@ -397,7 +396,7 @@ __device__ __forceinline__ void ppe_row32(const PpeArgs& a, index_t i, int l) {
   for (index_t o = a.wo[i] + l; o < we; o += G) {
     const index_t j = a.wi[o];
     const double4 q = ld4(a.wp, j), u = ld4(a.wu, j), nrm = ld4(a.wn, j);
-    const float w = basis_f32(q.x - pi.x, q.y - pi.y, q.z - pi.z, inv_re, b);
+    const float w = basis_f32(q.x - pi.x, q.y - pi.y, q.z - pi.z, a.inv_re, b);
     if (w <= 0.0f) continue;
     const float dux = static_cast<float>(u.x - uxi), duy = static_cast<float>(u.y - uyi),
                 duz = static_cast<float>(u.z - uzi);

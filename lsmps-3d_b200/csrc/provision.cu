@@ -147,7 +147,6 @@ __global__ void __launch_bounds__(kThreads, 8) laplacian32_kernel(LaplacianArgs 
   float* L = s_L[threadIdx.x / G];
   for (int c = l; c < 9; c += G) L[c] = rows.f32[static_cast<size_t>(i) * 36 + c];
   __syncwarp(group_mask<G>());
-  const float inv_re = static_cast<float>(a.inv_re);
   float b[9];
   double cx = 0.0, cy = 0.0, cz = 0.0;
   const index_t fe = a.fo[i + 1];
@@ -163,7 +162,7 @@ __global__ void __launch_bounds__(kThreads, 8) laplacian32_kernel(LaplacianArgs 
       un = ld4(a.fv, jn);
       if (o + 2 * G < fe) jnn = a.fi[o + 2 * G];
     }
-    const float w = basis_f32(q.x - pi.x, q.y - pi.y, q.z - pi.z, inv_re, b);
+    const float w = basis_f32(q.x - pi.x, q.y - pi.y, q.z - pi.z, a.inv_re, b);
     if (w <= 0.0f) continue;
     const double s = static_cast<double>(w * dot9f(L, b));
     cx = fma(s, u.x - ui.x, cx);
@@ -176,7 +175,7 @@ __global__ void __launch_bounds__(kThreads, 8) laplacian32_kernel(LaplacianArgs 
     const index_t j = a.wi[o];
     const double4 q = ld4(a.wp, j);
     const double4 u = ld4(a.wv, j);
-    const float w = wall_scale * basis_f32(q.x - pi.x, q.y - pi.y, q.z - pi.z, inv_re, b);
+    const float w = wall_scale * basis_f32(q.x - pi.x, q.y - pi.y, q.z - pi.z, a.inv_re, b);
     if (w <= 0.0f) continue;
     const double s = static_cast<double>(w * dot9f(L, b));
     cx = fma(s, u.x - ui.x, cx);

@@ -85,6 +85,14 @@ def kernel_bytes(nf: int, nw: int, kf: int, kw: int, c: int, s: int = 8) -> dict
             out[f"laplacian_kernel<{m}, {g}>"] = out[f"laplacian_kernel<{m}>"]
             out[f"gradient_shifting_kernel<{m}, {g}>"] = out[f"gradient_shifting_kernel<{m}>"]
         out[f"smooth_kernel<{g}>"] = out["smooth_kernel"]
+    # the mixed form's FP32-arithmetic kernels read and write what the mixed
+    # lane kernels do (their FP64 list passes touch only the few FP64-route
+    # particles)
+    for g in (1, 2, 4):
+        out[f"laplacian32_kernel<{g}>"] = out["laplacian_kernel<true>"]
+        out[f"gradient32_kernel<{g}>"] = out["gradient_shifting_kernel<true>"]
+    for g in (4, 8, 16):
+        out[f"ppe32_kernel<{g}>"] = out[f"ppe_lanes_kernel<{g}, true>"]
     out["classify_kernel"] = rows + pos_f + 2 * pos_w + 4 * nf
     out["expand_kernel"] = 4 * (nf + 1) + 4 * kf + 8 * nf
     count_fluid = 2 * pos_f + 8 * c + 4 * nf + 4 * nf

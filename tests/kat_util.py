@@ -81,6 +81,25 @@ def vec_err(g: dict, o: dict, comps, extra_scale: dict | None = None):
     return {c: rel_err(g[c], o[c], scale=scale if scale > 0 else None) for c in comps}
 
 
+EPS64 = 2.0 ** -52
+
+
+def inverse_err_over_kappa(got, ref, trace, reg):
+    """Per-particle error of 9 x 9 moment inverses (rows of 81 entries)
+    against a reference, max |dX| / max |X|, divided by 2^-52 kappa_est with
+    kappa_est = (trace + 9 reg) ||X||_F, an upper bound of the 2-norm
+    condition number within a factor of 27 (trace = the moment trace before
+    regularisation, reg = the regularisation added to each diagonal entry).
+    Rounding-level agreement reads O(1) whatever the conditioning."""
+    g = np.asarray(got, dtype=np.float64).reshape(-1, 81)
+    r = np.asarray(ref, dtype=np.float64).reshape(-1, 81)
+    if r.shape[0] == 0:
+        return 0.0
+    per = np.max(np.abs(g - r), axis=1) / np.max(np.abs(r), axis=1)
+    kappa = (np.asarray(trace) + 9.0 * np.asarray(reg)) * np.sqrt(np.einsum("ij,ij->i", r, r))
+    return float(np.max(per / (EPS64 * kappa)))
+
+
 def coef_rel_err(values, ref_values, floor_frac=1e-4):
     """Per-coefficient relative error of a matrix's values against a
     reference: max |a - r| / max(|r|, floor), floor = floor_frac times the

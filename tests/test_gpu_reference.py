@@ -20,11 +20,18 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 import reference as ref_mod  # noqa: E402
 
-from kat_util import rel_err, vec_err  # noqa: E402
+from kat_util import inverse_err_over_kappa, rel_err, vec_err  # noqa: E402
 
 if not ref_mod.available():
     pytest.skip("oracle/_ref/libref_lsmps.so not built (the reference sources are needed to build it)",
                 allow_module_level=True)
+
+# Floating outputs against the reference's CUDA path: within 1e-10 (measured
+# at most 5e-12); moment inverses (ours: in-register Cholesky, the
+# reference's: cuSOLVER potrf/potrs) within INVERSE_KAPPA_FACTOR * 2^-52 *
+# kappa_est per particle.
+PLAIN_RTOL = 1e-10
+INVERSE_KAPPA_FACTOR = 8.0
 
 CASES = [
     ("hydrostatic", dict(n=20, l0=0.01)),
@@ -84,10 +91,12 @@ def test_stages_against_reference_cuda(pkg, device_api, name, kw):
         gi = gm["inverse_matrices"].reshape(-1, 81)[ok]
         hi = hm["inverse_matrices"].reshape(-1, 81)[ok]
         per = np.max(np.abs(gi - hi), axis=1) / np.max(np.abs(hi), axis=1)
-        print(f"{name} kind {kind} vs reference cuSOLVER inverse: max rel {per.max():.3e}")
-        assert per.max() < 1e-6
+        ek = inverse_err_over_kappa(gi, hi, hm["moment_trace"][ok], hm["regularization_added"][ok])
+        print(f"{name} kind {kind} vs reference cuSOLVER inverse: max rel {per.max():.3e}, max over eps kappa "
+              f"{ek:.3f}")
+        assert ek < INVERSE_KAPPA_FACTOR
     for comp in ("vx", "vy", "vz"):
-        assert rel_err(dev.numpy("temporary_velocity")[comp], host.temporary_velocity[comp]) < 1e-9
+        assert rel_err(dev.numpy("temporary_velocity")[comp], host.temporary_velocity[comp]) < PLAIN_RTOL
         assert rel_err(dev.numpy("temporary_wall_velocity")[comp], host.temporary_wall_velocity[comp]) == 0.0
 
     # PPE rows
@@ -104,7 +113,7 @@ def test_stages_against_reference_cuda(pkg, device_api, name, kw):
         b = host.ppe[k][:nnz_written] if k == "values" else host.ppe[k]
         e = rel_err(a, b)
         print(f"{name} ppe {k} vs reference: max rel {e:.3e}")
-        assert e < 1e-6, k
+        assert e < PLAIN_RTOL, k
 
     # correction
     ref.correction()
@@ -116,7 +125,7 @@ def test_stages_against_reference_cuda(pkg, device_api, name, kw):
             "pressure": rel_err(f["pressure"], host.fluid["pressure"])}
     for comp, e in errs.items():
         print(f"{name} corrected {comp} vs reference: max rel {e:.3e}")
-        assert e < 1e-6, comp
+        assert e < PLAIN_RTOL, comp
 
     # neighbour rebuild on the moved particles
     ref.rebuild()
