@@ -691,6 +691,55 @@ lsmps_status lsmps_operators_backward(lsmps_ctx* ctx, const lsmps_fluid* fluid, 
                                       const lsmps_params* params, const double* f, const lsmps_vector* v,
                                       const lsmps_operator_out* cotangent, const double* inverse, double* f_bar,
                                       const lsmps_vector* v_bar, const lsmps_vector* x_bar);
+/* The step's operators with their wall terms, as a differentiable pair (no
+ * counterpart in the reference).  Per fluid particle i over its fluid and
+ * wall CSR rows, with the velocity Dirichlet-A moment matrix M_v (wall
+ * samples lambda_w w b b^T) and the pressure Neumann-A matrix M_p (wall
+ * terms lambda_w w q q^T with the Neumann vector q), both regularised as
+ * the step does (moment_matrix.cu:177-201, 254-309):
+ *   lap_*        velocity Laplacian of u, wall samples lambda_w w b (u_w - u_i)
+ *                (explicit_update.cu:178-248)
+ *   divergence   divergence of u with M_v (ppe_matrix.cu:355-361); 0 on the
+ *                Dirichlet rows (Surface and Splash)
+ *   grad_*       pressure gradient of p with M_p and the wall source
+ *                lambda_w w q (r_e rho g.n) (pressure_correction.cu:200-276);
+ *                0 for Splash
+ *   ppe_*        the PPE rows of the pressure Laplacian row of M_p, Dirichlet
+ *                rows for Surface and Splash (ppe_matrix.cu:243-370);
+ *                ppe_rhs = divergence / dt - wall_rhs
+ *   wall_rhs     the wall Neumann term sum 2 lambda_w w (g.n) (L.q) / r_e
+ * Inputs: fluid x, y, z, vx, vy, vz (u), pressure (p) and surface_type
+ * (NULL: all Inner); walls x, y, z, vx, vy, vz (u_w) and normals.  Labels,
+ * walls and both CSR tables are held fixed under differentiation.  Any
+ * output pointer may be NULL (not written; in the backward: zero cotangent;
+ * ppe_row_offsets / ppe_col_indices are not read). */
+typedef struct lsmps_step_operator_out {
+  size_t count;
+  double* lap_x;
+  double* lap_y;
+  double* lap_z;
+  double* divergence;
+  double* grad_x;
+  double* grad_y;
+  double* grad_z;
+  int32_t* ppe_row_offsets;
+  int32_t* ppe_col_indices;
+  double* ppe_values;
+  double* ppe_rhs;
+  double* wall_rhs;
+} lsmps_step_operator_out;
+lsmps_status lsmps_step_operators_forward(lsmps_ctx* ctx, const lsmps_fluid* fluid, const lsmps_walls* walls,
+                                          const lsmps_csr* fn, const lsmps_csr* wn, const lsmps_params* params,
+                                          const lsmps_step_operator_out* out);
+/* Gradients of L with respect to u (u_bar), p (p_bar) and the fluid
+ * positions (x_bar), each optional and overwritten; the inverses are
+ * recomputed from the positions.  Deterministic or atomic as set by
+ * lsmps_ctx_set_adjoint_atomic (the wall terms are the owner's own and need
+ * neither). */
+lsmps_status lsmps_step_operators_backward(lsmps_ctx* ctx, const lsmps_fluid* fluid, const lsmps_walls* walls,
+                                           const lsmps_csr* fn, const lsmps_csr* wn, const lsmps_params* params,
+                                           const lsmps_step_operator_out* cotangent, const lsmps_vector* u_bar,
+                                           double* p_bar, const lsmps_vector* x_bar);
 /* Form of lsmps_operators_backward (no counterpart in the reference).
  * 0 (default): deterministic -- the CSR is transposed (entries sorted stably
  * by neighbour) and every particle gathers the terms of its own row and of

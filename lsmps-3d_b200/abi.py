@@ -218,6 +218,14 @@ class OperatorOut(Structure):
     ]
 
 
+class StepOperatorOut(Structure):
+    _fields_ = [("count", c_size_t)] + [
+        (n, c_void_p)
+        for n in ("lap_x", "lap_y", "lap_z", "divergence", "grad_x", "grad_y", "grad_z", "ppe_row_offsets",
+                  "ppe_col_indices", "ppe_values", "ppe_rhs", "wall_rhs")
+    ]
+
+
 class StepState(Structure):
     _fields_ = [
         ("fluid", Fluid),
@@ -365,6 +373,10 @@ _SIGNATURES = {
                                         c_void_p]),
     "lsmps_operators_backward": (c_int, [c_void_p, P(Fluid), P(Csr), P(Params), c_void_p, P(Vector), P(OperatorOut),
                                          c_void_p, c_void_p, P(Vector), P(Vector)]),
+    "lsmps_step_operators_forward": (c_int, [c_void_p, P(Fluid), P(Walls), P(Csr), P(Csr), P(Params),
+                                             P(StepOperatorOut)]),
+    "lsmps_step_operators_backward": (c_int, [c_void_p, P(Fluid), P(Walls), P(Csr), P(Csr), P(Params),
+                                              P(StepOperatorOut), P(Vector), c_void_p, P(Vector)]),
 }
 
 

@@ -43,6 +43,7 @@
 // the result depends on the atomics' order at the rounding level).
 #include <algorithm>
 
+#include "adjoint.cuh"
 #include "cells.cuh"
 #include "impl.cuh"
 #include "packed.cuh"
@@ -75,39 +76,6 @@ struct OpsArgs {
   double* vbar[3];
   double* xbar[3];
 };
-
-__device__ __forceinline__ void basis_div(double dx, double dy, double dz, double inv_re, double b[9], double s[3]) {
-  s[0] = dx * inv_re;
-  s[1] = dy * inv_re;
-  s[2] = dz * inv_re;
-  b[0] = s[0];
-  b[1] = s[1];
-  b[2] = s[2];
-  b[3] = s[0] * s[0];
-  b[4] = s[1] * s[1];
-  b[5] = s[2] * s[2];
-  b[6] = s[0] * s[1];
-  b[7] = s[1] * s[2];
-  b[8] = s[2] * s[0];
-}
-
-__device__ __forceinline__ double dot9(const double* a, const double* b) {
-  double v = 0.0;
-#pragma unroll
-  for (int k = 0; k < 9; ++k) v = fma(a[k], b[k], v);
-  return v;
-}
-
-// y = X r for the column-major symmetric 9x9 X.
-__device__ __forceinline__ void apply(const double* __restrict__ x, const double r[9], double y[9]) {
-#pragma unroll
-  for (int a = 0; a < 9; ++a) y[a] = 0.0;
-#pragma unroll
-  for (int c = 0; c < 9; ++c) {
-#pragma unroll
-    for (int a = 0; a < 9; ++a) y[a] = fma(x[a + c * 9], r[c], y[a]);
-  }
-}
 
 __device__ __forceinline__ double opt(const double* p, index_t i) { return p ? p[i] : 0.0; }
 
@@ -383,26 +351,6 @@ __global__ void __launch_bounds__(kThreads) ops_adjoint_scatter_kernel(OpsArgs a
     if (phibar[p]) atomicAdd(&phibar[p][i], own_phi[p]);
 }
 
-// Transpose of the CSR, step 1: for every entry o of row i, key = its
-// neighbour (indices outside [0, n) become the sentinel n), value = o, and
-// owner[o] = i.  Eight lanes per row.
-__global__ void __launch_bounds__(kThreads) transpose_keys_kernel(const index_t* __restrict__ fo,
-                                                                  const index_t* __restrict__ fi, index_t n,
-                                                                  index_t* __restrict__ keys,
-                                                                  index_t* __restrict__ vals,
-                                                                  index_t* __restrict__ owner) {
-  const index_t i = static_cast<index_t>((static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x) / 8);
-  const int lane = threadIdx.x & 7;
-  if (i >= n) return;
-  const index_t ne = fo[i + 1];
-  for (index_t o = fo[i] + lane; o < ne; o += 8) {
-    const index_t j = fi[o];
-    keys[o] = (j >= 0 && j < n) ? j : n;
-    vals[o] = o;
-    owner[o] = i;
-  }
-}
-
 // Deterministic form: particle j sums, in a fixed order, the terms of its
 // incoming entries (the transpose row [tb[j], te[j]) of entry offsets,
 // ascending) and then subtracts those of its own row, and writes its
@@ -452,6 +400,80 @@ __global__ void __launch_bounds__(kThreads) ops_adjoint_gather_kernel(OpsArgs a,
 }
 
 }  // namespace
+
+// Transpose of the CSR, step 1: for every entry o of row i, key = its
+// neighbour (indices outside [0, n) become the sentinel n), value = o, and
+// owner[o] = i.  Eight lanes per row.
+__global__ void __launch_bounds__(kAdjThreads) transpose_keys_kernel(const index_t* __restrict__ fo,
+                                                                  const index_t* __restrict__ fi, index_t n,
+                                                                  index_t* __restrict__ keys,
+                                                                  index_t* __restrict__ vals,
+                                                                  index_t* __restrict__ owner) {
+  const index_t i = static_cast<index_t>((static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x) / 8);
+  const int lane = threadIdx.x & 7;
+  if (i >= n) return;
+  const index_t ne = fo[i + 1];
+  for (index_t o = fo[i] + lane; o < ne; o += 8) {
+    const index_t j = fi[o];
+    keys[o] = (j >= 0 && j < n) ? j : n;
+    vals[o] = o;
+    owner[o] = i;
+  }
+}
+
+lsmps_status build_csr_transpose(lsmps_ctx* ctx, Scratch& scratch, const lsmps_csr& fn, index_t n,
+                                 CsrTranspose* out) {
+  index_t total = 0;
+  if (cudaMemcpyAsync(&total, fn.offsets + n, sizeof(index_t), cudaMemcpyDeviceToHost, ctx->stream) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+    return fail(ctx, LSMPS_CUDA_ERROR, "reading the neighbour count failed");
+  if (total < 0 || static_cast<size_t>(total) > fn.neighbor_count)
+    return fail(ctx, LSMPS_INVALID_ARGUMENT, "neighbour table offsets exceed its capacity");
+  const size_t k = static_cast<size_t>(total);
+  const int tiles = total ? div_up(total, kSortTile) : 0;
+  const size_t hist_entries = static_cast<size_t>(tiles) * kRadixBins;
+  const size_t bytes = 5 * (k * sizeof(index_t) + 256) + 2 * ((n + 1) * sizeof(index_t) + 256) +
+                       hist_entries * sizeof(index_t) + 256 + 4 * scan_scratch_bytes(hist_entries + 1) + 4096;
+  if (!scratch.reserve(bytes)) return fail(ctx, LSMPS_CUDA_ERROR, "CSR transpose scratch allocation failed");
+  index_t* keys = scratch.take<index_t>(k + 1);
+  index_t* vals = scratch.take<index_t>(k + 1);
+  index_t* alt_keys = scratch.take<index_t>(k + 1);
+  index_t* alt_vals = scratch.take<index_t>(k + 1);
+  index_t* owner = scratch.take<index_t>(k + 1);
+  index_t* tb = scratch.take<index_t>(static_cast<size_t>(n) + 1);
+  index_t* te = scratch.take<index_t>(static_cast<size_t>(n) + 1);
+  index_t* hist = scratch.take<index_t>(hist_entries + 1);
+  if (!keys || !vals || !alt_keys || !alt_vals || !owner || !tb || !te || !hist)
+    return fail(ctx, LSMPS_CUDA_ERROR, "CSR transpose scratch exhausted");
+  cudaMemsetAsync(tb, 0xff, (static_cast<size_t>(n) + 1) * sizeof(index_t), ctx->stream);
+  cudaMemsetAsync(te, 0xff, (static_cast<size_t>(n) + 1) * sizeof(index_t), ctx->stream);
+  out->total = total;
+  out->tb = tb;
+  out->te = te;
+  out->tsrc = vals;
+  out->owner = owner;
+  if (total == 0) return check_launch(ctx, "CSR transpose");
+  launch(ctx, transpose_keys_kernel, dim3(div_up(static_cast<long long>(n) * 8, kAdjThreads)), dim3(kAdjThreads),
+         0, fn.offsets, fn.indices, n, keys, vals, owner);
+  const int passes = (key_bits(static_cast<long long>(n) + 1) + kRadixBits - 1) / kRadixBits;
+  index_t *k0 = keys, *v0 = vals, *k1 = alt_keys, *v1 = alt_vals;
+  for (int p = 0; p < passes; ++p) {
+    const int shift = p * kRadixBits;
+    launch(ctx, radix_hist_kernel, dim3(tiles), dim3(kSortThreads), 0, static_cast<const index_t*>(k0), total,
+           shift, hist, tiles);
+    lsmps_status st = exclusive_scan_i32(ctx, scratch, hist, hist, hist_entries, nullptr, nullptr);
+    if (st) return st;
+    launch(ctx, radix_scatter_kernel, dim3(tiles), dim3(kSortThreads), 0, static_cast<const index_t*>(k0),
+           static_cast<const index_t*>(v0), k1, v1, total, shift, static_cast<const index_t*>(hist), tiles);
+    std::swap(k0, k1);
+    std::swap(v0, v1);
+  }
+  const int range_blocks = static_cast<int>(std::min<long long>(div_up(total, 256), ctx->sm_count * 8LL));
+  launch(ctx, ranges_kernel, dim3(range_blocks), dim3(256), 0, static_cast<const index_t*>(k0), total, tb, te);
+  out->tsrc = v0;
+  return check_launch(ctx, "CSR transpose");
+}
 
 // Context scratch of the operator pair: the fluid-only inverse, its trace /
 // regularisation / info, and the backward stash.
@@ -525,64 +547,16 @@ lsmps_status moments(lsmps_ctx* ctx, const lsmps_fluid& fl, const lsmps_csr& fn,
   return st;
 }
 
-// The deterministic backward after the stash pass: the CSR's transpose by a
-// stable radix sort of the entries by neighbour (cells.cuh), its row ranges,
-// then the gather.  Reads the entry count back to size the sort (the call
-// allocates its scratch, so it is not made under stream capture anyway).
+// The deterministic backward after the stash pass: the CSR's transpose,
+// then the gather.
 lsmps_status transpose_and_gather(lsmps_ctx* ctx, const lsmps_csr& fn, const OpsArgs& a) {
-  const index_t n = a.n;
-  index_t total = 0;
-  if (cudaMemcpyAsync(&total, fn.offsets + n, sizeof(index_t), cudaMemcpyDeviceToHost, ctx->stream) !=
-          cudaSuccess ||
-      cudaStreamSynchronize(ctx->stream) != cudaSuccess)
-    return fail(ctx, LSMPS_CUDA_ERROR, "reading the neighbour count failed");
-  if (total < 0 || static_cast<size_t>(total) > fn.neighbor_count)
-    return fail(ctx, LSMPS_INVALID_ARGUMENT, "neighbour table offsets exceed its capacity");
-  const size_t k = static_cast<size_t>(total);
-  const int tiles = total ? div_up(total, kSortTile) : 0;
-  const size_t hist_entries = static_cast<size_t>(tiles) * kRadixBins;
   Scratch scratch(ctx);
-  const size_t bytes = 5 * (k * sizeof(index_t) + 256) + 2 * ((n + 1) * sizeof(index_t) + 256) +
-                       hist_entries * sizeof(index_t) + 256 + 4 * scan_scratch_bytes(hist_entries + 1) + 4096;
-  if (!scratch.reserve(bytes)) return fail(ctx, LSMPS_CUDA_ERROR, "adjoint transpose scratch allocation failed");
-  index_t* keys = scratch.take<index_t>(k + 1);
-  index_t* vals = scratch.take<index_t>(k + 1);
-  index_t* alt_keys = scratch.take<index_t>(k + 1);
-  index_t* alt_vals = scratch.take<index_t>(k + 1);
-  index_t* owner = scratch.take<index_t>(k + 1);
-  index_t* tb = scratch.take<index_t>(static_cast<size_t>(n) + 1);
-  index_t* te = scratch.take<index_t>(static_cast<size_t>(n) + 1);
-  index_t* hist = scratch.take<index_t>(hist_entries + 1);
-  if (!keys || !vals || !alt_keys || !alt_vals || !owner || !tb || !te || !hist)
-    return fail(ctx, LSMPS_CUDA_ERROR, "adjoint transpose scratch exhausted");
-  cudaMemsetAsync(tb, 0xff, (static_cast<size_t>(n) + 1) * sizeof(index_t), ctx->stream);
-  cudaMemsetAsync(te, 0xff, (static_cast<size_t>(n) + 1) * sizeof(index_t), ctx->stream);
-  if (total > 0) {
-    launch(ctx, transpose_keys_kernel, dim3(div_up(static_cast<long long>(n) * 8, kThreads)), dim3(kThreads), 0,
-           a.fo, a.fi, n, keys, vals, owner);
-    const int passes = (key_bits(static_cast<long long>(n) + 1) + kRadixBits - 1) / kRadixBits;
-    index_t *k0 = keys, *v0 = vals, *k1 = alt_keys, *v1 = alt_vals;
-    for (int p = 0; p < passes; ++p) {
-      const int shift = p * kRadixBits;
-      launch(ctx, radix_hist_kernel, dim3(tiles), dim3(kSortThreads), 0, static_cast<const index_t*>(k0), total,
-             shift, hist, tiles);
-      lsmps_status st = exclusive_scan_i32(ctx, scratch, hist, hist, hist_entries, nullptr, nullptr);
-      if (st) return st;
-      launch(ctx, radix_scatter_kernel, dim3(tiles), dim3(kSortThreads), 0, static_cast<const index_t*>(k0),
-             static_cast<const index_t*>(v0), k1, v1, total, shift, static_cast<const index_t*>(hist), tiles);
-      std::swap(k0, k1);
-      std::swap(v0, v1);
-    }
-    const int range_blocks = static_cast<int>(std::min<long long>(div_up(total, 256), ctx->sm_count * 8LL));
-    launch(ctx, ranges_kernel, dim3(range_blocks), dim3(256), 0, static_cast<const index_t*>(k0), total, tb, te);
-    launch(ctx, ops_adjoint_gather_kernel, dim3(div_up(n, kThreads)), dim3(kThreads), 0, a,
-           static_cast<const index_t*>(tb), static_cast<const index_t*>(te), static_cast<const index_t*>(v0),
-           static_cast<const index_t*>(owner));
-  } else {
-    launch(ctx, ops_adjoint_gather_kernel, dim3(div_up(n, kThreads)), dim3(kThreads), 0, a,
-           static_cast<const index_t*>(tb), static_cast<const index_t*>(te), static_cast<const index_t*>(vals),
-           static_cast<const index_t*>(owner));
-  }
+  CsrTranspose tr{};
+  lsmps_status st = build_csr_transpose(ctx, scratch, fn, a.n, &tr);
+  if (st) return st;
+  launch(ctx, ops_adjoint_gather_kernel, dim3(div_up(a.n, kThreads)), dim3(kThreads), 0, a,
+         static_cast<const index_t*>(tr.tb), static_cast<const index_t*>(tr.te), tr.tsrc,
+         static_cast<const index_t*>(tr.owner));
   return check_launch(ctx, "operators backward (transpose and gather)");
 }
 

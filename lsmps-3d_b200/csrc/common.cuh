@@ -209,6 +209,16 @@ struct lsmps_ctx {
   // Backward form: false = transpose + gather (deterministic, the default),
   // true = scatter with FP64 atomics (lsmps_ctx_set_adjoint_atomic).
   bool adjoint_atomic = false;
+  // The step operator pair (step_adjoint.cu): inverses, traces,
+  // regularisations, info and counts of the velocity Dirichlet-A and pressure
+  // Neumann-A kinds, and the backward's stash.
+  double* sop_inverse[2] = {nullptr, nullptr};
+  double* sop_trace[2] = {nullptr, nullptr};
+  double* sop_reg[2] = {nullptr, nullptr};
+  int32_t* sop_info[2] = {nullptr, nullptr};
+  int32_t* sop_count = nullptr;
+  double* sop_stash = nullptr;
+  size_t sop_cap = 0;
 };
 
 namespace lsmps {
@@ -242,6 +252,9 @@ void free_mixed(lsmps_ctx* ctx);
 // Grow / free the operator pair's scratch (adjoint.cu).
 bool ensure_adjoint(lsmps_ctx* ctx, size_t n);
 void free_adjoint(lsmps_ctx* ctx);
+// Grow / free the step operator pair's scratch (step_adjoint.cu).
+bool ensure_step_ops(lsmps_ctx* ctx, size_t n);
+void free_step_ops(lsmps_ctx* ctx);
 
 lsmps_status fail(lsmps_ctx* ctx, lsmps_status st, const char* what);
 lsmps_status check_launch(lsmps_ctx* ctx, const char* what);

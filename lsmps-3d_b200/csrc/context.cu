@@ -220,6 +220,7 @@ void lsmps_ctx_destroy(lsmps_ctx* ctx) {
     if (p) cudaFree(p);
   free_mixed(ctx);
   free_adjoint(ctx);
+  free_step_ops(ctx);
   if (ctx->d_status) cudaFree(ctx->d_status);
   if (ctx->h_status) cudaFreeHost(ctx->h_status);
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);

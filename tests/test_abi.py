@@ -76,12 +76,13 @@ def test_time_state_init(lib, pkg):
 
 STRUCTS = ["lsmps_fluid", "lsmps_walls", "lsmps_grid", "lsmps_cells", "lsmps_csr", "lsmps_vector",
            "lsmps_surface_diagnostics", "lsmps_moment", "lsmps_csr_matrix", "lsmps_ppe", "lsmps_params",
-           "lsmps_step_state", "lsmps_operator_out", "lsmps_solver_options", "lsmps_solver_report",
-           "lsmps_time_limits", "lsmps_time_state"]
+           "lsmps_step_state", "lsmps_operator_out", "lsmps_step_operator_out", "lsmps_solver_options",
+           "lsmps_solver_report", "lsmps_time_limits", "lsmps_time_state"]
 PY = {"lsmps_fluid": "Fluid", "lsmps_walls": "Walls", "lsmps_grid": "Grid", "lsmps_cells": "Cells",
       "lsmps_csr": "Csr", "lsmps_vector": "Vector", "lsmps_surface_diagnostics": "SurfaceDiagnostics",
       "lsmps_moment": "Moment", "lsmps_csr_matrix": "CsrMatrix", "lsmps_ppe": "Ppe", "lsmps_params": "Params",
       "lsmps_step_state": "StepState", "lsmps_operator_out": "OperatorOut",
+      "lsmps_step_operator_out": "StepOperatorOut",
       "lsmps_solver_options": "SolverOptions", "lsmps_solver_report": "SolverReport",
       "lsmps_time_limits": "TimeLimits", "lsmps_time_state": "TimeState"}
 
