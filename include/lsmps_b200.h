@@ -641,6 +641,23 @@ void lsmps_batch_destroy(lsmps_batch* batch);
 lsmps_status lsmps_batch_add(lsmps_batch* batch, const lsmps_params* params, const lsmps_step_state* state);
 int lsmps_batch_size(lsmps_batch* batch);
 lsmps_status lsmps_batch_capture(lsmps_batch* batch, int precision, int autotune_repeats);
+/* Form of the graph, chosen before capture (no counterpart in the reference).
+ * 1 (default): merged -- when the boxes differ only in their cell grids
+ * (origin, dims), all boxes are stepped as one particle set: each launch
+ * gathers the boxes' particle state (fluid SoA, labels, pressure input,
+ * walls) into the batch's merged buffers, runs one lsmps_step on the merged
+ * set (every kernel one grid-wide launch over all boxes; the cell hash and
+ * the neighbour search keep each particle on its own box's grid), and
+ * scatters every output back into the boxes' views.  The merged neighbour
+ * tables and cell lists stay the batch's own between launches (capture builds
+ * them from the boxes' positions; each launch ends with their rebuild): the
+ * boxes' copies are outputs, and changes a caller makes to them are not read.
+ * Boxes whose other parameters differ fall back to form 0.
+ * 0: one lsmps_step per box on the worker streams.
+ * Either way each box's results equal its own lsmps_step bit for bit.
+ * lsmps_batch_merged reports the form the last capture used. */
+lsmps_status lsmps_batch_set_merged(lsmps_batch* batch, int on);
+int lsmps_batch_merged(lsmps_batch* batch);
 /* stream: where the graph is launched (NULL: the batch's origin stream). */
 lsmps_status lsmps_batch_launch(lsmps_batch* batch, void* stream);
 lsmps_status lsmps_batch_synchronize(lsmps_batch* batch);

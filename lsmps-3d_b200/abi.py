@@ -361,6 +361,8 @@ _SIGNATURES = {
     ),
     "lsmps_step": (c_int, [c_void_p, P(Params), P(StepState)]),
     "lsmps_batch_create": (c_int, [c_int, c_int, P(c_void_p)]),
+    "lsmps_batch_set_merged": (c_int, [c_void_p, c_int]),
+    "lsmps_batch_merged": (c_int, [c_void_p]),
     "lsmps_batch_destroy": (None, [c_void_p]),
     "lsmps_batch_add": (c_int, [c_void_p, P(Params), P(StepState)]),
     "lsmps_batch_size": (c_int, [c_void_p]),

@@ -256,6 +256,16 @@ class Batch:
         self.boxes.append((b, params, state))
         self.check(_lib.lsmps_batch_add(self.h, r(params), r(state)))
 
+    def set_merged(self, on: bool) -> None:
+        """Merged form (all boxes as one particle set; the default) or one
+        step per box on the worker streams; chosen before capture."""
+        self.check(_lib.lsmps_batch_set_merged(self.h, 1 if on else 0))
+
+    @property
+    def merged(self) -> bool:
+        """Whether the last capture used the merged form."""
+        return bool(_lib.lsmps_batch_merged(self.h))
+
     def capture(self, precision: int = abi.PRECISION_MIXED, autotune_repeats: int = 0) -> None:
         self.check(_lib.lsmps_batch_capture(self.h, precision, autotune_repeats))
 

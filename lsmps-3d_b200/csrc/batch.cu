@@ -18,6 +18,7 @@
 #include <algorithm>
 #include <vector>
 
+#include "batch_impl.cuh"
 #include "impl.cuh"
 
 struct lsmps_batch {
@@ -32,6 +33,11 @@ struct lsmps_batch {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   std::string last_error;
+  // The merged form (batch_merged.cu): used when requested (the default) and
+  // the boxes differ only in their grids.
+  bool want_merged = true;
+  bool merged_active = false;
+  lsmps::MergedBatch merged;
 };
 
 namespace {
@@ -46,6 +52,37 @@ void release_graph(lsmps_batch* b) {
   if (b->graph) cudaGraphDestroy(b->graph);
   b->exec = nullptr;
   b->graph = nullptr;
+  if (b->merged_active) lsmps::release_merged(b->merged);
+  b->merged_active = false;
+}
+
+// The merged form: one particle set for all boxes, stepped on the origin
+// stream (gather, lsmps_step, scatter) and captured as the batch's graph.
+lsmps_status capture_merged(lsmps_batch* b, int precision, int autotune_repeats) {
+  std::string err;
+  lsmps_status st = lsmps::prepare_merged(b->merged, b->device, b->origin, b->params, b->states, precision,
+                                          autotune_repeats, err);
+  if (st) return batch_fail(b, st, err);
+  b->merged_active = true;
+  if (cudaStreamSynchronize(b->origin) != cudaSuccess) return batch_fail(b, LSMPS_CUDA_ERROR, "pre-capture sync");
+  if (cudaStreamBeginCapture(b->origin, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+    return batch_fail(b, LSMPS_CUDA_ERROR, "begin capture failed");
+  st = lsmps::queue_merged(b->merged, b->origin, err);
+  cudaGraph_t graph = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(b->origin, &graph);
+  if (e != cudaSuccess || st) {
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();
+    return st ? batch_fail(b, st, err)
+              : batch_fail(b, LSMPS_CUDA_ERROR, std::string("end capture: ") + cudaGetErrorString(e));
+  }
+  b->graph = graph;
+  if (cudaGraphInstantiate(&b->exec, b->graph, 0) != cudaSuccess) {
+    cudaGetLastError();
+    release_graph(b);
+    return batch_fail(b, LSMPS_CUDA_ERROR, "graph instantiation failed");
+  }
+  return LSMPS_OK;
 }
 
 }  // namespace
@@ -110,6 +147,7 @@ extern "C" lsmps_status lsmps_batch_capture(lsmps_batch* b, int precision, int a
   if (precision != LSMPS_PRECISION_PLAIN && precision != LSMPS_PRECISION_MIXED) return LSMPS_INVALID_ARGUMENT;
   if (cudaSetDevice(b->device) != cudaSuccess) return LSMPS_CUDA_ERROR;
   release_graph(b);
+  if (b->want_merged && lsmps::boxes_mergeable(b->params)) return capture_merged(b, precision, autotune_repeats);
   const int S = static_cast<int>(b->streams.size());
   // Reserve every worker context for its largest box, and tune its knobs on
   // that box, before anything is captured.
@@ -181,6 +219,13 @@ extern "C" lsmps_status lsmps_batch_synchronize(lsmps_batch* b) {
   if (!b) return LSMPS_INVALID_ARGUMENT;
   if (cudaStreamSynchronize(b->origin) != cudaSuccess) return batch_fail(b, LSMPS_CUDA_ERROR, "synchronize failed");
   lsmps_status first = LSMPS_OK;
+  if (b->merged_active && b->merged.ctx) {
+    const lsmps_status st = lsmps_ctx_synchronize(b->merged.ctx);
+    if (st) {
+      first = st;
+      b->last_error = lsmps_ctx_last_error(b->merged.ctx);
+    }
+  }
   for (lsmps_ctx* c : b->ctxs) {
     const lsmps_status st = lsmps_ctx_synchronize(c);
     if (st && !first) {
@@ -194,3 +239,12 @@ extern "C" lsmps_status lsmps_batch_synchronize(lsmps_batch* b) {
 extern "C" void* lsmps_batch_stream(lsmps_batch* b) { return b ? static_cast<void*>(b->origin) : nullptr; }
 
 extern "C" const char* lsmps_batch_last_error(lsmps_batch* b) { return b ? b->last_error.c_str() : ""; }
+
+extern "C" lsmps_status lsmps_batch_set_merged(lsmps_batch* b, int on) {
+  if (!b || (on != 0 && on != 1)) return LSMPS_INVALID_ARGUMENT;
+  if (b->graph) return batch_fail(b, LSMPS_INVALID_ARGUMENT, "the form is chosen before capture");
+  b->want_merged = on != 0;
+  return LSMPS_OK;
+}
+
+extern "C" int lsmps_batch_merged(lsmps_batch* b) { return b && b->merged_active ? 1 : 0; }

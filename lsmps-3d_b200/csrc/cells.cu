@@ -59,6 +59,33 @@ __global__ void hash_kernel(const double* __restrict__ x, const double* __restri
   }
 }
 
+// hash_kernel for a merged batch: particle t belongs to the box whose range
+// of this set holds it (field 1: fluid, 2: walls) and is hashed on that box's
+// grid (cell size shared), offset by the box's first global cell.
+__global__ void hash_boxes_kernel(const double* __restrict__ x, const double* __restrict__ y,
+                                  const double* __restrict__ z, index_t n, const BoxGrid* __restrict__ boxes,
+                                  int nbox, int field, double cell_size, index_t* __restrict__ keys,
+                                  index_t* __restrict__ vals, index_t* __restrict__ cell_begin,
+                                  index_t* __restrict__ cell_end, index_t ncell, DeviceStatus* __restrict__ status) {
+  const index_t total = n > ncell ? n : ncell;
+  for (index_t t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    if (t < ncell) {
+      cell_begin[t] = -1;
+      cell_end[t] = -1;
+    }
+    if (t < n) {
+      const BoxGrid& g = boxes[box_of(boxes, nbox, t, field)];
+      bool bad = false;
+      const index_t ix = cell_coord(x[t], g.origin[0], cell_size, g.dims[0], bad);
+      const index_t iy = cell_coord(y[t], g.origin[1], cell_size, g.dims[1], bad);
+      const index_t iz = cell_coord(z[t], g.origin[2], cell_size, g.dims[2], bad);
+      if (bad) raise_flag(status, kFlagNonFinite);
+      keys[t] = g.cell_base + (iz * g.dims[1] + iy) * g.dims[0] + ix;
+      vals[t] = t;
+    }
+  }
+}
+
 // Per-tile histogram of one digit, stored digit-major: hist[d * tiles + tile].
 __global__ void __launch_bounds__(kSortThreads) radix_hist_kernel(const index_t* __restrict__ keys, index_t n,
                                                                   int shift, index_t* __restrict__ hist,
@@ -162,7 +189,7 @@ size_t cell_list_scratch_bytes(size_t n, size_t ncell) {
 
 lsmps_status build_cell_list_impl(lsmps_ctx* ctx, Scratch& scratch, const double* x, const double* y,
                                   const double* z, size_t count, const lsmps_grid& grid,
-                                  const lsmps_cells& cells) {
+                                  const lsmps_cells& cells, const BoxGrid* boxes, int box_field) {
   lsmps_status st = validate_grid(ctx, grid);
   if (st) return st;
   const long long ncell = static_cast<long long>(grid.dims[0]) * grid.dims[1] * grid.dims[2];
@@ -188,8 +215,12 @@ lsmps_status build_cell_list_impl(lsmps_ctx* ctx, Scratch& scratch, const double
   index_t* v1 = (passes & 1) ? cells.sorted_indices : alt_vals;
   const long long work = n > ncell ? n : ncell;
   const int hash_blocks = static_cast<int>(std::min<long long>(div_up(work, 256), ctx->sm_count * 8LL));
-  launch(ctx, hash_kernel, dim3(hash_blocks), dim3(256), 0, x, y, z, n, grid, k0, v0, cells.cell_begin,
-         cells.cell_end, static_cast<index_t>(ncell), ctx->d_status);
+  if (boxes)
+    launch(ctx, hash_boxes_kernel, dim3(hash_blocks), dim3(256), 0, x, y, z, n, boxes, ctx->nbox, box_field,
+           grid.cell_size, k0, v0, cells.cell_begin, cells.cell_end, static_cast<index_t>(ncell), ctx->d_status);
+  else
+    launch(ctx, hash_kernel, dim3(hash_blocks), dim3(256), 0, x, y, z, n, grid, k0, v0, cells.cell_begin,
+           cells.cell_end, static_cast<index_t>(ncell), ctx->d_status);
   if (n == 0) return check_launch(ctx, "cell hash");
   for (int p = 0; p < passes; ++p) {
     const int shift = p * kRadixBits;

@@ -101,6 +101,36 @@ __device__ __forceinline__ void neumann_a(double dx, double dy, double dz, doubl
 
 inline int div_up(long long a, long long b) { return static_cast<int>((a + b - 1) / b); }
 
+// One box of a merged batch (batch.cu): independent particle boxes stepped
+// as one particle set, each with its own cell grid.  Box b's cells are the
+// global cells [cell_base, cell_base + dims product), its fluid particles
+// [fluid_base, next box's), its walls [wall_base, next box's).  The cell
+// hash and the neighbour search of a merged set look each particle's or
+// cell's box up in this table; every other kernel is per particle and needs
+// nothing of it.
+struct BoxGrid {
+  double origin[3];
+  int dims[3];
+  index_t cell_base;
+  index_t fluid_base;
+  index_t wall_base;
+};
+
+// The box holding global cell c (or particle t, with field = the box's first
+// index of that set): the last box whose base is <= the value.
+__device__ __forceinline__ int box_of(const BoxGrid* __restrict__ boxes, int nbox, index_t v, int field) {
+  int lo = 0, hi = nbox - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    const index_t base = field == 0 ? boxes[mid].cell_base : field == 1 ? boxes[mid].fluid_base : boxes[mid].wall_base;
+    if (base <= v)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
 // Lane groups: G consecutive lanes of a warp (G a power of two dividing 32)
 // share one particle.  group_mask names the calling thread's group only, so
 // the shuffles stay valid when other groups of the warp have left.
@@ -209,6 +239,10 @@ struct lsmps_ctx {
   // Backward form: false = transpose + gather (deterministic, the default),
   // true = scatter with FP64 atomics (lsmps_ctx_set_adjoint_atomic).
   bool adjoint_atomic = false;
+  // Merged batch (batch.cu): the boxes' grid table in device memory while
+  // this context steps a merged particle set, else NULL.
+  const lsmps::BoxGrid* boxes = nullptr;
+  int nbox = 0;
   // The step operator pair (step_adjoint.cu): inverses, traces,
   // regularisations, info and counts of the velocity Dirichlet-A and pressure
   // Neumann-A kinds, and the backward's stash.
@@ -301,9 +335,14 @@ lsmps_status exclusive_scan_i32(lsmps_ctx* ctx, Scratch& scratch, const index_t*
 // Cell-list build shared by lsmps_build_cell_list and the neighbour search
 // (cells.cu).
 size_t cell_list_scratch_bytes(size_t n, size_t ncell);
+// boxes (a merged batch's device table, ctx->nbox entries): hash each
+// particle on its box's grid (box_field 1: fluid ranges, 2: wall ranges);
+// grid then only supplies the cell size and the total cell count
+// (dims product).
 lsmps_status build_cell_list_impl(lsmps_ctx* ctx, Scratch& scratch, const double* x, const double* y,
                                   const double* z, size_t count, const lsmps_grid& grid,
-                                  const lsmps_cells& cells);
+                                  const lsmps_cells& cells, const BoxGrid* boxes = nullptr,
+                                  int box_field = 0);
 lsmps_status validate_grid(lsmps_ctx* ctx, const lsmps_grid& grid);
 
 }  // namespace lsmps

@@ -78,7 +78,45 @@ struct CsrArgs {
   // src_sorted[k]), so that staging a cell reads one contiguous range.
   const double4* src_pos;
   DeviceStatus* status;
+  // merged batch (batch.cu): every box's cells and grid, or NULL for one box
+  // on a.grid; the cell size (a.grid.cell_size) is shared by all boxes
+  const BoxGrid* boxes;
+  int nbox;
 };
+
+// A home cell's place in its grid: its coordinates, the grid's dims and
+// origin, and the box's first global cell (0 for one box).
+struct CellFrame {
+  int dims[3];
+  int cx, cy, cz;
+  index_t base;
+  double origin[3];
+};
+
+__device__ __forceinline__ CellFrame frame_of(const CsrArgs& a, index_t c) {
+  CellFrame f;
+  if (a.boxes) {
+    const BoxGrid& g = a.boxes[box_of(a.boxes, a.nbox, c, 0)];
+    f.base = g.cell_base;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      f.dims[k] = g.dims[k];
+      f.origin[k] = g.origin[k];
+    }
+  } else {
+    f.base = 0;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      f.dims[k] = a.grid.dims[k];
+      f.origin[k] = a.grid.origin[k];
+    }
+  }
+  const index_t lc = c - f.base;
+  f.cx = lc % f.dims[0];
+  f.cy = (lc / f.dims[0]) % f.dims[1];
+  f.cz = lc / (f.dims[0] * f.dims[1]);
+  return f;
+}
 
 // src_pos[k] = {x, y, z, 0} of particle sorted[k].
 __global__ void sorted_positions_kernel(const double* __restrict__ x, const double* __restrict__ y,
@@ -140,19 +178,18 @@ __global__ void __launch_bounds__(kCountWarps * kWarp) csr_count_kernel(CsrArgs 
   unsigned* far = s_far[w];
   index_t* cb = s_cb[w];
   index_t* pre = s_pre[w];
-  const int dimx = a.grid.dims[0], dimy = a.grid.dims[1], dimz = a.grid.dims[2];
   for (index_t c = blockIdx.x * kCountWarps + w; c < a.ncell; c += gridDim.x * kCountWarps) {
     const index_t hb = a.home_begin[c];
     if (hb < 0) continue;  // uniform across the warp
     const index_t he = a.home_end[c];
-    const int cx = c % dimx;
-    const int cy = (c / dimx) % dimy;
-    const int cz = c / (dimx * dimy);
+    const CellFrame fr = frame_of(a, c);
+    const int dimx = fr.dims[0], dimy = fr.dims[1], dimz = fr.dims[2];
+    const int cx = fr.cx, cy = fr.cy, cz = fr.cz;
     index_t b = -1, n = 0;
     if (lane < 27) {
       const int nz = cz + lane / 9 - 1, ny = cy + (lane / 3) % 3 - 1, nx = cx + lane % 3 - 1;
       if (nz >= 0 && nz < dimz && ny >= 0 && ny < dimy && nx >= 0 && nx < dimx) {
-        const index_t cell = (nz * dimy + ny) * dimx + nx;
+        const index_t cell = fr.base + (nz * dimy + ny) * dimx + nx;
         b = a.src_begin[cell];
         const index_t e = a.src_end[cell];
         if (b >= 0 && e >= 0) n = e - b;
@@ -191,9 +228,9 @@ __global__ void __launch_bounds__(kCountWarps * kWarp) csr_count_kernel(CsrArgs 
       __syncwarp();
       continue;
     }
-    const double ccx = a.grid.origin[0] + (cx + 0.5) * a.grid.cell_size;
-    const double ccy = a.grid.origin[1] + (cy + 0.5) * a.grid.cell_size;
-    const double ccz = a.grid.origin[2] + (cz + 0.5) * a.grid.cell_size;
+    const double ccx = fr.origin[0] + (cx + 0.5) * a.grid.cell_size;
+    const double ccy = fr.origin[1] + (cy + 0.5) * a.grid.cell_size;
+    const double ccz = fr.origin[2] + (cz + 0.5) * a.grid.cell_size;
     const int chunks = static_cast<int>((nc + kWarp - 1) / kWarp);
     {
       // kStageBatch loads in flight per lane: the staging is a chain of L2
@@ -324,21 +361,20 @@ __global__ void __launch_bounds__(kCsrThreads) csr_count_cell_kernel(CsrArgs a) 
   __shared__ index_t s_cnt[27];
   __shared__ index_t s_pre[28];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int dimx = a.grid.dims[0], dimy = a.grid.dims[1], dimz = a.grid.dims[2];
   const float hi2 = a.lo2 + a.band;
   for (index_t c = blockIdx.x; c < a.ncell; c += gridDim.x) {
     const index_t hb = a.home_begin[c];
     if (hb < 0) continue;  // uniform across the block
     const index_t he = a.home_end[c];
-    const int cx = c % dimx;
-    const int cy = (c / dimx) % dimy;
-    const int cz = c / (dimx * dimy);
+    const CellFrame fr = frame_of(a, c);
+    const int dimx = fr.dims[0], dimy = fr.dims[1], dimz = fr.dims[2];
+    const int cx = fr.cx, cy = fr.cy, cz = fr.cz;
     if (warp == 0) {  // the 27 source cells and their starts, one warp scan
       index_t b = -1, n = 0;
       if (lane < 27) {
         const int nz = cz + lane / 9 - 1, ny = cy + (lane / 3) % 3 - 1, nx = cx + lane % 3 - 1;
         if (nz >= 0 && nz < dimz && ny >= 0 && ny < dimy && nx >= 0 && nx < dimx) {
-          const index_t cell = (nz * dimy + ny) * dimx + nx;
+          const index_t cell = fr.base + (nz * dimy + ny) * dimx + nx;
           b = a.src_begin[cell];
           const index_t e = a.src_end[cell];
           if (b >= 0 && e >= 0) n = e - b;
@@ -359,9 +395,9 @@ __global__ void __launch_bounds__(kCsrThreads) csr_count_cell_kernel(CsrArgs a) 
     }
     __syncthreads();
     const index_t nc = s_pre[27];
-    const double ccx = a.grid.origin[0] + (cx + 0.5) * a.grid.cell_size;
-    const double ccy = a.grid.origin[1] + (cy + 0.5) * a.grid.cell_size;
-    const double ccz = a.grid.origin[2] + (cz + 0.5) * a.grid.cell_size;
+    const double ccx = fr.origin[0] + (cx + 0.5) * a.grid.cell_size;
+    const double ccy = fr.origin[1] + (cy + 0.5) * a.grid.cell_size;
+    const double ccz = fr.origin[2] + (cz + 0.5) * a.grid.cell_size;
     if (nc <= kStageCap) {
       int t = 0;  // each thread's source cell only moves forward
       for (index_t k = threadIdx.x; k < nc; k += kCsrThreads) {
@@ -480,7 +516,6 @@ __global__ void __launch_bounds__(kCsrThreads) csr_write_kernel(CsrArgs a) {
   __shared__ unsigned char s_nth[256 * 8];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const unsigned lanemask_lt = (1u << lane) - 1u;
-  const int dimx = a.grid.dims[0], dimy = a.grid.dims[1], dimz = a.grid.dims[2];
   for (int b = threadIdx.x; b < 256; b += kCsrThreads) {
     int k = 0;
     for (int bit = 0; bit < 8; ++bit)
@@ -494,15 +529,15 @@ __global__ void __launch_bounds__(kCsrThreads) csr_write_kernel(CsrArgs a) {
     const index_t hb = a.home_begin[c];
     if (hb < 0) continue;  // uniform across the block
     const index_t he = a.home_end[c];
-    const int cx = c % dimx;
-    const int cy = (c / dimx) % dimy;
-    const int cz = c / (dimx * dimy);
+    const CellFrame fr = frame_of(a, c);
+    const int dimx = fr.dims[0], dimy = fr.dims[1], dimz = fr.dims[2];
+    const int cx = fr.cx, cy = fr.cy, cz = fr.cz;
     if (warp == 0) {  // the 27 source cells and their starts, one warp scan
       index_t b = -1, n = 0;
       if (lane < 27) {
         const int nz = cz + lane / 9 - 1, ny = cy + (lane / 3) % 3 - 1, nx = cx + lane % 3 - 1;
         if (nz >= 0 && nz < dimz && ny >= 0 && ny < dimy && nx >= 0 && nx < dimx) {
-          const index_t cell = (nz * dimy + ny) * dimx + nx;
+          const index_t cell = fr.base + (nz * dimy + ny) * dimx + nx;
           b = a.src_begin[cell];
           const index_t e = a.src_end[cell];
           if (b >= 0 && e >= 0) n = e - b;
@@ -624,6 +659,8 @@ lsmps_status one_neighbor_list(lsmps_ctx* ctx, Scratch& scratch, const lsmps_flu
   a.lo2 = static_cast<float>(r2n) - kScreenMargin;
   a.band = 2.0f * kScreenMargin * 1.001f;
   a.ncell = static_cast<index_t>(static_cast<long long>(grid.dims[0]) * grid.dims[1] * grid.dims[2]);
+  a.boxes = ctx->boxes;
+  a.nbox = ctx->nbox;
   a.exclude_self = exclude_self ? 1 : 0;
   // the count pass finds a particle's own bit through the home cell's place
   // in the source list, so the self-excluding table must use one cell list
@@ -680,12 +717,14 @@ lsmps_status build_neighbor_lists_impl(lsmps_ctx* ctx, Scratch& scratch, const l
   double4* src_pos = scratch.take<double4>(std::max(fluid.count, walls.count) + 1);
   if (!bits || !src_pos) return fail(ctx, LSMPS_CUDA_ERROR, "neighbour scratch exhausted");
   ctx->built_order = nullptr;
-  lsmps_status st = build_cell_list_impl(ctx, scratch, fluid.x, fluid.y, fluid.z, fluid.count, p.grid, fc);
+  lsmps_status st =
+      build_cell_list_impl(ctx, scratch, fluid.x, fluid.y, fluid.z, fluid.count, p.grid, fc, ctx->boxes, 1);
   if (!st) {
     ctx->built_order = fc.sorted_indices;
     ctx->built_order_count = fluid.count;
   }
-  if (!st) st = build_cell_list_impl(ctx, scratch, walls.x, walls.y, walls.z, walls.count, p.grid, wc);
+  if (!st)
+    st = build_cell_list_impl(ctx, scratch, walls.x, walls.y, walls.z, walls.count, p.grid, wc, ctx->boxes, 2);
   // the two tables run one after the other on the stream and share the masks
   if (!st)
     st = one_neighbor_list(ctx, scratch, fluid, fluid.x, fluid.y, fluid.z, fc, fc, p.grid, radius, true, fn,
