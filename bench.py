@@ -441,10 +441,11 @@ def run_ours(args, world, rank, local):
 
 
 def run_batched(args, world, rank, local):
-    """64 independent boxes stepped by one captured CUDA graph over 8 worker
-    streams (the project autotuner sets each worker's knobs), and the same
-    boxes stepped one after another by lsmps_step with no graph, each in
-    both precision forms; the headline is the graph in the mixed form."""
+    """64 independent boxes stepped by one captured CUDA graph: merged (all
+    boxes as one particle set; the headline, mixed form) and one step per box
+    on 8 worker streams; and the same boxes stepped one after another by
+    lsmps_step with no graph; each in both precision forms (the project
+    autotuner sets the knobs of each graph)."""
     import torch
 
     pkg = graft_entry.load_package()
@@ -486,11 +487,13 @@ def run_batched(args, world, rank, local):
         seq = {"plain": sequential(pkg.abi.PRECISION_PLAIN), "mixed": sequential(pkg.abi.PRECISION_MIXED)}
         ctx.close()
 
-    def graph(prec, steps, sample):
+    def graph(prec, steps, sample, merged=True):
         batch = api.Batch(local, streams=8)
+        batch.set_merged(merged)
         for b, p, _ in bufs:
             batch.add(b, p)
         batch.capture(precision=prec, autotune_repeats=2)
+        assert batch.merged == merged
         stream = torch.cuda.ExternalStream(batch.stream, device=device)
         for _ in range(args.warmup):
             batch.launch()
@@ -513,6 +516,8 @@ def run_batched(args, world, rank, local):
         return e0.elapsed_time(e1) / steps, (sampler.summary() if sampler else None)
 
     plain_ms, _ = graph(pkg.abi.PRECISION_PLAIN, max(1, args.steps // 2), False)
+    streams_mixed_ms, _ = graph(pkg.abi.PRECISION_MIXED, max(1, args.steps // 2), False, merged=False)
+    streams_plain_ms, _ = graph(pkg.abi.PRECISION_PLAIN, max(1, args.steps // 2), False, merged=False)
     mixed_ms, clocks = graph(pkg.abi.PRECISION_MIXED, args.steps, True)
     ms = max_over_ranks(world, mixed_ms, device)
     value = world * n_total / (ms * 1e-3)
@@ -537,7 +542,10 @@ def run_batched(args, world, rank, local):
                    "n_wall_total": sum(c.n_wall for c in boxes), "graph_streams": 8,
                    "precision": "mixed (headline); every combination below",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
-        "graph": {"mixed": rate(mixed_ms), "plain": rate(plain_ms)},
+        "graph": {"mixed": rate(mixed_ms), "plain": rate(plain_ms),
+                  "what": "merged form: all boxes as one particle set, one launch per stage over every box"},
+        "graph_per_box_streams": {"mixed": rate(streams_mixed_ms), "plain": rate(streams_plain_ms),
+                                  "what": "one lsmps_step per box on 8 worker streams"},
         "sequential": {"mixed": rate(seq["mixed"]), "plain": rate(seq["plain"]),
                        "what": "the same 64 boxes stepped one after another with lsmps_step, no graph"},
         "graph_over_sequential": {"mixed": seq["mixed"] / mixed_ms, "plain": seq["plain"] / plain_ms},
