@@ -148,7 +148,9 @@ __global__ void scatter_particles_kernel(MergedArgs a) {
     s.fluid_cells.sorted_indices[k] = m.fluid_cells.sorted_indices[t] - b.fb;
     // row offsets of both tables and of the PPE rows
     const index_t ef = m.fluid_neighbors.offsets[b.fb], ew = m.wall_neighbors.offsets[b.fb];
-    const index_t rb = b.fb + ef;  // the box's first PPE slot
+    // the box's first PPE slot (the PPE rows were assembled on the tables the
+    // step started from, before its rebuild)
+    const index_t rb = m.ppe.matrix.row_offsets[b.fb];
     s.fluid_neighbors.offsets[k] = m.fluid_neighbors.offsets[t] - ef;
     s.wall_neighbors.offsets[k] = m.wall_neighbors.offsets[t] - ew;
     s.ppe.matrix.row_offsets[k] = m.ppe.matrix.row_offsets[t] - rb;
@@ -189,12 +191,12 @@ __global__ void scatter_cells_kernel(MergedArgs a) {
 
 // The box holding entry e of a table whose rows are the merged fluid
 // particles: the last box whose first row starts at or before e.
-__device__ __forceinline__ int box_of_entry(const MergedArgs& a, const index_t* offsets, index_t e, index_t shift) {
+__device__ __forceinline__ int box_of_entry(const MergedArgs& a, const index_t* offsets, index_t e) {
   int lo = 0, hi = a.nbox - 1;
   while (lo < hi) {
     const int mid = (lo + hi + 1) >> 1;
     const index_t fb = a.io[mid].fb;
-    if (offsets[fb] + shift * fb <= e)
+    if (offsets[fb] <= e)
       lo = mid;
     else
       hi = mid - 1;
@@ -218,7 +220,7 @@ __global__ void scatter_entries_kernel(MergedArgs a) {
   // its own: such entries are not copied and the capacity flag is raised
   // (with the box's required count), as a solo step would report.
   for (index_t e = blockIdx.x * blockDim.x + threadIdx.x; e < kf; e += stride) {
-    const BoxIO& b = a.io[box_of_entry(a, a.m.fluid_neighbors.offsets, e, 0)];
+    const BoxIO& b = a.io[box_of_entry(a, a.m.fluid_neighbors.offsets, e)];
     const index_t eb = e - a.m.fluid_neighbors.offsets[b.fb];
     if (static_cast<size_t>(eb) < b.s.fluid_neighbors.neighbor_count)
       b.s.fluid_neighbors.indices[eb] = a.m.fluid_neighbors.indices[e] - b.fb;
@@ -226,17 +228,20 @@ __global__ void scatter_entries_kernel(MergedArgs a) {
       record_required(a.status, static_cast<unsigned long long>(eb) + 1);
   }
   for (index_t e = blockIdx.x * blockDim.x + threadIdx.x; e < kw; e += stride) {
-    const BoxIO& b = a.io[box_of_entry(a, a.m.wall_neighbors.offsets, e, 0)];
+    const BoxIO& b = a.io[box_of_entry(a, a.m.wall_neighbors.offsets, e)];
     const index_t eb = e - a.m.wall_neighbors.offsets[b.fb];
     if (static_cast<size_t>(eb) < b.s.wall_neighbors.neighbor_count)
       b.s.wall_neighbors.indices[eb] = a.m.wall_neighbors.indices[e] - b.wb;
     else
       record_required(a.status, static_cast<unsigned long long>(eb) + 1);
   }
-  // PPE slots: box b's rows occupy [fb + offsets[fb], fb + nf + offsets[fb + nf])
-  for (index_t z = blockIdx.x * blockDim.x + threadIdx.x; z < a.nf + kf; z += stride) {
-    const BoxIO& b = a.io[box_of_entry(a, a.m.fluid_neighbors.offsets, z, 1)];
-    const index_t zb = z - (b.fb + a.m.fluid_neighbors.offsets[b.fb]);
+  // PPE slots: box b's rows occupy [row_offsets[fb], row_offsets[fb + nf])
+  // of the rows the step assembled (on the tables before its rebuild)
+  const index_t nz = static_cast<index_t>(min(static_cast<unsigned long long>(a.m.ppe.matrix.row_offsets[a.nf]),
+                                              static_cast<unsigned long long>(a.m.ppe.matrix.nnz)));
+  for (index_t z = blockIdx.x * blockDim.x + threadIdx.x; z < nz; z += stride) {
+    const BoxIO& b = a.io[box_of_entry(a, a.m.ppe.matrix.row_offsets, z)];
+    const index_t zb = z - a.m.ppe.matrix.row_offsets[b.fb];
     if (static_cast<size_t>(zb) >= b.s.ppe.matrix.nnz) {
       record_required(a.status, static_cast<unsigned long long>(zb) + 1);
       continue;

@@ -32,6 +32,7 @@
 
 #include "f32x2.cuh"
 #include "impl.cuh"
+#include "packed.cuh"
 
 namespace lsmps {
 namespace {
@@ -250,7 +251,7 @@ __global__ void __launch_bounds__(kCountWarps * kWarp) csr_count_kernel(CsrArgs 
         }
 #pragma unroll
         for (int u = 0; u < kStageBatch; ++u)
-          if (pos[u] >= 0) q[u] = a.src_pos[pos[u]];
+          if (pos[u] >= 0) q[u] = ld4(a.src_pos, pos[u]);
 #pragma unroll
         for (int u = 0; u < kStageBatch; ++u) {
           const index_t k = k0 + u * kWarp;
@@ -332,7 +333,7 @@ __global__ void __launch_bounds__(kCountWarps * kWarp) csr_count_kernel(CsrArgs 
           }
           bool in = false;
           if (pos >= 0) {
-            const double4 sp = a.src_pos[pos];
+            const double4 sp = ld4(a.src_pos, pos);
             in = within_radius(xi, yi, zi, sp.x, sp.y, sp.z, a.r2);
           }
           lo = in ? (lo | (1u << bit)) : (lo & ~(1u << bit));
@@ -404,7 +405,7 @@ __global__ void __launch_bounds__(kCsrThreads) csr_count_cell_kernel(CsrArgs a) 
         while (s_pre[t + 1] <= k) ++t;
         const index_t pos = s_cb[t] + (k - s_pre[t]);
         s_idx[k] = a.src_sorted[pos];
-        const double4 q = a.src_pos[pos];
+        const double4 q = ld4(a.src_pos, pos);
         s_rel[k] = make_float4(to_rel(q.x, ccx, a.inv_h), to_rel(q.y, ccy, a.inv_h), to_rel(q.z, ccz, a.inv_h), 0.0f);
       }
       __syncthreads();

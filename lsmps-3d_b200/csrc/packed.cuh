@@ -31,12 +31,16 @@ void pack4(lsmps_ctx* ctx, const double* a, const double* b, const double* c, co
 void pack4_label(lsmps_ctx* ctx, const double* a, const double* b, const double* c, const int32_t* label, size_t n,
                  double4* out);
 
-// One record through the read-only path: two 16-byte loads of one sector.
+// One record through the read-only path as one 32-byte vector load (sm_100:
+// a single load instruction per record and lane, where two 16-byte loads
+// cost two passes of the L1 data pipe for the same sector).  The records
+// are 32-byte aligned (cudaMalloc'ed arrays of 32-byte records).
 __device__ __forceinline__ double4 ld4(const double4* __restrict__ p, index_t j) {
-  const double2* q = reinterpret_cast<const double2*>(p + j);
-  const double2 a = __ldg(q);
-  const double2 b = __ldg(q + 1);
-  return make_double4(a.x, a.y, b.x, b.y);
+  double4 r;
+  asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
+      : "=d"(r.x), "=d"(r.y), "=d"(r.z), "=d"(r.w)
+      : "l"(p + j));
+  return r;
 }
 
 }  // namespace lsmps
