@@ -118,7 +118,21 @@ def cotangents(pkg, ops):
 
 
 def torch_operators(x, f, v, off, idx, p):
-    """The operators in plain torch float64 (the FP64 reference)."""
+    """The operators in plain torch float64 (the FP64 reference).  Matrix
+    products are written as elementwise products and sums and torch runs on
+    one thread here, so that the reference's own rounding does not depend on
+    the BLAS kernel or the thread count of the process."""
+    import torch
+
+    threads = torch.get_num_threads()
+    torch.set_num_threads(1)
+    try:
+        return _torch_operators(x, f, v, off, idx, p)
+    finally:
+        torch.set_num_threads(threads)
+
+
+def _torch_operators(x, f, v, off, idx, p):
     import torch
 
     n = x.shape[0]
@@ -141,10 +155,10 @@ def torch_operators(x, f, v, off, idx, p):
     def R(phi):
         return torch.zeros(n, 9, dtype=x.dtype).index_add(0, rows, (w * (phi[cols] - phi[rows]))[:, None] * b)
 
-    yf = (X @ R(f)[:, :, None])[..., 0]
+    yf = (X * R(f)[:, None, :]).sum(2)
     out = {"grad_x": yf[:, 0] / re, "grad_y": yf[:, 1] / re, "grad_z": yf[:, 2] / re,
            "laplacian": 2.0 * (yf[:, 3] + yf[:, 4] + yf[:, 5]) / re ** 2}
-    div = sum((X @ R(v[c])[:, :, None])[:, c, 0] for c in range(3)) / re
+    div = sum((X[:, c, :] * R(v[c])).sum(1) for c in range(3)) / re
     out["divergence"] = div
     ell = X[:, 3, :] + X[:, 4, :] + X[:, 5, :]
     a = 2.0 * w * (ell[rows] * b).sum(1) / (re * re * p.density)
@@ -175,16 +189,13 @@ def test_forward_and_adjoint_match_fp64_autograd(pkg, device_api):
     vr = [torch.from_numpy(a.copy()).requires_grad_(True) for a in v_np]
     ref = torch_operators(xr, fr, vr, ops.off, ops.idx, ops.p)
     assert np.array_equal(out["ppe_row_offsets"].cpu().numpy()[:-1], (np.arange(ops.n) + ops.off[:-1]))
-    # v is divergence-free (each component is constant along its own axis), so
-    # the divergence and the PPE rhs are discretization noise about 1e-3 of
-    # the velocity-gradient scale 2 pi / L; their errors are measured against
-    # that scale, the others against their own maximum.
-    grad_scale = 2.0 * np.pi / (64 * case.l0)
-    floor = {"divergence": grad_scale, "ppe_rhs": grad_scale / ops.p.time_step}
+    # Every output against its own maximum (v is divergence-free, so the
+    # divergence and the PPE rhs are discretization noise of about 1e-3 of the
+    # velocity-gradient scale: their own maximum is the strict measure).
     for k, r in ref.items():
         g = out[k].cpu().numpy()
         rn = r.detach().numpy()
-        err = np.max(np.abs(g - rn)) / max(np.max(np.abs(rn)), floor.get(k, 0.0), 1e-300)
+        err = np.max(np.abs(g - rn)) / max(np.max(np.abs(rn)), 1e-300)
         print(f"\nforward {k}: {err:.2e}")
         assert err < FORWARD_RTOL, (k, err)
     loss = sum((cot[k].cpu() * r).sum() for k, r in ref.items())

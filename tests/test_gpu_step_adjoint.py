@@ -137,7 +137,20 @@ def basis(s):
 
 
 def torch_step_operators(x, u, p, xw, nw, uw, off, idx, woff, widx, labels, prm):
-    """The step's operators in plain torch float64 (the FP64 reference)."""
+    """The step's operators in plain torch float64 (the FP64 reference), on
+    one thread and with matrix products written as elementwise sums, so that
+    its rounding does not depend on the BLAS kernel or the thread count."""
+    import torch
+
+    threads = torch.get_num_threads()
+    torch.set_num_threads(1)
+    try:
+        return _torch_step_operators(x, u, p, xw, nw, uw, off, idx, woff, widx, labels, prm)
+    finally:
+        torch.set_num_threads(threads)
+
+
+def _torch_step_operators(x, u, p, xw, nw, uw, off, idx, woff, widx, labels, prm):
     import torch
 
     n = x.shape[0]
@@ -178,7 +191,7 @@ def torch_step_operators(x, u, p, xw, nw, uw, off, idx, woff, widx, labels, prm)
     z = torch.zeros(n, 9, dtype=x.dtype)
     RV = torch.stack([z.index_add(0, rows, (w * (u[cols, c] - u[rows, c]))[:, None] * b)
                       .index_add(0, wrows, (ww * (uw[wcols, c] - u[wrows, c]))[:, None] * bw) for c in range(3)], 2)
-    yV = XV @ RV
+    yV = (XV[:, :, :, None] * RV[:, None, :, :]).sum(2)
     out = {}
     lap = 2.0 * (yV[:, 3, :] + yV[:, 4, :] + yV[:, 5, :]) / re ** 2
     out["lap_x"], out["lap_y"], out["lap_z"] = lap[:, 0], lap[:, 1], lap[:, 2]
@@ -186,7 +199,7 @@ def torch_step_operators(x, u, p, xw, nw, uw, off, idx, woff, widx, labels, prm)
     div = (yV[:, 0, 0] + yV[:, 1, 1] + yV[:, 2, 2]) / re * keep
     gn = (nn * g).sum(1)
     RP = z.index_add(0, rows, (w * (p[cols] - p[rows]))[:, None] * b).index_add(0, wrows, (ww * re * rho * gn)[:, None] * q)
-    yP = (XP @ RP[:, :, None])[..., 0]
+    yP = (XP * RP[:, None, :]).sum(2)
     gmask = (~spl).to(x.dtype)
     out["grad_x"], out["grad_y"], out["grad_z"] = (yP[:, c] / re * gmask for c in range(3))
     L = XP[:, 3, :] + XP[:, 4, :] + XP[:, 5, :]
