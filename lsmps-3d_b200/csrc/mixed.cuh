@@ -27,6 +27,13 @@ inline MixedRows mixed_rows_of(const lsmps_ctx* ctx, int kind) {
                    ctx->mixed_count ? ctx->mixed_count + kind : nullptr};
 }
 
+// Row t (0..3) of particle i as floats (particles without the flag).
+__device__ __forceinline__ void load_row9f(const MixedRows& r, index_t i, int t, float out[9]) {
+  const float* p = r.f32 + static_cast<size_t>(i) * 36 + t * 9;
+#pragma unroll
+  for (int c = 0; c < 9; ++c) out[c] = p[c];
+}
+
 // FP32 geometry of one neighbour from the FP64 coordinate difference d:
 // s = d / r_e rounded to FP32, the Type-A basis of s, and the weight
 // w = 1 - |s| (0 outside the support).  The weight is formed as
@@ -52,6 +59,22 @@ __device__ __forceinline__ float basis_f32(double dx, double dy, double dz, doub
   b[7] = sy * sz;
   b[8] = sz * sx;
   return w;
+}
+
+// a . b for a row of 9 floats at a 16-byte aligned address (shared memory):
+// read as two float4 and one float, three loads instead of nine.
+__device__ __forceinline__ float dot9f_a16(const float* __restrict__ a, const float b[9]) {
+  const float4 p = *reinterpret_cast<const float4*>(a);
+  const float4 q = *reinterpret_cast<const float4*>(a + 4);
+  float v = p.x * b[0];
+  v = fmaf(p.y, b[1], v);
+  v = fmaf(p.z, b[2], v);
+  v = fmaf(p.w, b[3], v);
+  v = fmaf(q.x, b[4], v);
+  v = fmaf(q.y, b[5], v);
+  v = fmaf(q.z, b[6], v);
+  v = fmaf(q.w, b[7], v);
+  return fmaf(a[8], b[8], v);
 }
 
 __device__ __forceinline__ float dot9f(const float a[9], const float b[9]) {

@@ -348,16 +348,18 @@ __device__ __forceinline__ void ppe_row32(const PpeArgs& a, index_t i, int l) {
   const double4 pi = ld4(a.fp, i);
   // The group's four operator rows in shared memory (read by broadcast in
   // every neighbour's dot products; they hold no registers): the pressure
-  // Laplacian row L, then the velocity gradient rows 0, 1, 2.  The stride of
-  // 40 floats keeps the 16-byte row reads of neighbouring groups on
-  // different banks.
-  __shared__ __align__(16) float s_rows[kThreads / G][40];
+  // Laplacian row L, then the velocity gradient rows 0, 1, 2, each padded to
+  // 12 floats so that every row starts on 16 bytes and is read as two float4
+  // and one float.  Within a quarter warp the groups' rows sit 48 floats
+  // apart: different banks.
+  __shared__ __align__(16) float s_rows[kThreads / G][48];
   float* L = s_rows[threadIdx.x / G];
-  const float* gx = L + 9;
-  const float* gy = L + 18;
-  const float* gz = L + 27;
+  const float* gx = L + 12;
+  const float* gy = L + 24;
+  const float* gz = L + 36;
   for (int c = l; c < 36; c += G)
-    L[c] = c < 9 ? a.prows.f32[static_cast<size_t>(i) * 36 + c] : a.vrows.f32[static_cast<size_t>(i) * 36 + c];
+    L[(c / 9) * 12 + c % 9] =
+        c < 9 ? a.prows.f32[static_cast<size_t>(i) * 36 + c] : a.vrows.f32[static_cast<size_t>(i) * 36 + c];
   __syncwarp(group_mask<G>());
   float b[9];
   const double uxi = a.tvx[i], uyi = a.tvy[i], uzi = a.tvz[i];
@@ -379,11 +381,11 @@ __device__ __forceinline__ void ppe_row32(const PpeArgs& a, index_t i, int l) {
     const float w = basis_f32(q.x - pi.x, q.y - pi.y, q.z - pi.z, a.inv_re, b);
     float off = 0.0f;
     if (w > 0.0f) {
-      off = w * dot9f(L, b) * scale;
+      off = w * dot9f_a16(L, b) * scale;
       diag -= static_cast<double>(off);
       const float dux = static_cast<float>(u.x - uxi), duy = static_cast<float>(u.y - uyi),
                   duz = static_cast<float>(u.z - uzi);
-      const float cx = dot9f(gx, b), cy = dot9f(gy, b), cz = dot9f(gz, b);
+      const float cx = dot9f_a16(gx, b), cy = dot9f_a16(gy, b), cz = dot9f_a16(gz, b);
       dsum += static_cast<double>(w * fmaf(cx, dux, fmaf(cy, duy, cz * duz)));
     }
     a.col[row + 1 + o - nb] = j;
@@ -400,14 +402,14 @@ __device__ __forceinline__ void ppe_row32(const PpeArgs& a, index_t i, int l) {
     if (w <= 0.0f) continue;
     const float dux = static_cast<float>(u.x - uxi), duy = static_cast<float>(u.y - uyi),
                 duz = static_cast<float>(u.z - uzi);
-    const float cx = dot9f(gx, b), cy = dot9f(gy, b), cz = dot9f(gz, b);
+    const float cx = dot9f_a16(gx, b), cy = dot9f_a16(gy, b), cz = dot9f_a16(gz, b);
     dsum += static_cast<double>(vws * w * fmaf(cx, dux, fmaf(cy, duy, cz * duz)));
     const float nx = static_cast<float>(nrm.x), ny = static_cast<float>(nrm.y), nz = static_cast<float>(nrm.z);
     // wall Neumann vector (moment_matrix.cu:177-201) of the scaled offset
     const float q9[9] = {nx, ny, nz, 2.0f * b[0] * nx, 2.0f * b[1] * ny, 2.0f * b[2] * nz,
                          fmaf(b[1], nx, b[0] * ny), fmaf(b[2], ny, b[1] * nz), fmaf(b[0], nz, b[2] * nx)};
     const double ng = a.gx * nrm.x + a.gy * nrm.y + a.gz * nrm.z;
-    wall_rhs += static_cast<double>(pws * w * dot9f(L, q9)) * ng * a.inv_re;
+    wall_rhs += static_cast<double>(pws * w * dot9f_a16(L, q9)) * ng * a.inv_re;
   }
   const unsigned mask = group_mask<G>();
   diag = group_sum<G>(diag, mask);

@@ -135,7 +135,7 @@ __global__ void __launch_bounds__(kThreads, 5) laplacian_kernel(LaplacianArgs a,
 // times the FP64 velocity difference accumulates in FP64.  Particles whose
 // velocity rows took the FP64 route are left to laplacian_list_kernel.
 template <int G>
-__global__ void __launch_bounds__(kThreads, 8) laplacian32_kernel(LaplacianArgs a, MixedRows rows) {
+__global__ void __launch_bounds__(kThreads, 7) laplacian32_kernel(LaplacianArgs a, MixedRows rows) {
   const index_t t = (blockIdx.x * blockDim.x + threadIdx.x) / G;
   const int l = threadIdx.x & (G - 1);
   if (t >= a.n) return;  // the whole group
@@ -143,10 +143,9 @@ __global__ void __launch_bounds__(kThreads, 8) laplacian32_kernel(LaplacianArgs 
   if (rows.flag[i]) return;
   const double4 pi = ld4(a.fp, i);
   const double4 ui = ld4(a.fv, i);
-  __shared__ float s_L[kThreads / G][12];
-  float* L = s_L[threadIdx.x / G];
-  for (int c = l; c < 9; c += G) L[c] = rows.f32[static_cast<size_t>(i) * 36 + c];
-  __syncwarp(group_mask<G>());
+  // the Laplacian row in registers (9 floats)
+  float L[9];
+  load_row9f(rows, i, 0, L);
   float b[9];
   double cx = 0.0, cy = 0.0, cz = 0.0;
   const index_t fe = a.fo[i + 1];
