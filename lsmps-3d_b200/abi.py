@@ -14,7 +14,10 @@ from ctypes import POINTER, Structure, c_char_p, c_double, c_int, c_int32, c_siz
 
 PKG_DIR = os.path.dirname(os.path.abspath(__file__))
 LIB_NAME = "liblsmps_b200.so"
-LIB_PATH = os.path.join(PKG_DIR, LIB_NAME)
+CHECKED_LIB_NAME = "liblsmps_b200_checked.so"
+# LSMPS_B200_LIBRARY selects another build of the same library, e.g. the
+# bounds-checked one (build.py --bounds-check), for the whole process.
+LIB_PATH = os.environ.get("LSMPS_B200_LIBRARY") or os.path.join(PKG_DIR, LIB_NAME)
 
 # Status codes (lsmps_status).
 OK = 0

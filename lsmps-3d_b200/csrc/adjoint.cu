@@ -521,7 +521,7 @@ lsmps_status check_inputs(lsmps_ctx* ctx, const lsmps_fluid& fl, const lsmps_csr
   if (v.count < fl.count) return fail(ctx, LSMPS_INVALID_ARGUMENT, "vector field smaller than fluid");
   if (fl.count && (!fl.x || !fl.y || !fl.z || !f || !v.x || !v.y || !v.z || !fn.offsets || !fn.indices))
     return fail(ctx, LSMPS_INVALID_ARGUMENT, "operator inputs missing");
-  return LSMPS_OK;
+  return check_neighbor_tables(ctx, fl.count, 0, fn, nullptr);
 }
 
 // Fluid-only Type-A moments into the context's inverse (or `inverse`).

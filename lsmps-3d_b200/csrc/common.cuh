@@ -24,6 +24,7 @@ constexpr unsigned kFlagCapacity = 1u;
 constexpr unsigned kFlagNonFinite = 2u;
 constexpr unsigned kFlagIndexOverflow = 4u;
 constexpr unsigned kFlagNonSpd = 8u;
+constexpr unsigned kFlagBadIndex = 16u;  // bounds-checked build: a table entry out of range
 
 // Written by kernels, read back once per synchronous call (or per
 // lsmps_ctx_synchronize in asynchronous mode).
@@ -297,6 +298,15 @@ lsmps_status begin_call(lsmps_ctx* ctx);
 // End an API call: in synchronous mode wait and fold the device status.
 lsmps_status end_call(lsmps_ctx* ctx, lsmps_status st);
 lsmps_status fold_status(lsmps_ctx* ctx);
+// Bounds-checked build (bounds.cu): validate a CSR table (rows + 1 offsets,
+// entries below `capacity`, indices below n_src) before kernels read it;
+// returns LSMPS_INVALID_ARGUMENT with `what` when it is not valid.  A no-op
+// in the normal build.
+lsmps_status check_table(lsmps_ctx* ctx, const index_t* offsets, const index_t* indices, size_t rows,
+                         unsigned long long capacity, size_t n_src, const char* what);
+// The fluid table (indices into the fluid) and, if given, the wall table.
+lsmps_status check_neighbor_tables(lsmps_ctx* ctx, size_t n_fluid, size_t n_wall, const lsmps_csr& fn,
+                                   const lsmps_csr* wn);
 
 // Event pair for the next profiled launch (grown on demand, reused across steps).
 lsmps_ctx::ProfileRecord* profile_slot(lsmps_ctx* ctx, const char* name);

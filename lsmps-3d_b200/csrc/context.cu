@@ -136,6 +136,10 @@ lsmps_status fold_status(lsmps_ctx* ctx) {
   const DeviceStatus s = *ctx->h_status;
   cudaMemsetAsync(ctx->d_status, 0, sizeof(DeviceStatus), ctx->stream);
   ctx->fallbacks += s.fallbacks;
+  if (s.flags & kFlagBadIndex) {
+    ctx->last_error = "neighbour table offset or index out of range";
+    return LSMPS_INVALID_ARGUMENT;
+  }
   if (s.flags & kFlagNonFinite) {
     ctx->last_error = "non-finite particle coordinate";
     return LSMPS_NON_FINITE;

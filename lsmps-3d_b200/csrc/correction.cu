@@ -361,6 +361,7 @@ lsmps_status pressure_gradient_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const 
   if (f.count > 0 && (!pressure || !pm.inverse_matrices))
     return fail(ctx, LSMPS_INVALID_ARGUMENT, "Pressure gradient requires pressure and inverse buffers");
   if (f.count == 0) return LSMPS_OK;
+  if (const lsmps_status cs = check_neighbor_tables(ctx, f.count, w.count, fn, &wn)) return cs;
   GatherArgs a{f, w, fn.offsets, fn.indices, wn.offsets, wn.indices, p};
   launch(ctx, gradient_kernel, dim3(div_up(static_cast<long long>(f.count), kThreads)), dim3(kThreads), 0, a,
          pressure, static_cast<const double*>(pm.inverse_matrices), pm.support_radius, pm.wall_weight_scale, g.x, g.y,
@@ -374,6 +375,7 @@ lsmps_status particle_shifting_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const 
   if (st) return st;
   if ((st = check_vector(ctx, f, s, "PS displacement workspace is too small"))) return st;
   if (f.count == 0) return LSMPS_OK;
+  if (const lsmps_status cs = check_neighbor_tables(ctx, f.count, w.count, fn, &wn)) return cs;
   GatherArgs a{f, w, fn.offsets, fn.indices, wn.offsets, wn.indices, p};
   launch(ctx, shifting_kernel, dim3(div_up(static_cast<long long>(f.count), kThreads)), dim3(kThreads), 0, a, s.x, s.y,
          s.z);
@@ -401,6 +403,9 @@ lsmps_status anti_penetration_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const l
                                    const lsmps_params& p) {
   const double clearance = p.wall_clearance_ratio * p.particle_spacing;
   if (f.count == 0 || clearance <= 0.0) return LSMPS_OK;
+  if (const lsmps_status cs = check_table(ctx, wn.offsets, wn.indices, f.count, wn.neighbor_count, w.count,
+                                          "wall neighbour table: offset or index out of range"))
+    return cs;
   launch(ctx, anti_penetration_kernel, dim3(div_up(static_cast<long long>(f.count), kThreads)), dim3(kThreads), 0, f,
          w, static_cast<const index_t*>(wn.offsets), static_cast<const index_t*>(wn.indices), clearance);
   return check_launch(ctx, "anti-penetration");
@@ -412,6 +417,7 @@ lsmps_status smooth_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const lsmps_csr& 
   if (st) return st;
   if ((st = check_vector(ctx, f, sm, "Velocity smoothing workspace is too small"))) return st;
   if (f.count == 0) return LSMPS_OK;
+  if (const lsmps_status cs = check_neighbor_tables(ctx, f.count, 0, fn, nullptr)) return cs;
   if (!ensure_packs(ctx, f.count, 0)) return fail(ctx, LSMPS_CUDA_ERROR, "pack allocation failed");
   pack4(ctx, f.x, f.y, f.z, nullptr, f.count, ctx->pack_fluid[0]);
   pack4_label(ctx, f.vx, f.vy, f.vz, f.surface_type, f.count, ctx->pack_fluid[1]);
@@ -927,6 +933,7 @@ lsmps_status gradient_shifting_stage(lsmps_ctx* ctx, const lsmps_fluid& f, const
                                      const lsmps_params& p, const lsmps_moment& pm, const lsmps_vector& g,
                                      const lsmps_vector& s, bool mixed) {
   if (f.count == 0) return LSMPS_OK;
+  if (const lsmps_status cs = check_neighbor_tables(ctx, f.count, w.count, fn, &wn)) return cs;
   GatherArgs a{f, w, fn.offsets, fn.indices, wn.offsets, wn.indices, p};
   if (!ensure_packs(ctx, f.count, w.count)) return fail(ctx, LSMPS_CUDA_ERROR, "pack allocation failed");
   pack4(ctx, f.x, f.y, f.z, pressure, f.count, ctx->pack_fluid[0]);

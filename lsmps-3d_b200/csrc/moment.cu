@@ -1158,6 +1158,7 @@ lsmps_status mixed_step_moments_impl(lsmps_ctx* ctx, const lsmps_fluid& fluid, c
     return fail(ctx, LSMPS_INVALID_ARGUMENT, "Moment matrix neighbor lists are smaller than fluid particle count");
   const index_t n = static_cast<index_t>(fluid.count);
   if (n == 0) return LSMPS_OK;
+  if (const lsmps_status cs = check_neighbor_tables(ctx, fluid.count, walls.count, fn, &wn)) return cs;
   if (!vm.moment_trace || !vm.regularization_added || !vm.info || !pm.moment_trace || !pm.regularization_added ||
       !pm.info)
     return fail(ctx, LSMPS_INVALID_ARGUMENT, "Invalid Moment matrix cache buffers");
@@ -1209,6 +1210,7 @@ lsmps_status prepare_moments_impl(lsmps_ctx* ctx, const lsmps_fluid& fluid, cons
     if (mk.kind == LSMPS_MOMENT_PRESSURE_WALL_NEUMANN_A && pressure_a < 0) pressure_a = k;
   }
   if (n == 0) return LSMPS_OK;
+  if (const lsmps_status cs = check_neighbor_tables(ctx, fluid.count, walls.count, fn, &wn)) return cs;
   auto out_of = [](const lsmps_moment& mk) {
     return KindOut{boundary_of(mk.kind), mk.inverse_matrices, mk.moment_trace, mk.regularization_added, mk.info,
                    mk.inversion_count};

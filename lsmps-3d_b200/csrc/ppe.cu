@@ -482,6 +482,7 @@ lsmps_status assemble_ppe_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const lsmps
   if (pm.kind != LSMPS_MOMENT_PRESSURE_WALL_NEUMANN_A || pm.matrix_size != 9 || pm.particle_count < f.count)
     return fail(ctx, LSMPS_NOT_PREPARED, "PPE requires a prepared pressure Type-A moment matrix");
   if (f.count == 0) return LSMPS_OK;
+  if (const lsmps_status cs = check_neighbor_tables(ctx, f.count, w.count, fn, &wn)) return cs;
   if (!ws.matrix.row_offsets || !ws.matrix.col_indices || !ws.matrix.values || !ws.rhs || !ws.divergence ||
       !tv.vx || !tv.vy || !tv.vz || !vm.inverse_matrices || !pm.inverse_matrices)
     return fail(ctx, LSMPS_INVALID_ARGUMENT, "PPE workspace requires matrix, rhs, divergence and velocity buffers");
@@ -538,6 +539,7 @@ lsmps_status assemble_ppe_mixed_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const
   if (ws.matrix.rows < f.count || ws.matrix.cols < f.count || ws.matrix.nnz < f.count + fn.neighbor_count)
     return fail(ctx, LSMPS_INVALID_ARGUMENT, "PPE matrix workspace is smaller than the requested fluid system");
   if (f.count == 0) return LSMPS_OK;
+  if (const lsmps_status cs = check_neighbor_tables(ctx, f.count, w.count, fn, &wn)) return cs;
   if (!ws.matrix.row_offsets || !ws.matrix.col_indices || !ws.matrix.values || !ws.rhs || !ws.divergence ||
       !tv.vx || !tv.vy || !tv.vz)
     return fail(ctx, LSMPS_INVALID_ARGUMENT, "PPE workspace requires matrix, rhs, divergence and velocity buffers");

@@ -264,6 +264,7 @@ lsmps_status velocity_laplacian_mixed_impl(lsmps_ctx* ctx, const lsmps_fluid& f,
                                            const lsmps_vector& lap) {
   if (lap.count < f.count) return fail(ctx, LSMPS_INVALID_ARGUMENT, "Provision laplacian workspace is too small");
   if (f.count == 0) return LSMPS_OK;
+  if (const lsmps_status cs = check_neighbor_tables(ctx, f.count, w.count, fn, &wn)) return cs;
   if (!lap.x || !lap.y || !lap.z || !f.vx || !f.vy || !f.vz)
     return fail(ctx, LSMPS_INVALID_ARGUMENT, "Provision buffers missing");
   if (w.count > 0 && (!w.vx || !w.vy || !w.vz)) return fail(ctx, LSMPS_INVALID_ARGUMENT, "wall velocity missing");
@@ -307,6 +308,7 @@ lsmps_status velocity_laplacian_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const
     return fail(ctx, LSMPS_NOT_PREPARED, "Provision requires a prepared velocity Type-A moment matrix");
   if (lap.count < f.count) return fail(ctx, LSMPS_INVALID_ARGUMENT, "Provision laplacian workspace is too small");
   if (f.count == 0) return LSMPS_OK;
+  if (const lsmps_status cs = check_neighbor_tables(ctx, f.count, w.count, fn, &wn)) return cs;
   if (!vm.inverse_matrices || !lap.x || !lap.y || !lap.z || !f.vx || !f.vy || !f.vz)
     return fail(ctx, LSMPS_INVALID_ARGUMENT, "Provision buffers missing");
   if (w.count > 0 && (!w.vx || !w.vy || !w.vz)) return fail(ctx, LSMPS_INVALID_ARGUMENT, "wall velocity missing");

@@ -220,6 +220,9 @@ lsmps_status solve_ppe_impl(lsmps_ctx* ctx, const lsmps_csr_matrix& A, const dou
                             const lsmps_solver_options& opt, lsmps_solver_report* report) {
   if (report) *report = lsmps_solver_report{0, 0, 0.0, 0.0};
   if (A.rows == 0) return LSMPS_OK;
+  if (const lsmps_status cs = check_table(ctx, A.row_offsets, A.col_indices, A.rows, A.nnz, A.cols,
+                                          "PPE matrix: row offset or column index out of range"))
+    return cs;
   if (A.rows != A.cols || !A.row_offsets || !A.col_indices || !A.values || !b || !x)
     return fail(ctx, LSMPS_INVALID_ARGUMENT, "AMGX PPE solve requires a square CSR matrix, rhs, and solution buffer");
   if (A.rows > static_cast<size_t>(INT32_MAX)) return fail(ctx, LSMPS_INDEX_OVERFLOW, "PPE rows exceed 32-bit indices");

@@ -585,7 +585,7 @@ lsmps_status check_step_inputs(lsmps_ctx* ctx, const lsmps_fluid& f, const lsmps
     return fail(ctx, LSMPS_INVALID_ARGUMENT, "step operator inputs missing");
   if (w.count && (!w.x || !w.y || !w.z || !w.vx || !w.vy || !w.vz || !w.normal_x || !w.normal_y || !w.normal_z))
     return fail(ctx, LSMPS_INVALID_ARGUMENT, "wall positions, velocities and normals are required");
-  return LSMPS_OK;
+  return check_neighbor_tables(ctx, f.count, w.count, fn, &wn);
 }
 
 // Both kinds' inverses (plain FP64) into the context's step-operator scratch,

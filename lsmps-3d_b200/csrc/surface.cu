@@ -310,6 +310,7 @@ lsmps_status virtual_light_impl(lsmps_ctx* ctx, const lsmps_fluid& fluid, const 
   if (!open_count && !open_fraction)
     return fail(ctx, LSMPS_INVALID_ARGUMENT, "Virtual light diagnostics require at least one output buffer");
   if (fluid.count == 0) return LSMPS_OK;
+  if (const lsmps_status cs = check_neighbor_tables(ctx, fluid.count, walls.count, fn, &wn)) return cs;
   if (!ensure_packs(ctx, fluid.count, walls.count)) return fail(ctx, LSMPS_CUDA_ERROR, "pack allocation failed");
   pack4(ctx, fluid.x, fluid.y, fluid.z, nullptr, fluid.count, ctx->pack_fluid[0]);
   pack4(ctx, walls.x, walls.y, walls.z, nullptr, walls.count, ctx->pack_wall[0]);
@@ -350,6 +351,7 @@ lsmps_status classify_surface_impl(lsmps_ctx* ctx, const lsmps_fluid& fluid, con
   const double n0 = reference_number_density(p.particle_spacing, p.support_radius);
   if (!(n0 > 0.0)) return fail(ctx, LSMPS_INVALID_ARGUMENT, "Reference number density must be positive");
   if (fluid.count == 0) return LSMPS_OK;
+  if (const lsmps_status cs = check_neighbor_tables(ctx, fluid.count, walls.count, fn, &wn)) return cs;
   if (!fluid.surface_type) return fail(ctx, LSMPS_INVALID_ARGUMENT, "surface_type buffer missing");
   SurfaceArgs a{};
   a.fluid = fluid;
