@@ -188,6 +188,10 @@ struct lsmps_ctx {
   // combine, PPE right-hand side, velocity/position update) instead of
   // lsmps_params::time_step, while set (lsmps_ctx_set_device_time_step).
   const double* device_dt = nullptr;
+  // lsmps_ctx_set_step_events: waited for before the step's provision stage /
+  // recorded after its pressure correction (cudaEvent_t, or NULL).
+  void* step_input_event = nullptr;
+  void* step_output_event = nullptr;
   // Order in which the per-particle gather kernels of lsmps_step visit the
   // fluid (the fluid cell list's sorted indices: particles of one cell on
   // adjacent threads, so their neighbour records are shared in cache), or

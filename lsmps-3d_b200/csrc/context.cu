@@ -309,6 +309,13 @@ int lsmps_ctx_knob(lsmps_ctx* ctx, int knob) {
   return ctx->knob[knob];
 }
 
+lsmps_status lsmps_ctx_set_step_events(lsmps_ctx* ctx, void* input_event, void* output_event) {
+  if (!ctx) return LSMPS_INVALID_ARGUMENT;
+  ctx->step_input_event = input_event;
+  ctx->step_output_event = output_event;
+  return LSMPS_OK;
+}
+
 lsmps_status lsmps_ctx_set_profiling(lsmps_ctx* ctx, int on) {
   if (!ctx) return LSMPS_INVALID_ARGUMENT;
   ctx->profiling = on != 0;

@@ -8,6 +8,15 @@
 
 using namespace lsmps;
 
+namespace {
+
+void wait_for_inputs(lsmps_ctx* ctx, bool overlap) {
+  if (overlap && ctx->step_input_event)
+    cudaStreamWaitEvent(ctx->stream, static_cast<cudaEvent_t>(ctx->step_input_event), 0);
+}
+
+}  // namespace
+
 extern "C" lsmps_status lsmps_step(lsmps_ctx* ctx, const lsmps_params* params, const lsmps_step_state* s) {
   if (!ctx || !params || !s) return LSMPS_INVALID_ARGUMENT;
   lsmps_status st = begin_call(ctx);
@@ -28,6 +37,11 @@ extern "C" lsmps_status lsmps_step(lsmps_ctx* ctx, const lsmps_params* params, c
   // geometry changes every step, so every step builds them once.  Each stage
   // is an NVTX range.
   const bool mixed = ctx->precision == LSMPS_PRECISION_MIXED;
+  // The caller's copy/compute overlap events (lsmps_ctx_set_step_events),
+  // outside stream capture only.
+  cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+  cudaStreamIsCapturing(ctx->stream, &capture);
+  const bool overlap = capture == cudaStreamCaptureStatusNone;
   {
     StageRange range("lsmps moments + velocity Laplacian");
     if (mixed) {
@@ -35,12 +49,14 @@ extern "C" lsmps_status lsmps_step(lsmps_ctx* ctx, const lsmps_params* params, c
       // read the compact FP32 operator rows instead of the full inverses.
       st = mixed_step_moments_impl(ctx, s->fluid, s->walls, s->fluid_neighbors, s->wall_neighbors, *params,
                                    s->velocity_moment, s->pressure_moment);
+      if (!st) wait_for_inputs(ctx, overlap);
       if (!st)
         st = velocity_laplacian_mixed_impl(ctx, s->fluid, s->walls, s->fluid_neighbors, s->wall_neighbors,
                                            s->velocity_moment, s->velocity_laplacian);
     } else {
       const lsmps_moment kinds[2] = {s->velocity_moment, s->pressure_moment};
       st = prepare_moments_impl(ctx, s->fluid, s->walls, s->fluid_neighbors, s->wall_neighbors, *params, kinds, 2);
+      if (!st) wait_for_inputs(ctx, overlap);
       if (!st)
         st = velocity_laplacian_impl(ctx, s->fluid, s->walls, s->fluid_neighbors, s->wall_neighbors,
                                      s->velocity_moment, s->velocity_laplacian);
@@ -65,6 +81,9 @@ extern "C" lsmps_status lsmps_step(lsmps_ctx* ctx, const lsmps_params* params, c
       st = pressure_correction_impl(ctx, s->fluid, s->walls, s->fluid_neighbors, s->wall_neighbors,
                                     s->temporary_velocity, s->pressure, *params, s->pressure_moment,
                                     s->pressure_gradient, s->ps_displacement, s->smoothed_velocity, mixed);
+    if (!st && overlap && ctx->step_output_event &&
+        cudaEventRecord(static_cast<cudaEvent_t>(ctx->step_output_event), ctx->stream) != cudaSuccess)
+      st = check_launch(ctx, "step output event");
   }
   {
     StageRange range("lsmps neighbour rebuild + labels");
