@@ -74,6 +74,9 @@ def parse_args():
     ap.add_argument("--no-renumbered", action="store_true",
                     help="skip the extra timing after lsmps_reorder_fluid (fluid renumbered in cell order)")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch-shape knobs")
+    ap.add_argument("--no-scattered", action="store_true",
+                    help="skip the forms on the splash variant with the lifted particles scattered off the lattice "
+                         "(ill-conditioned Surface/Splash matrices: the mixed form's FP64 route at full size)")
     ap.add_argument("--knobs", default=None,
                     help="comma-separated launch-shape knob values (moment variant, PPE lanes, gather lanes) to use "
                          "instead of autotuning, e.g. 2,1,1 (what the autotuner picks at 2M)")
@@ -405,6 +408,53 @@ def run_ours(args, world, rank, local):
                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e,
                    "steps": k_e2e,
                    "copies": "pinned host <-> device, overlapped with the step where its data dependences allow"}
+        # The same forms on the splash variant whose lifted 5% is scattered
+        # off the lattice (sparse, ill-conditioned Surface/Splash matrices):
+        # the generator's lattice-column splash holds none at 2M, so this is
+        # where the mixed form's FP64 route runs at full size.
+        scattered = None
+        if not args.no_scattered and args.workload == "splash":
+            case_s = pkg.cases.CASES["splash_scattered"]()
+            p_s = case_s.params
+            dev_s = api.device_buffers(case_s, device=device)
+            state_s = dev_s.step_state(p_s)
+
+            def reset_s():
+                dev_s.load_case(case_s)
+                ctx.set_synchronous(True)
+                ctx.build_neighbor_lists(dev_s, p_s)
+                ctx.classify_surface(dev_s, p_s)
+                ctx.set_synchronous(False)
+
+            timing = {}
+            for form, prec, kappa in forms:
+                ctx.set_precision(prec)
+                ctx.set_condition_threshold(kappa)
+                reset_s()
+                for _ in range(args.warmup):
+                    ctx.step(dev_s, p_s, state_s)
+                ctx.synchronize()
+                f0 = ctx.fp64_fallbacks
+                k_s = max(1, min(args.steps, 5))
+                barrier(world)
+                torch.cuda.synchronize(device)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                for _ in range(k_s):
+                    ctx.step(dev_s, p_s, state_s)
+                e1.record(stream)
+                ctx.synchronize()
+                torch.cuda.synchronize(device)
+                ms_s = max_over_ranks(world, e0.elapsed_time(e1) / k_s, device)
+                timing[form] = {"ms_per_step": ms_s, "value": world * case_s.n_fluid / (ms_s * 1e-3),
+                                "fp64_fallbacks_per_step": (ctx.fp64_fallbacks - f0) / k_s}
+            err_s = None
+            if "plain" in timing and "mixed" in timing:
+                err_s = mixed_error(pkg, torch, ctx, dev_s, case_s, p_s, state_s, reset_s, default_kappa)
+            scattered = {"workload": "splash dam break 200x50x200 (2M fluid) with the lifted 5% scattered uniformly "
+                                     "over the tank floor plan, 0-10 l0 above the free surface (seed 3)",
+                         "forms": timing, "error": err_s}
+            del dev_s, state_s
         ctx.close()
 
     head_form = forms[-1][0]
@@ -475,6 +525,7 @@ def run_ours(args, world, rank, local):
         "clocks": h["clocks"],
         "e2e": e2e,
         "renumbered": renumbered,
+        "scattered_splash": scattered,
     }
     return out, case
 

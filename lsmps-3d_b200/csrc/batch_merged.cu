@@ -204,51 +204,127 @@ __device__ __forceinline__ int box_of_entry(const MergedArgs& a, const index_t* 
   return lo;
 }
 
+// The box of entry e for a thread whose entries only increase: one search
+// for the first entry, then a walk forward past the boxes whose rows start
+// at or before e (a grid-stride step crosses a box boundary rarely).
+struct EntryCursor {
+  const MergedArgs* a;
+  const index_t* offsets;
+  int b = -1;
+  index_t next = 0;  // first entry of box b + 1 (INT32_MAX past the last box)
+  __device__ index_t start_of(int k) const {
+    return k < a->nbox ? offsets[a->io[k].fb] : static_cast<index_t>(0x7fffffff);
+  }
+  // Box b ends with start_of(b) <= e < start_of(b + 1): the last box whose
+  // rows start at or before e (boxes without fluid share their successor's
+  // start and are walked past).
+  __device__ int box(index_t e) {
+    if (b < 0) {
+      b = box_of_entry(*a, offsets, e);
+      next = start_of(b + 1);
+    }
+    while (e >= next) {
+      ++b;
+      next = start_of(b + 1);
+    }
+    return b;
+  }
+};
+
+// Where a thread's current box sends entries of one table: the box's first
+// merged entry, the index shift into the box's numbering, the box's own
+// buffers and capacity; reloaded only when the cursor moves to another box.
+struct EntryTarget {
+  int box = -1;
+  index_t start = 0;
+  index_t shift = 0;
+  unsigned long long cap = 0;
+  index_t* idx = nullptr;
+  double* val = nullptr;
+};
+
+// Table t: 0 fluid rows, 1 wall rows, 2 PPE slots (column and value).
+template <int T>
+__device__ __forceinline__ void load_target(const MergedArgs& a, const index_t* offsets, int bi, EntryTarget& g) {
+  const BoxIO& b = a.io[bi];
+  g.box = bi;
+  g.start = offsets[b.fb];
+  if (T == 0) {
+    g.shift = b.fb;
+    g.cap = b.s.fluid_neighbors.neighbor_count;
+    g.idx = b.s.fluid_neighbors.indices;
+  } else if (T == 1) {
+    g.shift = b.wb;
+    g.cap = b.s.wall_neighbors.neighbor_count;
+    g.idx = b.s.wall_neighbors.indices;
+  } else {
+    g.shift = b.fb;
+    g.cap = b.s.ppe.matrix.nnz;
+    g.idx = b.s.ppe.matrix.col_indices;
+    g.val = b.s.ppe.matrix.values;
+  }
+}
+
+// Entries [0, total) of table T into the boxes' buffers, kUnroll entries
+// per thread and round, one grid stride apart (each load coalesced across
+// the warp; the round's loads issued together).  A box's rows
+// may fit the merged capacity (the sum of the boxes') but not its own: such
+// entries are not copied and the capacity flag is raised with the box's
+// required count, as a solo step would report.
+template <int T>
+__device__ void scatter_table(const MergedArgs& a, const index_t* offsets, const index_t* src_idx,
+                              const double* src_val, index_t total) {
+  constexpr int kUnroll = 4;
+  const long long step = static_cast<long long>(gridDim.x) * blockDim.x;
+  EntryCursor cur{&a, offsets};
+  EntryTarget g;
+  for (long long e0 = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; e0 < total;
+       e0 += step * kUnroll) {
+    index_t v[kUnroll];
+    double x[kUnroll];
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+      if (e0 + u * step < total) {
+        const index_t e = static_cast<index_t>(e0 + u * step);
+        v[u] = src_idx[e];
+        if (T == 2) x[u] = src_val[e];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+      if (e0 + u * step >= total) break;
+      const index_t e = static_cast<index_t>(e0 + u * step);
+      const int bi = cur.box(e);
+      if (bi != g.box) load_target<T>(a, offsets, bi, g);
+      const index_t eb = e - g.start;
+      if (static_cast<unsigned long long>(eb) >= g.cap) {
+        record_required(a.status, static_cast<unsigned long long>(eb) + 1);
+        continue;
+      }
+      g.idx[eb] = v[u] - g.shift;
+      if (T == 2) g.val[eb] = x[u];
+    }
+  }
+}
+
 // The rows of both neighbour tables and the PPE slots (column indices
 // shifted to the box's numbering).  A box with no fluid has no entries;
-// box_of_entry skips it because its first row starts where the next box's
-// does.
+// the cursor walks past it because its first row starts where the next
+// box's does.
 __global__ void scatter_entries_kernel(MergedArgs a) {
-  const index_t stride = gridDim.x * blockDim.x;
   // the rebuilt totals, held to the merged capacities (beyond them the
   // rebuild wrote nothing and has raised the capacity flag)
   const index_t kf = static_cast<index_t>(min(static_cast<unsigned long long>(a.m.fluid_neighbors.offsets[a.nf]),
                                               static_cast<unsigned long long>(a.m.fluid_neighbors.neighbor_count)));
   const index_t kw = static_cast<index_t>(min(static_cast<unsigned long long>(a.m.wall_neighbors.offsets[a.nf]),
                                               static_cast<unsigned long long>(a.m.wall_neighbors.neighbor_count)));
-  // A box's rows may fit the merged capacity (the sum of the boxes') but not
-  // its own: such entries are not copied and the capacity flag is raised
-  // (with the box's required count), as a solo step would report.
-  for (index_t e = blockIdx.x * blockDim.x + threadIdx.x; e < kf; e += stride) {
-    const BoxIO& b = a.io[box_of_entry(a, a.m.fluid_neighbors.offsets, e)];
-    const index_t eb = e - a.m.fluid_neighbors.offsets[b.fb];
-    if (static_cast<size_t>(eb) < b.s.fluid_neighbors.neighbor_count)
-      b.s.fluid_neighbors.indices[eb] = a.m.fluid_neighbors.indices[e] - b.fb;
-    else
-      record_required(a.status, static_cast<unsigned long long>(eb) + 1);
-  }
-  for (index_t e = blockIdx.x * blockDim.x + threadIdx.x; e < kw; e += stride) {
-    const BoxIO& b = a.io[box_of_entry(a, a.m.wall_neighbors.offsets, e)];
-    const index_t eb = e - a.m.wall_neighbors.offsets[b.fb];
-    if (static_cast<size_t>(eb) < b.s.wall_neighbors.neighbor_count)
-      b.s.wall_neighbors.indices[eb] = a.m.wall_neighbors.indices[e] - b.wb;
-    else
-      record_required(a.status, static_cast<unsigned long long>(eb) + 1);
-  }
+  scatter_table<0>(a, a.m.fluid_neighbors.offsets, a.m.fluid_neighbors.indices, nullptr, kf);
+  scatter_table<1>(a, a.m.wall_neighbors.offsets, a.m.wall_neighbors.indices, nullptr, kw);
   // PPE slots: box b's rows occupy [row_offsets[fb], row_offsets[fb + nf])
   // of the rows the step assembled (on the tables before its rebuild)
   const index_t nz = static_cast<index_t>(min(static_cast<unsigned long long>(a.m.ppe.matrix.row_offsets[a.nf]),
                                               static_cast<unsigned long long>(a.m.ppe.matrix.nnz)));
-  for (index_t z = blockIdx.x * blockDim.x + threadIdx.x; z < nz; z += stride) {
-    const BoxIO& b = a.io[box_of_entry(a, a.m.ppe.matrix.row_offsets, z)];
-    const index_t zb = z - a.m.ppe.matrix.row_offsets[b.fb];
-    if (static_cast<size_t>(zb) >= b.s.ppe.matrix.nnz) {
-      record_required(a.status, static_cast<unsigned long long>(zb) + 1);
-      continue;
-    }
-    b.s.ppe.matrix.col_indices[zb] = a.m.ppe.matrix.col_indices[z] - b.fb;
-    b.s.ppe.matrix.values[zb] = a.m.ppe.matrix.values[z];
-  }
+  scatter_table<2>(a, a.m.ppe.matrix.row_offsets, a.m.ppe.matrix.col_indices, a.m.ppe.matrix.values, nz);
 }
 
 // Plain form: the 81-entry inverses of both kinds.
