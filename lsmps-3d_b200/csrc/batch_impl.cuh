@@ -17,6 +17,7 @@ struct MergedBatch {
   lsmps_ctx* ctx = nullptr;
   std::vector<void*> allocations;
   BoxGrid* grids = nullptr;
+  PpeBoxOut* box_ppe = nullptr;  // per box: its own PPE matrix (the merged step writes the rows there)
   void* io = nullptr;  // per box: its views, counts and merged bases
   lsmps_step_state state{};
   lsmps_params params{};

@@ -17,7 +17,10 @@
 // One launch of the graph: gather the boxes' particle state (fluid SoA,
 // labels, the pressure input, walls) into the merged buffers -> lsmps_step
 // on the merged set -> scatter every output back into the boxes' own views
-// (indices shifted back to the box's numbering).  The merged neighbour
+// (indices shifted back to the box's numbering).  The PPE rows need no
+// scatter: the merged context writes each box's rows straight into the box's
+// own matrix (lsmps_ctx::box_ppe, columns in the box's numbering); only
+// their row offsets come from the merged set.  The merged neighbour
 // tables and cell lists are the batch's own between launches: capture builds
 // them from the boxes' current positions, and every launch ends with their
 // rebuild, as a step does; the copies in the boxes' buffers are outputs.
@@ -240,10 +243,9 @@ struct EntryTarget {
   index_t shift = 0;
   unsigned long long cap = 0;
   index_t* idx = nullptr;
-  double* val = nullptr;
 };
 
-// Table t: 0 fluid rows, 1 wall rows, 2 PPE slots (column and value).
+// Table T: 0 fluid rows, 1 wall rows.
 template <int T>
 __device__ __forceinline__ void load_target(const MergedArgs& a, const index_t* offsets, int bi, EntryTarget& g) {
   const BoxIO& b = a.io[bi];
@@ -253,15 +255,10 @@ __device__ __forceinline__ void load_target(const MergedArgs& a, const index_t* 
     g.shift = b.fb;
     g.cap = b.s.fluid_neighbors.neighbor_count;
     g.idx = b.s.fluid_neighbors.indices;
-  } else if (T == 1) {
+  } else {
     g.shift = b.wb;
     g.cap = b.s.wall_neighbors.neighbor_count;
     g.idx = b.s.wall_neighbors.indices;
-  } else {
-    g.shift = b.fb;
-    g.cap = b.s.ppe.matrix.nnz;
-    g.idx = b.s.ppe.matrix.col_indices;
-    g.val = b.s.ppe.matrix.values;
   }
 }
 
@@ -272,8 +269,7 @@ __device__ __forceinline__ void load_target(const MergedArgs& a, const index_t* 
 // entries are not copied and the capacity flag is raised with the box's
 // required count, as a solo step would report.
 template <int T>
-__device__ void scatter_table(const MergedArgs& a, const index_t* offsets, const index_t* src_idx,
-                              const double* src_val, index_t total) {
+__device__ void scatter_table(const MergedArgs& a, const index_t* offsets, const index_t* src_idx, index_t total) {
   constexpr int kUnroll = 4;
   const long long step = static_cast<long long>(gridDim.x) * blockDim.x;
   EntryCursor cur{&a, offsets};
@@ -281,13 +277,11 @@ __device__ void scatter_table(const MergedArgs& a, const index_t* offsets, const
   for (long long e0 = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; e0 < total;
        e0 += step * kUnroll) {
     index_t v[kUnroll];
-    double x[kUnroll];
 #pragma unroll
     for (int u = 0; u < kUnroll; ++u) {
       if (e0 + u * step < total) {
         const index_t e = static_cast<index_t>(e0 + u * step);
         v[u] = src_idx[e];
-        if (T == 2) x[u] = src_val[e];
       }
     }
 #pragma unroll
@@ -302,13 +296,12 @@ __device__ void scatter_table(const MergedArgs& a, const index_t* offsets, const
         continue;
       }
       g.idx[eb] = v[u] - g.shift;
-      if (T == 2) g.val[eb] = x[u];
     }
   }
 }
 
-// The rows of both neighbour tables and the PPE slots (column indices
-// shifted to the box's numbering).  A box with no fluid has no entries;
+// The rows of both neighbour tables (indices shifted to the box's
+// numbering).  A box with no fluid has no entries;
 // the cursor walks past it because its first row starts where the next
 // box's does.
 __global__ void scatter_entries_kernel(MergedArgs a) {
@@ -318,13 +311,9 @@ __global__ void scatter_entries_kernel(MergedArgs a) {
                                               static_cast<unsigned long long>(a.m.fluid_neighbors.neighbor_count)));
   const index_t kw = static_cast<index_t>(min(static_cast<unsigned long long>(a.m.wall_neighbors.offsets[a.nf]),
                                               static_cast<unsigned long long>(a.m.wall_neighbors.neighbor_count)));
-  scatter_table<0>(a, a.m.fluid_neighbors.offsets, a.m.fluid_neighbors.indices, nullptr, kf);
-  scatter_table<1>(a, a.m.wall_neighbors.offsets, a.m.wall_neighbors.indices, nullptr, kw);
-  // PPE slots: box b's rows occupy [row_offsets[fb], row_offsets[fb + nf])
-  // of the rows the step assembled (on the tables before its rebuild)
-  const index_t nz = static_cast<index_t>(min(static_cast<unsigned long long>(a.m.ppe.matrix.row_offsets[a.nf]),
-                                              static_cast<unsigned long long>(a.m.ppe.matrix.nnz)));
-  scatter_table<2>(a, a.m.ppe.matrix.row_offsets, a.m.ppe.matrix.col_indices, a.m.ppe.matrix.values, nz);
+  scatter_table<0>(a, a.m.fluid_neighbors.offsets, a.m.fluid_neighbors.indices, kf);
+  scatter_table<1>(a, a.m.wall_neighbors.offsets, a.m.wall_neighbors.indices, kw);
+  // (the PPE slots were written into the boxes' own matrices by the step)
 }
 
 // Plain form: the 81-entry inverses of both kinds.
@@ -473,11 +462,20 @@ lsmps_status prepare_merged(MergedBatch& mb, int device, cudaStream_t stream,
   m.ppe.matrix.cols = nf;
   m.ppe.matrix.nnz = nf + capf;
   m.ppe.matrix.row_offsets = i32(nf + 1);
-  m.ppe.matrix.col_indices = i32(nf + capf);
-  m.ppe.matrix.values = d(nf + capf);
+  // The merged context writes every box's PPE rows straight into the box's
+  // own matrix (lsmps_ctx::box_ppe), so the merged matrix holds only the
+  // row offsets; its slot arrays are placeholders that are never written
+  // (the view keeps the merged capacity, which the assembly checks).
+  m.ppe.matrix.col_indices = i32(16);
+  m.ppe.matrix.values = d(16);
   m.ppe.rhs = d(nf), m.ppe.pressure = d(nf), m.ppe.divergence = d(nf), m.ppe.pressure_laplacian = d(nf);
   m.pressure = d(nf);
   mb.grids = static_cast<BoxGrid*>(alloc(grids.size() * sizeof(BoxGrid)));
+  std::vector<PpeBoxOut> ppe_out(nbox);
+  for (int b = 0; b < nbox; ++b)
+    ppe_out[b] = PpeBoxOut{states[b].ppe.matrix.col_indices, states[b].ppe.matrix.values,
+                           static_cast<unsigned long long>(states[b].ppe.matrix.nnz)};
+  mb.box_ppe = static_cast<PpeBoxOut*>(alloc(ppe_out.size() * sizeof(PpeBoxOut)));
   mb.io = alloc(io.size() * sizeof(BoxIO));
   if (!ok) {
     cudaGetLastError();
@@ -486,6 +484,8 @@ lsmps_status prepare_merged(MergedBatch& mb, int device, cudaStream_t stream,
     return LSMPS_CUDA_ERROR;
   }
   if (cudaMemcpy(mb.grids, grids.data(), grids.size() * sizeof(BoxGrid), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(mb.box_ppe, ppe_out.data(), ppe_out.size() * sizeof(PpeBoxOut), cudaMemcpyHostToDevice) !=
+          cudaSuccess ||
       cudaMemcpy(mb.io, io.data(), io.size() * sizeof(BoxIO), cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemset(mom[0]->inversion_count, 0, sizeof(int32_t)) != cudaSuccess ||
       cudaMemset(mom[1]->inversion_count, 0, sizeof(int32_t)) != cudaSuccess) {
@@ -513,6 +513,7 @@ lsmps_status prepare_merged(MergedBatch& mb, int device, cudaStream_t stream,
   lsmps_ctx_set_precision(mb.ctx, precision);
   mb.ctx->boxes = mb.grids;
   mb.ctx->nbox = nbox;
+  mb.ctx->box_ppe = mb.box_ppe;
   // The merged tables and labels from the boxes' current positions (as the
   // boxes' own tables were built), then the scratch for the step and,
   // optionally, the launch shapes tuned on the merged set.

@@ -117,6 +117,15 @@ struct BoxGrid {
   index_t wall_base;
 };
 
+// Where a merged batch's PPE rows go: box b's own matrix (its column and
+// value arrays and their capacity), written by the PPE kernels directly so
+// that the slots need no copy out of the merged matrix.
+struct PpeBoxOut {
+  index_t* col;
+  double* val;
+  unsigned long long cap;
+};
+
 // The box holding global cell c (or particle t, with field = the box's first
 // index of that set): the last box whose base is <= the value.
 __device__ __forceinline__ int box_of(const BoxGrid* __restrict__ boxes, int nbox, index_t v, int field) {
@@ -248,6 +257,9 @@ struct lsmps_ctx {
   // this context steps a merged particle set, else NULL.
   const lsmps::BoxGrid* boxes = nullptr;
   int nbox = 0;
+  // ... and where each box's PPE rows go (device table, nbox entries), or
+  // NULL to write them into the matrix the call is given.
+  const lsmps::PpeBoxOut* box_ppe = nullptr;
   // The step operator pair (step_adjoint.cu): inverses, traces,
   // regularisations, info and counts of the velocity Dirichlet-A and pressure
   // Neumann-A kinds, and the backward's stash.

@@ -56,7 +56,43 @@ struct PpeArgs {
   const double4* wu;
   const double4* wn;
   const int32_t* order;  // visiting order of the lane kernel (lsmps_ctx::order) or NULL
+  // Merged batch (lsmps_ctx::box_ppe): each row written into its box's own
+  // matrix, columns in the box's numbering; NULL: into col / val.
+  const PpeBoxOut* box_out;
+  const BoxGrid* boxes;
+  int nbox;
+  DeviceStatus* status;
 };
+
+// Where row i's slots go: the matrix given (r0 = the row's first slot), or,
+// in a merged batch, its box's own matrix, with the box's first fluid index
+// subtracted from every column (the box's rows start at merged slot
+// fb + fo[fb]).  False (and the capacity flag raised with the slots the box
+// needs so far) when the row does not fit its box's matrix: nothing of the
+// row is written.
+struct PpeDest {
+  index_t* col;
+  double* val;
+  index_t r0;
+  index_t shift;
+};
+
+__device__ __forceinline__ bool ppe_dest(const PpeArgs& a, index_t i, index_t row, index_t entries, PpeDest& d) {
+  if (!a.box_out) {
+    d = PpeDest{a.col, a.val, row, 0};
+    return true;
+  }
+  const int bx = box_of(a.boxes, a.nbox, i, 1);
+  const index_t fb = a.boxes[bx].fluid_base;
+  const PpeBoxOut o = a.box_out[bx];
+  d = PpeDest{o.col, o.val, row - (fb + a.fo[fb]), fb};
+  const unsigned long long need = static_cast<unsigned long long>(d.r0) + 1ull + static_cast<unsigned long long>(entries);
+  if (need > o.cap) {
+    record_required(a.status, need);
+    return false;
+  }
+  return true;
+}
 
 __device__ __forceinline__ double dot9(const double a[9], const double b[9]) {
   double v = 0.0;
@@ -104,13 +140,15 @@ __global__ void __launch_bounds__(kThreads) ppe_kernel(PpeArgs a) {
   const index_t row = i + nb;
   a.row_offsets[i] = row;
   if (i + 1 == n) a.row_offsets[n] = n + ne;
+  PpeDest d;
+  if (!ppe_dest(a, i, row, ne - nb, d)) return;
   const int type = a.fluid.surface_type ? a.fluid.surface_type[i] : LSMPS_SURFACE_INNER;
   if (type == LSMPS_SURFACE_SURFACE || type == LSMPS_SURFACE_SPLASH) {
-    a.col[row] = i;
-    a.val[row] = 1.0;
+    d.col[d.r0] = i - d.shift;
+    d.val[d.r0] = 1.0;
     for (index_t o = nb; o < ne; ++o) {
-      a.col[row + 1 + o - nb] = a.fi[o];
-      a.val[row + 1 + o - nb] = 0.0;
+      d.col[d.r0 + 1 + o - nb] = a.fi[o] - d.shift;
+      d.val[d.r0 + 1 + o - nb] = 0.0;
     }
     a.rhs[i] = 0.0;
     a.divergence[i] = 0.0;
@@ -143,8 +181,8 @@ __global__ void __launch_bounds__(kThreads) ppe_kernel(PpeArgs a) {
       diag -= off;
       acc_rhs(b, w, a.tvx[j] - uxi, a.tvy[j] - uyi, a.tvz[j] - uzi, rx, ry, rz);
     }
-    a.col[row + 1 + o - nb] = j;
-    a.val[row + 1 + o - nb] = off;
+    d.col[d.r0 + 1 + o - nb] = j - d.shift;
+    d.val[d.r0 + 1 + o - nb] = off;
   }
   double wall_rhs = 0.0;
   const index_t we = a.wo[i + 1];
@@ -163,8 +201,8 @@ __global__ void __launch_bounds__(kThreads) ppe_kernel(PpeArgs a) {
   }
   const double* __restrict__ vinv = a.vinv + static_cast<size_t>(i) * 81;
   const double div = (coeff_row(vinv, rx, 0) + coeff_row(vinv, ry, 1) + coeff_row(vinv, rz, 2)) * a.inv_re;
-  a.col[row] = i;
-  a.val[row] = diag;
+  d.col[d.r0] = i - d.shift;
+  d.val[d.r0] = diag;
   a.divergence[i] = div;
   a.rhs[i] = div / (a.dt_dev ? *a.dt_dev : a.dt) - wall_rhs;
   if (a.wall_rhs_out) a.wall_rhs_out[i] = wall_rhs;
@@ -191,15 +229,17 @@ __device__ __forceinline__ void ppe_row(const PpeArgs& a, index_t i, int l, bool
     a.row_offsets[i] = row;
     if (i + 1 == n) a.row_offsets[n] = n + ne;
   }
+  PpeDest d;
+  if (!ppe_dest(a, i, row, ne - nb, d)) return;  // uniform over the lane group
   const int type = a.fluid.surface_type ? a.fluid.surface_type[i] : LSMPS_SURFACE_INNER;
   if (type == LSMPS_SURFACE_SURFACE || type == LSMPS_SURFACE_SPLASH) {
     for (index_t o = nb + l; o < ne; o += G) {
-      a.col[row + 1 + o - nb] = a.fi[o];
-      a.val[row + 1 + o - nb] = 0.0;
+      d.col[d.r0 + 1 + o - nb] = a.fi[o] - d.shift;
+      d.val[d.r0 + 1 + o - nb] = 0.0;
     }
     if (l == 0) {
-      a.col[row] = i;
-      a.val[row] = 1.0;
+      d.col[d.r0] = i - d.shift;
+      d.val[d.r0] = 1.0;
       a.rhs[i] = 0.0;
       a.divergence[i] = 0.0;
       if (a.wall_rhs_out) a.wall_rhs_out[i] = 0.0;
@@ -271,8 +311,8 @@ __device__ __forceinline__ void ppe_row(const PpeArgs& a, index_t i, int l, bool
       diag -= off;
       dsum = fma(w, div_term(gx, gy, gz, b, u.x - uxi, u.y - uyi, u.z - uzi), dsum);
     }
-    a.col[row + 1 + o - nb] = j;
-    a.val[row + 1 + o - nb] = off;
+    d.col[d.r0 + 1 + o - nb] = j - d.shift;
+    d.val[d.r0 + 1 + o - nb] = off;
   }
   double wall_rhs = 0.0;
   const index_t we = a.wo[i + 1];
@@ -296,8 +336,8 @@ __device__ __forceinline__ void ppe_row(const PpeArgs& a, index_t i, int l, bool
   dsum = group_sum<G>(dsum, mask);
   if (l != 0) return;
   const double div = dsum * a.inv_re;
-  a.col[row] = i;
-  a.val[row] = diag;
+  d.col[d.r0] = i - d.shift;
+  d.val[d.r0] = diag;
   a.divergence[i] = div;
   a.rhs[i] = div / (a.dt_dev ? *a.dt_dev : a.dt) - wall_rhs;
   if (a.wall_rhs_out) a.wall_rhs_out[i] = wall_rhs;
@@ -330,15 +370,17 @@ __device__ __forceinline__ void ppe_row32(const PpeArgs& a, index_t i, int l) {
     if (i + 1 == n) a.row_offsets[n] = n + ne;
   }
   if (a.vrows.flag[i] | a.prows.flag[i]) return;  // FP64 rows: ppe_list_kernel
+  PpeDest d;
+  if (!ppe_dest(a, i, row, ne - nb, d)) return;  // uniform over the lane group
   const int type = a.fluid.surface_type ? a.fluid.surface_type[i] : LSMPS_SURFACE_INNER;
   if (type == LSMPS_SURFACE_SURFACE || type == LSMPS_SURFACE_SPLASH) {
     for (index_t o = nb + l; o < ne; o += G) {
-      a.col[row + 1 + o - nb] = a.fi[o];
-      a.val[row + 1 + o - nb] = 0.0;
+      d.col[d.r0 + 1 + o - nb] = a.fi[o] - d.shift;
+      d.val[d.r0 + 1 + o - nb] = 0.0;
     }
     if (l == 0) {
-      a.col[row] = i;
-      a.val[row] = 1.0;
+      d.col[d.r0] = i - d.shift;
+      d.val[d.r0] = 1.0;
       a.rhs[i] = 0.0;
       a.divergence[i] = 0.0;
       if (a.wall_rhs_out) a.wall_rhs_out[i] = 0.0;
@@ -388,8 +430,8 @@ __device__ __forceinline__ void ppe_row32(const PpeArgs& a, index_t i, int l) {
       const float cx = dot9f_a16(gx, b), cy = dot9f_a16(gy, b), cz = dot9f_a16(gz, b);
       dsum += static_cast<double>(w * fmaf(cx, dux, fmaf(cy, duy, cz * duz)));
     }
-    a.col[row + 1 + o - nb] = j;
-    a.val[row + 1 + o - nb] = static_cast<double>(off);
+    d.col[d.r0 + 1 + o - nb] = j - d.shift;
+    d.val[d.r0 + 1 + o - nb] = static_cast<double>(off);
   }
   double wall_rhs = 0.0;
   const index_t we = a.wo[i + 1];
@@ -417,8 +459,8 @@ __device__ __forceinline__ void ppe_row32(const PpeArgs& a, index_t i, int l) {
   dsum = group_sum<G>(dsum, mask);
   if (l != 0) return;
   const double div = dsum * a.inv_re;
-  a.col[row] = i;
-  a.val[row] = diag;
+  d.col[d.r0] = i - d.shift;
+  d.val[d.r0] = diag;
   a.divergence[i] = div;
   a.rhs[i] = div / (a.dt_dev ? *a.dt_dev : a.dt) - wall_rhs;
   if (a.wall_rhs_out) a.wall_rhs_out[i] = wall_rhs;
@@ -517,6 +559,10 @@ lsmps_status assemble_ppe_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const lsmps
   a.order = ctx->order;
   a.col = ws.matrix.col_indices;
   a.val = ws.matrix.values;
+  a.box_out = ctx->box_ppe;
+  a.boxes = ctx->boxes;
+  a.nbox = ctx->nbox;
+  a.status = ctx->d_status;
   a.rhs = ws.rhs;
   a.divergence = ws.divergence;
   a.wall_rhs_out = ws.pressure_laplacian;
@@ -576,6 +622,10 @@ lsmps_status assemble_ppe_mixed_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const
   a.order = ctx->order;
   a.col = ws.matrix.col_indices;
   a.val = ws.matrix.values;
+  a.box_out = ctx->box_ppe;
+  a.boxes = ctx->boxes;
+  a.nbox = ctx->nbox;
+  a.status = ctx->d_status;
   a.rhs = ws.rhs;
   a.divergence = ws.divergence;
   a.wall_rhs_out = ws.pressure_laplacian;
