@@ -194,12 +194,27 @@ __global__ void __launch_bounds__(kSurfaceThreads) expand_kernel(const double4* 
   const double4 own = ld4(fp, i);
   bool near = false;
   const index_t fe = fo[i + 1];
-  for (index_t o = fo[i] + l; o < fe && !near; o += kExpandLanes) {
-    const index_t j = fi[o];
-    if (type[j] != LSMPS_SURFACE_SURFACE) continue;
-    const double4 q = ld4(fp, j);
-    const double dx = q.x - own.x, dy = q.y - own.y, dz = q.z - own.z;
-    near = dx * dx + dy * dy + dz * dz <= r2;
+  // kExpandBatch entries per lane and round: their indices, then their
+  // labels, are loaded together, so a round costs two dependent load
+  // latencies instead of two per entry.
+  constexpr int kExpandBatch = 4;
+  for (index_t o = fo[i] + l; o < fe && !near; o += kExpandLanes * kExpandBatch) {
+    index_t j[kExpandBatch];
+    int32_t lab[kExpandBatch];
+#pragma unroll
+    for (int k = 0; k < kExpandBatch; ++k) {
+      const index_t e = o + k * kExpandLanes;
+      j[k] = e < fe ? fi[e] : -1;
+    }
+#pragma unroll
+    for (int k = 0; k < kExpandBatch; ++k) lab[k] = j[k] >= 0 ? type[j[k]] : LSMPS_SURFACE_INNER;
+#pragma unroll
+    for (int k = 0; k < kExpandBatch; ++k) {
+      if (lab[k] != LSMPS_SURFACE_SURFACE) continue;
+      const double4 q = ld4(fp, j[k]);
+      const double dx = q.x - own.x, dy = q.y - own.y, dz = q.z - own.z;
+      near = near || dx * dx + dy * dy + dz * dz <= r2;
+    }
   }
   // Only Inner rows are written and only Surface labels are read, so the
   // in-place update is race-free.
