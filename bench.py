@@ -340,30 +340,33 @@ def run_ours(args, world, rank, local):
         # previous step's outputs, consistent with the neighbour tables and
         # labels that step rebuilt on the device.  The copies overlap the
         # step where its data dependences allow (lsmps_ctx_set_step_events):
-        # the positions and wall geometry go first, the velocities, pressure,
-        # labels and wall velocities follow on a copy stream while the moments
-        # are built, and the fluid positions, velocities and pressure go back
-        # while the neighbour rebuild and the labels run; the labels last.
+        # the fluid positions go first; the wall geometry (read after the
+        # fluid moment sums), then the velocities, pressure, labels and wall
+        # velocities (read from the provision on) follow on a copy stream
+        # while the moments are built; the fluid positions, velocities and
+        # pressure go back while the neighbour rebuild and the labels run; the
+        # labels last.
         e2e = None
         if not args.no_e2e:
             ctx.set_precision(forms[-1][1])
             ctx.set_condition_threshold(forms[-1][2])
             reset()
-            first = [("fluid", k) for k in ("x", "y", "z")] + \
-                    [("walls", k) for k in ("x", "y", "z", "normal_x", "normal_y", "normal_z")]
+            first = [("fluid", k) for k in ("x", "y", "z")]
+            geometry = [("walls", k) for k in ("x", "y", "z", "normal_x", "normal_y", "normal_z")]
             second = [("fluid", k) for k in ("vx", "vy", "vz", "pressure", "surface_type")] + \
                      [("walls", k) for k in ("vx", "vy", "vz")]
             out_early = [("fluid", k) for k in ("x", "y", "z", "vx", "vy", "vz", "pressure")]
             out_late = [("fluid", "surface_type")]
-            host_in = {f: getattr(dev, f[0])[f[1]].detach().to("cpu").pin_memory() for f in first + second}
+            host_in = {f: getattr(dev, f[0])[f[1]].detach().to("cpu").pin_memory() for f in first + geometry + second}
             h2d = sum(t.numel() * t.element_size() for t in host_in.values())
             d2h = sum(host_in[f].numel() * host_in[f].element_size() for f in out_early + out_late)
             k_e2e = max(1, min(args.steps, 5))
             copy_stream = torch.cuda.Stream(device)
-            ev_in, ev_out = torch.cuda.Event(), torch.cuda.Event()
-            ev_in.record(copy_stream)  # creates the events before their handles are passed on
+            ev_wall, ev_in, ev_out = torch.cuda.Event(), torch.cuda.Event(), torch.cuda.Event()
+            ev_wall.record(copy_stream)  # creates the events before their handles are passed on
+            ev_in.record(copy_stream)
             ev_out.record(stream)
-            ctx.set_step_events(ev_in.cuda_event, ev_out.cuda_event)
+            ctx.set_step_events(ev_wall.cuda_event, ev_in.cuda_event, ev_out.cuda_event)
 
             def dev_of(f):
                 return getattr(dev, f[0])[f[1]]
@@ -377,6 +380,9 @@ def run_ours(args, world, rank, local):
                 for f in first:
                     dev_of(f).copy_(host_in[f], non_blocking=True)
                 with torch.cuda.stream(copy_stream):
+                    for f in geometry:
+                        dev_of(f).copy_(host_in[f], non_blocking=True)
+                    ev_wall.record(copy_stream)
                     for f in second:
                         dev_of(f).copy_(host_in[f], non_blocking=True)
                     ev_in.record(copy_stream)
@@ -402,7 +408,7 @@ def run_ours(args, world, rank, local):
             e1.record(stream)
             ctx.synchronize()
             torch.cuda.synchronize(device)
-            ctx.set_step_events(None, None)
+            ctx.set_step_events(None, None, None)
             ms_e2e = max_over_ranks(world, e0.elapsed_time(e1) / k_e2e, device)
             e2e = {"value": world * case.n_fluid / (ms_e2e * 1e-3), "unit": "particles/s",
                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e,

@@ -620,20 +620,22 @@ lsmps_status lsmps_ctx_set_device_time_step(lsmps_ctx* ctx, const double* device
  * precision mode. */
 lsmps_status lsmps_step(lsmps_ctx* ctx, const lsmps_params* params, const lsmps_step_state* state);
 /* Copy/compute overlap for a caller whose particle state lives in host memory
- * (no counterpart in the reference, whose state stays on the device).  Both
- * are cudaEvent_t handles (NULL clears), used by every following lsmps_step of
- * this context while its stream is not being captured:
+ * (no counterpart in the reference, whose state stays on the device).  All
+ * are cudaEvent_t handles (NULL: not used), used by every following lsmps_step
+ * of this context while its stream is not being captured; only the fluid
+ * positions must be in place when the step is queued:
+ *   wall_event   - the step waits for it before it first reads the walls'
+ *                  positions and normals (in the mixed form after the fluid
+ *                  moment sums, in the plain form before the moment stage);
  *   input_event  - the step waits for it after its moment stage and before the
  *                  provision stage: the fluid velocities, pressure and labels
  *                  and the wall velocities may still be arriving while the
- *                  moments are built (the fluid positions and the wall
- *                  positions and normals must be in place when the step is
- *                  queued);
+ *                  moments are built;
  *   output_event - the step records it once the pressure correction is done:
  *                  the fluid positions, velocities and pressure are final and
  *                  can be copied out while the neighbour rebuild and the labels
  *                  run (the labels are final only at the end of the step). */
-lsmps_status lsmps_ctx_set_step_events(lsmps_ctx* ctx, void* input_event, void* output_event);
+lsmps_status lsmps_ctx_set_step_events(lsmps_ctx* ctx, void* wall_event, void* input_event, void* output_event);
 
 /* ------------------------------------------------------------------------- */
 /* Batched boxes in one CUDA graph (no counterpart in the reference)          */

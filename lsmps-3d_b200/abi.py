@@ -378,7 +378,7 @@ _SIGNATURES = {
                                         c_void_p]),
     "lsmps_operators_backward": (c_int, [c_void_p, P(Fluid), P(Csr), P(Params), c_void_p, P(Vector), P(OperatorOut),
                                          c_void_p, c_void_p, P(Vector), P(Vector)]),
-    "lsmps_ctx_set_step_events": (c_int, [c_void_p, c_void_p, c_void_p]),
+    "lsmps_ctx_set_step_events": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     "lsmps_step_operators_forward": (c_int, [c_void_p, P(Fluid), P(Walls), P(Csr), P(Csr), P(Params),
                                              P(StepOperatorOut)]),
     "lsmps_step_operators_backward": (c_int, [c_void_p, P(Fluid), P(Walls), P(Csr), P(Csr), P(Params),

@@ -224,10 +224,11 @@ class Context:
         (an abi.TimeState in device memory)."""
         self.check(_lib.lsmps_advance_time(self.h, r(b.fluid_view()), r(limits), ctypes.c_void_p(state_ptr)))
 
-    def set_step_events(self, input_event: int | None, output_event: int | None) -> None:
+    def set_step_events(self, wall_event: int | None, input_event: int | None, output_event: int | None) -> None:
         """lsmps_ctx_set_step_events: raw cudaEvent_t handles (e.g. a recorded
-        torch.cuda.Event's cuda_event), or None to clear."""
-        self.check(_lib.lsmps_ctx_set_step_events(self.h, ctypes.c_void_p(input_event or 0),
+        torch.cuda.Event's cuda_event), or None for an event not used."""
+        self.check(_lib.lsmps_ctx_set_step_events(self.h, ctypes.c_void_p(wall_event or 0),
+                                                  ctypes.c_void_p(input_event or 0),
                                                   ctypes.c_void_p(output_event or 0)))
 
     def set_device_time_step(self, ptr: int | None) -> None:

@@ -199,8 +199,13 @@ struct lsmps_ctx {
   const double* device_dt = nullptr;
   // lsmps_ctx_set_step_events: waited for before the step's provision stage /
   // recorded after its pressure correction (cudaEvent_t, or NULL).
+  void* step_wall_event = nullptr;
   void* step_input_event = nullptr;
   void* step_output_event = nullptr;
+  // Set by lsmps_step around its moment stage (the step's wall event, or
+  // NULL): the mixed moment stage waits for it right before it packs the
+  // walls, after the fluid sums.
+  void* walls_wait_event = nullptr;
   // Order in which the per-particle gather kernels of lsmps_step visit the
   // fluid (the fluid cell list's sorted indices: particles of one cell on
   // adjacent threads, so their neighbour records are shared in cache), or

@@ -309,8 +309,9 @@ int lsmps_ctx_knob(lsmps_ctx* ctx, int knob) {
   return ctx->knob[knob];
 }
 
-lsmps_status lsmps_ctx_set_step_events(lsmps_ctx* ctx, void* input_event, void* output_event) {
+lsmps_status lsmps_ctx_set_step_events(lsmps_ctx* ctx, void* wall_event, void* input_event, void* output_event) {
   if (!ctx) return LSMPS_INVALID_ARGUMENT;
+  ctx->step_wall_event = wall_event;
   ctx->step_input_event = input_event;
   ctx->step_output_event = output_event;
   return LSMPS_OK;

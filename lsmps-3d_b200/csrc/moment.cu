@@ -1094,8 +1094,12 @@ int boundary_of(int kind) {
 // Queue the two mixed-form stages for the velocity (kv) and pressure (kp)
 // Type-A kinds; positions are already packed into ctx->pack_fluid[0] and the
 // wall packs.
+// The walls' position and normal packs are made here, after the fluid sums
+// (for the split kernel before it), once the context's walls_wait_event (a
+// host-resident caller's wall copy, lsmps_step only) has been waited for.
 lsmps_status launch_mixed(lsmps_ctx* ctx, index_t n, const lsmps_csr& fn, const lsmps_csr& wn,
-                          const lsmps_params& p, const KindOut& kv, const KindOut& kp, bool full) {
+                          const lsmps_params& p, const KindOut& kv, const KindOut& kp, bool full,
+                          const lsmps_walls& walls) {
   if (!ensure_mixed(ctx, static_cast<size_t>(n))) return fail(ctx, LSMPS_CUDA_ERROR, "mixed-form allocation failed");
   const double inv_re = 1.0 / p.support_radius;
   MixedSumArgs sa{n, ctx->pack_fluid[0], fn.offsets, fn.indices, inv_re, ctx->mixed_sums, ctx->order};
@@ -1127,7 +1131,14 @@ lsmps_status launch_mixed(lsmps_ctx* ctx, index_t n, const lsmps_csr& fn, const 
   cudaMemsetAsync(ctx->mixed_count, 0, 4 * sizeof(unsigned int), ctx->stream);
   ra.status = ctx->d_status;
   ra.order = ctx->order;
+  auto pack_walls = [&]() {
+    if (ctx->walls_wait_event)
+      cudaStreamWaitEvent(ctx->stream, static_cast<cudaEvent_t>(ctx->walls_wait_event), 0);
+    pack4(ctx, walls.x, walls.y, walls.z, nullptr, walls.count, ctx->pack_wall[0]);
+    pack4(ctx, walls.normal_x, walls.normal_y, walls.normal_z, nullptr, walls.count, ctx->pack_wall[2]);
+  };
   if (split) {
+    pack_walls();
     // one kernel: row halves on two warps, one kind per warp
     if (full)
       launch(ctx, moment_mixed_split_kernel<true>, dim3(div_up(n, kWarp)), dim3(kRowThreads), 0, sa, ra);
@@ -1136,6 +1147,7 @@ lsmps_status launch_mixed(lsmps_ctx* ctx, index_t n, const lsmps_csr& fn, const 
     return LSMPS_OK;
   }
   launch(ctx, moment_sums_kernel, dim3(div_up(n, kSumThreads)), dim3(kSumThreads), 0, sa);
+  pack_walls();
   const dim3 grid(div_up(n, kRowThreads), 2);
   if (full)
     launch(ctx, moment_rows_kernel<true>, grid, dim3(kRowThreads), 0, ra);
@@ -1164,11 +1176,9 @@ lsmps_status mixed_step_moments_impl(lsmps_ctx* ctx, const lsmps_fluid& fluid, c
     return fail(ctx, LSMPS_INVALID_ARGUMENT, "Invalid Moment matrix cache buffers");
   if (!ensure_packs(ctx, fluid.count, walls.count)) return fail(ctx, LSMPS_CUDA_ERROR, "pack allocation failed");
   pack4(ctx, fluid.x, fluid.y, fluid.z, nullptr, fluid.count, ctx->pack_fluid[0]);
-  pack4(ctx, walls.x, walls.y, walls.z, nullptr, walls.count, ctx->pack_wall[0]);
-  pack4(ctx, walls.normal_x, walls.normal_y, walls.normal_z, nullptr, walls.count, ctx->pack_wall[2]);
   const KindOut kv{1, vm.inverse_matrices, vm.moment_trace, vm.regularization_added, vm.info, vm.inversion_count};
   const KindOut kp{2, pm.inverse_matrices, pm.moment_trace, pm.regularization_added, pm.info, pm.inversion_count};
-  lsmps_status st = launch_mixed(ctx, n, fn, wn, p, kv, kp, false);
+  lsmps_status st = launch_mixed(ctx, n, fn, wn, p, kv, kp, false, walls);
   if (st) return st;
   return check_launch(ctx, "mixed moment rows");
 }
@@ -1218,18 +1228,22 @@ lsmps_status prepare_moments_impl(lsmps_ctx* ctx, const lsmps_fluid& fluid, cons
   const dim3 grid(div_up(n, kMomentThreads)), block(kMomentThreads);
   if (!ensure_packs(ctx, fluid.count, walls.count)) return fail(ctx, LSMPS_CUDA_ERROR, "pack allocation failed");
   pack4(ctx, fluid.x, fluid.y, fluid.z, nullptr, fluid.count, ctx->pack_fluid[0]);
-  pack4(ctx, walls.x, walls.y, walls.z, nullptr, walls.count, ctx->pack_wall[0]);
-  pack4(ctx, walls.normal_x, walls.normal_y, walls.normal_z, nullptr, walls.count, ctx->pack_wall[2]);
+  // (the mixed form packs the walls itself, after its fluid sums)
+  const bool fused = velocity_a >= 0 && pressure_a >= 0;
+  if (!(fused && ctx->precision == LSMPS_PRECISION_MIXED)) {
+    pack4(ctx, walls.x, walls.y, walls.z, nullptr, walls.count, ctx->pack_wall[0]);
+    pack4(ctx, walls.normal_x, walls.normal_y, walls.normal_z, nullptr, walls.count, ctx->pack_wall[2]);
+  }
   MomentPackedArgs pa{n, ctx->pack_fluid[0], ctx->pack_wall[0], ctx->pack_wall[2], fn.offsets, fn.indices,
                       wn.offsets, wn.indices, base.inv_re, base.lambda, base.wall_scale, KindOut{}, KindOut{},
                       ctx->d_status, ctx->order};
-  const bool fused = velocity_a >= 0 && pressure_a >= 0;
   const bool capped = ctx->knob[LSMPS_KNOB_MOMENT_OCCUPANCY] == 1;
   const bool split = ctx->knob[LSMPS_KNOB_MOMENT_OCCUPANCY] == 2;
   if (fused && ctx->precision == LSMPS_PRECISION_MIXED) {
     // Mixed form: FP32 assembly and factorisation with FP64 refinement; the
     // full inverse is written (FP64) for the caller's views.
-    lsmps_status st = launch_mixed(ctx, n, fn, wn, p, out_of(kinds[velocity_a]), out_of(kinds[pressure_a]), true);
+    lsmps_status st =
+        launch_mixed(ctx, n, fn, wn, p, out_of(kinds[velocity_a]), out_of(kinds[pressure_a]), true, walls);
     if (st) return st;
   } else if (fused) {
     // The step's two kinds share the fluid sums: one pass over the rows.

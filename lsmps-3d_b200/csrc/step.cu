@@ -47,14 +47,20 @@ extern "C" lsmps_status lsmps_step(lsmps_ctx* ctx, const lsmps_params* params, c
     if (mixed) {
       // FP32 assembly and factorisation with FP64 refinement; the consumers
       // read the compact FP32 operator rows instead of the full inverses.
+      // (the walls are first read after the fluid sums: the moment stage
+      // waits for the caller's wall event there)
+      ctx->walls_wait_event = overlap ? ctx->step_wall_event : nullptr;
       st = mixed_step_moments_impl(ctx, s->fluid, s->walls, s->fluid_neighbors, s->wall_neighbors, *params,
                                    s->velocity_moment, s->pressure_moment);
+      ctx->walls_wait_event = nullptr;
       if (!st) wait_for_inputs(ctx, overlap);
       if (!st)
         st = velocity_laplacian_mixed_impl(ctx, s->fluid, s->walls, s->fluid_neighbors, s->wall_neighbors,
                                            s->velocity_moment, s->velocity_laplacian);
     } else {
       const lsmps_moment kinds[2] = {s->velocity_moment, s->pressure_moment};
+      if (overlap && ctx->step_wall_event)
+        cudaStreamWaitEvent(ctx->stream, static_cast<cudaEvent_t>(ctx->step_wall_event), 0);
       st = prepare_moments_impl(ctx, s->fluid, s->walls, s->fluid_neighbors, s->wall_neighbors, *params, kinds, 2);
       if (!st) wait_for_inputs(ctx, overlap);
       if (!st)
