@@ -94,3 +94,61 @@ def test_graph_batch_64_boxes_matches_solo_steps(pkg, device_api, precision):
         for k in ("row_offsets", "rhs", "divergence"):
             assert np.array_equal(gp[k], rp[k]), (case.name, k)
         assert np.array_equal(gp["values"][:nnz], rp["values"][:nnz]), case.name
+        assert np.array_equal(gp["col_indices"][:nnz], rp["col_indices"][:nnz]), case.name
+
+
+def test_merged_batch_reports_a_box_over_its_own_capacity(pkg, device_api):
+    """A box whose own neighbour tables and PPE matrix are too small for its
+    rows (the merged set's tables, the sum of the boxes', are large enough):
+    the launch reports LSMPS_CAPACITY_EXCEEDED, writes nothing past that box's
+    capacities (guard entries beyond them keep their fill), and the other
+    boxes still equal their solo steps."""
+    import torch
+
+    boxes = pkg.cases.batched_boxes(count=3, seed=5, n_min=2_000, n_max=6_000)
+    small = 1
+    bufs, refs = [], {}
+    c = device_api.Context(0)
+    try:
+        c.set_precision(1)
+        for k, case in enumerate(boxes):
+            p = case.params
+            b = device_api.device_buffers(case)
+            if k == small:
+                # views 16 entries per particle wide over the full-size arrays;
+                # everything past them is a guard
+                b.cap_f = 16 * case.n_fluid
+                b.nnz_cap = case.n_fluid + b.cap_f
+                b.fluid_neighbors["indices"][b.cap_f:] = -7
+                b.ppe["col_indices"][b.nnz_cap:] = -7
+            else:
+                c.build_neighbor_lists(b, p)
+                c.classify_surface(b, p)
+                r = device_api.device_buffers(case)
+                c.build_neighbor_lists(r, p)
+                c.classify_surface(r, p)
+                c.step(r, p)
+                refs[k] = r
+            bufs.append((b, p))
+    finally:
+        c.close()
+    torch.cuda.synchronize()
+    batch = device_api.Batch(0, streams=3)
+    try:
+        for b, p in bufs:
+            batch.add(b, p)
+        batch.capture(precision=1, autotune_repeats=0)
+        assert batch.merged
+        batch.launch()
+        with pytest.raises(device_api.LsmpsError) as err:
+            batch.synchronize()
+        assert err.value.status == pkg.abi.CAPACITY_EXCEEDED, err.value
+    finally:
+        batch.close()
+    b = bufs[small][0]
+    assert torch.all(b.fluid_neighbors["indices"][b.cap_f:] == -7)
+    assert torch.all(b.ppe["col_indices"][b.nnz_cap:] == -7)
+    for k, r in refs.items():
+        got, want = bufs[k][0].numpy("fluid"), r.numpy("fluid")
+        for name in want:
+            assert np.array_equal(got[name], want[name]), (k, name)
