@@ -952,12 +952,29 @@ __device__ __forceinline__ void mixed_rows_of_particle(const MixedRowArgs& a, in
         for (int g = 0; g < kGroup; ++g) d[g][r] = static_cast<float>(res[g]);
       }
       chol_solve_group(l, dinv, d);
+      if (Full) {
 #pragma unroll
-      for (int g = 0; g < kGroup; ++g) {
-        double y[9];
+        for (int g = 0; g < kGroup; ++g) {
+          double y[9];
 #pragma unroll
-        for (int r = 0; r < 9; ++r) y[r] = static_cast<double>(y0[g][r]) + static_cast<double>(d[g][r]);
-        store_target<Full>(a, kind, i, t0 + g, y, false);
+          for (int r = 0; r < 9; ++r) y[r] = static_cast<double>(y0[g][r]) + static_cast<double>(d[g][r]);
+          store_target<Full>(a, kind, i, t0 + g, y, false);
+        }
+      } else {
+        // The group's rows are adjacent in the particle's 36 floats and start
+        // on 8 bytes (t0 * 9 floats, t0 even): written as float pairs, half
+        // the store instructions of the scalar form, the same values.
+        static_assert(Full || kGroup == 2, "row pairs");
+        float f[kGroup * 9];
+#pragma unroll
+        for (int g = 0; g < kGroup; ++g) {
+#pragma unroll
+          for (int r = 0; r < 9; ++r)
+            f[g * 9 + r] = static_cast<float>(static_cast<double>(y0[g][r]) + static_cast<double>(d[g][r]));
+        }
+        float2* out = reinterpret_cast<float2*>(a.rows[kind] + static_cast<size_t>(i) * 36 + t0 * 9);
+#pragma unroll
+        for (int k = 0; k < kGroup * 9 / 2; ++k) out[k] = make_float2(f[2 * k], f[2 * k + 1]);
       }
     }
     ko.trace[i] = trace;
