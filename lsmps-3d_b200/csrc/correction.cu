@@ -785,13 +785,14 @@ __global__ void __launch_bounds__(kThreads, 6) gradient32_kernel(GatherArgs a, G
     if (l != 0) return;
   }
   {
-    const float* g = out.prows.f32 + static_cast<size_t>(i) * 36;
+    float g[27];
+    load_rows123f(out.prows, i, g);
     double c0 = 0.0, c1 = 0.0, c2 = 0.0;
 #pragma unroll
     for (int col = 0; col < 9; ++col) {
-      c0 = fma(static_cast<double>(g[9 + col]), rd[col], c0);
-      c1 = fma(static_cast<double>(g[18 + col]), rd[col], c1);
-      c2 = fma(static_cast<double>(g[27 + col]), rd[col], c2);
+      c0 = fma(static_cast<double>(g[col]), rd[col], c0);
+      c1 = fma(static_cast<double>(g[9 + col]), rd[col], c1);
+      c2 = fma(static_cast<double>(g[18 + col]), rd[col], c2);
     }
     out.gx[i] = c0 * inv_re;
     out.gy[i] = c1 * inv_re;

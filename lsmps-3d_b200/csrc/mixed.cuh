@@ -27,11 +27,35 @@ inline MixedRows mixed_rows_of(const lsmps_ctx* ctx, int kind) {
                    ctx->mixed_count ? ctx->mixed_count + kind : nullptr};
 }
 
-// Row t (0..3) of particle i as floats (particles without the flag).
+// Row t (0..3) of particle i as floats (particles without the flag).  A
+// particle's 36 floats start on 16 bytes: row 0 is read as two float4 and
+// one float.
 __device__ __forceinline__ void load_row9f(const MixedRows& r, index_t i, int t, float out[9]) {
   const float* p = r.f32 + static_cast<size_t>(i) * 36 + t * 9;
+  if (t == 0) {
+    const float4 a = reinterpret_cast<const float4*>(p)[0];
+    const float4 b = reinterpret_cast<const float4*>(p)[1];
+    out[0] = a.x, out[1] = a.y, out[2] = a.z, out[3] = a.w;
+    out[4] = b.x, out[5] = b.y, out[6] = b.z, out[7] = b.w;
+    out[8] = p[8];
+    return;
+  }
 #pragma unroll
   for (int c = 0; c < 9; ++c) out[c] = p[c];
+}
+
+// Rows 1, 2, 3 of particle i (floats 9..35) as g[0..26]: read as seven
+// float4 over floats 8..35 (16-byte aligned), the first value dropped.
+__device__ __forceinline__ void load_rows123f(const MixedRows& r, index_t i, float g[27]) {
+  const float4* p = reinterpret_cast<const float4*>(r.f32 + static_cast<size_t>(i) * 36 + 8);
+  float v[28];
+#pragma unroll
+  for (int k = 0; k < 7; ++k) {
+    const float4 q = p[k];
+    v[4 * k] = q.x, v[4 * k + 1] = q.y, v[4 * k + 2] = q.z, v[4 * k + 3] = q.w;
+  }
+#pragma unroll
+  for (int c = 0; c < 27; ++c) g[c] = v[c + 1];
 }
 
 // FP32 geometry of one neighbour from the FP64 coordinate difference d:

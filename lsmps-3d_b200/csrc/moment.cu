@@ -961,9 +961,10 @@ __device__ __forceinline__ void mixed_rows_of_particle(const MixedRowArgs& a, in
           store_target<Full>(a, kind, i, t0 + g, y, false);
         }
       } else {
-        // The group's rows are adjacent in the particle's 36 floats and start
-        // on 8 bytes (t0 * 9 floats, t0 even): written as float pairs, half
-        // the store instructions of the scalar form, the same values.
+        // The group's rows are adjacent in the particle's 36 floats (144
+        // bytes) and start on 16 bytes (the first pair) or 8 bytes (the
+        // second): written as float quadruples and pairs, fewer store
+        // instructions than the scalar form, the same values.
         static_assert(Full || kGroup == 2, "row pairs");
         float f[kGroup * 9];
 #pragma unroll
@@ -972,9 +973,17 @@ __device__ __forceinline__ void mixed_rows_of_particle(const MixedRowArgs& a, in
           for (int r = 0; r < 9; ++r)
             f[g * 9 + r] = static_cast<float>(static_cast<double>(y0[g][r]) + static_cast<double>(d[g][r]));
         }
-        float2* out = reinterpret_cast<float2*>(a.rows[kind] + static_cast<size_t>(i) * 36 + t0 * 9);
+        float* base = a.rows[kind] + static_cast<size_t>(i) * 36 + t0 * 9;
+        if (t0 == 0) {
+          float4* out4 = reinterpret_cast<float4*>(base);
 #pragma unroll
-        for (int k = 0; k < kGroup * 9 / 2; ++k) out[k] = make_float2(f[2 * k], f[2 * k + 1]);
+          for (int k = 0; k < 4; ++k) out4[k] = make_float4(f[4 * k], f[4 * k + 1], f[4 * k + 2], f[4 * k + 3]);
+          reinterpret_cast<float2*>(base)[8] = make_float2(f[16], f[17]);
+        } else {
+          float2* out = reinterpret_cast<float2*>(base);
+#pragma unroll
+          for (int k = 0; k < kGroup * 9 / 2; ++k) out[k] = make_float2(f[2 * k], f[2 * k + 1]);
+        }
       }
     }
     ko.trace[i] = trace;
