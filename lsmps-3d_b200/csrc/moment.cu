@@ -170,8 +170,46 @@ __device__ __forceinline__ void store_inverse(const double (&t)[N * (N + 1) / 2]
   }
 }
 
+// The inverse X = L^-T L^-1 from the inverted factor t, written by the
+// warp's active lanes together: in three passes of nine columns' 27 entries
+// each lane stages its particle's entries in shared memory (stage: 27 x 32
+// doubles), then the warp writes them particle by particle, 27 consecutive
+// doubles per store instruction, instead of 81 scattered 8-byte stores per
+// lane.  The active lanes are the lowest ones (lanes past the particle count
+// have left).  Same values as store_inverse (the same fused products in the
+// same order); NaN where the factorisation failed (ok = false).
+__device__ __forceinline__ void warp_store_inverse(const double (&t)[45], bool ok, double* out, double* stage,
+                                                   unsigned active) {
+  const int lane = threadIdx.x & (kWarp - 1);
+  const int nact = __popc(active);
+  const unsigned long long mine = reinterpret_cast<unsigned long long>(out);
+#pragma unroll
+  for (int pass = 0; pass < 3; ++pass) {
+#pragma unroll
+    for (int cc = 0; cc < 3; ++cc) {
+      const int c = 3 * pass + cc;
+#pragma unroll
+      for (int r = 0; r < 9; ++r) {
+        const int lo = r > c ? r : c;
+        double x = 0.0;
+#pragma unroll
+        for (int k = lo; k < 9; ++k) x = fma(t[tri(k, r)], t[tri(k, c)], x);
+        stage[(cc * 9 + r) * kWarp + lane] = ok ? x : __longlong_as_double(0x7ff8000000000000LL);
+      }
+    }
+    __syncwarp(active);
+    for (unsigned rem = active; rem; rem &= rem - 1) {
+      const int p = __ffs(rem) - 1;
+      double* op = reinterpret_cast<double*>(__shfl_sync(active, mine, p));
+      for (int e = lane; e < 27; e += nact) op[27 * pass + e] = stage[e * kWarp + p];
+    }
+    __syncwarp(active);
+  }
+}
+
 // Adds the wall term of boundary kind B (0 none, 1 Dirichlet sample,
-// 2 pressure Neumann) to m, regularises, inverts and stores one kind.
+// 2 pressure Neumann) to m, regularises, inverts and stores one kind (with
+// stage, by the warp's active lanes together: warp_store_inverse).
 template <int N, int B>
 __device__ __forceinline__ void finish_kind(double (&m)[N * (N + 1) / 2], const MomentArgs& a, const KindOut& ko,
                                             index_t i, double xi, double yi, double zi) {
@@ -384,7 +422,8 @@ struct MomentPackedArgs {
 
 template <int B>
 __device__ __forceinline__ void finish_a(double (&s)[kMonomials], const MomentPackedArgs& a, const KindOut& ko,
-                                         index_t i, const double4& pi) {
+                                         index_t i, const double4& pi, double* stage = nullptr,
+                                         unsigned active = 0u) {
   const index_t wb = a.wo[i], we = a.wo[i + 1];
   if (B == 1) {
     for (index_t o = wb; o < we; ++o) {
@@ -426,11 +465,15 @@ __device__ __forceinline__ void finish_a(double (&s)[kMonomials], const MomentPa
   for (int r = 0; r < 9; ++r) m[tri(r, r)] += reg;
   const int info = cholesky<9>(m);
   double* out = ko.inverse + static_cast<size_t>(i) * 81;
-  if (info == 0) {
-    invert_lower<9>(m);
+  if (info == 0) invert_lower<9>(m);
+  if (stage) {
+    warp_store_inverse(m, info == 0, out, stage, active);
+  } else if (info == 0) {
     store_inverse<9>(m, out);
   } else {
     for (int e = 0; e < 81; ++e) out[e] = __longlong_as_double(0x7ff8000000000000LL);
+  }
+  if (info != 0) {
     atomicAdd(&a.status->non_spd, 1u);
     raise_flag(a.status, kFlagNonSpd);
   }
@@ -523,13 +566,18 @@ __global__ void __launch_bounds__(2 * kWarp, 8) moment_a_split_kernel(MomentPack
 #pragma unroll
   for (int e = 0; e < kMonomials; ++e) s_half[half][e][lane] = s[e];
   __syncthreads();
-  if (!live) return;
 #pragma unroll
   for (int e = 0; e < kMonomials; ++e) s[e] = s_half[0][e][lane] + s_half[1][e][lane];
+  // each warp then stages its kind's inverses in its half of s_half
+  __syncthreads();
+  const unsigned active = __ballot_sync(0xffffffffu, live);
+  if (!live) return;
+  double* stage = &s_half[half][0][0];
+  static_assert(kMonomials >= 27, "the stage holds 27 x 32 doubles");
   if (half == 0)
-    finish_a<1>(s, a, a.k0, i, pi);
+    finish_a<1>(s, a, a.k0, i, pi, stage, active);
   else
-    finish_a<2>(s, a, a.k1, i, pi);
+    finish_a<2>(s, a, a.k1, i, pi, stage, active);
 }
 
 // ---------------------------------------------------------------------------
