@@ -172,14 +172,15 @@ __device__ __forceinline__ void store_inverse(const double (&t)[N * (N + 1) / 2]
 
 // The inverse X = L^-T L^-1 from the inverted factor t, written by the
 // warp's active lanes together: in three passes of nine columns' 27 entries
-// each lane stages its particle's entries in shared memory (stage: 27 x 32
-// doubles), then the warp writes them particle by particle, 27 consecutive
+// each lane stages its particle's entries in shared memory (stage: 27 rows
+// of the warp's 32 lanes, `stride` doubles apart), then the warp writes them
+// particle by particle, 27 consecutive
 // doubles per store instruction, instead of 81 scattered 8-byte stores per
 // lane.  The active lanes are the lowest ones (lanes past the particle count
 // have left).  Same values as store_inverse (the same fused products in the
 // same order); NaN where the factorisation failed (ok = false).
 __device__ __forceinline__ void warp_store_inverse(const double (&t)[45], bool ok, double* out, double* stage,
-                                                   unsigned active) {
+                                                   int stride, unsigned active) {
   const int lane = threadIdx.x & (kWarp - 1);
   const int nact = __popc(active);
   const unsigned long long mine = reinterpret_cast<unsigned long long>(out);
@@ -194,14 +195,14 @@ __device__ __forceinline__ void warp_store_inverse(const double (&t)[45], bool o
         double x = 0.0;
 #pragma unroll
         for (int k = lo; k < 9; ++k) x = fma(t[tri(k, r)], t[tri(k, c)], x);
-        stage[(cc * 9 + r) * kWarp + lane] = ok ? x : __longlong_as_double(0x7ff8000000000000LL);
+        stage[(cc * 9 + r) * stride + lane] = ok ? x : __longlong_as_double(0x7ff8000000000000LL);
       }
     }
     __syncwarp(active);
     for (unsigned rem = active; rem; rem &= rem - 1) {
       const int p = __ffs(rem) - 1;
       double* op = reinterpret_cast<double*>(__shfl_sync(active, mine, p));
-      for (int e = lane; e < 27; e += nact) op[27 * pass + e] = stage[e * kWarp + p];
+      for (int e = lane; e < 27; e += nact) op[27 * pass + e] = stage[e * stride + p];
     }
     __syncwarp(active);
   }
@@ -423,7 +424,7 @@ struct MomentPackedArgs {
 template <int B>
 __device__ __forceinline__ void finish_a(double (&s)[kMonomials], const MomentPackedArgs& a, const KindOut& ko,
                                          index_t i, const double4& pi, double* stage = nullptr,
-                                         unsigned active = 0u) {
+                                         int stride = kWarp, unsigned active = 0u) {
   const index_t wb = a.wo[i], we = a.wo[i + 1];
   if (B == 1) {
     for (index_t o = wb; o < we; ++o) {
@@ -467,7 +468,7 @@ __device__ __forceinline__ void finish_a(double (&s)[kMonomials], const MomentPa
   double* out = ko.inverse + static_cast<size_t>(i) * 81;
   if (info == 0) invert_lower<9>(m);
   if (stage) {
-    warp_store_inverse(m, info == 0, out, stage, active);
+    warp_store_inverse(m, info == 0, out, stage, stride, active);
   } else if (info == 0) {
     store_inverse<9>(m, out);
   } else {
@@ -484,15 +485,21 @@ __device__ __forceinline__ void finish_a(double (&s)[kMonomials], const MomentPa
 
 // Type-A kinds B0 (and B1 >= 0) from one pass over the fluid row.  MinBlocks
 // is the register budget variant (LSMPS_KNOB_MOMENT_OCCUPANCY).
+// The last kind's inverses are written through shared memory by the warp
+// (warp_store_inverse; the first of two kinds with scalar stores, its
+// shared memory still holding the second kind's sums).
 template <int B0, int B1, int MinBlocks>
 __global__ void __launch_bounds__(kMomentThreads, MinBlocks) moment_a_kernel(MomentPackedArgs a) {
-  extern __shared__ double s_mono[];  // [kMonomials][kMomentThreads] when B1 >= 0
+  // [kMonomials][kMomentThreads] when B1 >= 0, else [27][kMomentThreads]
+  extern __shared__ double s_mono[];
   const index_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     if (a.k0.count) atomicAdd(a.k0.count, 1);
     if (B1 >= 0 && a.k1.count) atomicAdd(a.k1.count, 1);
   }
+  const unsigned active = __ballot_sync(0xffffffffu, t < a.n);
   if (t >= a.n) return;
+  double* stage = s_mono + (threadIdx.x & ~(kWarp - 1));
   const index_t i = visit(a.order, t);
   const double4 pi = ld4(a.fp, i);
   double s[kMonomials];
@@ -516,12 +523,14 @@ __global__ void __launch_bounds__(kMomentThreads, MinBlocks) moment_a_kernel(Mom
 #pragma unroll
     for (int e = 0; e < kMonomials; ++e) s_mono[e * kMomentThreads + threadIdx.x] = s[e];
   }
-  finish_a<B0>(s, a, a.k0, i, pi);
-  if (B1 >= 0) {
-#pragma unroll
-    for (int e = 0; e < kMonomials; ++e) s[e] = s_mono[e * kMomentThreads + threadIdx.x];
-    finish_a<(B1 < 0 ? 0 : B1)>(s, a, a.k1, i, pi);
+  if (B1 < 0) {
+    finish_a<B0>(s, a, a.k0, i, pi, stage, kMomentThreads, active);
+    return;
   }
+  finish_a<B0>(s, a, a.k0, i, pi);
+#pragma unroll
+  for (int e = 0; e < kMonomials; ++e) s[e] = s_mono[e * kMomentThreads + threadIdx.x];
+  finish_a<(B1 < 0 ? 0 : B1)>(s, a, a.k1, i, pi, stage, kMomentThreads, active);
 }
 
 // The velocity and pressure kinds with the two warps of a 64-thread block
@@ -575,9 +584,9 @@ __global__ void __launch_bounds__(2 * kWarp, 8) moment_a_split_kernel(MomentPack
   double* stage = &s_half[half][0][0];
   static_assert(kMonomials >= 27, "the stage holds 27 x 32 doubles");
   if (half == 0)
-    finish_a<1>(s, a, a.k0, i, pi, stage, active);
+    finish_a<1>(s, a, a.k0, i, pi, stage, kWarp, active);
   else
-    finish_a<2>(s, a, a.k1, i, pi, stage, active);
+    finish_a<2>(s, a, a.k1, i, pi, stage, kWarp, active);
 }
 
 // ---------------------------------------------------------------------------
@@ -1300,6 +1309,8 @@ lsmps_status prepare_moments_impl(lsmps_ctx* ctx, const lsmps_fluid& fluid, cons
                    mk.inversion_count};
   };
   const dim3 grid(div_up(n, kMomentThreads)), block(kMomentThreads);
+  // single-kind launches: the warps' inverse staging (27 x kMomentThreads doubles)
+  constexpr size_t kStageBytes = sizeof(double) * 27 * kMomentThreads;
   if (!ensure_packs(ctx, fluid.count, walls.count)) return fail(ctx, LSMPS_CUDA_ERROR, "pack allocation failed");
   pack4(ctx, fluid.x, fluid.y, fluid.z, nullptr, fluid.count, ctx->pack_fluid[0]);
   // (the mixed form packs the walls itself, after its fluid sums)
@@ -1338,10 +1349,10 @@ lsmps_status prepare_moments_impl(lsmps_ctx* ctx, const lsmps_fluid& fluid, cons
     a.k0 = out_of(kinds[k]);
     switch (kinds[k].kind) {
       case LSMPS_MOMENT_VELOCITY_WALL_DIRICHLET_A:
-        launch_named(ctx, "moment_a_kernel<V>", moment_a_kernel<1, -1, 1>, grid, block, 0, a);
+        launch_named(ctx, "moment_a_kernel<V>", moment_a_kernel<1, -1, 1>, grid, block, kStageBytes, a);
         break;
       case LSMPS_MOMENT_PRESSURE_WALL_NEUMANN_A:
-        launch_named(ctx, "moment_a_kernel<P>", moment_a_kernel<2, -1, 1>, grid, block, 0, a);
+        launch_named(ctx, "moment_a_kernel<P>", moment_a_kernel<2, -1, 1>, grid, block, kStageBytes, a);
         break;
       case LSMPS_MOMENT_PRESSURE_WALL_NEUMANN_B: {
         MomentArgs b = base;
@@ -1350,7 +1361,7 @@ lsmps_status prepare_moments_impl(lsmps_ctx* ctx, const lsmps_fluid& fluid, cons
         break;
       }
       default:
-        launch_named(ctx, "moment_a_kernel<F>", moment_a_kernel<0, -1, 1>, grid, block, 0, a);
+        launch_named(ctx, "moment_a_kernel<F>", moment_a_kernel<0, -1, 1>, grid, block, kStageBytes, a);
         break;
     }
   }
