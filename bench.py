@@ -335,67 +335,23 @@ def run_ours(args, world, rank, local):
 
         # end to end through the C ABI with host buffers: the particle state
         # lives in pinned host memory; every step copies it in, steps, and
-        # copies the moved fluid state back into the same host buffers, which
-        # the next step copies in again.  So each step's inputs are the
-        # previous step's outputs, consistent with the neighbour tables and
-        # labels that step rebuilt on the device.  The copies overlap the
-        # step where its data dependences allow (lsmps_ctx_set_step_events):
-        # the fluid positions go first; the wall geometry (read after the
-        # fluid moment sums), then the velocities, pressure, labels and wall
-        # velocities (read from the provision on) follow on a copy stream
-        # while the moments are built; the fluid positions, velocities and
-        # pressure go back while the neighbour rebuild and the labels run; the
-        # labels last.
+        # copies the moved fluid state and labels back into the same host
+        # buffers, which the next step copies in again.  So each step's
+        # inputs are the previous step's outputs, consistent with the
+        # neighbour tables and labels that step rebuilt on the device.  The
+        # copies overlap the steps where their data dependences allow
+        # (host_loop.HostResidentLoop: two device position buffers and the
+        # library's step events).
         e2e = None
         if not args.no_e2e:
+            host_loop = import_module("lsmps3d_b200.host_loop")
             ctx.set_precision(forms[-1][1])
             ctx.set_condition_threshold(forms[-1][2])
             reset()
-            first = [("fluid", k) for k in ("x", "y", "z")]
-            geometry = [("walls", k) for k in ("x", "y", "z", "normal_x", "normal_y", "normal_z")]
-            second = [("fluid", k) for k in ("vx", "vy", "vz", "pressure", "surface_type")] + \
-                     [("walls", k) for k in ("vx", "vy", "vz")]
-            out_early = [("fluid", k) for k in ("x", "y", "z", "vx", "vy", "vz", "pressure")]
-            out_late = [("fluid", "surface_type")]
-            host_in = {f: getattr(dev, f[0])[f[1]].detach().to("cpu").pin_memory() for f in first + geometry + second}
-            h2d = sum(t.numel() * t.element_size() for t in host_in.values())
-            d2h = sum(host_in[f].numel() * host_in[f].element_size() for f in out_early + out_late)
             k_e2e = max(1, min(args.steps, 5))
-            copy_stream = torch.cuda.Stream(device)
-            ev_wall, ev_in, ev_out = torch.cuda.Event(), torch.cuda.Event(), torch.cuda.Event()
-            ev_wall.record(copy_stream)  # creates the events before their handles are passed on
-            ev_in.record(copy_stream)
-            ev_out.record(stream)
-            ctx.set_step_events(ev_wall.cuda_event, ev_in.cuda_event, ev_out.cuda_event)
-
-            def dev_of(f):
-                return getattr(dev, f[0])[f[1]]
-
-            def e2e_step():
-                # the previous step's copies out are done before its host
-                # buffers are read again, and its labels before they are
-                # overwritten
-                stream.wait_stream(copy_stream)
-                copy_stream.wait_stream(stream)
-                for f in first:
-                    dev_of(f).copy_(host_in[f], non_blocking=True)
-                with torch.cuda.stream(copy_stream):
-                    for f in geometry:
-                        dev_of(f).copy_(host_in[f], non_blocking=True)
-                    ev_wall.record(copy_stream)
-                    for f in second:
-                        dev_of(f).copy_(host_in[f], non_blocking=True)
-                    ev_in.record(copy_stream)
-                ctx.step(dev, p, state)
-                copy_stream.wait_event(ev_out)
-                with torch.cuda.stream(copy_stream):
-                    for f in out_early:
-                        host_in[f].copy_(dev_of(f), non_blocking=True)
-                for f in out_late:
-                    host_in[f].copy_(dev_of(f), non_blocking=True)
-
-            e2e_step()
-            stream.wait_stream(copy_stream)
+            loop = host_loop.HostResidentLoop(ctx, dev, p)
+            loop.step()
+            loop.sync()
             ctx.synchronize()
             torch.cuda.synchronize(device)
             barrier(world)
@@ -403,17 +359,18 @@ def run_ours(args, world, rank, local):
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
             for _ in range(k_e2e):
-                e2e_step()
-            stream.wait_stream(copy_stream)
+                loop.step()
+            loop.sync()
             e1.record(stream)
             ctx.synchronize()
             torch.cuda.synchronize(device)
-            ctx.set_step_events(None, None, None)
+            loop.close()
             ms_e2e = max_over_ranks(world, e0.elapsed_time(e1) / k_e2e, device)
             e2e = {"value": world * case.n_fluid / (ms_e2e * 1e-3), "unit": "particles/s",
-                   "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e,
-                   "steps": k_e2e,
-                   "copies": "pinned host <-> device, overlapped with the step where its data dependences allow"}
+                   "h2d_bytes_per_step": loop.h2d_bytes, "d2h_bytes_per_step": loop.d2h_bytes,
+                   "ms_per_step": ms_e2e, "steps": k_e2e,
+                   "copies": "pinned host <-> device every step, overlapped with the steps where their data "
+                             "dependences allow (two device position buffers, step events)"}
         # The same forms on the splash variant whose lifted 5% is scattered
         # off the lattice (sparse, ill-conditioned Surface/Splash matrices):
         # the generator's lattice-column splash holds none at 2M, so this is
