@@ -37,7 +37,11 @@ class HostResidentLoop:
     host memory (`host_fluid`, `host_walls`: the buffers' current contents
     at construction).  step() queues one step and its copies; sync() waits
     for everything queued and leaves the host arrays holding the last
-    step's outputs; close() clears the context's step events."""
+    step's outputs; close() clears the context's step events.  Queue it on
+    the context's own stream (the current torch stream at construction) and
+    put the context in asynchronous mode (Context.set_synchronous(False)):
+    a synchronous context waits at the end of every step, which still gives
+    the same results but leaves less to overlap."""
 
     def __init__(self, ctx, buffers, params):
         import torch
