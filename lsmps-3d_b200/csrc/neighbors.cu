@@ -209,6 +209,11 @@ __global__ void __launch_bounds__(kCountWarps * kWarp) csr_count_kernel(CsrArgs 
     }
     if (lane == 0) pre[27] = nc;
     __syncwarp();
+    if (nc == 0) {
+      // no candidates (most home cells of the wall table): empty rows
+      for (index_t h = hb + lane; h < he; h += kWarp) a.offsets[a.home_sorted[h]] = 0;
+      continue;
+    }
     if (nc > kStageCap) {
       // More candidates than the stage holds (overloaded edge cells): exact
       // tests straight from global memory; only the count is needed here.
@@ -396,6 +401,13 @@ __global__ void __launch_bounds__(kCsrThreads) csr_count_cell_kernel(CsrArgs a) 
     }
     __syncthreads();
     const index_t nc = s_pre[27];
+    if (nc == 0) {
+      // no candidates: empty rows (every thread has read nc before warp 0
+      // moves on to the next cell)
+      for (index_t h = hb + threadIdx.x; h < he; h += kCsrThreads) a.offsets[a.home_sorted[h]] = 0;
+      __syncthreads();
+      continue;
+    }
     const double ccx = fr.origin[0] + (cx + 0.5) * a.grid.cell_size;
     const double ccy = fr.origin[1] + (cy + 0.5) * a.grid.cell_size;
     const double ccz = fr.origin[2] + (cz + 0.5) * a.grid.cell_size;
@@ -559,6 +571,12 @@ __global__ void __launch_bounds__(kCsrThreads) csr_write_kernel(CsrArgs a) {
     }
     __syncthreads();
     const index_t nc = s_pre[27];
+    if (nc == 0) {
+      // no candidates, so no rows to write (every thread has read nc before
+      // warp 0 moves on to the next cell)
+      __syncthreads();
+      continue;
+    }
     const bool staged = nc <= kStageCap;
     if (staged) {
       int t = 0;  // each thread's source cell only moves forward
