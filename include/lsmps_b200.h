@@ -294,6 +294,19 @@ lsmps_status lsmps_ctx_set_condition_threshold(lsmps_ctx* ctx, double threshold)
  * neighbours' records in cache) when this context built that list last
  * (1, the default), or in index order (0).  Results are identical either way. */
 lsmps_status lsmps_ctx_set_cell_order(lsmps_ctx* ctx, int on);
+/* Cell-sorted rows (1, the default): this context's builds of the fluid table
+ * also write, beside every entry's neighbour index, the neighbour's position in
+ * the fluid cell list (context memory, 4 bytes per entry of the table's
+ * capacity), and while lsmps_step visits the fluid in cell order its gather
+ * kernels read those rows and neighbour records packed in cell order, so the
+ * records of a home cell's neighbours lie in a few contiguous runs whatever
+ * the caller's particle numbering.  The tables, and every result, are the
+ * same either way; 0 reads the rows' indices and records in index order. */
+lsmps_status lsmps_ctx_set_sorted_rows(lsmps_ctx* ctx, int on);
+/* Copy the first `count` entries of the cell-sorted rows this context holds
+ * (of its last build of the fluid table) to device memory `dst`, on the
+ * context's stream; LSMPS_NOT_PREPARED when none are held. */
+lsmps_status lsmps_ctx_copy_sorted_rows(lsmps_ctx* ctx, int32_t* dst, size_t count);
 uint64_t lsmps_ctx_fp64_fallbacks(lsmps_ctx* ctx);
 /* Launch-shape knobs (no counterpart in the reference, whose kernels all use
  * one thread per particle in 128-thread blocks).  Values are indices into each

@@ -306,6 +306,8 @@ _SIGNATURES = {
     "lsmps_ctx_set_profiling": (c_int, [c_void_p, c_int]),
     "lsmps_ctx_set_condition_threshold": (c_int, [c_void_p, c_double]),
     "lsmps_ctx_set_cell_order": (c_int, [c_void_p, c_int]),
+    "lsmps_ctx_set_sorted_rows": (c_int, [c_void_p, c_int]),
+    "lsmps_ctx_copy_sorted_rows": (c_int, [c_void_p, c_void_p, c_size_t]),
     "lsmps_ctx_set_adjoint_atomic": (c_int, [c_void_p, c_int]),
     "lsmps_ctx_fp64_fallbacks": (c_uint64, [c_void_p]),
     "lsmps_ctx_set_knob": (c_int, [c_void_p, c_int, c_int]),

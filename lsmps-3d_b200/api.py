@@ -110,6 +110,20 @@ class Context:
         """lsmps_step visits the fluid in cell order (default) or index order."""
         self.check(_lib.lsmps_ctx_set_cell_order(self.h, 1 if on else 0))
 
+    def sorted_rows(self, count: int):
+        """The first `count` entries of the context's cell-sorted rows (numpy)."""
+        import torch
+
+        out = torch.empty(max(count, 1), dtype=torch.int32, device=f"cuda:{self.device}")
+        self.check(_lib.lsmps_ctx_copy_sorted_rows(self.h, ctypes.c_void_p(out.data_ptr()), count))
+        torch.cuda.synchronize()
+        return out[:count].cpu().numpy()
+
+    def set_sorted_rows(self, on: bool) -> None:
+        """lsmps_step's gathers read cell-sorted rows and records (default)
+        or the rows' indices and records in index order."""
+        self.check(_lib.lsmps_ctx_set_sorted_rows(self.h, 1 if on else 0))
+
     def set_adjoint_atomic(self, on: bool) -> None:
         """Operator backward: scatter with FP64 atomics (True) or the
         deterministic transpose + gather (False, the default)."""

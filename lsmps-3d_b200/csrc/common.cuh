@@ -155,6 +155,10 @@ __device__ __forceinline__ index_t visit(const int32_t* __restrict__ order, inde
   return order ? order[t] : t;
 }
 
+// Where the particle visited at position t finds its own packed record: at t
+// when the records are packed in cell-sorted (visiting) order, else at i.
+__device__ __forceinline__ index_t self_of(int sorted, index_t t, index_t i) { return sorted ? t : i; }
+
 // Sum over the lanes of a group; every lane of the group ends with the total.
 template <int G>
 __device__ __forceinline__ double group_sum(double v, unsigned mask) {
@@ -217,6 +221,25 @@ struct lsmps_ctx {
   // the fluid, is used as a visiting order.
   const int32_t* built_order = nullptr;
   size_t built_order_count = 0;
+  // Cell-sorted rows of the fluid table: for every CSR entry, the neighbour's
+  // position in the fluid cell list (its sorted position) instead of its
+  // index, written by this context's builds of the table next to the indices
+  // (capacity: entries), and the table (offsets array), cell list and particle
+  // count they describe (spos_table NULL: none valid).  While lsmps_step
+  // visits the fluid in the order of that cell list, its gather kernels read
+  // these rows and fluid records packed in cell-sorted order, so a home
+  // cell's neighbours come from a few contiguous runs of records whatever
+  // the caller's numbering (sorted_rows; results identical either way).
+  // sorted_labels holds the labels in cell-sorted order for the NearSurface
+  // expansion.
+  int32_t* fluid_spos = nullptr;
+  size_t fluid_spos_cap = 0;
+  int32_t* sorted_labels = nullptr;
+  size_t sorted_labels_cap = 0;
+  const int32_t* spos_table = nullptr;
+  const int32_t* spos_order = nullptr;
+  size_t spos_count = 0;
+  bool sorted_rows = true;
   // CSR count pass shape: false = warp per home cell, lane per home particle
   // (the fastest on a GPU the build has to itself); true = block per home
   // cell, warp per two home particles, which leaves the streams of a batched
@@ -302,6 +325,9 @@ class Scratch {
 // Grow the pack arrays to hold nf fluid and nw wall records (outside stream
 // capture; returns false if that is impossible).
 bool ensure_packs(lsmps_ctx* ctx, size_t nf, size_t nw);
+// The cell-sorted row array for `entries` fluid CSR entries and the sorted
+// label array for nf particles (outside capture; false: not available).
+bool ensure_sorted_rows(lsmps_ctx* ctx, size_t entries, size_t nf);
 // Grow the mixed-form arrays to nf fluid particles (outside stream capture).
 bool ensure_mixed(lsmps_ctx* ctx, size_t nf);
 void free_mixed(lsmps_ctx* ctx);

@@ -104,6 +104,38 @@ bool ensure_packs(lsmps_ctx* ctx, size_t nf, size_t nw) {
   return true;
 }
 
+bool ensure_sorted_rows(lsmps_ctx* ctx, size_t entries, size_t nf) {
+  if (entries <= ctx->fluid_spos_cap && nf <= ctx->sorted_labels_cap) return true;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  cudaStreamIsCapturing(ctx->stream, &cap);
+  if (cap != cudaStreamCaptureStatusNone) return false;
+  cudaStreamSynchronize(ctx->stream);
+  ctx->spos_table = nullptr;
+  if (entries > ctx->fluid_spos_cap) {
+    if (ctx->fluid_spos) cudaFree(ctx->fluid_spos);
+    ctx->fluid_spos = nullptr;
+    ctx->fluid_spos_cap = 0;
+    if (cudaMalloc(&ctx->fluid_spos, entries * sizeof(int32_t)) != cudaSuccess) {
+      cudaGetLastError();
+      ctx->fluid_spos = nullptr;
+      return false;
+    }
+    ctx->fluid_spos_cap = entries;
+  }
+  if (nf > ctx->sorted_labels_cap) {
+    if (ctx->sorted_labels) cudaFree(ctx->sorted_labels);
+    ctx->sorted_labels = nullptr;
+    ctx->sorted_labels_cap = 0;
+    if (cudaMalloc(&ctx->sorted_labels, nf * sizeof(int32_t)) != cudaSuccess) {
+      cudaGetLastError();
+      ctx->sorted_labels = nullptr;
+      return false;
+    }
+    ctx->sorted_labels_cap = nf;
+  }
+  return true;
+}
+
 lsmps_status fail(lsmps_ctx* ctx, lsmps_status st, const char* what) {
   if (ctx) ctx->last_error = what;
   return st;
@@ -222,6 +254,8 @@ void lsmps_ctx_destroy(lsmps_ctx* ctx) {
     if (p) cudaFree(p);
   for (auto p : ctx->pack_wall)
     if (p) cudaFree(p);
+  if (ctx->fluid_spos) cudaFree(ctx->fluid_spos);
+  if (ctx->sorted_labels) cudaFree(ctx->sorted_labels);
   free_mixed(ctx);
   free_adjoint(ctx);
   free_step_ops(ctx);

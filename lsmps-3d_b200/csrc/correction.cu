@@ -46,6 +46,7 @@ struct GatherArgs {
   const double4* wp = nullptr;
   const double4* wn = nullptr;
   const int32_t* order = nullptr;  // visiting order of the fused kernel (lsmps_ctx::order) or NULL
+  int sorted = 0;  // fused kernels: fi and fpp in cell-sorted positions (sorted_rows_of)
 };
 
 // compute_pressure_gradient_kernel, pressure_correction.cu:200-276
@@ -252,16 +253,17 @@ __global__ void __launch_bounds__(kThreads) smooth_kernel(index_t n, const doubl
                                                           const index_t* __restrict__ fo,
                                                           const index_t* __restrict__ fi, double re, double strength,
                                                           double* ox, double* oy, double* oz,
-                                                          const int32_t* __restrict__ order) {
+                                                          const int32_t* __restrict__ order, int sorted) {
   // G lanes per particle (lane l takes entries l, l + G, ...); the group
   // leaves or continues as a whole.
   const index_t t = (blockIdx.x * blockDim.x + threadIdx.x) / G;
   const int l = threadIdx.x & (G - 1);
   if (t >= n) return;
   const index_t i = visit(order, t);
+  const index_t self = self_of(sorted, t, i);
   const double inv_re = 1.0 / re;
   constexpr double kSplash = static_cast<double>(LSMPS_SURFACE_SPLASH);
-  const double4 ui = ld4(fv, i);
+  const double4 ui = ld4(fv, self);
   if (strength <= 0.0 || ui.w == kSplash) {
     if (l == 0) {
       ox[i] = ui.x;
@@ -270,7 +272,7 @@ __global__ void __launch_bounds__(kThreads) smooth_kernel(index_t n, const doubl
     }
     return;
   }
-  const double4 pi = ld4(fp, i);
+  const double4 pi = ld4(fp, self);
   double ws = 0.0, ax = 0.0, ay = 0.0, az = 0.0;
   const index_t fe = fo[i + 1];
   index_t o = fo[i] + l;
@@ -419,26 +421,30 @@ lsmps_status smooth_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const lsmps_csr& 
   if (f.count == 0) return LSMPS_OK;
   if (const lsmps_status cs = check_neighbor_tables(ctx, f.count, 0, fn, nullptr)) return cs;
   if (!ensure_packs(ctx, f.count, 0)) return fail(ctx, LSMPS_CUDA_ERROR, "pack allocation failed");
-  pack4(ctx, f.x, f.y, f.z, nullptr, f.count, ctx->pack_fluid[0]);
-  pack4_label(ctx, f.vx, f.vy, f.vz, f.surface_type, f.count, ctx->pack_fluid[1]);
+  const index_t* srows = sorted_rows_of(ctx, fn, f.count);
+  const index_t* pord = srows ? ctx->order : nullptr;
+  const index_t* fi = srows ? srows : static_cast<const index_t*>(fn.indices);
+  const int sorted = srows ? 1 : 0;
+  pack4(ctx, f.x, f.y, f.z, nullptr, f.count, ctx->pack_fluid[0], pord);
+  pack4_label(ctx, f.vx, f.vy, f.vz, f.surface_type, f.count, ctx->pack_fluid[1], pord);
   const long long n = static_cast<long long>(f.count);
   const double4* fp = ctx->pack_fluid[0];
   const double4* fv = ctx->pack_fluid[1];
   switch (ctx->knob[LSMPS_KNOB_GATHER_LANES]) {
     case 1:
       launch(ctx, smooth_kernel<2>, dim3(div_up(2 * n, kThreads)), dim3(kThreads), 0, static_cast<index_t>(n), fp, fv,
-             static_cast<const index_t*>(fn.offsets), static_cast<const index_t*>(fn.indices), p.support_radius,
-             p.velocity_smoothing_strength, sm.x, sm.y, sm.z, ctx->order);
+             static_cast<const index_t*>(fn.offsets), fi, p.support_radius, p.velocity_smoothing_strength, sm.x,
+             sm.y, sm.z, ctx->order, sorted);
       break;
     case 2:
       launch(ctx, smooth_kernel<4>, dim3(div_up(4 * n, kThreads)), dim3(kThreads), 0, static_cast<index_t>(n), fp, fv,
-             static_cast<const index_t*>(fn.offsets), static_cast<const index_t*>(fn.indices), p.support_radius,
-             p.velocity_smoothing_strength, sm.x, sm.y, sm.z, ctx->order);
+             static_cast<const index_t*>(fn.offsets), fi, p.support_radius, p.velocity_smoothing_strength, sm.x,
+             sm.y, sm.z, ctx->order, sorted);
       break;
     default:
       launch(ctx, smooth_kernel<1>, dim3(div_up(n, kThreads)), dim3(kThreads), 0, static_cast<index_t>(n), fp, fv,
-             static_cast<const index_t*>(fn.offsets), static_cast<const index_t*>(fn.indices), p.support_radius,
-             p.velocity_smoothing_strength, sm.x, sm.y, sm.z, ctx->order);
+             static_cast<const index_t*>(fn.offsets), fi, p.support_radius, p.velocity_smoothing_strength, sm.x,
+             sm.y, sm.z, ctx->order, sorted);
       break;
   }
   if (copy_back)
@@ -483,7 +489,7 @@ struct GradShiftOut {
 // shuffles and lane 0 finishes the particle.
 template <bool Mixed, int G>
 __device__ __forceinline__ void gradient_shifting_of(const GatherArgs& a, const GradShiftOut& out, index_t i,
-                                                     int l) {
+                                                     index_t self, int l) {
   double* pressure = out.pressure;
   double* fluid_pressure = out.fluid_pressure;
   const double* __restrict__ pinv = out.pinv;
@@ -506,7 +512,7 @@ __device__ __forceinline__ void gradient_shifting_of(const GatherArgs& a, const 
     }
     return;
   }
-  const double4 own = ld4(a.fpp, i);
+  const double4 own = ld4(a.fpp, self);
   const double xi = own.x, yi = own.y, zi = own.z;
   const double inv_re = 1.0 / re;
   const double dmin = a.p.ps_min_distance_ratio * a.p.particle_spacing;
@@ -652,7 +658,8 @@ __global__ void __launch_bounds__(kThreads, 6) gradient_shifting_kernel(GatherAr
   const index_t t = static_cast<index_t>(tt / G);
   const int l = static_cast<int>(tt % G);
   if (t >= static_cast<index_t>(a.fluid.count)) return;  // the whole group
-  gradient_shifting_of<Mixed, G>(a, out, visit(a.order, t), l);
+  const index_t i = visit(a.order, t);
+  gradient_shifting_of<Mixed, G>(a, out, i, self_of(a.sorted, t, i), l);
 }
 
 // The FP64-route particles of the pressure kind (gradient_shifting_of<true,
@@ -662,8 +669,11 @@ __global__ void __launch_bounds__(kThreads, 6) gradient_shifting_list_kernel(Gat
   const index_t groups = static_cast<index_t>(gridDim.x * blockDim.x / G);
   const int l = threadIdx.x & (G - 1);
   const index_t count = static_cast<index_t>(*out.prows.count);
-  for (index_t t = static_cast<index_t>((blockIdx.x * blockDim.x + threadIdx.x) / G); t < count; t += groups)
-    gradient_shifting_of<true, G>(a, out, out.prows.list[t], l);
+  for (index_t t = static_cast<index_t>((blockIdx.x * blockDim.x + threadIdx.x) / G); t < count; t += groups) {
+    const index_t vt = out.prows.list[t];  // a visiting position
+    const index_t i = visit(a.order, vt);
+    gradient_shifting_of<true, G>(a, out, i, self_of(a.sorted, vt, i), l);
+  }
 }
 
 // Mixed form with FP32 arithmetic for the gradient: each neighbour's offset
@@ -698,7 +708,7 @@ __global__ void __launch_bounds__(kThreads, 6) gradient32_kernel(GatherArgs a, G
     }
     return;
   }
-  const double4 own = ld4(a.fpp, i);
+  const double4 own = ld4(a.fpp, self_of(a.sorted, t, i));
   const double inv_re = 1.0 / out.re;
   const double dmin = a.p.ps_min_distance_ratio * a.p.particle_spacing;
   const float dmin_s2 = static_cast<float>(dmin * inv_re * dmin * inv_re) * (1.0f + 1e-5f);
@@ -935,9 +945,11 @@ lsmps_status gradient_shifting_stage(lsmps_ctx* ctx, const lsmps_fluid& f, const
                                      const lsmps_vector& s, bool mixed) {
   if (f.count == 0) return LSMPS_OK;
   if (const lsmps_status cs = check_neighbor_tables(ctx, f.count, w.count, fn, &wn)) return cs;
-  GatherArgs a{f, w, fn.offsets, fn.indices, wn.offsets, wn.indices, p};
+  const index_t* srows = sorted_rows_of(ctx, fn, f.count);
+  GatherArgs a{f, w, fn.offsets, srows ? srows : fn.indices, wn.offsets, wn.indices, p};
+  a.sorted = srows ? 1 : 0;
   if (!ensure_packs(ctx, f.count, w.count)) return fail(ctx, LSMPS_CUDA_ERROR, "pack allocation failed");
-  pack4(ctx, f.x, f.y, f.z, pressure, f.count, ctx->pack_fluid[0]);
+  pack4(ctx, f.x, f.y, f.z, pressure, f.count, ctx->pack_fluid[0], srows ? ctx->order : nullptr);
   pack4(ctx, w.x, w.y, w.z, nullptr, w.count, ctx->pack_wall[0]);
   pack4(ctx, w.normal_x, w.normal_y, w.normal_z, nullptr, w.count, ctx->pack_wall[2]);
   a.fpp = ctx->pack_fluid[0];

@@ -7,6 +7,19 @@
 
 namespace lsmps {
 
+// The cell-sorted rows of fluid table fn (n particles) when the gathers may
+// read them: this context's last build of that table wrote them for the cell
+// list the fluid is being visited by (lsmps_ctx::order, set inside
+// lsmps_step).  The gathers then read these rows and fluid records packed in
+// that order (pack4's `order`), and a particle finds its own record at its
+// visiting position (self_of).  NULL: CSR indices and records by index.
+inline const index_t* sorted_rows_of(const lsmps_ctx* ctx, const lsmps_csr& fn, size_t n) {
+  return (ctx->sorted_rows && ctx->order && ctx->spos_table == fn.offsets && ctx->spos_order == ctx->order &&
+          ctx->spos_count == n && n > 0)
+             ? ctx->fluid_spos
+             : nullptr;
+}
+
 double reference_number_density(double l0, double re);
 lsmps_status classify_surface_impl(lsmps_ctx* ctx, const lsmps_fluid& fluid, const lsmps_walls& walls,
                                    const lsmps_csr& fn, const lsmps_csr& wn, const lsmps_params& p,

@@ -419,6 +419,7 @@ struct MomentPackedArgs {
   KindOut k1;
   DeviceStatus* status;
   const int32_t* order;  // visiting order (lsmps_ctx::order) or NULL
+  int sorted;            // fi and fp in cell-sorted positions (sorted_rows_of)
 };
 
 template <int B>
@@ -501,7 +502,7 @@ __global__ void __launch_bounds__(kMomentThreads, MinBlocks) moment_a_kernel(Mom
   if (t >= a.n) return;
   double* stage = s_mono + (threadIdx.x & ~(kWarp - 1));
   const index_t i = visit(a.order, t);
-  const double4 pi = ld4(a.fp, i);
+  const double4 pi = ld4(a.fp, self_of(a.sorted, t, i));
   double s[kMonomials];
 #pragma unroll
   for (int e = 0; e < kMonomials; ++e) s[e] = 0.0;
@@ -549,7 +550,7 @@ __global__ void __launch_bounds__(2 * kWarp, 8) moment_a_split_kernel(MomentPack
   }
   const bool live = t < a.n;
   const index_t i = live ? visit(a.order, t) : 0;
-  const double4 pi = live ? ld4(a.fp, i) : make_double4(0.0, 0.0, 0.0, 0.0);
+  const double4 pi = live ? ld4(a.fp, self_of(a.sorted, t, i)) : make_double4(0.0, 0.0, 0.0, 0.0);
   double s[kMonomials];
 #pragma unroll
   for (int e = 0; e < kMonomials; ++e) s[e] = 0.0;
@@ -627,6 +628,7 @@ struct MixedSumArgs {
   double inv_re;
   double* sums;          // [kMonomials][n], by visiting position
   const int32_t* order;  // visiting order (lsmps_ctx::order) or NULL
+  int sorted;            // fi and fp in cell-sorted positions (sorted_rows_of)
 };
 
 // Kahan step for the 31 weighted monomials of one neighbour (the same
@@ -693,7 +695,7 @@ __global__ void __launch_bounds__(kSumThreads) moment_sums_kernel(MixedSumArgs a
   const index_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= a.n) return;
   const index_t i = visit(a.order, t);
-  const double4 pi = ld4(a.fp, i);
+  const double4 pi = ld4(a.fp, self_of(a.sorted, t, i));
   // Kahan sums and compensations, two monomials per register pair
   f32x2 sum[16], comp[16];
 #pragma unroll
@@ -754,10 +756,11 @@ struct MixedRowArgs {
   float* rows[2];     // compact FP32 rows per kind (unless Full)
   double* rows64[2];  // compact FP64 rows of the FP64-route particles (unless Full)
   uint8_t* flag[2];   // 1 where rows64 holds the particle's rows (unless Full)
-  int32_t* list[2];   // the FP64-route particles, appended (unless Full)
+  int32_t* list[2];   // the FP64-route particles' visiting positions, appended (unless Full)
   unsigned int* count;
   DeviceStatus* status;
   const int32_t* order;  // visiting order (the sums are stored by visiting position) or NULL
+  int sorted;            // fi and fp in cell-sorted positions (sorted_rows_of)
 };
 
 // v <- L^-T L^-1 v with the packed lower factor and its reciprocal diagonal.
@@ -938,10 +941,12 @@ __device__ __forceinline__ double assemble_kind(const MixedRowArgs& a, int kind,
   return trace;
 }
 
-// Stage 2 of one particle and kind from its fluid monomial totals s (the
-// thread's column of shared memory m holds the kind's matrix).
+// Stage 2 of one particle (index i, visiting position vt: what the FP64-route
+// list records) and kind from its fluid monomial totals s (the thread's
+// column of shared memory m holds the kind's matrix).
 template <bool Full>
-__device__ __forceinline__ void mixed_rows_of_particle(const MixedRowArgs& a, int kind, index_t i, const double4& pi,
+__device__ __forceinline__ void mixed_rows_of_particle(const MixedRowArgs& a, int kind, index_t vt, index_t i,
+                                                       const double4& pi,
                                                        double (&s)[kMonomials], double* m) {
   const KindOut& ko = a.k[kind];
   constexpr int kTargets = Full ? 9 : 4;
@@ -1073,7 +1078,7 @@ __device__ __forceinline__ void mixed_rows_of_particle(const MixedRowArgs& a, in
   ko.reg[i] = reg;
   if (!Full) {
     a.flag[kind][i] = 1;
-    a.list[kind][atomicAdd(&a.count[kind], 1u)] = i;
+    a.list[kind][atomicAdd(&a.count[kind], 1u)] = vt;
   }
   double l64[45];
 #pragma unroll
@@ -1113,7 +1118,7 @@ __global__ void __launch_bounds__(kRowThreads, 6) moment_rows_kernel(MixedRowArg
   double s[kMonomials];
 #pragma unroll
   for (int e = 0; e < kMonomials; ++e) s[e] = a.sums[e * n + t];
-  mixed_rows_of_particle<Full>(a, kind, i, ld4(a.fp, i), s, s_m + threadIdx.x);
+  mixed_rows_of_particle<Full>(a, kind, t, i, ld4(a.fp, self_of(a.sorted, t, i)), s, s_m + threadIdx.x);
 }
 
 // Both stages in one kernel (the step's path): the two warps of a 64-thread
@@ -1130,7 +1135,7 @@ __global__ void __launch_bounds__(kRowThreads, 6) moment_mixed_split_kernel(Mixe
   if (blockIdx.x == 0 && lane == 0 && a.k[half].count) atomicAdd(a.k[half].count, 1);
   const bool live = t < a.n;
   const index_t i = live ? visit(a.order, t) : 0;
-  const double4 pi = live ? ld4(a.fp, i) : make_double4(0.0, 0.0, 0.0, 0.0);
+  const double4 pi = live ? ld4(a.fp, self_of(a.sorted, t, i)) : make_double4(0.0, 0.0, 0.0, 0.0);
   {
     float sum[kMonomials], comp[kMonomials];
 #pragma unroll
@@ -1161,7 +1166,7 @@ __global__ void __launch_bounds__(kRowThreads, 6) moment_mixed_split_kernel(Mixe
   double s[kMonomials];
 #pragma unroll
   for (int e = 0; e < kMonomials; ++e) s[e] = s_half[0][e][lane] + s_half[1][e][lane];
-  mixed_rows_of_particle<Full>(a, half, i, pi, s, s_m + threadIdx.x);
+  mixed_rows_of_particle<Full>(a, half, t, i, pi, s, s_m + threadIdx.x);
 }
 
 // make_matrix_request, moment_matrix.cu:494-538: boundary of each kind.
@@ -1185,7 +1190,9 @@ lsmps_status launch_mixed(lsmps_ctx* ctx, index_t n, const lsmps_csr& fn, const 
                           const lsmps_walls& walls) {
   if (!ensure_mixed(ctx, static_cast<size_t>(n))) return fail(ctx, LSMPS_CUDA_ERROR, "mixed-form allocation failed");
   const double inv_re = 1.0 / p.support_radius;
-  MixedSumArgs sa{n, ctx->pack_fluid[0], fn.offsets, fn.indices, inv_re, ctx->mixed_sums, ctx->order};
+  const index_t* srows = sorted_rows_of(ctx, fn, static_cast<size_t>(n));
+  const index_t* fi = srows ? srows : fn.indices;
+  MixedSumArgs sa{n, ctx->pack_fluid[0], fn.offsets, fi, inv_re, ctx->mixed_sums, ctx->order, srows ? 1 : 0};
   const bool split = ctx->knob[LSMPS_KNOB_MOMENT_OCCUPANCY] == 2;
   MixedRowArgs ra{};
   ra.n = n;
@@ -1202,7 +1209,8 @@ lsmps_status launch_mixed(lsmps_ctx* ctx, index_t n, const lsmps_csr& fn, const 
   ra.k[0] = kv;
   ra.k[1] = kp;
   ra.fo = fn.offsets;
-  ra.fi = fn.indices;
+  ra.fi = fi;
+  ra.sorted = srows ? 1 : 0;
   for (int k = 0; k < 2; ++k) {
     ra.rows[k] = ctx->mixed_rows[k];
     ra.rows64[k] = ctx->mixed_rows64[k];
@@ -1258,7 +1266,8 @@ lsmps_status mixed_step_moments_impl(lsmps_ctx* ctx, const lsmps_fluid& fluid, c
       !pm.info)
     return fail(ctx, LSMPS_INVALID_ARGUMENT, "Invalid Moment matrix cache buffers");
   if (!ensure_packs(ctx, fluid.count, walls.count)) return fail(ctx, LSMPS_CUDA_ERROR, "pack allocation failed");
-  pack4(ctx, fluid.x, fluid.y, fluid.z, nullptr, fluid.count, ctx->pack_fluid[0]);
+  pack4(ctx, fluid.x, fluid.y, fluid.z, nullptr, fluid.count, ctx->pack_fluid[0],
+        sorted_rows_of(ctx, fn, fluid.count) ? ctx->order : nullptr);
   const KindOut kv{1, vm.inverse_matrices, vm.moment_trace, vm.regularization_added, vm.info, vm.inversion_count};
   const KindOut kp{2, pm.inverse_matrices, pm.moment_trace, pm.regularization_added, pm.info, pm.inversion_count};
   lsmps_status st = launch_mixed(ctx, n, fn, wn, p, kv, kp, false, walls);
@@ -1312,16 +1321,17 @@ lsmps_status prepare_moments_impl(lsmps_ctx* ctx, const lsmps_fluid& fluid, cons
   // single-kind launches: the warps' inverse staging (27 x kMomentThreads doubles)
   constexpr size_t kStageBytes = sizeof(double) * 27 * kMomentThreads;
   if (!ensure_packs(ctx, fluid.count, walls.count)) return fail(ctx, LSMPS_CUDA_ERROR, "pack allocation failed");
-  pack4(ctx, fluid.x, fluid.y, fluid.z, nullptr, fluid.count, ctx->pack_fluid[0]);
+  const index_t* srows = sorted_rows_of(ctx, fn, fluid.count);
+  pack4(ctx, fluid.x, fluid.y, fluid.z, nullptr, fluid.count, ctx->pack_fluid[0], srows ? ctx->order : nullptr);
   // (the mixed form packs the walls itself, after its fluid sums)
   const bool fused = velocity_a >= 0 && pressure_a >= 0;
   if (!(fused && ctx->precision == LSMPS_PRECISION_MIXED)) {
     pack4(ctx, walls.x, walls.y, walls.z, nullptr, walls.count, ctx->pack_wall[0]);
     pack4(ctx, walls.normal_x, walls.normal_y, walls.normal_z, nullptr, walls.count, ctx->pack_wall[2]);
   }
-  MomentPackedArgs pa{n, ctx->pack_fluid[0], ctx->pack_wall[0], ctx->pack_wall[2], fn.offsets, fn.indices,
-                      wn.offsets, wn.indices, base.inv_re, base.lambda, base.wall_scale, KindOut{}, KindOut{},
-                      ctx->d_status, ctx->order};
+  MomentPackedArgs pa{n, ctx->pack_fluid[0], ctx->pack_wall[0], ctx->pack_wall[2], fn.offsets,
+                      srows ? srows : fn.indices, wn.offsets, wn.indices, base.inv_re, base.lambda,
+                      base.wall_scale, KindOut{}, KindOut{}, ctx->d_status, ctx->order, srows ? 1 : 0};
   const bool capped = ctx->knob[LSMPS_KNOB_MOMENT_OCCUPANCY] == 1;
   const bool split = ctx->knob[LSMPS_KNOB_MOMENT_OCCUPANCY] == 2;
   if (fused && ctx->precision == LSMPS_PRECISION_MIXED) {

@@ -69,6 +69,9 @@ struct CsrArgs {
   int exclude_self;
   index_t* offsets;  // count pass: per-particle counts; write pass: row offsets
   index_t* indices;
+  // write pass, or NULL: each entry's sorted position (the position of the
+  // neighbour in the source cell list) beside its index
+  index_t* spos;
   unsigned long long capacity;
   const index_t* total;  // write pass: offsets[N]
   // Per home particle, one 32-bit accept mask per 32 staged candidates
@@ -522,6 +525,7 @@ __device__ __forceinline__ int nth_set_bit(unsigned w, int n, const unsigned cha
 // gives each chunk's base), so rows come out in the reference's order.
 __global__ void __launch_bounds__(kCsrThreads) csr_write_kernel(CsrArgs a) {
   __shared__ index_t s_idx[kStageCap];
+  __shared__ index_t s_sp[kStageCap];  // the candidates' sorted positions (a.spos only)
   __shared__ index_t s_cb[27];
   __shared__ index_t s_cnt[27];
   __shared__ index_t s_pre[28];
@@ -582,7 +586,9 @@ __global__ void __launch_bounds__(kCsrThreads) csr_write_kernel(CsrArgs a) {
       int t = 0;  // each thread's source cell only moves forward
       for (index_t k = threadIdx.x; k < nc; k += kCsrThreads) {
         while (s_pre[t + 1] <= k) ++t;
-        s_idx[k] = a.src_sorted[s_cb[t] + (k - s_pre[t])];
+        const index_t pos = s_cb[t] + (k - s_pre[t]);
+        s_idx[k] = a.src_sorted[pos];
+        s_sp[k] = pos;
       }
     }
     __syncthreads();
@@ -618,7 +624,10 @@ __global__ void __launch_bounds__(kCsrThreads) csr_write_kernel(CsrArgs a) {
           if (e < total) {
             const unsigned long long pos = static_cast<unsigned long long>(out) + e;
             const int bit = nth_set_bit(m, e - cbase, s_nth);
-            if (pos < a.capacity) a.indices[pos] = s_idx[ch * kWarp + bit];
+            if (pos < a.capacity) {
+              a.indices[pos] = s_idx[ch * kWarp + bit];
+              if (a.spos) a.spos[pos] = s_sp[ch * kWarp + bit];
+            }
           }
         }
         __syncwarp();
@@ -641,7 +650,10 @@ __global__ void __launch_bounds__(kCsrThreads) csr_write_kernel(CsrArgs a) {
           const unsigned m = __ballot_sync(0xffffffffu, pass);
           if (pass) {
             const unsigned long long pos = static_cast<unsigned long long>(out) + __popc(m & lanemask_lt);
-            if (pos < a.capacity) a.indices[pos] = j;
+            if (pos < a.capacity) {
+              a.indices[pos] = j;
+              if (a.spos) a.spos[pos] = b + k;
+            }
           }
           out += __popc(m);
         }
@@ -654,7 +666,7 @@ __global__ void __launch_bounds__(kCsrThreads) csr_write_kernel(CsrArgs a) {
 lsmps_status one_neighbor_list(lsmps_ctx* ctx, Scratch& scratch, const lsmps_fluid& fluid, const double* sx,
                                const double* sy, const double* sz, const lsmps_cells& home, const lsmps_cells& src,
                                const lsmps_grid& grid, double radius, bool exclude_self, const lsmps_csr& out,
-                               size_t n_src, unsigned* bits, double4* src_pos) {
+                               size_t n_src, unsigned* bits, double4* src_pos, index_t* spos) {
   if (fluid.count > out.particle_count || !out.offsets)
     return fail(ctx, LSMPS_INVALID_ARGUMENT, "Neighbor list particle capacity is smaller than fluid count");
   const size_t n = fluid.count;
@@ -687,6 +699,7 @@ lsmps_status one_neighbor_list(lsmps_ctx* ctx, Scratch& scratch, const lsmps_flu
     return fail(ctx, LSMPS_INVALID_ARGUMENT, "self-excluding neighbour table needs one cell list");
   a.offsets = out.offsets;
   a.indices = out.indices;
+  a.spos = spos;
   a.capacity = out.neighbor_count;
   a.total = out.offsets + n;
   a.bits = bits;
@@ -744,13 +757,24 @@ lsmps_status build_neighbor_lists_impl(lsmps_ctx* ctx, Scratch& scratch, const l
   }
   if (!st)
     st = build_cell_list_impl(ctx, scratch, walls.x, walls.y, walls.z, walls.count, p.grid, wc, ctx->boxes, 2);
+  // The fluid table's cell-sorted rows go to the context's own array, where
+  // they stay for the next step's gathers.
+  ctx->spos_table = nullptr;
+  index_t* spos = nullptr;
+  if (ctx->sorted_rows && fluid.count > 0 && ensure_sorted_rows(ctx, fn.neighbor_count, fluid.count))
+    spos = ctx->fluid_spos;
   // the two tables run one after the other on the stream and share the masks
   if (!st)
     st = one_neighbor_list(ctx, scratch, fluid, fluid.x, fluid.y, fluid.z, fc, fc, p.grid, radius, true, fn,
-                           fluid.count, bits, src_pos);
+                           fluid.count, bits, src_pos, spos);
+  if (!st && spos) {
+    ctx->spos_table = fn.offsets;
+    ctx->spos_order = fc.sorted_indices;
+    ctx->spos_count = fluid.count;
+  }
   if (!st)
     st = one_neighbor_list(ctx, scratch, fluid, walls.x, walls.y, walls.z, fc, wc, p.grid, radius, false, wn,
-                           walls.count, bits, src_pos);
+                           walls.count, bits, src_pos, nullptr);
   return st;
 }
 

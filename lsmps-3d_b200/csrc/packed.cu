@@ -5,16 +5,20 @@ namespace lsmps {
 
 __global__ void pack4_kernel(const double* __restrict__ a, const double* __restrict__ b,
                              const double* __restrict__ c, const double* __restrict__ d, index_t n,
-                             double4* __restrict__ out) {
-  for (index_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    out[i] = make_double4(a[i], b[i], c[i], d ? d[i] : 0.0);
+                             double4* __restrict__ out, const index_t* __restrict__ order) {
+  for (index_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const index_t j = order ? order[i] : i;
+    out[i] = make_double4(a[j], b[j], c[j], d ? d[j] : 0.0);
+  }
 }
 
 __global__ void pack4_label_kernel(const double* __restrict__ a, const double* __restrict__ b,
                                    const double* __restrict__ c, const int32_t* __restrict__ label, index_t n,
-                                   double4* __restrict__ out) {
-  for (index_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    out[i] = make_double4(a[i], b[i], c[i], label ? static_cast<double>(label[i]) : 0.0);
+                                   double4* __restrict__ out, const index_t* __restrict__ order) {
+  for (index_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const index_t j = order ? order[i] : i;
+    out[i] = make_double4(a[j], b[j], c[j], label ? static_cast<double>(label[j]) : 0.0);
+  }
 }
 
 int stream_blocks(lsmps_ctx* ctx, size_t n) {
@@ -24,16 +28,17 @@ int stream_blocks(lsmps_ctx* ctx, size_t n) {
 }
 
 void pack4(lsmps_ctx* ctx, const double* a, const double* b, const double* c, const double* d, size_t n,
-           double4* out) {
+           double4* out, const index_t* order) {
   if (n == 0) return;
-  launch(ctx, pack4_kernel, dim3(stream_blocks(ctx, n)), dim3(256), 0, a, b, c, d, static_cast<index_t>(n), out);
+  launch(ctx, pack4_kernel, dim3(stream_blocks(ctx, n)), dim3(256), 0, a, b, c, d, static_cast<index_t>(n), out,
+         order);
 }
 
 void pack4_label(lsmps_ctx* ctx, const double* a, const double* b, const double* c, const int32_t* label, size_t n,
-                 double4* out) {
+                 double4* out, const index_t* order) {
   if (n == 0) return;
   launch(ctx, pack4_label_kernel, dim3(stream_blocks(ctx, n)), dim3(256), 0, a, b, c, label,
-         static_cast<index_t>(n), out);
+         static_cast<index_t>(n), out, order);
 }
 
 }  // namespace lsmps

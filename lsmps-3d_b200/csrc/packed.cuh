@@ -13,23 +13,25 @@
 
 namespace lsmps {
 
-// {a[i], b[i], c[i], d ? d[i] : 0}
+// out[k] = {a[j], b[j], c[j], d ? d[j] : 0} with j = order ? order[k] : k
+// (order: a cell list's sorted indices, for records in cell-sorted order)
 __global__ void pack4_kernel(const double* __restrict__ a, const double* __restrict__ b,
                              const double* __restrict__ c, const double* __restrict__ d, index_t n,
-                             double4* __restrict__ out);
+                             double4* __restrict__ out, const index_t* __restrict__ order);
 
-// {a[i], b[i], c[i], (double)label[i]} (label may be null -> 0)
+// out[k] = {a[j], b[j], c[j], (double)label[j]} (label may be null -> 0), j as above
 __global__ void pack4_label_kernel(const double* __restrict__ a, const double* __restrict__ b,
                                    const double* __restrict__ c, const int32_t* __restrict__ label, index_t n,
-                                   double4* __restrict__ out);
+                                   double4* __restrict__ out, const index_t* __restrict__ order);
 
 int stream_blocks(lsmps_ctx* ctx, size_t n);
 
-// Queue a pack of three (or four) SoA arrays into out[n].
+// Queue a pack of three (or four) SoA arrays into out[n], in index order or,
+// with `order`, in that order.
 void pack4(lsmps_ctx* ctx, const double* a, const double* b, const double* c, const double* d, size_t n,
-           double4* out);
+           double4* out, const index_t* order = nullptr);
 void pack4_label(lsmps_ctx* ctx, const double* a, const double* b, const double* c, const int32_t* label, size_t n,
-                 double4* out);
+                 double4* out, const index_t* order = nullptr);
 
 // One record through the read-only path as one 32-byte vector load (sm_100:
 // a single load instruction per record and lane, where two 16-byte loads

@@ -56,6 +56,13 @@ struct PpeArgs {
   const double4* wu;
   const double4* wn;
   const int32_t* order;  // visiting order of the lane kernel (lsmps_ctx::order) or NULL
+  // The lane kernels' neighbour rows for the records: fi, or the table's
+  // cell-sorted rows with fp / fu packed in that order (sorted = 1; a
+  // column written is then order[sorted position], the neighbour's index:
+  // the entries of nearby rows fall in a few lines of the cell list, where
+  // fi[o] would be one more line per row).
+  const index_t* fs;
+  int sorted;
   // Merged batch (lsmps_ctx::box_ppe): each row written into its box's own
   // matrix, columns in the box's numbering; NULL: into col / val.
   const PpeBoxOut* box_out;
@@ -221,7 +228,7 @@ __global__ void __launch_bounds__(kThreads) ppe_kernel(PpeArgs a) {
 // diagonal (minus the sum of the off-diagonal values) and the RHS sums stay
 // FP64.
 template <int G, bool Mixed>
-__device__ __forceinline__ void ppe_row(const PpeArgs& a, index_t i, int l, bool write_offsets) {
+__device__ __forceinline__ void ppe_row(const PpeArgs& a, index_t i, index_t self, int l, bool write_offsets) {
   const index_t n = static_cast<index_t>(a.fluid.count);
   const index_t nb = a.fo[i], ne = a.fo[i + 1];
   const index_t row = i + nb;
@@ -246,7 +253,7 @@ __device__ __forceinline__ void ppe_row(const PpeArgs& a, index_t i, int l, bool
     }
     return;
   }
-  const double4 pi = ld4(a.fp, i);
+  const double4 pi = ld4(a.fp, self);
   const double xi = pi.x, yi = pi.y, zi = pi.z;
   // The pressure Laplacian row, once per group in shared memory: read by
   // broadcast in every neighbour's dot product, it holds no registers.
@@ -290,17 +297,19 @@ __device__ __forceinline__ void ppe_row(const PpeArgs& a, index_t i, int l, bool
   // Each lane loads its next neighbour's records, and the index after that,
   // while it works on this one.
   index_t o = nb + l;
-  index_t jn = o < ne ? a.fi[o] : i;
-  index_t jnn = o + G < ne ? a.fi[o + G] : i;
+  index_t jn = o < ne ? a.fs[o] : i;
+  index_t jnn = o + G < ne ? a.fs[o + G] : i;
   double4 qn = ld4(a.fp, jn), un = ld4(a.fu, jn);
+  index_t cn = a.sorted ? a.order[jn] : jn;
   for (; o < ne; o += G) {
-    const index_t j = jn;
+    const index_t j = cn;  // the column
     const double4 q = qn, u = un;
     if (o + G < ne) {
       jn = jnn;
       qn = ld4(a.fp, jn);
       un = ld4(a.fu, jn);
-      if (o + 2 * G < ne) jnn = a.fi[o + 2 * G];
+      cn = a.sorted ? a.order[jn] : jn;
+      if (o + 2 * G < ne) jnn = a.fs[o + 2 * G];
     }
     const double dx = q.x - xi, dy = q.y - yi, dz = q.z - zi;
     const double w = lin_weight_mul(sqrt(dx * dx + dy * dy + dz * dz), a.inv_re);
@@ -349,7 +358,8 @@ __global__ void __launch_bounds__(kThreads, 4) ppe_lanes_kernel(PpeArgs a) {
   const int l = threadIdx.x & (G - 1);
   // Whole groups leave together, so the shuffles see full groups.
   if (t >= static_cast<index_t>(a.fluid.count)) return;
-  ppe_row<G, Mixed>(a, visit(a.order, t), l, true);
+  const index_t i = visit(a.order, t);
+  ppe_row<G, Mixed>(a, i, self_of(a.sorted, t, i), l, true);
 }
 
 // The mixed form with FP32 arithmetic; the particles whose rows took the
@@ -361,7 +371,7 @@ __global__ void __launch_bounds__(kThreads, 4) ppe_lanes_kernel(PpeArgs a) {
 // FP32 operator rows; the diagonal (minus the sum of the stored off-diagonal
 // values), the divergence sum and the wall Neumann sum accumulate in FP64.
 template <int G>
-__device__ __forceinline__ void ppe_row32(const PpeArgs& a, index_t i, int l) {
+__device__ __forceinline__ void ppe_row32(const PpeArgs& a, index_t i, index_t self, int l) {
   const index_t n = static_cast<index_t>(a.fluid.count);
   const index_t nb = a.fo[i], ne = a.fo[i + 1];
   const index_t row = i + nb;
@@ -387,7 +397,7 @@ __device__ __forceinline__ void ppe_row32(const PpeArgs& a, index_t i, int l) {
     }
     return;
   }
-  const double4 pi = ld4(a.fp, i);
+  const double4 pi = ld4(a.fp, self);
   // The group's four operator rows in shared memory (read by broadcast in
   // every neighbour's dot products; they hold no registers): the pressure
   // Laplacian row L, then the velocity gradient rows 0, 1, 2, each padded to
@@ -408,17 +418,19 @@ __device__ __forceinline__ void ppe_row32(const PpeArgs& a, index_t i, int l) {
   const float scale = static_cast<float>(2.0 / (a.re * a.re * a.density));
   double dsum = 0.0, diag = 0.0;
   index_t o = nb + l;
-  index_t jn = o < ne ? a.fi[o] : i;
-  index_t jnn = o + G < ne ? a.fi[o + G] : i;
+  index_t jn = o < ne ? a.fs[o] : i;
+  index_t jnn = o + G < ne ? a.fs[o + G] : i;
   double4 qn = ld4(a.fp, jn), un = ld4(a.fu, jn);
+  index_t cn = a.sorted ? a.order[jn] : jn;
   for (; o < ne; o += G) {
-    const index_t j = jn;
+    const index_t j = cn;  // the column
     const double4 q = qn, u = un;
     if (o + G < ne) {
       jn = jnn;
       qn = ld4(a.fp, jn);
       un = ld4(a.fu, jn);
-      if (o + 2 * G < ne) jnn = a.fi[o + 2 * G];
+      cn = a.sorted ? a.order[jn] : jn;
+      if (o + 2 * G < ne) jnn = a.fs[o + 2 * G];
     }
     const float w = basis_f32(q.x - pi.x, q.y - pi.y, q.z - pi.z, a.inv_re, b);
     float off = 0.0f;
@@ -471,7 +483,8 @@ __global__ void __launch_bounds__(kThreads, 7) ppe32_kernel(PpeArgs a) {
   const index_t t = (blockIdx.x * blockDim.x + threadIdx.x) / G;
   const int l = threadIdx.x & (G - 1);
   if (t >= static_cast<index_t>(a.fluid.count)) return;
-  ppe_row32<G>(a, visit(a.order, t), l);
+  const index_t i = visit(a.order, t);
+  ppe_row32<G>(a, i, self_of(a.sorted, t, i), l);
 }
 
 // The rows of the FP64-route particles (FP64 arithmetic, ppe_row<G, true>):
@@ -485,19 +498,23 @@ __global__ void __launch_bounds__(kThreads, 4) ppe_list_kernel(PpeArgs a) {
   const int l = threadIdx.x & (G - 1);
   const index_t nv = static_cast<index_t>(*a.vrows.count), np = static_cast<index_t>(*a.prows.count);
   for (index_t t = g0; t < nv + np; t += groups) {
-    const index_t i = t < nv ? a.vrows.list[t] : a.prows.list[t - nv];
+    const index_t vt = t < nv ? a.vrows.list[t] : a.prows.list[t - nv];  // a visiting position
+    const index_t i = visit(a.order, vt);
     if (t >= nv && a.vrows.flag[i]) continue;
-    ppe_row<G, true>(a, i, l, false);
+    ppe_row<G, true>(a, i, self_of(a.sorted, vt, i), l, false);
   }
 }
 
 // Neighbour records of the lane kernels: positions and u* of the fluid,
 // positions, u* and normals of the walls.
 bool pack_ppe(lsmps_ctx* ctx, const lsmps_fluid& f, const lsmps_walls& w, const lsmps_fluid& tv,
-              const lsmps_walls& tw, PpeArgs& a) {
+              const lsmps_walls& tw, const lsmps_csr& fn, PpeArgs& a) {
   if (!ensure_packs(ctx, f.count, w.count)) return false;
-  pack4(ctx, f.x, f.y, f.z, nullptr, f.count, ctx->pack_fluid[0]);
-  pack4(ctx, tv.vx, tv.vy, tv.vz, nullptr, f.count, ctx->pack_fluid[1]);
+  const index_t* srows = sorted_rows_of(ctx, fn, f.count);
+  a.fs = srows ? srows : a.fi;
+  a.sorted = srows ? 1 : 0;
+  pack4(ctx, f.x, f.y, f.z, nullptr, f.count, ctx->pack_fluid[0], srows ? ctx->order : nullptr);
+  pack4(ctx, tv.vx, tv.vy, tv.vz, nullptr, f.count, ctx->pack_fluid[1], srows ? ctx->order : nullptr);
   pack4(ctx, w.x, w.y, w.z, nullptr, w.count, ctx->pack_wall[0]);
   pack4(ctx, tw.vx, tw.vy, tw.vz, nullptr, w.count, ctx->pack_wall[1]);
   pack4(ctx, w.normal_x, w.normal_y, w.normal_z, nullptr, w.count, ctx->pack_wall[2]);
@@ -566,7 +583,8 @@ lsmps_status assemble_ppe_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const lsmps
   a.rhs = ws.rhs;
   a.divergence = ws.divergence;
   a.wall_rhs_out = ws.pressure_laplacian;
-  if (ctx->knob[LSMPS_KNOB_PPE_LANES] != 0 && !pack_ppe(ctx, f, w, tv, tw, a))
+  a.fs = a.fi;
+  if (ctx->knob[LSMPS_KNOB_PPE_LANES] != 0 && !pack_ppe(ctx, f, w, tv, tw, fn, a))
     return fail(ctx, LSMPS_CUDA_ERROR, "pack allocation failed");
   const long long rows = static_cast<long long>(f.count);
   switch (ctx->knob[LSMPS_KNOB_PPE_LANES]) {
@@ -629,7 +647,7 @@ lsmps_status assemble_ppe_mixed_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const
   a.rhs = ws.rhs;
   a.divergence = ws.divergence;
   a.wall_rhs_out = ws.pressure_laplacian;
-  if (!pack_ppe(ctx, f, w, tv, tw, a)) return fail(ctx, LSMPS_CUDA_ERROR, "pack allocation failed");
+  if (!pack_ppe(ctx, f, w, tv, tw, fn, a)) return fail(ctx, LSMPS_CUDA_ERROR, "pack allocation failed");
   const long long rows = static_cast<long long>(f.count);
   const dim3 list_grid(static_cast<unsigned>(ctx->sm_count * 2));
   switch (ctx->knob[LSMPS_KNOB_PPE_LANES]) {

@@ -37,6 +37,7 @@ struct LaplacianArgs {
   double* ly;
   double* lz;
   const int32_t* order;  // visiting order (lsmps_ctx::order) or NULL
+  int sorted;            // fi and the fluid packs in cell-sorted positions (sorted_rows_of)
 };
 
 // Mixed (the mixed form): the row comes from the mixed-form operator rows
@@ -47,9 +48,10 @@ struct LaplacianArgs {
 // entries l, l + G, ... of both rows and the groups' partial sums are added
 // with shuffles (a rounding-level reassociation for G > 1).
 template <bool Mixed, int G>
-__device__ __forceinline__ void laplacian_of(const LaplacianArgs& a, const MixedRows& rows, index_t i, int l) {
-  const double4 pi = ld4(a.fp, i);
-  const double4 ui = ld4(a.fv, i);
+__device__ __forceinline__ void laplacian_of(const LaplacianArgs& a, const MixedRows& rows, index_t i, index_t self,
+                                             int l) {
+  const double4 pi = ld4(a.fp, self);
+  const double4 ui = ld4(a.fv, self);
   // The particle's Laplacian row L (the sum of the inverse's rows 3..5, or
   // the mixed-form row) is applied to every neighbour's basis vector:
   // sum_j w_j (L . b_j) (u_j - u_i) equals L . sum_j w_j b_j (u_j - u_i) up
@@ -126,7 +128,8 @@ __global__ void __launch_bounds__(kThreads, 5) laplacian_kernel(LaplacianArgs a,
   const index_t t = (blockIdx.x * blockDim.x + threadIdx.x) / G;
   const int l = threadIdx.x & (G - 1);
   if (t >= a.n) return;  // the whole group
-  laplacian_of<Mixed, G>(a, rows, visit(a.order, t), l);
+  const index_t i = visit(a.order, t);
+  laplacian_of<Mixed, G>(a, rows, i, self_of(a.sorted, t, i), l);
 }
 
 // Mixed form with FP32 arithmetic: each neighbour's offset is formed in FP64
@@ -141,8 +144,9 @@ __global__ void __launch_bounds__(kThreads, 7) laplacian32_kernel(LaplacianArgs 
   if (t >= a.n) return;  // the whole group
   const index_t i = visit(a.order, t);
   if (rows.flag[i]) return;
-  const double4 pi = ld4(a.fp, i);
-  const double4 ui = ld4(a.fv, i);
+  const index_t self = self_of(a.sorted, t, i);
+  const double4 pi = ld4(a.fp, self);
+  const double4 ui = ld4(a.fv, self);
   // the Laplacian row in registers (9 floats)
   float L[9];
   load_row9f(rows, i, 0, L);
@@ -201,8 +205,11 @@ __global__ void __launch_bounds__(kThreads, 5) laplacian_list_kernel(LaplacianAr
   const index_t groups = static_cast<index_t>(gridDim.x * blockDim.x / G);
   const int l = threadIdx.x & (G - 1);
   const index_t count = static_cast<index_t>(*rows.count);
-  for (index_t t = static_cast<index_t>((blockIdx.x * blockDim.x + threadIdx.x) / G); t < count; t += groups)
-    laplacian_of<true, G>(a, rows, rows.list[t], l);
+  for (index_t t = static_cast<index_t>((blockIdx.x * blockDim.x + threadIdx.x) / G); t < count; t += groups) {
+    const index_t vt = rows.list[t];  // a visiting position
+    const index_t i = visit(a.order, vt);
+    laplacian_of<true, G>(a, rows, i, self_of(a.sorted, vt, i), l);
+  }
 }
 
 // combine_explicit_velocity_kernel, explicit_update.cu:250-270
@@ -271,13 +278,15 @@ lsmps_status velocity_laplacian_mixed_impl(lsmps_ctx* ctx, const lsmps_fluid& f,
   if (!ctx->mixed_rows[0] || !ctx->mixed_count || ctx->mixed_cap < f.count)
     return fail(ctx, LSMPS_NOT_PREPARED, "mixed velocity operator rows were not prepared");
   if (!ensure_packs(ctx, f.count, w.count)) return fail(ctx, LSMPS_CUDA_ERROR, "pack allocation failed");
-  pack4(ctx, f.vx, f.vy, f.vz, nullptr, f.count, ctx->pack_fluid[1]);
+  const index_t* srows = sorted_rows_of(ctx, fn, f.count);
+  pack4(ctx, f.vx, f.vy, f.vz, nullptr, f.count, ctx->pack_fluid[1], srows ? ctx->order : nullptr);
   pack4(ctx, w.vx, w.vy, w.vz, nullptr, w.count, ctx->pack_wall[1]);
-  // fluid and wall positions are still packed from the moment stage
+  // fluid and wall positions are still packed from the moment stage (in the
+  // same order: the rows' form is the same within a step)
   LaplacianArgs a{static_cast<index_t>(f.count), ctx->pack_fluid[0], ctx->pack_fluid[1], ctx->pack_wall[0],
-                  ctx->pack_wall[1], fn.offsets, fn.indices, wn.offsets, wn.indices, nullptr,
+                  ctx->pack_wall[1], fn.offsets, srows ? srows : fn.indices, wn.offsets, wn.indices, nullptr,
                   vm.support_radius, 1.0 / vm.support_radius, vm.wall_weight_scale, lap.x, lap.y, lap.z,
-                  ctx->order};
+                  ctx->order, srows ? 1 : 0};
   const MixedRows rows = mixed_rows_of(ctx, 0);
   const long long n = a.n;
   const dim3 list_grid(static_cast<unsigned>(ctx->sm_count * 2));
@@ -313,14 +322,16 @@ lsmps_status velocity_laplacian_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const
     return fail(ctx, LSMPS_INVALID_ARGUMENT, "Provision buffers missing");
   if (w.count > 0 && (!w.vx || !w.vy || !w.vz)) return fail(ctx, LSMPS_INVALID_ARGUMENT, "wall velocity missing");
   if (!ensure_packs(ctx, f.count, w.count)) return fail(ctx, LSMPS_CUDA_ERROR, "pack allocation failed");
-  pack4(ctx, f.x, f.y, f.z, nullptr, f.count, ctx->pack_fluid[0]);
-  pack4(ctx, f.vx, f.vy, f.vz, nullptr, f.count, ctx->pack_fluid[1]);
+  const index_t* srows = sorted_rows_of(ctx, fn, f.count);
+  const index_t* pord = srows ? ctx->order : nullptr;
+  pack4(ctx, f.x, f.y, f.z, nullptr, f.count, ctx->pack_fluid[0], pord);
+  pack4(ctx, f.vx, f.vy, f.vz, nullptr, f.count, ctx->pack_fluid[1], pord);
   pack4(ctx, w.x, w.y, w.z, nullptr, w.count, ctx->pack_wall[0]);
   pack4(ctx, w.vx, w.vy, w.vz, nullptr, w.count, ctx->pack_wall[1]);
   LaplacianArgs a{static_cast<index_t>(f.count), ctx->pack_fluid[0], ctx->pack_fluid[1], ctx->pack_wall[0],
-                  ctx->pack_wall[1], fn.offsets, fn.indices, wn.offsets, wn.indices, vm.inverse_matrices,
-                  vm.support_radius, 1.0 / vm.support_radius, vm.wall_weight_scale, lap.x, lap.y, lap.z,
-                  ctx->order};
+                  ctx->pack_wall[1], fn.offsets, srows ? srows : fn.indices, wn.offsets, wn.indices,
+                  vm.inverse_matrices, vm.support_radius, 1.0 / vm.support_radius, vm.wall_weight_scale, lap.x,
+                  lap.y, lap.z, ctx->order, srows ? 1 : 0};
   launch_laplacian<false>(ctx, a, MixedRows{});
   return check_launch(ctx, "velocity laplacian");
 }

@@ -73,6 +73,10 @@ struct SurfaceArgs {
   const double4* wp;
   const double4* wn;
   const int32_t* order;  // visiting order (lsmps_ctx::order) or NULL
+  // fi and fp in cell-sorted positions (sorted_rows_of): the labels are also
+  // written by visiting position into sorted_labels, for the expansion
+  int sorted;
+  int32_t* sorted_labels;
 };
 
 __global__ void __launch_bounds__(kSurfaceThreads) classify_kernel(SurfaceArgs a) {
@@ -84,7 +88,7 @@ __global__ void __launch_bounds__(kSurfaceThreads) classify_kernel(SurfaceArgs a
   const index_t fcount = fe - fb, wcount = we - wb;
   const index_t cls = a.p.include_wall_neighbors ? fcount + wcount : fcount;
   const double re = a.p.support_radius;
-  const double4 own = ld4(a.fp, i);
+  const double4 own = ld4(a.fp, self_of(a.sorted, t, i));
   const double px = own.x, py = own.y, pz = own.z;
   double nd = 0.0, sx = 0.0, sy = 0.0, sz = 0.0;
   int weighted = 0;
@@ -152,6 +156,7 @@ __global__ void __launch_bounds__(kSurfaceThreads) classify_kernel(SurfaceArgs a
     type = LSMPS_SURFACE_SURFACE;
   }
   a.fluid.surface_type[i] = type;
+  if (a.sorted) a.sorted_labels[t] = type;
   const lsmps_surface_diagnostics& d = a.diag;
   if (d.fluid_neighbor_count) d.fluid_neighbor_count[i] = fcount;
   if (d.wall_neighbor_count) d.wall_neighbor_count[i] = wcount;
@@ -182,16 +187,22 @@ __global__ void __launch_bounds__(kSurfaceThreads) classify_kernel(SurfaceArgs a
 // found a Surface neighbour within r_ns, which does not depend on the order.
 constexpr int kExpandLanes = 4;
 
+// With cell-sorted rows (sorted_labels non-NULL), fi and fp are in sorted
+// positions and the neighbours' labels are read from sorted_labels.
 __global__ void __launch_bounds__(kSurfaceThreads) expand_kernel(const double4* __restrict__ fp, int32_t* type,
                                                                  index_t n, const index_t* __restrict__ fo,
                                                                  const index_t* __restrict__ fi, double r2,
-                                                                 const int32_t* __restrict__ order) {
+                                                                 const int32_t* __restrict__ order,
+                                                                 const int32_t* __restrict__ sorted_labels) {
   const index_t t = (blockIdx.x * blockDim.x + threadIdx.x) / kExpandLanes;
   const int l = threadIdx.x & (kExpandLanes - 1);
   if (t >= n) return;  // the whole group
   const index_t i = visit(order, t);
-  if (type[i] != LSMPS_SURFACE_INNER) return;
-  const double4 own = ld4(fp, i);
+  // (the particle's own label from classify: sorted_labels[t] equals type[i]
+  // until this thread writes it)
+  if ((sorted_labels ? sorted_labels[t] : type[i]) != LSMPS_SURFACE_INNER) return;
+  const int32_t* __restrict__ nlab = sorted_labels ? sorted_labels : type;
+  const double4 own = ld4(fp, sorted_labels ? t : i);
   bool near = false;
   const index_t fe = fo[i + 1];
   // kExpandBatch entries per lane and round: their indices, then their
@@ -207,7 +218,7 @@ __global__ void __launch_bounds__(kSurfaceThreads) expand_kernel(const double4* 
       j[k] = e < fe ? fi[e] : -1;
     }
 #pragma unroll
-    for (int k = 0; k < kExpandBatch; ++k) lab[k] = j[k] >= 0 ? type[j[k]] : LSMPS_SURFACE_INNER;
+    for (int k = 0; k < kExpandBatch; ++k) lab[k] = j[k] >= 0 ? nlab[j[k]] : LSMPS_SURFACE_INNER;
 #pragma unroll
     for (int k = 0; k < kExpandBatch; ++k) {
       if (lab[k] != LSMPS_SURFACE_SURFACE) continue;
@@ -368,18 +379,21 @@ lsmps_status classify_surface_impl(lsmps_ctx* ctx, const lsmps_fluid& fluid, con
   if (fluid.count == 0) return LSMPS_OK;
   if (const lsmps_status cs = check_neighbor_tables(ctx, fluid.count, walls.count, fn, &wn)) return cs;
   if (!fluid.surface_type) return fail(ctx, LSMPS_INVALID_ARGUMENT, "surface_type buffer missing");
+  const index_t* srows = sorted_rows_of(ctx, fn, fluid.count);
   SurfaceArgs a{};
   a.fluid = fluid;
   a.walls = walls;
   a.fo = fn.offsets;
-  a.fi = fn.indices;
+  a.fi = srows ? srows : fn.indices;
+  a.sorted = srows ? 1 : 0;
+  a.sorted_labels = srows ? ctx->sorted_labels : nullptr;
   a.wo = wn.offsets;
   a.wi = wn.indices;
   a.p = p;
   a.n0 = n0;
   if (diag) a.diag = *diag;
   if (!ensure_packs(ctx, fluid.count, walls.count)) return fail(ctx, LSMPS_CUDA_ERROR, "pack allocation failed");
-  pack4(ctx, fluid.x, fluid.y, fluid.z, nullptr, fluid.count, ctx->pack_fluid[0]);
+  pack4(ctx, fluid.x, fluid.y, fluid.z, nullptr, fluid.count, ctx->pack_fluid[0], srows ? ctx->order : nullptr);
   pack4(ctx, walls.x, walls.y, walls.z, nullptr, walls.count, ctx->pack_wall[0]);
   pack4(ctx, walls.normal_x, walls.normal_y, walls.normal_z, nullptr, walls.count, ctx->pack_wall[2]);
   a.fp = ctx->pack_fluid[0];
@@ -392,8 +406,8 @@ lsmps_status classify_surface_impl(lsmps_ctx* ctx, const lsmps_fluid& fluid, con
     launch(ctx, expand_kernel, dim3(div_up(static_cast<long long>(n) * kExpandLanes, kSurfaceThreads)),
            dim3(kSurfaceThreads), 0,
            static_cast<const double4*>(ctx->pack_fluid[0]), fluid.surface_type, n,
-           static_cast<const index_t*>(fn.offsets), static_cast<const index_t*>(fn.indices),
-           p.near_surface_radius * p.near_surface_radius, static_cast<const int32_t*>(ctx->order));
+           static_cast<const index_t*>(fn.offsets), a.fi, p.near_surface_radius * p.near_surface_radius,
+           static_cast<const int32_t*>(ctx->order), static_cast<const int32_t*>(a.sorted_labels));
   }
   return check_launch(ctx, "surface classification");
 }

@@ -145,3 +145,20 @@ extern "C" lsmps_status lsmps_ctx_set_cell_order(lsmps_ctx* ctx, int on) {
   ctx->cell_order = on != 0;
   return LSMPS_OK;
 }
+
+extern "C" lsmps_status lsmps_ctx_copy_sorted_rows(lsmps_ctx* ctx, int32_t* dst, size_t count) {
+  if (!ctx || (count > 0 && !dst)) return LSMPS_INVALID_ARGUMENT;
+  if (!ctx->spos_table || count > ctx->fluid_spos_cap)
+    return lsmps::fail(ctx, LSMPS_NOT_PREPARED, "no cell-sorted rows of that length are held");
+  if (count && cudaMemcpyAsync(dst, ctx->fluid_spos, count * sizeof(int32_t), cudaMemcpyDeviceToDevice,
+                               ctx->stream) != cudaSuccess)
+    return lsmps::check_launch(ctx, "sorted rows copy");
+  return ctx->synchronous ? lsmps_ctx_synchronize(ctx) : LSMPS_OK;
+}
+
+extern "C" lsmps_status lsmps_ctx_set_sorted_rows(lsmps_ctx* ctx, int on) {
+  if (!ctx) return LSMPS_INVALID_ARGUMENT;
+  ctx->sorted_rows = on != 0;
+  if (!ctx->sorted_rows) ctx->spos_table = nullptr;
+  return LSMPS_OK;
+}
