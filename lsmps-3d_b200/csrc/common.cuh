@@ -240,6 +240,15 @@ struct lsmps_ctx {
   const int32_t* spos_order = nullptr;
   size_t spos_count = 0;
   bool sorted_rows = true;
+  // Inside lsmps_step (step_packs): which record packs already hold what a
+  // later stage of the same step would pack again (bit 0: wall positions in
+  // pack_wall[0], bit 1: wall normals in pack_wall[2], bit 2: fluid positions
+  // in pack_fluid[0], packed in packs_fluid_order).  The walls do not move
+  // during a step and the fluid does not move before the correction; any
+  // other pack into those buffers clears its bit (packed.cu).
+  bool step_packs = false;
+  unsigned packs_ready = 0;
+  const int32_t* packs_fluid_order = nullptr;
   // CSR count pass shape: false = warp per home cell, lane per home particle
   // (the fastest on a GPU the build has to itself); true = block per home
   // cell, warp per two home particles, which leaves the streams of a batched

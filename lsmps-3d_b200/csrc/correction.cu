@@ -950,8 +950,8 @@ lsmps_status gradient_shifting_stage(lsmps_ctx* ctx, const lsmps_fluid& f, const
   a.sorted = srows ? 1 : 0;
   if (!ensure_packs(ctx, f.count, w.count)) return fail(ctx, LSMPS_CUDA_ERROR, "pack allocation failed");
   pack4(ctx, f.x, f.y, f.z, pressure, f.count, ctx->pack_fluid[0], srows ? ctx->order : nullptr);
-  pack4(ctx, w.x, w.y, w.z, nullptr, w.count, ctx->pack_wall[0]);
-  pack4(ctx, w.normal_x, w.normal_y, w.normal_z, nullptr, w.count, ctx->pack_wall[2]);
+  pack_wall_positions(ctx, w);
+  pack_wall_normals(ctx, w);
   a.fpp = ctx->pack_fluid[0];
   a.wp = ctx->pack_wall[0];
   a.wn = ctx->pack_wall[2];

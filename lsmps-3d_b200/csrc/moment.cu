@@ -1225,8 +1225,8 @@ lsmps_status launch_mixed(lsmps_ctx* ctx, index_t n, const lsmps_csr& fn, const 
   auto pack_walls = [&]() {
     if (ctx->walls_wait_event)
       cudaStreamWaitEvent(ctx->stream, static_cast<cudaEvent_t>(ctx->walls_wait_event), 0);
-    pack4(ctx, walls.x, walls.y, walls.z, nullptr, walls.count, ctx->pack_wall[0]);
-    pack4(ctx, walls.normal_x, walls.normal_y, walls.normal_z, nullptr, walls.count, ctx->pack_wall[2]);
+    pack_wall_positions(ctx, walls);
+    pack_wall_normals(ctx, walls);
   };
   if (split) {
     pack_walls();
@@ -1266,8 +1266,7 @@ lsmps_status mixed_step_moments_impl(lsmps_ctx* ctx, const lsmps_fluid& fluid, c
       !pm.info)
     return fail(ctx, LSMPS_INVALID_ARGUMENT, "Invalid Moment matrix cache buffers");
   if (!ensure_packs(ctx, fluid.count, walls.count)) return fail(ctx, LSMPS_CUDA_ERROR, "pack allocation failed");
-  pack4(ctx, fluid.x, fluid.y, fluid.z, nullptr, fluid.count, ctx->pack_fluid[0],
-        sorted_rows_of(ctx, fn, fluid.count) ? ctx->order : nullptr);
+  pack_fluid_positions(ctx, fluid, sorted_rows_of(ctx, fn, fluid.count) ? ctx->order : nullptr);
   const KindOut kv{1, vm.inverse_matrices, vm.moment_trace, vm.regularization_added, vm.info, vm.inversion_count};
   const KindOut kp{2, pm.inverse_matrices, pm.moment_trace, pm.regularization_added, pm.info, pm.inversion_count};
   lsmps_status st = launch_mixed(ctx, n, fn, wn, p, kv, kp, false, walls);
@@ -1322,12 +1321,12 @@ lsmps_status prepare_moments_impl(lsmps_ctx* ctx, const lsmps_fluid& fluid, cons
   constexpr size_t kStageBytes = sizeof(double) * 27 * kMomentThreads;
   if (!ensure_packs(ctx, fluid.count, walls.count)) return fail(ctx, LSMPS_CUDA_ERROR, "pack allocation failed");
   const index_t* srows = sorted_rows_of(ctx, fn, fluid.count);
-  pack4(ctx, fluid.x, fluid.y, fluid.z, nullptr, fluid.count, ctx->pack_fluid[0], srows ? ctx->order : nullptr);
+  pack_fluid_positions(ctx, fluid, srows ? ctx->order : nullptr);
   // (the mixed form packs the walls itself, after its fluid sums)
   const bool fused = velocity_a >= 0 && pressure_a >= 0;
   if (!(fused && ctx->precision == LSMPS_PRECISION_MIXED)) {
-    pack4(ctx, walls.x, walls.y, walls.z, nullptr, walls.count, ctx->pack_wall[0]);
-    pack4(ctx, walls.normal_x, walls.normal_y, walls.normal_z, nullptr, walls.count, ctx->pack_wall[2]);
+    pack_wall_positions(ctx, walls);
+    pack_wall_normals(ctx, walls);
   }
   MomentPackedArgs pa{n, ctx->pack_fluid[0], ctx->pack_wall[0], ctx->pack_wall[2], fn.offsets,
                       srows ? srows : fn.indices, wn.offsets, wn.indices, base.inv_re, base.lambda,

@@ -33,6 +33,14 @@ void pack4(lsmps_ctx* ctx, const double* a, const double* b, const double* c, co
 void pack4_label(lsmps_ctx* ctx, const double* a, const double* b, const double* c, const int32_t* label, size_t n,
                  double4* out, const index_t* order = nullptr);
 
+// The wall positions {x, y, z, 0} into pack_wall[0], the wall normals into
+// pack_wall[2], the fluid positions into pack_fluid[0] (in `order`, as
+// pack4).  Inside lsmps_step a repeated request finds the pack made earlier
+// in the step (lsmps_ctx::packs_ready) and queues nothing.
+void pack_wall_positions(lsmps_ctx* ctx, const lsmps_walls& w);
+void pack_wall_normals(lsmps_ctx* ctx, const lsmps_walls& w);
+void pack_fluid_positions(lsmps_ctx* ctx, const lsmps_fluid& f, const index_t* order);
+
 // One record through the read-only path as one 32-byte vector load (sm_100:
 // a single load instruction per record and lane, where two 16-byte loads
 // cost two passes of the L1 data pipe for the same sector).  The records

@@ -513,11 +513,11 @@ bool pack_ppe(lsmps_ctx* ctx, const lsmps_fluid& f, const lsmps_walls& w, const 
   const index_t* srows = sorted_rows_of(ctx, fn, f.count);
   a.fs = srows ? srows : a.fi;
   a.sorted = srows ? 1 : 0;
-  pack4(ctx, f.x, f.y, f.z, nullptr, f.count, ctx->pack_fluid[0], srows ? ctx->order : nullptr);
+  pack_fluid_positions(ctx, f, srows ? ctx->order : nullptr);
   pack4(ctx, tv.vx, tv.vy, tv.vz, nullptr, f.count, ctx->pack_fluid[1], srows ? ctx->order : nullptr);
-  pack4(ctx, w.x, w.y, w.z, nullptr, w.count, ctx->pack_wall[0]);
+  pack_wall_positions(ctx, w);
   pack4(ctx, tw.vx, tw.vy, tw.vz, nullptr, w.count, ctx->pack_wall[1]);
-  pack4(ctx, w.normal_x, w.normal_y, w.normal_z, nullptr, w.count, ctx->pack_wall[2]);
+  pack_wall_normals(ctx, w);
   a.fp = ctx->pack_fluid[0];
   a.fu = ctx->pack_fluid[1];
   a.wp = ctx->pack_wall[0];

@@ -324,9 +324,9 @@ lsmps_status velocity_laplacian_impl(lsmps_ctx* ctx, const lsmps_fluid& f, const
   if (!ensure_packs(ctx, f.count, w.count)) return fail(ctx, LSMPS_CUDA_ERROR, "pack allocation failed");
   const index_t* srows = sorted_rows_of(ctx, fn, f.count);
   const index_t* pord = srows ? ctx->order : nullptr;
-  pack4(ctx, f.x, f.y, f.z, nullptr, f.count, ctx->pack_fluid[0], pord);
+  pack_fluid_positions(ctx, f, pord);
   pack4(ctx, f.vx, f.vy, f.vz, nullptr, f.count, ctx->pack_fluid[1], pord);
-  pack4(ctx, w.x, w.y, w.z, nullptr, w.count, ctx->pack_wall[0]);
+  pack_wall_positions(ctx, w);
   pack4(ctx, w.vx, w.vy, w.vz, nullptr, w.count, ctx->pack_wall[1]);
   LaplacianArgs a{static_cast<index_t>(f.count), ctx->pack_fluid[0], ctx->pack_fluid[1], ctx->pack_wall[0],
                   ctx->pack_wall[1], fn.offsets, srows ? srows : fn.indices, wn.offsets, wn.indices,

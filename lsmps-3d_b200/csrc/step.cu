@@ -37,6 +37,10 @@ extern "C" lsmps_status lsmps_step(lsmps_ctx* ctx, const lsmps_params* params, c
   // geometry changes every step, so every step builds them once.  Each stage
   // is an NVTX range.
   const bool mixed = ctx->precision == LSMPS_PRECISION_MIXED;
+  // Record packs made by one stage are reused by the next where their
+  // contents are the same (packed.cuh).
+  ctx->step_packs = true;
+  ctx->packs_ready = 0;
   // The caller's copy/compute overlap events (lsmps_ctx_set_step_events),
   // outside stream capture only.
   cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
@@ -100,5 +104,7 @@ extern "C" lsmps_status lsmps_step(lsmps_ctx* ctx, const lsmps_params* params, c
       st = classify_surface_impl(ctx, s->fluid, s->walls, s->fluid_neighbors, s->wall_neighbors, *params, nullptr);
   }
   ctx->order = nullptr;
+  ctx->step_packs = false;
+  ctx->packs_ready = 0;
   return end_call(ctx, st);
 }

@@ -394,8 +394,8 @@ lsmps_status classify_surface_impl(lsmps_ctx* ctx, const lsmps_fluid& fluid, con
   if (diag) a.diag = *diag;
   if (!ensure_packs(ctx, fluid.count, walls.count)) return fail(ctx, LSMPS_CUDA_ERROR, "pack allocation failed");
   pack4(ctx, fluid.x, fluid.y, fluid.z, nullptr, fluid.count, ctx->pack_fluid[0], srows ? ctx->order : nullptr);
-  pack4(ctx, walls.x, walls.y, walls.z, nullptr, walls.count, ctx->pack_wall[0]);
-  pack4(ctx, walls.normal_x, walls.normal_y, walls.normal_z, nullptr, walls.count, ctx->pack_wall[2]);
+  pack_wall_positions(ctx, walls);
+  pack_wall_normals(ctx, walls);
   a.fp = ctx->pack_fluid[0];
   a.wp = ctx->pack_wall[0];
   a.wn = ctx->pack_wall[2];
