@@ -261,7 +261,8 @@ struct lsmps_ctx {
   size_t pack_wall_cap = 0;
   // Mixed form (LSMPS_PRECISION_MIXED): per fluid particle the 31 FP64 fluid
   // moment sums ([31][n]) and the compact FP32 operator rows of the velocity
-  // and pressure inverses ([n][36]: Laplacian row, then rows 0, 1, 2).
+  // and pressure inverses ([n][36]: Laplacian row, then rows 0, 1, 2), both
+  // by visiting position (lsmps_ctx::order), as are the FP64 rows and flags.
   double* mixed_sums = nullptr;
   float* mixed_rows[2] = {nullptr, nullptr};
   double* mixed_rows64[2] = {nullptr, nullptr};  // rows of matrices factorised in FP64

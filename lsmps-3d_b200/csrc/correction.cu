@@ -489,7 +489,8 @@ struct GradShiftOut {
 // shuffles and lane 0 finishes the particle.
 template <bool Mixed, int G>
 __device__ __forceinline__ void gradient_shifting_of(const GatherArgs& a, const GradShiftOut& out, index_t i,
-                                                     index_t self, int l) {
+                                                     index_t vt, int l) {
+  const index_t self = self_of(a.sorted, vt, i);
   double* pressure = out.pressure;
   double* fluid_pressure = out.fluid_pressure;
   const double* __restrict__ pinv = out.pinv;
@@ -596,13 +597,13 @@ __device__ __forceinline__ void gradient_shifting_of(const GatherArgs& a, const 
   }
   if (do_grad && Mixed) {
     double g[9], c0 = 0.0, c1 = 0.0, c2 = 0.0;
-    load_row9(prows, i, 1, g);
+    load_row9(prows, vt, 1, g);
 #pragma unroll
     for (int col = 0; col < 9; ++col) c0 = fma(g[col], rhs[col], c0);
-    load_row9(prows, i, 2, g);
+    load_row9(prows, vt, 2, g);
 #pragma unroll
     for (int col = 0; col < 9; ++col) c1 = fma(g[col], rhs[col], c1);
-    load_row9(prows, i, 3, g);
+    load_row9(prows, vt, 3, g);
 #pragma unroll
     for (int col = 0; col < 9; ++col) c2 = fma(g[col], rhs[col], c2);
     gx[i] = c0 * inv_re;
@@ -659,7 +660,7 @@ __global__ void __launch_bounds__(kThreads, 6) gradient_shifting_kernel(GatherAr
   const int l = static_cast<int>(tt % G);
   if (t >= static_cast<index_t>(a.fluid.count)) return;  // the whole group
   const index_t i = visit(a.order, t);
-  gradient_shifting_of<Mixed, G>(a, out, i, self_of(a.sorted, t, i), l);
+  gradient_shifting_of<Mixed, G>(a, out, i, t, l);
 }
 
 // The FP64-route particles of the pressure kind (gradient_shifting_of<true,
@@ -672,7 +673,7 @@ __global__ void __launch_bounds__(kThreads, 6) gradient_shifting_list_kernel(Gat
   for (index_t t = static_cast<index_t>((blockIdx.x * blockDim.x + threadIdx.x) / G); t < count; t += groups) {
     const index_t vt = out.prows.list[t];  // a visiting position
     const index_t i = visit(a.order, vt);
-    gradient_shifting_of<true, G>(a, out, i, self_of(a.sorted, vt, i), l);
+    gradient_shifting_of<true, G>(a, out, i, vt, l);
   }
 }
 
@@ -692,7 +693,7 @@ __global__ void __launch_bounds__(kThreads, 6) gradient32_kernel(GatherArgs a, G
   const int l = static_cast<int>(tt % G);
   if (t >= static_cast<index_t>(a.fluid.count)) return;  // the whole group
   const index_t i = visit(a.order, t);
-  if (out.prows.flag[i]) return;
+  if (out.prows.flag[t]) return;
   const double praw = out.pressure[i];
   const double pi = praw < 0.0 ? 0.0 : praw;
   if (l == 0) {
@@ -796,7 +797,7 @@ __global__ void __launch_bounds__(kThreads, 6) gradient32_kernel(GatherArgs a, G
   }
   {
     float g[27];
-    load_rows123f(out.prows, i, g);
+    load_rows123f(out.prows, t, g);
     double c0 = 0.0, c1 = 0.0, c2 = 0.0;
 #pragma unroll
     for (int col = 0; col < 9; ++col) {

@@ -14,11 +14,13 @@
 
 namespace lsmps {
 
+// The rows of particle number t in the visiting order (lsmps_ctx::order;
+// the particle's index where there is none).
 struct MixedRows {
   const float* f32;           // [n][36]
-  const double* f64;          // [n][36], valid where flag[i] != 0
+  const double* f64;          // [n][36], valid where flag[t] != 0
   const uint8_t* flag;        // [n]
-  const int32_t* list;        // the flagged particles, *count of them
+  const int32_t* list;        // the flagged visiting positions, *count of them
   const unsigned int* count;
 };
 
@@ -27,7 +29,7 @@ inline MixedRows mixed_rows_of(const lsmps_ctx* ctx, int kind) {
                    ctx->mixed_count ? ctx->mixed_count + kind : nullptr};
 }
 
-// Row t (0..3) of particle i as floats (particles without the flag).  A
+// Row t (0..3) at visiting position i as floats (positions without the flag).  A
 // particle's 36 floats start on 16 bytes: row 0 is read as two float4 and
 // one float.
 __device__ __forceinline__ void load_row9f(const MixedRows& r, index_t i, int t, float out[9]) {
@@ -44,7 +46,7 @@ __device__ __forceinline__ void load_row9f(const MixedRows& r, index_t i, int t,
   for (int c = 0; c < 9; ++c) out[c] = p[c];
 }
 
-// Rows 1, 2, 3 of particle i (floats 9..35) as g[0..26]: read as seven
+// Rows 1, 2, 3 at visiting position i (floats 9..35) as g[0..26]: read as seven
 // float4 over floats 8..35 (16-byte aligned), the first value dropped.
 __device__ __forceinline__ void load_rows123f(const MixedRows& r, index_t i, float g[27]) {
   const float4* p = reinterpret_cast<const float4*>(r.f32 + static_cast<size_t>(i) * 36 + 8);
@@ -108,7 +110,7 @@ __device__ __forceinline__ float dot9f(const float a[9], const float b[9]) {
   return v;
 }
 
-// Row t (0..3) of particle i as doubles.
+// Row t (0..3) of the particle at visiting position i as doubles.
 __device__ __forceinline__ void load_row9(const MixedRows& r, index_t i, int t, double out[9]) {
   const size_t base = static_cast<size_t>(i) * 36 + t * 9;
   if (r.flag[i]) {

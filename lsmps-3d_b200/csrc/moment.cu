@@ -753,9 +753,11 @@ struct MixedRowArgs {
   double wall_scale;
   double kappa_threshold;
   KindOut k[2];       // velocity Dirichlet-A, pressure Neumann-A
-  float* rows[2];     // compact FP32 rows per kind (unless Full)
-  double* rows64[2];  // compact FP64 rows of the FP64-route particles (unless Full)
-  uint8_t* flag[2];   // 1 where rows64 holds the particle's rows (unless Full)
+  // compact rows per kind (unless Full), by visiting position: FP32, the
+  // FP64 ones of the FP64-route particles, and 1 where rows64 holds them
+  float* rows[2];
+  double* rows64[2];
+  uint8_t* flag[2];
   int32_t* list[2];   // the FP64-route particles' visiting positions, appended (unless Full)
   unsigned int* count;
   DeviceStatus* status;
@@ -868,8 +870,8 @@ __device__ __forceinline__ double target(int t, int r) {
 }
 
 template <bool Full>
-__device__ __forceinline__ void store_target(const MixedRowArgs& a, int kind, index_t i, int t, const double (&y)[9],
-                                             bool fp64) {
+__device__ __forceinline__ void store_target(const MixedRowArgs& a, int kind, index_t i, index_t vt, int t,
+                                             const double (&y)[9], bool fp64) {
   if (Full) {
     double* out = a.k[kind].inverse + static_cast<size_t>(i) * 81;
 #pragma unroll
@@ -879,11 +881,11 @@ __device__ __forceinline__ void store_target(const MixedRowArgs& a, int kind, in
       out[t + r * 9] = y[r];
     }
   } else if (fp64) {
-    double* out = a.rows64[kind] + static_cast<size_t>(i) * 36 + t * 9;
+    double* out = a.rows64[kind] + static_cast<size_t>(vt) * 36 + t * 9;
 #pragma unroll
     for (int r = 0; r < 9; ++r) out[r] = y[r];
   } else {
-    float* out = a.rows[kind] + static_cast<size_t>(i) * 36 + t * 9;
+    float* out = a.rows[kind] + static_cast<size_t>(vt) * 36 + t * 9;
 #pragma unroll
     for (int r = 0; r < 9; ++r) out[r] = static_cast<float>(y[r]);
   }
@@ -1020,7 +1022,7 @@ __device__ __forceinline__ void mixed_rows_of_particle(const MixedRowArgs& a, in
           double y[9];
 #pragma unroll
           for (int r = 0; r < 9; ++r) y[r] = static_cast<double>(y0[g][r]) + static_cast<double>(d[g][r]);
-          store_target<Full>(a, kind, i, t0 + g, y, false);
+          store_target<Full>(a, kind, i, vt, t0 + g, y, false);
         }
       } else {
         // The group's rows are adjacent in the particle's 36 floats (144
@@ -1035,7 +1037,7 @@ __device__ __forceinline__ void mixed_rows_of_particle(const MixedRowArgs& a, in
           for (int r = 0; r < 9; ++r)
             f[g * 9 + r] = static_cast<float>(static_cast<double>(y0[g][r]) + static_cast<double>(d[g][r]));
         }
-        float* base = a.rows[kind] + static_cast<size_t>(i) * 36 + t0 * 9;
+        float* base = a.rows[kind] + static_cast<size_t>(vt) * 36 + t0 * 9;
         if (t0 == 0) {
           float4* out4 = reinterpret_cast<float4*>(base);
 #pragma unroll
@@ -1051,7 +1053,7 @@ __device__ __forceinline__ void mixed_rows_of_particle(const MixedRowArgs& a, in
     ko.trace[i] = trace;
     ko.reg[i] = reg;
     ko.info[i] = 0;
-    if (!Full) a.flag[kind][i] = 0;
+    if (!Full) a.flag[kind][vt] = 0;
     return;
   }
   // FP64 route: the matrix is re-assembled in FP64 from the particle's rows
@@ -1077,7 +1079,7 @@ __device__ __forceinline__ void mixed_rows_of_particle(const MixedRowArgs& a, in
   ko.trace[i] = trace;
   ko.reg[i] = reg;
   if (!Full) {
-    a.flag[kind][i] = 1;
+    a.flag[kind][vt] = 1;
     a.list[kind][atomicAdd(&a.count[kind], 1u)] = vt;
   }
   double l64[45];
@@ -1089,7 +1091,7 @@ __device__ __forceinline__ void mixed_rows_of_particle(const MixedRowArgs& a, in
     double nan9[9];
 #pragma unroll
     for (int r = 0; r < 9; ++r) nan9[r] = __longlong_as_double(0x7ff8000000000000LL);
-    for (int t = 0; t < kTargets; ++t) store_target<Full>(a, kind, i, t, nan9, true);
+    for (int t = 0; t < kTargets; ++t) store_target<Full>(a, kind, i, vt, t, nan9, true);
     atomicAdd(&a.status->non_spd, 1u);
     raise_flag(a.status, kFlagNonSpd);
     return;
@@ -1102,7 +1104,7 @@ __device__ __forceinline__ void mixed_rows_of_particle(const MixedRowArgs& a, in
 #pragma unroll
     for (int r = 0; r < 9; ++r) y[r] = target<Full>(t, r);
     chol_solve(l64, dinv64, y);
-    store_target<Full>(a, kind, i, t, y, true);
+    store_target<Full>(a, kind, i, vt, t, y, true);
   }
 }
 

@@ -228,7 +228,8 @@ __global__ void __launch_bounds__(kThreads) ppe_kernel(PpeArgs a) {
 // diagonal (minus the sum of the off-diagonal values) and the RHS sums stay
 // FP64.
 template <int G, bool Mixed>
-__device__ __forceinline__ void ppe_row(const PpeArgs& a, index_t i, index_t self, int l, bool write_offsets) {
+__device__ __forceinline__ void ppe_row(const PpeArgs& a, index_t i, index_t vt, int l, bool write_offsets) {
+  const index_t self = self_of(a.sorted, vt, i);
   const index_t n = static_cast<index_t>(a.fluid.count);
   const index_t nb = a.fo[i], ne = a.fo[i + 1];
   const index_t row = i + nb;
@@ -262,7 +263,7 @@ __device__ __forceinline__ void ppe_row(const PpeArgs& a, index_t i, index_t sel
   if (l == 0) {
     double Lr[9];
     if (Mixed) {
-      load_row9(a.prows, i, 0, Lr);
+      load_row9(a.prows, vt, 0, Lr);
     } else {
       const double* __restrict__ pinv = a.pinv + static_cast<size_t>(i) * 81;
 #pragma unroll
@@ -280,9 +281,9 @@ __device__ __forceinline__ void ppe_row(const PpeArgs& a, index_t i, index_t sel
   // up to rounding, with one accumulator instead of 27.
   double gx[9], gy[9], gz[9], b[9];
   if (Mixed) {
-    load_row9(a.vrows, i, 1, gx);
-    load_row9(a.vrows, i, 2, gy);
-    load_row9(a.vrows, i, 3, gz);
+    load_row9(a.vrows, vt, 1, gx);
+    load_row9(a.vrows, vt, 2, gy);
+    load_row9(a.vrows, vt, 3, gz);
   } else {
     const double* __restrict__ vinv = a.vinv + static_cast<size_t>(i) * 81;
 #pragma unroll
@@ -359,7 +360,7 @@ __global__ void __launch_bounds__(kThreads, 4) ppe_lanes_kernel(PpeArgs a) {
   // Whole groups leave together, so the shuffles see full groups.
   if (t >= static_cast<index_t>(a.fluid.count)) return;
   const index_t i = visit(a.order, t);
-  ppe_row<G, Mixed>(a, i, self_of(a.sorted, t, i), l, true);
+  ppe_row<G, Mixed>(a, i, t, l, true);
 }
 
 // The mixed form with FP32 arithmetic; the particles whose rows took the
@@ -371,7 +372,8 @@ __global__ void __launch_bounds__(kThreads, 4) ppe_lanes_kernel(PpeArgs a) {
 // FP32 operator rows; the diagonal (minus the sum of the stored off-diagonal
 // values), the divergence sum and the wall Neumann sum accumulate in FP64.
 template <int G>
-__device__ __forceinline__ void ppe_row32(const PpeArgs& a, index_t i, index_t self, int l) {
+__device__ __forceinline__ void ppe_row32(const PpeArgs& a, index_t i, index_t vt, int l) {
+  const index_t self = self_of(a.sorted, vt, i);
   const index_t n = static_cast<index_t>(a.fluid.count);
   const index_t nb = a.fo[i], ne = a.fo[i + 1];
   const index_t row = i + nb;
@@ -379,7 +381,7 @@ __device__ __forceinline__ void ppe_row32(const PpeArgs& a, index_t i, index_t s
     a.row_offsets[i] = row;
     if (i + 1 == n) a.row_offsets[n] = n + ne;
   }
-  if (a.vrows.flag[i] | a.prows.flag[i]) return;  // FP64 rows: ppe_list_kernel
+  if (a.vrows.flag[vt] | a.prows.flag[vt]) return;  // FP64 rows: ppe_list_kernel
   PpeDest d;
   if (!ppe_dest(a, i, row, ne - nb, d)) return;  // uniform over the lane group
   const int type = a.fluid.surface_type ? a.fluid.surface_type[i] : LSMPS_SURFACE_INNER;
@@ -411,7 +413,7 @@ __device__ __forceinline__ void ppe_row32(const PpeArgs& a, index_t i, index_t s
   const float* gz = L + 36;
   for (int c = l; c < 36; c += G)
     L[(c / 9) * 12 + c % 9] =
-        c < 9 ? a.prows.f32[static_cast<size_t>(i) * 36 + c] : a.vrows.f32[static_cast<size_t>(i) * 36 + c];
+        c < 9 ? a.prows.f32[static_cast<size_t>(vt) * 36 + c] : a.vrows.f32[static_cast<size_t>(vt) * 36 + c];
   __syncwarp(group_mask<G>());
   float b[9];
   const double uxi = a.tvx[i], uyi = a.tvy[i], uzi = a.tvz[i];
@@ -484,7 +486,7 @@ __global__ void __launch_bounds__(kThreads, 7) ppe32_kernel(PpeArgs a) {
   const int l = threadIdx.x & (G - 1);
   if (t >= static_cast<index_t>(a.fluid.count)) return;
   const index_t i = visit(a.order, t);
-  ppe_row32<G>(a, i, self_of(a.sorted, t, i), l);
+  ppe_row32<G>(a, i, t, l);
 }
 
 // The rows of the FP64-route particles (FP64 arithmetic, ppe_row<G, true>):
@@ -500,8 +502,8 @@ __global__ void __launch_bounds__(kThreads, 4) ppe_list_kernel(PpeArgs a) {
   for (index_t t = g0; t < nv + np; t += groups) {
     const index_t vt = t < nv ? a.vrows.list[t] : a.prows.list[t - nv];  // a visiting position
     const index_t i = visit(a.order, vt);
-    if (t >= nv && a.vrows.flag[i]) continue;
-    ppe_row<G, true>(a, i, self_of(a.sorted, vt, i), l, false);
+    if (t >= nv && a.vrows.flag[vt]) continue;
+    ppe_row<G, true>(a, i, vt, l, false);
   }
 }
 

@@ -48,8 +48,9 @@ struct LaplacianArgs {
 // entries l, l + G, ... of both rows and the groups' partial sums are added
 // with shuffles (a rounding-level reassociation for G > 1).
 template <bool Mixed, int G>
-__device__ __forceinline__ void laplacian_of(const LaplacianArgs& a, const MixedRows& rows, index_t i, index_t self,
+__device__ __forceinline__ void laplacian_of(const LaplacianArgs& a, const MixedRows& rows, index_t i, index_t vt,
                                              int l) {
+  const index_t self = self_of(a.sorted, vt, i);
   const double4 pi = ld4(a.fp, self);
   const double4 ui = ld4(a.fv, self);
   // The particle's Laplacian row L (the sum of the inverse's rows 3..5, or
@@ -59,7 +60,7 @@ __device__ __forceinline__ void laplacian_of(const LaplacianArgs& a, const Mixed
   // three accumulators instead of 27.
   double L[9];
   if (Mixed) {
-    load_row9(rows, i, 0, L);
+    load_row9(rows, vt, 0, L);
   } else {
     const double* __restrict__ inv = a.inverse + static_cast<size_t>(i) * 81;
 #pragma unroll
@@ -129,7 +130,7 @@ __global__ void __launch_bounds__(kThreads, 5) laplacian_kernel(LaplacianArgs a,
   const int l = threadIdx.x & (G - 1);
   if (t >= a.n) return;  // the whole group
   const index_t i = visit(a.order, t);
-  laplacian_of<Mixed, G>(a, rows, i, self_of(a.sorted, t, i), l);
+  laplacian_of<Mixed, G>(a, rows, i, t, l);
 }
 
 // Mixed form with FP32 arithmetic: each neighbour's offset is formed in FP64
@@ -143,13 +144,13 @@ __global__ void __launch_bounds__(kThreads, 7) laplacian32_kernel(LaplacianArgs 
   const int l = threadIdx.x & (G - 1);
   if (t >= a.n) return;  // the whole group
   const index_t i = visit(a.order, t);
-  if (rows.flag[i]) return;
+  if (rows.flag[t]) return;
   const index_t self = self_of(a.sorted, t, i);
   const double4 pi = ld4(a.fp, self);
   const double4 ui = ld4(a.fv, self);
   // the Laplacian row in registers (9 floats)
   float L[9];
-  load_row9f(rows, i, 0, L);
+  load_row9f(rows, t, 0, L);
   float b[9];
   double cx = 0.0, cy = 0.0, cz = 0.0;
   const index_t fe = a.fo[i + 1];
@@ -208,7 +209,7 @@ __global__ void __launch_bounds__(kThreads, 5) laplacian_list_kernel(LaplacianAr
   for (index_t t = static_cast<index_t>((blockIdx.x * blockDim.x + threadIdx.x) / G); t < count; t += groups) {
     const index_t vt = rows.list[t];  // a visiting position
     const index_t i = visit(a.order, vt);
-    laplacian_of<true, G>(a, rows, i, self_of(a.sorted, vt, i), l);
+    laplacian_of<true, G>(a, rows, i, vt, l);
   }
 }
 
