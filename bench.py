@@ -348,7 +348,7 @@ def run_ours(args, world, rank, local):
             ctx.set_precision(forms[-1][1])
             ctx.set_condition_threshold(forms[-1][2])
             reset()
-            k_e2e = max(1, min(args.steps, 5))
+            k_e2e = max(1, args.steps)  # the same step count as `value`
             loop = host_loop.HostResidentLoop(ctx, dev, p)
             loop.step()
             loop.sync()
