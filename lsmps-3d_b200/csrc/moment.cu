@@ -427,9 +427,17 @@ __device__ __forceinline__ void finish_a(double (&s)[kMonomials], const MomentPa
                                          index_t i, const double4& pi, double* stage = nullptr,
                                          int stride = kWarp, unsigned active = 0u) {
   const index_t wb = a.wo[i], we = a.wo[i + 1];
-  if (B == 1) {
+  // The wall loops load the next wall's record(s) while this one is used,
+  // with the index one further ahead.
+  if (B == 1 && wb < we) {
+    double4 qn = ld4(a.wp, a.wi[wb]);
+    index_t jnn = wb + 1 < we ? a.wi[wb + 1] : 0;
     for (index_t o = wb; o < we; ++o) {
-      const double4 q = ld4(a.wp, a.wi[o]);
+      const double4 q = qn;
+      if (o + 1 < we) {
+        qn = ld4(a.wp, jnn);
+        if (o + 2 < we) jnn = a.wi[o + 2];
+      }
       const double dx = q.x - pi.x, dy = q.y - pi.y, dz = q.z - pi.z;
       const double d2 = dx * dx + dy * dy + dz * dz;
       if (d2 <= 0.0) continue;
@@ -444,17 +452,24 @@ __device__ __forceinline__ void finish_a(double (&s)[kMonomials], const MomentPa
 #pragma unroll
     for (int c = 0; c <= r; ++c) m[tri(r, c)] = s[entry_slot(r, c)];
   }
-  if (B == 2) {
+  if (B == 2 && wb < we) {
     double q9[9];
+    index_t jn = a.wi[wb];
+    index_t jnn = wb + 1 < we ? a.wi[wb + 1] : 0;
+    double4 qn = ld4(a.wp, jn), nn = ld4(a.wn, jn);
     for (index_t o = wb; o < we; ++o) {
-      const index_t j = a.wi[o];
-      const double4 q = ld4(a.wp, j);
+      const double4 q = qn, nrm = nn;
+      if (o + 1 < we) {
+        jn = jnn;
+        qn = ld4(a.wp, jn);
+        nn = ld4(a.wn, jn);
+        if (o + 2 < we) jnn = a.wi[o + 2];
+      }
       const double dx = q.x - pi.x, dy = q.y - pi.y, dz = q.z - pi.z;
       const double d2 = dx * dx + dy * dy + dz * dz;
       if (d2 <= 0.0) continue;
       const double w = a.wall_scale * (1.0 - sqrt(d2) * a.inv_re);
       if (w <= 0.0) continue;
-      const double4 nrm = ld4(a.wn, j);
       neumann<9>(dx, dy, dz, nrm.x, nrm.y, nrm.z, a.inv_re, q9);
       add_outer<9>(m, q9, w);
     }
@@ -898,9 +913,17 @@ __device__ __forceinline__ void store_target(const MixedRowArgs& a, int kind, in
 __device__ __forceinline__ double assemble_kind(const MixedRowArgs& a, int kind, index_t i, const double4& pi,
                                                 double (&s)[kMonomials], double* m, double* reg) {
   const index_t wb = a.wo[i], we = a.wo[i + 1];
-  if (kind == 0) {
+  // The wall loops load the next wall's record(s) while this one is used,
+  // with the index one further ahead.
+  if (kind == 0 && wb < we) {
+    double4 qn = ld4(a.wp, a.wi[wb]);
+    index_t jnn = wb + 1 < we ? a.wi[wb + 1] : 0;
     for (index_t o = wb; o < we; ++o) {
-      const double4 q = ld4(a.wp, a.wi[o]);
+      const double4 q = qn;
+      if (o + 1 < we) {
+        qn = ld4(a.wp, jnn);
+        if (o + 2 < we) jnn = a.wi[o + 2];
+      }
       const double dx = q.x - pi.x, dy = q.y - pi.y, dz = q.z - pi.z;
       const double d2 = dx * dx + dy * dy + dz * dz;
       if (d2 <= 0.0) continue;
@@ -915,22 +938,53 @@ __device__ __forceinline__ double assemble_kind(const MixedRowArgs& a, int kind,
     for (int c = 0; c <= r; ++c) m[tri(r, c) * kRowThreads] = s[entry_slot(r, c)];
   }
   if (kind == 1) {
-    double q9[9];
+    // The wall terms w q q^T in row order, two walls per pass over the 45
+    // entries in shared memory (each entry gets the first wall's term, then
+    // the second's: the same sums as one wall per pass, half the traffic).
+    double qa[9], qb[9], wa = 0.0;
+    bool held = false;
+    index_t jn = wb < we ? a.wi[wb] : 0;
+    index_t jnn = wb + 1 < we ? a.wi[wb + 1] : 0;
+    double4 qn = make_double4(0.0, 0.0, 0.0, 0.0), nn = qn;
+    if (wb < we) {
+      qn = ld4(a.wp, jn);
+      nn = ld4(a.wn, jn);
+    }
     for (index_t o = wb; o < we; ++o) {
-      const index_t j = a.wi[o];
-      const double4 q = ld4(a.wp, j);
+      const double4 q = qn, nrm = nn;
+      if (o + 1 < we) {
+        jn = jnn;
+        qn = ld4(a.wp, jn);
+        nn = ld4(a.wn, jn);
+        if (o + 2 < we) jnn = a.wi[o + 2];
+      }
       const double dx = q.x - pi.x, dy = q.y - pi.y, dz = q.z - pi.z;
       const double d2 = dx * dx + dy * dy + dz * dz;
       if (d2 <= 0.0) continue;
       const double w = a.wall_scale * (1.0 - sqrt(d2) * a.inv_re);
       if (w <= 0.0) continue;
-      const double4 nrm = ld4(a.wn, j);
-      neumann<9>(dx, dy, dz, nrm.x, nrm.y, nrm.z, a.inv_re, q9);
+      if (!held) {
+        neumann<9>(dx, dy, dz, nrm.x, nrm.y, nrm.z, a.inv_re, qa);
+        wa = w;
+        held = true;
+        continue;
+      }
+      neumann<9>(dx, dy, dz, nrm.x, nrm.y, nrm.z, a.inv_re, qb);
 #pragma unroll
       for (int r = 0; r < 9; ++r) {
-        const double wr = w * q9[r];
+        const double war = wa * qa[r], wbr = w * qb[r];
 #pragma unroll
-        for (int c = 0; c <= r; ++c) m[tri(r, c) * kRowThreads] = fma(wr, q9[c], m[tri(r, c) * kRowThreads]);
+        for (int c = 0; c <= r; ++c)
+          m[tri(r, c) * kRowThreads] = fma(wbr, qb[c], fma(war, qa[c], m[tri(r, c) * kRowThreads]));
+      }
+      held = false;
+    }
+    if (held) {
+#pragma unroll
+      for (int r = 0; r < 9; ++r) {
+        const double war = wa * qa[r];
+#pragma unroll
+        for (int c = 0; c <= r; ++c) m[tri(r, c) * kRowThreads] = fma(war, qa[c], m[tri(r, c) * kRowThreads]);
       }
     }
   }
