@@ -559,29 +559,42 @@ __device__ __forceinline__ void gradient_shifting_of(const GatherArgs& a, const 
     }
   }
   const index_t we = a.wo[i + 1];
-  for (index_t o = a.wo[i] + l; o < we; o += G) {
-    const index_t j = a.wi[o];
-    const double4 q = ld4(a.wp, j), nrm = ld4(a.wn, j);
-    const double dx = q.x - xi, dy = q.y - yi, dz = q.z - zi;
-    const double d = sqrt(dx * dx + dy * dy + dz * dz);
-    const double wnx = nrm.x, wny = nrm.y, wnz = nrm.z;
-    if (do_grad) {
-      const double w = wall_scale * correction_weight_mul(d, inv_re);
-      if (w > 0.0) {
-        double q[9];
-        neumann_a(dx, dy, dz, wnx, wny, wnz, inv_re, q);
-        const double ng = a.p.gravity[0] * wnx + a.p.gravity[1] * wny + a.p.gravity[2] * wnz;
-        const double wr = re * a.p.density * ng;
-#pragma unroll
-        for (int r = 0; r < 9; ++r) rhs[r] = fma(w * q[r], wr, rhs[r]);
+  {  // the next wall's records are loaded while this one is used
+    index_t o = a.wo[i] + l;
+    index_t jn = o < we ? a.wi[o] : 0;
+    double4 qn = make_double4(0.0, 0.0, 0.0, 0.0), nrmn = qn;
+    if (o < we) {
+      qn = ld4(a.wp, jn);
+      nrmn = ld4(a.wn, jn);
+    }
+    for (; o < we; o += G) {
+      const double4 q = qn, nrm = nrmn;
+      if (o + G < we) {
+        jn = a.wi[o + G];
+        qn = ld4(a.wp, jn);
+        nrmn = ld4(a.wn, jn);
       }
-    }
-    if (do_shift && d > 0.0 && d < dmin) {
-      const double push = scale * (dmin - d);
-      shx = fma(push, wnx, shx);
-      shy = fma(push, wny, shy);
-      shz = fma(push, wnz, shz);
-    }
+      const double dx = q.x - xi, dy = q.y - yi, dz = q.z - zi;
+      const double d = sqrt(dx * dx + dy * dy + dz * dz);
+      const double wnx = nrm.x, wny = nrm.y, wnz = nrm.z;
+      if (do_grad) {
+        const double w = wall_scale * correction_weight_mul(d, inv_re);
+        if (w > 0.0) {
+          double q[9];
+          neumann_a(dx, dy, dz, wnx, wny, wnz, inv_re, q);
+          const double ng = a.p.gravity[0] * wnx + a.p.gravity[1] * wny + a.p.gravity[2] * wnz;
+          const double wr = re * a.p.density * ng;
+#pragma unroll
+          for (int r = 0; r < 9; ++r) rhs[r] = fma(w * q[r], wr, rhs[r]);
+        }
+      }
+      if (do_shift && d > 0.0 && d < dmin) {
+        const double push = scale * (dmin - d);
+        shx = fma(push, wnx, shx);
+        shy = fma(push, wny, shy);
+        shz = fma(push, wnz, shz);
+      }
+  }
   }
   if (G > 1) {
     const unsigned gm = group_mask<G>();
@@ -754,31 +767,44 @@ __global__ void __launch_bounds__(kThreads, 6) gradient32_kernel(GatherArgs a, G
   const float wscale = static_cast<float>(out.wall_scale);
   const float wr = static_cast<float>(out.re * a.p.density);
   const index_t we = a.wo[i + 1];
-  for (index_t o = a.wo[i] + l; o < we; o += G) {
-    const index_t j = a.wi[o];
-    const double4 q = ld4(a.wp, j), nrm = ld4(a.wn, j);
-    const double dx = q.x - own.x, dy = q.y - own.y, dz = q.z - own.z;
-    const float w = wscale * basis_f32(dx, dy, dz, inv_re, b);
-    const float s2 = b[3] + b[4] + b[5];
-    const float nxf = static_cast<float>(nrm.x), nyf = static_cast<float>(nrm.y), nzf = static_cast<float>(nrm.z);
-    if (w > 0.0f && s2 > 0.0f) {
-      // wall Neumann vector (moment_matrix.cu:177-201) of the scaled offset
-      const float q9[9] = {nxf, nyf, nzf, 2.0f * b[0] * nxf, 2.0f * b[1] * nyf, 2.0f * b[2] * nzf,
-                           fmaf(b[1], nxf, b[0] * nyf), fmaf(b[2], nyf, b[1] * nzf), fmaf(b[0], nzf, b[2] * nxf)};
-      const float ng = static_cast<float>(a.p.gravity[0] * nrm.x + a.p.gravity[1] * nrm.y + a.p.gravity[2] * nrm.z);
-      const float wq = w * wr * ng;
-#pragma unroll
-      for (int r = 0; r < 9; ++r) rhs[r] = fmaf(wq, q9[r], rhs[r]);
+  {  // the next wall's records are loaded while this one is used
+    index_t o = a.wo[i] + l;
+    index_t jn = o < we ? a.wi[o] : 0;
+    double4 qn = make_double4(0.0, 0.0, 0.0, 0.0), nrmn = qn;
+    if (o < we) {
+      qn = ld4(a.wp, jn);
+      nrmn = ld4(a.wn, jn);
     }
-    if (do_shift && s2 < dmin_s2) {
-      const double d = sqrt(dx * dx + dy * dy + dz * dz);
-      if (d > 0.0 && d < dmin) {
-        const double push = scale * (dmin - d);
-        shx = fma(push, nrm.x, shx);
-        shy = fma(push, nrm.y, shy);
-        shz = fma(push, nrm.z, shz);
+    for (; o < we; o += G) {
+      const double4 q = qn, nrm = nrmn;
+      if (o + G < we) {
+        jn = a.wi[o + G];
+        qn = ld4(a.wp, jn);
+        nrmn = ld4(a.wn, jn);
       }
-    }
+      const double dx = q.x - own.x, dy = q.y - own.y, dz = q.z - own.z;
+      const float w = wscale * basis_f32(dx, dy, dz, inv_re, b);
+      const float s2 = b[3] + b[4] + b[5];
+      const float nxf = static_cast<float>(nrm.x), nyf = static_cast<float>(nrm.y), nzf = static_cast<float>(nrm.z);
+      if (w > 0.0f && s2 > 0.0f) {
+        // wall Neumann vector (moment_matrix.cu:177-201) of the scaled offset
+        const float q9[9] = {nxf, nyf, nzf, 2.0f * b[0] * nxf, 2.0f * b[1] * nyf, 2.0f * b[2] * nzf,
+                             fmaf(b[1], nxf, b[0] * nyf), fmaf(b[2], nyf, b[1] * nzf), fmaf(b[0], nzf, b[2] * nxf)};
+        const float ng = static_cast<float>(a.p.gravity[0] * nrm.x + a.p.gravity[1] * nrm.y + a.p.gravity[2] * nrm.z);
+        const float wq = w * wr * ng;
+#pragma unroll
+        for (int r = 0; r < 9; ++r) rhs[r] = fmaf(wq, q9[r], rhs[r]);
+      }
+      if (do_shift && s2 < dmin_s2) {
+        const double d = sqrt(dx * dx + dy * dy + dz * dz);
+        if (d > 0.0 && d < dmin) {
+          const double push = scale * (dmin - d);
+          shx = fma(push, nrm.x, shx);
+          shy = fma(push, nrm.y, shy);
+          shz = fma(push, nrm.z, shz);
+        }
+      }
+  }
   }
   double rd[9];
 #pragma unroll

@@ -451,21 +451,36 @@ __device__ __forceinline__ void ppe_row32(const PpeArgs& a, index_t i, index_t v
   const index_t we = a.wo[i + 1];
   const float vws = static_cast<float>(a.vwall_scale);
   const float pws = static_cast<float>(2.0 * a.pwall_scale);
-  for (index_t o = a.wo[i] + l; o < we; o += G) {
-    const index_t j = a.wi[o];
-    const double4 q = ld4(a.wp, j), u = ld4(a.wu, j), nrm = ld4(a.wn, j);
-    const float w = basis_f32(q.x - pi.x, q.y - pi.y, q.z - pi.z, a.inv_re, b);
-    if (w <= 0.0f) continue;
-    const float dux = static_cast<float>(u.x - uxi), duy = static_cast<float>(u.y - uyi),
-                duz = static_cast<float>(u.z - uzi);
-    const float cx = dot9f_a16(gx, b), cy = dot9f_a16(gy, b), cz = dot9f_a16(gz, b);
-    dsum += static_cast<double>(vws * w * fmaf(cx, dux, fmaf(cy, duy, cz * duz)));
-    const float nx = static_cast<float>(nrm.x), ny = static_cast<float>(nrm.y), nz = static_cast<float>(nrm.z);
-    // wall Neumann vector (moment_matrix.cu:177-201) of the scaled offset
-    const float q9[9] = {nx, ny, nz, 2.0f * b[0] * nx, 2.0f * b[1] * ny, 2.0f * b[2] * nz,
-                         fmaf(b[1], nx, b[0] * ny), fmaf(b[2], ny, b[1] * nz), fmaf(b[0], nz, b[2] * nx)};
-    const double ng = a.gx * nrm.x + a.gy * nrm.y + a.gz * nrm.z;
-    wall_rhs += static_cast<double>(pws * w * dot9f_a16(L, q9)) * ng * a.inv_re;
+  {  // the next wall's records are loaded while this one is used
+    index_t o = a.wo[i] + l;
+    index_t jn = o < we ? a.wi[o] : 0;
+    double4 qn = make_double4(0.0, 0.0, 0.0, 0.0), un = qn, nrmn = qn;
+    if (o < we) {
+      qn = ld4(a.wp, jn);
+      un = ld4(a.wu, jn);
+      nrmn = ld4(a.wn, jn);
+    }
+    for (; o < we; o += G) {
+      const double4 q = qn, u = un, nrm = nrmn;
+      if (o + G < we) {
+        jn = a.wi[o + G];
+        qn = ld4(a.wp, jn);
+        un = ld4(a.wu, jn);
+        nrmn = ld4(a.wn, jn);
+      }
+      const float w = basis_f32(q.x - pi.x, q.y - pi.y, q.z - pi.z, a.inv_re, b);
+      if (w <= 0.0f) continue;
+      const float dux = static_cast<float>(u.x - uxi), duy = static_cast<float>(u.y - uyi),
+                  duz = static_cast<float>(u.z - uzi);
+      const float cx = dot9f_a16(gx, b), cy = dot9f_a16(gy, b), cz = dot9f_a16(gz, b);
+      dsum += static_cast<double>(vws * w * fmaf(cx, dux, fmaf(cy, duy, cz * duz)));
+      const float nx = static_cast<float>(nrm.x), ny = static_cast<float>(nrm.y), nz = static_cast<float>(nrm.z);
+      // wall Neumann vector (moment_matrix.cu:177-201) of the scaled offset
+      const float q9[9] = {nx, ny, nz, 2.0f * b[0] * nx, 2.0f * b[1] * ny, 2.0f * b[2] * nz,
+                           fmaf(b[1], nx, b[0] * ny), fmaf(b[2], ny, b[1] * nz), fmaf(b[0], nz, b[2] * nx)};
+      const double ng = a.gx * nrm.x + a.gy * nrm.y + a.gz * nrm.z;
+      wall_rhs += static_cast<double>(pws * w * dot9f_a16(L, q9)) * ng * a.inv_re;
+  }
   }
   const unsigned mask = group_mask<G>();
   diag = group_sum<G>(diag, mask);

@@ -95,21 +95,33 @@ __device__ __forceinline__ void laplacian_of(const LaplacianArgs& a, const Mixed
     cz = fma(s, u.z - ui.z, cz);
   }
   const index_t we = a.wo[i + 1];
-  for (index_t o = a.wo[i] + l; o < we; o += G) {
-    const index_t j = a.wi[o];
-    const double4 q = ld4(a.wp, j);
-    const double4 u = ld4(a.wv, j);
-    const double dx = q.x - pi.x, dy = q.y - pi.y, dz = q.z - pi.z;
-    const double w = a.wall_scale * lin_weight_mul(sqrt(dx * dx + dy * dy + dz * dz), a.inv_re);
-    if (w <= 0.0) continue;
-    basis_a_mul(dx, dy, dz, a.inv_re, b);
-    double lb = 0.0;
+  {  // the next wall's records are loaded while this one is used
+    index_t o = a.wo[i] + l;
+    index_t jn = o < we ? a.wi[o] : 0;
+    double4 qn = make_double4(0.0, 0.0, 0.0, 0.0), un = qn;
+    if (o < we) {
+      qn = ld4(a.wp, jn);
+      un = ld4(a.wv, jn);
+    }
+    for (; o < we; o += G) {
+      const double4 q = qn, u = un;
+      if (o + G < we) {
+        jn = a.wi[o + G];
+        qn = ld4(a.wp, jn);
+        un = ld4(a.wv, jn);
+      }
+      const double dx = q.x - pi.x, dy = q.y - pi.y, dz = q.z - pi.z;
+      const double w = a.wall_scale * lin_weight_mul(sqrt(dx * dx + dy * dy + dz * dz), a.inv_re);
+      if (w <= 0.0) continue;
+      basis_a_mul(dx, dy, dz, a.inv_re, b);
+      double lb = 0.0;
 #pragma unroll
-    for (int r = 0; r < 9; ++r) lb = fma(L[r], b[r], lb);
-    const double s = w * lb;
-    cx = fma(s, u.x - ui.x, cx);
-    cy = fma(s, u.y - ui.y, cy);
-    cz = fma(s, u.z - ui.z, cz);
+      for (int r = 0; r < 9; ++r) lb = fma(L[r], b[r], lb);
+      const double s = w * lb;
+      cx = fma(s, u.x - ui.x, cx);
+      cy = fma(s, u.y - ui.y, cy);
+      cz = fma(s, u.z - ui.z, cz);
+  }
   }
   if (G > 1) {
     const unsigned mask = group_mask<G>();
@@ -175,16 +187,28 @@ __global__ void __launch_bounds__(kThreads, 7) laplacian32_kernel(LaplacianArgs 
   }
   const float wall_scale = static_cast<float>(a.wall_scale);
   const index_t we = a.wo[i + 1];
-  for (index_t o = a.wo[i] + l; o < we; o += G) {
-    const index_t j = a.wi[o];
-    const double4 q = ld4(a.wp, j);
-    const double4 u = ld4(a.wv, j);
-    const float w = wall_scale * basis_f32(q.x - pi.x, q.y - pi.y, q.z - pi.z, a.inv_re, b);
-    if (w <= 0.0f) continue;
-    const double s = static_cast<double>(w * dot9f(L, b));
-    cx = fma(s, u.x - ui.x, cx);
-    cy = fma(s, u.y - ui.y, cy);
-    cz = fma(s, u.z - ui.z, cz);
+  {  // the next wall's records are loaded while this one is used
+    index_t o = a.wo[i] + l;
+    index_t jn = o < we ? a.wi[o] : 0;
+    double4 qn = make_double4(0.0, 0.0, 0.0, 0.0), un = qn;
+    if (o < we) {
+      qn = ld4(a.wp, jn);
+      un = ld4(a.wv, jn);
+    }
+    for (; o < we; o += G) {
+      const double4 q = qn, u = un;
+      if (o + G < we) {
+        jn = a.wi[o + G];
+        qn = ld4(a.wp, jn);
+        un = ld4(a.wv, jn);
+      }
+      const float w = wall_scale * basis_f32(q.x - pi.x, q.y - pi.y, q.z - pi.z, a.inv_re, b);
+      if (w <= 0.0f) continue;
+      const double s = static_cast<double>(w * dot9f(L, b));
+      cx = fma(s, u.x - ui.x, cx);
+      cy = fma(s, u.y - ui.y, cy);
+      cz = fma(s, u.z - ui.z, cz);
+  }
   }
   if (G > 1) {
     const unsigned mask = group_mask<G>();
