@@ -869,10 +869,11 @@ __global__ void __launch_bounds__(kThreads, 6) gradient32_kernel(GatherArgs a, G
 // updated state and the walls, so running it right after the update in the
 // same thread gives the same result as the two reference kernels.
 __global__ void __launch_bounds__(kThreads) update_anti_penetration_kernel(
-    lsmps_fluid f, lsmps_walls w, const index_t* __restrict__ wo, const index_t* __restrict__ wi,
+    lsmps_fluid f, const index_t* __restrict__ wo, const index_t* __restrict__ wi,
     const double* __restrict__ tx, const double* __restrict__ ty, const double* __restrict__ tz, double dt_host,
     const double* __restrict__ dtp, double density, const double* __restrict__ gx, const double* __restrict__ gy, const double* __restrict__ gz,
-    const double* __restrict__ sx, const double* __restrict__ sy, const double* __restrict__ sz, double clearance) {
+    const double* __restrict__ sx, const double* __restrict__ sy, const double* __restrict__ sz, double clearance,
+    const double4* __restrict__ wp, const double4* __restrict__ wn) {
   const index_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= static_cast<index_t>(f.count)) return;
   const double dt = dtp ? *dtp : dt_host;
@@ -889,12 +890,21 @@ __global__ void __launch_bounds__(kThreads) update_anti_penetration_kernel(
   x += 0.5 * dt * (ox + vx) + sx[i];
   y += 0.5 * dt * (oy + vy) + sy[i];
   z += 0.5 * dt * (oz + vz) + sz[i];
-  if (clearance > 0.0) {
-    const index_t we = wo[i + 1];
-    for (index_t o = wo[i]; o < we; ++o) {
-      const index_t j = wi[o];
-      const double nx = w.normal_x[j], ny = w.normal_y[j], nz = w.normal_z[j];
-      const double sd = (x - w.x[j]) * nx + (y - w.y[j]) * ny + (z - w.z[j]) * nz;
+  if (clearance > 0.0 && wo[i] < wo[i + 1]) {
+    // the wall records {x, y, z, -} and {nx, ny, nz, -}, the next wall's
+    // loaded while this one is applied (in row order)
+    const index_t wb = wo[i], we = wo[i + 1];
+    index_t jn = wi[wb];
+    double4 qn = ld4(wp, jn), nn = ld4(wn, jn);
+    for (index_t o = wb; o < we; ++o) {
+      const double4 q = qn, nrm = nn;
+      if (o + 1 < we) {
+        jn = wi[o + 1];
+        qn = ld4(wp, jn);
+        nn = ld4(wn, jn);
+      }
+      const double nx = nrm.x, ny = nrm.y, nz = nrm.z;
+      const double sd = (x - q.x) * nx + (y - q.y) * ny + (z - q.z) * nz;
       if (sd >= clearance) continue;
       const double c = clearance - sd;
       x += c * nx;
@@ -1016,12 +1026,13 @@ lsmps_status pressure_correction_impl(lsmps_ctx* ctx, const lsmps_fluid& f, cons
   st = gradient_shifting_stage(ctx, f, w, fn, wn, pressure, p, pm, g, s, mixed);
   if (st) return st;
   const int blocks = div_up(static_cast<long long>(f.count), kThreads);
-  launch(ctx, update_anti_penetration_kernel, dim3(blocks), dim3(kThreads), 0, f, w,
+  launch(ctx, update_anti_penetration_kernel, dim3(blocks), dim3(kThreads), 0, f,
          static_cast<const index_t*>(wn.offsets), static_cast<const index_t*>(wn.indices),
          static_cast<const double*>(t.vx), static_cast<const double*>(t.vy), static_cast<const double*>(t.vz),
          p.time_step, ctx->device_dt, p.density, static_cast<const double*>(g.x), static_cast<const double*>(g.y),
          static_cast<const double*>(g.z), static_cast<const double*>(s.x), static_cast<const double*>(s.y),
-         static_cast<const double*>(s.z), p.wall_clearance_ratio * p.particle_spacing);
+         static_cast<const double*>(s.z), p.wall_clearance_ratio * p.particle_spacing,
+         static_cast<const double4*>(ctx->pack_wall[0]), static_cast<const double4*>(ctx->pack_wall[2]));
   st = check_launch(ctx, "gradient/shifting, update/anti-penetration");
   if (!st) st = smooth_impl(ctx, f, fn, p, sm, true);
   return st;

@@ -39,32 +39,21 @@ struct Basis3 {
   double x[3], y[3], z[3];
 };
 
-// add_wall_basis_direction, surface_detection.cu:123-149.  The loops run
-// over the three slots with compile-time indices (a slot is used below
-// b.count), so the basis stays in registers; the arithmetic and its order
-// are the reference's.
+// add_wall_basis_direction, surface_detection.cu:123-149
 __device__ __forceinline__ void add_direction(Basis3& b, double x, double y, double z, double thr) {
   double rx = x, ry = y, rz = z;
-#pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    if (k < b.count) {
-      const double proj = rx * b.x[k] + ry * b.y[k] + rz * b.z[k];
-      rx -= proj * b.x[k];
-      ry -= proj * b.y[k];
-      rz -= proj * b.z[k];
-    }
+  for (int k = 0; k < b.count; ++k) {
+    const double proj = rx * b.x[k] + ry * b.y[k] + rz * b.z[k];
+    rx -= proj * b.x[k];
+    ry -= proj * b.y[k];
+    rz -= proj * b.z[k];
   }
   const double len2 = rx * rx + ry * ry + rz * rz;
   if (len2 <= thr * thr || b.count >= 3) return;
   const double inv = safe_rsqrt(len2);
-#pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    if (k == b.count) {
-      b.x[k] = rx * inv;
-      b.y[k] = ry * inv;
-      b.z[k] = rz * inv;
-    }
-  }
+  b.x[b.count] = rx * inv;
+  b.y[b.count] = ry * inv;
+  b.z[b.count] = rz * inv;
   ++b.count;
 }
 
@@ -114,15 +103,9 @@ __global__ void __launch_bounds__(kSurfaceThreads) classify_kernel(SurfaceArgs a
     }
     accumulate(q.x - px, q.y - py, q.z - pz, re, nd, sx, sy, sz, weighted);
   }
-  if (a.p.include_wall_neighbors && wb < we) {
-    double4 wq = ld4(a.wp, a.wi[wb]);
-    index_t wjn = wb + 1 < we ? a.wi[wb + 1] : 0;
+  if (a.p.include_wall_neighbors) {
     for (index_t o = wb; o < we; ++o) {
-      const double4 q = wq;
-      if (o + 1 < we) {
-        wq = ld4(a.wp, wjn);
-        if (o + 2 < we) wjn = a.wi[o + 2];
-      }
+      const double4 q = ld4(a.wp, a.wi[o]);
       accumulate(q.x - px, q.y - py, q.z - pz, re, nd, sx, sy, sz, weighted);
     }
   }
@@ -136,35 +119,22 @@ __global__ void __launch_bounds__(kSurfaceThreads) classify_kernel(SurfaceArgs a
     // build_wall_basis, surface_detection.cu:151-197
     Basis3 basis;
     basis.count = 0;
-    index_t jn = wb < we ? a.wi[wb] : 0;
-    index_t jnn = wb + 1 < we ? a.wi[wb + 1] : 0;
-    double4 qn = make_double4(0.0, 0.0, 0.0, 0.0), nn = qn;
-    if (wb < we) {
-      qn = ld4(a.wp, jn);
-      nn = ld4(a.wn, jn);
-    }
     for (index_t o = wb; o < we; ++o) {
-      const double4 q = qn, nrm = nn;
-      if (o + 1 < we) {
-        jn = jnn;
-        qn = ld4(a.wp, jn);
-        nn = ld4(a.wn, jn);
-        if (o + 2 < we) jnn = a.wi[o + 2];
-      }
+      const index_t j = a.wi[o];
+      const double4 q = ld4(a.wp, j);
       const double dx = q.x - px, dy = q.y - py, dz = q.z - pz;
       const double d2 = dx * dx + dy * dy + dz * dz;
       if (d2 <= 0.0) continue;
       const double d = sqrt(d2);
       if (lin_weight(d, re) <= 0.0) continue;
+      const double4 nrm = ld4(a.wn, j);
       const double nx = nrm.x, ny = nrm.y, nz = nrm.z;
       const double nl2 = nx * nx + ny * ny + nz * nz;
       if (nl2 <= 0.0) continue;
       const double inv = safe_rsqrt(nl2);
       add_direction(basis, -nx * inv, -ny * inv, -nz * inv, a.p.wall_normal_independence_threshold);
     }
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      if (k >= basis.count) break;
+    for (int k = 0; k < basis.count; ++k) {
       const double proj = ax * basis.x[k] + ay * basis.y[k] + az * basis.z[k];
       if (proj > 0.0) {
         ax -= proj * basis.x[k];
