@@ -301,7 +301,9 @@ lsmps_status lsmps_ctx_set_cell_order(lsmps_ctx* ctx, int on);
  * kernels read those rows and neighbour records packed in cell order, so the
  * records of a home cell's neighbours lie in a few contiguous runs whatever
  * the caller's particle numbering.  The tables, and every result, are the
- * same either way; 0 reads the rows' indices and records in index order. */
+ * same either way; 0 reads the rows' indices and records in index order.  The
+ * kept rows describe the table as this context built it: a caller that edits
+ * the fluid table's indices before the next step sets 0. */
 lsmps_status lsmps_ctx_set_sorted_rows(lsmps_ctx* ctx, int on);
 /* Copy the first `count` entries of the cell-sorted rows this context holds
  * (of its last build of the fluid table) to device memory `dst`, on the

@@ -75,6 +75,7 @@ bool ensure_packs(lsmps_ctx* ctx, size_t nf, size_t nw) {
   cudaStreamIsCapturing(ctx->stream, &cap);
   if (cap != cudaStreamCaptureStatusNone) return false;
   cudaStreamSynchronize(ctx->stream);
+  ctx->packs_ready = 0;  // new buffers hold nothing a stage could reuse
   if (nf > ctx->pack_fluid_cap) {
     for (auto& p : ctx->pack_fluid) {
       if (p) cudaFree(p);
