@@ -57,6 +57,15 @@ def test_host_only_entry_points(lib, pkg):
             assert a == b, name
 
 
+def test_context_options_reject_a_missing_context(lib, pkg):
+    # Host-side argument checks of the context switches (no device touched).
+    inv = pkg.abi.INVALID_ARGUMENT
+    assert lib.lsmps_ctx_set_sorted_rows(None, 1) == inv
+    assert lib.lsmps_ctx_copy_sorted_rows(None, None, 0) == inv
+    assert lib.lsmps_ctx_set_cell_order(None, 1) == inv
+    assert lib.lsmps_ctx_set_step_events(None, None, None, None) == inv
+
+
 def test_solver_options_default(lib, pkg):
     o = pkg.abi.SolverOptions()
     lib.lsmps_solver_options_default(ctypes.byref(o))
